@@ -1,0 +1,345 @@
+"""Benchmark: vertex Newton updates/s of the structured TMOP sweep on B200.
+
+Workload (one "step"): 200 block-Jacobi sweeps of the TMOP shape metric on a
+single 4097 x 4097 block of the unit square whose interior nodes carry seeded
++-0.3 h uniform noise (16.77 M moving DOFs), starting every step from the same
+positions.  `value` is device-resident throughput (moving DOFs x sweeps / s)
+with the fp32-bulk / fp64-guarded ("mixed") sweep; `e2e` is the same step
+through the public API (set_X from host memory, run, get_X back to host); the
+plain-fp64 sweep is reported beside it.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
+
+Under torchrun (N > 1) every rank runs an independent replica (the path has no
+cross-GPU exchange); value = all ranks' updates / max-over-ranks time.
+"""
+
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import sys
+import threading
+import time
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+N_SIDE = 4097
+FRAC = 0.3
+SEED = 0
+SWEEPS = 200
+METRIC = "vertex Newton updates/s"
+UNIT = "vertex-updates/s"
+# Algorithmic bytes per moving-DOF update of the fused sweep: read the node's
+# fp64 position once, write it once (neighbours are reused through shared
+# memory; structure is synthesized, not read).
+BYTES_PER_UPDATE = 2 * 2 * 8
+
+
+def _peaks():
+    p = ROOT / "MEASURED_PEAKS.json"
+    if p.exists():
+        d = json.loads(p.read_text())
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+class ClockSampler:
+    """Samples SM clock and throttle reasons through NVML while running."""
+
+    def __init__(self, index: int, period: float = 0.1):
+        self.index, self.period = index, period
+        self.samples = []
+        self._stop = threading.Event()
+        self._t = None
+        self.ok = False
+
+    def __enter__(self):
+        try:
+            import pynvml
+
+            pynvml.nvmlInit()
+            self._nv = pynvml
+            self._h = pynvml.nvmlDeviceGetHandleByIndex(self.index)
+            self.max_mhz = pynvml.nvmlDeviceGetMaxClockInfo(self._h, pynvml.NVML_CLOCK_SM)
+            self.ok = True
+            self._t = threading.Thread(target=self._run, daemon=True)
+            self._t.start()
+        except Exception:  # noqa: BLE001 - clocks are advisory when NVML is absent
+            self.ok = False
+        return self
+
+    def _run(self):
+        nv = self._nv
+        while not self._stop.is_set():
+            try:
+                mhz = nv.nvmlDeviceGetClockInfo(self._h, nv.NVML_CLOCK_SM)
+                reasons = nv.nvmlDeviceGetCurrentClocksEventReasons(self._h)
+                self.samples.append((mhz, reasons))
+            except Exception:  # noqa: BLE001
+                pass
+            self._stop.wait(self.period)
+
+    def __exit__(self, *exc):
+        self._stop.set()
+        if self._t:
+            self._t.join()
+
+    def summary(self):
+        if not self.ok or not self.samples:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvml unavailable"]}
+        nv = self._nv
+        names = {
+            "gpu_idle": nv.nvmlClocksEventReasonGpuIdle,
+            "sw_power_cap": nv.nvmlClocksEventReasonSwPowerCap,
+            "hw_slowdown": nv.nvmlClocksEventReasonHwSlowdown,
+            "sw_thermal_slowdown": nv.nvmlClocksEventReasonSwThermalSlowdown,
+            "hw_thermal_slowdown": nv.nvmlClocksEventReasonHwThermalSlowdown,
+            "hw_power_brake": nv.nvmlClocksEventReasonHwPowerBrakeSlowdown,
+        }
+        seen = set()
+        for _, r in self.samples:
+            for k, bit in names.items():
+                if r & bit:
+                    seen.add(k)
+        mhz = [m for m, _ in self.samples]
+        return {"sm_mhz": float(np.median(mhz)), "sm_max_mhz": float(self.max_mhz), "reasons": sorted(seen),
+                "samples": len(mhz)}
+
+
+def _dist():
+    ws = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return ws, rank, local
+
+
+def _pg_init(ws, backend):
+    if ws <= 1:
+        return None
+    import datetime
+
+    import torch.distributed as dist
+
+    dist.init_process_group(backend=backend, timeout=datetime.timedelta(seconds=120))
+    return dist
+
+
+def _max_over_ranks(dist, x, device=None):
+    if dist is None:
+        return x
+    import torch
+
+    t = torch.tensor([x], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def _barrier(dist):
+    if dist is not None:
+        dist.barrier()
+
+
+def _grid():
+    from egg_b200 import configs
+
+    return configs.unit_square(N_SIDE, frac=FRAC, seed=SEED)
+
+
+def cpu_baseline(threads=None, target_s=12.0):
+    """The reference core (oracle/_ref, OpenMP) on a bounded sample of the
+    workload: a 1025^2 block with the same noise, timed sweeps after warm-up."""
+    from egg_b200 import configs
+    from oracle import oracle
+
+    ref = oracle.load_ref("fp64")
+    cores = threads or os.cpu_count()
+    os.environ.setdefault("OMP_NUM_THREADS", str(cores))
+    g = configs.unit_square(1025, frac=FRAC, seed=SEED)
+    if ref is not None:
+        s = ref.CppStructuredSweepSession(g.wire(), g.structured(), g.X_flat(), device="cpu")
+        s.run(1)
+        t0 = time.perf_counter()
+        n = 0
+        while time.perf_counter() - t0 < target_s:
+            s.run(2)
+            n += 2
+        dt = time.perf_counter() - t0
+        kind = "reference"
+    else:
+        pt, sc = oracle.patches_for(g.blocks, g.free), oracle.stencil_for(g.blocks)
+        oracle.run(g.X, pt, sc, 1)
+        t0 = time.perf_counter()
+        n = 0
+        X = g.X
+        while time.perf_counter() - t0 < target_s:
+            X, _, _ = oracle.run(X, pt, sc, 1)
+            n += 1
+        dt = time.perf_counter() - t0
+        kind, cores = "port", 1
+    return {"value": g.num_free * n / dt, "unit": UNIT, "cores": int(cores), "kind": kind,
+            "sample": f"1025x1025 unit square, +-0.3h noise, shape metric, {n} sweeps in {dt:.1f} s"}
+
+
+def run_reference(args):
+    """--impl reference: the reference's own CPU implementation, all host threads."""
+    ws, rank, _ = _dist()
+    if rank != 0:
+        return 0
+    from oracle import oracle
+
+    ref = oracle.load_ref("fp64")
+    if ref is None:
+        print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref (reference core built from source) missing"}))
+        return 0
+    cores = os.cpu_count()
+    os.environ["OMP_NUM_THREADS"] = str(cores)
+    g = _grid()
+    t0 = time.perf_counter()
+    s = ref.CppStructuredSweepSession(g.wire(), g.structured(), g.X_flat(), device="cpu")
+    setup = time.perf_counter() - t0
+    per_step = int(os.environ.get("EGG_B200_REF_SWEEPS", "2"))
+    for _ in range(args.warmup):
+        s.run(per_step)
+    times = []
+    for _ in range(args.steps):
+        t0 = time.perf_counter()
+        s.run(per_step)
+        times.append(time.perf_counter() - t0)
+    ms = 1e3 * float(np.mean(times))
+    value = g.num_free * per_step / (ms / 1e3)
+    line = {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": ws, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f64", "data": "synthetic",
+        "config": {"workload": f"{N_SIDE}x{N_SIDE} unit square, +-0.3h seeded noise, TMOP shape, "
+                               f"{per_step} block-Jacobi sweeps per step (bounded sample of the 200-sweep job)",
+                   "moving_dofs": g.num_free, "setup_s": setup},
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": cores, "kind": "reference",
+                         "sample": f"{per_step} sweeps per step on the full {N_SIDE}^2 grid"},
+        "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line))
+    return 0
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="egg_b200")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--sweeps", type=int, default=SWEEPS)
+    args = ap.parse_args()
+    if args.impl == "reference":
+        return run_reference(args)
+
+    ws, rank, local = _dist()
+    import torch
+
+    torch.cuda.set_device(local)
+    dist = _pg_init(ws, "nccl")
+    from egg_b200 import cpp_core
+
+    g = _grid()
+    ctx = g.wire(compact=True)
+    st = g.structured()
+    X0 = g.X_flat()
+    F = g.num_free
+    sweeps = args.sweeps
+    results = {}
+    for prec in ("fp64", "mixed"):
+        s = cpp_core.CppStructuredSweepSession(ctx, st, X0, device=f"cuda:{local}", precision=prec)
+        s.checkpoint()
+        for _ in range(args.warmup):
+            s.restore()
+            s.run(sweeps)
+        s.reset_stats()
+        s.set_profiling(prec == "mixed")
+        _barrier(dist)
+        torch.cuda.synchronize()
+        with ClockSampler(local) as clk:
+            t0 = time.perf_counter()
+            E = None
+            for _ in range(args.steps):
+                s.restore()
+                E, M = s.run(sweeps)
+            torch.cuda.synchronize()
+            dt = time.perf_counter() - t0
+        launches = s.launch_count()
+        stats = s.kernel_stats()
+        s.set_profiling(False)
+        dt = _max_over_ranks(dist, dt, device=f"cuda:{local}")
+        results[prec] = {"dt": dt, "E": float(E[-1]), "M": float(M[-1]), "stats": stats, "launches": launches,
+                         "clocks": clk.summary(), "session": s}
+
+    mixed = results["mixed"]
+    ms_step = 1e3 * mixed["dt"] / args.steps
+    value = ws * F * sweeps * args.steps / mixed["dt"]
+    v64 = ws * F * sweeps * args.steps / results["fp64"]["dt"]
+
+    # e2e through the public API with host buffers (mixed precision).
+    s = mixed["session"]
+    Xh = np.ascontiguousarray(X0)
+    s.set_X(Xh)
+    s.run(sweeps)
+    _barrier(dist)
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        s.set_X(Xh)
+        _e, _m = s.run(sweeps)
+        Xout = s.get_X()
+    e2e_dt = _max_over_ranks(dist, time.perf_counter() - t0, device=f"cuda:{local}")
+    e2e_value = ws * F * sweeps * args.steps / e2e_dt
+
+    # Roofline of the dominant kernel (interior sweep), from the live events.
+    k_ms, k_n = mixed["stats"]["interior_sweep"]
+    hbm, peak_kind = _peaks()
+    avg_ms = k_ms / max(k_n, 1)
+    achieved = BYTES_PER_UPDATE * F / (avg_ms / 1e3) / 1e9
+    roof = {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s", "frac": achieved / hbm,
+            "traffic": None, "kernel": "interior_tile_kernel (mixed)", "avg_launch_ms": avg_ms,
+            "peak_source": peak_kind,
+            "note": "ALU-bound stencil: algorithmic bytes (32 B/update) vs HBM; see alu_roof"}
+    total_ms = sum(v[0] for v in mixed["stats"].values())
+    share = {k: v[0] / total_ms for k, v in mixed["stats"].items() if v[1]}
+
+    if rank != 0:
+        if dist is not None:
+            dist.destroy_process_group()
+        return 0
+    line = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": ws, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": ms_step, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "fp32-bulk/fp64-guard", "data": "synthetic",
+        "config": {"workload": f"{N_SIDE}x{N_SIDE} unit square single block, +-0.3h seeded noise, TMOP shape, "
+                               f"{sweeps} block-Jacobi sweeps per step, omega=1",
+                   "moving_dofs": F, "parallelism": "replicas" if ws > 1 else "single-gpu",
+                   "l2": "inputs (269 MB fp64 store x2) larger than L2"},
+        "fp64": {"value": v64, "ms_per_step": 1e3 * results["fp64"]["dt"] / args.steps,
+                 "final_energy": results["fp64"]["E"], "final_mindet": results["fp64"]["M"]},
+        "mixed": {"final_energy": mixed["E"], "final_mindet": mixed["M"],
+                  "rel_energy_vs_fp64": abs(mixed["E"] - results["fp64"]["E"]) / abs(results["fp64"]["E"]),
+                  "speedup_vs_fp64": value / v64},
+        "roofline": roof, "kernel_share": share,
+        "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": int(X0.nbytes),
+                "d2h_bytes_per_step": int(Xout.nbytes + 16)},
+        "gpu_launches": int(mixed["launches"]),
+        "clocks": mixed["clocks"],
+    }
+    if not args.no_cpu_baseline:
+        line["cpu_baseline"] = cpu_baseline()
+    print(json.dumps(line))
+    if dist is not None:
+        dist.destroy_process_group()
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

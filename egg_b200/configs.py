@@ -1,0 +1,172 @@
+"""Seeded synthetic multi-block grids for the smoother workloads.
+
+Every generator returns a :class:`Grid` (per-block global-id arrays, positions in
+global node order, the moving-DOF mask).  Positions are built by transfinite
+interpolation of straight/circular block edges and perturbed with
+``numpy.random.default_rng(seed)``; nothing is read from disk.
+
+* :func:`unit_square`   one n x n block on [0,1]^2, interior noise +-frac*h
+  (the 4097^2 +-0.3h sweep workload and its small parity cases).
+* :func:`disk_oh`       unit disk as a 5-block O-H grid: centre square of
+  half-width 0.35 plus four curved blocks to the unit circle; circle fixed,
+  every other node perturbed by +-frac * (local min edge length).
+* :func:`tangled_square` n x n unit square with seeded interior nodes displaced
+  by 0.8-1.5 h in random directions until a target fraction of cells holds an
+  inverted corner sample (the untangling workload).
+"""
+
+from __future__ import annotations
+
+from dataclasses import dataclass, field
+
+import numpy as np
+
+from . import wire as _wire
+
+__all__ = ["Grid", "unit_square", "disk_oh", "tangled_square", "grid_mindet", "mean_size_w_inv"]
+
+
+@dataclass
+class Grid:
+    name: str
+    d: int
+    blocks: list[np.ndarray]
+    X: np.ndarray  # (N, d) float64, global node order
+    free: np.ndarray  # (N,) bool
+    meta: dict = field(default_factory=dict)
+
+    @property
+    def num_nodes(self) -> int:
+        return int(self.X.shape[0])
+
+    @property
+    def num_free(self) -> int:
+        return int(self.free.sum())
+
+    def wire(self, *, w_inv=None, compact: bool = False) -> dict:
+        return _wire.flat_wire(self.blocks, self.free, self.d, w_inv=w_inv, compact=compact)
+
+    def structured(self) -> dict:
+        return _wire.structured_tables(self.blocks)
+
+    def X_flat(self) -> np.ndarray:
+        return np.ascontiguousarray(self.X, dtype=np.float64).ravel()
+
+
+def _min_edge(blocks: list[np.ndarray], X: np.ndarray) -> np.ndarray:
+    """Per-node minimum length of its incident block edges."""
+    h = np.full(X.shape[0], np.inf)
+    for ids in blocks:
+        for ax in range(ids.ndim):
+            a = np.take(ids, range(0, ids.shape[ax] - 1), axis=ax).reshape(-1)
+            b = np.take(ids, range(1, ids.shape[ax]), axis=ax).reshape(-1)
+            ln = np.linalg.norm(X[a] - X[b], axis=1)
+            np.minimum.at(h, a, ln)
+            np.minimum.at(h, b, ln)
+    return h
+
+
+def unit_square(n: int, frac: float = 0.3, seed: int = 0) -> Grid:
+    """One n x n block on the unit square; node (i, j) at (i h, j h)."""
+    ids = np.arange(n * n, dtype=np.int64).reshape(n, n)
+    t = np.linspace(0.0, 1.0, n)
+    X = np.stack(np.meshgrid(t, t, indexing="ij"), axis=-1).reshape(-1, 2).copy()
+    free = np.zeros((n, n), dtype=bool)
+    free[1:-1, 1:-1] = True
+    free = free.reshape(-1)
+    h = 1.0 / (n - 1)
+    rng = np.random.default_rng(seed)
+    if frac > 0:
+        X[free] += rng.uniform(-frac * h, frac * h, size=(int(free.sum()), 2))
+    return Grid(f"square{n}", 2, [ids], X, free, {"h": h, "frac": frac, "seed": seed})
+
+
+def _dedupe(points: list[np.ndarray]):
+    """Global ids for per-block point arrays, merging coincident nodes."""
+    flat = np.concatenate([p.reshape(-1, 2) for p in points])
+    key = np.round(flat * 1e9).astype(np.int64)
+    _, first, inv = np.unique(key, axis=0, return_index=True, return_inverse=True)
+    # Ids in first-appearance order, so block 0 (the centre) numbers first.
+    order = np.argsort(first, kind="stable")
+    rank = np.empty_like(order)
+    rank[order] = np.arange(order.size)
+    gid = rank[inv.reshape(-1)]
+    X = flat[np.sort(first)]
+    blocks, off = [], 0
+    for p in points:
+        m = p.shape[0] * p.shape[1]
+        blocks.append(gid[off : off + m].reshape(p.shape[0], p.shape[1]))
+        off += m
+    return blocks, X
+
+
+def disk_oh(n: int = 65, frac: float = 0.25, seed: int = 0, half_width: float = 0.35) -> Grid:
+    """Unit disk, 5-block O-H topology, every block n x n nodes."""
+    a = half_width
+    s = np.linspace(-a, a, n)
+    sq = np.stack(np.meshgrid(s, s, indexing="ij"), axis=-1)  # (n, n, 2): axis0 = x, axis1 = y
+    u = np.linspace(0.0, 1.0, n)[:, None, None]
+    pts = [sq]
+    # Curved blocks: axis 0 radial (outward), axis 1 counter-clockwise.
+    sides = [
+        (np.stack([np.full(n, a), s], axis=1), -0.25 * np.pi),  # right
+        (np.stack([s[::-1], np.full(n, a)], axis=1), 0.25 * np.pi),  # top
+        (np.stack([np.full(n, -a), s[::-1]], axis=1), 0.75 * np.pi),  # left
+        (np.stack([s, np.full(n, -a)], axis=1), 1.25 * np.pi),  # bottom
+    ]
+    for inner, th0 in sides:
+        th = th0 + np.linspace(0.0, 0.5 * np.pi, n)
+        outer = np.stack([np.cos(th), np.sin(th)], axis=1)
+        pts.append((1.0 - u) * inner[None, :, :] + u * outer[None, :, :])
+    blocks, X = _dedupe(pts)
+    N = X.shape[0]
+    free = np.ones(N, dtype=bool)
+    for b in blocks[1:]:
+        free[b[-1, :]] = False  # circle
+    h = _min_edge(blocks, X)
+    rng = np.random.default_rng(seed)
+    noise = rng.uniform(-1.0, 1.0, size=(N, 2)) * (frac * h)[:, None]
+    X = X + np.where(free[:, None], noise, 0.0)
+    return Grid(f"disk_oh{n}", 2, blocks, X, free, {"frac": frac, "seed": seed, "half_width": a})
+
+
+def grid_mindet(blocks, X, d=2) -> np.ndarray:
+    """det A of every canonical corner sample (energy-stencil order)."""
+    _, gc, gn, sg = _wire.cell_stencil(blocks, d)
+    c0 = sg[0][:, None] * (X[gn[0]] - X[gc])
+    c1 = sg[1][:, None] * (X[gn[1]] - X[gc])
+    return c0[:, 0] * c1[:, 1] - c1[:, 0] * c0[:, 1]
+
+
+def tangled_square(n: int = 1025, target: float = 0.05, seed: int = 0, batch: int | None = None) -> Grid:
+    """n x n unit square with ~``target`` of cells inverted by node displacements."""
+    g = unit_square(n, frac=0.0, seed=seed)
+    h = 1.0 / (n - 1)
+    rng = np.random.default_rng(seed)
+    X = g.X.copy()
+    interior = np.flatnonzero(g.free)
+    order = rng.permutation(interior)
+    ncell = (n - 1) ** 2
+    batch = batch or max(1, ncell // 400)
+    used = 0
+    frac_bad = 0.0
+    while frac_bad < target and used < order.size:
+        pick = order[used : used + batch]
+        used += pick.size
+        r = rng.uniform(0.8, 1.5, size=pick.size) * h
+        th = rng.uniform(0.0, 2.0 * np.pi, size=pick.size)
+        X[pick, 0] += r * np.cos(th)
+        X[pick, 1] += r * np.sin(th)
+        det = grid_mindet(g.blocks, X).reshape(ncell, 4)
+        frac_bad = float((det <= 0).any(axis=1).mean())
+    return Grid(
+        f"tangled{n}", 2, g.blocks, X, g.free,
+        {"h": h, "seed": seed, "displaced": int(used), "inverted_cell_fraction": frac_bad},
+    )
+
+
+def mean_size_w_inv(blocks, X, d=2) -> np.ndarray:
+    """Inverse of the mean-size target W = hbar I (det W = mean det A)."""
+    vol = abs(float(grid_mindet(blocks, X, d).mean()))
+    hbar = vol ** (1.0 / d)
+    return np.eye(d) / hbar

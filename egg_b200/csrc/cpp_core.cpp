@@ -1,0 +1,527 @@
+// pybind11 module `cpp_core`: the reference's Python-facing surface
+// (src/bindings.cpp:1541-2130, module egg._cpp.cpp_core) over the egg_b200
+// C-ABI.  Dict/array unpacking and argument checks live here; every numeric
+// operation runs on the GPU through libegg_b200.so.  Python passes float64 and
+// gets float64 back, as in the reference.
+#include "egg_b200.h"
+
+#include <pybind11/numpy.h>
+#include <pybind11/pybind11.h>
+#include <pybind11/stl.h>
+
+#include <cstdlib>
+#include <memory>
+#include <stdexcept>
+#include <string>
+#include <vector>
+
+namespace py = pybind11;
+
+namespace
+{
+
+using IArr = py::array_t<int32_t, py::array::c_style | py::array::forcecast>;
+using DArr = py::array_t<double, py::array::c_style | py::array::forcecast>;
+
+[[noreturn]] void raise_status(int st)
+{
+    const std::string msg = egg_b200_last_error();
+    if (st == EGG_B200_EINVAL) { throw py::value_error(msg); }
+    if (st == EGG_B200_ENOTSUP) {
+        PyErr_SetString(PyExc_NotImplementedError, msg.c_str());
+        throw py::error_already_set();
+    }
+    throw std::runtime_error(msg);
+}
+
+void check(int st)
+{
+    if (st != EGG_B200_OK) { raise_status(st); }
+}
+
+// Default arithmetic of new sessions: EGG_B200_PRECISION=mixed selects fp32
+// bulk; anything else (or unset) is plain fp64, the reference's double build.
+int default_precision()
+{
+    const char* v = std::getenv("EGG_B200_PRECISION");
+    if (v && (std::string(v) == "mixed" || std::string(v) == "fp32")) { return EGG_B200_PREC_MIXED; }
+    return EGG_B200_PREC_FP64;
+}
+
+int parse_precision(const py::object& p)
+{
+    if (p.is_none()) { return default_precision(); }
+    const std::string s = p.cast<std::string>();
+    if (s == "fp64" || s == "double") { return EGG_B200_PREC_FP64; }
+    if (s == "mixed" || s == "fp32") { return EGG_B200_PREC_MIXED; }
+    throw py::value_error("precision must be 'fp64' or 'mixed', got '" + s + "'");
+}
+
+int objective_of(const std::string& phase)
+{
+    if (phase == "untangle") { return EGG_B200_OBJ_UNTANGLE; }
+    if (phase == "shape_size") { return EGG_B200_OBJ_SHAPE_SIZE; }
+    return EGG_B200_OBJ_SHAPE;
+}
+
+int device_of(const std::string& device)
+{
+    if (device == "cpu") {
+        throw std::runtime_error(
+          "select_queue: egg_b200 runs on the GPU only; device='cpu' has no implementation here "
+          "(use device='gpu' or 'auto')");
+    }
+    if (device == "gpu" || device == "auto") { return -1; }
+    if (device.rfind("cuda:", 0) == 0) { return std::stoi(device.substr(5)); }
+    throw py::value_error("device must be 'auto', 'gpu' or 'cuda:N', got '" + device + "'");
+}
+
+// Keeps every numpy buffer handed to the C-ABI alive until the call returns.
+struct Keep {
+    std::vector<py::object> objs;
+    const int32_t* ints(const py::handle& h, int64_t* n = nullptr)
+    {
+        IArr a = IArr::ensure(h);
+        if (!a) { throw py::value_error("expected an integer array"); }
+        objs.push_back(a);
+        if (n) { *n = int64_t(a.size()); }
+        return a.size() ? a.data() : nullptr;
+    }
+    const double* reals(const py::handle& h, int64_t* n = nullptr)
+    {
+        DArr a = DArr::ensure(h);
+        if (!a) { throw py::value_error("expected a float array"); }
+        objs.push_back(a);
+        if (n) { *n = int64_t(a.size()); }
+        return a.size() ? a.data() : nullptr;
+    }
+};
+
+int64_t checked_num_nodes(const DArr& X, int d)
+{
+    auto buf = X.request();
+    if (buf.ndim != 1) {
+        throw py::value_error("X must be a flat 1-D array of length d*N; got ndim=" + std::to_string(buf.ndim) +
+                              " (did you pass an (N, d) array? ravel() it first).");
+    }
+    if (buf.shape[0] % d != 0) {
+        throw py::value_error("X length must be a multiple of d (" + std::to_string(d) +
+                              " coordinates per node); got " + std::to_string(buf.shape[0]) + ".");
+    }
+    return int64_t(buf.shape[0]) / d;
+}
+
+struct Desc {
+    egg_b200_session_desc d {};
+    Keep keep;
+    std::vector<int32_t> shapes, bgd, tags;
+};
+
+// Fill the C-ABI descriptor from the reference's two dicts + X
+// (src/bindings.cpp:332-489 unpack_context, :757 apply_structured_remap).
+void fill_desc(Desc& D, const py::dict& ctx, const py::dict& st, const DArr& X, int dim, int prec, int dev)
+{
+    if (dim != 2 && dim != 3) {
+        throw py::value_error("egg C++ core: dimension must be 2 or 3, got " + std::to_string(dim));
+    }
+    auto& d = D.d;
+    d.dim = dim;
+    d.precision = prec;
+    d.device = dev;
+    d.num_nodes = checked_num_nodes(X, dim);
+    D.keep.objs.push_back(X);
+    d.X = X.size() ? X.data() : nullptr;
+
+    // structured
+    py::list shapes = st["interior_shapes"].cast<py::list>();
+    py::list bgd = st["block_global_dof"].cast<py::list>();
+    if (py::len(bgd) != py::len(shapes)) {
+        throw py::value_error("structured: block_global_dof count != interior_shapes count");
+    }
+    d.num_blocks = int32_t(py::len(shapes));
+    for (size_t b = 0; b < py::len(shapes); ++b) {
+        IArr s = IArr::ensure(shapes[b]);
+        if (!s || s.size() != dim) { throw py::value_error("structured: each interior shape must have D entries"); }
+        int64_t n = 1;
+        for (int k = 0; k < dim; ++k) {
+            D.shapes.push_back(s.data()[k]);
+            n *= s.data()[k];
+        }
+        IArr ids = IArr::ensure(bgd[b]);
+        if (!ids || int64_t(ids.size()) != n) {
+            throw py::value_error("structured: block_global_dof length != prod(shape)");
+        }
+        D.bgd.insert(D.bgd.end(), ids.data(), ids.data() + ids.size());
+    }
+    d.interior_shapes = D.shapes.data();
+    d.block_global_dof = D.bgd.data();
+    int64_t n1 = 0, n2 = 0, n3 = 0, n4 = 0;
+    d.halo_src_block = D.keep.ints(st["halo_src_block"], &n1);
+    d.halo_src_padded = D.keep.ints(st["halo_src_padded"], &n2);
+    d.halo_dst_block = D.keep.ints(st["halo_dst_block"], &n3);
+    d.halo_dst_padded = D.keep.ints(st["halo_dst_padded"], &n4);
+    if (n3 != n1 || n2 != n1 * dim || n4 != n1 * dim) { throw py::value_error("structured: halo table lengths disagree"); }
+    d.num_halo = n1;
+    d.sing_block = D.keep.ints(st["sing_block"], &n1);
+    d.sing_logical = D.keep.ints(st["sing_logical"], &n2);
+    if (n2 != n1 * dim) { throw py::value_error("structured: sing table lengths disagree"); }
+    d.num_sing = n1;
+
+    // groups: the reference merges all groups into one view; this core takes
+    // exactly one group (build_flat_context emits one).
+    py::list groups = ctx["groups"].cast<py::list>();
+    if (py::len(groups) > 1) { throw py::value_error("unpack_context: this core takes a single DOF group"); }
+    if (py::len(groups) == 1) {
+        py::dict g = groups[0].cast<py::dict>();
+        d.ndof = g["D"].cast<int64_t>();
+        int64_t n = 0;
+        d.dof_idx = D.keep.ints(g["dof_idx"], &n);
+        if (n != d.ndof) { throw py::value_error("validate_context: group[0] dof_idx size " + std::to_string(n) + " != " + std::to_string(d.ndof)); }
+        d.P_of = D.keep.ints(g["P_of"], &n);
+        if (n != d.ndof) { throw py::value_error("validate_context: group[0] P_of size " + std::to_string(n) + " != " + std::to_string(d.ndof)); }
+        if (g.contains("interior_block")) {
+            d.interior_block = D.keep.ints(g["interior_block"], &n);
+            if (n != d.ndof) { throw py::value_error("validate_context: group[0] interior_block size mismatch"); }
+            d.interior_logical = D.keep.ints(g["interior_logical"], &n);
+            if (n != d.ndof * dim) { throw py::value_error("validate_context: group[0] interior_logical size mismatch"); }
+        }
+        d.gc = D.keep.ints(g["gc"], &d.total_samples);
+        for (int k = 0; k < dim; ++k) {
+            d.gn[k] = D.keep.ints(g[("gn" + std::to_string(k)).c_str()], &n);
+            if (n != d.total_samples) { throw py::value_error("validate_context: group[0] gn" + std::to_string(k) + " size mismatch"); }
+            d.s[k] = D.keep.reals(g[("s" + std::to_string(k)).c_str()], &n);
+            if (n != d.total_samples) { throw py::value_error("validate_context: group[0] s" + std::to_string(k) + " size mismatch"); }
+        }
+        d.role = D.keep.ints(g["role"], &n);
+        if (n != d.total_samples) { throw py::value_error("validate_context: group[0] role size mismatch"); }
+        d.W_inv = D.keep.reals(g["W_inv"], &d.W_inv_len);
+        if (g.contains("weight")) { d.weight = D.keep.reals(g["weight"], &d.weight_len); }
+        // Entity partitions: every DOF must be covered exactly once; non-Free
+        // tags mark constrained boundary DOFs.
+        D.tags.assign(size_t(d.ndof), -1);
+        if (g.contains("entities")) {
+            for (auto item : g["entities"].cast<py::dict>()) {
+                py::dict ed = item.second.cast<py::dict>();
+                if (!ed.contains("tag")) {
+                    throw py::value_error("unpack_context: entities carries a '__blob__' group (unsupported)");
+                }
+                const int tag = ed["tag"].cast<int>();
+                IArr dl = IArr::ensure(ed["dof_local"]);
+                for (py::ssize_t i = 0; i < dl.size(); ++i) {
+                    const int32_t v = dl.data()[i];
+                    if (v < 0 || v >= d.ndof) { throw py::value_error("validate_context: dof_local out of range"); }
+                    if (D.tags[v] != -1) { throw py::value_error("validate_context: dof_local covered by more than one SoA partition"); }
+                    D.tags[v] = tag;
+                }
+            }
+            for (int64_t i = 0; i < d.ndof; ++i) {
+                if (D.tags[i] == -1) {
+                    throw py::value_error("validate_context: group[0] DOF " + std::to_string(i) + " not covered by any SoA partition");
+                }
+            }
+        } else {
+            std::fill(D.tags.begin(), D.tags.end(), 0);
+        }
+        d.entity_tag = D.tags.data();
+    }
+
+    py::dict es = ctx["energy_stencil"].cast<py::dict>();
+    d.es_num_samples = es["num_samples"].cast<int64_t>();
+    d.es_structured = es.contains("structured") ? es["structured"].cast<int>() : 0;
+    if (!d.es_structured) {
+        int64_t n = 0;
+        d.es_gc = D.keep.ints(es["gc"], &n);
+        if (n != d.es_num_samples) { throw py::value_error("validate_context: energy_stencil gc size mismatch"); }
+        for (int k = 0; k < dim; ++k) {
+            d.es_gn[k] = D.keep.ints(es[("gn" + std::to_string(k)).c_str()], &n);
+            if (n != d.es_num_samples) { throw py::value_error("validate_context: energy_stencil gn size mismatch"); }
+            d.es_s[k] = D.keep.reals(es[("s" + std::to_string(k)).c_str()], &n);
+            if (n != d.es_num_samples) { throw py::value_error("validate_context: energy_stencil s size mismatch"); }
+        }
+    }
+    d.es_W_inv = D.keep.reals(es["W_inv"], &d.es_W_inv_len);
+    if (es.contains("weight")) { d.es_weight = D.keep.reals(es["weight"], &d.es_weight_len); }
+}
+
+py::array_t<double> vec(const std::vector<double>& v)
+{
+    py::array_t<double> out(py::ssize_t(v.size()));
+    std::copy(v.begin(), v.end(), out.mutable_data());
+    return out;
+}
+
+class Session
+{
+  public:
+    Session(const py::dict& ctx, const py::dict& st, const DArr& X, const std::string& device, int dim,
+            const py::object& control, const py::object& precision) :
+        dim_(dim)
+    {
+        if (!control.is_none()) {
+            PyErr_SetString(PyExc_NotImplementedError,
+                            "egg_b200: control-net sessions (control=...) are not built yet");
+            throw py::error_already_set();
+        }
+        Desc D;
+        fill_desc(D, ctx, st, X, dim, parse_precision(precision), device_of(device));
+        egg_b200_session* h = nullptr;
+        {
+            py::gil_scoped_release nogil;
+            const int rc = egg_b200_session_create(&D.d, &h);
+            if (rc != EGG_B200_OK) {
+                py::gil_scoped_acquire g;
+                raise_status(rc);
+            }
+        }
+        h_.reset(h);
+        M_ = D.d.num_nodes;
+    }
+
+    std::tuple<py::array_t<double>, py::array_t<double>> run(int n_sweeps, const std::string& phase, double delta,
+                                                             double omega, int report_every)
+    {
+        const int k = report_every <= 0 ? std::max(n_sweeps, 1) : report_every;
+        const int64_t cap = n_sweeps > 0 ? (int64_t(n_sweeps) + k - 1) / k : 0;
+        std::vector<double> E(static_cast<size_t>(cap)), Md(static_cast<size_t>(cap));
+        int64_t nrep = 0;
+        int rc;
+        {
+            py::gil_scoped_release nogil;
+            rc = egg_b200_session_run(h_.get(), n_sweeps, objective_of(phase), delta, omega, report_every, E.data(),
+                                      Md.data(), cap, &nrep);
+        }
+        check(rc);
+        E.resize(size_t(nrep));
+        Md.resize(size_t(nrep));
+        return {vec(E), vec(Md)};
+    }
+
+    std::tuple<py::array_t<double>, py::array_t<double>> run_fas(int, int, int, int, double, int,
+                                                                 const std::string& phase)
+    {
+        if (phase == "untangle") {
+            throw py::value_error("run_fas: FAS supports the shape phase only, not \"untangle\"");
+        }
+        PyErr_SetString(PyExc_NotImplementedError, "egg_b200: run_fas is not built yet");
+        throw py::error_already_set();
+    }
+
+    py::list mg_levels() { return py::list(); }
+
+    py::array_t<double> get_X()
+    {
+        std::vector<double> X(size_t(M_ * dim_));
+        int rc;
+        {
+            py::gil_scoped_release nogil;
+            rc = egg_b200_session_get_X(h_.get(), X.data(), int64_t(X.size()));
+        }
+        check(rc);
+        return vec(X);
+    }
+
+    void set_X(const DArr& X)
+    {
+        int rc;
+        {
+            py::gil_scoped_release nogil;
+            rc = egg_b200_session_set_X(h_.get(), X.data(), int64_t(X.size()));
+        }
+        check(rc);
+    }
+
+    std::tuple<double, double> energy(const std::string& phase, double delta)
+    {
+        double e = 0, m = 0;
+        check(egg_b200_session_energy(h_.get(), objective_of(phase), delta, &e, &m));
+        return {e, m};
+    }
+
+    py::dict info()
+    {
+        int64_t v[10];
+        check(egg_b200_session_info(h_.get(), v, 10));
+        py::dict d;
+        const char* keys[10] = {"dim",    "num_nodes", "store_nodes", "ndof",  "interior_dofs", "stored_dofs",
+                                "copies", "energy_samples", "structured_energy", "precision"};
+        for (int i = 0; i < 10; ++i) { d[keys[i]] = v[i]; }
+        d["precision"] = v[9] == EGG_B200_PREC_MIXED ? "mixed" : "fp64";
+        return d;
+    }
+
+    void set_profiling(bool on) { check(egg_b200_session_set_profiling(h_.get(), on ? 1 : 0)); }
+
+    py::dict kernel_stats()
+    {
+        static const char* names[6] = {"interior_sweep", "stored_sweep", "broadcast", "reduce", "reduce_final", "copy"};
+        py::dict d;
+        for (int k = 0; k < 6; ++k) {
+            double ms = 0;
+            int64_t n = 0;
+            check(egg_b200_session_kernel_stats(h_.get(), k, &ms, &n));
+            d[names[k]] = py::make_tuple(ms, n);
+        }
+        return d;
+    }
+
+    void reset_stats() { check(egg_b200_session_reset_stats(h_.get())); }
+
+    void checkpoint()
+    {
+        py::gil_scoped_release nogil;
+        const int rc = egg_b200_session_checkpoint(h_.get());
+        py::gil_scoped_acquire g;
+        check(rc);
+    }
+
+    void restore()
+    {
+        py::gil_scoped_release nogil;
+        const int rc = egg_b200_session_restore(h_.get());
+        py::gil_scoped_acquire g;
+        check(rc);
+    }
+
+    int64_t launch_count()
+    {
+        int64_t n = 0;
+        check(egg_b200_session_launch_count(h_.get(), &n));
+        return n;
+    }
+
+    [[noreturn]] void no_control()
+    {
+        throw py::value_error("run_control: session was built without a control wire");
+    }
+
+  private:
+    struct Del {
+        void operator()(egg_b200_session* s) const { egg_b200_session_destroy(s); }
+    };
+    int dim_;
+    int64_t M_ = 0;
+    std::unique_ptr<egg_b200_session, Del> h_;
+};
+
+}  // namespace
+
+PYBIND11_MODULE(cpp_core, m)
+{
+    m.doc() = "egg compute core, B200 (sm_100a) CUDA build.";
+    m.def("ping", [] { return 0; }, "Liveness check; returns 0.");
+    // B-spline degree caps of the reference build (constrained boundaries are
+    // not on this core's path; the values are kept for wire encoders).
+    m.attr("MAX_BSPLINE_DEGREE") = 5;
+    m.attr("MAX_BSPLINE_CURVE_DEGREE") = 7;
+    m.attr("REAL_IS_FLOAT") = default_precision() == EGG_B200_PREC_MIXED;
+    m.attr("ABI_VERSION") = egg_b200_abi_version();
+
+    m.def("device_count", [] {
+        int n = 0;
+        check(egg_b200_device_count(&n));
+        return n;
+    });
+
+    py::class_<Session>(m, "CppStructuredSweepSession",
+                        "Persistent device-resident structured smoothing session (B200 CUDA core).")
+      .def(py::init<py::dict, py::dict, DArr, const std::string&, int, const py::object&, const py::object&>(),
+           py::arg("ctx_arrays"), py::arg("structured"), py::arg("X"), py::kw_only(), py::arg("device") = "auto",
+           py::arg("dim") = 2, py::arg("control") = py::none(), py::arg("precision") = py::none())
+      .def("run", &Session::run, py::arg("n_sweeps"), py::kw_only(), py::arg("phase") = "barrier",
+           py::arg("delta") = 0.0, py::arg("omega") = 1.0, py::arg("report_every") = 0,
+           "Run n_sweeps of block-Jacobi on the resident X; returns (energies, mindets).")
+      .def("run_fas", &Session::run_fas, py::arg("n_cycles"), py::kw_only(), py::arg("nu_pre") = 2,
+           py::arg("nu_post") = 2, py::arg("nu_coarse") = 32, py::arg("omega") = 1.0, py::arg("max_levels") = 32,
+           py::arg("phase") = "barrier")
+      .def("mg_levels", &Session::mg_levels)
+      .def("get_X", &Session::get_X, "Download X gathered back to global node order, shape (N*dim,).")
+      .def("set_X", &Session::set_X, py::arg("X"), "Upload X (global node order) into every copy.")
+      .def("energy", &Session::energy, py::arg("phase") = "barrier", py::arg("delta") = 0.0,
+           "(energy, min det A) of the resident state.")
+      .def("info", &Session::info)
+      .def("set_profiling", &Session::set_profiling, py::arg("enable"))
+      .def("kernel_stats", &Session::kernel_stats)
+      .def("reset_stats", &Session::reset_stats)
+      .def("checkpoint", &Session::checkpoint, "Copy the resident positions to a device-side checkpoint.")
+      .def("restore", &Session::restore, "Restore the resident positions from the device-side checkpoint.")
+      .def("launch_count", &Session::launch_count)
+      .def("run_control", [](Session& s, int, const std::string&, double, double, double, int, double, bool, bool) {
+          s.no_control();
+      }, py::arg("n_outer"), py::kw_only(), py::arg("phase") = "barrier", py::arg("grad_tol") = 1e-8,
+         py::arg("alpha_min") = 1e-4, py::arg("lm0") = 0.0, py::arg("pcg_max_iter") = 200, py::arg("pcg_rtol") = 1e-10,
+         py::arg("pcg_forcing") = true, py::arg("model_db") = true)
+      .def("get_C", [](Session& s) { s.no_control(); })
+      .def("set_C", [](Session& s, const DArr&) { s.no_control(); }, py::arg("C"));
+
+    m.def(
+      "cpp_structured_sweep",
+      [](const py::dict& ctx, const py::dict& st, const DArr& X, int n_sweeps, const std::string& device,
+         const std::string& phase, double delta, int dim, double omega, int report_every, const py::object& precision) {
+          Session s(ctx, st, X, device, dim, py::none(), precision);
+          auto [e, m] = s.run(n_sweeps, phase, delta, omega, report_every);
+          return std::make_tuple(s.get_X(), e, m);
+      },
+      py::arg("ctx_arrays"), py::arg("structured"), py::arg("X"), py::arg("n_sweeps"), py::kw_only(),
+      py::arg("device") = "auto", py::arg("phase") = "barrier", py::arg("delta") = 0.0, py::arg("dim") = 2,
+      py::arg("omega") = 1.0, py::arg("report_every") = 0, py::arg("precision") = py::none(),
+      "Run n_sweeps of block-Jacobi; returns (X_out, energies, mindets), X_out in global node order.");
+
+    m.def(
+      "metric_eval",
+      [](const DArr& t, const std::string& metric, double delta) {
+          int obj;
+          if (metric == "shape_2d") {
+              obj = EGG_B200_OBJ_SHAPE;
+          } else if (metric == "shape_size") {
+              obj = EGG_B200_OBJ_SHAPE_SIZE;
+          } else if (metric == "untangle") {
+              obj = EGG_B200_OBJ_UNTANGLE;
+          } else {
+              throw py::value_error("metric_eval: unknown metric '" + metric + "'");
+          }
+          if (t.size() != 4) { throw py::value_error("metric_eval: t must have 4 entries"); }
+          double mu = 0;
+          std::vector<double> g(4), h(16);
+          check(egg_b200_metric_eval(obj, delta, t.data(), 1, &mu, g.data(), h.data()));
+          return std::make_tuple(mu, vec(g), vec(h));
+      },
+      py::arg("t"), py::arg("metric") = "shape_2d", py::arg("delta") = 0.0,
+      "Evaluate a named 2D metric on the GPU. Returns (mu, grad(4,), hess(16,)).");
+
+    m.def(
+      "patch_eval",
+      [](const DArr& X, const IArr& gc, const IArr& gn0, const IArr& gn1, const DArr& s0, const DArr& s1,
+         const DArr& W, const IArr& role, const py::object&) {
+          const int P = int(gc.size());
+          if (gn0.size() != P || gn1.size() != P || s0.size() != P || s1.size() != P || role.size() != P ||
+              W.size() != 4 * P) {
+              throw py::value_error("patch_eval: inconsistent patch array sizes");
+          }
+          std::vector<double> g(2), h(4), st(2);
+          double e = 0, md = 0;
+          check(egg_b200_patch_eval(EGG_B200_OBJ_SHAPE, 0.0, X.data(), int64_t(X.size() / 2), P, gc.data(), gn0.data(),
+                                    gn1.data(), s0.data(), s1.data(), W.data(), role.data(), g.data(), h.data(), &e,
+                                    &md, st.data()));
+          return std::make_tuple(vec(g), vec(h), e, md);
+      },
+      py::arg("X"), py::arg("gc"), py::arg("gn0"), py::arg("gn1"), py::arg("s0"), py::arg("s1"), py::arg("W_inv"),
+      py::arg("role"), py::arg("J") = py::none(),
+      "Per-DOF patch evaluation on the GPU. Returns (grad(2,), hess(4,), energy, mindet).");
+
+    m.def(
+      "newton_step",
+      [](const DArr& grad, const DArr& hess, const DArr& pos, int tag, const py::object&) {
+          if (tag != 0) {
+              PyErr_SetString(PyExc_NotImplementedError, "newton_step: constrained entity tags are not supported");
+              throw py::error_already_set();
+          }
+          if (grad.size() != 2 || hess.size() != 4 || pos.size() != 2) {
+              throw py::value_error("newton_step: grad(2), hess(4), pos(2) expected");
+          }
+          std::vector<double> x(2);
+          check(egg_b200_newton_step(grad.data(), hess.data(), x.data()));
+          return vec(x);
+      },
+      py::arg("grad"), py::arg("hess"), py::arg("pos"), py::arg("tag") = 0, py::arg("params") = py::none(),
+      "Free-DOF Newton step -H^{-1} g with the zero/non-finite fallbacks. Returns delta(2,).");
+}

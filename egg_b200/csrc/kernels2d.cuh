@@ -1,0 +1,763 @@
+// 2D sweep kernels of the egg_b200 core (sm_100a).
+//
+// Store layout: every block is a dense row-major (n0, n1) array of nodes with
+// the two coordinates interleaved (double2 per node); blocks are packed back to
+// back.  No ghost ring: cross-block reads go to owner slots (stored-patch DOFs)
+// or to the block's own refreshed copies of shared interface nodes.
+//
+// One block-Jacobi sweep (src/sweep.hpp:1938 jacobi_sweep_once) is
+//   broadcast_kernel     owner -> non-owner copies on the read buffer
+//   interior_tile_kernel structured-interior DOFs (patch synthesized, W_inv = I)
+//   stored_patch_kernel  every other moving DOF (ragged stored patch)
+// Both sweep kernels read X_in (frozen snapshot) and write X_out.
+#pragma once
+
+#include "metric.cuh"
+
+#include <cstdint>
+#include <cuda_runtime.h>
+#include <type_traits>
+
+namespace egg_b200
+{
+
+struct BlockInfo {
+    int64_t off;  // first node slot of the block in the packed store
+    int32_t n[3]; // node counts per axis (n[2] = 1 in 2D)
+    int32_t pad;
+};
+
+struct Tile2 {
+    int32_t block;
+    int32_t i0;  // first DOF row (logical, >= 1)
+    int32_t j0;  // first DOF column
+    int32_t pad;
+};
+
+// Relative threshold of the fp64 guard in mixed precision: a sample whose
+// |det A| < kGuard * |a0| |a1| (sine of the corner angle below 1e-3) is
+// re-evaluated in fp64.
+constexpr double kGuard = 1e-3;
+
+__device__ __forceinline__ double2 ld2(const double2* p) { return *p; }
+
+// ---------------------------------------------------------------------------
+// One sample from its two edge vectors e0 = s0 (n0 - c), e1 = s1 (n1 - c)
+// (already signed).  vec(T) = [e0.x, e1.x, e0.y, e1.y] (A[:,k] = e_k, W = I).
+// ---------------------------------------------------------------------------
+template <class C> struct SampleOut {
+    C mu, det;
+    C g[4];
+    C H[16];
+};
+
+template <int KIND, class C>
+__device__ __forceinline__ void sample_full_c(C ax, C bx, C ay, C by, C delta, SampleOut<C>& o)
+{
+    const C t[4] = {ax, bx, ay, by};
+    mu_eval<C>(KIND, t, delta, o.mu, o.g, o.H);
+    o.det = det2(t);
+}
+
+// Full per-sample evaluation from fp64 edge vectors, in working precision C
+// (fp64 re-evaluation for near-degenerate samples when C = float).
+template <int KIND, class C>
+__device__ __forceinline__ void sample_full(double ax, double bx, double ay, double by, double delta,
+                                            SampleOut<C>& o)
+{
+    if constexpr (std::is_same_v<C, double>) {
+        sample_full_c<KIND, double>(ax, bx, ay, by, delta, o);
+    } else {
+        const float fax = float(ax), fbx = float(bx), fay = float(ay), fby = float(by);
+        const float d = fax * fby - fbx * fay;
+        const float n0 = fax * fax + fay * fay, n1 = fbx * fbx + fby * fby;
+        if (d * d < float(kGuard * kGuard) * n0 * n1) {
+            SampleOut<double> od;
+            sample_full_c<KIND, double>(ax, bx, ay, by, delta, od);
+            o.mu = float(od.mu);
+            o.det = float(od.det);
+            for (int i = 0; i < 4; ++i) { o.g[i] = float(od.g[i]); }
+            for (int i = 0; i < 16; ++i) { o.H[i] = float(od.H[i]); }
+        } else {
+            sample_full_c<KIND, float>(fax, fbx, fay, fby, float(delta), o);
+        }
+    }
+}
+
+// Value + det only (line-search trials), working precision C with fp64 guard.
+template <int KIND, class C>
+__device__ __forceinline__ C sample_mu_c(C ax, C bx, C ay, C by, C delta, C& det)
+{
+    const C t[4] = {ax, bx, ay, by};
+    det = det2(t);
+    return mu_value<C>(KIND, t, delta);
+}
+
+// ---------------------------------------------------------------------------
+// Owner -> non-owner copy refresh (src/structured_halo.hpp:197 fused_halo_broadcast).
+// ---------------------------------------------------------------------------
+__global__ void broadcast2_kernel(double2* __restrict__ X, const int32_t* __restrict__ src,
+                                  const int32_t* __restrict__ dst, int64_t n)
+{
+    for (int64_t e = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; e < n;
+         e += int64_t(gridDim.x) * blockDim.x) {
+        X[dst[e]] = X[src[e]];
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Fused structured-interior sweep.  One CTA = one tile of (CI-1) x (CJ-1)
+// DOFs; CI*CJ threads.  Phase 1 stages the (CI+1) x (CJ+1) node window in
+// shared memory; phase 2 evaluates each of the CI*CJ cells' four corner
+// samples ONCE (value, det, gradient and the role-contracted Hessian for the
+// three nodes each sample moves) - the reference re-evaluates every sample
+// for each of the 4 DOFs that share it; phase 3 gathers the 16-occurrence
+// patch of each DOF from its 4 cells, takes the 2x2 Newton step, backtracks
+// (<= 10 halvings) on the patch energy with the node substituted, applies
+// the omega blend and writes X_out.  Patch semantics follow
+// src/structured_patch.hpp:89-258 and src/sweep.hpp:1534-1650.
+// ---------------------------------------------------------------------------
+template <int CI, int CJ, class C> struct TileShared2 {
+    static constexpr int NC = CI * CJ;
+    double2 P[(CI + 1) * (CJ + 1)];
+    C mu[4][NC];
+    C det[4][NC];
+    C gh[4][5][NC];  // per local corner a: gx, gy, hxx, hxy, hyy
+    uint8_t bad[NC]; // cell holds an inverted or badly shaped sample
+};
+
+// Mixed precision: a DOF whose patch touches a cell with an inverted sample or
+// a corner angle below asin(kBadCell) is relaxed entirely in fp64 (patch,
+// Newton step and line search), since accept/reject decisions next to such
+// cells are ill-conditioned in fp32.
+constexpr double kBadCell = 0.1;
+
+// Complete fp64 update of the DOF at window node (ti+1, tj+1): 16-occurrence
+// patch (W_inv = I) evaluated from the staged positions, 2x2 Newton step,
+// <= 10 halvings, omega blend.  Same semantics as the shared-sample path.
+template <int KIND>
+__device__ double2 dof_update_fp64(const double2* __restrict__ P, int PW, int ti, int tj, double tx, double ty,
+                                   double delta, double omega)
+{
+    const double2 pos = P[(ti + 1) * PW + (tj + 1)];
+    double g0 = 0, g1 = 0, hxx = 0, hxy = 0, hyy = 0, e0 = 0;
+    auto node = [&](int u, int v) { return P[(ti + u) * PW + (tj + v)]; };
+#pragma unroll 1
+    for (int cell = 0; cell < 4; ++cell) {
+        const int ci = cell >> 1, cj = cell & 1;
+        const int a = (1 - ci) * 2 + (1 - cj);
+#pragma unroll 1
+        for (int b = 0; b < 4; ++b) {
+            const double s0 = (b & 2) ? -1.0 : 1.0, s1 = (b & 1) ? -1.0 : 1.0;
+            const double2 pc = node(ci + (b >> 1), cj + (b & 1));
+            const int b0 = b ^ 2, b1 = b ^ 1;
+            const double2 p0 = node(ci + (b0 >> 1), cj + (b0 & 1));
+            const double2 p1 = node(ci + (b1 >> 1), cj + (b1 & 1));
+            SampleOut<double> o;
+            sample_full_c<KIND, double>(s0 * (p0.x - pc.x), s1 * (p1.x - pc.x), s0 * (p0.y - pc.y),
+                                        s1 * (p1.y - pc.y), delta, o);
+            e0 += o.mu;
+            if (b == a) {
+                g0 -= s0 * o.g[0] + s1 * o.g[1];
+                g1 -= s0 * o.g[2] + s1 * o.g[3];
+                hxx += o.H[0] + o.H[5] + s0 * s1 * (o.H[1] + o.H[4]);
+                hxy += o.H[2] + o.H[7] + s0 * s1 * (o.H[3] + o.H[6]);
+                hyy += o.H[10] + o.H[15] + s0 * s1 * (o.H[11] + o.H[14]);
+            } else if (b0 == a) {
+                g0 += s0 * o.g[0];
+                g1 += s0 * o.g[2];
+                hxx += o.H[0];
+                hxy += o.H[2];
+                hyy += o.H[10];
+            } else if (b1 == a) {
+                g0 += s1 * o.g[1];
+                g1 += s1 * o.g[3];
+                hxx += o.H[5];
+                hxy += o.H[7];
+                hyy += o.H[15];
+            }
+        }
+    }
+    const double gv[2] = {g0 - tx, g1 - ty};
+    const double Hm[4] = {hxx, hxy, hxy, hyy};
+    double dl[2];
+    solve2<double>(Hm, gv, dl);
+    double alpha = 1.0;
+#pragma unroll 1
+    for (int it = 0; it < 10; ++it) {
+        const double dx = alpha * dl[0], dy = alpha * dl[1];
+        const double2 tr = make_double2(pos.x + dx, pos.y + dy);
+        double e = 0.0, md = INFINITY;
+#pragma unroll 1
+        for (int cell = 0; cell < 4; ++cell) {
+            const int ci = cell >> 1, cj = cell & 1;
+            const int a = (1 - ci) * 2 + (1 - cj);
+#pragma unroll 1
+            for (int b = 0; b < 4; ++b) {
+                const double s0 = (b & 2) ? -1.0 : 1.0, s1 = (b & 1) ? -1.0 : 1.0;
+                const int b0 = b ^ 2, b1 = b ^ 1;
+                const double2 pc = (b == a) ? tr : node(ci + (b >> 1), cj + (b & 1));
+                const double2 p0 = (b0 == a) ? tr : node(ci + (b0 >> 1), cj + (b0 & 1));
+                const double2 p1 = (b1 == a) ? tr : node(ci + (b1 >> 1), cj + (b1 & 1));
+                double d;
+                e += sample_mu_c<KIND, double>(s0 * (p0.x - pc.x), s1 * (p1.x - pc.x), s0 * (p0.y - pc.y),
+                                               s1 * (p1.y - pc.y), delta, d);
+                md = fmin(md, d);
+            }
+        }
+        e -= tx * dx + ty * dy;
+        if (isfinite(e) && e <= e0 + Tol<double>::energy && (KIND == kUntangle || md > 0.0)) {
+            return make_double2(pos.x + omega * dx, pos.y + omega * dy);
+        }
+        alpha *= 0.5;
+    }
+    return pos;
+}
+
+template <int CI, int CJ, int KIND, class C>
+__global__ void __launch_bounds__(CI* CJ)
+  interior_tile_kernel(const double2* __restrict__ Xin, double2* __restrict__ Xout,
+                       const Tile2* __restrict__ tiles, const BlockInfo* __restrict__ blocks,
+                       const uint8_t* __restrict__ active, const double2* __restrict__ tau,
+                       double delta, double omega)
+{
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    using S = TileShared2<CI, CJ, C>;
+    S& sm = *reinterpret_cast<S*>(smem_raw);
+    constexpr int NC = CI * CJ;
+    constexpr int PW = CJ + 1;
+
+    const Tile2 tile = tiles[blockIdx.x];
+    const BlockInfo bi = blocks[tile.block];
+    const int n0 = bi.n[0], n1 = bi.n[1];
+    const int r0 = tile.i0 - 1, c0 = tile.j0 - 1;  // node window origin
+    const int tid = threadIdx.x;
+
+    // Phase 1: node window.
+    for (int k = tid; k < (CI + 1) * (CJ + 1); k += NC) {
+        const int r = k / PW, c = k % PW;
+        const int gi = r0 + r, gj = c0 + c;
+        double2 v = make_double2(0.0, 0.0);
+        if (gi < n0 && gj < n1) { v = Xin[bi.off + int64_t(gi) * n1 + gj]; }
+        sm.P[k] = v;
+    }
+    __syncthreads();
+
+    // Phase 2: cell (ci, cj) with base node window (ci, cj); thread = cell.
+    {
+        const int ci = tid / CJ, cj = tid % CJ;
+        const bool valid = (r0 + ci <= n0 - 2) && (c0 + cj <= n1 - 2);
+        C mu4[4], det4[4];
+        C acc[4][5];
+        bool bad = false;
+#pragma unroll
+        for (int a = 0; a < 4; ++a) {
+#pragma unroll
+            for (int q = 0; q < 5; ++q) { acc[a][q] = C(0); }
+        }
+        if (valid) {
+            const double2 p[4] = {sm.P[ci * PW + cj], sm.P[ci * PW + cj + 1],
+                                  sm.P[(ci + 1) * PW + cj], sm.P[(ci + 1) * PW + cj + 1]};
+#pragma unroll
+            for (int b = 0; b < 4; ++b) {
+                const double s0 = (b & 2) ? -1.0 : 1.0;
+                const double s1 = (b & 1) ? -1.0 : 1.0;
+                const double2 pc = p[b], pn0 = p[b ^ 2], pn1 = p[b ^ 1];
+                const double ax = s0 * (pn0.x - pc.x), bx = s1 * (pn1.x - pc.x);
+                const double ay = s0 * (pn0.y - pc.y), by = s1 * (pn1.y - pc.y);
+                if constexpr (std::is_same_v<C, float>) {
+                    const double dd = ax * by - bx * ay;
+                    const double nn = (ax * ax + ay * ay) * (bx * bx + by * by);
+                    bad = bad || dd <= 0.0 || dd * dd < kBadCell * kBadCell * nn;
+                }
+                SampleOut<C> o;
+                sample_full<KIND, C>(ax, bx, ay, by, delta, o);
+                mu4[b] = o.mu;
+                det4[b] = o.det;
+                const C cs0 = C(s0), cs1 = C(s1);
+                // role 1: node b^2 is the axis-0 neighbour; role 2: node b^1.
+                const C g1x = cs0 * o.g[0], g1y = cs0 * o.g[2];
+                const C g2x = cs1 * o.g[1], g2y = cs1 * o.g[3];
+                const C h1xx = o.H[0], h1xy = o.H[2], h1yy = o.H[10];
+                const C h2xx = o.H[5], h2xy = o.H[7], h2yy = o.H[15];
+                const C ss = cs0 * cs1;
+                acc[b ^ 2][0] += g1x;
+                acc[b ^ 2][1] += g1y;
+                acc[b ^ 2][2] += h1xx;
+                acc[b ^ 2][3] += h1xy;
+                acc[b ^ 2][4] += h1yy;
+                acc[b ^ 1][0] += g2x;
+                acc[b ^ 1][1] += g2y;
+                acc[b ^ 1][2] += h2xx;
+                acc[b ^ 1][3] += h2xy;
+                acc[b ^ 1][4] += h2yy;
+                acc[b][0] -= g1x + g2x;
+                acc[b][1] -= g1y + g2y;
+                acc[b][2] += h1xx + h2xx + ss * (o.H[1] + o.H[4]);
+                acc[b][3] += h1xy + h2xy + ss * (o.H[3] + o.H[6]);
+                acc[b][4] += h1yy + h2yy + ss * (o.H[11] + o.H[14]);
+            }
+        } else {
+#pragma unroll
+            for (int b = 0; b < 4; ++b) {
+                mu4[b] = C(0);
+                det4[b] = C(1);
+            }
+        }
+        sm.bad[tid] = bad ? 1 : 0;
+#pragma unroll
+        for (int b = 0; b < 4; ++b) {
+            sm.mu[b][tid] = mu4[b];
+            sm.det[b][tid] = det4[b];
+#pragma unroll
+            for (int q = 0; q < 5; ++q) { sm.gh[b][q][tid] = acc[b][q]; }
+        }
+    }
+    __syncthreads();
+
+    // Phase 3: DOFs.
+    constexpr int DI = CI - 1, DJ = CJ - 1;
+    if (tid >= DI * DJ) { return; }
+    const int ti = tid / DJ, tj = tid % DJ;
+    const int gi = tile.i0 + ti, gj = tile.j0 + tj;
+    if (gi > n0 - 2 || gj > n1 - 2) { return; }
+    const int64_t slot = bi.off + int64_t(gi) * n1 + gj;
+    if (!active[slot]) { return; }
+
+    C g0 = 0, g1 = 0, hxx = 0, hxy = 0, hyy = 0, e0 = 0, econst = 0;
+    C mdconst = C(INFINITY);
+#pragma unroll
+    for (int ci = 0; ci < 2; ++ci) {
+#pragma unroll
+        for (int cj = 0; cj < 2; ++cj) {
+            const int cell = (ti + ci) * CJ + (tj + cj);
+            const int a = (1 - ci) * 2 + (1 - cj);
+            g0 += sm.gh[a][0][cell];
+            g1 += sm.gh[a][1][cell];
+            hxx += sm.gh[a][2][cell];
+            hxy += sm.gh[a][3][cell];
+            hyy += sm.gh[a][4][cell];
+            e0 += (sm.mu[0][cell] + sm.mu[1][cell]) + (sm.mu[2][cell] + sm.mu[3][cell]);
+            econst += sm.mu[a ^ 3][cell];
+            mdconst = fmin(mdconst, sm.det[a ^ 3][cell]);
+        }
+    }
+    C tx = 0, ty = 0;
+    double txd = 0.0, tyd = 0.0;
+    if (tau != nullptr) {
+        const double2 tv = tau[slot];
+        txd = tv.x;
+        tyd = tv.y;
+        tx = C(tv.x);
+        ty = C(tv.y);
+    }
+    if constexpr (std::is_same_v<C, float>) {
+        const int c00 = ti * CJ + tj;
+        if (sm.bad[c00] | sm.bad[c00 + 1] | sm.bad[c00 + CJ] | sm.bad[c00 + CJ + 1]) {
+            Xout[slot] = dof_update_fp64<KIND>(sm.P, PW, ti, tj, txd, tyd, delta, omega);
+            return;
+        }
+    }
+    const C gv[2] = {g0 - tx, g1 - ty};
+    const C Hm[4] = {hxx, hxy, hxy, hyy};
+    C dlt[2];
+    solve2<C>(Hm, gv, dlt);
+
+    // Neighbour offsets relative to the DOF, in working precision.
+    const double2 pos = sm.P[(ti + 1) * PW + (tj + 1)];
+    C rx[3][3], ry[3][3];
+#pragma unroll
+    for (int u = 0; u < 3; ++u) {
+#pragma unroll
+        for (int v = 0; v < 3; ++v) {
+            const double2 q = sm.P[(ti + u) * PW + (tj + v)];
+            rx[u][v] = C(q.x - pos.x);
+            ry[u][v] = C(q.y - pos.y);
+        }
+    }
+
+    C alpha = C(1);
+    C ax_acc = C(0), ay_acc = C(0);
+    bool accepted = false;
+    for (int it = 0; it < 10 && !accepted; ++it) {
+        const C dx = alpha * dlt[0], dy = alpha * dlt[1];
+        C e = econst;
+        C md = mdconst;
+#pragma unroll
+        for (int ci = 0; ci < 2; ++ci) {
+#pragma unroll
+            for (int cj = 0; cj < 2; ++cj) {
+                const int a = (1 - ci) * 2 + (1 - cj);
+#pragma unroll
+                for (int r = 0; r < 3; ++r) {
+                    const int b = (r == 0) ? a : ((r == 1) ? (a ^ 2) : (a ^ 1));
+                    const int bn0 = b ^ 2, bn1 = b ^ 1;
+                    // node window coords of corner / neighbours (cell base (ci, cj))
+                    const int cu = ci + (b >> 1), cv = cj + (b & 1);
+                    const int u0 = ci + (bn0 >> 1), v0 = cj + (bn0 & 1);
+                    const int u1 = ci + (bn1 >> 1), v1 = cj + (bn1 & 1);
+                    const C pcx = (b == a) ? dx : rx[cu][cv];
+                    const C pcy = (b == a) ? dy : ry[cu][cv];
+                    const C p0x = (bn0 == a) ? dx : rx[u0][v0];
+                    const C p0y = (bn0 == a) ? dy : ry[u0][v0];
+                    const C p1x = (bn1 == a) ? dx : rx[u1][v1];
+                    const C p1y = (bn1 == a) ? dy : ry[u1][v1];
+                    const C s0 = (b & 2) ? C(-1) : C(1);
+                    const C s1 = (b & 1) ? C(-1) : C(1);
+                    C ax = s0 * (p0x - pcx), bx = s1 * (p1x - pcx);
+                    C ay = s0 * (p0y - pcy), by = s1 * (p1y - pcy);
+                    C d;
+                    C m;
+                    if constexpr (std::is_same_v<C, float>) {
+                        const float dd = ax * by - bx * ay;
+                        const float nn0 = ax * ax + ay * ay, nn1 = bx * bx + by * by;
+                        if (dd * dd < float(kGuard * kGuard) * nn0 * nn1) {
+                            // fp64 re-evaluation from the staged fp64 positions
+                            const double2 qc = sm.P[(ti + cu) * PW + (tj + cv)];
+                            const double2 q0 = sm.P[(ti + u0) * PW + (tj + v0)];
+                            const double2 q1 = sm.P[(ti + u1) * PW + (tj + v1)];
+                            const double tX = pos.x + double(dx), tY = pos.y + double(dy);
+                            const double cX = (b == a) ? tX : qc.x, cY = (b == a) ? tY : qc.y;
+                            const double X0 = (bn0 == a) ? tX : q0.x, Y0 = (bn0 == a) ? tY : q0.y;
+                            const double X1 = (bn1 == a) ? tX : q1.x, Y1 = (bn1 == a) ? tY : q1.y;
+                            double dd64;
+                            const double m64 = sample_mu_c<KIND, double>(
+                              double(s0) * (X0 - cX), double(s1) * (X1 - cX), double(s0) * (Y0 - cY),
+                              double(s1) * (Y1 - cY), delta, dd64);
+                            m = float(m64);
+                            d = float(dd64);
+                        } else {
+                            m = sample_mu_c<KIND, float>(ax, bx, ay, by, float(delta), d);
+                        }
+                    } else {
+                        m = sample_mu_c<KIND, double>(ax, bx, ay, by, delta, d);
+                    }
+                    e += m;
+                    md = fmin(md, d);
+                }
+            }
+        }
+        e -= tx * dx + ty * dy;
+        const bool ok = isfinite(e) && (e <= e0 + Tol<C>::energy) &&
+                        (KIND == kUntangle || md > C(0));
+        if (ok) {
+            ax_acc = dx;
+            ay_acc = dy;
+            accepted = true;
+        } else {
+            alpha *= C(0.5);
+        }
+    }
+    double2 out = pos;
+    if (accepted) {
+        out.x = pos.x + omega * double(ax_acc);
+        out.y = pos.y + omega * double(ay_acc);
+    }
+    Xout[slot] = out;
+}
+
+// ---------------------------------------------------------------------------
+// Stored-patch sweep (fp64): one thread per DOF over its ragged occurrence
+// slice; general W_inv, per-sample weights and the FAS tau shift.  Mirrors
+// src/patch.hpp:325 patch_eval + src/sweep.hpp:1534 interior_update_kernel.
+// ---------------------------------------------------------------------------
+struct StoredPatch2 {
+    int64_t n;              // DOFs
+    const int32_t* slot;    // [n] owner slot of each DOF
+    const int64_t* off;     // [n+1] occurrence ranges
+    const int32_t* gc;      // [occ] owner slots
+    const int32_t* gn0;
+    const int32_t* gn1;
+    const int8_t* s0;       // [occ] +-1
+    const int8_t* s1;
+    const int32_t* role;    // [occ]
+    const double* W;        // [occ*4] or [4]
+    int32_t w_stride;       // 4 or 0
+    const double* wt;       // [occ] or [1]
+    int32_t wt_stride;      // 1 or 0
+};
+
+__device__ __forceinline__ void assemble_T(const double2 c, const double2 n0, const double2 n1,
+                                           double s0, double s1, const double* w, double t[4],
+                                           double& detA)
+{
+    const double A00 = s0 * (n0.x - c.x), A01 = s1 * (n1.x - c.x);
+    const double A10 = s0 * (n0.y - c.y), A11 = s1 * (n1.y - c.y);
+    detA = A00 * A11 - A01 * A10;
+    t[0] = A00 * w[0] + A01 * w[2];
+    t[1] = A00 * w[1] + A01 * w[3];
+    t[2] = A10 * w[0] + A11 * w[2];
+    t[3] = A10 * w[1] + A11 * w[3];
+}
+
+template <int KIND>
+__device__ void stored_patch_eval(const StoredPatch2& sp, const double2* X, int64_t d, double delta,
+                                  double g[2], double h[4], double& e0, double& mdet)
+{
+    g[0] = g[1] = 0.0;
+    h[0] = h[1] = h[2] = h[3] = 0.0;
+    e0 = 0.0;
+    mdet = INFINITY;
+    for (int64_t p = sp.off[d]; p < sp.off[d + 1]; ++p) {
+        const double* w = sp.W + p * sp.w_stride;
+        const double s0 = sp.s0[p], s1 = sp.s1[p];
+        double t[4], detA;
+        assemble_T(X[sp.gc[p]], X[sp.gn0[p]], X[sp.gn1[p]], s0, s1, w, t, detA);
+        mdet = fmin(mdet, detA);
+        const double wt = sp.wt[p * sp.wt_stride];
+        const int role = sp.role[p];
+        double mu, gg[4], H[16];
+        mu_eval<double>(KIND, t, delta, mu, gg, H);
+        e0 += wt * mu;
+        if (role < 0) { continue; }
+        // Jb (4x2): row a = (i, c): column i holds v_c, v = -(s0 w[0,c] + s1 w[1,c])
+        // for the corner, s_ax w[ax, c] for an axis-ax neighbour.
+        double v[2];
+        for (int c = 0; c < 2; ++c) {
+            v[c] = (role == 0) ? -(s0 * w[0 * 2 + c] + s1 * w[1 * 2 + c])
+                               : ((role == 1) ? s0 * w[0 * 2 + c] : s1 * w[1 * 2 + c]);
+        }
+        for (int i = 0; i < 2; ++i) {
+            g[i] += wt * (gg[i * 2 + 0] * v[0] + gg[i * 2 + 1] * v[1]);
+            for (int j = 0; j < 2; ++j) {
+                double acc = 0.0;
+                for (int c = 0; c < 2; ++c) {
+                    for (int c2 = 0; c2 < 2; ++c2) { acc += v[c] * H[(i * 2 + c) * 4 + (j * 2 + c2)] * v[c2]; }
+                }
+                h[i * 2 + j] += wt * acc;
+            }
+        }
+    }
+}
+
+template <int KIND>
+__device__ void stored_trial(const StoredPatch2& sp, const double2* X, int64_t d, int32_t dslot,
+                             double2 trial, double delta, double& e, double& md)
+{
+    e = 0.0;
+    md = INFINITY;
+    for (int64_t p = sp.off[d]; p < sp.off[d + 1]; ++p) {
+        const double* w = sp.W + p * sp.w_stride;
+        const int32_t ic = sp.gc[p], i0 = sp.gn0[p], i1 = sp.gn1[p];
+        const double2 c = (ic == dslot) ? trial : X[ic];
+        const double2 n0 = (i0 == dslot) ? trial : X[i0];
+        const double2 n1 = (i1 == dslot) ? trial : X[i1];
+        double t[4], detA;
+        assemble_T(c, n0, n1, double(sp.s0[p]), double(sp.s1[p]), w, t, detA);
+        e += sp.wt[p * sp.wt_stride] * mu_value<double>(KIND, t, delta);
+        md = fmin(md, detA);
+    }
+}
+
+template <int KIND>
+__global__ void stored_patch_kernel(StoredPatch2 sp, const double2* __restrict__ Xin,
+                                    double2* __restrict__ Xout, const double2* __restrict__ tau,
+                                    double delta, double omega)
+{
+    const int64_t d = blockIdx.x * int64_t(blockDim.x) + threadIdx.x;
+    if (d >= sp.n) { return; }
+    const int32_t slot = sp.slot[d];
+    const double2 pos = Xin[slot];
+    double g[2], h[4], e0, md0;
+    stored_patch_eval<KIND>(sp, Xin, d, delta, g, h, e0, md0);
+    double tx = 0.0, ty = 0.0;
+    if (tau != nullptr) {
+        tx = tau[slot].x;
+        ty = tau[slot].y;
+        g[0] -= tx;
+        g[1] -= ty;
+        e0 -= tx * pos.x + ty * pos.y;
+    }
+    double dl[2];
+    solve2<double>(h, g, dl);
+    double alpha = 1.0;
+    double2 cur = pos;
+    for (int it = 0; it < 10; ++it) {
+        const double2 trial = make_double2(pos.x + alpha * dl[0], pos.y + alpha * dl[1]);
+        double e, md;
+        stored_trial<KIND>(sp, Xin, d, slot, trial, delta, e, md);
+        e -= tx * trial.x + ty * trial.y;
+        if (isfinite(e) && e <= e0 + Tol<double>::energy && (KIND == kUntangle || md > 0.0)) {
+            cur = trial;
+            break;
+        }
+        alpha *= 0.5;
+    }
+    if (omega != 1.0) {
+        cur.x = pos.x + omega * (cur.x - pos.x);
+        cur.y = pos.y + omega * (cur.y - pos.y);
+    }
+    Xout[slot] = cur;
+}
+
+// ---------------------------------------------------------------------------
+// Energy / min-det reductions (fp64, compensated, deterministic two-pass).
+// ---------------------------------------------------------------------------
+struct Comp {
+    double s, c;
+};
+
+__device__ __forceinline__ void comp_add(Comp& a, double x)
+{
+    const double t = a.s + x;
+    if (fabs(a.s) >= fabs(x)) {
+        a.c += (a.s - t) + x;
+    } else {
+        a.c += (x - t) + a.s;
+    }
+    a.s = t;
+}
+
+__device__ __forceinline__ Comp comp_merge(Comp a, Comp b)
+{
+    Comp r = a;
+    comp_add(r, b.s);
+    r.c += b.c;
+    return r;
+}
+
+// Block-level reduction of (compensated sum, min) into partial slot blockIdx.x.
+__device__ __forceinline__ void block_reduce_store(Comp acc, double mn, double* part_s,
+                                                   double* part_c, double* part_m)
+{
+    __shared__ double ss[32], sc[32], sm[32];
+    for (int o = 16; o > 0; o >>= 1) {
+        Comp other;
+        other.s = __shfl_down_sync(0xffffffffu, acc.s, o);
+        other.c = __shfl_down_sync(0xffffffffu, acc.c, o);
+        const double om = __shfl_down_sync(0xffffffffu, mn, o);
+        acc = comp_merge(acc, other);
+        mn = fmin(mn, om);
+    }
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    if (lane == 0) {
+        ss[wid] = acc.s;
+        sc[wid] = acc.c;
+        sm[wid] = mn;
+    }
+    __syncthreads();
+    if (wid == 0) {
+        const int nw = (blockDim.x + 31) >> 5;
+        Comp a {0.0, 0.0};
+        double m = INFINITY;
+        if (lane < nw) {
+            a.s = ss[lane];
+            a.c = sc[lane];
+            m = sm[lane];
+        }
+        for (int o = 16; o > 0; o >>= 1) {
+            Comp other;
+            other.s = __shfl_down_sync(0xffffffffu, a.s, o);
+            other.c = __shfl_down_sync(0xffffffffu, a.c, o);
+            const double om = __shfl_down_sync(0xffffffffu, m, o);
+            a = comp_merge(a, other);
+            m = fmin(m, om);
+        }
+        if (lane == 0) {
+            part_s[blockIdx.x] = a.s;
+            part_c[blockIdx.x] = a.c;
+            part_m[blockIdx.x] = m;
+        }
+    }
+}
+
+struct EnergyStructured2 {
+    int32_t nblocks;
+    const BlockInfo* blocks;
+    const int64_t* cell_off;  // [nblocks+1] prefix of (n0-1)(n1-1)
+    int64_t ncell;
+    const double* W;          // [4] or [ncell*4*4]
+    int32_t w_stride;         // 0 or 4 (per sample)
+    const double* wt;         // [1] or [ncell*4]
+    int32_t wt_stride;
+};
+
+template <int KIND>
+__global__ void energy_structured2_kernel(EnergyStructured2 es, const double2* __restrict__ X,
+                                          double delta, double* part_s, double* part_c,
+                                          double* part_m)
+{
+    Comp acc {0.0, 0.0};
+    double mn = INFINITY;
+    for (int64_t c = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; c < es.ncell;
+         c += int64_t(gridDim.x) * blockDim.x) {
+        int lo = 0, hi = es.nblocks - 1;
+        while (lo < hi) {
+            const int mid = (lo + hi + 1) >> 1;
+            if (es.cell_off[mid] <= c) {
+                lo = mid;
+            } else {
+                hi = mid - 1;
+            }
+        }
+        const BlockInfo bi = es.blocks[lo];
+        const int64_t lc = c - es.cell_off[lo];
+        const int cw = bi.n[1] - 1;
+        const int i = int(lc / cw), j = int(lc % cw);
+        const int64_t base = bi.off + int64_t(i) * bi.n[1] + j;
+        const double2 p[4] = {X[base], X[base + 1], X[base + bi.n[1]], X[base + bi.n[1] + 1]};
+#pragma unroll
+        for (int b = 0; b < 4; ++b) {
+            const int64_t sid = c * 4 + b;
+            const double* w = es.W + sid * es.w_stride;
+            double t[4], detA;
+            assemble_T(p[b], p[b ^ 2], p[b ^ 1], (b & 2) ? -1.0 : 1.0, (b & 1) ? -1.0 : 1.0, w, t,
+                       detA);
+            comp_add(acc, es.wt[sid * es.wt_stride] * mu_value<double>(KIND, t, delta));
+            mn = fmin(mn, detA);
+        }
+    }
+    block_reduce_store(acc, mn, part_s, part_c, part_m);
+}
+
+struct EnergyStored2 {
+    int64_t n;
+    const int32_t* gc;
+    const int32_t* gn0;
+    const int32_t* gn1;
+    const int8_t* s0;
+    const int8_t* s1;
+    const double* W;
+    int32_t w_stride;
+    const double* wt;
+    int32_t wt_stride;
+};
+
+template <int KIND>
+__global__ void energy_stored2_kernel(EnergyStored2 es, const double2* __restrict__ X, double delta,
+                                      double* part_s, double* part_c, double* part_m)
+{
+    Comp acc {0.0, 0.0};
+    double mn = INFINITY;
+    for (int64_t i = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; i < es.n;
+         i += int64_t(gridDim.x) * blockDim.x) {
+        double t[4], detA;
+        assemble_T(X[es.gc[i]], X[es.gn0[i]], X[es.gn1[i]], double(es.s0[i]), double(es.s1[i]),
+                   es.W + i * es.w_stride, t, detA);
+        comp_add(acc, es.wt[i * es.wt_stride] * mu_value<double>(KIND, t, delta));
+        mn = fmin(mn, detA);
+    }
+    block_reduce_store(acc, mn, part_s, part_c, part_m);
+}
+
+// Single-CTA final pass over the partials, fixed order: out[0] = energy, out[1] = min det.
+__global__ void reduce_finalize_kernel(const double* part_s, const double* part_c,
+                                       const double* part_m, int n, double* out_e, double* out_m)
+{
+    Comp acc {0.0, 0.0};
+    double mn = INFINITY;
+    for (int i = threadIdx.x; i < n; i += blockDim.x) {
+        acc = comp_merge(acc, Comp {part_s[i], part_c[i]});
+        mn = fmin(mn, part_m[i]);
+    }
+    __shared__ double ps[1], pc[1], pm[1];
+    // reuse the block reducer with blockIdx.x == 0 semantics
+    block_reduce_store(acc, mn, ps, pc, pm);
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        *out_e = ps[0] + pc[0];
+        *out_m = pm[0];
+    }
+}
+
+}  // namespace egg_b200

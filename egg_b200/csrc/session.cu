@@ -1,0 +1,1169 @@
+// egg_b200 session: host-side validation and structured remap, device-resident
+// state, the block-Jacobi driver, and the C-ABI declared in include/egg_b200.h.
+#include "egg_b200.h"
+#include "kernels2d.cuh"
+
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <limits>
+#include <memory>
+#include <stdexcept>
+#include <string>
+#include <vector>
+
+namespace egg_b200
+{
+
+// ---------------------------------------------------------------------------
+// Errors
+// ---------------------------------------------------------------------------
+struct Error : std::runtime_error {
+    int code;
+    Error(int c, const std::string& m) : std::runtime_error(m), code(c) {}
+};
+
+thread_local std::string g_last_error;
+
+#define EGG_CK(call)                                                                        \
+    do {                                                                                    \
+        cudaError_t e__ = (call);                                                           \
+        if (e__ != cudaSuccess) {                                                           \
+            throw Error(EGG_B200_ERUNTIME, std::string("CUDA error: ") + cudaGetErrorString(e__) + \
+                                             " at " + __FILE__ + ":" + std::to_string(__LINE__)); \
+        }                                                                                   \
+    } while (0)
+
+[[noreturn]] void invalid(const std::string& m) { throw Error(EGG_B200_EINVAL, m); }
+
+// ---------------------------------------------------------------------------
+// Device buffers
+// ---------------------------------------------------------------------------
+template <class T> struct DevBuf {
+    T* p = nullptr;
+    size_t n = 0;
+    DevBuf() = default;
+    DevBuf(const DevBuf&) = delete;
+    DevBuf& operator=(const DevBuf&) = delete;
+    ~DevBuf() { reset(); }
+    void reset()
+    {
+        if (p) { cudaFree(p); }
+        p = nullptr;
+        n = 0;
+    }
+    void alloc(size_t count)
+    {
+        reset();
+        if (count) { EGG_CK(cudaMalloc(reinterpret_cast<void**>(&p), count * sizeof(T))); }
+        n = count;
+    }
+    void upload(const std::vector<T>& h)
+    {
+        alloc(h.size());
+        if (n) { EGG_CK(cudaMemcpy(p, h.data(), n * sizeof(T), cudaMemcpyHostToDevice)); }
+    }
+};
+
+// Tile shapes (cells per CTA) of the interior kernel by working precision.
+constexpr int kCI64 = 8, kCJ64 = 32;
+constexpr int kCI32 = 8, kCJ32 = 32;
+
+enum KernelId { kKInterior = 0, kKStored = 1, kKBroadcast = 2, kKReduce = 3, kKFinal = 4, kKCopy = 5, kKCount = 6 };
+
+struct Session {
+    int dim = 2;
+    int prec = EGG_B200_PREC_FP64;
+    int device = 0;
+    cudaStream_t stream = nullptr;
+
+    int64_t M = 0;       // global nodes
+    int64_t nstore = 0;  // packed store nodes
+    std::vector<BlockInfo> blocks_h;
+    std::vector<int32_t> g2s;       // global -> owner slot (-1 if in no block)
+    std::vector<int32_t> slot_gid;  // store slot -> global id
+    std::vector<double> X_init;     // initial global X (for nodes in no block)
+
+    DevBuf<double> Xbuf[2];
+    int cur = 0;  // index of the canonical buffer
+
+    DevBuf<BlockInfo> blocks_d;
+    // interior DOFs
+    int64_t n_interior = 0;
+    DevBuf<uint8_t> active_d;
+    DevBuf<Tile2> tiles_d;
+    int64_t ntiles = 0;
+    // stored DOFs
+    int64_t n_stored = 0;
+    DevBuf<int32_t> st_slot, st_gc, st_gn0, st_gn1, st_role;
+    DevBuf<int64_t> st_off;
+    DevBuf<int8_t> st_s0, st_s1;
+    DevBuf<double> st_W, st_wt;
+    int st_wstride = 0, st_wtstride = 0;
+    // owner -> copy broadcast
+    int64_t nshare = 0;
+    DevBuf<int32_t> sh_src, sh_dst;
+    // energy stencil
+    bool es_struct = false;
+    int64_t es_ns = 0;
+    DevBuf<int64_t> es_cell_off;
+    int64_t es_ncell = 0;
+    DevBuf<int32_t> es_gc, es_gn0, es_gn1;
+    DevBuf<int8_t> es_s0, es_s1;
+    DevBuf<double> es_W, es_wt;
+    int es_wstride = 0, es_wtstride = 0;
+    // reductions
+    int red_grid = 0;
+    DevBuf<double> part;      // [3 * red_grid]
+    DevBuf<double> red_out;   // [2 * capacity]
+    // profiling
+    bool profiling = false;
+    int64_t launches = 0;  // every kernel launch (copies excluded)
+    DevBuf<double> ckpt;   // device-side checkpoint of the store
+    bool has_ckpt = false;
+    double k_ms[kKCount] = {};
+    int64_t k_launch[kKCount] = {};
+    std::vector<std::pair<int, std::pair<cudaEvent_t, cudaEvent_t>>> pending;
+    std::vector<cudaEvent_t> event_pool;
+
+    ~Session()
+    {
+        if (stream) { cudaStreamSynchronize(stream); }
+        for (auto& p : pending) {
+            event_pool.push_back(p.second.first);
+            event_pool.push_back(p.second.second);
+        }
+        for (cudaEvent_t e : event_pool) { cudaEventDestroy(e); }
+        if (stream) { cudaStreamDestroy(stream); }
+    }
+
+    cudaEvent_t take_event()
+    {
+        if (!event_pool.empty()) {
+            cudaEvent_t e = event_pool.back();
+            event_pool.pop_back();
+            return e;
+        }
+        cudaEvent_t e;
+        EGG_CK(cudaEventCreate(&e));
+        return e;
+    }
+
+    template <class F> void timed(int kid, F&& launch)
+    {
+        if (kid != kKCopy) { ++launches; }
+        if (!profiling) {
+            launch();
+            EGG_CK(cudaGetLastError());
+            return;
+        }
+        cudaEvent_t a = take_event(), b = take_event();
+        EGG_CK(cudaEventRecord(a, stream));
+        launch();
+        EGG_CK(cudaGetLastError());
+        EGG_CK(cudaEventRecord(b, stream));
+        pending.push_back({kid, {a, b}});
+    }
+
+    void harvest()
+    {
+        for (auto& p : pending) {
+            float ms = 0.f;
+            EGG_CK(cudaEventElapsedTime(&ms, p.second.first, p.second.second));
+            k_ms[p.first] += ms;
+            k_launch[p.first] += 1;
+            event_pool.push_back(p.second.first);
+            event_pool.push_back(p.second.second);
+        }
+        pending.clear();
+    }
+
+    void sync()
+    {
+        EGG_CK(cudaStreamSynchronize(stream));
+        harvest();
+    }
+
+    double* X(int i) { return Xbuf[i].p; }
+};
+
+// ---------------------------------------------------------------------------
+// Session construction
+// ---------------------------------------------------------------------------
+static void check_len(int64_t got, int64_t want, const std::string& what)
+{
+    if (got != want) {
+        invalid("validate_context: " + what + " size " + std::to_string(got) + " != " + std::to_string(want));
+    }
+}
+
+static void require_ptr(const void* p, int64_t n, const std::string& what)
+{
+    if (n > 0 && p == nullptr) { invalid("session desc: " + what + " is NULL"); }
+}
+
+static bool rows_uniform(const double* W, int64_t rows, int width)
+{
+    for (int64_t r = 1; r < rows; ++r) {
+        if (std::memcmp(W + r * width, W, sizeof(double) * width) != 0) { return false; }
+    }
+    return true;
+}
+
+// Opt the interior kernels into >48 KB of dynamic shared memory (once per
+// device and precision).
+template <int CI, int CJ, class C> static void set_smem_attr()
+{
+    const int smem = int(sizeof(TileShared2<CI, CJ, C>));
+    EGG_CK(cudaFuncSetAttribute(interior_tile_kernel<CI, CJ, kShape, C>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+    EGG_CK(cudaFuncSetAttribute(interior_tile_kernel<CI, CJ, kUntangle, C>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+    EGG_CK(cudaFuncSetAttribute(interior_tile_kernel<CI, CJ, kShapeSize, C>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+}
+
+static void configure_kernels(int prec)
+{
+    if (prec == EGG_B200_PREC_FP64) {
+        set_smem_attr<kCI64, kCJ64, double>();
+    } else {
+        set_smem_attr<kCI32, kCJ32, float>();
+    }
+}
+
+static Session* create_session(const egg_b200_session_desc& d)
+{
+    const int D = d.dim;
+    if (D != 2 && D != 3) { invalid("egg C++ core: dimension must be 2 or 3, got " + std::to_string(D)); }
+    if (D == 3) { throw Error(EGG_B200_ENOTSUP, "egg_b200: 3D sessions are not built yet"); }
+    if (d.precision != EGG_B200_PREC_FP64 && d.precision != EGG_B200_PREC_MIXED) {
+        invalid("session desc: unknown precision " + std::to_string(d.precision));
+    }
+    const int64_t M = d.num_nodes;
+    if (M < 0) { invalid("session desc: negative num_nodes"); }
+    require_ptr(d.X, M, "X");
+
+    auto S = std::make_unique<Session>();
+    S->dim = D;
+    S->prec = d.precision;
+    S->M = M;
+    S->X_init.assign(d.X, d.X + M * D);
+
+    // Host-side validation and remap come first, so malformed input is
+    // rejected (ValueError) before any device is touched.
+
+    // ---- blocks ----------------------------------------------------------
+    const int nb = d.num_blocks;
+    if (nb < 0) { invalid("structured: negative block count"); }
+    require_ptr(d.interior_shapes, nb, "interior_shapes");
+    S->blocks_h.resize(nb);
+    int64_t off = 0;
+    for (int b = 0; b < nb; ++b) {
+        BlockInfo bi {};
+        bi.off = off;
+        int64_t cnt = 1;
+        for (int k = 0; k < 3; ++k) { bi.n[k] = 1; }
+        for (int k = 0; k < D; ++k) {
+            const int32_t nk = d.interior_shapes[b * D + k];
+            if (nk < 1) { invalid("structured: interior shape entries must be >= 1"); }
+            bi.n[k] = nk;
+            cnt *= nk;
+        }
+        S->blocks_h[b] = bi;
+        off += cnt;
+    }
+    if (off > std::numeric_limits<int32_t>::max()) { throw Error(EGG_B200_ENOTSUP, "egg_b200: store exceeds 2^31 nodes"); }
+    S->nstore = off;
+    require_ptr(d.block_global_dof, off, "block_global_dof");
+    S->slot_gid.assign(d.block_global_dof, d.block_global_dof + off);
+    for (int64_t i = 0; i < off; ++i) {
+        const int32_t g = S->slot_gid[i];
+        if (g < 0 || g >= M) { invalid("structured: block_global_dof id " + std::to_string(g) + " out of range"); }
+    }
+
+    // Owner (lowest block containing the node) and its slot; singular override.
+    std::vector<int32_t> owner_block(M, -1);
+    S->g2s.assign(M, -1);
+    for (int b = 0; b < nb; ++b) {
+        const BlockInfo& bi = S->blocks_h[b];
+        const int64_t cnt = int64_t(bi.n[0]) * bi.n[1] * bi.n[2];
+        for (int64_t f = 0; f < cnt; ++f) {
+            const int32_t g = S->slot_gid[bi.off + f];
+            if (owner_block[g] < 0) {
+                owner_block[g] = b;
+                S->g2s[g] = int32_t(bi.off + f);
+            }
+        }
+    }
+    require_ptr(d.sing_block, d.num_sing, "sing_block");
+    require_ptr(d.sing_logical, d.num_sing * D, "sing_logical");
+    for (int64_t s = 0; s < d.num_sing; ++s) {
+        const int32_t b = d.sing_block[s];
+        if (b < 0 || b >= nb) { invalid("structured: sing_block out of range"); }
+        const BlockInfo& bi = S->blocks_h[b];
+        int64_t f = 0;
+        for (int k = 0; k < D; ++k) {
+            const int32_t l = d.sing_logical[s * D + k];
+            if (l < 0 || l >= bi.n[k]) { invalid("structured: sing_logical out of range"); }
+            f = f * bi.n[k] + l;
+        }
+        const int32_t g = S->slot_gid[bi.off + f];
+        owner_block[g] = b;
+        S->g2s[g] = int32_t(bi.off + f);
+    }
+    // Halo tables: validated (indices in the padded range); this core reads
+    // cross-block neighbours from owner slots and needs no ghost fills.
+    for (const auto* p : {d.halo_src_block, d.halo_dst_block}) { require_ptr(p, d.num_halo, "halo block table"); }
+    for (const auto* p : {d.halo_src_padded, d.halo_dst_padded}) { require_ptr(p, d.num_halo * D, "halo padded table"); }
+    for (int64_t e = 0; e < d.num_halo; ++e) {
+        for (int side = 0; side < 2; ++side) {
+            const int32_t b = side ? d.halo_dst_block[e] : d.halo_src_block[e];
+            const int32_t* pad = side ? d.halo_dst_padded : d.halo_src_padded;
+            if (b < 0 || b >= nb) { invalid("structured: halo block index out of range"); }
+            for (int k = 0; k < D; ++k) {
+                const int32_t v = pad[e * D + k];
+                if (v < 0 || v > S->blocks_h[b].n[k] + 1) { invalid("structured: halo padded index out of range"); }
+            }
+        }
+    }
+    // Owner -> non-owner copies.
+    std::vector<int32_t> sh_src, sh_dst;
+    for (int b = 0; b < nb; ++b) {
+        const BlockInfo& bi = S->blocks_h[b];
+        const int64_t cnt = int64_t(bi.n[0]) * bi.n[1] * bi.n[2];
+        for (int64_t f = 0; f < cnt; ++f) {
+            const int32_t g = S->slot_gid[bi.off + f];
+            if (owner_block[g] == b && S->g2s[g] == int32_t(bi.off + f)) { continue; }
+            sh_src.push_back(S->g2s[g]);
+            sh_dst.push_back(int32_t(bi.off + f));
+        }
+    }
+    S->nshare = int64_t(sh_src.size());
+
+    // ---- group -----------------------------------------------------------
+    const int64_t ndof = d.ndof;
+    const int64_t ts = d.total_samples;
+    if (ndof < 0 || ts < 0) { invalid("validate_context: negative sizes"); }
+    require_ptr(d.dof_idx, ndof, "dof_idx");
+    require_ptr(d.P_of, ndof, "P_of");
+    require_ptr(d.gc, ts, "gc");
+    require_ptr(d.role, ts, "role");
+    for (int k = 0; k < D; ++k) {
+        require_ptr(d.gn[k], ts, "gn" + std::to_string(k));
+        require_ptr(d.s[k], ts, "s" + std::to_string(k));
+    }
+    const bool w_uniform = d.W_inv_len == D * D;
+    if (!w_uniform) { check_len(d.W_inv_len, ts * D * D, "group[0] W_inv"); }
+    require_ptr(d.W_inv, d.W_inv_len, "W_inv");
+    if (d.weight_len != 0 && d.weight_len != 1) { check_len(d.weight_len, ts, "group[0] weight"); }
+    require_ptr(d.weight, d.weight_len, "weight");
+    int64_t sumP = 0;
+    for (int64_t i = 0; i < ndof; ++i) {
+        if (d.P_of[i] < 0) { invalid("validate_context: group[0] negative P_of"); }
+        sumP += d.P_of[i];
+    }
+    if (sumP != ts) {
+        invalid("validate_context: group[0] sum(P_of) " + std::to_string(sumP) + " != total_samples " + std::to_string(ts));
+    }
+    for (int64_t p = 0; p < ts; ++p) {
+        const int32_t r = d.role[p];
+        if (r < -1 || r > D) {
+            invalid("validate_context: group[0] role " + std::to_string(r) + " out of range [-1, " + std::to_string(D) + "]");
+        }
+        auto chk = [&](int32_t v, const char* nm) {
+            if (v < 0 || v >= M) {
+                invalid(std::string("validate_context: group[0] ") + nm + " index " + std::to_string(v) +
+                        " out of range [0, " + std::to_string(M) + ")");
+            }
+        };
+        chk(d.gc[p], "gc");
+        for (int k = 0; k < D; ++k) { chk(d.gn[k][p], ("gn" + std::to_string(k)).c_str()); }
+    }
+
+    std::vector<uint8_t> active(off, 0);
+    std::vector<int32_t> st_slot;
+    std::vector<int64_t> st_off {0};
+    std::vector<int32_t> st_gc, st_gn0, st_gn1, st_role;
+    std::vector<int8_t> st_s0, st_s1;
+    std::vector<double> st_W, st_wt;
+    std::vector<uint8_t> seen_slot(off, 0);
+    int64_t poff = 0;
+    for (int64_t i = 0; i < ndof; ++i) {
+        const int32_t gid = d.dof_idx[i];
+        const int64_t P = d.P_of[i];
+        const int64_t p0 = poff;
+        poff += P;
+        if (gid < 0 || gid >= M) {
+            invalid("validate_context: group[0] dof_idx index " + std::to_string(gid) + " out of range [0, " +
+                    std::to_string(M) + ")");
+        }
+        if (d.entity_tag && d.entity_tag[i] != 0) {
+            throw Error(EGG_B200_ENOTSUP,
+                        "egg_b200: constrained (non-Free) boundary DOFs are not supported by this core yet");
+        }
+        const int32_t slot = S->g2s[gid];
+        if (slot < 0) {
+            invalid("structured: dof_idx references global node " + std::to_string(gid) +
+                    " absent from every block's interior map");
+        }
+        if (seen_slot[slot]) { invalid("validate_context: DOF " + std::to_string(gid) + " listed twice"); }
+        seen_slot[slot] = 1;
+        const int32_t ib = d.interior_block ? d.interior_block[i] : -1;
+        if (ib >= 0) {
+            if (ib >= nb) { invalid("structured: interior_block out of range"); }
+            const BlockInfo& bi = S->blocks_h[ib];
+            int64_t f = 0;
+            for (int k = 0; k < D; ++k) {
+                const int32_t l = d.interior_logical[i * D + k];
+                if (l < 1 || l > bi.n[k] - 2) { invalid("structured: interior_logical not strictly interior"); }
+                f = f * bi.n[k] + l;
+            }
+            if (S->slot_gid[bi.off + f] != gid) {
+                invalid("structured: interior_block/interior_logical does not name the DOF's node");
+            }
+            active[bi.off + f] = 1;
+            S->n_interior++;
+            continue;
+        }
+        st_slot.push_back(slot);
+        for (int64_t p = p0; p < p0 + P; ++p) {
+            auto remap = [&](int32_t g) {
+                const int32_t s = S->g2s[g];
+                if (s < 0) {
+                    invalid("structured: a patch sample references global node " + std::to_string(g) +
+                            " absent from every block's interior map");
+                }
+                return s;
+            };
+            st_gc.push_back(remap(d.gc[p]));
+            st_gn0.push_back(remap(d.gn[0][p]));
+            st_gn1.push_back(remap(d.gn[1][p]));
+            st_s0.push_back(d.s[0][p] < 0 ? int8_t(-1) : int8_t(1));
+            st_s1.push_back(d.s[1][p] < 0 ? int8_t(-1) : int8_t(1));
+            st_role.push_back(d.role[p]);
+            if (!w_uniform) {
+                for (int e = 0; e < D * D; ++e) { st_W.push_back(d.W_inv[p * D * D + e]); }
+            }
+            if (d.weight_len > 1) { st_wt.push_back(d.weight[p]); }
+        }
+        st_off.push_back(int64_t(st_gc.size()));
+    }
+    S->n_stored = int64_t(st_slot.size());
+    if (w_uniform || st_W.empty()) {
+        st_W.assign(d.W_inv, d.W_inv + (w_uniform ? D * D : 0));
+        if (st_W.empty()) { st_W = {1.0, 0.0, 0.0, 1.0}; }
+        S->st_wstride = 0;
+    } else if (rows_uniform(st_W.data(), int64_t(st_W.size()) / (D * D), D * D)) {
+        st_W.resize(D * D);
+        S->st_wstride = 0;
+    } else {
+        S->st_wstride = D * D;
+    }
+    if (st_wt.empty()) {
+        st_wt = {d.weight_len == 1 ? d.weight[0] : 1.0};
+        S->st_wtstride = 0;
+    } else {
+        S->st_wtstride = 1;
+    }
+
+    // ---- energy stencil -------------------------------------------------
+    int64_t ncell = 0;
+    std::vector<int64_t> cell_off(nb + 1, 0);
+    for (int b = 0; b < nb; ++b) {
+        const BlockInfo& bi = S->blocks_h[b];
+        int64_t c = 1;
+        for (int k = 0; k < D; ++k) { c *= std::max(0, bi.n[k] - 1); }
+        cell_off[b] = ncell;
+        ncell += c;
+    }
+    cell_off[nb] = ncell;
+    const int nc = 1 << D;
+    const int64_t ns = d.es_num_samples;
+    if (ns < 0) { invalid("validate_context: energy_stencil negative num_samples"); }
+    const bool es_w_uniform = d.es_W_inv_len == D * D;
+    if (!es_w_uniform) { check_len(d.es_W_inv_len, ns * D * D, "energy_stencil W_inv"); }
+    require_ptr(d.es_W_inv, d.es_W_inv_len, "energy_stencil W_inv");
+    if (d.es_weight_len > 1) { check_len(d.es_weight_len, ns, "energy_stencil weight"); }
+    bool structured = false;
+    if (d.es_structured) {
+        if (ns != ncell * nc) { invalid("energy_stencil: structured stencil size does not match the blocks"); }
+        structured = true;
+    } else {
+        require_ptr(d.es_gc, ns, "energy_stencil gc");
+        for (int k = 0; k < D; ++k) {
+            require_ptr(d.es_gn[k], ns, "energy_stencil gn");
+            require_ptr(d.es_s[k], ns, "energy_stencil s");
+        }
+        for (int64_t i = 0; i < ns; ++i) {
+            auto chk = [&](int32_t v) {
+                if (v < 0 || v >= M) {
+                    invalid("validate_context: energy_stencil index " + std::to_string(v) + " out of range [0, " +
+                            std::to_string(M) + ")");
+                }
+                if (S->g2s[v] < 0) {
+                    invalid("structured: an energy-stencil index references a global node absent from every "
+                            "block's interior map");
+                }
+            };
+            chk(d.es_gc[i]);
+            for (int k = 0; k < D; ++k) { chk(d.es_gn[k][i]); }
+        }
+        // Canonical cell stencil of the blocks?
+        if (ns == ncell * nc) {
+            structured = true;
+            for (int b = 0; b < nb && structured; ++b) {
+                const BlockInfo& bi = S->blocks_h[b];
+                const int w = bi.n[1];
+                for (int i = 0; i + 1 < bi.n[0] && structured; ++i) {
+                    for (int j = 0; j + 1 < w && structured; ++j) {
+                        const int64_t cell = cell_off[b] + int64_t(i) * (w - 1) + j;
+                        int32_t cg[4];
+                        for (int a = 0; a < 4; ++a) { cg[a] = S->slot_gid[bi.off + int64_t(i + (a >> 1)) * w + j + (a & 1)]; }
+                        for (int bb = 0; bb < 4; ++bb) {
+                            const int64_t sid = cell * 4 + bb;
+                            if (d.es_gc[sid] != cg[bb] || d.es_gn[0][sid] != cg[bb ^ 2] || d.es_gn[1][sid] != cg[bb ^ 1] ||
+                                d.es_s[0][sid] != ((bb & 2) ? -1.0 : 1.0) || d.es_s[1][sid] != ((bb & 1) ? -1.0 : 1.0)) {
+                                structured = false;
+                                break;
+                            }
+                        }
+                    }
+                }
+            }
+        }
+    }
+    S->es_struct = structured;
+    S->es_ns = ns;
+    S->es_ncell = ncell;
+    std::vector<double> es_W_h, es_wt_h;
+    std::vector<int32_t> es_a, es_b0, es_b1;
+    std::vector<int8_t> es_s0h, es_s1h;
+    if (es_w_uniform || ns == 0) {
+        es_W_h.assign(d.es_W_inv, d.es_W_inv + (es_w_uniform ? D * D : 0));
+        if (es_W_h.empty()) { es_W_h = {1.0, 0.0, 0.0, 1.0}; }
+        S->es_wstride = 0;
+    } else if (rows_uniform(d.es_W_inv, ns, D * D)) {
+        es_W_h.assign(d.es_W_inv, d.es_W_inv + D * D);
+        S->es_wstride = 0;
+    } else {
+        es_W_h.assign(d.es_W_inv, d.es_W_inv + ns * D * D);
+        S->es_wstride = D * D;
+    }
+    if (d.es_weight_len > 1) {
+        es_wt_h.assign(d.es_weight, d.es_weight + ns);
+        S->es_wtstride = 1;
+    } else {
+        es_wt_h = {d.es_weight_len == 1 ? d.es_weight[0] : 1.0};
+        S->es_wtstride = 0;
+    }
+    if (!structured) {
+        es_a.resize(ns);
+        es_b0.resize(ns);
+        es_b1.resize(ns);
+        es_s0h.resize(ns);
+        es_s1h.resize(ns);
+        for (int64_t i = 0; i < ns; ++i) {
+            es_a[i] = S->g2s[d.es_gc[i]];
+            es_b0[i] = S->g2s[d.es_gn[0][i]];
+            es_b1[i] = S->g2s[d.es_gn[1][i]];
+            es_s0h[i] = d.es_s[0][i] < 0 ? -1 : 1;
+            es_s1h[i] = d.es_s[1][i] < 0 ? -1 : 1;
+        }
+    }
+
+    // ---- interior tiles --------------------------------------------------
+    const int CI = S->prec == EGG_B200_PREC_FP64 ? kCI64 : kCI32;
+    const int CJ = S->prec == EGG_B200_PREC_FP64 ? kCJ64 : kCJ32;
+    std::vector<Tile2> tiles;
+    for (int b = 0; b < nb; ++b) {
+        const BlockInfo& bi = S->blocks_h[b];
+        if (bi.n[0] < 3 || bi.n[1] < 3) { continue; }
+        for (int i0 = 1; i0 <= bi.n[0] - 2; i0 += CI - 1) {
+            for (int j0 = 1; j0 <= bi.n[1] - 2; j0 += CJ - 1) {
+                bool any = false;
+                for (int i = i0; i < std::min(i0 + CI - 1, bi.n[0] - 1) && !any; ++i) {
+                    for (int j = j0; j < std::min(j0 + CJ - 1, bi.n[1] - 1); ++j) {
+                        if (active[bi.off + int64_t(i) * bi.n[1] + j]) {
+                            any = true;
+                            break;
+                        }
+                    }
+                }
+                if (any) { tiles.push_back(Tile2 {b, i0, j0, 0}); }
+            }
+        }
+    }
+    S->ntiles = int64_t(tiles.size());
+
+    // ---- device --------------------------------------------------------------
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) {
+        cudaGetLastError();
+        throw Error(EGG_B200_ENODEV, "select_queue: no CUDA device available (egg_b200 runs on the GPU only)");
+    }
+    if (d.device >= 0) {
+        if (d.device >= ndev) { invalid("session desc: device ordinal out of range"); }
+        EGG_CK(cudaSetDevice(d.device));
+    }
+    EGG_CK(cudaGetDevice(&S->device));
+    EGG_CK(cudaStreamCreateWithFlags(&S->stream, cudaStreamNonBlocking));
+    configure_kernels(S->prec);
+
+    // ---- upload -----------------------------------------------------------
+    S->es_W.upload(es_W_h);
+    S->es_wt.upload(es_wt_h);
+    if (structured) {
+        S->es_cell_off.upload(cell_off);
+    } else {
+        S->es_gc.upload(es_a);
+        S->es_gn0.upload(es_b0);
+        S->es_gn1.upload(es_b1);
+        S->es_s0.upload(es_s0h);
+        S->es_s1.upload(es_s1h);
+    }
+    S->blocks_d.upload(S->blocks_h);
+    S->active_d.upload(active);
+    S->tiles_d.upload(tiles);
+    S->st_slot.upload(st_slot);
+    S->st_off.upload(st_off);
+    S->st_gc.upload(st_gc);
+    S->st_gn0.upload(st_gn0);
+    S->st_gn1.upload(st_gn1);
+    S->st_role.upload(st_role);
+    S->st_s0.upload(st_s0);
+    S->st_s1.upload(st_s1);
+    S->st_W.upload(st_W);
+    S->st_wt.upload(st_wt);
+    S->sh_src.upload(sh_src);
+    S->sh_dst.upload(sh_dst);
+    std::vector<double> Xs(off * D);
+    for (int64_t i = 0; i < off; ++i) {
+        for (int k = 0; k < D; ++k) { Xs[i * D + k] = d.X[int64_t(S->slot_gid[i]) * D + k]; }
+    }
+    S->Xbuf[0].upload(Xs);
+    S->Xbuf[1].alloc(Xs.size());
+    S->cur = 0;
+    S->red_grid = 148 * 4;
+    S->part.alloc(3 * size_t(S->red_grid));
+    S->red_out.alloc(2);
+    EGG_CK(cudaDeviceSynchronize());
+    return S.release();
+}
+
+// ---------------------------------------------------------------------------
+// Sweep driver
+// ---------------------------------------------------------------------------
+template <int KIND> static void launch_interior(Session& S, const double* xin, double* xout, const double* tau,
+                                                double delta, double omega)
+{
+    if (S.ntiles == 0) { return; }
+    const auto* xi = reinterpret_cast<const double2*>(xin);
+    auto* xo = reinterpret_cast<double2*>(xout);
+    const auto* tv = reinterpret_cast<const double2*>(tau);
+    if (S.prec == EGG_B200_PREC_FP64) {
+        constexpr int CI = kCI64, CJ = kCJ64;
+        auto kern = interior_tile_kernel<CI, CJ, KIND, double>;
+        const size_t smem = sizeof(TileShared2<CI, CJ, double>);
+        S.timed(kKInterior, [&] {
+            kern<<<unsigned(S.ntiles), CI * CJ, smem, S.stream>>>(xi, xo, S.tiles_d.p, S.blocks_d.p, S.active_d.p, tv,
+                                                                  delta, omega);
+        });
+    } else {
+        constexpr int CI = kCI32, CJ = kCJ32;
+        auto kern = interior_tile_kernel<CI, CJ, KIND, float>;
+        const size_t smem = sizeof(TileShared2<CI, CJ, float>);
+        S.timed(kKInterior, [&] {
+            kern<<<unsigned(S.ntiles), CI * CJ, smem, S.stream>>>(xi, xo, S.tiles_d.p, S.blocks_d.p, S.active_d.p, tv,
+                                                                  delta, omega);
+        });
+    }
+}
+
+static StoredPatch2 stored_view(Session& S)
+{
+    StoredPatch2 sp;
+    sp.n = S.n_stored;
+    sp.slot = S.st_slot.p;
+    sp.off = S.st_off.p;
+    sp.gc = S.st_gc.p;
+    sp.gn0 = S.st_gn0.p;
+    sp.gn1 = S.st_gn1.p;
+    sp.s0 = S.st_s0.p;
+    sp.s1 = S.st_s1.p;
+    sp.role = S.st_role.p;
+    sp.W = S.st_W.p;
+    sp.w_stride = S.st_wstride;
+    sp.wt = S.st_wt.p;
+    sp.wt_stride = S.st_wtstride;
+    return sp;
+}
+
+template <int KIND> static void launch_stored(Session& S, const double* xin, double* xout, const double* tau,
+                                              double delta, double omega)
+{
+    if (S.n_stored == 0) { return; }
+    const StoredPatch2 sp = stored_view(S);
+    const unsigned grid = unsigned((S.n_stored + 127) / 128);
+    S.timed(kKStored, [&] {
+        stored_patch_kernel<KIND><<<grid, 128, 0, S.stream>>>(sp, reinterpret_cast<const double2*>(xin),
+                                                              reinterpret_cast<double2*>(xout),
+                                                              reinterpret_cast<const double2*>(tau), delta, omega);
+    });
+}
+
+static void launch_broadcast(Session& S, double* x)
+{
+    if (S.nshare == 0) { return; }
+    const unsigned grid = unsigned(std::min<int64_t>((S.nshare + 255) / 256, 148 * 8));
+    S.timed(kKBroadcast, [&] {
+        broadcast2_kernel<<<grid, 256, 0, S.stream>>>(reinterpret_cast<double2*>(x), S.sh_src.p, S.sh_dst.p, S.nshare);
+    });
+}
+
+template <int KIND> static void launch_reduce(Session& S, const double* x, double delta, double* out_e, double* out_m)
+{
+    double* ps = S.part.p;
+    double* pc = ps + S.red_grid;
+    double* pm = pc + S.red_grid;
+    const auto* X2 = reinterpret_cast<const double2*>(x);
+    if (S.es_struct) {
+        EnergyStructured2 es;
+        es.nblocks = int32_t(S.blocks_h.size());
+        es.blocks = S.blocks_d.p;
+        es.cell_off = S.es_cell_off.p;
+        es.ncell = S.es_ncell;
+        es.W = S.es_W.p;
+        es.w_stride = S.es_wstride == 0 ? 0 : 4;
+        es.wt = S.es_wt.p;
+        es.wt_stride = S.es_wtstride;
+        S.timed(kKReduce, [&] {
+            energy_structured2_kernel<KIND><<<S.red_grid, 256, 0, S.stream>>>(es, X2, delta, ps, pc, pm);
+        });
+    } else {
+        EnergyStored2 es;
+        es.n = S.es_ns;
+        es.gc = S.es_gc.p;
+        es.gn0 = S.es_gn0.p;
+        es.gn1 = S.es_gn1.p;
+        es.s0 = S.es_s0.p;
+        es.s1 = S.es_s1.p;
+        es.W = S.es_W.p;
+        es.w_stride = S.es_wstride;
+        es.wt = S.es_wt.p;
+        es.wt_stride = S.es_wtstride;
+        S.timed(kKReduce, [&] {
+            energy_stored2_kernel<KIND><<<S.red_grid, 256, 0, S.stream>>>(es, X2, delta, ps, pc, pm);
+        });
+    }
+    S.timed(kKFinal, [&] { reduce_finalize_kernel<<<1, 1024, 0, S.stream>>>(ps, pc, pm, S.red_grid, out_e, out_m); });
+}
+
+template <int KIND> static void run_impl(Session& S, int n_sweeps, double delta, double omega, int report_every,
+                                         std::vector<double>& E, std::vector<double>& Md)
+{
+    const int k = report_every <= 0 ? n_sweeps : report_every;
+    const int64_t nrep = (int64_t(n_sweeps) + k - 1) / k;
+    if (S.red_out.n < size_t(2 * nrep)) { S.red_out.alloc(size_t(2 * nrep)); }
+    const size_t bytes = size_t(S.nstore) * S.dim * sizeof(double);
+    double* xin = S.X(S.cur);
+    double* xout = S.X(1 - S.cur);
+    S.timed(kKCopy, [&] { EGG_CK(cudaMemcpyAsync(xout, xin, bytes, cudaMemcpyDeviceToDevice, S.stream)); });
+    int64_t ridx = 0;
+    for (int s = 0; s < n_sweeps; ++s) {
+        launch_broadcast(S, xin);
+        launch_interior<KIND>(S, xin, xout, nullptr, delta, omega);
+        launch_stored<KIND>(S, xin, xout, nullptr, delta, omega);
+        if ((s + 1) % k == 0 || s == n_sweeps - 1) {
+            launch_broadcast(S, xout);
+            launch_reduce<KIND>(S, xout, delta, S.red_out.p + 2 * ridx, S.red_out.p + 2 * ridx + 1);
+            ++ridx;
+        }
+        std::swap(xin, xout);
+        S.cur = 1 - S.cur;
+        if ((s + 1) % 64 == 0 && S.profiling) { S.sync(); }
+    }
+    std::vector<double> buf(size_t(2 * nrep));
+    if (nrep) {
+        EGG_CK(cudaMemcpyAsync(buf.data(), S.red_out.p, buf.size() * sizeof(double), cudaMemcpyDeviceToHost, S.stream));
+    }
+    S.sync();
+    E.resize(size_t(nrep));
+    Md.resize(size_t(nrep));
+    for (int64_t i = 0; i < nrep; ++i) {
+        E[i] = buf[2 * i];
+        Md[i] = buf[2 * i + 1];
+    }
+}
+
+template <int KIND> static void energy_impl(Session& S, double delta, double& e, double& m)
+{
+    launch_broadcast(S, S.X(S.cur));
+    launch_reduce<KIND>(S, S.X(S.cur), delta, S.red_out.p, S.red_out.p + 1);
+    double buf[2];
+    EGG_CK(cudaMemcpyAsync(buf, S.red_out.p, sizeof(buf), cudaMemcpyDeviceToHost, S.stream));
+    S.sync();
+    e = buf[0];
+    m = buf[1];
+}
+
+// ---------------------------------------------------------------------------
+// Oracle-primitive kernels
+// ---------------------------------------------------------------------------
+__global__ void metric_eval_kernel(int kind, double delta, const double* t, int64_t n, double* mu, double* g,
+                                   double* H)
+{
+    const int64_t i = blockIdx.x * int64_t(blockDim.x) + threadIdx.x;
+    if (i >= n) { return; }
+    double m, gg[4], hh[16];
+    mu_eval<double>(kind, t + 4 * i, delta, m, gg, hh);
+    mu[i] = m;
+    for (int k = 0; k < 4; ++k) { g[4 * i + k] = gg[k]; }
+    for (int k = 0; k < 16; ++k) { H[16 * i + k] = hh[k]; }
+}
+
+template <int KIND> __global__ void patch_eval_kernel(StoredPatch2 sp, const double2* X, double delta, double* out)
+{
+    double g[2], h[4], e0, md;
+    stored_patch_eval<KIND>(sp, X, 0, delta, g, h, e0, md);
+    double st[2];
+    solve2<double>(h, g, st);
+    out[0] = g[0];
+    out[1] = g[1];
+    for (int k = 0; k < 4; ++k) { out[2 + k] = h[k]; }
+    out[6] = e0;
+    out[7] = md;
+    out[8] = st[0];
+    out[9] = st[1];
+}
+
+__global__ void newton_step_kernel(const double* g, const double* h, double* out) { solve2<double>(h, g, out); }
+
+template <class F> static int guarded(F&& f)
+{
+    try {
+        f();
+        return EGG_B200_OK;
+    } catch (const Error& e) {
+        g_last_error = e.what();
+        return e.code;
+    } catch (const std::bad_alloc&) {
+        g_last_error = "egg_b200: host out of memory";
+        return EGG_B200_ERUNTIME;
+    } catch (const std::exception& e) {
+        g_last_error = e.what();
+        return EGG_B200_ERUNTIME;
+    }
+}
+
+static void check_objective(int obj)
+{
+    if (obj != EGG_B200_OBJ_SHAPE && obj != EGG_B200_OBJ_UNTANGLE && obj != EGG_B200_OBJ_SHAPE_SIZE) {
+        invalid("unknown objective kind " + std::to_string(obj));
+    }
+}
+
+}  // namespace egg_b200
+
+// ===========================================================================
+// C-ABI
+// ===========================================================================
+using namespace egg_b200;
+
+struct egg_b200_session {
+    Session* impl;
+};
+
+extern "C" {
+
+int egg_b200_abi_version(void) { return EGG_B200_ABI_VERSION; }
+
+const char* egg_b200_last_error(void) { return g_last_error.c_str(); }
+
+int egg_b200_device_count(int* count)
+{
+    return guarded([&] {
+        int n = 0;
+        if (cudaGetDeviceCount(&n) != cudaSuccess) {
+            cudaGetLastError();
+            n = 0;
+        }
+        *count = n;
+    });
+}
+
+int egg_b200_session_create(const egg_b200_session_desc* desc, egg_b200_session** out)
+{
+    return guarded([&] {
+        if (!desc || !out) { invalid("egg_b200_session_create: NULL argument"); }
+        *out = nullptr;
+        Session* s = create_session(*desc);
+        *out = new egg_b200_session {s};
+    });
+}
+
+int egg_b200_session_destroy(egg_b200_session* s)
+{
+    return guarded([&] {
+        if (!s) { return; }
+        delete s->impl;
+        delete s;
+    });
+}
+
+int egg_b200_session_run(egg_b200_session* s, int32_t n_sweeps, int32_t objective, double delta, double omega,
+                         int32_t report_every, double* energies, double* mindets, int64_t capacity,
+                         int64_t* n_reported)
+{
+    return guarded([&] {
+        if (!s) { invalid("run: NULL session"); }
+        check_objective(objective);
+        if (n_sweeps < 0) { invalid("run: n_sweeps must be >= 0"); }
+        Session& S = *s->impl;
+        EGG_CK(cudaSetDevice(S.device));
+        std::vector<double> E, Md;
+        if (n_sweeps > 0) {
+            switch (objective) {
+            case EGG_B200_OBJ_SHAPE: run_impl<kShape>(S, n_sweeps, delta, omega, report_every, E, Md); break;
+            case EGG_B200_OBJ_UNTANGLE: run_impl<kUntangle>(S, n_sweeps, delta, omega, report_every, E, Md); break;
+            default: run_impl<kShapeSize>(S, n_sweeps, delta, omega, report_every, E, Md); break;
+            }
+        }
+        if (n_reported) { *n_reported = int64_t(E.size()); }
+        if (int64_t(E.size()) > capacity) { invalid("run: report buffer too small"); }
+        for (size_t i = 0; i < E.size(); ++i) {
+            if (energies) { energies[i] = E[i]; }
+            if (mindets) { mindets[i] = Md[i]; }
+        }
+    });
+}
+
+int egg_b200_session_energy(egg_b200_session* s, int32_t objective, double delta, double* energy, double* mindet)
+{
+    return guarded([&] {
+        if (!s) { invalid("energy: NULL session"); }
+        check_objective(objective);
+        Session& S = *s->impl;
+        EGG_CK(cudaSetDevice(S.device));
+        double e = 0, m = 0;
+        switch (objective) {
+        case EGG_B200_OBJ_SHAPE: energy_impl<kShape>(S, delta, e, m); break;
+        case EGG_B200_OBJ_UNTANGLE: energy_impl<kUntangle>(S, delta, e, m); break;
+        default: energy_impl<kShapeSize>(S, delta, e, m); break;
+        }
+        if (energy) { *energy = e; }
+        if (mindet) { *mindet = m; }
+    });
+}
+
+int egg_b200_session_get_X(egg_b200_session* s, double* X, int64_t len)
+{
+    return guarded([&] {
+        if (!s || !X) { invalid("get_X: NULL argument"); }
+        Session& S = *s->impl;
+        const int D = S.dim;
+        if (len != S.M * D) { invalid("get_X: output length " + std::to_string(len) + " != num_nodes*dim"); }
+        EGG_CK(cudaSetDevice(S.device));
+        std::vector<double> store(size_t(S.nstore) * D);
+        if (!store.empty()) {
+            EGG_CK(cudaMemcpyAsync(store.data(), S.X(S.cur), store.size() * sizeof(double), cudaMemcpyDeviceToHost,
+                                   S.stream));
+        }
+        S.sync();
+        for (int64_t g = 0; g < S.M; ++g) {
+            const int32_t slot = S.g2s[g];
+            for (int k = 0; k < D; ++k) {
+                X[g * D + k] = slot >= 0 ? store[size_t(slot) * D + k] : S.X_init[g * D + k];
+            }
+        }
+    });
+}
+
+int egg_b200_session_set_X(egg_b200_session* s, const double* X, int64_t len)
+{
+    return guarded([&] {
+        if (!s || !X) { invalid("set_X: NULL argument"); }
+        Session& S = *s->impl;
+        const int D = S.dim;
+        if (len != S.M * D) { invalid("set_X: input length != num_nodes*dim"); }
+        EGG_CK(cudaSetDevice(S.device));
+        std::vector<double> store(size_t(S.nstore) * D);
+        for (int64_t i = 0; i < S.nstore; ++i) {
+            for (int k = 0; k < D; ++k) { store[i * D + k] = X[int64_t(S.slot_gid[i]) * D + k]; }
+        }
+        S.X_init.assign(X, X + len);
+        if (!store.empty()) {
+            EGG_CK(cudaMemcpyAsync(S.X(S.cur), store.data(), store.size() * sizeof(double), cudaMemcpyHostToDevice,
+                                   S.stream));
+        }
+        S.sync();
+    });
+}
+
+int egg_b200_session_info(egg_b200_session* s, int64_t* out, int32_t n)
+{
+    return guarded([&] {
+        if (!s || !out) { invalid("info: NULL argument"); }
+        Session& S = *s->impl;
+        const int64_t v[10] = {S.dim,         S.M,      S.nstore, S.n_interior + S.n_stored, S.n_interior, S.n_stored,
+                               S.nshare,      S.es_ns,  S.es_struct ? 1 : 0, S.prec};
+        for (int i = 0; i < n && i < 10; ++i) { out[i] = v[i]; }
+    });
+}
+
+int egg_b200_session_set_profiling(egg_b200_session* s, int32_t enable)
+{
+    return guarded([&] {
+        if (!s) { invalid("set_profiling: NULL session"); }
+        s->impl->sync();
+        s->impl->profiling = enable != 0;
+    });
+}
+
+int egg_b200_session_kernel_stats(egg_b200_session* s, int32_t kernel_id, double* total_ms, int64_t* launches)
+{
+    return guarded([&] {
+        if (!s) { invalid("kernel_stats: NULL session"); }
+        if (kernel_id < 0 || kernel_id >= kKCount) { invalid("kernel_stats: unknown kernel id"); }
+        s->impl->sync();
+        if (total_ms) { *total_ms = s->impl->k_ms[kernel_id]; }
+        if (launches) { *launches = s->impl->k_launch[kernel_id]; }
+    });
+}
+
+int egg_b200_session_checkpoint(egg_b200_session* s)
+{
+    return guarded([&] {
+        if (!s) { invalid("checkpoint: NULL session"); }
+        Session& S = *s->impl;
+        EGG_CK(cudaSetDevice(S.device));
+        const size_t n = size_t(S.nstore) * S.dim;
+        if (S.ckpt.n != n) { S.ckpt.alloc(n); }
+        if (n) { EGG_CK(cudaMemcpyAsync(S.ckpt.p, S.X(S.cur), n * sizeof(double), cudaMemcpyDeviceToDevice, S.stream)); }
+        S.sync();
+        S.has_ckpt = true;
+    });
+}
+
+int egg_b200_session_restore(egg_b200_session* s)
+{
+    return guarded([&] {
+        if (!s) { invalid("restore: NULL session"); }
+        Session& S = *s->impl;
+        if (!S.has_ckpt) { invalid("restore: no checkpoint taken"); }
+        EGG_CK(cudaSetDevice(S.device));
+        const size_t n = size_t(S.nstore) * S.dim;
+        if (n) { EGG_CK(cudaMemcpyAsync(S.X(S.cur), S.ckpt.p, n * sizeof(double), cudaMemcpyDeviceToDevice, S.stream)); }
+        S.sync();
+    });
+}
+
+int egg_b200_session_launch_count(egg_b200_session* s, int64_t* launches)
+{
+    return guarded([&] {
+        if (!s || !launches) { invalid("launch_count: NULL argument"); }
+        *launches = s->impl->launches;
+    });
+}
+
+int egg_b200_session_reset_stats(egg_b200_session* s)
+{
+    return guarded([&] {
+        if (!s) { invalid("reset_stats: NULL session"); }
+        s->impl->sync();
+        s->impl->launches = 0;
+        for (int k = 0; k < kKCount; ++k) {
+            s->impl->k_ms[k] = 0;
+            s->impl->k_launch[k] = 0;
+        }
+    });
+}
+
+int egg_b200_metric_eval(int32_t objective, double delta, const double* t, int64_t n, double* mu, double* grad,
+                         double* hess)
+{
+    return guarded([&] {
+        check_objective(objective);
+        if (n < 0) { invalid("metric_eval: negative n"); }
+        if (n == 0) { return; }
+        if (!t || !mu || !grad || !hess) { invalid("metric_eval: NULL argument"); }
+        DevBuf<double> dt, dm, dg, dh;
+        dt.upload(std::vector<double>(t, t + 4 * n));
+        dm.alloc(n);
+        dg.alloc(4 * n);
+        dh.alloc(16 * n);
+        metric_eval_kernel<<<unsigned((n + 127) / 128), 128>>>(objective, delta, dt.p, n, dm.p, dg.p, dh.p);
+        EGG_CK(cudaGetLastError());
+        EGG_CK(cudaMemcpy(mu, dm.p, n * sizeof(double), cudaMemcpyDeviceToHost));
+        EGG_CK(cudaMemcpy(grad, dg.p, 4 * n * sizeof(double), cudaMemcpyDeviceToHost));
+        EGG_CK(cudaMemcpy(hess, dh.p, 16 * n * sizeof(double), cudaMemcpyDeviceToHost));
+    });
+}
+
+int egg_b200_patch_eval(int32_t objective, double delta, const double* X, int64_t n_nodes, int32_t P,
+                        const int32_t* gc, const int32_t* gn0, const int32_t* gn1, const double* s0, const double* s1,
+                        const double* W_inv, const int32_t* role, double* grad, double* hess, double* energy,
+                        double* mindet, double* step)
+{
+    return guarded([&] {
+        check_objective(objective);
+        if (P < 0 || n_nodes <= 0) { invalid("patch_eval: bad sizes"); }
+        for (int p = 0; p < P; ++p) {
+            for (int32_t v : {gc[p], gn0[p], gn1[p]}) {
+                if (v < 0 || v >= n_nodes) { invalid("patch_eval: node index out of range"); }
+            }
+            if (role[p] < -1 || role[p] > 2) { invalid("patch_eval: role out of range"); }
+        }
+        DevBuf<double> dX, dW, dwt, dout;
+        DevBuf<int32_t> dgc, dgn0, dgn1, drole, dslot;
+        DevBuf<int64_t> doff;
+        DevBuf<int8_t> ds0, ds1;
+        dX.upload(std::vector<double>(X, X + 2 * n_nodes));
+        dW.upload(std::vector<double>(W_inv, W_inv + 4 * P));
+        dwt.upload(std::vector<double>{1.0});
+        dgc.upload(std::vector<int32_t>(gc, gc + P));
+        dgn0.upload(std::vector<int32_t>(gn0, gn0 + P));
+        dgn1.upload(std::vector<int32_t>(gn1, gn1 + P));
+        drole.upload(std::vector<int32_t>(role, role + P));
+        std::vector<int8_t> a(P), b(P);
+        for (int p = 0; p < P; ++p) {
+            a[p] = s0[p] < 0 ? -1 : 1;
+            b[p] = s1[p] < 0 ? -1 : 1;
+        }
+        ds0.upload(a);
+        ds1.upload(b);
+        doff.upload(std::vector<int64_t>{0, P});
+        dslot.upload(std::vector<int32_t>{0});
+        dout.alloc(10);
+        StoredPatch2 sp {1, dslot.p, doff.p, dgc.p, dgn0.p, dgn1.p, ds0.p, ds1.p, drole.p, dW.p, 4, dwt.p, 0};
+        switch (objective) {
+        case EGG_B200_OBJ_SHAPE: patch_eval_kernel<kShape><<<1, 1>>>(sp, reinterpret_cast<const double2*>(dX.p), delta, dout.p); break;
+        case EGG_B200_OBJ_UNTANGLE: patch_eval_kernel<kUntangle><<<1, 1>>>(sp, reinterpret_cast<const double2*>(dX.p), delta, dout.p); break;
+        default: patch_eval_kernel<kShapeSize><<<1, 1>>>(sp, reinterpret_cast<const double2*>(dX.p), delta, dout.p); break;
+        }
+        EGG_CK(cudaGetLastError());
+        double o[10];
+        EGG_CK(cudaMemcpy(o, dout.p, sizeof(o), cudaMemcpyDeviceToHost));
+        grad[0] = o[0];
+        grad[1] = o[1];
+        for (int k = 0; k < 4; ++k) { hess[k] = o[2 + k]; }
+        *energy = o[6];
+        *mindet = o[7];
+        step[0] = o[8];
+        step[1] = o[9];
+    });
+}
+
+int egg_b200_newton_step(const double* grad, const double* hess, double* step)
+{
+    return guarded([&] {
+        if (!grad || !hess || !step) { invalid("newton_step: NULL argument"); }
+        DevBuf<double> dg, dh, ds;
+        dg.upload(std::vector<double>(grad, grad + 2));
+        dh.upload(std::vector<double>(hess, hess + 4));
+        ds.alloc(2);
+        newton_step_kernel<<<1, 1>>>(dg.p, dh.p, ds.p);
+        EGG_CK(cudaGetLastError());
+        EGG_CK(cudaMemcpy(step, ds.p, 2 * sizeof(double), cudaMemcpyDeviceToHost));
+    });
+}
+
+}  // extern "C"

@@ -1,0 +1,318 @@
+"""Builders for the sweep-context wire and the structured block tables.
+
+The egg core consumes two dicts (``ctx_arrays`` and ``structured``) whose
+format is fixed by the reference's pybind boundary:
+
+* ``ctx_arrays = {"groups": [group], "energy_stencil": stencil}`` as assembled by
+  ``egg/smoothing/flat_context.py:136-346`` (``build_flat_context``) and unpacked
+  by ``src/bindings.cpp:332-489`` (``unpack_context``);
+* ``structured = {interior_shapes, block_global_dof, halo_src_block,
+  halo_src_padded, halo_dst_block, halo_dst_padded, sing_block,
+  sing_logical}`` as packed by ``egg/smoothing/cpp_backend.py:679-691``.
+
+This module produces the same dicts from per-block global-node-id arrays with
+vectorised numpy, so tests and benchmarks can build inputs without the egg
+Python package.  Conventions (kept identical because the wire is an interface):
+
+* A block is an integer array of global node ids with shape ``(n_0, ..., n_{d-1})``;
+  cells are enumerated block by block in C order.
+* Corner index ``b`` in ``0 .. 2**d - 1`` packs per-axis offset bits with axis 0
+  most significant; sample id ``= 2**d * cell + b``
+  (``egg/smoothing/flat_context.py:40-121``).
+* Sample ``(cell, b)`` has corner ``C[cell, b]``, axis-``k`` neighbour
+  ``C[cell, b ^ bit_k]`` and sign ``+1`` if bit ``k`` of ``b`` is clear else ``-1``.
+* A node at local corner ``a`` meets sample ``b`` of the same cell with role
+  ``0`` (``a == b``), ``1 + k`` (``a ^ b == bit_k``) or ``-1`` otherwise.
+* Interior-eligible DOFs (logical index in ``[1, n-2]`` on every axis of their
+  block, target a uniform multiple of the identity) carry no stored samples:
+  ``interior_block``/``interior_logical`` name them and ``P_of`` is 0
+  (``egg/smoothing/flat_context.py:211-238``).
+
+Extension (accepted by this repository's core only): ``compact=True`` emits the
+energy stencil as ``{"num_samples": ns, "structured": 1, "W_inv": row}`` with no
+per-sample index arrays, for the canonical cell stencil of the blocks.  The
+reference core requires the explicit arrays (``compact=False``).
+"""
+
+from __future__ import annotations
+
+import numpy as np
+
+__all__ = [
+    "axis_bits",
+    "role_table",
+    "cell_corner_ids",
+    "cell_stencil",
+    "flat_wire",
+    "structured_tables",
+    "free_mask_from_fixed",
+]
+
+
+def axis_bits(d: int) -> np.ndarray:
+    """Corner-index bit of each axis (axis 0 is the most significant bit)."""
+    return np.array([1 << (d - 1 - k) for k in range(d)], dtype=np.int64)
+
+
+def role_table(d: int) -> np.ndarray:
+    """``role[a, b]`` of local corner ``a`` in the sample at local corner ``b``."""
+    nc = 1 << d
+    bits = axis_bits(d)
+    role = np.full((nc, nc), -1, dtype=np.int32)
+    b = np.arange(nc)
+    role[b, b] = 0
+    for k in range(d):
+        role[b, b ^ bits[k]] = 1 + k
+    return role
+
+
+def cell_corner_ids(blocks: list[np.ndarray], d: int) -> np.ndarray:
+    """``C[cell, a]``: global id of local corner ``a`` of every cell, all blocks."""
+    nc = 1 << d
+    cols_all = []
+    for ids in blocks:
+        ids = np.asarray(ids)
+        shp = ids.shape
+        if any(s < 2 for s in shp):
+            continue
+        cols = []
+        for a in range(nc):
+            sl = tuple(
+                slice((a >> (d - 1 - ax)) & 1, ((a >> (d - 1 - ax)) & 1) + shp[ax] - 1)
+                for ax in range(d)
+            )
+            cols.append(ids[sl].reshape(-1))
+        cols_all.append(np.stack(cols, axis=1))
+    if not cols_all:
+        return np.zeros((0, nc), dtype=np.int64)
+    return np.concatenate(cols_all).astype(np.int64)
+
+
+def cell_stencil(blocks: list[np.ndarray], d: int):
+    """Per-sample ``(gc, gn[d], s[d])`` in canonical sample order."""
+    nc = 1 << d
+    bits = axis_bits(d)
+    C = cell_corner_ids(blocks, d)
+    b = np.arange(nc)
+    sgn = np.where((b[:, None] & bits[None, :]) == 0, 1.0, -1.0)  # (nc, d)
+    gc = C.reshape(-1)
+    gn = [C[:, b ^ bits[k]].reshape(-1) for k in range(d)]
+    s = [np.tile(sgn[:, k], C.shape[0]) for k in range(d)]
+    return C, gc, gn, s
+
+
+def free_mask_from_fixed(n_nodes: int, fixed_ids) -> np.ndarray:
+    m = np.ones(n_nodes, dtype=bool)
+    m[np.asarray(fixed_ids, dtype=np.int64)] = False
+    return m
+
+
+def flat_wire(
+    blocks: list[np.ndarray],
+    free_mask: np.ndarray,
+    d: int,
+    *,
+    w_inv: np.ndarray | None = None,
+    compact: bool = False,
+) -> dict:
+    """The ``{"groups", "energy_stencil"}`` wire for Free (unconstrained) DOFs.
+
+    ``w_inv`` is one ``(d, d)`` inverse target shared by every sample (default
+    identity) or ``(ns, d, d)`` per sample in canonical order.  Mirrors
+    ``build_flat_context`` (``egg/smoothing/flat_context.py:136-346``) for the
+    case without constraints, interface, curvature or directional terms.
+    ``compact`` drops the energy-stencil index arrays (see module docstring) and
+    sends a uniform target as one shared row.
+    """
+    blocks = [np.asarray(b) for b in blocks]
+    nc = 1 << d
+    dd = d * d
+    N = int(free_mask.shape[0])
+    if w_inv is None:
+        w_inv = np.eye(d)
+    w_inv = np.asarray(w_inv, dtype=np.float64)
+    uniform_w = w_inv.shape == (d, d)
+    w0 = w_inv if uniform_w else (w_inv[0] if len(w_inv) else np.eye(d))
+    synth_interior = bool(
+        np.allclose(w0, w0[0, 0] * np.eye(d)) and (uniform_w or np.allclose(w_inv, w0))
+    )
+
+    # Interior-eligible nodes: strictly inside one block on every axis.
+    node_block = np.full(N, -1, dtype=np.int32)
+    node_logical = np.zeros((N, d), dtype=np.int32)
+    if synth_interior:
+        for bi, ids in enumerate(blocks):
+            sh = ids.shape
+            if any(s < 3 for s in sh):
+                continue
+            inner = ids[tuple(slice(1, s - 1) for s in sh)].reshape(-1)
+            grids = np.meshgrid(*[np.arange(1, s - 1, dtype=np.int32) for s in sh], indexing="ij")
+            node_block[inner] = bi
+            node_logical[inner] = np.stack([g.reshape(-1) for g in grids], axis=1)
+    node_interior = node_block >= 0
+
+    C = cell_corner_ids(blocks, d)
+    ncell = C.shape[0]
+    ns = ncell * nc
+    bits = axis_bits(d)
+    bidx = np.arange(nc)
+    sgn = np.where((bidx[:, None] & bits[None, :]) == 0, 1.0, -1.0)
+    role = role_table(d)
+
+    # Membership only for stored-patch DOFs (moving, not interior-eligible):
+    # restrict to cells that touch such a node, so large grids with few stored
+    # DOFs never materialise the full node x sample table.
+    stored_node = free_mask & ~node_interior
+    touch = stored_node[C]  # (ncell, nc)
+    cells = np.flatnonzero(touch.any(axis=1))
+    Ct = C[cells]  # (m, nc)
+    # Rows (cell, a, b) restricted to stored nodes at corner a.
+    m_node = np.repeat(Ct[:, :, None], nc, axis=2).reshape(-1)
+    m_sid = (nc * cells[:, None, None] + bidx[None, None, :]).repeat(nc, axis=1).reshape(-1)
+    m_role = np.tile(role.reshape(-1), cells.shape[0])
+    keep = stored_node[m_node]
+    m_node, m_sid, m_role = m_node[keep], m_sid[keep], m_role[keep]
+    perm = np.argsort(m_node, kind="stable")
+    m_node, m_sid, m_role = m_node[perm], m_sid[perm], m_role[perm]
+
+    def fields(sid: np.ndarray, *, uniform_out: bool) -> dict:
+        cell = sid // nc
+        b = sid % nc
+        out = {"gc": C[cell, b].astype(np.int32)}
+        for k in range(d):
+            out[f"gn{k}"] = C[cell, b ^ bits[k]].astype(np.int32)
+            out[f"s{k}"] = sgn[b, k].astype(np.float64)
+        if uniform_w and uniform_out:
+            W = w_inv.reshape(1, dd)
+        elif uniform_w:
+            W = np.broadcast_to(w_inv, (sid.shape[0], d, d)).reshape(-1, dd)
+        else:
+            W = w_inv[sid].reshape(-1, dd)
+        out["W_inv"] = np.ascontiguousarray(W, dtype=np.float64)
+        return out
+
+    groups = []
+    dofs = np.flatnonzero(free_mask)
+    if dofs.size:
+        P_of = np.zeros(dofs.size, dtype=np.int32)
+        if m_node.size:
+            uniq, cnt = np.unique(m_node, return_counts=True)
+            P_of[np.searchsorted(dofs, uniq)] = cnt
+        g = {
+            "D": int(dofs.size),
+            "role": m_role.astype(np.int32),
+            "dof_idx": dofs.astype(np.int32),
+            "P_of": P_of,
+            "interior_block": np.ascontiguousarray(node_block[dofs]),
+            "interior_logical": np.ascontiguousarray(node_logical[dofs]),
+            "entities": {
+                "free": {
+                    "tag": 0,
+                    "kFields": 0,
+                    "dof_local": np.arange(dofs.size, dtype=np.int32),
+                    "records": np.zeros(0, dtype=np.float64),
+                }
+            },
+        }
+        g.update(fields(m_sid, uniform_out=True))
+        groups.append(g)
+
+    if compact:
+        if not uniform_w:
+            raise ValueError("compact wire requires a uniform target")
+        es = {"num_samples": int(ns), "structured": 1, "W_inv": w_inv.reshape(1, dd).copy()}
+    else:
+        es = {"num_samples": int(ns)}
+        es.update(fields(np.arange(ns, dtype=np.int64), uniform_out=True))
+    return {"groups": groups, "energy_stencil": es}
+
+
+def structured_tables(blocks: list[np.ndarray]) -> dict:
+    """The ``structured`` dict for hand-assembled blocks (shared-id twin matching).
+
+    Follows ``build_structured_context_from_block_maps``
+    (``egg/smoothing/cpp_backend.py:120-244``): a face node that also lives in
+    another block gets a ghost entry filled by the node one step behind its twin
+    (the lowest-block copy of that node when it is itself shared); ambiguous
+    cases are left out.  Singularity tables stay empty.
+    """
+    blocks = [np.asarray(b) for b in blocks]
+    d = blocks[0].ndim
+    shapes = [tuple(int(s) for s in b.shape) for b in blocks]
+    flat = [np.ascontiguousarray(b.reshape(-1), dtype=np.int32) for b in blocks]
+    n_ids = max(int(f.max()) for f in flat if f.size) + 1
+    counts = np.zeros(n_ids, dtype=np.int64)
+    for f in flat:
+        counts += np.bincount(f, minlength=n_ids)
+    shared = counts > 1
+    where: dict[int, list] = {}
+    for bi, ids in enumerate(blocks):
+        for logical in zip(*np.nonzero(shared[ids])):
+            li = tuple(int(c) for c in logical)
+            where.setdefault(int(ids[li]), []).append((bi, li))
+    member = []
+    for f in flat:
+        m = np.zeros(n_ids, dtype=bool)
+        m[f] = True
+        member.append(m)
+
+    def behind(dst_block: int, gid: int):
+        found = None
+        loc = None
+        for bj, lj in where.get(gid, ()):
+            if bj == dst_block:
+                continue
+            shp = shapes[bj]
+            for ax in range(d):
+                if lj[ax] == 0:
+                    step = 1
+                elif lj[ax] == shp[ax] - 1:
+                    step = -1
+                else:
+                    continue
+                inner = list(lj)
+                inner[ax] += step
+                g_in = int(blocks[bj][tuple(inner)])
+                if member[dst_block][g_in]:
+                    continue
+                if found is not None and found != g_in:
+                    return None
+                found = g_in
+                loc = (bj, tuple(inner))
+        if found is None:
+            return None
+        if shared[found]:
+            return min(where[found])
+        return loc
+
+    sb, sp, db, dp = [], [], [], []
+    for bi, ids in enumerate(blocks):
+        shp = shapes[bi]
+        for ax in range(d):
+            for side in (0, 1):
+                fixed = 0 if side == 0 else shp[ax] - 1
+                face = np.take(ids, fixed, axis=ax)
+                for free_idx in zip(*np.nonzero(shared[face])):
+                    gid = int(face[free_idx])
+                    logical = list(free_idx[:ax]) + [fixed] + list(free_idx[ax:])
+                    hit = behind(bi, gid)
+                    if hit is None:
+                        continue
+                    bj, inner = hit
+                    ghost = [c + 1 for c in logical]
+                    ghost[ax] = 0 if side == 0 else shp[ax] + 1
+                    sb.append(bj)
+                    sp.append(tuple(c + 1 for c in inner))
+                    db.append(bi)
+                    dp.append(tuple(ghost))
+    rows = lambda v: np.asarray(v, dtype=np.int32).reshape(-1, d)  # noqa: E731
+    return {
+        "interior_shapes": [np.asarray(s, dtype=np.int32) for s in shapes],
+        "block_global_dof": flat,
+        "halo_src_block": np.asarray(sb, dtype=np.int32),
+        "halo_src_padded": rows(sp),
+        "halo_dst_block": np.asarray(db, dtype=np.int32),
+        "halo_dst_padded": rows(dp),
+        "sing_block": np.zeros(0, dtype=np.int32),
+        "sing_logical": np.zeros((0, d), dtype=np.int32),
+    }

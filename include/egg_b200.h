@@ -1,0 +1,191 @@
+/* egg_b200 C-ABI: the B200 (sm_100a) structured TMOP smoother/untangler core.
+ *
+ * Plain C types only (pointers, sizes, ints, doubles); no exceptions cross the
+ * boundary.  Every entry point returns an int status (EGG_B200_OK on success);
+ * egg_b200_last_error() gives the message of the last failure on the calling
+ * thread.  Each entry point names the reference interface it replaces
+ * (file:line in the reference checkout).  All calls are synchronous: they
+ * return after the session's CUDA stream has drained, like the reference's
+ * q.wait() at every call boundary.
+ */
+#ifndef EGG_B200_H
+#define EGG_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define EGG_B200_ABI_VERSION 1
+
+/* Status codes.  EINVAL maps to Python ValueError, the others to RuntimeError
+ * (the reference's std::invalid_argument / std::runtime_error split,
+ * src/bindings.cpp:80-90,98-252,64-69). */
+#define EGG_B200_OK 0
+#define EGG_B200_EINVAL 1
+#define EGG_B200_ERUNTIME 2
+#define EGG_B200_ENODEV 3
+#define EGG_B200_ENOTSUP 4
+
+/* Objective kinds (src/metric.hpp:984-997 make_objective: "untangle",
+ * "shape_size", anything else -> shape barrier). */
+#define EGG_B200_OBJ_SHAPE 0
+#define EGG_B200_OBJ_UNTANGLE 1
+#define EGG_B200_OBJ_SHAPE_SIZE 2
+
+/* Arithmetic of the sweep: plain fp64, or fp32 bulk with fp64 positions,
+ * fp64 re-evaluation of near-degenerate samples and fp64 reductions. */
+#define EGG_B200_PREC_FP64 0
+#define EGG_B200_PREC_MIXED 1
+
+typedef struct egg_b200_session egg_b200_session;
+
+/* Everything the reference's session constructor takes, flattened:
+ *   ctx_arrays (the "groups"/"energy_stencil" wire, egg/smoothing/flat_context.py:275-346)
+ *   structured (egg/smoothing/cpp_backend.py:679-691)
+ *   X0 (float64, global node order).
+ * One merged group of moving DOFs, as the reference merges its groups
+ * (src/sweep.hpp:729 build_merged_view).  Optional pointers may be NULL with
+ * their length 0. */
+typedef struct egg_b200_session_desc {
+    int32_t dim;       /* 2 or 3 */
+    int32_t precision; /* EGG_B200_PREC_* */
+    int32_t device;    /* CUDA device ordinal, -1 = current */
+    int32_t reserved0;
+
+    int64_t num_nodes; /* M global nodes */
+    const double* X;   /* [M*dim] */
+
+    /* structured blocks */
+    int32_t num_blocks;
+    int32_t reserved1;
+    const int32_t* interior_shapes;  /* [num_blocks*dim] */
+    const int32_t* block_global_dof; /* concatenation of every block's row-major id array */
+    int64_t num_halo;
+    const int32_t* halo_src_block;  /* [num_halo] */
+    const int32_t* halo_src_padded; /* [num_halo*dim] */
+    const int32_t* halo_dst_block;  /* [num_halo] */
+    const int32_t* halo_dst_padded; /* [num_halo*dim] */
+    int64_t num_sing;
+    const int32_t* sing_block;   /* [num_sing] */
+    const int32_t* sing_logical; /* [num_sing*dim] */
+
+    /* merged group of moving DOFs */
+    int64_t ndof;
+    const int32_t* dof_idx;          /* [ndof] global node id */
+    const int32_t* P_of;             /* [ndof] stored occurrences per DOF */
+    const int32_t* interior_block;   /* [ndof] or NULL; -1 = stored patch */
+    const int32_t* interior_logical; /* [ndof*dim] or NULL */
+    const int32_t* entity_tag;       /* [ndof] or NULL (all Free); non-zero = constrained */
+    int64_t total_samples;           /* sum(P_of) */
+    const int32_t* gc;               /* [total_samples] */
+    const int32_t* gn[3];            /* [total_samples] each, first dim used */
+    const double* s[3];              /* [total_samples] each */
+    const int32_t* role;             /* [total_samples] in [-1, dim] */
+    const double* W_inv;             /* [dim*dim] (uniform) or [total_samples*dim*dim] */
+    int64_t W_inv_len;
+    const double* weight; /* NULL, [1] or [total_samples] */
+    int64_t weight_len;
+
+    /* energy stencil */
+    int64_t es_num_samples;
+    int32_t es_structured; /* 1: canonical cell stencil of the blocks, no index arrays */
+    int32_t reserved2;
+    const int32_t* es_gc;
+    const int32_t* es_gn[3];
+    const double* es_s[3];
+    const double* es_W_inv; /* [dim*dim] or [es_num_samples*dim*dim] */
+    int64_t es_W_inv_len;
+    const double* es_weight; /* NULL, [1] or [es_num_samples] */
+    int64_t es_weight_len;
+} egg_b200_session_desc;
+
+/* Library / device. */
+int egg_b200_abi_version(void);
+const char* egg_b200_last_error(void);
+int egg_b200_device_count(int* count);
+
+/* Build a device-resident session: validate, re-home the global context onto
+ * the packed per-block store and upload it once.
+ * Replaces src/bindings.cpp:1153 make_structured_session and the
+ * CppStructuredSweepSession constructor (src/bindings.cpp:1268-1281). */
+int egg_b200_session_create(const egg_b200_session_desc* desc, egg_b200_session** out);
+
+/* Release every device allocation of the session (RAII end of the reference
+ * session, src/device.hpp:51). */
+int egg_b200_session_destroy(egg_b200_session* s);
+
+/* n_sweeps of double-buffered block-Jacobi on the resident store; writes
+ * ceil(n/k) (k = report_every, or 1 report when report_every <= 0) energies
+ * and min-dets.  Replaces CppStructuredSweepSession::run
+ * (src/bindings.cpp:1292-1304) -> run_block_jacobi (src/sweep.hpp:2027). */
+int egg_b200_session_run(egg_b200_session* s, int32_t n_sweeps, int32_t objective, double delta,
+                         double omega, int32_t report_every, double* energies, double* mindets,
+                         int64_t capacity, int64_t* n_reported);
+
+/* Energy and min det A of the resident state under an objective (the
+ * reduction of src/sweep.hpp:1881 reduce_energy_mindet, without a sweep). */
+int egg_b200_session_energy(egg_b200_session* s, int32_t objective, double delta, double* energy,
+                            double* mindet);
+
+/* Download the resident positions in GLOBAL node order ([num_nodes*dim]).
+ * Replaces CppStructuredSweepSession::get_X (src/bindings.cpp:1359-1376). */
+int egg_b200_session_get_X(egg_b200_session* s, double* X, int64_t len);
+
+/* Upload positions in global node order, scattered into every copy.
+ * Replaces SweepDeviceContextT::upload_X (src/sweep.hpp:552-557). */
+int egg_b200_session_set_X(egg_b200_session* s, const double* X, int64_t len);
+
+/* Session facts: [0] dim, [1] global nodes, [2] packed store nodes, [3] moving
+ * DOFs, [4] structured-interior DOFs, [5] stored-patch DOFs, [6] owner->copy
+ * entries, [7] energy samples, [8] structured energy stencil (0/1),
+ * [9] precision. */
+int egg_b200_session_info(egg_b200_session* s, int64_t* out, int32_t n);
+
+/* Per-kernel CUDA-event timing on the session stream (off by default).
+ * kernel ids: 0 interior sweep, 1 stored-patch sweep, 2 owner->copy broadcast,
+ * 3 energy reduction, 4 reduction finalize, 5 buffer copy. */
+int egg_b200_session_set_profiling(egg_b200_session* s, int32_t enable);
+int egg_b200_session_kernel_stats(egg_b200_session* s, int32_t kernel_id, double* total_ms,
+                                  int64_t* launches);
+int egg_b200_session_reset_stats(egg_b200_session* s);
+
+/* Device-side checkpoint of the resident positions (one extra store-sized
+ * buffer) and restore from it; no host traffic.  The reference has no solver
+ * checkpoint (sessions are resumed by get_X/set_X, src/bindings.cpp:1359);
+ * this is the device-resident form of that round trip. */
+int egg_b200_session_checkpoint(egg_b200_session* s);
+int egg_b200_session_restore(egg_b200_session* s);
+
+/* Kernel launches issued by the session since creation or the last
+ * reset_stats (every kernel of this library counts, copies excluded). */
+int egg_b200_session_launch_count(egg_b200_session* s, int64_t* launches);
+
+/* Device evaluation of the per-sample metric on n vec(T) rows (the GPU twin of
+ * the reference's oracle binding metric_eval, src/bindings.cpp:1778-1800):
+ * t [n*4] -> mu [n], grad [n*4], hess [n*16]. */
+int egg_b200_metric_eval(int32_t objective, double delta, const double* t, int64_t n, double* mu,
+                         double* grad, double* hess);
+
+/* Device evaluation of one stored patch (grad, hess, energy, mindet) and its
+ * Newton step (the GPU twin of the oracle bindings patch_eval / newton_step,
+ * src/bindings.cpp:1858-2005).  X [n_nodes*2]; per occurrence gc, gn0, gn1,
+ * s0, s1, W_inv [P*4], role.  out: grad[2], hess[4], energy, mindet, step[2]. */
+int egg_b200_patch_eval(int32_t objective, double delta, const double* X, int64_t n_nodes,
+                        int32_t P, const int32_t* gc, const int32_t* gn0, const int32_t* gn1,
+                        const double* s0, const double* s1, const double* W_inv,
+                        const int32_t* role, double* grad, double* hess, double* energy,
+                        double* mindet, double* step);
+
+/* Free-DOF Newton step -H^{-1} g with the zero-gradient and non-finite
+ * fallbacks, evaluated on the device (the oracle binding newton_step,
+ * src/bindings.cpp:2100-2130, for the Free tag). grad[2], hess[4] -> step[2]. */
+int egg_b200_newton_step(const double* grad, const double* hess, double* step);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* EGG_B200_H */

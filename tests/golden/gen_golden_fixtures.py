@@ -1,0 +1,182 @@
+"""Generate the committed golden fixtures under tests/golden/.
+
+Two sources, both from the reference checkout (run in a container that has it):
+
+1. The reference's own golden vectors, read as data from its C++ test headers
+   ``tests/cpp/golden_metric.hpp``, ``golden_metric_3d.hpp`` and
+   ``golden_patch.hpp`` (written by the reference's ``tests/cpp/gen_golden.py``
+   from its C++ oracle bindings) -> ``golden_metric.json``,
+   ``golden_metric_3d.json``, ``golden_patch.json``.
+2. Runs of the reference core itself, built from source by
+   ``oracle/build_ref.sh`` into ``oracle/_ref``, on small seeded grids from
+   ``egg_b200.configs`` -> ``ref_sweeps.npz`` (first-sweep positions and
+   energy / min-det trajectories), so the GPU tests can compare against the
+   reference without the reference present.
+
+Usage: python tests/golden/gen_golden_fixtures.py [REFERENCE_ROOT]
+"""
+
+from __future__ import annotations
+
+import json
+import re
+import sys
+from pathlib import Path
+
+import numpy as np
+
+HERE = Path(__file__).resolve().parent
+ROOT = HERE.parent.parent
+sys.path.insert(0, str(ROOT))
+
+_NUM = r"[+-]?(?:\d+\.?\d*|\.\d+)(?:[eE][+-]?\d+)?"
+
+
+def _blocks(text: str) -> list[str]:
+    """Top-level ``{ ... }`` records of the kSamples initializer."""
+    start = text.index("= {{") + 4
+    out, depth, cur = [], 0, []
+    for ch in text[start:]:
+        if ch == "{":
+            depth += 1
+            if depth == 1:
+                cur = []
+                continue
+        elif ch == "}":
+            if depth == 0:
+                break
+            depth -= 1
+            if depth == 0:
+                out.append("".join(cur))
+                continue
+        if depth >= 1:
+            cur.append(ch)
+    return out
+
+
+def _fields(rec: str) -> dict:
+    out = {}
+    for m in re.finditer(r"\.(\w+)\s*=\s*(\{[^}]*\}|[^,\n]+)", rec):
+        key, val = m.group(1), m.group(2).strip()
+        nums = [float(x) for x in re.findall(_NUM, val)]
+        out[key] = nums if val.startswith("{") else nums[0]
+    return out
+
+
+def parse_header(path: Path) -> list[dict]:
+    return [_fields(r) for r in _blocks(path.read_text())]
+
+
+def gen_reference_vectors(ref_root: Path) -> None:
+    cpp = ref_root / "tests" / "cpp"
+    for name in ("golden_metric", "golden_metric_3d", "golden_patch"):
+        recs = parse_header(cpp / f"{name}.hpp")
+        (HERE / f"{name}.json").write_text(
+            json.dumps({"source": f"tests/cpp/{name}.hpp", "records": recs}, indent=1)
+        )
+        print(f"{name}: {len(recs)} records")
+
+
+# Small seeded cases shared with tests/test_sweep_gpu.py.
+CASES = {
+    "square33": ("unit_square", dict(n=33, frac=0.3, seed=1), None),
+    "square65": ("unit_square", dict(n=65, frac=0.3, seed=7), None),
+    "disk_oh17": ("disk_oh", dict(n=17, frac=0.25, seed=2), None),
+    "disk_oh33": ("disk_oh", dict(n=33, frac=0.25, seed=5), None),
+    "tangled33": ("tangled_square", dict(n=33, seed=4), None),
+}
+RUNS = [
+    # (case, phase, delta, omega, n_sweeps)
+    ("square33", "barrier", 0.0, 1.0, 40),
+    ("square65", "barrier", 0.0, 0.8, 40),
+    ("disk_oh17", "barrier", 0.0, 1.0, 40),
+    ("disk_oh33", "barrier", 0.0, 0.8, 40),
+    ("square33", "shape_size", 0.0, 1.0, 40),
+    ("tangled33", "untangle", 2e-4, 0.5, 40),
+]
+
+
+def case_grid(name: str):
+    from egg_b200 import configs
+
+    fn, kw, _ = CASES[name]
+    return getattr(configs, fn)(**kw)
+
+
+def _runs_for(prec: str) -> dict:
+    from oracle import oracle
+
+    ref = oracle.load_ref(prec)
+    if ref is None:
+        raise SystemExit(f"oracle/_ref/{prec} missing: run oracle/build_ref.sh first")
+    assert bool(ref.REAL_IS_FLOAT) == (prec == "fp32")
+    out = {}
+    for case, phase, delta, omega, n in RUNS:
+        g = case_grid(case)
+        ctx, st = g.wire(), g.structured()
+        X1, e1, m1 = ref.cpp_structured_sweep(ctx, st, g.X_flat(), 1, device="cpu", phase=phase,
+                                               delta=delta, omega=omega, report_every=1)
+        Xn, en, mn = ref.cpp_structured_sweep(ctx, st, g.X_flat(), n, device="cpu", phase=phase,
+                                               delta=delta, omega=omega, report_every=1)
+        key = f"{prec}/{case}/{phase}/{omega}"
+        out[key + "/X1"] = X1
+        out[key + "/Xn"] = Xn
+        out[key + "/E"] = en
+        out[key + "/M"] = mn
+        out[key + "/E1"] = e1
+    return out
+
+
+def gen_reference_runs() -> None:
+    """One process per precision: two extension modules named cpp_core cannot
+    coexist in one interpreter."""
+    import subprocess
+    import tempfile
+
+    out = {}
+    for prec in ("fp64", "fp32"):
+        with tempfile.TemporaryDirectory() as td:
+            f = Path(td) / "runs.npz"
+            subprocess.run([sys.executable, __file__, "--runs", prec, str(f)], check=True)
+            out.update(dict(np.load(f)))
+    np.savez_compressed(HERE / "ref_sweeps.npz", **out)
+    print(f"ref_sweeps.npz: {len(out)} arrays")
+
+
+def gen_reference_wire(ref_root: Path) -> None:
+    """The reference's own wire builders on a small multi-block grid."""
+    sys.path.insert(0, str(ref_root))
+    from egg.smoothing.cpp_backend import build_structured_context_from_block_maps, structured_arrays
+    from egg.smoothing.flat_context import build_flat_context
+
+    g = case_grid("disk_oh17")
+    out = {}
+    for tag, w in (("eye", np.eye(2)), ("aniso", np.array([[1.0, 0.2], [0.0, 1.3]]))):
+        ctx = build_flat_context([np.asarray(b) for b in g.blocks], g.free, {}, 2, w_inv=w)
+        for k, v in ctx["groups"][0].items():
+            if isinstance(v, np.ndarray):
+                out[f"{tag}/group/{k}"] = v
+        for k, v in ctx["energy_stencil"].items():
+            if isinstance(v, np.ndarray):
+                out[f"{tag}/es/{k}"] = v
+    st = structured_arrays(build_structured_context_from_block_maps(2, g.blocks))
+    for k, v in st.items():
+        if isinstance(v, list):
+            for i, a in enumerate(v):
+                out[f"st/{k}/{i}"] = np.asarray(a)
+        else:
+            out[f"st/{k}"] = np.asarray(v)
+    np.savez_compressed(HERE / "ref_wire_disk_oh17.npz", **out)
+    print(f"ref_wire_disk_oh17.npz: {len(out)} arrays")
+
+
+if __name__ == "__main__" and len(sys.argv) == 4 and sys.argv[1] == "--runs":
+    np.savez(sys.argv[3], **_runs_for(sys.argv[2]))
+    raise SystemExit(0)
+
+if __name__ == "__main__":
+    args = [a for a in sys.argv[1:] if not a.startswith("--")]
+    ref_root = Path(args[0]) if args else Path("/root/reference")
+    gen_reference_vectors(ref_root)
+    gen_reference_runs()
+    gen_reference_wire(ref_root)

@@ -1,0 +1,91 @@
+"""The CPU oracle pinned against the reference: its golden vectors, recorded
+runs of the reference core, and (when built here) the reference core itself."""
+
+from __future__ import annotations
+
+import json
+
+import numpy as np
+import pytest
+
+from oracle import oracle
+from tests.conftest import GOLDEN
+from tests.golden.gen_golden_fixtures import RUNS, case_grid
+
+
+def _records(name):
+    return json.loads((GOLDEN / f"{name}.json").read_text())["records"]
+
+
+@pytest.mark.parametrize("rec", _records("golden_metric"), ids=lambda r: str(r["t"][:2]))
+def test_metric_matches_reference_golden(rec):
+    mu, g, H = oracle.metric(np.array(rec["t"]), "shape")
+    np.testing.assert_allclose(mu, rec["mu"], rtol=1e-13, atol=1e-14)
+    np.testing.assert_allclose(g, rec["grad"], rtol=1e-12, atol=1e-13)
+    np.testing.assert_allclose(H, rec["hess"], rtol=1e-12, atol=1e-12)
+
+
+@pytest.mark.parametrize("i", range(5))
+def test_patch_matches_reference_golden(i):
+    r = _records("golden_patch")[i]
+    P = int(r["P"])
+    n = int(r["n_nodes"])
+    X = np.array(r["X"][: 2 * n])
+    g, h, e, md, st = oracle.patch(
+        X, np.array(r["gc"][:P]), np.array(r["gn0"][:P]), np.array(r["gn1"][:P]), np.array(r["s0"][:P]),
+        np.array(r["s1"][:P]), np.array(r["W_inv"][: 4 * P]), np.array(r["role"][:P]))
+    np.testing.assert_allclose(g, r["grad"], rtol=1e-12, atol=1e-12)
+    np.testing.assert_allclose(h, r["hess"], rtol=1e-12, atol=1e-12)
+    np.testing.assert_allclose(e, r["energy"], rtol=1e-13, atol=1e-14)
+    np.testing.assert_allclose(md, r["mindet"], rtol=1e-13, atol=1e-14)
+    if int(r["tag"]) == 0:  # Free DOF: plain 2x2 Newton step
+        np.testing.assert_allclose(st, r["delta"], rtol=1e-12, atol=1e-13)
+
+
+def test_untangle_closed_form_matches_finite_differences():
+    rng = np.random.default_rng(0)
+    for _ in range(20):
+        t = rng.normal(size=4)
+        delta = 0.3
+        mu, g, H = oracle.metric(t, "untangle", delta)
+        eps = 1e-6
+        for k in range(4):
+            tp, tm = t.copy(), t.copy()
+            tp[k] += eps
+            tm[k] -= eps
+            mp, gp, _ = oracle.metric(tp, "untangle", delta)
+            mm, gm, _ = oracle.metric(tm, "untangle", delta)
+            assert abs((mp - mm) / (2 * eps) - g[k]) < 1e-6 * (1 + abs(g[k]))
+            np.testing.assert_allclose((gp - gm) / (2 * eps), H[4 * k : 4 * k + 4], rtol=1e-5, atol=1e-5)
+
+
+_REF = np.load(GOLDEN / "ref_sweeps.npz")
+
+
+@pytest.mark.parametrize("run", RUNS, ids=lambda r: f"{r[0]}-{r[1]}-{r[3]}")
+def test_oracle_matches_recorded_reference(run):
+    case, phase, delta, omega, n = run
+    g = case_grid(case)
+    pt = oracle.patches_for(g.blocks, g.free)
+    sc = oracle.stencil_for(g.blocks)
+    key = f"fp64/{case}/{phase}/{omega}"
+    X1, _, _ = oracle.run(g.X, pt, sc, 1, phase=phase, delta=delta, omega=omega, report_every=1)
+    h = 1.0 / (max(b.shape[0] for b in g.blocks) - 1)
+    assert np.abs(X1.ravel() - _REF[key + "/X1"]).max() <= 1e-12 * h
+    Xn, E, M = oracle.run(g.X, pt, sc, n, phase=phase, delta=delta, omega=omega, report_every=1)
+    np.testing.assert_allclose(E, _REF[key + "/E"], rtol=1e-10)
+    np.testing.assert_allclose(M, _REF[key + "/M"], rtol=1e-9, atol=1e-15)
+
+
+def test_oracle_matches_reference_build_when_present():
+    ref = oracle.load_ref("fp64")
+    if ref is None:
+        pytest.skip("oracle/_ref not built in this environment")
+    g = case_grid("disk_oh17")
+    X, E, M = ref.cpp_structured_sweep(g.wire(), g.structured(), g.X_flat(), 7, device="cpu", omega=0.8,
+                                       report_every=2)
+    Xo, Eo, Mo = oracle.run(g.X, oracle.patches_for(g.blocks, g.free), oracle.stencil_for(g.blocks), 7,
+                            omega=0.8, report_every=2)
+    assert np.abs(Xo.ravel() - X).max() < 1e-14
+    np.testing.assert_allclose(Eo, E, rtol=1e-13)
+    np.testing.assert_allclose(Mo, M, rtol=1e-13)
