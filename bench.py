@@ -145,10 +145,10 @@ def _barrier(dist):
         dist.barrier()
 
 
-def _grid():
+def _grid(n=N_SIDE):
     from egg_b200 import configs
 
-    return configs.unit_square(N_SIDE, frac=FRAC, seed=SEED)
+    return configs.unit_square(n, frac=FRAC, seed=SEED)
 
 
 def cpu_baseline(threads=None, target_s=12.0):
@@ -236,6 +236,9 @@ def main():
     ap.add_argument("--impl", default="egg_b200")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--sweeps", type=int, default=SWEEPS)
+    ap.add_argument("--only", choices=["fp64", "mixed"], default=None,
+                    help="time one precision only and skip e2e (profiling runs)")
+    ap.add_argument("--n", type=int, default=N_SIDE, help="grid side (profiling runs)")
     args = ap.parse_args()
     if args.impl == "reference":
         return run_reference(args)
@@ -247,15 +250,16 @@ def main():
     dist = _pg_init(ws, "nccl")
     from egg_b200 import cpp_core
 
-    g = _grid()
+    g = _grid(args.n)
     ctx = g.wire(compact=True)
     st = g.structured()
     X0 = g.X_flat()
     F = g.num_free
     sweeps = args.sweeps
     results = {}
-    for prec in ("fp64", "mixed"):
+    for prec in ([args.only] if args.only else ["fp64", "mixed"]):
         s = cpp_core.CppStructuredSweepSession(ctx, st, X0, device=f"cuda:{local}", precision=prec)
+        s.autotune("barrier", 3)
         s.checkpoint()
         for _ in range(args.warmup):
             s.restore()
@@ -277,8 +281,17 @@ def main():
         s.set_profiling(False)
         dt = _max_over_ranks(dist, dt, device=f"cuda:{local}")
         results[prec] = {"dt": dt, "E": float(E[-1]), "M": float(M[-1]), "stats": stats, "launches": launches,
-                         "clocks": clk.summary(), "session": s}
+                         "clocks": clk.summary(), "session": s, "variants": s.variants()}
 
+    if args.only:
+        r = results[args.only]
+        if rank == 0:
+            print(json.dumps({"only": args.only, "n": args.n, "sweeps": sweeps, "steps": args.steps,
+                              "variants": r["variants"], "ms_per_step": 1e3 * r["dt"] / args.steps,
+                              "value": ws * F * sweeps * args.steps / r["dt"], "E": r["E"], "M": r["M"]}))
+        if dist is not None:
+            dist.destroy_process_group()
+        return 0
     mixed = results["mixed"]
     ms_step = 1e3 * mixed["dt"] / args.steps
     value = ws * F * sweeps * args.steps / mixed["dt"]
@@ -328,6 +341,7 @@ def main():
                   "rel_energy_vs_fp64": abs(mixed["E"] - results["fp64"]["E"]) / abs(results["fp64"]["E"]),
                   "speedup_vs_fp64": value / v64},
         "roofline": roof, "kernel_share": share,
+        "autotune": {"mixed": mixed["variants"], "fp64": results["fp64"]["variants"]},
         "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": int(X0.nbytes),
                 "d2h_bytes_per_step": int(Xout.nbytes + 16)},
         "gpu_launches": int(mixed["launches"]),

@@ -382,6 +382,33 @@ class Session
         check(rc);
     }
 
+    int autotune(const std::string& phase, int reps)
+    {
+        int32_t v = 0;
+        py::gil_scoped_release nogil;
+        const int rc = egg_b200_session_autotune(h_.get(), objective_of(phase), reps, &v);
+        py::gil_scoped_acquire g;
+        check(rc);
+        return v;
+    }
+
+    void set_variant(int v) { check(egg_b200_session_set_variant(h_.get(), v)); }
+
+    py::dict variants()
+    {
+        int32_t v = 0, shape[12];
+        double t[4];
+        check(egg_b200_session_variant_info(h_.get(), &v, shape, t, 3));
+        py::dict d;
+        d["variant"] = v;
+        py::list lst;
+        for (int i = 0; i < 3; ++i) {
+            lst.append(py::make_tuple(shape[3 * i], shape[3 * i + 1], shape[3 * i + 2], t[i]));
+        }
+        d["table"] = lst;
+        return d;
+    }
+
     int64_t launch_count()
     {
         int64_t n = 0;
@@ -445,6 +472,9 @@ PYBIND11_MODULE(cpp_core, m)
       .def("checkpoint", &Session::checkpoint, "Copy the resident positions to a device-side checkpoint.")
       .def("restore", &Session::restore, "Restore the resident positions from the device-side checkpoint.")
       .def("launch_count", &Session::launch_count)
+      .def("autotune", &Session::autotune, py::arg("phase") = "barrier", py::arg("reps") = 3)
+      .def("set_variant", &Session::set_variant, py::arg("variant"))
+      .def("variants", &Session::variants)
       .def("run_control", [](Session& s, int, const std::string&, double, double, double, int, double, bool, bool) {
           s.no_control();
       }, py::arg("n_outer"), py::kw_only(), py::arg("phase") = "barrier", py::arg("grad_tol") = 1e-8,

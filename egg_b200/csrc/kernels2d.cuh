@@ -93,6 +93,100 @@ __device__ __forceinline__ C sample_mu_c(C ax, C bx, C ay, C by, C delta, C& det
     return mu_value<C>(KIND, t, delta);
 }
 
+// Per-sample contributions to the three nodes a sample moves, without forming
+// the full 4x4 metric Hessian: only its 10 distinct entries enter
+//   role 1 (axis-0 neighbour)  grad s0 (g0, g2),  jhj (H00, H02, H22)
+//   role 2 (axis-1 neighbour)  grad s1 (g1, g3),  jhj (H11, H13, H33)
+//   role 0 (corner)            grad -(role1 + role2),
+//                              jhj  role1 + role2 + s0 s1 (2 H01, H03 + H12, 2 H23)
+// (role_Jb / accumulate_sample of src/patch.hpp:204-320 with W_inv = I).
+template <class C> struct RoleOut {
+    C mu, det;
+    C r[3][5];  // [role 0, 1, 2][gx, gy, hxx, hxy, hyy]
+};
+
+template <int KIND, class C>
+__device__ __forceinline__ void sample_roles_c(C a, C b, C c, C d, C s0, C s1, C delta, RoleOut<C>& o)
+{
+    const C t[4] = {a, b, c, d};
+    const C cof[4] = {d, -c, -b, a};
+    const C D = a * d - b * c;
+    const C s = a * a + b * b + c * c + d * d;
+    ScaleFn<C> sf = (KIND == kUntangle) ? untangle_scale(D, delta) : shape_scale(D);
+    const C m = s * sf.f;
+    C g2[4];
+#pragma unroll
+    for (int i = 0; i < 4; ++i) { g2[i] = C(2) * sf.f * t[i] + s * sf.fp * cof[i]; }
+    const C dm1 = D - C(1);
+    auto P = [](int i, int j) -> C {
+        const int k = i * 4 + j;
+        return (k == 3 || k == 12) ? C(1) : ((k == 6 || k == 9) ? C(-1) : C(0));
+    };
+    auto H = [&](int i, int j) -> C {
+        const C h2 = (i == j ? C(2) * sf.f : C(0)) + C(2) * sf.fp * (t[i] * cof[j] + cof[i] * t[j]) +
+                     s * sf.fpp * cof[i] * cof[j] + s * sf.fp * P(i, j);
+        if (KIND != kShapeSize) { return h2; }
+        return C(2) * g2[i] * g2[j] + C(2) * m * h2 + C(2) * cof[i] * cof[j] + C(2) * dm1 * P(i, j);
+    };
+    C g[4];
+    if (KIND == kShapeSize) {
+        o.mu = m * m - C(1) + dm1 * dm1;
+#pragma unroll
+        for (int i = 0; i < 4; ++i) { g[i] = C(2) * m * g2[i] + C(2) * dm1 * cof[i]; }
+    } else {
+        o.mu = m - C(1);
+#pragma unroll
+        for (int i = 0; i < 4; ++i) { g[i] = g2[i]; }
+    }
+    o.det = D;
+    const C h00 = H(0, 0), h01 = H(0, 1), h02 = H(0, 2), h03 = H(0, 3), h11 = H(1, 1);
+    const C h12 = H(1, 2), h13 = H(1, 3), h22 = H(2, 2), h23 = H(2, 3), h33 = H(3, 3);
+    o.r[1][0] = s0 * g[0];
+    o.r[1][1] = s0 * g[2];
+    o.r[1][2] = h00;
+    o.r[1][3] = h02;
+    o.r[1][4] = h22;
+    o.r[2][0] = s1 * g[1];
+    o.r[2][1] = s1 * g[3];
+    o.r[2][2] = h11;
+    o.r[2][3] = h13;
+    o.r[2][4] = h33;
+    const C ss = s0 * s1;
+    o.r[0][0] = -(o.r[1][0] + o.r[2][0]);
+    o.r[0][1] = -(o.r[1][1] + o.r[2][1]);
+    o.r[0][2] = h00 + h11 + C(2) * ss * h01;
+    o.r[0][3] = h02 + h13 + ss * (h03 + h12);
+    o.r[0][4] = h22 + h33 + C(2) * ss * h23;
+}
+
+// Role contributions from fp64 edge vectors in working precision C, with the
+// fp64 re-evaluation of near-degenerate samples when C = float.
+template <int KIND, class C>
+__device__ __forceinline__ void sample_roles(double ax, double bx, double ay, double by, double s0, double s1,
+                                             double delta, RoleOut<C>& o)
+{
+    if constexpr (std::is_same_v<C, double>) {
+        sample_roles_c<KIND, double>(ax, bx, ay, by, s0, s1, delta, o);
+    } else {
+        const float fax = float(ax), fbx = float(bx), fay = float(ay), fby = float(by);
+        const float d = fax * fby - fbx * fay;
+        const float n0 = fax * fax + fay * fay, n1 = fbx * fbx + fby * fby;
+        if (d * d < float(kGuard * kGuard) * n0 * n1) {
+            RoleOut<double> od;
+            sample_roles_c<KIND, double>(ax, bx, ay, by, s0, s1, delta, od);
+            o.mu = float(od.mu);
+            o.det = float(od.det);
+#pragma unroll
+            for (int r = 0; r < 3; ++r) {
+#pragma unroll
+                for (int q = 0; q < 5; ++q) { o.r[r][q] = float(od.r[r][q]); }
+            }
+        } else {
+            sample_roles_c<KIND, float>(fax, fbx, fay, fby, float(s0), float(s1), float(delta), o);
+        }
+    }
+}
+
 // ---------------------------------------------------------------------------
 // Owner -> non-owner copy refresh (src/structured_halo.hpp:197 fused_halo_broadcast).
 // ---------------------------------------------------------------------------
@@ -214,8 +308,8 @@ __device__ double2 dof_update_fp64(const double2* __restrict__ P, int PW, int ti
     return pos;
 }
 
-template <int CI, int CJ, int KIND, class C>
-__global__ void __launch_bounds__(CI* CJ)
+template <int CI, int CJ, int MINB, int KIND, class C>
+__global__ void __launch_bounds__(CI* CJ, MINB)
   interior_tile_kernel(const double2* __restrict__ Xin, double2* __restrict__ Xout,
                        const Tile2* __restrict__ tiles, const BlockInfo* __restrict__ blocks,
                        const uint8_t* __restrict__ active, const double2* __restrict__ tau,
@@ -244,25 +338,27 @@ __global__ void __launch_bounds__(CI* CJ)
     __syncthreads();
 
     // Phase 2: cell (ci, cj) with base node window (ci, cj); thread = cell.
+    // Each thread owns column `tid` of the shared cell arrays and accumulates
+    // the role contributions of its four samples there (no register array).
     {
         const int ci = tid / CJ, cj = tid % CJ;
         const bool valid = (r0 + ci <= n0 - 2) && (c0 + cj <= n1 - 2);
-        C mu4[4], det4[4];
-        C acc[4][5];
         bool bad = false;
 #pragma unroll
         for (int a = 0; a < 4; ++a) {
 #pragma unroll
-            for (int q = 0; q < 5; ++q) { acc[a][q] = C(0); }
+            for (int q = 0; q < 5; ++q) { sm.gh[a][q][tid] = C(0); }
+            sm.mu[a][tid] = C(0);
+            sm.det[a][tid] = C(1);
         }
         if (valid) {
-            const double2 p[4] = {sm.P[ci * PW + cj], sm.P[ci * PW + cj + 1],
-                                  sm.P[(ci + 1) * PW + cj], sm.P[(ci + 1) * PW + cj + 1]};
 #pragma unroll
             for (int b = 0; b < 4; ++b) {
                 const double s0 = (b & 2) ? -1.0 : 1.0;
                 const double s1 = (b & 1) ? -1.0 : 1.0;
-                const double2 pc = p[b], pn0 = p[b ^ 2], pn1 = p[b ^ 1];
+                const double2 pc = sm.P[(ci + (b >> 1)) * PW + cj + (b & 1)];
+                const double2 pn0 = sm.P[(ci + ((b ^ 2) >> 1)) * PW + cj + (b & 1)];
+                const double2 pn1 = sm.P[(ci + (b >> 1)) * PW + cj + ((b ^ 1) & 1)];
                 const double ax = s0 * (pn0.x - pc.x), bx = s1 * (pn1.x - pc.x);
                 const double ay = s0 * (pn0.y - pc.y), by = s1 * (pn1.y - pc.y);
                 if constexpr (std::is_same_v<C, float>) {
@@ -270,48 +366,19 @@ __global__ void __launch_bounds__(CI* CJ)
                     const double nn = (ax * ax + ay * ay) * (bx * bx + by * by);
                     bad = bad || dd <= 0.0 || dd * dd < kBadCell * kBadCell * nn;
                 }
-                SampleOut<C> o;
-                sample_full<KIND, C>(ax, bx, ay, by, delta, o);
-                mu4[b] = o.mu;
-                det4[b] = o.det;
-                const C cs0 = C(s0), cs1 = C(s1);
-                // role 1: node b^2 is the axis-0 neighbour; role 2: node b^1.
-                const C g1x = cs0 * o.g[0], g1y = cs0 * o.g[2];
-                const C g2x = cs1 * o.g[1], g2y = cs1 * o.g[3];
-                const C h1xx = o.H[0], h1xy = o.H[2], h1yy = o.H[10];
-                const C h2xx = o.H[5], h2xy = o.H[7], h2yy = o.H[15];
-                const C ss = cs0 * cs1;
-                acc[b ^ 2][0] += g1x;
-                acc[b ^ 2][1] += g1y;
-                acc[b ^ 2][2] += h1xx;
-                acc[b ^ 2][3] += h1xy;
-                acc[b ^ 2][4] += h1yy;
-                acc[b ^ 1][0] += g2x;
-                acc[b ^ 1][1] += g2y;
-                acc[b ^ 1][2] += h2xx;
-                acc[b ^ 1][3] += h2xy;
-                acc[b ^ 1][4] += h2yy;
-                acc[b][0] -= g1x + g2x;
-                acc[b][1] -= g1y + g2y;
-                acc[b][2] += h1xx + h2xx + ss * (o.H[1] + o.H[4]);
-                acc[b][3] += h1xy + h2xy + ss * (o.H[3] + o.H[6]);
-                acc[b][4] += h1yy + h2yy + ss * (o.H[11] + o.H[14]);
-            }
-        } else {
+                RoleOut<C> o;
+                sample_roles<KIND, C>(ax, bx, ay, by, s0, s1, delta, o);
+                sm.mu[b][tid] = o.mu;
+                sm.det[b][tid] = o.det;
 #pragma unroll
-            for (int b = 0; b < 4; ++b) {
-                mu4[b] = C(0);
-                det4[b] = C(1);
+                for (int q = 0; q < 5; ++q) {
+                    sm.gh[b][q][tid] += o.r[0][q];
+                    sm.gh[b ^ 2][q][tid] += o.r[1][q];
+                    sm.gh[b ^ 1][q][tid] += o.r[2][q];
+                }
             }
         }
         sm.bad[tid] = bad ? 1 : 0;
-#pragma unroll
-        for (int b = 0; b < 4; ++b) {
-            sm.mu[b][tid] = mu4[b];
-            sm.det[b][tid] = det4[b];
-#pragma unroll
-            for (int q = 0; q < 5; ++q) { sm.gh[b][q][tid] = acc[b][q]; }
-        }
     }
     __syncthreads();
 

@@ -6,6 +6,7 @@
 #include <algorithm>
 #include <cmath>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <limits>
 #include <memory>
@@ -66,9 +67,16 @@ template <class T> struct DevBuf {
     }
 };
 
-// Tile shapes (cells per CTA) of the interior kernel by working precision.
-constexpr int kCI64 = 8, kCJ64 = 32;
-constexpr int kCI32 = 8, kCJ32 = 32;
+// Launch variants of the interior kernel: cells per CTA (CI x CJ) and the
+// minimum resident CTAs per SM requested from the register allocator.  The
+// session's autotuner times each on the session's own data and keeps the
+// fastest (egg_b200_session_autotune).
+struct Variant {
+    int ci, cj, minb;
+};
+constexpr int kNumVariants = 3;
+constexpr Variant kVar64[kNumVariants] = {{8, 32, 1}, {8, 32, 2}, {8, 16, 4}};
+constexpr Variant kVar32[kNumVariants] = {{8, 32, 2}, {8, 32, 3}, {16, 32, 1}};
 
 enum KernelId { kKInterior = 0, kKStored = 1, kKBroadcast = 2, kKReduce = 3, kKFinal = 4, kKCopy = 5, kKCount = 6 };
 
@@ -92,8 +100,13 @@ struct Session {
     // interior DOFs
     int64_t n_interior = 0;
     DevBuf<uint8_t> active_d;
-    DevBuf<Tile2> tiles_d;
+    std::vector<uint8_t> active_h;
+    DevBuf<Tile2> tiles_d;   // tiles of the current variant's shape
     int64_t ntiles = 0;
+    int tile_ci = 0, tile_cj = 0;
+    int variant = 0;
+    bool tuned = false;
+    double variant_ms[kNumVariants] = {};
     // stored DOFs
     int64_t n_stored = 0;
     DevBuf<int32_t> st_slot, st_gc, st_gn0, st_gn1, st_role;
@@ -211,23 +224,59 @@ static bool rows_uniform(const double* W, int64_t rows, int width)
     return true;
 }
 
-// Opt the interior kernels into >48 KB of dynamic shared memory (once per
-// device and precision).
-template <int CI, int CJ, class C> static void set_smem_attr()
+// Opt the interior kernels into >48 KB of dynamic shared memory.
+template <int CI, int CJ, int MINB, class C> static void set_smem_attr()
 {
     const int smem = int(sizeof(TileShared2<CI, CJ, C>));
-    EGG_CK(cudaFuncSetAttribute(interior_tile_kernel<CI, CJ, kShape, C>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
-    EGG_CK(cudaFuncSetAttribute(interior_tile_kernel<CI, CJ, kUntangle, C>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
-    EGG_CK(cudaFuncSetAttribute(interior_tile_kernel<CI, CJ, kShapeSize, C>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+    EGG_CK(cudaFuncSetAttribute(interior_tile_kernel<CI, CJ, MINB, kShape, C>,
+                                cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+    EGG_CK(cudaFuncSetAttribute(interior_tile_kernel<CI, CJ, MINB, kUntangle, C>,
+                                cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+    EGG_CK(cudaFuncSetAttribute(interior_tile_kernel<CI, CJ, MINB, kShapeSize, C>,
+                                cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
 }
 
 static void configure_kernels(int prec)
 {
     if (prec == EGG_B200_PREC_FP64) {
-        set_smem_attr<kCI64, kCJ64, double>();
+        set_smem_attr<kVar64[0].ci, kVar64[0].cj, kVar64[0].minb, double>();
+        set_smem_attr<kVar64[1].ci, kVar64[1].cj, kVar64[1].minb, double>();
+        set_smem_attr<kVar64[2].ci, kVar64[2].cj, kVar64[2].minb, double>();
     } else {
-        set_smem_attr<kCI32, kCJ32, float>();
+        set_smem_attr<kVar32[0].ci, kVar32[0].cj, kVar32[0].minb, float>();
+        set_smem_attr<kVar32[1].ci, kVar32[1].cj, kVar32[1].minb, float>();
+        set_smem_attr<kVar32[2].ci, kVar32[2].cj, kVar32[2].minb, float>();
     }
+}
+
+// Tile list of a CI x CJ cell tiling ((CI-1) x (CJ-1) DOFs per tile) over
+// every block's structured interior, keeping tiles that hold a moving DOF.
+static void set_tiles(Session& S, Variant v)
+{
+    if (S.tile_ci == v.ci && S.tile_cj == v.cj) { return; }
+    std::vector<Tile2> tiles;
+    for (int b = 0; b < int(S.blocks_h.size()); ++b) {
+        const BlockInfo& bi = S.blocks_h[b];
+        if (bi.n[0] < 3 || bi.n[1] < 3) { continue; }
+        for (int i0 = 1; i0 <= bi.n[0] - 2; i0 += v.ci - 1) {
+            for (int j0 = 1; j0 <= bi.n[1] - 2; j0 += v.cj - 1) {
+                bool any = false;
+                for (int i = i0; i < std::min(i0 + v.ci - 1, bi.n[0] - 1) && !any; ++i) {
+                    for (int j = j0; j < std::min(j0 + v.cj - 1, bi.n[1] - 1); ++j) {
+                        if (S.active_h[bi.off + int64_t(i) * bi.n[1] + j]) {
+                            any = true;
+                            break;
+                        }
+                    }
+                }
+                if (any) { tiles.push_back(Tile2 {b, i0, j0, 0}); }
+            }
+        }
+    }
+    S.tiles_d.upload(tiles);
+    S.ntiles = int64_t(tiles.size());
+    S.tile_ci = v.ci;
+    S.tile_cj = v.cj;
 }
 
 static Session* create_session(const egg_b200_session_desc& d)
@@ -570,29 +619,7 @@ static Session* create_session(const egg_b200_session_desc& d)
         }
     }
 
-    // ---- interior tiles --------------------------------------------------
-    const int CI = S->prec == EGG_B200_PREC_FP64 ? kCI64 : kCI32;
-    const int CJ = S->prec == EGG_B200_PREC_FP64 ? kCJ64 : kCJ32;
-    std::vector<Tile2> tiles;
-    for (int b = 0; b < nb; ++b) {
-        const BlockInfo& bi = S->blocks_h[b];
-        if (bi.n[0] < 3 || bi.n[1] < 3) { continue; }
-        for (int i0 = 1; i0 <= bi.n[0] - 2; i0 += CI - 1) {
-            for (int j0 = 1; j0 <= bi.n[1] - 2; j0 += CJ - 1) {
-                bool any = false;
-                for (int i = i0; i < std::min(i0 + CI - 1, bi.n[0] - 1) && !any; ++i) {
-                    for (int j = j0; j < std::min(j0 + CJ - 1, bi.n[1] - 1); ++j) {
-                        if (active[bi.off + int64_t(i) * bi.n[1] + j]) {
-                            any = true;
-                            break;
-                        }
-                    }
-                }
-                if (any) { tiles.push_back(Tile2 {b, i0, j0, 0}); }
-            }
-        }
-    }
-    S->ntiles = int64_t(tiles.size());
+    S->active_h = std::move(active);
 
     // ---- device --------------------------------------------------------------
     int ndev = 0;
@@ -621,8 +648,9 @@ static Session* create_session(const egg_b200_session_desc& d)
         S->es_s1.upload(es_s1h);
     }
     S->blocks_d.upload(S->blocks_h);
-    S->active_d.upload(active);
-    S->tiles_d.upload(tiles);
+    S->active_d.upload(S->active_h);
+    S->variant = 0;
+    set_tiles(*S, S->prec == EGG_B200_PREC_FP64 ? kVar64[0] : kVar32[0]);
     S->st_slot.upload(st_slot);
     S->st_off.upload(st_off);
     S->st_gc.upload(st_gc);
@@ -652,30 +680,91 @@ static Session* create_session(const egg_b200_session_desc& d)
 // ---------------------------------------------------------------------------
 // Sweep driver
 // ---------------------------------------------------------------------------
+template <int CI, int CJ, int MINB, int KIND, class C>
+static void launch_tile(Session& S, const double* xin, double* xout, const double* tau, double delta, double omega)
+{
+    const size_t smem = sizeof(TileShared2<CI, CJ, C>);
+    const auto* xi = reinterpret_cast<const double2*>(xin);
+    auto* xo = reinterpret_cast<double2*>(xout);
+    const auto* tv = reinterpret_cast<const double2*>(tau);
+    S.timed(kKInterior, [&] {
+        interior_tile_kernel<CI, CJ, MINB, KIND, C><<<unsigned(S.ntiles), CI * CJ, smem, S.stream>>>(
+          xi, xo, S.tiles_d.p, S.blocks_d.p, S.active_d.p, tv, delta, omega);
+    });
+}
+
 template <int KIND> static void launch_interior(Session& S, const double* xin, double* xout, const double* tau,
                                                 double delta, double omega)
 {
     if (S.ntiles == 0) { return; }
-    const auto* xi = reinterpret_cast<const double2*>(xin);
-    auto* xo = reinterpret_cast<double2*>(xout);
-    const auto* tv = reinterpret_cast<const double2*>(tau);
     if (S.prec == EGG_B200_PREC_FP64) {
-        constexpr int CI = kCI64, CJ = kCJ64;
-        auto kern = interior_tile_kernel<CI, CJ, KIND, double>;
-        const size_t smem = sizeof(TileShared2<CI, CJ, double>);
-        S.timed(kKInterior, [&] {
-            kern<<<unsigned(S.ntiles), CI * CJ, smem, S.stream>>>(xi, xo, S.tiles_d.p, S.blocks_d.p, S.active_d.p, tv,
-                                                                  delta, omega);
-        });
+        switch (S.variant) {
+        case 0: launch_tile<kVar64[0].ci, kVar64[0].cj, kVar64[0].minb, KIND, double>(S, xin, xout, tau, delta, omega); break;
+        case 1: launch_tile<kVar64[1].ci, kVar64[1].cj, kVar64[1].minb, KIND, double>(S, xin, xout, tau, delta, omega); break;
+        default: launch_tile<kVar64[2].ci, kVar64[2].cj, kVar64[2].minb, KIND, double>(S, xin, xout, tau, delta, omega); break;
+        }
     } else {
-        constexpr int CI = kCI32, CJ = kCJ32;
-        auto kern = interior_tile_kernel<CI, CJ, KIND, float>;
-        const size_t smem = sizeof(TileShared2<CI, CJ, float>);
-        S.timed(kKInterior, [&] {
-            kern<<<unsigned(S.ntiles), CI * CJ, smem, S.stream>>>(xi, xo, S.tiles_d.p, S.blocks_d.p, S.active_d.p, tv,
-                                                                  delta, omega);
-        });
+        switch (S.variant) {
+        case 0: launch_tile<kVar32[0].ci, kVar32[0].cj, kVar32[0].minb, KIND, float>(S, xin, xout, tau, delta, omega); break;
+        case 1: launch_tile<kVar32[1].ci, kVar32[1].cj, kVar32[1].minb, KIND, float>(S, xin, xout, tau, delta, omega); break;
+        default: launch_tile<kVar32[2].ci, kVar32[2].cj, kVar32[2].minb, KIND, float>(S, xin, xout, tau, delta, omega); break;
+        }
     }
+}
+
+static Variant variant_shape(const Session& S, int v)
+{
+    return S.prec == EGG_B200_PREC_FP64 ? kVar64[v] : kVar32[v];
+}
+
+// Time every interior-kernel variant on the resident data (reads the
+// canonical buffer, writes the scratch buffer, so the state is untouched) and
+// keep the fastest.
+template <int KIND> static void autotune_impl(Session& S, int reps)
+{
+    if (S.n_interior == 0) {
+        S.tuned = true;
+        return;
+    }
+    cudaEvent_t a, b;
+    EGG_CK(cudaEventCreate(&a));
+    EGG_CK(cudaEventCreate(&b));
+    const bool prof = S.profiling;
+    S.profiling = false;
+    const int64_t launches = S.launches;
+    double best = 1e300;
+    int best_v = 0;
+    for (int v = 0; v < kNumVariants; ++v) {
+        S.variant = v;
+        set_tiles(S, variant_shape(S, v));
+        launch_interior<KIND>(S, S.X(S.cur), S.X(1 - S.cur), nullptr, 0.0, 1.0);
+        EGG_CK(cudaEventRecord(a, S.stream));
+        for (int r = 0; r < reps; ++r) {
+            launch_interior<KIND>(S, S.X(S.cur), S.X(1 - S.cur), nullptr, 0.0, 1.0);
+        }
+        EGG_CK(cudaEventRecord(b, S.stream));
+        EGG_CK(cudaEventSynchronize(b));
+        float ms = 0.f;
+        EGG_CK(cudaEventElapsedTime(&ms, a, b));
+        S.variant_ms[v] = double(ms) / reps;
+        if (S.variant_ms[v] < best) {
+            best = S.variant_ms[v];
+            best_v = v;
+        }
+    }
+    cudaEventDestroy(a);
+    cudaEventDestroy(b);
+    S.variant = best_v;
+    set_tiles(S, variant_shape(S, best_v));
+    S.profiling = prof;
+    S.launches = launches;
+    S.tuned = true;
+}
+
+static bool autotune_enabled()
+{
+    const char* v = std::getenv("EGG_B200_AUTOTUNE");
+    return !(v && std::string(v) == "0");
 }
 
 static StoredPatch2 stored_view(Session& S)
@@ -760,6 +849,7 @@ template <int KIND> static void launch_reduce(Session& S, const double* x, doubl
 template <int KIND> static void run_impl(Session& S, int n_sweeps, double delta, double omega, int report_every,
                                          std::vector<double>& E, std::vector<double>& Md)
 {
+    if (!S.tuned && autotune_enabled()) { autotune_impl<KIND>(S, 3); }
     const int k = report_every <= 0 ? n_sweeps : report_every;
     const int64_t nrep = (int64_t(n_sweeps) + k - 1) / k;
     if (S.red_out.n < size_t(2 * nrep)) { S.red_out.alloc(size_t(2 * nrep)); }
@@ -1053,6 +1143,55 @@ int egg_b200_session_restore(egg_b200_session* s)
         const size_t n = size_t(S.nstore) * S.dim;
         if (n) { EGG_CK(cudaMemcpyAsync(S.X(S.cur), S.ckpt.p, n * sizeof(double), cudaMemcpyDeviceToDevice, S.stream)); }
         S.sync();
+    });
+}
+
+int egg_b200_session_autotune(egg_b200_session* s, int32_t objective, int32_t reps, int32_t* chosen)
+{
+    return guarded([&] {
+        if (!s) { invalid("autotune: NULL session"); }
+        check_objective(objective);
+        Session& S = *s->impl;
+        EGG_CK(cudaSetDevice(S.device));
+        const int r = reps > 0 ? reps : 3;
+        switch (objective) {
+        case EGG_B200_OBJ_SHAPE: autotune_impl<kShape>(S, r); break;
+        case EGG_B200_OBJ_UNTANGLE: autotune_impl<kUntangle>(S, r); break;
+        default: autotune_impl<kShapeSize>(S, r); break;
+        }
+        if (chosen) { *chosen = S.variant; }
+    });
+}
+
+int egg_b200_session_set_variant(egg_b200_session* s, int32_t variant)
+{
+    return guarded([&] {
+        if (!s) { invalid("set_variant: NULL session"); }
+        if (variant < 0 || variant >= kNumVariants) { invalid("set_variant: variant out of range"); }
+        Session& S = *s->impl;
+        EGG_CK(cudaSetDevice(S.device));
+        S.variant = variant;
+        set_tiles(S, variant_shape(S, variant));
+        S.tuned = true;
+    });
+}
+
+int egg_b200_session_variant_info(egg_b200_session* s, int32_t* variant, int32_t* shape, double* times_ms,
+                                  int32_t n)
+{
+    return guarded([&] {
+        if (!s) { invalid("variant_info: NULL session"); }
+        Session& S = *s->impl;
+        if (variant) { *variant = S.variant; }
+        for (int v = 0; v < n && v < kNumVariants; ++v) {
+            const Variant vs = variant_shape(S, v);
+            if (shape) {
+                shape[3 * v] = vs.ci;
+                shape[3 * v + 1] = vs.cj;
+                shape[3 * v + 2] = vs.minb;
+            }
+            if (times_ms) { times_ms[v] = S.variant_ms[v]; }
+        }
     });
 }
 

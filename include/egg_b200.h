@@ -159,6 +159,17 @@ int egg_b200_session_reset_stats(egg_b200_session* s);
 int egg_b200_session_checkpoint(egg_b200_session* s);
 int egg_b200_session_restore(egg_b200_session* s);
 
+/* Autotuner of the interior sweep kernel: times each launch variant (cells
+ * per CTA, resident CTAs per SM) on the session's own resident data without
+ * changing it, keeps the fastest and returns its index.  Runs automatically
+ * before the first sweep unless EGG_B200_AUTOTUNE=0.  No counterpart in the
+ * reference (AdaptiveCpp picks launch shapes itself). */
+int egg_b200_session_autotune(egg_b200_session* s, int32_t objective, int32_t reps, int32_t* chosen);
+int egg_b200_session_set_variant(egg_b200_session* s, int32_t variant);
+/* Current variant, per-variant (ci, cj, min CTAs/SM) [3*n] and tuned times [n]. */
+int egg_b200_session_variant_info(egg_b200_session* s, int32_t* variant, int32_t* shape, double* times_ms,
+                                  int32_t n);
+
 /* Kernel launches issued by the session since creation or the last
  * reset_stats (every kernel of this library counts, copies excluded). */
 int egg_b200_session_launch_count(egg_b200_session* s, int64_t* launches);
