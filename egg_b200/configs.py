@@ -13,6 +13,11 @@ interpolation of straight/circular block edges and perturbed with
 * :func:`tangled_square` n x n unit square with seeded interior nodes displaced
   by 0.8-1.5 h in random directions until a target fraction of cells holds an
   inverted corner sample (the untangling workload).
+* :func:`unit_cube`     one n^3 block on [0,1]^3 with interior noise.
+* :func:`sphere_in_cube` 7-block hex grid of the cube [-1,1]^3: a centre block
+  mapped onto the ball r = 0.5 and six shell blocks from the sphere to the cube
+  faces; cube boundary fixed, every other node perturbed by +-frac * (local min
+  edge length).
 """
 
 from __future__ import annotations
@@ -23,7 +28,10 @@ import numpy as np
 
 from . import wire as _wire
 
-__all__ = ["Grid", "unit_square", "disk_oh", "tangled_square", "grid_mindet", "mean_size_w_inv"]
+__all__ = [
+    "Grid", "unit_square", "disk_oh", "tangled_square", "unit_cube", "two_cubes", "sphere_in_cube",
+    "grid_mindet", "mean_size_w_inv",
+]
 
 
 @dataclass
@@ -83,7 +91,8 @@ def unit_square(n: int, frac: float = 0.3, seed: int = 0) -> Grid:
 
 def _dedupe(points: list[np.ndarray]):
     """Global ids for per-block point arrays, merging coincident nodes."""
-    flat = np.concatenate([p.reshape(-1, 2) for p in points])
+    d = points[0].shape[-1]
+    flat = np.concatenate([p.reshape(-1, d) for p in points])
     key = np.round(flat * 1e9).astype(np.int64)
     _, first, inv = np.unique(key, axis=0, return_index=True, return_inverse=True)
     # Ids in first-appearance order, so block 0 (the centre) numbers first.
@@ -94,8 +103,9 @@ def _dedupe(points: list[np.ndarray]):
     X = flat[np.sort(first)]
     blocks, off = [], 0
     for p in points:
-        m = p.shape[0] * p.shape[1]
-        blocks.append(gid[off : off + m].reshape(p.shape[0], p.shape[1]))
+        shp = p.shape[:-1]
+        m = int(np.prod(shp))
+        blocks.append(gid[off : off + m].reshape(shp))
         off += m
     return blocks, X
 
@@ -170,3 +180,84 @@ def mean_size_w_inv(blocks, X, d=2) -> np.ndarray:
     vol = abs(float(grid_mindet(blocks, X, d).mean()))
     hbar = vol ** (1.0 / d)
     return np.eye(d) / hbar
+
+
+def unit_cube(n: int, frac: float = 0.2, seed: int = 0) -> Grid:
+    """One n^3 block on the unit cube; node (i, j, k) at (i h, j h, k h)."""
+    ids = np.arange(n**3, dtype=np.int64).reshape(n, n, n)
+    t = np.linspace(0.0, 1.0, n)
+    X = np.stack(np.meshgrid(t, t, t, indexing="ij"), axis=-1).reshape(-1, 3).copy()
+    free = np.zeros((n, n, n), dtype=bool)
+    free[1:-1, 1:-1, 1:-1] = True
+    free = free.reshape(-1)
+    h = 1.0 / (n - 1)
+    rng = np.random.default_rng(seed)
+    if frac > 0:
+        X[free] += rng.uniform(-frac * h, frac * h, size=(int(free.sum()), 3))
+    return Grid(f"cube{n}", 3, [ids], X, free, {"h": h, "frac": frac, "seed": seed})
+
+
+def two_cubes(n: int, frac: float = 0.2, seed: int = 0) -> Grid:
+    """Two n^3 unit cubes sharing the x = 1 face (conforming 3D interface)."""
+    t = np.linspace(0.0, 1.0, n)
+    P = np.stack(np.meshgrid(t, t, t, indexing="ij"), axis=-1)
+    blocks, X = _dedupe([P, P + np.array([1.0, 0.0, 0.0])])
+    free = np.ones(X.shape[0], dtype=bool)
+    for b in blocks:
+        for ax in range(3):
+            for side in (0, -1):
+                face = np.take(b, side, axis=ax)
+                if not (ax == 0 and ((b is blocks[0] and side == -1) or (b is blocks[1] and side == 0))):
+                    free[face.reshape(-1)] = False
+    h = 1.0 / (n - 1)
+    rng = np.random.default_rng(seed)
+    noise = rng.uniform(-frac * h, frac * h, size=X.shape)
+    X = X + np.where(free[:, None], noise, 0.0)
+    return Grid(f"two_cubes{n}", 3, blocks, X, free, {"h": h, "frac": frac, "seed": seed})
+
+
+# Shell blocks: outward normal n and tangents t1, t2 with n x t1 = t2, so each
+# block's (radial, t1, t2) logical axes are right-handed.
+_SHELLS = [
+    ((1, 0, 0), (0, 1, 0), (0, 0, 1)),
+    ((-1, 0, 0), (0, 0, 1), (0, 1, 0)),
+    ((0, 1, 0), (0, 0, 1), (1, 0, 0)),
+    ((0, -1, 0), (1, 0, 0), (0, 0, 1)),
+    ((0, 0, 1), (1, 0, 0), (0, 1, 0)),
+    ((0, 0, -1), (0, 1, 0), (1, 0, 0)),
+]
+
+
+def sphere_in_cube(n: int = 129, frac: float = 0.2, seed: int = 0, radius: float = 0.5,
+                   core: float = 0.25) -> Grid:
+    """7-block sphere-in-cube hex grid of [-1,1]^3, every block n^3 nodes.
+
+    Centre block: the cube [-core, core]^3.  Shell block with outward normal
+    n: along its radial axis a node moves from the centre cube's face (r = 0)
+    through the sphere of ``radius`` (r = 1/2, a node layer when n is odd) to
+    the outer cube face (r = 1), piecewise linearly; its other two axes follow
+    the face tangents.  Every block corner keeps three non-coplanar edges.
+    """
+    u = np.linspace(-1.0, 1.0, n)
+    P = np.stack(np.meshgrid(u, u, u, indexing="ij"), axis=-1)
+    pts = [core * P]
+    r = np.linspace(0.0, 1.0, n)[:, None, None, None]
+    for nrm, t1, t2 in _SHELLS:
+        nrm, t1, t2 = (np.asarray(v, dtype=np.float64) for v in (nrm, t1, t2))
+        V, W = np.meshgrid(u, u, indexing="ij")
+        d = nrm[None, None, :] + V[..., None] * t1[None, None, :] + W[..., None] * t2[None, None, :]
+        inner = core * d
+        sph = radius * d / np.linalg.norm(d, axis=-1, keepdims=True)
+        lo = inner[None] + np.minimum(2.0 * r, 1.0) * (sph - inner)[None]
+        x = np.where(r <= 0.5, lo, sph[None] + (2.0 * r - 1.0) * (d - sph)[None])
+        pts.append(x)
+    blocks, X = _dedupe(pts)
+    N = X.shape[0]
+    free = np.ones(N, dtype=bool)
+    for b in blocks[1:]:
+        free[b[-1]] = False  # outer cube faces
+    h = _min_edge(blocks, X)
+    rng = np.random.default_rng(seed)
+    noise = rng.uniform(-1.0, 1.0, size=(N, 3)) * (frac * h)[:, None]
+    X = X + np.where(free[:, None], noise, 0.0)
+    return Grid(f"sphere_in_cube{n}", 3, blocks, X, free, {"frac": frac, "seed": seed, "radius": radius})

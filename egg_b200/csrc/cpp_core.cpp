@@ -396,14 +396,14 @@ class Session
 
     py::dict variants()
     {
-        int32_t v = 0, shape[12];
+        int32_t v = 0, shape[16];
         double t[4];
         check(egg_b200_session_variant_info(h_.get(), &v, shape, t, 3));
         py::dict d;
         d["variant"] = v;
         py::list lst;
         for (int i = 0; i < 3; ++i) {
-            lst.append(py::make_tuple(shape[3 * i], shape[3 * i + 1], shape[3 * i + 2], t[i]));
+            lst.append(py::make_tuple(shape[4 * i], shape[4 * i + 1], shape[4 * i + 2], shape[4 * i + 3], t[i]));
         }
         d["table"] = lst;
         return d;
@@ -517,6 +517,32 @@ PYBIND11_MODULE(cpp_core, m)
       },
       py::arg("t"), py::arg("metric") = "shape_2d", py::arg("delta") = 0.0,
       "Evaluate a named 2D metric on the GPU. Returns (mu, grad(4,), hess(16,)).");
+
+    m.def(
+      "metric_eval_3d",
+      [](const DArr& t, const py::object& v_obj, const std::string& metric, double delta) {
+          int obj = EGG_B200_OBJ_SHAPE;
+          if (metric == "shape_size") {
+              obj = EGG_B200_OBJ_SHAPE_SIZE;
+          } else if (metric == "untangle") {
+              obj = EGG_B200_OBJ_UNTANGLE;
+          } else if (metric != "cond3" && metric != "shape") {
+              throw py::value_error("metric_eval_3d: unknown metric '" + metric + "'");
+          }
+          if (t.size() != 9) { throw py::value_error("metric_eval_3d: t must have 9 entries"); }
+          std::vector<double> v = {1.0, 1.0, 1.0};
+          if (!v_obj.is_none()) {
+              DArr va = DArr::ensure(v_obj);
+              if (!va || va.size() != 3) { throw py::value_error("metric_eval_3d: v must have 3 entries"); }
+              v.assign(va.data(), va.data() + 3);
+          }
+          double mu = 0;
+          std::vector<double> g(9), hv(6);
+          check(egg_b200_metric3_probe(obj, delta, t.data(), v.data(), 1, &mu, g.data(), hv.data()));
+          return std::make_tuple(mu, vec(g), vec(hv));
+      },
+      py::arg("t"), py::arg("v") = py::none(), py::arg("metric") = "cond3", py::arg("delta") = 0.0,
+      "3D metric on the GPU: (mu, grad over vec(T) (9,), contracted Hessian along e_i v^T packed (6,)).");
 
     m.def(
       "patch_eval",

@@ -1,0 +1,180 @@
+// 3D TMOP metrics (host + device).
+//
+//   shape       mu = |T|^2 |cof T|^2 / (9 D^2) - 1                 (src/metric.hpp:199-275)
+//   shape_size  mu_shape + (D - 1)^2                               (src/metric.hpp:241-246)
+//   untangle    D -> Dh = (D + sqrt(D^2 + 4 delta^2)) / 2          (src/metric.hpp:250-262)
+//
+// vec(T) row-major, T = A W_inv, A[:,k] = s_k (nbr_k - corner).  Written as
+//   mu + 1 = s q F(D) / 9,  s = |T|^2,  C = cof T,  q = |C|^2,  F = 1/D^2 | 1/Dh^2.
+//
+// A node of a sample moves T along rank-one directions B_i = e_i v^T (row i of
+// T changes by v; v = -W^T s for the corner, s_ax W[ax,:] for the axis-ax
+// neighbour, src/patch.hpp:204-233).  Along such directions the second
+// derivative of det T and of the cofactor vanish (two equal rows), leaving
+//   a = T v, c = C v, w_r = T_r x v (row r of T),
+//   k_i = C_{i+1}.w_{i+2} - C_{i+2}.w_{i+1},  m_ii = |w_{i+1}|^2 + |w_{i+2}|^2,
+//   m_{i,i+1} = -w_i.w_{i+1}  (indices mod 3),
+// and with s' = 2a, q' = 2k, q'' = 2m, F' = F_D c, F'' = F_DD c c^T:
+//   dmu/dx_i      = (2 a_i q F + 2 s k_i F + s q F_D c_i) / 9
+//   d2mu/dx_i dx_j = (2 d_ij |v|^2 q F + 2 s m_ij F + s q F_DD c_i c_j
+//                    + 4F (a_i k_j + a_j k_i) + 2 q F_D (a_i c_j + a_j c_i)
+//                    + 2 s F_D (k_i c_j + k_j c_i)) / 9
+// (+ 2(D-1) c_i and + 2 c_i c_j for shape_size).  This is the node gradient
+// and J_b^T H J_b contraction of the reference (src/metric.hpp:756-808 forms
+// it by six directional second derivatives) without the 81-entry Hessian.
+#pragma once
+
+#include "metric.cuh"
+
+namespace egg_b200
+{
+
+template <class R> struct Shared3 {
+    R t[9];
+    R C[9];
+    R D, s, q, F, FD, FDD;
+};
+
+template <class R> EGG_HD R det3(const R t[9])
+{
+    return t[0] * (t[4] * t[8] - t[5] * t[7]) - t[1] * (t[3] * t[8] - t[5] * t[6]) +
+           t[2] * (t[3] * t[7] - t[4] * t[6]);
+}
+
+template <class R> EGG_HD void cof3(const R t[9], R C[9])
+{
+    C[0] = t[4] * t[8] - t[5] * t[7];
+    C[1] = t[5] * t[6] - t[3] * t[8];
+    C[2] = t[3] * t[7] - t[4] * t[6];
+    C[3] = t[2] * t[7] - t[1] * t[8];
+    C[4] = t[0] * t[8] - t[2] * t[6];
+    C[5] = t[1] * t[6] - t[0] * t[7];
+    C[6] = t[1] * t[5] - t[2] * t[4];
+    C[7] = t[2] * t[3] - t[0] * t[5];
+    C[8] = t[0] * t[4] - t[1] * t[3];
+}
+
+template <class R> EGG_HD void shared3(int kind, const R t[9], R delta, Shared3<R>& o)
+{
+    R s = R(0), q = R(0);
+#pragma unroll
+    for (int i = 0; i < 9; ++i) {
+        o.t[i] = t[i];
+        s += t[i] * t[i];
+    }
+    cof3<R>(t, o.C);
+#pragma unroll
+    for (int i = 0; i < 9; ++i) { q += o.C[i] * o.C[i]; }
+    const R D = t[0] * o.C[0] + t[1] * o.C[1] + t[2] * o.C[2];
+    o.D = D;
+    o.s = s;
+    o.q = q;
+    if (kind == kUntangle) {
+        const R r = sqrt(D * D + R(4) * delta * delta);
+        const R Dh = R(0.5) * (D + r);
+        const R d1 = Dh / r, d2 = R(2) * delta * delta / (r * r * r);
+        const R inv = R(1) / Dh;
+        const R inv2 = inv * inv;
+        o.F = inv2;
+        o.FD = R(-2) * d1 * inv2 * inv;
+        o.FDD = R(6) * d1 * d1 * inv2 * inv2 - R(2) * d2 * inv2 * inv;
+    } else {
+        const R inv = R(1) / D;
+        const R inv2 = inv * inv;
+        o.F = inv2;
+        o.FD = R(-2) * inv2 * inv;
+        o.FDD = R(6) * inv2 * inv2;
+    }
+}
+
+template <class R> EGG_HD R mu3_from(int kind, const Shared3<R>& S)
+{
+    R mu = S.s * S.q * S.F * R(1.0 / 9.0) - R(1);
+    if (kind == kShapeSize) { mu += (S.D - R(1)) * (S.D - R(1)); }
+    return mu;
+}
+
+template <class R> EGG_HD R mu3_value(int kind, const R t[9], R delta, R& det)
+{
+    Shared3<R> S;
+    shared3<R>(kind, t, delta, S);
+    det = S.D;
+    return mu3_from<R>(kind, S);
+}
+
+// Node gradient g[3] and contracted Hessian h[6] = (xx, xy, xz, yy, yz, zz)
+// of one sample along the rank-one directions e_i v^T.
+template <class R> EGG_HD void role3(int kind, const Shared3<R>& S, const R v[3], R g[3], R h[6])
+{
+    const R* t = S.t;
+    const R* C = S.C;
+    R a[3], c[3], w[3][3];
+#pragma unroll
+    for (int i = 0; i < 3; ++i) {
+        a[i] = t[3 * i] * v[0] + t[3 * i + 1] * v[1] + t[3 * i + 2] * v[2];
+        c[i] = C[3 * i] * v[0] + C[3 * i + 1] * v[1] + C[3 * i + 2] * v[2];
+        w[i][0] = t[3 * i + 1] * v[2] - t[3 * i + 2] * v[1];
+        w[i][1] = t[3 * i + 2] * v[0] - t[3 * i] * v[2];
+        w[i][2] = t[3 * i] * v[1] - t[3 * i + 1] * v[0];
+    }
+    auto dot3 = [](const R* x, const R* y) { return x[0] * y[0] + x[1] * y[1] + x[2] * y[2]; };
+    R k[3];
+#pragma unroll
+    for (int i = 0; i < 3; ++i) {
+        const int i1 = (i + 1) % 3, i2 = (i + 2) % 3;
+        k[i] = dot3(C + 3 * i1, w[i2]) - dot3(C + 3 * i2, w[i1]);
+    }
+    const R W00 = dot3(w[0], w[0]), W11 = dot3(w[1], w[1]), W22 = dot3(w[2], w[2]);
+    const R W01 = dot3(w[0], w[1]), W12 = dot3(w[1], w[2]), W02 = dot3(w[0], w[2]);
+    const R m[3][3] = {{W11 + W22, -W01, -W02}, {-W01, W00 + W22, -W12}, {-W02, -W12, W00 + W11}};
+    const R vv = v[0] * v[0] + v[1] * v[1] + v[2] * v[2];
+    const R s = S.s, q = S.q, F = S.F, FD = S.FD, FDD = S.FDD;
+    const R n9 = R(1.0 / 9.0);
+    const R dm1x2 = R(2) * (S.D - R(1));
+#pragma unroll
+    for (int i = 0; i < 3; ++i) {
+        g[i] = (R(2) * a[i] * q * F + R(2) * s * k[i] * F + s * q * FD * c[i]) * n9;
+        if (kind == kShapeSize) { g[i] += dm1x2 * c[i]; }
+    }
+    int e = 0;
+#pragma unroll
+    for (int i = 0; i < 3; ++i) {
+#pragma unroll
+        for (int j = i; j < 3; ++j) {
+            R hij = (i == j ? R(2) * vv * q * F : R(0)) + R(2) * s * m[i][j] * F + s * q * FDD * c[i] * c[j] +
+                    R(4) * F * (a[i] * k[j] + a[j] * k[i]) + R(2) * q * FD * (a[i] * c[j] + a[j] * c[i]) +
+                    R(2) * s * FD * (k[i] * c[j] + k[j] * c[i]);
+            hij *= n9;
+            if (kind == kShapeSize) { hij += R(2) * c[i] * c[j]; }
+            h[e++] = hij;
+        }
+    }
+}
+
+// Newton step -H^{-1} g for a symmetric 3x3 (packed xx, xy, xz, yy, yz, zz)
+// with the reference fallbacks (src/solve.hpp:52-77).
+template <class R> EGG_HD void solve3(const R h[6], const R g[3], R x[3])
+{
+    const R gn = sqrt(g[0] * g[0] + g[1] * g[1] + g[2] * g[2]);
+    if (gn < Tol<R>::znorm) {
+        x[0] = x[1] = x[2] = R(0);
+        return;
+    }
+    const R H[9] = {h[0], h[1], h[2], h[1], h[3], h[4], h[2], h[4], h[5]};
+    const R c00 = H[4] * H[8] - H[5] * H[7], c01 = -(H[3] * H[8] - H[5] * H[6]), c02 = H[3] * H[7] - H[4] * H[6];
+    const R det = H[0] * c00 + H[1] * c01 + H[2] * c02;
+    const R inv = R(1) / det;
+    const R c10 = -(H[1] * H[8] - H[2] * H[7]), c11 = H[0] * H[8] - H[2] * H[6], c12 = -(H[0] * H[7] - H[1] * H[6]);
+    const R c20 = H[1] * H[5] - H[2] * H[4], c21 = -(H[0] * H[5] - H[2] * H[3]), c22 = H[0] * H[4] - H[1] * H[3];
+    x[0] = -inv * (c00 * g[0] + c10 * g[1] + c20 * g[2]);
+    x[1] = -inv * (c01 * g[0] + c11 * g[1] + c21 * g[2]);
+    x[2] = -inv * (c02 * g[0] + c12 * g[1] + c22 * g[2]);
+    if (!(isfinite(x[0]) && isfinite(x[1]) && isfinite(x[2]))) {
+        const R cc = R(-0.1) / gn;
+        x[0] = cc * g[0];
+        x[1] = cc * g[1];
+        x[2] = cc * g[2];
+    }
+}
+
+}  // namespace egg_b200

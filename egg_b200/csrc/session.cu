@@ -2,6 +2,7 @@
 // state, the block-Jacobi driver, and the C-ABI declared in include/egg_b200.h.
 #include "egg_b200.h"
 #include "kernels2d.cuh"
+#include "kernels3d.cuh"
 
 #include <algorithm>
 #include <cmath>
@@ -71,12 +72,15 @@ template <class T> struct DevBuf {
 // minimum resident CTAs per SM requested from the register allocator.  The
 // session's autotuner times each on the session's own data and keeps the
 // fastest (egg_b200_session_autotune).
+// 2D: (ci, cj) cells per CTA; 3D: (ci, cj, ck) DOFs per CTA.
 struct Variant {
-    int ci, cj, minb;
+    int ci, cj, ck, minb;
 };
 constexpr int kNumVariants = 3;
-constexpr Variant kVar64[kNumVariants] = {{8, 32, 1}, {8, 32, 2}, {8, 16, 4}};
-constexpr Variant kVar32[kNumVariants] = {{8, 32, 2}, {8, 32, 3}, {16, 32, 1}};
+constexpr Variant kVar64[kNumVariants] = {{8, 32, 1, 1}, {8, 32, 1, 2}, {8, 16, 1, 4}};
+constexpr Variant kVar32[kNumVariants] = {{8, 32, 1, 2}, {8, 32, 1, 3}, {16, 32, 1, 1}};
+constexpr Variant kVar3_64[kNumVariants] = {{4, 8, 8, 1}, {4, 8, 8, 2}, {2, 8, 16, 2}};
+constexpr Variant kVar3_32[kNumVariants] = {{4, 8, 8, 1}, {4, 8, 8, 2}, {2, 8, 16, 2}};
 
 enum KernelId { kKInterior = 0, kKStored = 1, kKBroadcast = 2, kKReduce = 3, kKFinal = 4, kKCopy = 5, kKCount = 6 };
 
@@ -101,17 +105,18 @@ struct Session {
     int64_t n_interior = 0;
     DevBuf<uint8_t> active_d;
     std::vector<uint8_t> active_h;
-    DevBuf<Tile2> tiles_d;   // tiles of the current variant's shape
+    DevBuf<Tile2> tiles_d;   // 2D tiles of the current variant's shape
+    DevBuf<Tile3> tiles3_d;  // 3D tiles of the current variant's shape
     int64_t ntiles = 0;
-    int tile_ci = 0, tile_cj = 0;
+    int tile_ci = 0, tile_cj = 0, tile_ck = 0;
     int variant = 0;
     bool tuned = false;
     double variant_ms[kNumVariants] = {};
     // stored DOFs
     int64_t n_stored = 0;
-    DevBuf<int32_t> st_slot, st_gc, st_gn0, st_gn1, st_role;
+    DevBuf<int32_t> st_slot, st_gc, st_gn0, st_gn1, st_gn2, st_role;
     DevBuf<int64_t> st_off;
-    DevBuf<int8_t> st_s0, st_s1;
+    DevBuf<int8_t> st_s0, st_s1, st_s2;
     DevBuf<double> st_W, st_wt;
     int st_wstride = 0, st_wtstride = 0;
     // owner -> copy broadcast
@@ -122,8 +127,8 @@ struct Session {
     int64_t es_ns = 0;
     DevBuf<int64_t> es_cell_off;
     int64_t es_ncell = 0;
-    DevBuf<int32_t> es_gc, es_gn0, es_gn1;
-    DevBuf<int8_t> es_s0, es_s1;
+    DevBuf<int32_t> es_gc, es_gn0, es_gn1, es_gn2;
+    DevBuf<int8_t> es_s0, es_s1, es_s2;
     DevBuf<double> es_W, es_wt;
     int es_wstride = 0, es_wtstride = 0;
     // reductions
@@ -216,6 +221,13 @@ static void require_ptr(const void* p, int64_t n, const std::string& what)
     if (n > 0 && p == nullptr) { invalid("session desc: " + what + " is NULL"); }
 }
 
+static std::vector<double> identity_row(int D)
+{
+    std::vector<double> w(size_t(D) * D, 0.0);
+    for (int k = 0; k < D; ++k) { w[size_t(k) * D + k] = 1.0; }
+    return w;
+}
+
 static bool rows_uniform(const double* W, int64_t rows, int width)
 {
     for (int64_t r = 1; r < rows; ++r) {
@@ -236,8 +248,9 @@ template <int CI, int CJ, int MINB, class C> static void set_smem_attr()
                                 cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
 }
 
-static void configure_kernels(int prec)
+static void configure_kernels(int prec, int dim)
 {
+    if (dim == 3) { return; }  // 3D kernels use < 48 KB of static shared memory
     if (prec == EGG_B200_PREC_FP64) {
         set_smem_attr<kVar64[0].ci, kVar64[0].cj, kVar64[0].minb, double>();
         set_smem_attr<kVar64[1].ci, kVar64[1].cj, kVar64[1].minb, double>();
@@ -249,41 +262,66 @@ static void configure_kernels(int prec)
     }
 }
 
-// Tile list of a CI x CJ cell tiling ((CI-1) x (CJ-1) DOFs per tile) over
-// every block's structured interior, keeping tiles that hold a moving DOF.
+static Variant variant_shape(const Session& S, int v)
+{
+    if (S.dim == 3) { return S.prec == EGG_B200_PREC_FP64 ? kVar3_64[v] : kVar3_32[v]; }
+    return S.prec == EGG_B200_PREC_FP64 ? kVar64[v] : kVar32[v];
+}
+
+// Tile list of the interior kernel for variant v over every block's
+// structured interior, keeping tiles that hold a moving DOF.  2D: CI x CJ
+// cells, (CI-1) x (CJ-1) DOFs per tile; 3D: CI x CJ x CK DOFs per tile.
 static void set_tiles(Session& S, Variant v)
 {
-    if (S.tile_ci == v.ci && S.tile_cj == v.cj) { return; }
-    std::vector<Tile2> tiles;
+    if (S.tile_ci == v.ci && S.tile_cj == v.cj && S.tile_ck == v.ck) { return; }
+    const int di = S.dim == 2 ? v.ci - 1 : v.ci, dj = S.dim == 2 ? v.cj - 1 : v.cj, dk = S.dim == 2 ? 1 : v.ck;
+    std::vector<Tile2> tiles2;
+    std::vector<Tile3> tiles3;
     for (int b = 0; b < int(S.blocks_h.size()); ++b) {
         const BlockInfo& bi = S.blocks_h[b];
-        if (bi.n[0] < 3 || bi.n[1] < 3) { continue; }
-        for (int i0 = 1; i0 <= bi.n[0] - 2; i0 += v.ci - 1) {
-            for (int j0 = 1; j0 <= bi.n[1] - 2; j0 += v.cj - 1) {
-                bool any = false;
-                for (int i = i0; i < std::min(i0 + v.ci - 1, bi.n[0] - 1) && !any; ++i) {
-                    for (int j = j0; j < std::min(j0 + v.cj - 1, bi.n[1] - 1); ++j) {
-                        if (S.active_h[bi.off + int64_t(i) * bi.n[1] + j]) {
-                            any = true;
-                            break;
+        if (bi.n[0] < 3 || bi.n[1] < 3 || (S.dim == 3 && bi.n[2] < 3)) { continue; }
+        const int hk = S.dim == 3 ? bi.n[2] - 2 : 1;
+        for (int i0 = 1; i0 <= bi.n[0] - 2; i0 += di) {
+            for (int j0 = 1; j0 <= bi.n[1] - 2; j0 += dj) {
+                for (int k0 = S.dim == 3 ? 1 : 0; k0 <= (S.dim == 3 ? hk : 0); k0 += dk) {
+                    bool any = false;
+                    for (int i = i0; i < std::min(i0 + di, bi.n[0] - 1) && !any; ++i) {
+                        for (int j = j0; j < std::min(j0 + dj, bi.n[1] - 1) && !any; ++j) {
+                            const int kend = S.dim == 3 ? std::min(k0 + dk, bi.n[2] - 1) : 1;
+                            for (int k = S.dim == 3 ? k0 : 0; k < kend; ++k) {
+                                if (S.active_h[bi.off + (int64_t(i) * bi.n[1] + j) * bi.n[2] + k]) {
+                                    any = true;
+                                    break;
+                                }
+                            }
                         }
                     }
+                    if (!any) { continue; }
+                    if (S.dim == 2) {
+                        tiles2.push_back(Tile2 {b, i0, j0, 0});
+                    } else {
+                        tiles3.push_back(Tile3 {b, i0, j0, k0});
+                    }
                 }
-                if (any) { tiles.push_back(Tile2 {b, i0, j0, 0}); }
             }
         }
     }
-    S.tiles_d.upload(tiles);
-    S.ntiles = int64_t(tiles.size());
+    if (S.dim == 2) {
+        S.tiles_d.upload(tiles2);
+        S.ntiles = int64_t(tiles2.size());
+    } else {
+        S.tiles3_d.upload(tiles3);
+        S.ntiles = int64_t(tiles3.size());
+    }
     S.tile_ci = v.ci;
     S.tile_cj = v.cj;
+    S.tile_ck = v.ck;
 }
 
 static Session* create_session(const egg_b200_session_desc& d)
 {
     const int D = d.dim;
     if (D != 2 && D != 3) { invalid("egg C++ core: dimension must be 2 or 3, got " + std::to_string(D)); }
-    if (D == 3) { throw Error(EGG_B200_ENOTSUP, "egg_b200: 3D sessions are not built yet"); }
     if (d.precision != EGG_B200_PREC_FP64 && d.precision != EGG_B200_PREC_MIXED) {
         invalid("session desc: unknown precision " + std::to_string(d.precision));
     }
@@ -431,8 +469,8 @@ static Session* create_session(const egg_b200_session_desc& d)
     std::vector<uint8_t> active(off, 0);
     std::vector<int32_t> st_slot;
     std::vector<int64_t> st_off {0};
-    std::vector<int32_t> st_gc, st_gn0, st_gn1, st_role;
-    std::vector<int8_t> st_s0, st_s1;
+    std::vector<int32_t> st_gc, st_gn0, st_gn1, st_gn2, st_role;
+    std::vector<int8_t> st_s0, st_s1, st_s2;
     std::vector<double> st_W, st_wt;
     std::vector<uint8_t> seen_slot(off, 0);
     int64_t poff = 0;
@@ -488,6 +526,10 @@ static Session* create_session(const egg_b200_session_desc& d)
             st_gn1.push_back(remap(d.gn[1][p]));
             st_s0.push_back(d.s[0][p] < 0 ? int8_t(-1) : int8_t(1));
             st_s1.push_back(d.s[1][p] < 0 ? int8_t(-1) : int8_t(1));
+            if (D == 3) {
+                st_gn2.push_back(remap(d.gn[2][p]));
+                st_s2.push_back(d.s[2][p] < 0 ? int8_t(-1) : int8_t(1));
+            }
             st_role.push_back(d.role[p]);
             if (!w_uniform) {
                 for (int e = 0; e < D * D; ++e) { st_W.push_back(d.W_inv[p * D * D + e]); }
@@ -499,7 +541,7 @@ static Session* create_session(const egg_b200_session_desc& d)
     S->n_stored = int64_t(st_slot.size());
     if (w_uniform || st_W.empty()) {
         st_W.assign(d.W_inv, d.W_inv + (w_uniform ? D * D : 0));
-        if (st_W.empty()) { st_W = {1.0, 0.0, 0.0, 1.0}; }
+        if (st_W.empty()) { st_W = identity_row(D); }
         S->st_wstride = 0;
     } else if (rows_uniform(st_W.data(), int64_t(st_W.size()) / (D * D), D * D)) {
         st_W.resize(D * D);
@@ -556,23 +598,40 @@ static Session* create_session(const egg_b200_session_desc& d)
             chk(d.es_gc[i]);
             for (int k = 0; k < D; ++k) { chk(d.es_gn[k][i]); }
         }
-        // Canonical cell stencil of the blocks?
+        // Canonical cell stencil of the blocks?  Sample 2^D * cell + b:
+        // corner at cell base + bits(b) (axis 0 most significant), axis-k
+        // neighbour at corner ^ bit_k, sign -1 where bit k of b is set.
         if (ns == ncell * nc) {
             structured = true;
             for (int b = 0; b < nb && structured; ++b) {
                 const BlockInfo& bi = S->blocks_h[b];
-                const int w = bi.n[1];
-                for (int i = 0; i + 1 < bi.n[0] && structured; ++i) {
-                    for (int j = 0; j + 1 < w && structured; ++j) {
-                        const int64_t cell = cell_off[b] + int64_t(i) * (w - 1) + j;
-                        int32_t cg[4];
-                        for (int a = 0; a < 4; ++a) { cg[a] = S->slot_gid[bi.off + int64_t(i + (a >> 1)) * w + j + (a & 1)]; }
-                        for (int bb = 0; bb < 4; ++bb) {
-                            const int64_t sid = cell * 4 + bb;
-                            if (d.es_gc[sid] != cg[bb] || d.es_gn[0][sid] != cg[bb ^ 2] || d.es_gn[1][sid] != cg[bb ^ 1] ||
-                                d.es_s[0][sid] != ((bb & 2) ? -1.0 : 1.0) || d.es_s[1][sid] != ((bb & 1) ? -1.0 : 1.0)) {
+                const int64_t c0 = std::max(0, bi.n[0] - 1), c1 = std::max(0, bi.n[1] - 1);
+                const int64_t c2 = D == 3 ? std::max(0, bi.n[2] - 1) : 1;
+                const int64_t cells = c0 * c1 * c2;
+                for (int64_t lc = 0; lc < cells && structured; ++lc) {
+                    const int64_t i = lc / (c1 * c2), j = (lc / c2) % c1, k = lc % c2;
+                    int32_t cg[8];
+                    for (int a = 0; a < nc; ++a) {
+                        int64_t u, v, w;
+                        if (D == 2) {
+                            u = i + (a >> 1);
+                            v = j + (a & 1);
+                            w = 0;
+                        } else {
+                            u = i + (a >> 2);
+                            v = j + ((a >> 1) & 1);
+                            w = k + (a & 1);
+                        }
+                        cg[a] = S->slot_gid[bi.off + (u * bi.n[1] + v) * bi.n[2] + w];
+                    }
+                    const int64_t cell = cell_off[b] + lc;
+                    for (int bb = 0; bb < nc && structured; ++bb) {
+                        const int64_t sid = cell * nc + bb;
+                        if (d.es_gc[sid] != cg[bb]) { structured = false; }
+                        for (int ax = 0; ax < D && structured; ++ax) {
+                            const int bit = 1 << (D - 1 - ax);
+                            if (d.es_gn[ax][sid] != cg[bb ^ bit] || d.es_s[ax][sid] != ((bb & bit) ? -1.0 : 1.0)) {
                                 structured = false;
-                                break;
                             }
                         }
                     }
@@ -584,11 +643,11 @@ static Session* create_session(const egg_b200_session_desc& d)
     S->es_ns = ns;
     S->es_ncell = ncell;
     std::vector<double> es_W_h, es_wt_h;
-    std::vector<int32_t> es_a, es_b0, es_b1;
-    std::vector<int8_t> es_s0h, es_s1h;
+    std::vector<int32_t> es_a, es_b0, es_b1, es_b2;
+    std::vector<int8_t> es_s0h, es_s1h, es_s2h;
     if (es_w_uniform || ns == 0) {
         es_W_h.assign(d.es_W_inv, d.es_W_inv + (es_w_uniform ? D * D : 0));
-        if (es_W_h.empty()) { es_W_h = {1.0, 0.0, 0.0, 1.0}; }
+        if (es_W_h.empty()) { es_W_h = identity_row(D); }
         S->es_wstride = 0;
     } else if (rows_uniform(d.es_W_inv, ns, D * D)) {
         es_W_h.assign(d.es_W_inv, d.es_W_inv + D * D);
@@ -617,6 +676,14 @@ static Session* create_session(const egg_b200_session_desc& d)
             es_s0h[i] = d.es_s[0][i] < 0 ? -1 : 1;
             es_s1h[i] = d.es_s[1][i] < 0 ? -1 : 1;
         }
+        if (D == 3) {
+            es_b2.resize(ns);
+            es_s2h.resize(ns);
+            for (int64_t i = 0; i < ns; ++i) {
+                es_b2[i] = S->g2s[d.es_gn[2][i]];
+                es_s2h[i] = d.es_s[2][i] < 0 ? -1 : 1;
+            }
+        }
     }
 
     S->active_h = std::move(active);
@@ -633,7 +700,7 @@ static Session* create_session(const egg_b200_session_desc& d)
     }
     EGG_CK(cudaGetDevice(&S->device));
     EGG_CK(cudaStreamCreateWithFlags(&S->stream, cudaStreamNonBlocking));
-    configure_kernels(S->prec);
+    configure_kernels(S->prec, S->dim);
 
     // ---- upload -----------------------------------------------------------
     S->es_W.upload(es_W_h);
@@ -646,11 +713,13 @@ static Session* create_session(const egg_b200_session_desc& d)
         S->es_gn1.upload(es_b1);
         S->es_s0.upload(es_s0h);
         S->es_s1.upload(es_s1h);
+        S->es_gn2.upload(es_b2);
+        S->es_s2.upload(es_s2h);
     }
     S->blocks_d.upload(S->blocks_h);
     S->active_d.upload(S->active_h);
     S->variant = 0;
-    set_tiles(*S, S->prec == EGG_B200_PREC_FP64 ? kVar64[0] : kVar32[0]);
+    set_tiles(*S, variant_shape(*S, 0));
     S->st_slot.upload(st_slot);
     S->st_off.upload(st_off);
     S->st_gc.upload(st_gc);
@@ -659,6 +728,8 @@ static Session* create_session(const egg_b200_session_desc& d)
     S->st_role.upload(st_role);
     S->st_s0.upload(st_s0);
     S->st_s1.upload(st_s1);
+    S->st_gn2.upload(st_gn2);
+    S->st_s2.upload(st_s2);
     S->st_W.upload(st_W);
     S->st_wt.upload(st_wt);
     S->sh_src.upload(sh_src);
@@ -693,10 +764,37 @@ static void launch_tile(Session& S, const double* xin, double* xout, const doubl
     });
 }
 
+template <int TI, int TJ, int TK, int MINB, int KIND, class C>
+static void launch_tile3(Session& S, const double* xin, double* xout, const double* tau, double delta, double omega)
+{
+    S.timed(kKInterior, [&] {
+        interior3_kernel<TI, TJ, TK, MINB, KIND, C><<<unsigned(S.ntiles), TI * TJ * TK, 0, S.stream>>>(
+          xin, xout, S.tiles3_d.p, S.blocks_d.p, S.active_d.p, tau, delta, omega);
+    });
+}
+
 template <int KIND> static void launch_interior(Session& S, const double* xin, double* xout, const double* tau,
                                                 double delta, double omega)
 {
     if (S.ntiles == 0) { return; }
+#define EGG_V3(T, C, i) launch_tile3<T[i].ci, T[i].cj, T[i].ck, T[i].minb, KIND, C>(S, xin, xout, tau, delta, omega)
+    if (S.dim == 3) {
+        if (S.prec == EGG_B200_PREC_FP64) {
+            switch (S.variant) {
+            case 0: EGG_V3(kVar3_64, double, 0); break;
+            case 1: EGG_V3(kVar3_64, double, 1); break;
+            default: EGG_V3(kVar3_64, double, 2); break;
+            }
+        } else {
+            switch (S.variant) {
+            case 0: EGG_V3(kVar3_32, float, 0); break;
+            case 1: EGG_V3(kVar3_32, float, 1); break;
+            default: EGG_V3(kVar3_32, float, 2); break;
+            }
+        }
+        return;
+    }
+#undef EGG_V3
     if (S.prec == EGG_B200_PREC_FP64) {
         switch (S.variant) {
         case 0: launch_tile<kVar64[0].ci, kVar64[0].cj, kVar64[0].minb, KIND, double>(S, xin, xout, tau, delta, omega); break;
@@ -710,11 +808,6 @@ template <int KIND> static void launch_interior(Session& S, const double* xin, d
         default: launch_tile<kVar32[2].ci, kVar32[2].cj, kVar32[2].minb, KIND, float>(S, xin, xout, tau, delta, omega); break;
         }
     }
-}
-
-static Variant variant_shape(const Session& S, int v)
-{
-    return S.prec == EGG_B200_PREC_FP64 ? kVar64[v] : kVar32[v];
 }
 
 // Time every interior-kernel variant on the resident data (reads the
@@ -790,6 +883,14 @@ template <int KIND> static void launch_stored(Session& S, const double* xin, dou
                                               double delta, double omega)
 {
     if (S.n_stored == 0) { return; }
+    if (S.dim == 3) {
+        StoredPatch3 sp {S.n_stored, S.st_slot.p, S.st_off.p, S.st_gc.p,  S.st_gn0.p, S.st_gn1.p,
+                         S.st_gn2.p, S.st_s0.p,   S.st_s1.p,  S.st_s2.p, S.st_role.p, S.st_W.p,
+                         S.st_wstride, S.st_wt.p, S.st_wtstride};
+        const unsigned grid = unsigned((S.n_stored + 127) / 128);
+        S.timed(kKStored, [&] { stored3_kernel<KIND><<<grid, 128, 0, S.stream>>>(sp, xin, xout, tau, delta, omega); });
+        return;
+    }
     const StoredPatch2 sp = stored_view(S);
     const unsigned grid = unsigned((S.n_stored + 127) / 128);
     S.timed(kKStored, [&] {
@@ -803,6 +904,10 @@ static void launch_broadcast(Session& S, double* x)
 {
     if (S.nshare == 0) { return; }
     const unsigned grid = unsigned(std::min<int64_t>((S.nshare + 255) / 256, 148 * 8));
+    if (S.dim == 3) {
+        S.timed(kKBroadcast, [&] { broadcast3_kernel<<<grid, 256, 0, S.stream>>>(x, S.sh_src.p, S.sh_dst.p, S.nshare); });
+        return;
+    }
     S.timed(kKBroadcast, [&] {
         broadcast2_kernel<<<grid, 256, 0, S.stream>>>(reinterpret_cast<double2*>(x), S.sh_src.p, S.sh_dst.p, S.nshare);
     });
@@ -821,11 +926,23 @@ template <int KIND> static void launch_reduce(Session& S, const double* x, doubl
         es.cell_off = S.es_cell_off.p;
         es.ncell = S.es_ncell;
         es.W = S.es_W.p;
-        es.w_stride = S.es_wstride == 0 ? 0 : 4;
+        es.w_stride = S.es_wstride;
         es.wt = S.es_wt.p;
         es.wt_stride = S.es_wtstride;
+        if (S.dim == 3) {
+            S.timed(kKReduce, [&] {
+                energy_structured3_kernel<KIND><<<S.red_grid, 256, 0, S.stream>>>(es, x, delta, ps, pc, pm);
+            });
+        } else {
+            S.timed(kKReduce, [&] {
+                energy_structured2_kernel<KIND><<<S.red_grid, 256, 0, S.stream>>>(es, X2, delta, ps, pc, pm);
+            });
+        }
+    } else if (S.dim == 3) {
+        EnergyStored3 es {S.es_ns,  S.es_gc.p, S.es_gn0.p,    S.es_gn1.p, S.es_gn2.p,     S.es_s0.p,
+                          S.es_s1.p, S.es_s2.p, S.es_W.p, S.es_wstride, S.es_wt.p, S.es_wtstride};
         S.timed(kKReduce, [&] {
-            energy_structured2_kernel<KIND><<<S.red_grid, 256, 0, S.stream>>>(es, X2, delta, ps, pc, pm);
+            energy_stored3_kernel<KIND><<<S.red_grid, 256, 0, S.stream>>>(es, x, delta, ps, pc, pm);
         });
     } else {
         EnergyStored2 es;
@@ -1186,9 +1303,10 @@ int egg_b200_session_variant_info(egg_b200_session* s, int32_t* variant, int32_t
         for (int v = 0; v < n && v < kNumVariants; ++v) {
             const Variant vs = variant_shape(S, v);
             if (shape) {
-                shape[3 * v] = vs.ci;
-                shape[3 * v + 1] = vs.cj;
-                shape[3 * v + 2] = vs.minb;
+                shape[4 * v] = vs.ci;
+                shape[4 * v + 1] = vs.cj;
+                shape[4 * v + 2] = vs.ck;
+                shape[4 * v + 3] = vs.minb;
             }
             if (times_ms) { times_ms[v] = S.variant_ms[v]; }
         }
@@ -1288,6 +1406,28 @@ int egg_b200_patch_eval(int32_t objective, double delta, const double* X, int64_
         *mindet = o[7];
         step[0] = o[8];
         step[1] = o[9];
+    });
+}
+
+int egg_b200_metric3_probe(int32_t objective, double delta, const double* t, const double* v, int64_t n,
+                           double* mu, double* grad9, double* hv)
+{
+    return guarded([&] {
+        check_objective(objective);
+        if (n < 0) { invalid("metric3_probe: negative n"); }
+        if (n == 0) { return; }
+        if (!t || !v || !mu || !grad9 || !hv) { invalid("metric3_probe: NULL argument"); }
+        DevBuf<double> dt, dv, dm, dg, dh;
+        dt.upload(std::vector<double>(t, t + 9 * n));
+        dv.upload(std::vector<double>(v, v + 3 * n));
+        dm.alloc(n);
+        dg.alloc(9 * n);
+        dh.alloc(6 * n);
+        metric3_probe_kernel<<<unsigned((n + 127) / 128), 128>>>(objective, delta, dt.p, dv.p, n, dm.p, dg.p, dh.p);
+        EGG_CK(cudaGetLastError());
+        EGG_CK(cudaMemcpy(mu, dm.p, n * sizeof(double), cudaMemcpyDeviceToHost));
+        EGG_CK(cudaMemcpy(grad9, dg.p, 9 * n * sizeof(double), cudaMemcpyDeviceToHost));
+        EGG_CK(cudaMemcpy(hv, dh.p, 6 * n * sizeof(double), cudaMemcpyDeviceToHost));
     });
 }
 

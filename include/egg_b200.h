@@ -166,7 +166,8 @@ int egg_b200_session_restore(egg_b200_session* s);
  * reference (AdaptiveCpp picks launch shapes itself). */
 int egg_b200_session_autotune(egg_b200_session* s, int32_t objective, int32_t reps, int32_t* chosen);
 int egg_b200_session_set_variant(egg_b200_session* s, int32_t variant);
-/* Current variant, per-variant (ci, cj, min CTAs/SM) [3*n] and tuned times [n]. */
+/* Current variant, per-variant shape (ci, cj, ck, min CTAs/SM) [4*n] -- 2D:
+ * cells per CTA, 3D: DOFs per CTA -- and the tuned times in ms [n]. */
 int egg_b200_session_variant_info(egg_b200_session* s, int32_t* variant, int32_t* shape, double* times_ms,
                                   int32_t n);
 
@@ -179,6 +180,14 @@ int egg_b200_session_launch_count(egg_b200_session* s, int64_t* launches);
  * t [n*4] -> mu [n], grad [n*4], hess [n*16]. */
 int egg_b200_metric_eval(int32_t objective, double delta, const double* t, int64_t n, double* mu,
                          double* grad, double* hess);
+
+/* Device evaluation of the 3D metric along the kernels' own code path: for n
+ * rows of vec(T) [9] and directions v [3]: mu [n], the gradient over vec(T)
+ * [9n] and the contracted Hessian sum_cc' v_c v_c' H[(i,c),(j,c')] packed
+ * (xx, xy, xz, yy, yz, zz) [6n].  GPU twin of the oracle binding
+ * metric_eval_3d (src/bindings.cpp:1806-1815). */
+int egg_b200_metric3_probe(int32_t objective, double delta, const double* t, const double* v, int64_t n,
+                           double* mu, double* grad9, double* hv);
 
 /* Device evaluation of one stored patch (grad, hess, energy, mindet) and its
  * Newton step (the GPU twin of the oracle bindings patch_eval / newton_step,

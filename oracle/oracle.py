@@ -60,6 +60,13 @@ def load():
         lib.oracle_metric2d.argtypes = [C.c_int, C.c_double, P, P, P, P]
         lib.oracle_patch2d.restype = None
         lib.oracle_patch2d.argtypes = [C.c_int, C.c_double, P, C.c_int32] + [P] * 7 + [P] * 5
+        lib.oracle_metric3d.restype = None
+        lib.oracle_metric3d.argtypes = [C.c_int, C.c_double, P, P, P, P]
+        lib.oracle_run3d.restype = I64
+        lib.oracle_run3d.argtypes = [C.c_int, C.c_double, C.c_double, C.c_int, C.c_int, I64, P, I64] + [P] * 11 + [
+            I64] + [P] * 8 + [I64, P, P]
+        lib.oracle_energy3d.restype = None
+        lib.oracle_energy3d.argtypes = [C.c_int, C.c_double, P, I64] + [P] * 8 + [I64, P, P]
         _lib = lib
     return _lib
 
@@ -90,6 +97,14 @@ def patch(X, gc, gn0, gn1, s0, s1, W, role, kind="shape", delta=0.0):
     lib.oracle_patch2d(KIND[kind], float(delta), _p(X), len(ints[0]), _p(ints[0]), _p(ints[1]), _p(ints[2]),
                        _p(reals[0]), _p(reals[1]), _p(reals[2]), _p(ints[3]), _p(g), _p(h), _p(e), _p(md), _p(st))
     return g, h, float(e[0]), float(md[0]), st
+
+
+def metric3(t, kind="shape", delta=0.0):
+    lib = load()
+    t = np.ascontiguousarray(t, dtype=np.float64)
+    mu, g, H = np.zeros(1), np.zeros(9), np.zeros(81)
+    lib.oracle_metric3d(KIND[kind], float(delta), _p(t), _p(mu), _p(g), _p(H))
+    return float(mu[0]), g, H
 
 
 def patches_for(blocks, free, w_inv=None, d=2):
@@ -133,17 +148,17 @@ def patches_for(blocks, free, w_inv=None, d=2):
     else:
         W = w_inv.reshape(-1, d * d)[sid].copy()
     W[interior[m_node]] = np.eye(d).reshape(-1)
-    return {
+    out = {
         "dof": dofs,
         "off": off,
         "gc": Cc[m_cell, m_b].astype(np.int32),
-        "gn0": Cc[m_cell, m_b ^ bits[0]].astype(np.int32),
-        "gn1": Cc[m_cell, m_b ^ bits[1]].astype(np.int32),
-        "s0": sgn[m_b, 0].copy(),
-        "s1": sgn[m_b, 1].copy(),
         "role": m_role.astype(np.int32),
         "W": np.ascontiguousarray(W),
     }
+    for k in range(d):
+        out[f"gn{k}"] = Cc[m_cell, m_b ^ bits[k]].astype(np.int32)
+        out[f"s{k}"] = sgn[m_b, k].copy()
+    return out
 
 
 def stencil_for(blocks, w_inv=None, d=2):
@@ -157,8 +172,11 @@ def stencil_for(blocks, w_inv=None, d=2):
         W, stride = w_inv.reshape(-1).copy(), 0
     else:
         W, stride = np.ascontiguousarray(w_inv.reshape(-1)), d * d
-    return {"gc": gc.astype(np.int32), "gn0": gn[0].astype(np.int32), "gn1": gn[1].astype(np.int32),
-            "s0": s[0], "s1": s[1], "W": W, "stride": stride}
+    out = {"gc": gc.astype(np.int32), "W": W, "stride": stride}
+    for k in range(d):
+        out[f"gn{k}"] = gn[k].astype(np.int32)
+        out[f"s{k}"] = s[k]
+    return out
 
 
 def run(X, patches, stencil, n_sweeps, *, phase="barrier", delta=0.0, omega=1.0, report_every=0):
@@ -178,6 +196,37 @@ def run(X, patches, stencil, n_sweeps, *, phase="barrier", delta=0.0, omega=1.0,
     if r < 0:
         raise MemoryError("oracle_run2d: allocation failed")
     return Xw.reshape(-1, 2), E[:r], M[:r]
+
+
+def run3(X, patches, stencil, n_sweeps, *, phase="barrier", delta=0.0, omega=1.0, report_every=0):
+    """3D block-Jacobi on a copy of X (N, 3); returns (X_out, energies, mindets)."""
+    lib = load()
+    Xw = np.ascontiguousarray(X, dtype=np.float64).reshape(-1).copy()
+    k = report_every if report_every > 0 else max(n_sweeps, 1)
+    nrep = (n_sweeps + k - 1) // k if n_sweeps > 0 else 0
+    E = np.zeros(max(nrep, 1))
+    M = np.zeros(max(nrep, 1))
+    pt, st = patches, stencil
+    r = lib.oracle_run3d(
+        KIND[phase], float(delta), float(omega), int(n_sweeps), int(report_every), Xw.size // 3, _p(Xw),
+        pt["dof"].size, _p(pt["dof"]), _p(pt["off"]), _p(pt["gc"]), _p(pt["gn0"]), _p(pt["gn1"]), _p(pt["gn2"]),
+        _p(pt["s0"]), _p(pt["s1"]), _p(pt["s2"]), _p(pt["role"]), _p(pt["W"]), st["gc"].size, _p(st["gc"]),
+        _p(st["gn0"]), _p(st["gn1"]), _p(st["gn2"]), _p(st["s0"]), _p(st["s1"]), _p(st["s2"]), _p(st["W"]),
+        st["stride"], _p(E), _p(M))
+    if r < 0:
+        raise MemoryError("oracle_run3d: allocation failed")
+    return Xw.reshape(-1, 3), E[:r], M[:r]
+
+
+def energy3(X, stencil, *, phase="barrier", delta=0.0):
+    lib = load()
+    Xw = np.ascontiguousarray(X, dtype=np.float64).reshape(-1)
+    e, m = np.zeros(1), np.zeros(1)
+    st = stencil
+    lib.oracle_energy3d(KIND[phase], float(delta), _p(Xw), st["gc"].size, _p(st["gc"]), _p(st["gn0"]),
+                        _p(st["gn1"]), _p(st["gn2"]), _p(st["s0"]), _p(st["s1"]), _p(st["s2"]), _p(st["W"]),
+                        st["stride"], _p(e), _p(m))
+    return float(e[0]), float(m[0])
 
 
 def energy(X, stencil, *, phase="barrier", delta=0.0):

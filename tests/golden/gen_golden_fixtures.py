@@ -84,6 +84,9 @@ CASES = {
     "disk_oh17": ("disk_oh", dict(n=17, frac=0.25, seed=2), None),
     "disk_oh33": ("disk_oh", dict(n=33, frac=0.25, seed=5), None),
     "tangled33": ("tangled_square", dict(n=33, seed=4), None),
+    "cube9": ("unit_cube", dict(n=9, frac=0.2, seed=3), None),
+    "two_cubes7": ("two_cubes", dict(n=7, frac=0.2, seed=4), None),
+    "sphere_in_cube7": ("sphere_in_cube", dict(n=7, frac=0.1, seed=5), None),
 }
 RUNS = [
     # (case, phase, delta, omega, n_sweeps)
@@ -93,6 +96,13 @@ RUNS = [
     ("disk_oh33", "barrier", 0.0, 0.8, 40),
     ("square33", "shape_size", 0.0, 1.0, 40),
     ("tangled33", "untangle", 2e-4, 0.5, 40),
+]
+RUNS3 = [
+    ("cube9", "barrier", 0.0, 1.0, 20),
+    ("two_cubes7", "barrier", 0.0, 0.8, 20),
+    ("sphere_in_cube7", "barrier", 0.0, 0.8, 20),
+    ("cube9", "shape_size", 0.0, 1.0, 10),
+    ("two_cubes7", "untangle", 1e-3, 0.5, 10),
 ]
 
 
@@ -111,13 +121,13 @@ def _runs_for(prec: str) -> dict:
         raise SystemExit(f"oracle/_ref/{prec} missing: run oracle/build_ref.sh first")
     assert bool(ref.REAL_IS_FLOAT) == (prec == "fp32")
     out = {}
-    for case, phase, delta, omega, n in RUNS:
+    for case, phase, delta, omega, n in RUNS + RUNS3:
         g = case_grid(case)
         ctx, st = g.wire(), g.structured()
         X1, e1, m1 = ref.cpp_structured_sweep(ctx, st, g.X_flat(), 1, device="cpu", phase=phase,
-                                               delta=delta, omega=omega, report_every=1)
+                                               delta=delta, omega=omega, report_every=1, dim=g.d)
         Xn, en, mn = ref.cpp_structured_sweep(ctx, st, g.X_flat(), n, device="cpu", phase=phase,
-                                               delta=delta, omega=omega, report_every=1)
+                                               delta=delta, omega=omega, report_every=1, dim=g.d)
         key = f"{prec}/{case}/{phase}/{omega}"
         out[key + "/X1"] = X1
         out[key + "/Xn"] = Xn

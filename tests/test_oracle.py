@@ -89,3 +89,29 @@ def test_oracle_matches_reference_build_when_present():
     assert np.abs(Xo.ravel() - X).max() < 1e-14
     np.testing.assert_allclose(Eo, E, rtol=1e-13)
     np.testing.assert_allclose(Mo, M, rtol=1e-13)
+
+
+from tests.golden.gen_golden_fixtures import RUNS3  # noqa: E402
+
+
+@pytest.mark.parametrize("rec", _records("golden_metric_3d"), ids=lambda r: str(r["t"][:2]))
+def test_metric3_matches_reference_golden(rec):
+    mu, g, H = oracle.metric3(np.array(rec["t"]), "shape")
+    np.testing.assert_allclose(mu, rec["mu"], rtol=1e-12, atol=1e-13)
+    np.testing.assert_allclose(g, rec["grad"], rtol=1e-11, atol=1e-12)
+    np.testing.assert_allclose(H, rec["hess"], rtol=1e-11, atol=1e-11 * (1 + np.abs(rec["hess"]).max()))
+
+
+@pytest.mark.parametrize("run", RUNS3, ids=lambda r: f"{r[0]}-{r[1]}-{r[3]}")
+def test_oracle3_matches_recorded_reference(run):
+    case, phase, delta, omega, n = run
+    g = case_grid(case)
+    pt = oracle.patches_for(g.blocks, g.free, d=3)
+    sc = oracle.stencil_for(g.blocks, d=3)
+    key = f"fp64/{case}/{phase}/{omega}"
+    h = float(__import__("egg_b200.configs", fromlist=["x"])._min_edge(g.blocks, g.X).min())
+    X1, _, _ = oracle.run3(g.X, pt, sc, 1, phase=phase, delta=delta, omega=omega, report_every=1)
+    assert np.abs(X1.ravel() - _REF[key + "/X1"]).max() <= 1e-12 * h
+    Xn, E, M = oracle.run3(g.X, pt, sc, n, phase=phase, delta=delta, omega=omega, report_every=1)
+    np.testing.assert_allclose(E, _REF[key + "/E"], rtol=1e-10)
+    np.testing.assert_allclose(M, _REF[key + "/M"], rtol=1e-9, atol=1e-15)
