@@ -26,7 +26,7 @@ EXT = sysconfig.get_config_var("EXT_SUFFIX")
 CORE = PKG / f"cpp_core{EXT}"
 
 CU_SOURCES = [CSRC / "session.cu"]
-CU_DEPS = sorted(CSRC.glob("*.cuh")) + [INCLUDE / "egg_b200.h"]
+CU_DEPS = sorted(CSRC.glob("*.cuh")) + sorted(CSRC.glob("*.inc")) + [INCLUDE / "egg_b200.h"]
 
 
 def _stale(target: Path, deps) -> bool:

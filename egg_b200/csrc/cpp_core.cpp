@@ -275,6 +275,7 @@ class Session
         }
         h_.reset(h);
         M_ = D.d.num_nodes;
+        nblocks_ = D.d.num_blocks;
     }
 
     std::tuple<py::array_t<double>, py::array_t<double>> run(int n_sweeps, const std::string& phase, double delta,
@@ -296,17 +297,44 @@ class Session
         return {vec(E), vec(Md)};
     }
 
-    std::tuple<py::array_t<double>, py::array_t<double>> run_fas(int, int, int, int, double, int,
+    std::tuple<py::array_t<double>, py::array_t<double>> run_fas(int n_cycles, int nu_pre, int nu_post,
+                                                                 int nu_coarse, double omega, int max_levels,
                                                                  const std::string& phase)
     {
-        if (phase == "untangle") {
-            throw py::value_error("run_fas: FAS supports the shape phase only, not \"untangle\"");
+        const int per = std::max(nu_pre + nu_post, 1);
+        const int64_t cap = std::max<int64_t>(int64_t(n_cycles) * per, 1);
+        std::vector<double> E(static_cast<size_t>(cap)), Md(static_cast<size_t>(cap));
+        int64_t nrep = 0;
+        int rc;
+        {
+            py::gil_scoped_release nogil;
+            rc = egg_b200_session_run_fas(h_.get(), n_cycles, nu_pre, nu_post, nu_coarse, omega, max_levels,
+                                          objective_of(phase), E.data(), Md.data(), cap, &nrep);
         }
-        PyErr_SetString(PyExc_NotImplementedError, "egg_b200: run_fas is not built yet");
-        throw py::error_already_set();
+        check(rc);
+        E.resize(size_t(nrep));
+        Md.resize(size_t(nrep));
+        return {vec(E), vec(Md)};
     }
 
-    py::list mg_levels() { return py::list(); }
+    py::list mg_levels()
+    {
+        int32_t n = 0;
+        check(egg_b200_session_mg_levels(h_.get(), &n));
+        py::list levels;
+        for (int32_t l = 0; l < n; ++l) {
+            std::vector<int32_t> sh(size_t(nblocks_) * dim_);
+            check(egg_b200_session_mg_level_shapes(h_.get(), l, sh.data(), int64_t(sh.size())));
+            py::list blocks;
+            for (int b = 0; b < nblocks_; ++b) {
+                py::tuple t(dim_);
+                for (int k = 0; k < dim_; ++k) { t[k] = sh[size_t(b) * dim_ + k]; }
+                blocks.append(t);
+            }
+            levels.append(blocks);
+        }
+        return levels;
+    }
 
     py::array_t<double> get_X()
     {
@@ -353,9 +381,10 @@ class Session
 
     py::dict kernel_stats()
     {
-        static const char* names[6] = {"interior_sweep", "stored_sweep", "broadcast", "reduce", "reduce_final", "copy"};
+        static const char* names[7] = {"interior_sweep", "stored_sweep", "broadcast", "reduce",
+                                       "reduce_final",   "copy",         "fas_transfer"};
         py::dict d;
-        for (int k = 0; k < 6; ++k) {
+        for (int k = 0; k < 7; ++k) {
             double ms = 0;
             int64_t n = 0;
             check(egg_b200_session_kernel_stats(h_.get(), k, &ms, &n));
@@ -426,6 +455,7 @@ class Session
         void operator()(egg_b200_session* s) const { egg_b200_session_destroy(s); }
     };
     int dim_;
+    int nblocks_ = 0;
     int64_t M_ = 0;
     std::unique_ptr<egg_b200_session, Del> h_;
 };

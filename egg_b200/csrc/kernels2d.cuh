@@ -231,7 +231,7 @@ constexpr double kBadCell = 0.1;
 // <= 10 halvings, omega blend.  Same semantics as the shared-sample path.
 template <int KIND>
 __device__ double2 dof_update_fp64(const double2* __restrict__ P, int PW, int ti, int tj, double tx, double ty,
-                                   double delta, double omega)
+                                   double delta, double omega, double2* gout = nullptr)
 {
     const double2 pos = P[(ti + 1) * PW + (tj + 1)];
     double g0 = 0, g1 = 0, hxx = 0, hxy = 0, hyy = 0, e0 = 0;
@@ -273,6 +273,10 @@ __device__ double2 dof_update_fp64(const double2* __restrict__ P, int PW, int ti
         }
     }
     const double gv[2] = {g0 - tx, g1 - ty};
+    if (gout != nullptr) {
+        *gout = make_double2(gv[0], gv[1]);
+        return pos;
+    }
     const double Hm[4] = {hxx, hxy, hxy, hyy};
     double dl[2];
     solve2<double>(Hm, gv, dl);
@@ -313,7 +317,7 @@ __global__ void __launch_bounds__(CI* CJ, MINB)
   interior_tile_kernel(const double2* __restrict__ Xin, double2* __restrict__ Xout,
                        const Tile2* __restrict__ tiles, const BlockInfo* __restrict__ blocks,
                        const uint8_t* __restrict__ active, const double2* __restrict__ tau,
-                       double delta, double omega)
+                       double delta, double omega, double2* __restrict__ grad_out)
 {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     using S = TileShared2<CI, CJ, C>;
@@ -421,11 +425,19 @@ __global__ void __launch_bounds__(CI* CJ, MINB)
     if constexpr (std::is_same_v<C, float>) {
         const int c00 = ti * CJ + tj;
         if (sm.bad[c00] | sm.bad[c00 + 1] | sm.bad[c00 + CJ] | sm.bad[c00 + CJ + 1]) {
-            Xout[slot] = dof_update_fp64<KIND>(sm.P, PW, ti, tj, txd, tyd, delta, omega);
+            if (grad_out != nullptr) {
+                dof_update_fp64<KIND>(sm.P, PW, ti, tj, txd, tyd, delta, omega, grad_out + slot);
+            } else {
+                Xout[slot] = dof_update_fp64<KIND>(sm.P, PW, ti, tj, txd, tyd, delta, omega);
+            }
             return;
         }
     }
     const C gv[2] = {g0 - tx, g1 - ty};
+    if (grad_out != nullptr) {  // gradient-only mode (FAS restriction / tau)
+        grad_out[slot] = make_double2(double(gv[0]), double(gv[1]));
+        return;
+    }
     const C Hm[4] = {hxx, hxy, hxy, hyy};
     C dlt[2];
     solve2<C>(Hm, gv, dlt);
@@ -619,7 +631,7 @@ __device__ void stored_trial(const StoredPatch2& sp, const double2* X, int64_t d
 template <int KIND>
 __global__ void stored_patch_kernel(StoredPatch2 sp, const double2* __restrict__ Xin,
                                     double2* __restrict__ Xout, const double2* __restrict__ tau,
-                                    double delta, double omega)
+                                    double delta, double omega, double2* __restrict__ grad_out)
 {
     const int64_t d = blockIdx.x * int64_t(blockDim.x) + threadIdx.x;
     if (d >= sp.n) { return; }
@@ -634,6 +646,10 @@ __global__ void stored_patch_kernel(StoredPatch2 sp, const double2* __restrict__
         g[0] -= tx;
         g[1] -= ty;
         e0 -= tx * pos.x + ty * pos.y;
+    }
+    if (grad_out != nullptr) {
+        grad_out[slot] = make_double2(g[0], g[1]);
+        return;
     }
     double dl[2];
     solve2<double>(h, g, dl);

@@ -92,7 +92,7 @@ __device__ __forceinline__ void sample3_shared(const double t64[9], double delta
 // redoes the DOF in fp64.
 template <int TI, int TJ, int TK, int KIND, class R>
 __device__ bool dof3_update(const Tile3Shared<TI, TJ, TK>& sm, int ti, int tj, int tk, const double tau[3],
-                            double delta, double omega, double out[3])
+                            double delta, double omega, double out[3], bool grad_only = false)
 {
     using W = Win3<TI, TJ, TK>;
     const int pid = W::idx(ti + 1, tj + 1, tk + 1);
@@ -153,6 +153,12 @@ __device__ bool dof3_update(const Tile3Shared<TI, TJ, TK>& sm, int ti, int tj, i
     }
     e0 += econst;
     const R gv[3] = {g[0] - R(tau[0]), g[1] - R(tau[1]), g[2] - R(tau[2])};
+    if (grad_only) {  // gradient-only mode (FAS restriction / tau)
+        out[0] = double(gv[0]);
+        out[1] = double(gv[1]);
+        out[2] = double(gv[2]);
+        return true;
+    }
     R dl[3];
     solve3<R>(h, gv, dl);
     R alpha = R(1);
@@ -208,7 +214,7 @@ template <int TI, int TJ, int TK, int MINB, int KIND, class C>
 __global__ void __launch_bounds__(TI* TJ* TK, MINB)
   interior3_kernel(const double* __restrict__ Xin, double* __restrict__ Xout, const Tile3* __restrict__ tiles,
                    const BlockInfo* __restrict__ blocks, const uint8_t* __restrict__ active,
-                   const double* __restrict__ tau, double delta, double omega)
+                   const double* __restrict__ tau, double delta, double omega, double* __restrict__ grad_out)
 {
     using W = Win3<TI, TJ, TK>;
     __shared__ Tile3Shared<TI, TJ, TK> sm;
@@ -244,12 +250,14 @@ __global__ void __launch_bounds__(TI* TJ* TK, MINB)
         tv[2] = tau[3 * slot + 2];
     }
     double out[3];
-    if (!dof3_update<TI, TJ, TK, KIND, C>(sm, ti, tj, tk, tv, delta, omega, out)) {
-        dof3_update<TI, TJ, TK, KIND, double>(sm, ti, tj, tk, tv, delta, omega, out);
+    const bool go = grad_out != nullptr;
+    if (!dof3_update<TI, TJ, TK, KIND, C>(sm, ti, tj, tk, tv, delta, omega, out, go)) {
+        dof3_update<TI, TJ, TK, KIND, double>(sm, ti, tj, tk, tv, delta, omega, out, go);
     }
-    Xout[3 * slot] = out[0];
-    Xout[3 * slot + 1] = out[1];
-    Xout[3 * slot + 2] = out[2];
+    double* dst = go ? grad_out : Xout;
+    dst[3 * slot] = out[0];
+    dst[3 * slot + 1] = out[1];
+    dst[3 * slot + 2] = out[2];
 }
 
 // ---------------------------------------------------------------------------
@@ -309,7 +317,7 @@ __device__ __forceinline__ void assemble_T3(const double* X, int32_t ic, const i
 
 template <int KIND>
 __global__ void stored3_kernel(StoredPatch3 sp, const double* __restrict__ Xin, double* __restrict__ Xout,
-                               const double* __restrict__ tau, double delta, double omega)
+                               const double* __restrict__ tau, double delta, double omega, double* __restrict__ grad_out)
 {
     const int64_t d = blockIdx.x * int64_t(blockDim.x) + threadIdx.x;
     if (d >= sp.n) { return; }
@@ -348,6 +356,10 @@ __global__ void stored3_kernel(StoredPatch3 sp, const double* __restrict__ Xin, 
             g[q] -= tv[q];
             e0 -= tv[q] * pos[q];
         }
+    }
+    if (grad_out != nullptr) {
+        for (int q = 0; q < 3; ++q) { grad_out[3 * int64_t(slot) + q] = g[q]; }
+        return;
     }
     double dl[3];
     solve3<double>(h, g, dl);

@@ -3,8 +3,14 @@
 #include "egg_b200.h"
 #include "kernels2d.cuh"
 #include "kernels3d.cuh"
+#include "fas.cuh"
 
 #include <algorithm>
+#include <array>
+#include <map>
+#include <set>
+#include <unordered_map>
+#include <unordered_set>
 #include <cmath>
 #include <cstdio>
 #include <cstdlib>
@@ -82,17 +88,50 @@ constexpr Variant kVar32[kNumVariants] = {{8, 32, 1, 2}, {8, 32, 1, 3}, {16, 32,
 constexpr Variant kVar3_64[kNumVariants] = {{4, 8, 8, 1}, {4, 8, 8, 2}, {2, 8, 16, 2}};
 constexpr Variant kVar3_32[kNumVariants] = {{4, 8, 8, 1}, {4, 8, 8, 2}, {2, 8, 16, 2}};
 
-enum KernelId { kKInterior = 0, kKStored = 1, kKBroadcast = 2, kKReduce = 3, kKFinal = 4, kKCopy = 5, kKCount = 6 };
+enum KernelId {
+    kKInterior = 0,
+    kKStored = 1,
+    kKBroadcast = 2,
+    kKReduce = 3,
+    kKFinal = 4,
+    kKCopy = 5,
+    kKTransfer = 6,
+    kKCount = 7
+};
 
-struct Session {
+// Device data of one relaxation level (the fine store or a coarse FAS level):
+// block layout, structured-interior DOFs (mask + tiles), stored-patch DOFs and
+// the owner -> copy broadcast table.
+struct LevelData {
+    int64_t nstore = 0;
+    std::vector<BlockInfo> blocks_h;
+    DevBuf<BlockInfo> blocks_d;
+    int64_t n_interior = 0;
+    std::vector<uint8_t> active_h;
+    DevBuf<uint8_t> active_d;
+    DevBuf<Tile2> tiles_d;   // 2D tiles of the current variant's shape
+    DevBuf<Tile3> tiles3_d;  // 3D tiles of the current variant's shape
+    int64_t ntiles = 0;
+    int tile_ci = 0, tile_cj = 0, tile_ck = 0;
+    int64_t n_stored = 0;
+    DevBuf<int32_t> st_slot, st_gc, st_gn0, st_gn1, st_gn2, st_role;
+    DevBuf<int64_t> st_off;
+    DevBuf<int8_t> st_s0, st_s1, st_s2;
+    DevBuf<double> st_W, st_wt;
+    int st_wstride = 0, st_wtstride = 0;
+    int64_t nshare = 0;
+    DevBuf<int32_t> sh_src, sh_dst;
+};
+
+#include "fas_types.inc"
+
+struct Session : LevelData {
     int dim = 2;
     int prec = EGG_B200_PREC_FP64;
     int device = 0;
     cudaStream_t stream = nullptr;
 
     int64_t M = 0;       // global nodes
-    int64_t nstore = 0;  // packed store nodes
-    std::vector<BlockInfo> blocks_h;
     std::vector<int32_t> g2s;       // global -> owner slot (-1 if in no block)
     std::vector<int32_t> slot_gid;  // store slot -> global id
     std::vector<double> X_init;     // initial global X (for nodes in no block)
@@ -100,28 +139,19 @@ struct Session {
     DevBuf<double> Xbuf[2];
     int cur = 0;  // index of the canonical buffer
 
-    DevBuf<BlockInfo> blocks_d;
-    // interior DOFs
-    int64_t n_interior = 0;
-    DevBuf<uint8_t> active_d;
-    std::vector<uint8_t> active_h;
-    DevBuf<Tile2> tiles_d;   // 2D tiles of the current variant's shape
-    DevBuf<Tile3> tiles3_d;  // 3D tiles of the current variant's shape
-    int64_t ntiles = 0;
-    int tile_ci = 0, tile_cj = 0, tile_ck = 0;
+    // FAS: relaxed-DOF slots of the fine level, the fine halo relation, the
+    // lazily built coarse hierarchy and fine scratch.
+    std::vector<uint8_t> free_h;
+    DevBuf<uint8_t> free_d;
+    HaloHost halo;
+    bool fas_built = false;
+    std::vector<std::unique_ptr<CoarseLevel>> levels;
+    DevBuf<double> fine_corr, fine_grad, trial;
+    std::vector<double> fas_alphas;
+
     int variant = 0;
     bool tuned = false;
     double variant_ms[kNumVariants] = {};
-    // stored DOFs
-    int64_t n_stored = 0;
-    DevBuf<int32_t> st_slot, st_gc, st_gn0, st_gn1, st_gn2, st_role;
-    DevBuf<int64_t> st_off;
-    DevBuf<int8_t> st_s0, st_s1, st_s2;
-    DevBuf<double> st_W, st_wt;
-    int st_wstride = 0, st_wtstride = 0;
-    // owner -> copy broadcast
-    int64_t nshare = 0;
-    DevBuf<int32_t> sh_src, sh_dst;
     // energy stencil
     bool es_struct = false;
     int64_t es_ns = 0;
@@ -271,14 +301,14 @@ static Variant variant_shape(const Session& S, int v)
 // Tile list of the interior kernel for variant v over every block's
 // structured interior, keeping tiles that hold a moving DOF.  2D: CI x CJ
 // cells, (CI-1) x (CJ-1) DOFs per tile; 3D: CI x CJ x CK DOFs per tile.
-static void set_tiles(Session& S, Variant v)
+static void set_tiles(Session& S, LevelData& L, Variant v)
 {
-    if (S.tile_ci == v.ci && S.tile_cj == v.cj && S.tile_ck == v.ck) { return; }
+    if (L.tile_ci == v.ci && L.tile_cj == v.cj && L.tile_ck == v.ck) { return; }
     const int di = S.dim == 2 ? v.ci - 1 : v.ci, dj = S.dim == 2 ? v.cj - 1 : v.cj, dk = S.dim == 2 ? 1 : v.ck;
     std::vector<Tile2> tiles2;
     std::vector<Tile3> tiles3;
-    for (int b = 0; b < int(S.blocks_h.size()); ++b) {
-        const BlockInfo& bi = S.blocks_h[b];
+    for (int b = 0; b < int(L.blocks_h.size()); ++b) {
+        const BlockInfo& bi = L.blocks_h[b];
         if (bi.n[0] < 3 || bi.n[1] < 3 || (S.dim == 3 && bi.n[2] < 3)) { continue; }
         const int hk = S.dim == 3 ? bi.n[2] - 2 : 1;
         for (int i0 = 1; i0 <= bi.n[0] - 2; i0 += di) {
@@ -289,7 +319,7 @@ static void set_tiles(Session& S, Variant v)
                         for (int j = j0; j < std::min(j0 + dj, bi.n[1] - 1) && !any; ++j) {
                             const int kend = S.dim == 3 ? std::min(k0 + dk, bi.n[2] - 1) : 1;
                             for (int k = S.dim == 3 ? k0 : 0; k < kend; ++k) {
-                                if (S.active_h[bi.off + (int64_t(i) * bi.n[1] + j) * bi.n[2] + k]) {
+                                if (L.active_h[bi.off + (int64_t(i) * bi.n[1] + j) * bi.n[2] + k]) {
                                     any = true;
                                     break;
                                 }
@@ -307,15 +337,15 @@ static void set_tiles(Session& S, Variant v)
         }
     }
     if (S.dim == 2) {
-        S.tiles_d.upload(tiles2);
-        S.ntiles = int64_t(tiles2.size());
+        L.tiles_d.upload(tiles2);
+        L.ntiles = int64_t(tiles2.size());
     } else {
-        S.tiles3_d.upload(tiles3);
-        S.ntiles = int64_t(tiles3.size());
+        L.tiles3_d.upload(tiles3);
+        L.ntiles = int64_t(tiles3.size());
     }
-    S.tile_ci = v.ci;
-    S.tile_cj = v.cj;
-    S.tile_ck = v.ck;
+    L.tile_ci = v.ci;
+    L.tile_cj = v.cj;
+    L.tile_ck = v.ck;
 }
 
 static Session* create_session(const egg_b200_session_desc& d)
@@ -539,6 +569,22 @@ static Session* create_session(const egg_b200_session_desc& d)
         st_off.push_back(int64_t(st_gc.size()));
     }
     S->n_stored = int64_t(st_slot.size());
+    S->free_h.assign(off, 0);
+    for (int32_t sl : st_slot) { S->free_h[sl] = 1; }
+    for (int64_t i = 0; i < off; ++i) {
+        if (active[i]) { S->free_h[i] = 1; }
+    }
+    for (int64_t e = 0; e < d.num_halo; ++e) {
+        std::array<int32_t, 3> sp {0, 0, 0}, dp {0, 0, 0};
+        for (int k = 0; k < D; ++k) {
+            sp[k] = d.halo_src_padded[e * D + k];
+            dp[k] = d.halo_dst_padded[e * D + k];
+        }
+        S->halo.sb.push_back(d.halo_src_block[e]);
+        S->halo.db.push_back(d.halo_dst_block[e]);
+        S->halo.sp.push_back(sp);
+        S->halo.dp.push_back(dp);
+    }
     if (w_uniform || st_W.empty()) {
         st_W.assign(d.W_inv, d.W_inv + (w_uniform ? D * D : 0));
         if (st_W.empty()) { st_W = identity_row(D); }
@@ -718,8 +764,9 @@ static Session* create_session(const egg_b200_session_desc& d)
     }
     S->blocks_d.upload(S->blocks_h);
     S->active_d.upload(S->active_h);
+    S->free_d.upload(S->free_h);
     S->variant = 0;
-    set_tiles(*S, variant_shape(*S, 0));
+    set_tiles(*S, *S, variant_shape(*S, 0));
     S->st_slot.upload(st_slot);
     S->st_off.upload(st_off);
     S->st_gc.upload(st_gc);
@@ -752,32 +799,36 @@ static Session* create_session(const egg_b200_session_desc& d)
 // Sweep driver
 // ---------------------------------------------------------------------------
 template <int CI, int CJ, int MINB, int KIND, class C>
-static void launch_tile(Session& S, const double* xin, double* xout, const double* tau, double delta, double omega)
+static void launch_tile(Session& S, LevelData& L, const double* xin, double* xout, const double* tau, double delta,
+                        double omega, double* gout)
 {
     const size_t smem = sizeof(TileShared2<CI, CJ, C>);
     const auto* xi = reinterpret_cast<const double2*>(xin);
     auto* xo = reinterpret_cast<double2*>(xout);
     const auto* tv = reinterpret_cast<const double2*>(tau);
     S.timed(kKInterior, [&] {
-        interior_tile_kernel<CI, CJ, MINB, KIND, C><<<unsigned(S.ntiles), CI * CJ, smem, S.stream>>>(
-          xi, xo, S.tiles_d.p, S.blocks_d.p, S.active_d.p, tv, delta, omega);
+        interior_tile_kernel<CI, CJ, MINB, KIND, C><<<unsigned(L.ntiles), CI * CJ, smem, S.stream>>>(
+          xi, xo, L.tiles_d.p, L.blocks_d.p, L.active_d.p, tv, delta, omega, reinterpret_cast<double2*>(gout));
     });
 }
 
 template <int TI, int TJ, int TK, int MINB, int KIND, class C>
-static void launch_tile3(Session& S, const double* xin, double* xout, const double* tau, double delta, double omega)
+static void launch_tile3(Session& S, LevelData& L, const double* xin, double* xout, const double* tau, double delta,
+                         double omega, double* gout)
 {
     S.timed(kKInterior, [&] {
-        interior3_kernel<TI, TJ, TK, MINB, KIND, C><<<unsigned(S.ntiles), TI * TJ * TK, 0, S.stream>>>(
-          xin, xout, S.tiles3_d.p, S.blocks_d.p, S.active_d.p, tau, delta, omega);
+        interior3_kernel<TI, TJ, TK, MINB, KIND, C><<<unsigned(L.ntiles), TI * TJ * TK, 0, S.stream>>>(
+          xin, xout, L.tiles3_d.p, L.blocks_d.p, L.active_d.p, tau, delta, omega, gout);
     });
 }
 
-template <int KIND> static void launch_interior(Session& S, const double* xin, double* xout, const double* tau,
-                                                double delta, double omega)
+template <int KIND>
+static void launch_interior(Session& S, LevelData& L, const double* xin, double* xout, const double* tau, double delta,
+                            double omega, double* gout = nullptr)
 {
-    if (S.ntiles == 0) { return; }
-#define EGG_V3(T, C, i) launch_tile3<T[i].ci, T[i].cj, T[i].ck, T[i].minb, KIND, C>(S, xin, xout, tau, delta, omega)
+    if (L.ntiles == 0) { return; }
+#define EGG_V3(T, C, i) \
+    launch_tile3<T[i].ci, T[i].cj, T[i].ck, T[i].minb, KIND, C>(S, L, xin, xout, tau, delta, omega, gout)
     if (S.dim == 3) {
         if (S.prec == EGG_B200_PREC_FP64) {
             switch (S.variant) {
@@ -797,15 +848,15 @@ template <int KIND> static void launch_interior(Session& S, const double* xin, d
 #undef EGG_V3
     if (S.prec == EGG_B200_PREC_FP64) {
         switch (S.variant) {
-        case 0: launch_tile<kVar64[0].ci, kVar64[0].cj, kVar64[0].minb, KIND, double>(S, xin, xout, tau, delta, omega); break;
-        case 1: launch_tile<kVar64[1].ci, kVar64[1].cj, kVar64[1].minb, KIND, double>(S, xin, xout, tau, delta, omega); break;
-        default: launch_tile<kVar64[2].ci, kVar64[2].cj, kVar64[2].minb, KIND, double>(S, xin, xout, tau, delta, omega); break;
+        case 0: launch_tile<kVar64[0].ci, kVar64[0].cj, kVar64[0].minb, KIND, double>(S, L, xin, xout, tau, delta, omega, gout); break;
+        case 1: launch_tile<kVar64[1].ci, kVar64[1].cj, kVar64[1].minb, KIND, double>(S, L, xin, xout, tau, delta, omega, gout); break;
+        default: launch_tile<kVar64[2].ci, kVar64[2].cj, kVar64[2].minb, KIND, double>(S, L, xin, xout, tau, delta, omega, gout); break;
         }
     } else {
         switch (S.variant) {
-        case 0: launch_tile<kVar32[0].ci, kVar32[0].cj, kVar32[0].minb, KIND, float>(S, xin, xout, tau, delta, omega); break;
-        case 1: launch_tile<kVar32[1].ci, kVar32[1].cj, kVar32[1].minb, KIND, float>(S, xin, xout, tau, delta, omega); break;
-        default: launch_tile<kVar32[2].ci, kVar32[2].cj, kVar32[2].minb, KIND, float>(S, xin, xout, tau, delta, omega); break;
+        case 0: launch_tile<kVar32[0].ci, kVar32[0].cj, kVar32[0].minb, KIND, float>(S, L, xin, xout, tau, delta, omega, gout); break;
+        case 1: launch_tile<kVar32[1].ci, kVar32[1].cj, kVar32[1].minb, KIND, float>(S, L, xin, xout, tau, delta, omega, gout); break;
+        default: launch_tile<kVar32[2].ci, kVar32[2].cj, kVar32[2].minb, KIND, float>(S, L, xin, xout, tau, delta, omega, gout); break;
         }
     }
 }
@@ -829,11 +880,11 @@ template <int KIND> static void autotune_impl(Session& S, int reps)
     int best_v = 0;
     for (int v = 0; v < kNumVariants; ++v) {
         S.variant = v;
-        set_tiles(S, variant_shape(S, v));
-        launch_interior<KIND>(S, S.X(S.cur), S.X(1 - S.cur), nullptr, 0.0, 1.0);
+        set_tiles(S, S, variant_shape(S, v));
+        launch_interior<KIND>(S, S, S.X(S.cur), S.X(1 - S.cur), nullptr, 0.0, 1.0);
         EGG_CK(cudaEventRecord(a, S.stream));
         for (int r = 0; r < reps; ++r) {
-            launch_interior<KIND>(S, S.X(S.cur), S.X(1 - S.cur), nullptr, 0.0, 1.0);
+            launch_interior<KIND>(S, S, S.X(S.cur), S.X(1 - S.cur), nullptr, 0.0, 1.0);
         }
         EGG_CK(cudaEventRecord(b, S.stream));
         EGG_CK(cudaEventSynchronize(b));
@@ -848,7 +899,7 @@ template <int KIND> static void autotune_impl(Session& S, int reps)
     cudaEventDestroy(a);
     cudaEventDestroy(b);
     S.variant = best_v;
-    set_tiles(S, variant_shape(S, best_v));
+    set_tiles(S, S, variant_shape(S, best_v));
     S.profiling = prof;
     S.launches = launches;
     S.tuned = true;
@@ -860,7 +911,7 @@ static bool autotune_enabled()
     return !(v && std::string(v) == "0");
 }
 
-static StoredPatch2 stored_view(Session& S)
+static StoredPatch2 stored_view(LevelData& S)
 {
     StoredPatch2 sp;
     sp.n = S.n_stored;
@@ -879,37 +930,41 @@ static StoredPatch2 stored_view(Session& S)
     return sp;
 }
 
-template <int KIND> static void launch_stored(Session& S, const double* xin, double* xout, const double* tau,
-                                              double delta, double omega)
+template <int KIND>
+static void launch_stored(Session& S, LevelData& L, const double* xin, double* xout, const double* tau, double delta,
+                          double omega, double* gout = nullptr)
 {
-    if (S.n_stored == 0) { return; }
+    if (L.n_stored == 0) { return; }
     if (S.dim == 3) {
-        StoredPatch3 sp {S.n_stored, S.st_slot.p, S.st_off.p, S.st_gc.p,  S.st_gn0.p, S.st_gn1.p,
-                         S.st_gn2.p, S.st_s0.p,   S.st_s1.p,  S.st_s2.p, S.st_role.p, S.st_W.p,
-                         S.st_wstride, S.st_wt.p, S.st_wtstride};
-        const unsigned grid = unsigned((S.n_stored + 127) / 128);
-        S.timed(kKStored, [&] { stored3_kernel<KIND><<<grid, 128, 0, S.stream>>>(sp, xin, xout, tau, delta, omega); });
+        StoredPatch3 sp {L.n_stored, L.st_slot.p, L.st_off.p, L.st_gc.p,  L.st_gn0.p, L.st_gn1.p,
+                         L.st_gn2.p, L.st_s0.p,   L.st_s1.p,  L.st_s2.p, L.st_role.p, L.st_W.p,
+                         L.st_wstride, L.st_wt.p, L.st_wtstride};
+        const unsigned grid = unsigned((L.n_stored + 127) / 128);
+        S.timed(kKStored, [&] {
+            stored3_kernel<KIND><<<grid, 128, 0, S.stream>>>(sp, xin, xout, tau, delta, omega, gout);
+        });
         return;
     }
-    const StoredPatch2 sp = stored_view(S);
-    const unsigned grid = unsigned((S.n_stored + 127) / 128);
+    const StoredPatch2 sp = stored_view(L);
+    const unsigned grid = unsigned((L.n_stored + 127) / 128);
     S.timed(kKStored, [&] {
         stored_patch_kernel<KIND><<<grid, 128, 0, S.stream>>>(sp, reinterpret_cast<const double2*>(xin),
                                                               reinterpret_cast<double2*>(xout),
-                                                              reinterpret_cast<const double2*>(tau), delta, omega);
+                                                              reinterpret_cast<const double2*>(tau), delta, omega,
+                                                              reinterpret_cast<double2*>(gout));
     });
 }
 
-static void launch_broadcast(Session& S, double* x)
+static void launch_broadcast(Session& S, LevelData& L, double* x)
 {
-    if (S.nshare == 0) { return; }
-    const unsigned grid = unsigned(std::min<int64_t>((S.nshare + 255) / 256, 148 * 8));
+    if (L.nshare == 0) { return; }
+    const unsigned grid = unsigned(std::min<int64_t>((L.nshare + 255) / 256, 148 * 8));
     if (S.dim == 3) {
-        S.timed(kKBroadcast, [&] { broadcast3_kernel<<<grid, 256, 0, S.stream>>>(x, S.sh_src.p, S.sh_dst.p, S.nshare); });
+        S.timed(kKBroadcast, [&] { broadcast3_kernel<<<grid, 256, 0, S.stream>>>(x, L.sh_src.p, L.sh_dst.p, L.nshare); });
         return;
     }
     S.timed(kKBroadcast, [&] {
-        broadcast2_kernel<<<grid, 256, 0, S.stream>>>(reinterpret_cast<double2*>(x), S.sh_src.p, S.sh_dst.p, S.nshare);
+        broadcast2_kernel<<<grid, 256, 0, S.stream>>>(reinterpret_cast<double2*>(x), L.sh_src.p, L.sh_dst.p, L.nshare);
     });
 }
 
@@ -976,11 +1031,11 @@ template <int KIND> static void run_impl(Session& S, int n_sweeps, double delta,
     S.timed(kKCopy, [&] { EGG_CK(cudaMemcpyAsync(xout, xin, bytes, cudaMemcpyDeviceToDevice, S.stream)); });
     int64_t ridx = 0;
     for (int s = 0; s < n_sweeps; ++s) {
-        launch_broadcast(S, xin);
-        launch_interior<KIND>(S, xin, xout, nullptr, delta, omega);
-        launch_stored<KIND>(S, xin, xout, nullptr, delta, omega);
+        launch_broadcast(S, S, xin);
+        launch_interior<KIND>(S, S, xin, xout, nullptr, delta, omega);
+        launch_stored<KIND>(S, S, xin, xout, nullptr, delta, omega);
         if ((s + 1) % k == 0 || s == n_sweeps - 1) {
-            launch_broadcast(S, xout);
+            launch_broadcast(S, S, xout);
             launch_reduce<KIND>(S, xout, delta, S.red_out.p + 2 * ridx, S.red_out.p + 2 * ridx + 1);
             ++ridx;
         }
@@ -1003,7 +1058,7 @@ template <int KIND> static void run_impl(Session& S, int n_sweeps, double delta,
 
 template <int KIND> static void energy_impl(Session& S, double delta, double& e, double& m)
 {
-    launch_broadcast(S, S.X(S.cur));
+    launch_broadcast(S, S, S.X(S.cur));
     launch_reduce<KIND>(S, S.X(S.cur), delta, S.red_out.p, S.red_out.p + 1);
     double buf[2];
     EGG_CK(cudaMemcpyAsync(buf, S.red_out.p, sizeof(buf), cudaMemcpyDeviceToHost, S.stream));
@@ -1011,6 +1066,8 @@ template <int KIND> static void energy_impl(Session& S, double delta, double& e,
     e = buf[0];
     m = buf[1];
 }
+
+#include "fas_host.inc"
 
 // ---------------------------------------------------------------------------
 // Oracle-primitive kernels
@@ -1139,6 +1196,62 @@ int egg_b200_session_run(egg_b200_session* s, int32_t n_sweeps, int32_t objectiv
         for (size_t i = 0; i < E.size(); ++i) {
             if (energies) { energies[i] = E[i]; }
             if (mindets) { mindets[i] = Md[i]; }
+        }
+    });
+}
+
+int egg_b200_session_run_fas(egg_b200_session* s, int32_t n_cycles, int32_t nu_pre, int32_t nu_post,
+                             int32_t nu_coarse, double omega, int32_t max_levels, int32_t objective,
+                             double* energies, double* mindets, int64_t capacity, int64_t* n_reported)
+{
+    return guarded([&] {
+        if (!s) { invalid("run_fas: NULL session"); }
+        check_objective(objective);
+        if (objective == EGG_B200_OBJ_UNTANGLE) {
+            invalid("run_fas: FAS supports the shape phase only, not \"untangle\"");
+        }
+        if (n_cycles < 0 || nu_pre < 0 || nu_post < 0 || nu_coarse < 0) { invalid("run_fas: negative counts"); }
+        Session& S = *s->impl;
+        EGG_CK(cudaSetDevice(S.device));
+        std::vector<double> E, Md;
+        if (n_cycles > 0) {
+            if (objective == EGG_B200_OBJ_SHAPE) {
+                run_fas_impl<kShape>(S, n_cycles, nu_pre, nu_post, nu_coarse, omega, max_levels, E, Md);
+            } else {
+                run_fas_impl<kShapeSize>(S, n_cycles, nu_pre, nu_post, nu_coarse, omega, max_levels, E, Md);
+            }
+        }
+        if (n_reported) { *n_reported = int64_t(E.size()); }
+        if (int64_t(E.size()) > capacity) { invalid("run_fas: report buffer too small"); }
+        for (size_t i = 0; i < E.size(); ++i) {
+            if (energies) { energies[i] = E[i]; }
+            if (mindets) { mindets[i] = Md[i]; }
+        }
+    });
+}
+
+int egg_b200_session_mg_levels(egg_b200_session* s, int32_t* n_levels)
+{
+    return guarded([&] {
+        if (!s || !n_levels) { invalid("mg_levels: NULL argument"); }
+        Session& S = *s->impl;
+        EGG_CK(cudaSetDevice(S.device));
+        ensure_hierarchy(S);
+        *n_levels = int32_t(S.levels.size());
+    });
+}
+
+int egg_b200_session_mg_level_shapes(egg_b200_session* s, int32_t level, int32_t* shapes, int64_t len)
+{
+    return guarded([&] {
+        if (!s || !shapes) { invalid("mg_level_shapes: NULL argument"); }
+        Session& S = *s->impl;
+        ensure_hierarchy(S);
+        if (level < 0 || level >= int32_t(S.levels.size())) { invalid("mg_level_shapes: level out of range"); }
+        const auto& bl = S.levels[level]->blocks_h;
+        if (len != int64_t(bl.size()) * S.dim) { invalid("mg_level_shapes: output length != num_blocks*dim"); }
+        for (size_t b = 0; b < bl.size(); ++b) {
+            for (int k = 0; k < S.dim; ++k) { shapes[b * S.dim + k] = bl[b].n[k]; }
         }
     });
 }
@@ -1288,7 +1401,7 @@ int egg_b200_session_set_variant(egg_b200_session* s, int32_t variant)
         Session& S = *s->impl;
         EGG_CK(cudaSetDevice(S.device));
         S.variant = variant;
-        set_tiles(S, variant_shape(S, variant));
+        set_tiles(S, S, variant_shape(S, variant));
         S.tuned = true;
     });
 }

@@ -125,6 +125,23 @@ int egg_b200_session_run(egg_b200_session* s, int32_t n_sweeps, int32_t objectiv
                          double omega, int32_t report_every, double* energies, double* mindets,
                          int64_t capacity, int64_t* n_reported);
 
+/* n_cycles FAS V-cycles (nu_pre / nu_post Jacobi sweeps per level, at most
+ * nu_coarse on the coarsest level, the hierarchy clipped to max_levels levels
+ * including the fine one) on the resident store; writes one energy / min det
+ * per cycle.  Shape objectives only (untangle -> EINVAL).  Falls back to
+ * n_cycles*(nu_pre+nu_post) Jacobi sweeps reported every nu_pre+nu_post when
+ * no coarse level exists.  Replaces CppStructuredSweepSession::run_fas
+ * (src/bindings.cpp:1311-1335) -> egg::run_fas (src/fas.hpp:398). */
+int egg_b200_session_run_fas(egg_b200_session* s, int32_t n_cycles, int32_t nu_pre, int32_t nu_post,
+                             int32_t nu_coarse, double omega, int32_t max_levels, int32_t objective,
+                             double* energies, double* mindets, int64_t capacity, int64_t* n_reported);
+
+/* Coarse hierarchy: number of coarse levels, and for level `level` (0 =
+ * first coarse level) each block's interior shape [num_blocks * dim].
+ * Replaces CppStructuredSweepSession::mg_levels (src/bindings.cpp:1339-1356). */
+int egg_b200_session_mg_levels(egg_b200_session* s, int32_t* n_levels);
+int egg_b200_session_mg_level_shapes(egg_b200_session* s, int32_t level, int32_t* shapes, int64_t len);
+
 /* Energy and min det A of the resident state under an objective (the
  * reduction of src/sweep.hpp:1881 reduce_energy_mindet, without a sweep). */
 int egg_b200_session_energy(egg_b200_session* s, int32_t objective, double delta, double* energy,
@@ -146,7 +163,7 @@ int egg_b200_session_info(egg_b200_session* s, int64_t* out, int32_t n);
 
 /* Per-kernel CUDA-event timing on the session stream (off by default).
  * kernel ids: 0 interior sweep, 1 stored-patch sweep, 2 owner->copy broadcast,
- * 3 energy reduction, 4 reduction finalize, 5 buffer copy. */
+ * 3 energy reduction, 4 reduction finalize, 5 buffer copy, 6 FAS transfers. */
 int egg_b200_session_set_profiling(egg_b200_session* s, int32_t enable);
 int egg_b200_session_kernel_stats(egg_b200_session* s, int32_t kernel_id, double* total_ms,
                                   int64_t* launches);

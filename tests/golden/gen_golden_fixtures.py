@@ -87,6 +87,10 @@ CASES = {
     "cube9": ("unit_cube", dict(n=9, frac=0.2, seed=3), None),
     "two_cubes7": ("two_cubes", dict(n=7, frac=0.2, seed=4), None),
     "sphere_in_cube7": ("sphere_in_cube", dict(n=7, frac=0.1, seed=5), None),
+    "square65s": ("unit_square", dict(n=65, frac=0.25, seed=12), None),
+    "disk_oh33s": ("disk_oh", dict(n=33, frac=0.2, seed=13), None),
+    "cube17": ("unit_cube", dict(n=17, frac=0.15, seed=14), None),
+    "sphere_in_cube9": ("sphere_in_cube", dict(n=9, frac=0.1, seed=15), None),
 }
 RUNS = [
     # (case, phase, delta, omega, n_sweeps)
@@ -96,6 +100,14 @@ RUNS = [
     ("disk_oh33", "barrier", 0.0, 0.8, 40),
     ("square33", "shape_size", 0.0, 1.0, 40),
     ("tangled33", "untangle", 2e-4, 0.5, 40),
+]
+# FAS V-cycles: (case, phase, n_cycles, nu_pre, nu_post, nu_coarse, omega, max_levels)
+FAS_RUNS = [
+    ("square65s", "barrier", 4, 2, 2, 32, 1.0, 32),
+    ("square65s", "shape_size", 3, 2, 2, 32, 0.8, 3),
+    ("disk_oh33s", "barrier", 4, 2, 2, 32, 0.8, 32),
+    ("cube17", "barrier", 3, 2, 2, 32, 1.0, 32),
+    ("sphere_in_cube9", "barrier", 3, 2, 2, 16, 0.8, 4),
 ]
 RUNS3 = [
     ("cube9", "barrier", 0.0, 1.0, 20),
@@ -134,6 +146,18 @@ def _runs_for(prec: str) -> dict:
         out[key + "/E"] = en
         out[key + "/M"] = mn
         out[key + "/E1"] = e1
+    for case, phase, nc, npre, npost, ncoarse, omega, ml in FAS_RUNS:
+        g = case_grid(case)
+        sess = ref.CppStructuredSweepSession(g.wire(), g.structured(), g.X_flat(), device="cpu", dim=g.d)
+        E, M = sess.run_fas(nc, nu_pre=npre, nu_post=npost, nu_coarse=ncoarse, omega=omega, max_levels=ml,
+                            phase=phase)
+        key = f"{prec}/fas/{case}/{phase}/{ml}"
+        out[key + "/E"] = E
+        out[key + "/M"] = M
+        out[key + "/X"] = sess.get_X()
+        levels = sess.mg_levels()
+        out[key + "/levels"] = np.array([[list(t) for t in lv] for lv in levels], dtype=np.int32).reshape(
+            len(levels), -1)
     return out
 
 

@@ -1,0 +1,96 @@
+"""FAS V-cycles on the GPU against the reference core's own run_fas
+(recorded per-cycle energies, final positions, hierarchy shapes) and the
+properties the reference tests check (tests/smoothing/test_fas.py)."""
+
+from __future__ import annotations
+
+import numpy as np
+import pytest
+
+from egg_b200 import configs
+from tests.conftest import GOLDEN
+from tests.golden.gen_golden_fixtures import FAS_RUNS, case_grid
+
+pytestmark = pytest.mark.gpu
+
+_REF = np.load(GOLDEN / "ref_sweeps.npz")
+
+
+def _hmin(g):
+    return float(configs._min_edge(g.blocks, g.X).min())
+
+
+def _session(core, g, precision="fp64"):
+    return core.CppStructuredSweepSession(g.wire(), g.structured(), g.X_flat(), dim=g.d, precision=precision)
+
+
+@pytest.mark.parametrize("run", FAS_RUNS, ids=lambda r: f"{r[0]}-{r[1]}-L{r[7]}")
+def test_fas_hierarchy_matches_reference(gpu, run):
+    case, phase, nc, npre, npost, ncoarse, omega, ml = run
+    g = case_grid(case)
+    s = _session(gpu, g)
+    got = np.array([[list(t) for t in lv] for lv in s.mg_levels()], dtype=np.int32).reshape(-1)
+    np.testing.assert_array_equal(got, _REF[f"fp64/fas/{case}/{phase}/{ml}/levels"].reshape(-1))
+
+
+@pytest.mark.parametrize("run", FAS_RUNS, ids=lambda r: f"{r[0]}-{r[1]}-L{r[7]}")
+def test_fas_fp64_matches_reference(gpu, run):
+    case, phase, nc, npre, npost, ncoarse, omega, ml = run
+    g = case_grid(case)
+    key = f"fp64/fas/{case}/{phase}/{ml}"
+    s = _session(gpu, g)
+    E, M = s.run_fas(nc, nu_pre=npre, nu_post=npost, nu_coarse=ncoarse, omega=omega, max_levels=ml, phase=phase)
+    np.testing.assert_allclose(E, _REF[key + "/E"], rtol=1e-8)
+    np.testing.assert_allclose(M, _REF[key + "/M"], rtol=1e-7, atol=1e-16)
+    assert np.abs(s.get_X() - _REF[key + "/X"]).max() <= 1e-8 * _hmin(g)
+
+
+@pytest.mark.parametrize("run", FAS_RUNS, ids=lambda r: f"{r[0]}-{r[1]}-L{r[7]}")
+def test_fas_mixed_tracks_reference(gpu, run):
+    case, phase, nc, npre, npost, ncoarse, omega, ml = run
+    g = case_grid(case)
+    key = f"fp64/fas/{case}/{phase}/{ml}"
+    s = _session(gpu, g, precision="mixed")
+    E, M = s.run_fas(nc, nu_pre=npre, nu_post=npost, nu_coarse=ncoarse, omega=omega, max_levels=ml, phase=phase)
+    e64, e32 = _REF[key + "/E"][-1], _REF[f"fp32/fas/{case}/{phase}/{ml}/E"][-1]
+    assert abs(E[-1] - e64) <= max(1e-6 * abs(e64), 2.0 * abs(e32 - e64)), (E[-1], e64, e32)
+    assert np.sign(M[-1]) == np.sign(_REF[key + "/M"][-1])
+
+
+def test_fas_monotone_and_beats_jacobi(gpu):
+    """Energy decreases every cycle, the barrier holds, and at equal fine-sweep
+    budget FAS reaches lower energy than block-Jacobi (reference test_fas.py:81-145)."""
+    g = configs.unit_square(129, frac=0.25, seed=21)
+    f = _session(gpu, g)
+    E, M = f.run_fas(6, nu_pre=2, nu_post=2)
+    assert np.all(np.diff(E) <= 1e-12 * abs(E[0])) and M[-1] > 0
+    j = _session(gpu, g)
+    Ej, _ = j.run(6 * 4, report_every=4)
+    assert E[-1] < Ej[-1]
+
+
+def test_fas_falls_back_to_jacobi_without_levels(gpu):
+    g = case_grid("square33")
+    a = _session(gpu, g)
+    Ea, Ma = a.run_fas(3, nu_pre=2, nu_post=2, max_levels=1)
+    b = _session(gpu, g)
+    Eb, Mb = b.run(12, report_every=4)
+    np.testing.assert_array_equal(Ea, Eb)
+
+
+def test_fas_rejects_untangle(gpu):
+    g = case_grid("square33")
+    s = _session(gpu, g)
+    with pytest.raises(ValueError, match="untangle"):
+        s.run_fas(1, phase="untangle")
+
+
+def test_fas_agrees_with_jacobi_minimiser(gpu):
+    """Long FAS reaches the energy of long Jacobi (same minimiser, different
+    path; reference tests/smoothing/test_fas.py:113-125 compares energies)."""
+    g = configs.unit_square(33, frac=0.2, seed=22)
+    f = _session(gpu, g)
+    Ef, _ = f.run_fas(40)
+    j = _session(gpu, g)
+    Ej, _ = j.run(4000)
+    assert Ef[-1] <= Ej[-1] + 1e-8 * max(1.0, abs(Ej[-1])), (Ef[-1], Ej[-1])
