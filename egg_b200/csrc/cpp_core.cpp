@@ -365,6 +365,13 @@ class Session
         return {e, m};
     }
 
+    std::tuple<double, double> energy_noalloc(const std::string& phase, double delta, int n_partials)
+    {
+        double e = 0, m = 0;
+        check(egg_b200_session_energy_noalloc(h_.get(), objective_of(phase), delta, n_partials, &e, &m));
+        return {e, m};
+    }
+
     py::dict info()
     {
         int64_t v[10];
@@ -495,6 +502,9 @@ PYBIND11_MODULE(cpp_core, m)
       .def("set_X", &Session::set_X, py::arg("X"), "Upload X (global node order) into every copy.")
       .def("energy", &Session::energy, py::arg("phase") = "barrier", py::arg("delta") = 0.0,
            "(energy, min det A) of the resident state.")
+      .def("energy_noalloc", &Session::energy_noalloc, py::arg("phase") = "barrier", py::arg("delta") = 0.0,
+           py::arg("n_partials") = 0,
+           "energy() through the allocation-free entry point (scratch in one static device array shared by all calls).")
       .def("info", &Session::info)
       .def("set_profiling", &Session::set_profiling, py::arg("enable"))
       .def("kernel_stats", &Session::kernel_stats)

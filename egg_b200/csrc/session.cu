@@ -17,6 +17,7 @@
 #include <cstring>
 #include <limits>
 #include <memory>
+#include <mutex>
 #include <stdexcept>
 #include <string>
 #include <vector>
@@ -1067,6 +1068,99 @@ template <int KIND> static void energy_impl(Session& S, double delta, double& e,
     m = buf[1];
 }
 
+// ---------------------------------------------------------------------------
+// Allocation-free energy: the reduction of energy_impl with its scratch in a
+// file-scope device array.  Layout (doubles): [0, 2) the results (energy,
+// min det), then three runs of n_partials CTA partials (compensated sum,
+// its error term, min det).  Each reduction CTA overwrites its own partial
+// slot, so only the two result slots are cleared before the launch.
+// ---------------------------------------------------------------------------
+constexpr int kNoAllocMaxPartials = EGG_B200_NOALLOC_MAX_PARTIALS;
+constexpr int kNoAllocMaxDevices = 64;
+__device__ __align__(256) double g_noalloc_scratch[3 * kNoAllocMaxPartials + 2];
+
+static std::mutex g_noalloc_mu;
+static double* g_noalloc_ptr[kNoAllocMaxDevices] = {};
+
+// Device address of g_noalloc_scratch, looked up once per device with that
+// device current.
+static double* noalloc_scratch(int device)
+{
+    if (device < 0 || device >= kNoAllocMaxDevices) { invalid("energy_noalloc: device ordinal out of range"); }
+    std::lock_guard<std::mutex> lock(g_noalloc_mu);
+    if (!g_noalloc_ptr[device]) {
+        void* p = nullptr;
+        EGG_CK(cudaGetSymbolAddress(&p, g_noalloc_scratch));
+        g_noalloc_ptr[device] = static_cast<double*>(p);
+    }
+    return g_noalloc_ptr[device];
+}
+
+template <int KIND>
+static void energy_noalloc_impl(Session& S, double delta, int grid, double* scratch, double& e, double& m)
+{
+    double* out = scratch;
+    double* ps = scratch + 2;
+    double* pc = ps + grid;
+    double* pm = pc + grid;
+    double* x = S.X(S.cur);
+    const auto* X2 = reinterpret_cast<const double2*>(x);
+    if (S.nshare) {
+        const unsigned bgrid = unsigned(std::min<int64_t>((S.nshare + 255) / 256, 148 * 8));
+        if (S.dim == 3) {
+            broadcast3_kernel<<<bgrid, 256, 0, S.stream>>>(x, S.sh_src.p, S.sh_dst.p, S.nshare);
+        } else {
+            broadcast2_kernel<<<bgrid, 256, 0, S.stream>>>(reinterpret_cast<double2*>(x), S.sh_src.p, S.sh_dst.p,
+                                                            S.nshare);
+        }
+        EGG_CK(cudaGetLastError());
+        ++S.launches;
+    }
+    EGG_CK(cudaMemsetAsync(out, 0, 2 * sizeof(double), S.stream));
+    if (S.es_struct) {
+        EnergyStructured2 es;
+        es.nblocks = int32_t(S.blocks_h.size());
+        es.blocks = S.blocks_d.p;
+        es.cell_off = S.es_cell_off.p;
+        es.ncell = S.es_ncell;
+        es.W = S.es_W.p;
+        es.w_stride = S.es_wstride;
+        es.wt = S.es_wt.p;
+        es.wt_stride = S.es_wtstride;
+        if (S.dim == 3) {
+            energy_structured3_kernel<KIND><<<grid, 256, 0, S.stream>>>(es, x, delta, ps, pc, pm);
+        } else {
+            energy_structured2_kernel<KIND><<<grid, 256, 0, S.stream>>>(es, X2, delta, ps, pc, pm);
+        }
+    } else if (S.dim == 3) {
+        EnergyStored3 es {S.es_ns,  S.es_gc.p, S.es_gn0.p,    S.es_gn1.p, S.es_gn2.p,     S.es_s0.p,
+                          S.es_s1.p, S.es_s2.p, S.es_W.p, S.es_wstride, S.es_wt.p, S.es_wtstride};
+        energy_stored3_kernel<KIND><<<grid, 256, 0, S.stream>>>(es, x, delta, ps, pc, pm);
+    } else {
+        EnergyStored2 es;
+        es.n = S.es_ns;
+        es.gc = S.es_gc.p;
+        es.gn0 = S.es_gn0.p;
+        es.gn1 = S.es_gn1.p;
+        es.s0 = S.es_s0.p;
+        es.s1 = S.es_s1.p;
+        es.W = S.es_W.p;
+        es.w_stride = S.es_wstride;
+        es.wt = S.es_wt.p;
+        es.wt_stride = S.es_wtstride;
+        energy_stored2_kernel<KIND><<<grid, 256, 0, S.stream>>>(es, X2, delta, ps, pc, pm);
+    }
+    EGG_CK(cudaGetLastError());
+    reduce_finalize_kernel<<<1, 1024, 0, S.stream>>>(ps, pc, pm, grid, out, out + 1);
+    EGG_CK(cudaGetLastError());
+    S.launches += 2;
+    double buf[2];
+    EGG_CK(cudaMemcpyAsync(buf, out, sizeof(buf), cudaMemcpyDeviceToHost, S.stream));
+    EGG_CK(cudaStreamSynchronize(S.stream));
+    e = buf[0];
+    m = buf[1];
+}
+
 #include "fas_host.inc"
 
 // ---------------------------------------------------------------------------
@@ -1268,6 +1362,32 @@ int egg_b200_session_energy(egg_b200_session* s, int32_t objective, double delta
         case EGG_B200_OBJ_SHAPE: energy_impl<kShape>(S, delta, e, m); break;
         case EGG_B200_OBJ_UNTANGLE: energy_impl<kUntangle>(S, delta, e, m); break;
         default: energy_impl<kShapeSize>(S, delta, e, m); break;
+        }
+        if (energy) { *energy = e; }
+        if (mindet) { *mindet = m; }
+    });
+}
+
+int egg_b200_session_energy_noalloc(egg_b200_session* s, int32_t objective, double delta, int32_t n_partials,
+                                    double* energy, double* mindet)
+{
+    return guarded([&] {
+        if (!s) { invalid("energy_noalloc: NULL session"); }
+        check_objective(objective);
+        if (n_partials < 0 || n_partials > kNoAllocMaxPartials) {
+            invalid("energy_noalloc: n_partials must lie in [0, " + std::to_string(kNoAllocMaxPartials) +
+                    "] (0 = the session's own count); got " + std::to_string(n_partials));
+        }
+        Session& S = *s->impl;
+        const int grid = n_partials ? n_partials : S.red_grid;
+        if (grid > kNoAllocMaxPartials) { invalid("energy_noalloc: session partial count exceeds the static array"); }
+        EGG_CK(cudaSetDevice(S.device));
+        double* scratch = noalloc_scratch(S.device);
+        double e = 0, m = 0;
+        switch (objective) {
+        case EGG_B200_OBJ_SHAPE: energy_noalloc_impl<kShape>(S, delta, grid, scratch, e, m); break;
+        case EGG_B200_OBJ_UNTANGLE: energy_noalloc_impl<kUntangle>(S, delta, grid, scratch, e, m); break;
+        default: energy_noalloc_impl<kShapeSize>(S, delta, grid, scratch, e, m); break;
         }
         if (energy) { *energy = e; }
         if (mindet) { *mindet = m; }

@@ -147,6 +147,25 @@ int egg_b200_session_mg_level_shapes(egg_b200_session* s, int32_t level, int32_t
 int egg_b200_session_energy(egg_b200_session* s, int32_t objective, double delta, double* energy,
                             double* mindet);
 
+/* The same energy and min det A through a variant that allocates nothing:
+ * the reduction's per-CTA partials and its two results live in one
+ * file-scope __device__ array of 3 * EGG_B200_NOALLOC_MAX_PARTIALS + 2
+ * doubles (96 KiB + 16 B per device) instead of session buffers, and the
+ * call makes no cudaMalloc, cudaFree or other allocating library call on
+ * its success path (a failure stores its message like every other entry
+ * point).  n_partials is the number of reduction CTAs: 0 picks the
+ * session's own count, which gives results bit-identical to
+ * egg_b200_session_energy; 1..EGG_B200_NOALLOC_MAX_PARTIALS sets it; larger
+ * or negative values fail with EGG_B200_EINVAL.  Every call on a device
+ * shares the one array: calls whose GPU work overlaps (concurrent host
+ * threads, or sessions on different streams) race on it.  Each call
+ * returns only after its own result has reached the host.
+ * No counterpart in the reference: it exists for callers that must not
+ * allocate device memory per call. */
+#define EGG_B200_NOALLOC_MAX_PARTIALS 4096
+int egg_b200_session_energy_noalloc(egg_b200_session* s, int32_t objective, double delta,
+                                    int32_t n_partials, double* energy, double* mindet);
+
 /* Download the resident positions in GLOBAL node order ([num_nodes*dim]).
  * Replaces CppStructuredSweepSession::get_X (src/bindings.cpp:1359-1376). */
 int egg_b200_session_get_X(egg_b200_session* s, double* X, int64_t len);
