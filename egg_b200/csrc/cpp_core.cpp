@@ -445,6 +445,13 @@ class Session
         return d;
     }
 
+    uintptr_t stream()
+    {
+        void* p = nullptr;
+        check(egg_b200_session_stream(h_.get(), &p));
+        return reinterpret_cast<uintptr_t>(p);
+    }
+
     int64_t launch_count()
     {
         int64_t n = 0;
@@ -512,6 +519,7 @@ PYBIND11_MODULE(cpp_core, m)
       .def("checkpoint", &Session::checkpoint, "Copy the resident positions to a device-side checkpoint.")
       .def("restore", &Session::restore, "Restore the resident positions from the device-side checkpoint.")
       .def("launch_count", &Session::launch_count)
+      .def("stream", &Session::stream, "The session's cudaStream_t as an integer (for host-side events).")
       .def("autotune", &Session::autotune, py::arg("phase") = "barrier", py::arg("reps") = 3)
       .def("set_variant", &Session::set_variant, py::arg("variant"))
       .def("variants", &Session::variants)

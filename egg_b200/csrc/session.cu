@@ -1554,6 +1554,14 @@ int egg_b200_session_launch_count(egg_b200_session* s, int64_t* launches)
     });
 }
 
+int egg_b200_session_stream(egg_b200_session* s, void** stream)
+{
+    return guarded([&] {
+        if (!s || !stream) { invalid("stream: NULL argument"); }
+        *stream = static_cast<void*>(s->impl->stream);
+    });
+}
+
 int egg_b200_session_reset_stats(egg_b200_session* s)
 {
     return guarded([&] {

@@ -211,6 +211,12 @@ int egg_b200_session_variant_info(egg_b200_session* s, int32_t* variant, int32_t
  * reset_stats (every kernel of this library counts, copies excluded). */
 int egg_b200_session_launch_count(egg_b200_session* s, int64_t* launches);
 
+/* The session's CUDA stream (a cudaStream_t), on which every kernel and copy
+ * of the session is issued, so that a host can record its own events around
+ * a call.  Session-specific instrumentation (the reference queue is
+ * internal). */
+int egg_b200_session_stream(egg_b200_session* s, void** stream);
+
 /* Device evaluation of the per-sample metric on n vec(T) rows (the GPU twin of
  * the reference's oracle binding metric_eval, src/bindings.cpp:1778-1800):
  * t [n*4] -> mu [n], grad [n*4], hess [n*16]. */
