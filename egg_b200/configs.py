@@ -261,3 +261,68 @@ def sphere_in_cube(n: int = 129, frac: float = 0.2, seed: int = 0, radius: float
     noise = rng.uniform(-1.0, 1.0, size=(N, 3)) * (frac * h)[:, None]
     X = X + np.where(free[:, None], noise, 0.0)
     return Grid(f"sphere_in_cube{n}", 3, blocks, X, free, {"frac": frac, "seed": seed, "radius": radius})
+
+
+def _log_uniform_odd(rng, lo: int, hi: int) -> int:
+    n = int(round(float(np.exp(rng.uniform(np.log(lo), np.log(hi))))))
+    n += 1 - n % 2
+    return int(min(max(n, lo), hi))
+
+
+def multiblock_mesh(seed: int, *, min_blocks: int = 3, max_blocks: int = 9, lo: int = 17, hi: int = 257,
+                    frac: float = 0.25) -> Grid:
+    """A conforming 2D multi-block mesh: a random 4-connected set of
+    `min_blocks..max_blocks` cells of an r x c arrangement of rectangles
+    (strips, L, T and zig-zag shapes arise), every row of cells sharing one
+    node count in y and every column one in x, counts log-uniform odd in
+    [lo, hi].  Uniform spacing h = 1 / (hi - 1); nodes on the outline of the
+    union are fixed, every other node carries seeded uniform noise of
+    +-frac h."""
+    rng = np.random.default_rng(seed)
+    nb = int(rng.integers(min_blocks, max_blocks + 1))
+    while True:
+        r, c = int(rng.integers(1, 4)), int(rng.integers(1, 10))
+        if r * c >= nb:
+            break
+    cells = [(int(rng.integers(r)), int(rng.integers(c)))]
+    steps = ((1, 0), (-1, 0), (0, 1), (0, -1))
+    while len(cells) < nb:
+        i, j = cells[int(rng.integers(len(cells)))]
+        di, dj = steps[int(rng.integers(4))]
+        cand = (i + di, j + dj)
+        if 0 <= cand[0] < r and 0 <= cand[1] < c and cand not in cells:
+            cells.append(cand)
+    cells.sort()
+    ny = [_log_uniform_odd(rng, lo, hi) for _ in range(r)]
+    nx = [_log_uniform_odd(rng, lo, hi) for _ in range(c)]
+    h = 1.0 / (hi - 1)
+    y0 = np.concatenate([[0.0], np.cumsum([(n - 1) * h for n in ny])])
+    x0 = np.concatenate([[0.0], np.cumsum([(n - 1) * h for n in nx])])
+    pts = []
+    for i, j in cells:
+        xs = x0[j] + h * np.arange(nx[j])
+        ys = y0[i] + h * np.arange(ny[i])
+        pts.append(np.stack(np.meshgrid(xs, ys, indexing="ij"), axis=-1))
+    blocks, X = _dedupe(pts)
+    # Outline: block-side edges that belong to one block only.
+    count: dict[tuple[int, int], int] = {}
+    for b in blocks:
+        for side in (b[0, :], b[-1, :], b[:, 0], b[:, -1]):
+            for u, v in zip(side[:-1], side[1:]):
+                e = (int(min(u, v)), int(max(u, v)))
+                count[e] = count.get(e, 0) + 1
+    fixed = np.zeros(X.shape[0], dtype=bool)
+    for (u, v), k in count.items():
+        if k == 1:
+            fixed[u] = fixed[v] = True
+    free = ~fixed
+    X = X.copy()
+    X[free] += rng.uniform(-frac * h, frac * h, size=(int(free.sum()), 2))
+    return Grid(f"mb{seed}", 2, blocks, X, free,
+                {"h": h, "frac": frac, "seed": seed, "cells": cells, "nx": nx, "ny": ny})
+
+
+def batch_meshes(n_meshes: int = 256, seed: int = 0, **kw) -> list[Grid]:
+    """Independent multi-block meshes for the batched sweep (mesh k uses seed
+    seed * 100003 + k)."""
+    return [multiblock_mesh(seed * 100003 + k, **kw) for k in range(n_meshes)]

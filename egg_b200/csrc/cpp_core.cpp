@@ -464,7 +464,8 @@ class Session
         throw py::value_error("run_control: session was built without a control wire");
     }
 
-  private:
+  protected:
+    explicit Session(int dim) : dim_(dim) {}
     struct Del {
         void operator()(egg_b200_session* s) const { egg_b200_session_destroy(s); }
     };
@@ -472,6 +473,113 @@ class Session
     int nblocks_ = 0;
     int64_t M_ = 0;
     std::unique_ptr<egg_b200_session, Del> h_;
+};
+
+// Several independent meshes in one device-resident session (one launch per
+// kernel over all meshes, per-mesh reports).
+class Batch : public Session
+{
+  public:
+    Batch(const py::sequence& meshes, const std::string& device, int dim, const py::object& precision) :
+        Session(dim)
+    {
+        const int prec = parse_precision(precision);
+        const int dev = device_of(device);
+        const size_t n = py::len(meshes);
+        if (n == 0) { throw py::value_error("CppBatchSweepSession: no meshes"); }
+        std::vector<Desc> descs(n);
+        std::vector<egg_b200_session_desc> raw(n);
+        for (size_t m = 0; m < n; ++m) {
+            py::sequence t = meshes[m].cast<py::sequence>();
+            if (py::len(t) != 3) { throw py::value_error("CppBatchSweepSession: each mesh is (ctx_arrays, structured, X)"); }
+            fill_desc(descs[m], t[0].cast<py::dict>(), t[1].cast<py::dict>(), DArr::ensure(t[2]), dim, prec, dev);
+            raw[m] = descs[m].d;
+        }
+        egg_b200_session* h = nullptr;
+        int rc;
+        {
+            py::gil_scoped_release nogil;
+            rc = egg_b200_batch_create(raw.data(), int32_t(n), &h);
+        }
+        check(rc);
+        h_.reset(h);
+        int32_t nm = 0;
+        offs_.resize(n + 1);
+        check(egg_b200_batch_size(h_.get(), &nm, offs_.data()));
+        n_ = nm;
+        M_ = offs_.back();
+        nblocks_ = 0;
+        for (const auto& d : raw) { nblocks_ += d.num_blocks; }
+    }
+
+    int num_meshes() const { return n_; }
+
+    std::vector<int64_t> node_offsets() const { return offs_; }
+
+    // (energies, mindets) of shape (n_meshes, reports).
+    std::tuple<py::array_t<double>, py::array_t<double>> run(int n_sweeps, const std::string& phase, double delta,
+                                                             double omega, int report_every)
+    {
+        const int k = report_every <= 0 ? std::max(n_sweeps, 1) : report_every;
+        const int64_t cap = n_sweeps > 0 ? (int64_t(n_sweeps) + k - 1) / k : 0;
+        std::vector<double> E(static_cast<size_t>(cap * n_)), Md(static_cast<size_t>(cap * n_));
+        int64_t nrep = 0;
+        int rc;
+        {
+            py::gil_scoped_release nogil;
+            rc = egg_b200_batch_run(h_.get(), n_sweeps, objective_of(phase), delta, omega, report_every, E.data(),
+                                    Md.data(), cap, &nrep);
+        }
+        check(rc);
+        py::array_t<double> e({int64_t(n_), nrep}), md({int64_t(n_), nrep});
+        auto ev = e.mutable_unchecked<2>();
+        auto mv = md.mutable_unchecked<2>();
+        for (int64_t r = 0; r < nrep; ++r) {
+            for (int m = 0; m < n_; ++m) {
+                ev(m, r) = E[size_t(r * n_ + m)];
+                mv(m, r) = Md[size_t(r * n_ + m)];
+            }
+        }
+        return {e, md};
+    }
+
+    std::tuple<py::array_t<double>, py::array_t<double>> energy(const std::string& phase, double delta)
+    {
+        std::vector<double> E(static_cast<size_t>(n_)), Md(static_cast<size_t>(n_));
+        check(egg_b200_batch_energy(h_.get(), objective_of(phase), delta, E.data(), Md.data()));
+        return {vec(E), vec(Md)};
+    }
+
+    // Per-mesh positions (each flat, global node order of its mesh).
+    py::list get_X_list()
+    {
+        py::array_t<double> all = get_X();
+        const double* p = all.data();
+        py::list out;
+        for (int m = 0; m < n_; ++m) {
+            std::vector<double> x(p + offs_[m] * dim_, p + offs_[m + 1] * dim_);
+            out.append(vec(x));
+        }
+        return out;
+    }
+
+    void set_X_list(const py::sequence& Xs)
+    {
+        if (int(py::len(Xs)) != n_) { throw py::value_error("set_X: one array per mesh is required"); }
+        std::vector<double> all(static_cast<size_t>(M_ * dim_));
+        for (int m = 0; m < n_; ++m) {
+            DArr a = DArr::ensure(Xs[m]);
+            if (!a || int64_t(a.size()) != (offs_[m + 1] - offs_[m]) * dim_) {
+                throw py::value_error("set_X: mesh " + std::to_string(m) + " has the wrong length");
+            }
+            std::copy(a.data(), a.data() + a.size(), all.begin() + offs_[m] * dim_);
+        }
+        set_X(DArr(py::array_t<double>(int64_t(all.size()), all.data())));
+    }
+
+  private:
+    int n_ = 0;
+    std::vector<int64_t> offs_;
 };
 
 }  // namespace
@@ -530,6 +638,21 @@ PYBIND11_MODULE(cpp_core, m)
          py::arg("pcg_forcing") = true, py::arg("model_db") = true)
       .def("get_C", [](Session& s) { s.no_control(); })
       .def("set_C", [](Session& s, const DArr&) { s.no_control(); }, py::arg("C"));
+
+    py::class_<Batch, Session>(m, "CppBatchSweepSession",
+                               "Several independent meshes swept together in one device-resident session.")
+      .def(py::init<py::sequence, const std::string&, int, const py::object&>(), py::arg("meshes"), py::kw_only(),
+           py::arg("device") = "auto", py::arg("dim") = 2, py::arg("precision") = py::none(),
+           "meshes: sequence of (ctx_arrays, structured, X) tuples, one per mesh.")
+      .def_property_readonly("num_meshes", &Batch::num_meshes)
+      .def("node_offsets", &Batch::node_offsets)
+      .def("run", &Batch::run, py::arg("n_sweeps"), py::kw_only(), py::arg("phase") = "barrier",
+           py::arg("delta") = 0.0, py::arg("omega") = 1.0, py::arg("report_every") = 0,
+           "Run n_sweeps on every mesh; returns (energies, mindets) of shape (num_meshes, reports).")
+      .def("energy", &Batch::energy, py::arg("phase") = "barrier", py::arg("delta") = 0.0,
+           "Per-mesh (energies, mindets) of the resident state.")
+      .def("get_X", &Batch::get_X_list, "Per-mesh positions, a list of flat arrays in each mesh's node order.")
+      .def("set_X", &Batch::set_X_list, py::arg("X"), "Upload per-mesh positions (a list of flat arrays).");
 
     m.def(
       "cpp_structured_sweep",

@@ -699,9 +699,9 @@ __device__ __forceinline__ Comp comp_merge(Comp a, Comp b)
     return r;
 }
 
-// Block-level reduction of (compensated sum, min) into partial slot blockIdx.x.
-__device__ __forceinline__ void block_reduce_store(Comp acc, double mn, double* part_s,
-                                                   double* part_c, double* part_m)
+// Block-level reduction of (compensated sum, min); thread 0 returns true and
+// holds the block's result in acc / mn.
+__device__ __forceinline__ bool block_reduce(Comp& acc, double& mn)
 {
     __shared__ double ss[32], sc[32], sm[32];
     for (int o = 16; o > 0; o >>= 1) {
@@ -719,29 +719,47 @@ __device__ __forceinline__ void block_reduce_store(Comp acc, double mn, double* 
         sm[wid] = mn;
     }
     __syncthreads();
-    if (wid == 0) {
-        const int nw = (blockDim.x + 31) >> 5;
-        Comp a {0.0, 0.0};
-        double m = INFINITY;
-        if (lane < nw) {
-            a.s = ss[lane];
-            a.c = sc[lane];
-            m = sm[lane];
-        }
-        for (int o = 16; o > 0; o >>= 1) {
-            Comp other;
-            other.s = __shfl_down_sync(0xffffffffu, a.s, o);
-            other.c = __shfl_down_sync(0xffffffffu, a.c, o);
-            const double om = __shfl_down_sync(0xffffffffu, m, o);
-            a = comp_merge(a, other);
-            m = fmin(m, om);
-        }
-        if (lane == 0) {
-            part_s[blockIdx.x] = a.s;
-            part_c[blockIdx.x] = a.c;
-            part_m[blockIdx.x] = m;
-        }
+    if (wid != 0) { return false; }
+    const int nw = (blockDim.x + 31) >> 5;
+    Comp a {0.0, 0.0};
+    double m = INFINITY;
+    if (lane < nw) {
+        a.s = ss[lane];
+        a.c = sc[lane];
+        m = sm[lane];
     }
+    for (int o = 16; o > 0; o >>= 1) {
+        Comp other;
+        other.s = __shfl_down_sync(0xffffffffu, a.s, o);
+        other.c = __shfl_down_sync(0xffffffffu, a.c, o);
+        const double om = __shfl_down_sync(0xffffffffu, m, o);
+        a = comp_merge(a, other);
+        m = fmin(m, om);
+    }
+    acc = a;
+    mn = m;
+    return lane == 0;
+}
+
+// Block reduction into partial slot blockIdx.y * gridDim.x + blockIdx.x
+// (blockIdx.y = segment of a segmented reduction, 0 otherwise).
+__device__ __forceinline__ void block_reduce_store(Comp acc, double mn, double* part_s,
+                                                   double* part_c, double* part_m)
+{
+    if (block_reduce(acc, mn)) {
+        const int64_t slot = int64_t(blockIdx.y) * gridDim.x + blockIdx.x;
+        part_s[slot] = acc.s;
+        part_c[slot] = acc.c;
+        part_m[slot] = mn;
+    }
+}
+
+// Item range of this CTA row: segment blockIdx.y of `seg` (prefix offsets),
+// or [0, n) without segments.
+__device__ __forceinline__ void segment_range(const int64_t* seg, int64_t n, int64_t& lo, int64_t& hi)
+{
+    lo = seg ? seg[blockIdx.y] : 0;
+    hi = seg ? seg[blockIdx.y + 1] : n;
 }
 
 struct EnergyStructured2 {
@@ -753,6 +771,7 @@ struct EnergyStructured2 {
     int32_t w_stride;         // 0 or 4 (per sample)
     const double* wt;         // [1] or [ncell*4]
     int32_t wt_stride;
+    const int64_t* seg = nullptr;  // per-mesh cell prefix offsets (segmented reduction) or null
 };
 
 template <int KIND>
@@ -762,7 +781,9 @@ __global__ void energy_structured2_kernel(EnergyStructured2 es, const double2* _
 {
     Comp acc {0.0, 0.0};
     double mn = INFINITY;
-    for (int64_t c = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; c < es.ncell;
+    int64_t c_lo, c_hi;
+    segment_range(es.seg, es.ncell, c_lo, c_hi);
+    for (int64_t c = c_lo + blockIdx.x * int64_t(blockDim.x) + threadIdx.x; c < c_hi;
          c += int64_t(gridDim.x) * blockDim.x) {
         int lo = 0, hi = es.nblocks - 1;
         while (lo < hi) {
@@ -804,6 +825,7 @@ struct EnergyStored2 {
     int32_t w_stride;
     const double* wt;
     int32_t wt_stride;
+    const int64_t* seg = nullptr;  // per-mesh sample prefix offsets or null
 };
 
 template <int KIND>
@@ -812,7 +834,9 @@ __global__ void energy_stored2_kernel(EnergyStored2 es, const double2* __restric
 {
     Comp acc {0.0, 0.0};
     double mn = INFINITY;
-    for (int64_t i = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; i < es.n;
+    int64_t i_lo, i_hi;
+    segment_range(es.seg, es.n, i_lo, i_hi);
+    for (int64_t i = i_lo + blockIdx.x * int64_t(blockDim.x) + threadIdx.x; i < i_hi;
          i += int64_t(gridDim.x) * blockDim.x) {
         double t[4], detA;
         assemble_T(X[es.gc[i]], X[es.gn0[i]], X[es.gn1[i]], double(es.s0[i]), double(es.s1[i]),
@@ -833,13 +857,27 @@ __global__ void reduce_finalize_kernel(const double* part_s, const double* part_
         acc = comp_merge(acc, Comp {part_s[i], part_c[i]});
         mn = fmin(mn, part_m[i]);
     }
-    __shared__ double ps[1], pc[1], pm[1];
-    // reuse the block reducer with blockIdx.x == 0 semantics
-    block_reduce_store(acc, mn, ps, pc, pm);
-    __syncthreads();
-    if (threadIdx.x == 0) {
-        *out_e = ps[0] + pc[0];
-        *out_m = pm[0];
+    if (block_reduce(acc, mn)) {
+        *out_e = acc.s + acc.c;
+        *out_m = mn;
+    }
+}
+
+// Segmented final pass: CTA m folds partials [m n, (m+1) n) into
+// out[2m] = energy and out[2m+1] = min det of segment m.
+__global__ void reduce_finalize_seg_kernel(const double* part_s, const double* part_c,
+                                           const double* part_m, int n, double* out)
+{
+    const int64_t base = int64_t(blockIdx.x) * n;
+    Comp acc {0.0, 0.0};
+    double mn = INFINITY;
+    for (int i = threadIdx.x; i < n; i += blockDim.x) {
+        acc = comp_merge(acc, Comp {part_s[base + i], part_c[base + i]});
+        mn = fmin(mn, part_m[base + i]);
+    }
+    if (block_reduce(acc, mn)) {
+        out[2 * int64_t(blockIdx.x)] = acc.s + acc.c;
+        out[2 * int64_t(blockIdx.x) + 1] = mn;
     }
 }
 

@@ -408,7 +408,9 @@ __global__ void energy_structured3_kernel(EnergyStructured2 es, const double* __
 {
     Comp acc {0.0, 0.0};
     double mn = INFINITY;
-    for (int64_t c = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; c < es.ncell;
+    int64_t c_lo, c_hi;
+    segment_range(es.seg, es.ncell, c_lo, c_hi);
+    for (int64_t c = c_lo + blockIdx.x * int64_t(blockDim.x) + threadIdx.x; c < c_hi;
          c += int64_t(gridDim.x) * blockDim.x) {
         int lo = 0, hi = es.nblocks - 1;
         while (lo < hi) {
@@ -456,6 +458,7 @@ struct EnergyStored3 {
     int32_t w_stride;
     const double* wt;
     int32_t wt_stride;
+    const int64_t* seg = nullptr;  // per-mesh sample prefix offsets or null
 };
 
 template <int KIND>
@@ -465,7 +468,10 @@ __global__ void energy_stored3_kernel(EnergyStored3 es, const double* __restrict
     Comp acc {0.0, 0.0};
     double mn = INFINITY;
     const double none[3] = {0, 0, 0};
-    for (int64_t i = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; i < es.n; i += int64_t(gridDim.x) * blockDim.x) {
+    int64_t i_lo, i_hi;
+    segment_range(es.seg, es.n, i_lo, i_hi);
+    for (int64_t i = i_lo + blockIdx.x * int64_t(blockDim.x) + threadIdx.x; i < i_hi;
+         i += int64_t(gridDim.x) * blockDim.x) {
         const double s[3] = {double(es.s0[i]), double(es.s1[i]), double(es.s2[i])};
         const int32_t in[3] = {es.gn0[i], es.gn1[i], es.gn2[i]};
         double t[9], detA;

@@ -166,6 +166,26 @@ struct Session : LevelData {
     int red_grid = 0;
     DevBuf<double> part;      // [3 * red_grid]
     DevBuf<double> red_out;   // [2 * capacity]
+    DevBuf<double> red_tmp;   // [2 * n_seg or 2]: report slot written inside a captured chunk
+    // batch: several independent meshes packed into one store
+    int n_seg = 0;                       // meshes (0: a plain single-mesh session)
+    std::vector<int64_t> mesh_node_off;  // [n_seg + 1] global node offsets
+    DevBuf<int64_t> seg_d;               // [n_seg + 1] energy-stencil item (cell or sample) offsets
+    int seg_gx = 0;                      // reduction CTAs per mesh
+    DevBuf<double> seg_part;             // [3 * seg_gx * n_seg]
+    // CUDA graphs of report chunks (k sweeps + the report reduction)
+    struct ChunkGraph {
+        int kind, k;
+        bool per_mesh;
+        double delta, omega;
+        const double* xin;
+        const double* xout;
+        const void* tiles;
+        int variant;
+        cudaGraphExec_t exec;
+        int64_t launches;
+    };
+    std::vector<ChunkGraph> graphs;
     // profiling
     bool profiling = false;
     int64_t launches = 0;  // every kernel launch (copies excluded)
@@ -176,9 +196,16 @@ struct Session : LevelData {
     std::vector<std::pair<int, std::pair<cudaEvent_t, cudaEvent_t>>> pending;
     std::vector<cudaEvent_t> event_pool;
 
+    void drop_graphs()
+    {
+        for (auto& g : graphs) { cudaGraphExecDestroy(g.exec); }
+        graphs.clear();
+    }
+
     ~Session()
     {
         if (stream) { cudaStreamSynchronize(stream); }
+        drop_graphs();
         for (auto& p : pending) {
             event_pool.push_back(p.second.first);
             event_pool.push_back(p.second.second);
@@ -305,6 +332,7 @@ static Variant variant_shape(const Session& S, int v)
 static void set_tiles(Session& S, LevelData& L, Variant v)
 {
     if (L.tile_ci == v.ci && L.tile_cj == v.cj && L.tile_ck == v.ck) { return; }
+    S.drop_graphs();
     const int di = S.dim == 2 ? v.ci - 1 : v.ci, dj = S.dim == 2 ? v.cj - 1 : v.cj, dk = S.dim == 2 ? 1 : v.ck;
     std::vector<Tile2> tiles2;
     std::vector<Tile3> tiles3;
@@ -1019,39 +1047,192 @@ template <int KIND> static void launch_reduce(Session& S, const double* x, doubl
     S.timed(kKFinal, [&] { reduce_finalize_kernel<<<1, 1024, 0, S.stream>>>(ps, pc, pm, S.red_grid, out_e, out_m); });
 }
 
+// Per-mesh energy / min det of a batch session: CTA row m reduces mesh m's
+// stencil items; out[2m] = energy, out[2m+1] = min det.
+template <int KIND> static void launch_reduce_seg(Session& S, const double* x, double delta, double* out)
+{
+    double* ps = S.seg_part.p;
+    const int64_t np = int64_t(S.seg_gx) * S.n_seg;
+    double* pc = ps + np;
+    double* pm = pc + np;
+    const dim3 grid(unsigned(S.seg_gx), unsigned(S.n_seg));
+    const auto* X2 = reinterpret_cast<const double2*>(x);
+    if (S.es_struct) {
+        EnergyStructured2 es;
+        es.nblocks = int32_t(S.blocks_h.size());
+        es.blocks = S.blocks_d.p;
+        es.cell_off = S.es_cell_off.p;
+        es.ncell = S.es_ncell;
+        es.W = S.es_W.p;
+        es.w_stride = S.es_wstride;
+        es.wt = S.es_wt.p;
+        es.wt_stride = S.es_wtstride;
+        es.seg = S.seg_d.p;
+        if (S.dim == 3) {
+            S.timed(kKReduce, [&] {
+                energy_structured3_kernel<KIND><<<grid, 256, 0, S.stream>>>(es, x, delta, ps, pc, pm);
+            });
+        } else {
+            S.timed(kKReduce, [&] {
+                energy_structured2_kernel<KIND><<<grid, 256, 0, S.stream>>>(es, X2, delta, ps, pc, pm);
+            });
+        }
+    } else if (S.dim == 3) {
+        EnergyStored3 es {S.es_ns,  S.es_gc.p, S.es_gn0.p,    S.es_gn1.p, S.es_gn2.p,     S.es_s0.p,
+                          S.es_s1.p, S.es_s2.p, S.es_W.p, S.es_wstride, S.es_wt.p, S.es_wtstride, S.seg_d.p};
+        S.timed(kKReduce, [&] {
+            energy_stored3_kernel<KIND><<<grid, 256, 0, S.stream>>>(es, x, delta, ps, pc, pm);
+        });
+    } else {
+        EnergyStored2 es;
+        es.n = S.es_ns;
+        es.gc = S.es_gc.p;
+        es.gn0 = S.es_gn0.p;
+        es.gn1 = S.es_gn1.p;
+        es.s0 = S.es_s0.p;
+        es.s1 = S.es_s1.p;
+        es.W = S.es_W.p;
+        es.w_stride = S.es_wstride;
+        es.wt = S.es_wt.p;
+        es.wt_stride = S.es_wtstride;
+        es.seg = S.seg_d.p;
+        S.timed(kKReduce, [&] {
+            energy_stored2_kernel<KIND><<<grid, 256, 0, S.stream>>>(es, X2, delta, ps, pc, pm);
+        });
+    }
+    S.timed(kKFinal, [&] {
+        reduce_finalize_seg_kernel<<<unsigned(S.n_seg), 256, 0, S.stream>>>(ps, pc, pm, S.seg_gx, out);
+    });
+}
+
+// One report's reduction: the whole store (2 doubles) or every mesh of a
+// batch (2 * n_seg doubles, mesh-major).
+template <int KIND> static void launch_report(Session& S, const double* x, double delta, bool per_mesh, double* out)
+{
+    if (per_mesh) {
+        launch_reduce_seg<KIND>(S, x, delta, out);
+    } else {
+        launch_reduce<KIND>(S, x, delta, out, out + 1);
+    }
+}
+
+// One block-Jacobi sweep xin -> xout (broadcast of the read buffer, then the
+// interior tiles and the stored-patch DOFs).
+template <int KIND> static void sweep_once(Session& S, double* xin, double* xout, double delta, double omega)
+{
+    launch_broadcast(S, S, xin);
+    launch_interior<KIND>(S, S, xin, xout, nullptr, delta, omega);
+    launch_stored<KIND>(S, S, xin, xout, nullptr, delta, omega);
+}
+
+static bool graphs_enabled()
+{
+    const char* e = std::getenv("EGG_B200_GRAPHS");
+    return !(e && e[0] == '0');
+}
+
+// CUDA graph of one report chunk: k sweeps starting from `xin`, then the
+// report reduction into red_tmp.  Captured once per (objective, delta,
+// omega, k, start buffer, tile variant) and replayed; kernel arguments are
+// baked in, so a change of tiles or buffers selects (or captures) another.
+template <int KIND>
+static Session::ChunkGraph& chunk_graph(Session& S, int k, bool per_mesh, double delta, double omega, double* xin,
+                                        double* xout)
+{
+    const void* tiles = S.dim == 3 ? static_cast<const void*>(S.tiles3_d.p) : static_cast<const void*>(S.tiles_d.p);
+    for (auto& g : S.graphs) {
+        if (g.kind == KIND && g.k == k && g.per_mesh == per_mesh && g.delta == delta && g.omega == omega &&
+            g.xin == xin && g.xout == xout && g.tiles == tiles && g.variant == S.variant) {
+            return g;
+        }
+    }
+    if (S.graphs.size() >= 16) { S.drop_graphs(); }
+    const int64_t before = S.launches;
+    EGG_CK(cudaStreamBeginCapture(S.stream, cudaStreamCaptureModeThreadLocal));
+    cudaGraph_t graph = nullptr;
+    try {
+        double* a = xin;
+        double* b = xout;
+        for (int s = 0; s < k; ++s) {
+            sweep_once<KIND>(S, a, b, delta, omega);
+            std::swap(a, b);
+        }
+        launch_broadcast(S, S, a);
+        launch_report<KIND>(S, a, delta, per_mesh, S.red_tmp.p);
+    } catch (...) {
+        cudaStreamEndCapture(S.stream, &graph);
+        if (graph) { cudaGraphDestroy(graph); }
+        cudaGetLastError();
+        S.launches = before;
+        throw;
+    }
+    EGG_CK(cudaStreamEndCapture(S.stream, &graph));
+    cudaGraphExec_t exec = nullptr;
+    const cudaError_t st = cudaGraphInstantiate(&exec, graph, 0);
+    cudaGraphDestroy(graph);
+    EGG_CK(st);
+    const int64_t n = S.launches - before;
+    S.launches = before;
+    S.graphs.push_back({KIND, k, per_mesh, delta, omega, xin, xout, tiles, S.variant, exec, n});
+    return S.graphs.back();
+}
+
 template <int KIND> static void run_impl(Session& S, int n_sweeps, double delta, double omega, int report_every,
-                                         std::vector<double>& E, std::vector<double>& Md)
+                                         std::vector<double>& E, std::vector<double>& Md, bool per_mesh = false)
 {
     if (!S.tuned && autotune_enabled()) { autotune_impl<KIND>(S, 3); }
     const int k = report_every <= 0 ? n_sweeps : report_every;
     const int64_t nrep = (int64_t(n_sweeps) + k - 1) / k;
-    if (S.red_out.n < size_t(2 * nrep)) { S.red_out.alloc(size_t(2 * nrep)); }
+    const int64_t width = per_mesh ? S.n_seg : 1;
+    if (S.red_out.n < size_t(2 * nrep * width)) { S.red_out.alloc(size_t(2 * nrep * width)); }
+    if (S.red_tmp.n < size_t(2 * width)) {
+        S.drop_graphs();  // captured chunks write the old red_tmp
+        S.red_tmp.alloc(size_t(2 * width));
+    }
     const size_t bytes = size_t(S.nstore) * S.dim * sizeof(double);
     double* xin = S.X(S.cur);
     double* xout = S.X(1 - S.cur);
     S.timed(kKCopy, [&] { EGG_CK(cudaMemcpyAsync(xout, xin, bytes, cudaMemcpyDeviceToDevice, S.stream)); });
+    // Whole report chunks replay a captured graph (not while profiling, which
+    // times every kernel with its own events).
+    const bool use_graphs = graphs_enabled() && !S.profiling && k >= 2;
     int64_t ridx = 0;
-    for (int s = 0; s < n_sweeps; ++s) {
-        launch_broadcast(S, S, xin);
-        launch_interior<KIND>(S, S, xin, xout, nullptr, delta, omega);
-        launch_stored<KIND>(S, S, xin, xout, nullptr, delta, omega);
+    int s = 0;
+    while (s < n_sweeps) {
+        double* slot = S.red_out.p + 2 * width * ridx;
+        if (use_graphs && s + k <= n_sweeps) {
+            Session::ChunkGraph& g = chunk_graph<KIND>(S, k, per_mesh, delta, omega, xin, xout);
+            EGG_CK(cudaGraphLaunch(g.exec, S.stream));
+            S.launches += g.launches;
+            EGG_CK(cudaMemcpyAsync(slot, S.red_tmp.p, size_t(2 * width) * sizeof(double), cudaMemcpyDeviceToDevice,
+                                   S.stream));
+            if (k % 2) {
+                std::swap(xin, xout);
+                S.cur = 1 - S.cur;
+            }
+            s += k;
+            ++ridx;
+            continue;
+        }
+        sweep_once<KIND>(S, xin, xout, delta, omega);
         if ((s + 1) % k == 0 || s == n_sweeps - 1) {
             launch_broadcast(S, S, xout);
-            launch_reduce<KIND>(S, xout, delta, S.red_out.p + 2 * ridx, S.red_out.p + 2 * ridx + 1);
+            launch_report<KIND>(S, xout, delta, per_mesh, slot);
             ++ridx;
         }
         std::swap(xin, xout);
         S.cur = 1 - S.cur;
-        if ((s + 1) % 64 == 0 && S.profiling) { S.sync(); }
+        ++s;
+        if (s % 64 == 0 && S.profiling) { S.sync(); }
     }
-    std::vector<double> buf(size_t(2 * nrep));
+    std::vector<double> buf(size_t(2 * nrep * width));
     if (nrep) {
         EGG_CK(cudaMemcpyAsync(buf.data(), S.red_out.p, buf.size() * sizeof(double), cudaMemcpyDeviceToHost, S.stream));
     }
     S.sync();
-    E.resize(size_t(nrep));
-    Md.resize(size_t(nrep));
-    for (int64_t i = 0; i < nrep; ++i) {
+    E.resize(size_t(nrep * width));
+    Md.resize(size_t(nrep * width));
+    for (int64_t i = 0; i < nrep * width; ++i) {
         E[i] = buf[2 * i];
         Md[i] = buf[2 * i + 1];
     }
@@ -1162,6 +1343,16 @@ static void energy_noalloc_impl(Session& S, double delta, int grid, double* scra
 }
 
 #include "fas_host.inc"
+#include "batch_host.inc"
+
+template <int KIND> static void batch_energy_impl(Session& S, double delta, std::vector<double>& out)
+{
+    launch_broadcast(S, S, S.X(S.cur));
+    launch_reduce_seg<KIND>(S, S.X(S.cur), delta, S.red_tmp.p);
+    out.resize(2 * size_t(S.n_seg));
+    EGG_CK(cudaMemcpyAsync(out.data(), S.red_tmp.p, out.size() * sizeof(double), cudaMemcpyDeviceToHost, S.stream));
+    S.sync();
+}
 
 // ---------------------------------------------------------------------------
 // Oracle-primitive kernels
@@ -1258,6 +1449,80 @@ int egg_b200_session_create(const egg_b200_session_desc* desc, egg_b200_session*
     });
 }
 
+int egg_b200_batch_create(const egg_b200_session_desc* descs, int32_t n_meshes, egg_b200_session** out)
+{
+    return guarded([&] {
+        if (!descs || !out) { invalid("egg_b200_batch_create: NULL argument"); }
+        *out = nullptr;
+        Session* s = create_batch(descs, n_meshes);
+        *out = new egg_b200_session {s};
+    });
+}
+
+int egg_b200_batch_size(egg_b200_session* s, int32_t* n_meshes, int64_t* node_offsets)
+{
+    return guarded([&] {
+        if (!s || !n_meshes) { invalid("batch_size: NULL argument"); }
+        const Session& S = *s->impl;
+        *n_meshes = S.n_seg;
+        if (node_offsets) {
+            for (size_t i = 0; i < S.mesh_node_off.size(); ++i) { node_offsets[i] = S.mesh_node_off[i]; }
+        }
+    });
+}
+
+int egg_b200_batch_run(egg_b200_session* s, int32_t n_sweeps, int32_t objective, double delta, double omega,
+                       int32_t report_every, double* energies, double* mindets, int64_t capacity,
+                       int64_t* n_reported)
+{
+    return guarded([&] {
+        if (!s) { invalid("batch_run: NULL session"); }
+        check_objective(objective);
+        if (n_sweeps < 0) { invalid("batch_run: n_sweeps must be >= 0"); }
+        Session& S = *s->impl;
+        if (S.n_seg <= 0) { invalid("batch_run: not a batch session"); }
+        EGG_CK(cudaSetDevice(S.device));
+        std::vector<double> E, Md;
+        if (n_sweeps > 0) {
+            switch (objective) {
+            case EGG_B200_OBJ_SHAPE: run_impl<kShape>(S, n_sweeps, delta, omega, report_every, E, Md, true); break;
+            case EGG_B200_OBJ_UNTANGLE:
+                run_impl<kUntangle>(S, n_sweeps, delta, omega, report_every, E, Md, true);
+                break;
+            default: run_impl<kShapeSize>(S, n_sweeps, delta, omega, report_every, E, Md, true); break;
+            }
+        }
+        const int64_t nrep = int64_t(E.size()) / S.n_seg;
+        if (n_reported) { *n_reported = nrep; }
+        if (nrep > capacity) { invalid("batch_run: report buffer too small"); }
+        for (size_t i = 0; i < E.size(); ++i) {
+            if (energies) { energies[i] = E[i]; }
+            if (mindets) { mindets[i] = Md[i]; }
+        }
+    });
+}
+
+int egg_b200_batch_energy(egg_b200_session* s, int32_t objective, double delta, double* energies, double* mindets)
+{
+    return guarded([&] {
+        if (!s) { invalid("batch_energy: NULL session"); }
+        check_objective(objective);
+        Session& S = *s->impl;
+        if (S.n_seg <= 0) { invalid("batch_energy: not a batch session"); }
+        EGG_CK(cudaSetDevice(S.device));
+        std::vector<double> out;
+        switch (objective) {
+        case EGG_B200_OBJ_SHAPE: batch_energy_impl<kShape>(S, delta, out); break;
+        case EGG_B200_OBJ_UNTANGLE: batch_energy_impl<kUntangle>(S, delta, out); break;
+        default: batch_energy_impl<kShapeSize>(S, delta, out); break;
+        }
+        for (int m = 0; m < S.n_seg; ++m) {
+            if (energies) { energies[m] = out[2 * m]; }
+            if (mindets) { mindets[m] = out[2 * m + 1]; }
+        }
+    });
+}
+
 int egg_b200_session_destroy(egg_b200_session* s)
 {
     return guarded([&] {
@@ -1306,6 +1571,9 @@ int egg_b200_session_run_fas(egg_b200_session* s, int32_t n_cycles, int32_t nu_p
         }
         if (n_cycles < 0 || nu_pre < 0 || nu_post < 0 || nu_coarse < 0) { invalid("run_fas: negative counts"); }
         Session& S = *s->impl;
+        if (S.n_seg > 0) {
+            throw Error(EGG_B200_ENOTSUP, "run_fas: FAS is not available on a batch session (one session per mesh)");
+        }
         EGG_CK(cudaSetDevice(S.device));
         std::vector<double> E, Md;
         if (n_cycles > 0) {

@@ -113,6 +113,28 @@ int egg_b200_device_count(int* count);
  * CppStructuredSweepSession constructor (src/bindings.cpp:1268-1281). */
 int egg_b200_session_create(const egg_b200_session_desc* desc, egg_b200_session** out);
 
+/* Batch session: n_meshes independent meshes (same dim, precision and
+ * device) packed into one store, so every sweep is one launch per kernel
+ * over all meshes and report chunks replay one captured CUDA graph.  Each
+ * desc is validated against its own mesh.  The handle works with the
+ * session calls above (run reports the sum over meshes and the global min;
+ * get_X / set_X use the meshes' nodes concatenated in order, mesh m at
+ * node_offsets[m]); run_fas is refused (ENOTSUP).  No counterpart in the
+ * reference, whose sessions hold one mesh each (src/bindings.cpp:1268-1281);
+ * a batch replaces n such sessions run one after another. */
+int egg_b200_batch_create(const egg_b200_session_desc* descs, int32_t n_meshes, egg_b200_session** out);
+/* Mesh count and, if node_offsets is not NULL, its n_meshes + 1 prefix
+ * offsets into the concatenated global node order. */
+int egg_b200_batch_size(egg_b200_session* s, int32_t* n_meshes, int64_t* node_offsets);
+/* run with per-mesh reports: energies / mindets [report * n_meshes + mesh],
+ * capacity and n_reported count reports (rows). */
+int egg_b200_batch_run(egg_b200_session* s, int32_t n_sweeps, int32_t objective, double delta, double omega,
+                       int32_t report_every, double* energies, double* mindets, int64_t capacity,
+                       int64_t* n_reported);
+/* Per-mesh energy and min det A of the resident state ([n_meshes] each). */
+int egg_b200_batch_energy(egg_b200_session* s, int32_t objective, double delta, double* energies,
+                          double* mindets);
+
 /* Release every device allocation of the session (RAII end of the reference
  * session, src/device.hpp:51). */
 int egg_b200_session_destroy(egg_b200_session* s);
