@@ -250,6 +250,70 @@ py::array_t<double> vec(const std::vector<double>& v)
     return out;
 }
 
+// The reference's single-block control wire (egg/smoothing/control_backend.py
+// build_control_wire) -> egg_b200_control_desc.
+void fill_control(egg_b200_control_desc& c, Keep& keep, const py::dict& w, int dim)
+{
+    if (w.contains("blocks")) {
+        PyErr_SetString(PyExc_NotImplementedError,
+                        "egg_b200: multi-block control topologies (control['blocks']) are not supported");
+        throw py::error_already_set();
+    }
+    if (w.contains("walls") && py::len(w["walls"]) > 0) {
+        PyErr_SetString(PyExc_NotImplementedError, "egg_b200: control walls (sliding boundary controls) are not supported");
+        throw py::error_already_set();
+    }
+    for (const char* k : {"block", "ctrl_shape", "k_supp", "C0", "free_idx", "b"}) {
+        if (!w.contains(k)) { throw py::value_error(std::string("control: missing key '") + k + "'"); }
+    }
+    c = egg_b200_control_desc {};
+    c.block = w["block"].cast<int32_t>();
+    c.k_supp = w["k_supp"].cast<int32_t>();
+    int64_t ncs = 0;
+    const int32_t* cs = keep.ints(w["ctrl_shape"], &ncs);
+    if (ncs != dim) { throw py::value_error("control: ctrl_shape must have D entries"); }
+    for (int k = 0; k < dim; ++k) {
+        c.ctrl_shape[k] = cs[k];
+        const std::string ok = "off" + std::to_string(k), wk = "wt" + std::to_string(k);
+        if (!w.contains(ok.c_str()) || !w.contains(wk.c_str())) {
+            throw py::value_error("control: missing per-axis basis table " + ok + "/" + wk);
+        }
+        int64_t nw = 0;
+        c.off[k] = keep.ints(w[ok.c_str()], &c.off_len[k]);
+        c.wt[k] = keep.reals(w[wk.c_str()], &nw);
+        if (nw != c.off_len[k] * int64_t(c.k_supp)) {
+            throw py::value_error("control: wt" + std::to_string(k) + " size != off size * k_supp");
+        }
+    }
+    int64_t nC = 0;
+    c.C0 = keep.reals(w["C0"], &nC);
+    int64_t nctrl = 1;
+    for (int k = 0; k < dim; ++k) { nctrl *= c.ctrl_shape[k]; }
+    if (nC != nctrl * dim) { throw py::value_error("control: C0 size != prod(ctrl_shape) * D"); }
+    c.free_idx = keep.ints(w["free_idx"], &c.n_free);
+    c.b = keep.reals(w["b"], &c.b_len);
+}
+
+py::dict control_report(int n_outer, const std::vector<double>& E, const std::vector<double>& M,
+                        const std::vector<double>& A, const std::vector<double>& PI, const std::vector<double>& PR,
+                        const int64_t* cnt, int32_t iters, int32_t conv)
+{
+    auto take = [](const std::vector<double>& v, int64_t off, int64_t n) {
+        return std::vector<double>(v.begin() + off, v.begin() + off + n);
+    };
+    (void)n_outer;
+    py::dict out;
+    out["energies"] = vec(take(E, 0, cnt[0]));
+    out["mindets"] = vec(take(M, 0, cnt[0]));
+    out["alphas"] = vec(take(A, 0, cnt[1]));
+    out["pcg_iters"] = vec(take(PI, 0, cnt[2]));
+    out["pcg_relres"] = vec(take(PR, 0, cnt[2]));
+    out["frame_jumps"] = vec(std::vector<double>());
+    out["iters"] = iters;
+    out["converged"] = bool(conv);
+    return out;
+}
+
 class Session
 {
   public:
@@ -257,13 +321,11 @@ class Session
             const py::object& control, const py::object& precision) :
         dim_(dim)
     {
-        if (!control.is_none()) {
-            PyErr_SetString(PyExc_NotImplementedError,
-                            "egg_b200: control-net sessions (control=...) are not built yet");
-            throw py::error_already_set();
-        }
         Desc D;
         fill_desc(D, ctx, st, X, dim, parse_precision(precision), device_of(device));
+        Keep ckeep;
+        egg_b200_control_desc cdesc;
+        if (!control.is_none()) { fill_control(cdesc, ckeep, control.cast<py::dict>(), dim); }
         egg_b200_session* h = nullptr;
         {
             py::gil_scoped_release nogil;
@@ -276,6 +338,50 @@ class Session
         h_.reset(h);
         M_ = D.d.num_nodes;
         nblocks_ = D.d.num_blocks;
+        if (!control.is_none()) { check(egg_b200_session_attach_control(h_.get(), &cdesc)); }
+    }
+
+    py::dict run_control(int n_outer, const std::string& phase, double grad_tol, double alpha_min, double lm0,
+                         int pcg_max_iter, double pcg_rtol, bool pcg_forcing, bool model_db)
+    {
+        (void)model_db;  // frozen-frame d b / d C modelling applies to sliding walls only
+        const int64_t ce = int64_t(n_outer) + 1, ca = std::max(n_outer, 1), cp = 8 * ca;
+        std::vector<double> E(static_cast<size_t>(ce)), M(static_cast<size_t>(ce)), A(static_cast<size_t>(ca));
+        std::vector<double> PI(static_cast<size_t>(cp)), PR(static_cast<size_t>(cp));
+        int64_t cnt[3] = {0, 0, 0};
+        int32_t iters = 0, conv = 0;
+        int rc;
+        {
+            py::gil_scoped_release nogil;
+            rc = egg_b200_session_run_control(h_.get(), n_outer, objective_of(phase), grad_tol, alpha_min, lm0,
+                                              pcg_max_iter, pcg_rtol, pcg_forcing ? 1 : 0, E.data(), M.data(),
+                                              A.data(), PI.data(), PR.data(), cnt, &iters, &conv);
+        }
+        check(rc);
+        return control_report(n_outer, E, M, A, PI, PR, cnt, iters, conv);
+    }
+
+    py::array_t<double> get_C()
+    {
+        int64_t n = 0;
+        check(egg_b200_session_control_size(h_.get(), &n));
+        if (n == 0) { throw py::value_error("get_C: session has no control wire"); }
+        std::vector<double> C(static_cast<size_t>(n));
+        check(egg_b200_session_get_C(h_.get(), C.data(), n));
+        return vec(C);
+    }
+
+    void set_C(const DArr& C)
+    {
+        int64_t n = 0;
+        check(egg_b200_session_control_size(h_.get(), &n));
+        if (n == 0) { throw py::value_error("set_C: session has no control wire"); }
+        int rc;
+        {
+            py::gil_scoped_release nogil;
+            rc = egg_b200_session_set_C(h_.get(), C.data(), int64_t(C.size()));
+        }
+        check(rc);
     }
 
     std::tuple<py::array_t<double>, py::array_t<double>> run(int n_sweeps, const std::string& phase, double delta,
@@ -388,10 +494,10 @@ class Session
 
     py::dict kernel_stats()
     {
-        static const char* names[7] = {"interior_sweep", "stored_sweep", "broadcast", "reduce",
-                                       "reduce_final",   "copy",         "fas_transfer"};
+        static const char* names[8] = {"interior_sweep", "stored_sweep", "broadcast",    "reduce",
+                                       "reduce_final",   "copy",         "fas_transfer", "control"};
         py::dict d;
-        for (int k = 0; k < 7; ++k) {
+        for (int k = 0; k < 8; ++k) {
             double ms = 0;
             int64_t n = 0;
             check(egg_b200_session_kernel_stats(h_.get(), k, &ms, &n));
@@ -459,11 +565,6 @@ class Session
         return n;
     }
 
-    [[noreturn]] void no_control()
-    {
-        throw py::value_error("run_control: session was built without a control wire");
-    }
-
   protected:
     explicit Session(int dim) : dim_(dim) {}
     struct Del {
@@ -480,7 +581,8 @@ class Session
 class Batch : public Session
 {
   public:
-    Batch(const py::sequence& meshes, const std::string& device, int dim, const py::object& precision) :
+    Batch(const py::sequence& meshes, const std::string& device, int dim, const py::object& precision,
+          const py::object& control) :
         Session(dim)
     {
         const int prec = parse_precision(precision);
@@ -494,6 +596,14 @@ class Batch : public Session
             if (py::len(t) != 3) { throw py::value_error("CppBatchSweepSession: each mesh is (ctx_arrays, structured, X)"); }
             fill_desc(descs[m], t[0].cast<py::dict>(), t[1].cast<py::dict>(), DArr::ensure(t[2]), dim, prec, dev);
             raw[m] = descs[m].d;
+        }
+        Keep ckeep;
+        std::vector<egg_b200_control_desc> cds;
+        if (!control.is_none()) {
+            py::sequence cl = control.cast<py::sequence>();
+            if (size_t(py::len(cl)) != n) { throw py::value_error("control: one wire per mesh is required"); }
+            cds.resize(n);
+            for (size_t m = 0; m < n; ++m) { fill_control(cds[m], ckeep, cl[m].cast<py::dict>(), dim); }
         }
         egg_b200_session* h = nullptr;
         int rc;
@@ -510,6 +620,36 @@ class Batch : public Session
         M_ = offs_.back();
         nblocks_ = 0;
         for (const auto& d : raw) { nblocks_ += d.num_blocks; }
+        if (!cds.empty()) { check(egg_b200_batch_attach_controls(h_.get(), cds.data())); }
+    }
+
+    // One report dict per mesh.
+    py::list run_control_batch(int n_outer, const std::string& phase, double grad_tol, double alpha_min, double lm0,
+                               int pcg_max_iter, double pcg_rtol, bool pcg_forcing, bool model_db)
+    {
+        (void)model_db;
+        const int64_t ce = int64_t(n_outer) + 1, ca = std::max(n_outer, 1), cp = 8 * ca;
+        const size_t n = size_t(n_);
+        std::vector<double> E(n * ce), M(n * ce), A(n * ca), PI(n * cp), PR(n * cp);
+        std::vector<int64_t> cnt(3 * n);
+        std::vector<int32_t> iters(n), conv(n);
+        int rc;
+        {
+            py::gil_scoped_release nogil;
+            rc = egg_b200_batch_run_control(h_.get(), n_outer, objective_of(phase), grad_tol, alpha_min, lm0,
+                                            pcg_max_iter, pcg_rtol, pcg_forcing ? 1 : 0, E.data(), M.data(), A.data(),
+                                            PI.data(), PR.data(), cnt.data(), iters.data(), conv.data());
+        }
+        check(rc);
+        py::list out;
+        for (size_t m = 0; m < n; ++m) {
+            auto sl = [&](const std::vector<double>& v, int64_t stride) {
+                return std::vector<double>(v.begin() + int64_t(m) * stride, v.begin() + int64_t(m + 1) * stride);
+            };
+            out.append(control_report(n_outer, sl(E, ce), sl(M, ce), sl(A, ca), sl(PI, cp), sl(PR, cp), &cnt[3 * m],
+                                      iters[m], conv[m]));
+        }
+        return out;
     }
 
     int num_meshes() const { return n_; }
@@ -631,19 +771,23 @@ PYBIND11_MODULE(cpp_core, m)
       .def("autotune", &Session::autotune, py::arg("phase") = "barrier", py::arg("reps") = 3)
       .def("set_variant", &Session::set_variant, py::arg("variant"))
       .def("variants", &Session::variants)
-      .def("run_control", [](Session& s, int, const std::string&, double, double, double, int, double, bool, bool) {
-          s.no_control();
-      }, py::arg("n_outer"), py::kw_only(), py::arg("phase") = "barrier", py::arg("grad_tol") = 1e-8,
-         py::arg("alpha_min") = 1e-4, py::arg("lm0") = 0.0, py::arg("pcg_max_iter") = 200, py::arg("pcg_rtol") = 1e-10,
-         py::arg("pcg_forcing") = true, py::arg("model_db") = true)
-      .def("get_C", [](Session& s) { s.no_control(); })
-      .def("set_C", [](Session& s, const DArr&) { s.no_control(); }, py::arg("C"));
+      .def("run_control", &Session::run_control, py::arg("n_outer"), py::kw_only(), py::arg("phase") = "barrier",
+           py::arg("grad_tol") = 1e-8, py::arg("alpha_min") = 1e-4, py::arg("lm0") = 0.0, py::arg("pcg_max_iter") = 200,
+           py::arg("pcg_rtol") = 1e-10, py::arg("pcg_forcing") = true, py::arg("model_db") = true,
+           "Damped reduced Gauss-Newton on the control net; returns the reference's report dict.")
+      .def("get_C", &Session::get_C, "The resident control lattice, flat (n_ctrl * dim,).")
+      .def("set_C", &Session::set_C, py::arg("C"), "Upload a control lattice and evaluate X = M C + b.");
 
     py::class_<Batch, Session>(m, "CppBatchSweepSession",
                                "Several independent meshes swept together in one device-resident session.")
-      .def(py::init<py::sequence, const std::string&, int, const py::object&>(), py::arg("meshes"), py::kw_only(),
-           py::arg("device") = "auto", py::arg("dim") = 2, py::arg("precision") = py::none(),
-           "meshes: sequence of (ctx_arrays, structured, X) tuples, one per mesh.")
+      .def(py::init<py::sequence, const std::string&, int, const py::object&, const py::object&>(), py::arg("meshes"),
+           py::kw_only(), py::arg("device") = "auto", py::arg("dim") = 2, py::arg("precision") = py::none(),
+           py::arg("control") = py::none(),
+           "meshes: sequence of (ctx_arrays, structured, X) tuples, one per mesh; control: one wire per mesh or None.")
+      .def("run_control", &Batch::run_control_batch, py::arg("n_outer"), py::kw_only(), py::arg("phase") = "barrier",
+           py::arg("grad_tol") = 1e-8, py::arg("alpha_min") = 1e-4, py::arg("lm0") = 0.0, py::arg("pcg_max_iter") = 200,
+           py::arg("pcg_rtol") = 1e-10, py::arg("pcg_forcing") = true, py::arg("model_db") = true,
+           "run_control on every mesh's net together; one report dict per mesh.")
       .def_property_readonly("num_meshes", &Batch::num_meshes)
       .def("node_offsets", &Batch::node_offsets)
       .def("run", &Batch::run, py::arg("n_sweeps"), py::kw_only(), py::arg("phase") = "barrier",

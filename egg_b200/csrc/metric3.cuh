@@ -151,6 +151,94 @@ template <class R> EGG_HD void role3(int kind, const Shared3<R>& S, const R v[3]
     }
 }
 
+// Full gradient over vec(T) and the Hessian-vector product H V along an
+// arbitrary V (both 9 entries, row-major), from
+//   d s = 2 T,  d q = 2 Q with Q = s T - T T^T T  (q = |cof T|^2 is the second
+//   invariant of T^T T in 3D),  d D = C,
+//   g = (q F ds + s F dq + s q F_D C) / 9,
+// differentiated along V (s' = 2 T:V, q' = 2 Q:V, D' = C:V, dC = cof'(T)[V]).
+// shape_size adds 2 (D - 1) C and 2 D' C + 2 (D - 1) dC.
+template <class R> EGG_HD void mu3_grad(int kind, const Shared3<R>& S, R g[9])
+{
+    const R* t = S.t;
+    R B[9];  // T^T T
+#pragma unroll
+    for (int i = 0; i < 3; ++i) {
+#pragma unroll
+        for (int j = 0; j < 3; ++j) { B[3 * i + j] = t[i] * t[j] + t[3 + i] * t[3 + j] + t[6 + i] * t[6 + j]; }
+    }
+    const R qF = S.q * S.F, sF = S.s * S.F, sqFD = S.s * S.q * S.FD;
+#pragma unroll
+    for (int i = 0; i < 3; ++i) {
+#pragma unroll
+        for (int j = 0; j < 3; ++j) {
+            const R TB = t[3 * i] * B[j] + t[3 * i + 1] * B[3 + j] + t[3 * i + 2] * B[6 + j];
+            const R Q = S.s * t[3 * i + j] - TB;
+            R v = (R(2) * qF * t[3 * i + j] + R(2) * sF * Q + sqFD * S.C[3 * i + j]) * R(1.0 / 9.0);
+            if (kind == kShapeSize) { v += R(2) * (S.D - R(1)) * S.C[3 * i + j]; }
+            g[3 * i + j] = v;
+        }
+    }
+}
+
+template <class R> EGG_HD void mu3_hvp(int kind, const Shared3<R>& S, const R V[9], R hv[9])
+{
+    const R* t = S.t;
+    const R* C = S.C;
+    R B[9], TtV[9];  // T^T T and T^T V
+#pragma unroll
+    for (int i = 0; i < 3; ++i) {
+#pragma unroll
+        for (int j = 0; j < 3; ++j) {
+            B[3 * i + j] = t[i] * t[j] + t[3 + i] * t[3 + j] + t[6 + i] * t[6 + j];
+            TtV[3 * i + j] = t[i] * V[j] + t[3 + i] * V[3 + j] + t[6 + i] * V[6 + j];
+        }
+    }
+    R Q[9], dC[9];
+    R a = R(0), qd = R(0), Dd = R(0);
+#pragma unroll
+    for (int i = 0; i < 3; ++i) {
+        const int i1 = (i + 1) % 3, i2 = (i + 2) % 3;
+#pragma unroll
+        for (int j = 0; j < 3; ++j) {
+            const int j1 = (j + 1) % 3, j2 = (j + 2) % 3;
+            const R TB = t[3 * i] * B[j] + t[3 * i + 1] * B[3 + j] + t[3 * i + 2] * B[6 + j];
+            Q[3 * i + j] = S.s * t[3 * i + j] - TB;
+            dC[3 * i + j] = V[3 * i1 + j1] * t[3 * i2 + j2] + t[3 * i1 + j1] * V[3 * i2 + j2] -
+                            V[3 * i1 + j2] * t[3 * i2 + j1] - t[3 * i1 + j2] * V[3 * i2 + j1];
+            a += t[3 * i + j] * V[3 * i + j];
+            qd += Q[3 * i + j] * V[3 * i + j];
+            Dd += C[3 * i + j] * V[3 * i + j];
+        }
+    }
+    const R s = S.s, q = S.q, F = S.F, FD = S.FD, FDD = S.FDD;
+    const R sd = R(2) * a;   // s'
+    const R qdd = R(2) * qd; // q'
+    const R c1 = R(2) * (qdd * F + q * FD * Dd);  // d(qF) * 2
+    const R c2 = sd * F + s * FD * Dd;            // d(sF)
+    const R c3 = sd * q * FD + s * qdd * FD + s * q * FDD * Dd;
+#pragma unroll
+    for (int i = 0; i < 3; ++i) {
+#pragma unroll
+        for (int j = 0; j < 3; ++j) {
+            // (V T^T T + T V^T T + T T^T V)_ij
+            R VB = R(0), TVtT = R(0), TTtV = R(0);
+#pragma unroll
+            for (int k = 0; k < 3; ++k) {
+                VB += V[3 * i + k] * B[3 * k + j];
+                TVtT += t[3 * i + k] * TtV[3 * j + k];
+                TTtV += t[3 * i + k] * TtV[3 * k + j];
+            }
+            const R ddq = R(2) * (sd * t[3 * i + j] + s * V[3 * i + j] - VB - TVtT - TTtV);
+            R v = c1 * t[3 * i + j] + R(2) * q * F * V[3 * i + j] + R(2) * c2 * Q[3 * i + j] + s * F * ddq +
+                  c3 * C[3 * i + j] + s * q * FD * dC[3 * i + j];
+            v *= R(1.0 / 9.0);
+            if (kind == kShapeSize) { v += R(2) * Dd * C[3 * i + j] + R(2) * (S.D - R(1)) * dC[3 * i + j]; }
+            hv[3 * i + j] = v;
+        }
+    }
+}
+
 // Newton step -H^{-1} g for a symmetric 3x3 (packed xx, xy, xz, yy, yz, zz)
 // with the reference fallbacks (src/solve.hpp:52-77).
 template <class R> EGG_HD void solve3(const R h[6], const R g[3], R x[3])

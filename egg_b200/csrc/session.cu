@@ -4,6 +4,7 @@
 #include "kernels2d.cuh"
 #include "kernels3d.cuh"
 #include "fas.cuh"
+#include "control.cuh"
 
 #include <algorithm>
 #include <array>
@@ -97,7 +98,8 @@ enum KernelId {
     kKFinal = 4,
     kKCopy = 5,
     kKTransfer = 6,
-    kKCount = 7
+    kKCtl = 7,
+    kKCount = 8
 };
 
 // Device data of one relaxation level (the fine store or a coarse FAS level):
@@ -125,6 +127,7 @@ struct LevelData {
 };
 
 #include "fas_types.inc"
+#include "control_types.inc"
 
 struct Session : LevelData {
     int dim = 2;
@@ -186,6 +189,8 @@ struct Session : LevelData {
         int64_t launches;
     };
     std::vector<ChunkGraph> graphs;
+    // control-net reduced Gauss-Newton (attached on request)
+    std::unique_ptr<ControlState> ctl;
     // profiling
     bool profiling = false;
     int64_t launches = 0;  // every kernel launch (copies excluded)
@@ -1410,6 +1415,8 @@ static void check_objective(int obj)
     }
 }
 
+#include "control_host.inc"
+
 }  // namespace egg_b200
 
 // ===========================================================================
@@ -1520,6 +1527,104 @@ int egg_b200_batch_energy(egg_b200_session* s, int32_t objective, double delta, 
             if (energies) { energies[m] = out[2 * m]; }
             if (mindets) { mindets[m] = out[2 * m + 1]; }
         }
+    });
+}
+
+int egg_b200_session_attach_control(egg_b200_session* s, const egg_b200_control_desc* desc)
+{
+    return guarded([&] {
+        if (!s || !desc) { invalid("attach_control: NULL argument"); }
+        Session& S = *s->impl;
+        if (S.n_seg > 0) { invalid("attach_control: a batch session takes one net per mesh (batch_attach_controls)"); }
+        attach_control(S, desc, 1, nullptr, nullptr);
+    });
+}
+
+int egg_b200_batch_attach_controls(egg_b200_session* s, const egg_b200_control_desc* descs)
+{
+    return guarded([&] {
+        if (!s || !descs) { invalid("batch_attach_controls: NULL argument"); }
+        Session& S = *s->impl;
+        if (S.n_seg <= 0) { invalid("batch_attach_controls: not a batch session"); }
+        // first block of each mesh: blocks are packed mesh by mesh
+        std::vector<int32_t> base(size_t(S.n_seg) + 1, 0);
+        std::vector<int> mesh(size_t(S.n_seg));
+        int32_t b = 0;
+        for (int m = 0; m < S.n_seg; ++m) {
+            base[size_t(m)] = b;
+            mesh[size_t(m)] = m;
+            while (b < int32_t(S.blocks_h.size()) && S.slot_gid[size_t(S.blocks_h[size_t(b)].off)] <
+                                                         S.mesh_node_off[size_t(m) + 1]) {
+                ++b;
+            }
+        }
+        base[size_t(S.n_seg)] = b;
+        attach_control(S, descs, S.n_seg, base.data(), mesh.data());
+    });
+}
+
+int egg_b200_session_run_control(egg_b200_session* s, int32_t n_outer, int32_t objective, double grad_tol,
+                                 double alpha_min, double lm0, int32_t pcg_max_iter, double pcg_rtol,
+                                 int32_t pcg_forcing, double* energies, double* mindets, double* alphas,
+                                 double* pcg_iters, double* pcg_relres, int64_t* counts, int32_t* iters,
+                                 int32_t* converged)
+{
+    return guarded([&] {
+        if (!s) { invalid("run_control: NULL session"); }
+        run_control_abi(*s->impl, n_outer, objective, grad_tol, alpha_min, lm0, pcg_max_iter, pcg_rtol, pcg_forcing,
+                        energies, mindets, alphas, pcg_iters, pcg_relres, counts, iters, converged, false);
+    });
+}
+
+int egg_b200_batch_run_control(egg_b200_session* s, int32_t n_outer, int32_t objective, double grad_tol,
+                               double alpha_min, double lm0, int32_t pcg_max_iter, double pcg_rtol,
+                               int32_t pcg_forcing, double* energies, double* mindets, double* alphas,
+                               double* pcg_iters, double* pcg_relres, int64_t* counts, int32_t* iters,
+                               int32_t* converged)
+{
+    return guarded([&] {
+        if (!s) { invalid("batch_run_control: NULL session"); }
+        run_control_abi(*s->impl, n_outer, objective, grad_tol, alpha_min, lm0, pcg_max_iter, pcg_rtol, pcg_forcing,
+                        energies, mindets, alphas, pcg_iters, pcg_relres, counts, iters, converged, true);
+    });
+}
+
+int egg_b200_session_control_size(egg_b200_session* s, int64_t* n_reals)
+{
+    return guarded([&] {
+        if (!s || !n_reals) { invalid("control_size: NULL argument"); }
+        const Session& S = *s->impl;
+        *n_reals = S.ctl ? S.ctl->total_ctrl * S.dim : 0;
+    });
+}
+
+int egg_b200_session_get_C(egg_b200_session* s, double* C, int64_t len)
+{
+    return guarded([&] {
+        if (!s || !C) { invalid("get_C: NULL argument"); }
+        Session& S = *s->impl;
+        if (!S.ctl) { invalid("get_C: session has no control wire"); }
+        check_len(len, S.ctl->total_ctrl * S.dim, "get_C buffer");
+        EGG_CK(cudaSetDevice(S.device));
+        EGG_CK(cudaMemcpyAsync(C, S.ctl->C.p, size_t(len) * sizeof(double), cudaMemcpyDeviceToHost, S.stream));
+        S.sync();
+    });
+}
+
+int egg_b200_session_set_C(egg_b200_session* s, const double* C, int64_t len)
+{
+    return guarded([&] {
+        if (!s || !C) { invalid("set_C: NULL argument"); }
+        Session& S = *s->impl;
+        if (!S.ctl) { invalid("set_C: session has no control wire"); }
+        if (len != S.ctl->total_ctrl * S.dim) {
+            invalid("set_c: expected " + std::to_string(S.ctl->total_ctrl * S.dim) + " reals, got " +
+                    std::to_string(len));
+        }
+        EGG_CK(cudaSetDevice(S.device));
+        EGG_CK(cudaMemcpyAsync(S.ctl->C.p, C, size_t(len) * sizeof(double), cudaMemcpyHostToDevice, S.stream));
+        ctl_eval_to_x(S);
+        S.sync();
     });
 }
 

@@ -102,6 +102,27 @@ typedef struct egg_b200_session_desc {
     int64_t es_weight_len;
 } egg_b200_session_desc;
 
+/* Control-net wire for one block (src/control_net.hpp:72-87 ControlNetHostT;
+ * built by egg/smoothing/control_backend.py:76 build_control_wire): the
+ * block's nodes are X = M C + b with M the tensor product of per-axis banded
+ * clamped B-spline bases, node i of axis k reading controls off[k][i] ..
+ * off[k][i] + k_supp - 1 with weights wt[k][i * k_supp + t].  Lattice and b
+ * are row-major (last axis fastest) with the dim coordinates innermost. */
+typedef struct egg_b200_control_desc {
+    int32_t block;         /* block the net drives */
+    int32_t k_supp;        /* support width per axis (degree + 1) */
+    int32_t ctrl_shape[3]; /* controls per axis (first dim used) */
+    int32_t reserved;
+    int64_t off_len[3];    /* entries of off[k]: the block's node count on axis k */
+    const int32_t* off[3]; /* first support control per node */
+    const double* wt[3];   /* [off_len[k] * k_supp] basis weights */
+    const double* C0;      /* [prod(ctrl_shape) * dim] initial lattice */
+    int64_t n_free;
+    const int32_t* free_idx; /* [n_free] flat lattice ids of the free controls */
+    int64_t b_len;           /* prod(node counts) * dim */
+    const double* b;         /* Boolean-sum boundary offset */
+} egg_b200_control_desc;
+
 /* Library / device. */
 int egg_b200_abi_version(void);
 const char* egg_b200_last_error(void);
@@ -131,9 +152,52 @@ int egg_b200_batch_size(egg_b200_session* s, int32_t* n_meshes, int64_t* node_of
 int egg_b200_batch_run(egg_b200_session* s, int32_t n_sweeps, int32_t objective, double delta, double omega,
                        int32_t report_every, double* energies, double* mindets, int64_t capacity,
                        int64_t* n_reported);
+/* One control net per mesh of a batch (desc[m].block is local to mesh m).
+ * No counterpart in the reference (one net per session there). */
+int egg_b200_batch_attach_controls(egg_b200_session* s, const egg_b200_control_desc* descs);
+/* run_control on every mesh's net at once: kernels cover all nets, every
+ * decision (convergence, step length, damping) is per mesh.  Outputs are
+ * mesh-major with per-mesh stride n_outer + 1 (energies, mindets), n_outer
+ * (alphas) and 8 * n_outer (pcg_*); counts is [n_meshes * 3]; iters and
+ * converged are [n_meshes]. */
+int egg_b200_batch_run_control(egg_b200_session* s, int32_t n_outer, int32_t objective, double grad_tol,
+                               double alpha_min, double lm0, int32_t pcg_max_iter, double pcg_rtol,
+                               int32_t pcg_forcing, double* energies, double* mindets, double* alphas,
+                               double* pcg_iters, double* pcg_relres, int64_t* counts, int32_t* iters,
+                               int32_t* converged);
+
 /* Per-mesh energy and min det A of the resident state ([n_meshes] each). */
 int egg_b200_batch_energy(egg_b200_session* s, int32_t objective, double delta, double* energies,
                           double* mindets);
+
+
+/* Attach a control net to a session (the reference builds it inside the
+ * session constructor, src/bindings.cpp:1234-1250 -> ControlSessionT,
+ * src/control_solve.hpp:355).  Validation as src/bindings.cpp:507-556
+ * (EINVAL).  ENOTSUP when the energy stencil is not the canonical cell
+ * stencil of the blocks, or when a free control moves a node on a face the
+ * block shares with another block. */
+int egg_b200_session_attach_control(egg_b200_session* s, const egg_b200_control_desc* desc);
+
+/* Damped reduced Gauss-Newton on the free controls with Jacobi-preconditioned
+ * matrix-free PCG (src/control_solve.hpp:533-700 run_plain, :761 pcg_solve;
+ * binding src/bindings.cpp:1382-1437 run_control).  Shape objectives only
+ * (untangle -> EINVAL); EINVAL without a control net.  Outputs (capacities in
+ * parentheses): energies and mindets (n_outer + 1, the initial state first),
+ * alphas (n_outer), pcg_iters and pcg_relres (8 * n_outer, one per PCG
+ * solve); counts[0..2] = entries written to energies, alphas, pcg_*. */
+int egg_b200_session_run_control(egg_b200_session* s, int32_t n_outer, int32_t objective, double grad_tol,
+                                 double alpha_min, double lm0, int32_t pcg_max_iter, double pcg_rtol,
+                                 int32_t pcg_forcing, double* energies, double* mindets, double* alphas,
+                                 double* pcg_iters, double* pcg_relres, int64_t* counts, int32_t* iters,
+                                 int32_t* converged);
+
+/* The resident control lattice (prod(ctrl_shape) * dim reals; stacked over
+ * the meshes of a batch): size, download, and upload followed by the
+ * evaluation X = M C + b into the store (src/bindings.cpp:1441-1480). */
+int egg_b200_session_control_size(egg_b200_session* s, int64_t* n_reals);
+int egg_b200_session_get_C(egg_b200_session* s, double* C, int64_t len);
+int egg_b200_session_set_C(egg_b200_session* s, const double* C, int64_t len);
 
 /* Release every device allocation of the session (RAII end of the reference
  * session, src/device.hpp:51). */
@@ -204,7 +268,8 @@ int egg_b200_session_info(egg_b200_session* s, int64_t* out, int32_t n);
 
 /* Per-kernel CUDA-event timing on the session stream (off by default).
  * kernel ids: 0 interior sweep, 1 stored-patch sweep, 2 owner->copy broadcast,
- * 3 energy reduction, 4 reduction finalize, 5 buffer copy, 6 FAS transfers. */
+ * 3 energy reduction, 4 reduction finalize, 5 buffer copy, 6 FAS transfers,
+ * 7 control-net kernels. */
 int egg_b200_session_set_profiling(egg_b200_session* s, int32_t enable);
 int egg_b200_session_kernel_stats(egg_b200_session* s, int32_t kernel_id, double* total_ms,
                                   int64_t* launches);

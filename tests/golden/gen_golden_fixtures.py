@@ -13,6 +13,10 @@ Two sources, both from the reference checkout (run in a container that has it):
    energy / min-det trajectories), so the GPU tests can compare against the
    reference without the reference present.
 
+3. Control-net runs of the same reference core and of the reference's NumPy
+   dense reduced-GN oracle (``egg.smoothing.control_ref``), with the control
+   wires built by the reference's own builders -> ``ref_control.npz``.
+
 Usage: python tests/golden/gen_golden_fixtures.py [REFERENCE_ROOT]
 """
 
@@ -206,6 +210,97 @@ def gen_reference_wire(ref_root: Path) -> None:
     print(f"ref_wire_disk_oh17.npz: {len(out)} arrays")
 
 
+# Control-net runs: (grid source, ctrl shape, controlled block, phase, n_outer,
+# run_control options, also run the reference's NumPy dense-GN oracle).
+CONTROL_CASES = {
+    "wavy13": ("wavy", dict(n=13), (6, 6), 0, "barrier", 30,
+               dict(pcg_max_iter=500, pcg_rtol=1e-12, pcg_forcing=False), True),
+    "wavy9": ("wavy", dict(n=9), (5, 5), 0, "barrier", 5, {}, False),
+    "wavy13ss": ("wavy", dict(n=13), (6, 6), 0, "shape_size", 12, {}, False),
+    "cube9c": ("unit_cube", dict(n=9, frac=0.15, seed=31), (5, 5, 5), 0, "barrier", 8, {}, False),
+    "disk17c": ("disk_oh", dict(n=17, frac=0.25, seed=2), (6, 6), 0, "barrier", 8, {}, False),
+}
+
+
+def control_case_grid(name: str, fx) -> "object":
+    """The case's grid as an egg_b200 configs.Grid (wavy grids come from the
+    fixture, which stores the reference-built nodes)."""
+    from egg_b200 import configs
+
+    src, kw, *_ = CONTROL_CASES[name]
+    if src != "wavy":
+        return getattr(configs, src)(**kw)
+    ids = np.asarray(fx[f"{name}/ids"])
+    X = np.asarray(fx[f"{name}/X0"])
+    free = np.zeros(X.shape[0], dtype=bool)
+    free[ids[1:-1, 1:-1].reshape(-1)] = True
+    return configs.Grid(name, 2, [ids], X, free, {})
+
+
+def _control_runs(ref_root: Path) -> dict:
+    sys.path.insert(0, str(ref_root))
+    from egg.geometry.control_net import tensor_map
+    from egg.smoothing.control_backend import build_control_wire
+    from egg.smoothing.control_ref import (boolean_sum_b, boundary_ctrl_mask, build_control_ref,
+                                           fit_control_net, run_control_ref)
+    from egg.smoothing.targets import IdentityTarget
+    from tests.smoothing.test_control_ref import _make_wavy_grid
+
+    from oracle import oracle
+
+    ref = oracle.load_ref("fp64")
+    out = {}
+    for name, (src, kw, ctrl, blk, phase, n_outer, opts, numpy_ref) in CONTROL_CASES.items():
+        if src == "wavy":
+            rg = _make_wavy_grid(**kw)
+            out[f"{name}/X0"] = np.asarray(rg.global_nodes, dtype=float)
+            out[f"{name}/ids"] = np.asarray(rg.block_dof_maps[0], dtype=np.int64)
+        g = control_case_grid(name, out)
+        ids = g.blocks[blk]
+        X0b = g.X[ids.reshape(-1)].reshape(ids.shape + (g.d,))
+        cmap = tensor_map(ids.shape, ctrl, degree=3)
+        C0 = fit_control_net(cmap, X0b)
+        bf = boolean_sum_b(cmap, C0, X0b)
+        wire = build_control_wire(cmap, C0, ~boundary_ctrl_mask(tuple(ctrl)), bf, block=blk)
+        for k, v in wire.items():
+            out[f"{name}/wire/{k}"] = np.asarray(v)
+        s = ref.CppStructuredSweepSession(g.wire(), g.structured(), g.X_flat(), device="cpu", dim=g.d,
+                                          control=wire)
+        rep = s.run_control(n_outer, phase=phase, **opts)
+        for k in ("energies", "mindets", "alphas", "pcg_iters", "pcg_relres"):
+            out[f"{name}/ref/{k}"] = np.asarray(rep[k], dtype=float)
+        out[f"{name}/ref/iters"] = np.int64(rep["iters"])
+        out[f"{name}/ref/converged"] = np.int64(bool(rep["converged"]))
+        out[f"{name}/ref/X"] = np.asarray(s.get_X())
+        out[f"{name}/ref/C"] = np.asarray(s.get_C())
+        print(name, "iters", rep["iters"], "E", rep["energies"][0], "->", rep["energies"][-1])
+        if numpy_ref:
+            rg2 = _make_wavy_grid(**kw)
+            cref = build_control_ref(rg2, IdentityTarget(d=2), ctrl)
+            r2 = run_control_ref(cref, max_outer=n_outer)
+            out[f"{name}/numpy/energies"] = np.asarray(r2["energies"], dtype=float)
+            out[f"{name}/numpy/iters"] = np.int64(r2["iters"])
+            out[f"{name}/numpy/X"] = np.asarray(rg2.global_nodes, dtype=float).reshape(-1)
+            print(name, "numpy iters", r2["iters"], "E", r2["energies"][-1])
+    return out
+
+
+def gen_reference_control(ref_root: Path) -> None:
+    import subprocess
+    import tempfile
+
+    with tempfile.TemporaryDirectory() as td:
+        f = Path(td) / "control.npz"
+        subprocess.run([sys.executable, __file__, "--control", str(ref_root), str(f)], check=True)
+        out = dict(np.load(f))
+    np.savez_compressed(HERE / "ref_control.npz", **out)
+    print(f"ref_control.npz: {len(out)} arrays")
+
+
+if __name__ == "__main__" and len(sys.argv) == 4 and sys.argv[1] == "--control":
+    np.savez(sys.argv[3], **_control_runs(Path(sys.argv[2])))
+    raise SystemExit(0)
+
 if __name__ == "__main__" and len(sys.argv) == 4 and sys.argv[1] == "--runs":
     np.savez(sys.argv[3], **_runs_for(sys.argv[2]))
     raise SystemExit(0)
@@ -216,3 +311,4 @@ if __name__ == "__main__":
     gen_reference_vectors(ref_root)
     gen_reference_runs()
     gen_reference_wire(ref_root)
+    gen_reference_control(ref_root)
