@@ -233,6 +233,30 @@ def run_reference(args):
     return 0
 
 
+def run_workload(args):
+    """One of the other measured configurations (bench_workloads.py), one GPU."""
+    import torch
+
+    import bench_workloads
+    from egg_b200 import cpp_core
+
+    ws, rank, local = _dist()
+    if ws > 1:
+        if rank == 0:
+            print(json.dumps({"workload": args.workload, "unavailable": "the extra workloads run on one GPU"}))
+        return 0
+    fn = bench_workloads.WORKLOADS[args.workload]
+    torch.cuda.set_device(local)
+    with ClockSampler(local) as clk:
+        line = fn(torch, cpp_core, args, local)
+    out = {"metric": METRIC, "unit": UNIT, "n_gpus": 1, "steps": args.steps, "warmup": args.warmup,
+           "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "data": "synthetic"}
+    out.update(line)
+    out["clocks"] = clk.summary()
+    print(json.dumps(out))
+    return 0
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -244,9 +268,13 @@ def main():
     ap.add_argument("--only", choices=["fp64", "mixed"], default=None,
                     help="time one precision only and skip e2e (profiling runs)")
     ap.add_argument("--n", type=int, default=N_SIDE, help="grid side (profiling runs)")
+    ap.add_argument("--workload", default="square4097",
+                    help="square4097 (default), disk_oh65, untangle1025, sphere129_fas, batch256")
     args = ap.parse_args()
     if args.impl == "reference":
         return run_reference(args)
+    if args.workload != "square4097":
+        return run_workload(args)
 
     ws, rank, local = _dist()
     import torch

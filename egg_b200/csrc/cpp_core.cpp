@@ -480,12 +480,12 @@ class Session
 
     py::dict info()
     {
-        int64_t v[10];
-        check(egg_b200_session_info(h_.get(), v, 10));
+        int64_t v[11];
+        check(egg_b200_session_info(h_.get(), v, 11));
         py::dict d;
-        const char* keys[10] = {"dim",    "num_nodes", "store_nodes", "ndof",  "interior_dofs", "stored_dofs",
-                                "copies", "energy_samples", "structured_energy", "precision"};
-        for (int i = 0; i < 10; ++i) { d[keys[i]] = v[i]; }
+        const char* keys[11] = {"dim",    "num_nodes",      "store_nodes",       "ndof",      "interior_dofs", "stored_dofs",
+                                "copies", "energy_samples", "structured_energy", "precision", "updates"};
+        for (int i = 0; i < 11; ++i) { d[keys[i]] = v[i]; }
         d["precision"] = v[9] == EGG_B200_PREC_MIXED ? "mixed" : "fp64";
         return d;
     }

@@ -186,7 +186,7 @@ struct Session : LevelData {
         const void* tiles;
         int variant;
         cudaGraphExec_t exec;
-        int64_t launches;
+        int64_t launches, updates;
     };
     std::vector<ChunkGraph> graphs;
     // control-net reduced Gauss-Newton (attached on request)
@@ -194,6 +194,7 @@ struct Session : LevelData {
     // profiling
     bool profiling = false;
     int64_t launches = 0;  // every kernel launch (copies excluded)
+    int64_t updates = 0;   // vertex Newton updates issued (every DOF relaxed once at any level)
     DevBuf<double> ckpt;   // device-side checkpoint of the store
     bool has_ckpt = false;
     double k_ms[kKCount] = {};
@@ -1128,6 +1129,7 @@ template <int KIND> static void sweep_once(Session& S, double* xin, double* xout
     launch_broadcast(S, S, xin);
     launch_interior<KIND>(S, S, xin, xout, nullptr, delta, omega);
     launch_stored<KIND>(S, S, xin, xout, nullptr, delta, omega);
+    S.updates += S.n_interior + S.n_stored;
 }
 
 static bool graphs_enabled()
@@ -1152,7 +1154,7 @@ static Session::ChunkGraph& chunk_graph(Session& S, int k, bool per_mesh, double
         }
     }
     if (S.graphs.size() >= 16) { S.drop_graphs(); }
-    const int64_t before = S.launches;
+    const int64_t before = S.launches, upd_before = S.updates;
     EGG_CK(cudaStreamBeginCapture(S.stream, cudaStreamCaptureModeThreadLocal));
     cudaGraph_t graph = nullptr;
     try {
@@ -1169,6 +1171,7 @@ static Session::ChunkGraph& chunk_graph(Session& S, int k, bool per_mesh, double
         if (graph) { cudaGraphDestroy(graph); }
         cudaGetLastError();
         S.launches = before;
+        S.updates = upd_before;
         throw;
     }
     EGG_CK(cudaStreamEndCapture(S.stream, &graph));
@@ -1176,9 +1179,10 @@ static Session::ChunkGraph& chunk_graph(Session& S, int k, bool per_mesh, double
     const cudaError_t st = cudaGraphInstantiate(&exec, graph, 0);
     cudaGraphDestroy(graph);
     EGG_CK(st);
-    const int64_t n = S.launches - before;
+    const int64_t n = S.launches - before, nu = S.updates - upd_before;
     S.launches = before;
-    S.graphs.push_back({KIND, k, per_mesh, delta, omega, xin, xout, tiles, S.variant, exec, n});
+    S.updates = upd_before;
+    S.graphs.push_back({KIND, k, per_mesh, delta, omega, xin, xout, tiles, S.variant, exec, n, nu});
     return S.graphs.back();
 }
 
@@ -1209,6 +1213,7 @@ template <int KIND> static void run_impl(Session& S, int n_sweeps, double delta,
             Session::ChunkGraph& g = chunk_graph<KIND>(S, k, per_mesh, delta, omega, xin, xout);
             EGG_CK(cudaGraphLaunch(g.exec, S.stream));
             S.launches += g.launches;
+            S.updates += g.updates;
             EGG_CK(cudaMemcpyAsync(slot, S.red_tmp.p, size_t(2 * width) * sizeof(double), cudaMemcpyDeviceToDevice,
                                    S.stream));
             if (k % 2) {
@@ -1816,9 +1821,9 @@ int egg_b200_session_info(egg_b200_session* s, int64_t* out, int32_t n)
     return guarded([&] {
         if (!s || !out) { invalid("info: NULL argument"); }
         Session& S = *s->impl;
-        const int64_t v[10] = {S.dim,         S.M,      S.nstore, S.n_interior + S.n_stored, S.n_interior, S.n_stored,
-                               S.nshare,      S.es_ns,  S.es_struct ? 1 : 0, S.prec};
-        for (int i = 0; i < n && i < 10; ++i) { out[i] = v[i]; }
+        const int64_t v[11] = {S.dim,    S.M,     S.nstore,           S.n_interior + S.n_stored, S.n_interior, S.n_stored,
+                               S.nshare, S.es_ns, S.es_struct ? 1 : 0, S.prec,                    S.updates};
+        for (int i = 0; i < n && i < 11; ++i) { out[i] = v[i]; }
     });
 }
 
@@ -1941,6 +1946,7 @@ int egg_b200_session_reset_stats(egg_b200_session* s)
         if (!s) { invalid("reset_stats: NULL session"); }
         s->impl->sync();
         s->impl->launches = 0;
+        s->impl->updates = 0;
         for (int k = 0; k < kKCount; ++k) {
             s->impl->k_ms[k] = 0;
             s->impl->k_launch[k] = 0;

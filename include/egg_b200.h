@@ -263,7 +263,8 @@ int egg_b200_session_set_X(egg_b200_session* s, const double* X, int64_t len);
 /* Session facts: [0] dim, [1] global nodes, [2] packed store nodes, [3] moving
  * DOFs, [4] structured-interior DOFs, [5] stored-patch DOFs, [6] owner->copy
  * entries, [7] energy samples, [8] structured energy stencil (0/1),
- * [9] precision. */
+ * [9] precision, [10] vertex Newton updates issued since creation or the
+ * last reset_stats (every DOF relaxed once, at any FAS level). */
 int egg_b200_session_info(egg_b200_session* s, int64_t* out, int32_t n);
 
 /* Per-kernel CUDA-event timing on the session stream (off by default).
