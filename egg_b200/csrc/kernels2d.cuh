@@ -312,6 +312,34 @@ __device__ double2 dof_update_fp64(const double2* __restrict__ P, int PW, int ti
     return pos;
 }
 
+// fp64 metric change of one near-degenerate trial sample, from the staged
+// fp64 positions of its corner qc and neighbours q0, q1; the moving node
+// (role 0 corner, 1 axis-0 neighbour, 2 axis-1 neighbour) is displaced by
+// (dx, dy).  Called from a separate loop after the fp32 pass, so its fp64
+// temporaries do not weigh on the fp32 line search's registers.
+template <int KIND>
+__device__ float dmu2_guard64(double2 qc, double2 q0, double2 q1, int role, double dx, double dy,
+                                           double s0, double s1, double delta, float& dn)
+{
+    double d0, d1;
+    const double m0 = sample_mu_c<KIND, double>(s0 * (q0.x - qc.x), s1 * (q1.x - qc.x), s0 * (q0.y - qc.y),
+                                                s1 * (q1.y - qc.y), delta, d0);
+    if (role == 0) {
+        qc.x += dx;
+        qc.y += dy;
+    } else if (role == 1) {
+        q0.x += dx;
+        q0.y += dy;
+    } else {
+        q1.x += dx;
+        q1.y += dy;
+    }
+    const double m1 = sample_mu_c<KIND, double>(s0 * (q0.x - qc.x), s1 * (q1.x - qc.x), s0 * (q0.y - qc.y),
+                                                s1 * (q1.y - qc.y), delta, d1);
+    dn = d1 > 0.0 ? fmaxf(float(d1), 1e-38f) : (d1 < 0.0 ? fminf(float(d1), -1e-38f) : 0.0f);
+    return float(m1 - m0);
+}
+
 template <int CI, int CJ, int MINB, int KIND, class C>
 __global__ void __launch_bounds__(CI* CJ, MINB)
   interior_tile_kernel(const double2* __restrict__ Xin, double2* __restrict__ Xout,
@@ -458,6 +486,81 @@ __global__ void __launch_bounds__(CI* CJ, MINB)
     C alpha = C(1);
     C ax_acc = C(0), ay_acc = C(0);
     bool accepted = false;
+    if constexpr (std::is_same_v<C, float>) {
+        // fp32: accept on the summed metric changes of the 12 samples the DOF
+        // moves (dmu2, free of the cancellation of e' - e0 where mu ~ 1), with
+        // the fp64 energy tolerance; near-degenerate trial samples are
+        // differenced in fp64.
+        for (int it = 0; it < 10 && !accepted; ++it) {
+            const float dx = alpha * dlt[0], dy = alpha * dlt[1];
+            float dsum = 0.0f;
+            float md = mdconst;
+            unsigned guard = 0u;
+#pragma unroll
+            for (int ci = 0; ci < 2; ++ci) {
+#pragma unroll
+                for (int cj = 0; cj < 2; ++cj) {
+                    const int a = (1 - ci) * 2 + (1 - cj);
+#pragma unroll
+                    for (int r = 0; r < 3; ++r) {
+                        const int b = (r == 0) ? a : ((r == 1) ? (a ^ 2) : (a ^ 1));
+                        const int bn0 = b ^ 2, bn1 = b ^ 1;
+                        const int cu = ci + (b >> 1), cv = cj + (b & 1);
+                        const int u0 = ci + (bn0 >> 1), v0 = cj + (bn0 & 1);
+                        const int u1 = ci + (bn1 >> 1), v1 = cj + (bn1 & 1);
+                        const float s0 = (b & 2) ? -1.0f : 1.0f;
+                        const float s1 = (b & 1) ? -1.0f : 1.0f;
+                        const float t[4] = {s0 * (rx[u0][v0] - rx[cu][cv]), s1 * (rx[u1][v1] - rx[cu][cv]),
+                                            s0 * (ry[u0][v0] - ry[cu][cv]), s1 * (ry[u1][v1] - ry[cu][cv])};
+                        float dt[4] = {0.0f, 0.0f, 0.0f, 0.0f};
+                        if (r == 0) {
+                            dt[0] = -s0 * dx;
+                            dt[1] = -s1 * dx;
+                            dt[2] = -s0 * dy;
+                            dt[3] = -s1 * dy;
+                        } else if (r == 1) {
+                            dt[0] = s0 * dx;
+                            dt[2] = s0 * dy;
+                        } else {
+                            dt[1] = s1 * dx;
+                            dt[3] = s1 * dy;
+                        }
+                        float dn;
+                        const float dm = dmu2<float>(KIND, t, dt, float(delta), dn);
+                        const float ax = t[0] + dt[0], bx = t[1] + dt[1], ay = t[2] + dt[2], by = t[3] + dt[3];
+                        if (dn * dn < float(kGuard * kGuard) * (ax * ax + ay * ay) * (bx * bx + by * by)) {
+                            guard |= 1u << (ci * 6 + cj * 3 + r);  // redone in fp64 below
+                        } else {
+                            dsum += dm;
+                            md = fminf(md, dn);
+                        }
+                    }
+                }
+            }
+#pragma unroll 1
+            for (int k = 0; guard && k < 12; ++k) {
+                if (!((guard >> k) & 1u)) { continue; }
+                const int ci = k / 6, cj = (k / 3) % 2, r = k % 3;
+                const int a = (1 - ci) * 2 + (1 - cj);
+                const int b = (r == 0) ? a : ((r == 1) ? (a ^ 2) : (a ^ 1));
+                const int bn0 = b ^ 2, bn1 = b ^ 1;
+                float dn;
+                dsum += dmu2_guard64<KIND>(sm.P[(ti + ci + (b >> 1)) * PW + (tj + cj + (b & 1))],
+                                           sm.P[(ti + ci + (bn0 >> 1)) * PW + (tj + cj + (bn0 & 1))],
+                                           sm.P[(ti + ci + (bn1 >> 1)) * PW + (tj + cj + (bn1 & 1))], r, double(dx),
+                                           double(dy), (b & 2) ? -1.0 : 1.0, (b & 1) ? -1.0 : 1.0, delta, dn);
+                md = fminf(md, dn);
+            }
+            dsum -= tx * dx + ty * dy;
+            if (isfinite(dsum) && dsum <= float(Tol<double>::energy) && (KIND == kUntangle || md > 0.0f)) {
+                ax_acc = dx;
+                ay_acc = dy;
+                accepted = true;
+            } else {
+                alpha *= 0.5f;
+            }
+        }
+    } else {
     for (int it = 0; it < 10 && !accepted; ++it) {
         const C dx = alpha * dlt[0], dy = alpha * dlt[1];
         C e = econst;
@@ -526,6 +629,7 @@ __global__ void __launch_bounds__(CI* CJ, MINB)
         } else {
             alpha *= C(0.5);
         }
+    }
     }
     double2 out = pos;
     if (accepted) {

@@ -90,6 +90,25 @@ __device__ __forceinline__ void sample3_shared(const double t64[9], double delta
 // working precision R.  Returns false (and leaves `out` untouched) when R is
 // float and the patch holds an inverted or badly shaped sample, so the caller
 // redoes the DOF in fp64.
+// fp64 metric change of one near-degenerate trial sample (cell base
+// (bu, bv, bw), corner b, the DOF at corner a moved from pos by d), from the
+// staged fp64 positions.  Out of line: it runs rarely and its fp64
+// temporaries would otherwise weigh on the fp32 line search's registers.
+template <int TI, int TJ, int TK, int KIND>
+__device__ __noinline__ float dmu3_guard64(const Tile3Shared<TI, TJ, TK>& sm, int bu, int bv, int bw, int b, int a,
+                                           const double pos[3], const double d[3], double delta, float& dn)
+{
+    const double none[3] = {0.0, 0.0, 0.0};
+    const double trial[3] = {pos[0] + d[0], pos[1] + d[1], pos[2] + d[2]};
+    double t0[9], t1[9], d0, d1;
+    edges3<TI, TJ, TK>(sm, bu, bv, bw, b, -1, none, t0);
+    edges3<TI, TJ, TK>(sm, bu, bv, bw, b, a, trial, t1);
+    const double m0 = mu3_value<double>(KIND, t0, delta, d0);
+    const double m1 = mu3_value<double>(KIND, t1, delta, d1);
+    dn = d1 > 0.0 ? fmaxf(float(d1), 1e-38f) : (d1 < 0.0 ? fminf(float(d1), -1e-38f) : 0.0f);
+    return float(m1 - m0);
+}
+
 template <int TI, int TJ, int TK, int KIND, class R>
 __device__ bool dof3_update(const Tile3Shared<TI, TJ, TK>& sm, int ti, int tj, int tk, const double tau[3],
                             double delta, double omega, double out[3], bool grad_only = false)
@@ -162,6 +181,56 @@ __device__ bool dof3_update(const Tile3Shared<TI, TJ, TK>& sm, int ti, int tj, i
     R dl[3];
     solve3<R>(h, gv, dl);
     R alpha = R(1);
+    if constexpr (std::is_same_v<R, float>) {
+        // fp32: accept on the summed metric changes of the 32 samples the DOF
+        // moves (dmu3, free of the cancellation of e' - e0), with the fp64
+        // energy tolerance; near-degenerate trial samples are differenced in
+        // fp64 out of line.
+#pragma unroll 1
+        for (int it = 0; it < 10; ++it) {
+            const float df[3] = {alpha * dl[0], alpha * dl[1], alpha * dl[2]};
+            const double d[3] = {double(df[0]), double(df[1]), double(df[2])};
+            float dsum = 0.0f;
+            float md = mdconst;
+#pragma unroll
+            for (int r = 0; r < 4; ++r) {
+#pragma unroll 1
+                for (int cell = 0; cell < 8; ++cell) {
+                    const int ci = cell >> 2, cj = (cell >> 1) & 1, ck = cell & 1;
+                    const int a = ((1 - ci) << 2) | ((1 - cj) << 1) | (1 - ck);
+                    const int b = r == 0 ? a : (a ^ bit3(r - 1));
+                    double t[9];
+                    edges3<TI, TJ, TK>(sm, ti + ci, tj + cj, tk + ck, b, -1, none, t);
+                    float tt[9], dt[9], tn[9];
+#pragma unroll
+                    for (int i = 0; i < 3; ++i) {
+#pragma unroll
+                        for (int k = 0; k < 3; ++k) {
+                            const float sk = (b & bit3(k)) ? -1.0f : 1.0f;
+                            tt[3 * i + k] = float(t[3 * i + k]);
+                            dt[3 * i + k] = r == 0 ? -sk * df[i] : (k == r - 1 ? sk * df[i] : 0.0f);
+                            tn[3 * i + k] = tt[3 * i + k] + dt[3 * i + k];
+                        }
+                    }
+                    float dn;
+                    float dm = dmu3<float>(KIND, tt, dt, float(delta), dn);
+                    if (!(fabsf(dn) > 0.0f) || below3<float>(tn, fabsf(dn), float(kGuard))) {
+                        dm = dmu3_guard64<TI, TJ, TK, KIND>(sm, ti + ci, tj + cj, tk + ck, b, a, pos, d, delta, dn);
+                    }
+                    dsum += dm;
+                    md = fminf(md, dn);
+                }
+            }
+            dsum -= float(tau[0]) * df[0] + float(tau[1]) * df[1] + float(tau[2]) * df[2];
+            if (isfinite(dsum) && dsum <= float(Tol<double>::energy) && (KIND == kUntangle || md > 0.0f)) {
+                out[0] = pos[0] + omega * d[0];
+                out[1] = pos[1] + omega * d[1];
+                out[2] = pos[2] + omega * d[2];
+                return true;
+            }
+            alpha *= 0.5f;
+        }
+    } else {
 #pragma unroll 1
     for (int it = 0; it < 10; ++it) {
         const double d[3] = {double(alpha * dl[0]), double(alpha * dl[1]), double(alpha * dl[2])};
@@ -203,6 +272,7 @@ __device__ bool dof3_update(const Tile3Shared<TI, TJ, TK>& sm, int ti, int tj, i
             return true;
         }
         alpha *= R(0.5);
+    }
     }
     out[0] = pos[0];
     out[1] = pos[1];

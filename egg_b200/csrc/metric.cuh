@@ -142,6 +142,64 @@ template <class R> EGG_HD void mu_eval(int kind, const R t[4], R delta, R& mu, R
     }
 }
 
+// Change of the metric mu(T + dT) - mu(T), formed without subtracting two
+// metric values, for line searches in working precision: the accept test
+// e' <= e0 + tol is a test on the sum of these changes, which fp32 resolves
+// even where mu itself is ~1 and a step changes it by 1e-12 (the size term
+// of shape_size at small cells).  With s = |T|^2 and D = det T:
+//   ds = 2 T:dT + |dT|^2,   dD = cof(T):dT + det(dT)   (exact, no cancellation)
+//   shape        d(s/2D) = (ds D - s dD) / (2 D D')
+//   shape_size   d(m^2) + d((D-1)^2) = dm (2m + dm) + dD (D' + D - 2)
+//   untangle     D -> Dh = (D + r)/2, r = sqrt(D^2 + 4 delta^2), with Dh and
+//                dDh in forms free of cancellation for either sign of D.
+// Returns the change; dnew = det(T + dT).
+// a / b inside the difference forms: fp32 on the device uses the fast
+// division (about 2 ulp), ample for an accept test on a sum of changes.
+template <class R> EGG_HD R ls_div(R a, R b) { return a / b; }
+#if defined(__CUDACC__)
+template <> __host__ __device__ __forceinline__ float ls_div<float>(float a, float b)
+{
+#if defined(__CUDA_ARCH__)
+    return __fdividef(a, b);
+#else
+    return a / b;
+#endif
+}
+#endif
+
+template <class R> EGG_HD R untangle_dh_stable(R D, R r, R delta)
+{
+    return D >= R(0) ? R(0.5) * (D + r) : ls_div(R(2) * delta * delta, r - D);
+}
+
+template <class R> EGG_HD R untangle_ddh(R D, R Dn, R r, R rn, R dD, R delta)
+{
+    const R q = ls_div(Dn + D, rn + r);
+    return (Dn + D >= R(0)) ? R(0.5) * dD * (R(1) + q) : ls_div(R(2) * delta * delta * dD * (R(1) - q), (rn - Dn) * (r - D));
+}
+
+template <class R> EGG_HD R dmu2(int kind, const R t[4], const R dt[4], R delta, R& dnew)
+{
+    const R s = t[0] * t[0] + t[1] * t[1] + t[2] * t[2] + t[3] * t[3];
+    const R D = t[0] * t[3] - t[1] * t[2];
+    const R ds = R(2) * (t[0] * dt[0] + t[1] * dt[1] + t[2] * dt[2] + t[3] * dt[3]) +
+                 (dt[0] * dt[0] + dt[1] * dt[1] + dt[2] * dt[2] + dt[3] * dt[3]);
+    const R dD = (t[0] * dt[3] + dt[0] * t[3] - t[1] * dt[2] - dt[1] * t[2]) + (dt[0] * dt[3] - dt[1] * dt[2]);
+    const R Dn = D + dD;
+    dnew = Dn;
+    if (kind == kUntangle) {
+        const R d2 = R(4) * delta * delta;
+        const R r = sqrt(D * D + d2), rn = sqrt(Dn * Dn + d2);
+        const R Dh = untangle_dh_stable(D, r, delta), Dhn = untangle_dh_stable(Dn, rn, delta);
+        const R dDh = untangle_ddh(D, Dn, r, rn, dD, delta);
+        return ls_div(ds * Dh - s * dDh, R(2) * Dh * Dhn);
+    }
+    const R dm = ls_div(ds * D - s * dD, R(2) * D * Dn);
+    if (kind == kShape) { return dm; }
+    const R m = ls_div(s, R(2) * D);
+    return dm * (R(2) * m + dm) + dD * (Dn + D - R(2));
+}
+
 // Barrier accept policy: shape-type objectives never cross det A <= 0; the
 // untangle surrogate accepts any finite energy decrease (src/metric.hpp:855,981).
 EGG_HD bool accept_mindet(int kind, double md) { return kind == kUntangle ? true : (md > 0.0); }

@@ -239,6 +239,55 @@ template <class R> EGG_HD void mu3_hvp(int kind, const Shared3<R>& S, const R V[
     }
 }
 
+// Change mu(T + dT) - mu(T) without subtracting metric values (see dmu2 in
+// metric.cuh): with C = cof T, q = |C|^2 and the exact 3x3 expansions
+//   cof(T + dT) = C + N(T, dT) + cof(dT)          (N the mixed cofactor)
+//   det(T + dT) = D + C:dT + T:cof(dT) + det(dT),
+// mu + 1 = s q F(D) / 9 changes by (d(sq) F' + s q dF) / 9 with
+// d(sq) = ds q + s dq + ds dq and dF = F(D') - F(D) in product form.
+template <class R> EGG_HD R dmu3(int kind, const R t[9], const R dt[9], R delta, R& dnew)
+{
+    R C[9], Cd[9];
+    cof3<R>(t, C);
+    cof3<R>(dt, Cd);
+    R s = R(0), ds = R(0), q = R(0), dq = R(0), dD = R(0);
+#pragma unroll
+    for (int i = 0; i < 3; ++i) {
+        const int i1 = (i + 1) % 3, i2 = (i + 2) % 3;
+#pragma unroll
+        for (int j = 0; j < 3; ++j) {
+            const int j1 = (j + 1) % 3, j2 = (j + 2) % 3;
+            const int k = 3 * i + j;
+            const R N = dt[3 * i1 + j1] * t[3 * i2 + j2] + t[3 * i1 + j1] * dt[3 * i2 + j2] -
+                        dt[3 * i1 + j2] * t[3 * i2 + j1] - t[3 * i1 + j2] * dt[3 * i2 + j1];
+            const R dc = N + Cd[k];
+            s += t[k] * t[k];
+            ds += R(2) * t[k] * dt[k] + dt[k] * dt[k];
+            q += C[k] * C[k];
+            dq += R(2) * C[k] * dc + dc * dc;
+            dD += C[k] * dt[k] + t[k] * Cd[k];
+        }
+    }
+    dD += det3<R>(dt);
+    const R D = t[0] * C[0] + t[1] * C[1] + t[2] * C[2];
+    const R Dn = D + dD;
+    dnew = Dn;
+    R x = D, xn = Dn, dx = dD;  // the argument of F = 1/x^2
+    if (kind == kUntangle) {
+        const R d2 = R(4) * delta * delta;
+        const R r = sqrt(D * D + d2), rn = sqrt(Dn * Dn + d2);
+        x = untangle_dh_stable(D, r, delta);
+        xn = untangle_dh_stable(Dn, rn, delta);
+        dx = untangle_ddh(D, Dn, r, rn, dD, delta);
+    }
+    const R F = ls_div(R(1), x * x), Fn = ls_div(R(1), xn * xn);
+    const R dF = -dx * (x + xn) * F * Fn;
+    const R dsq = ds * q + s * dq + ds * dq;
+    R dm = (dsq * Fn + s * q * dF) * R(1.0 / 9.0);
+    if (kind == kShapeSize) { dm += dD * (Dn + D - R(2)); }
+    return dm;
+}
+
 // Newton step -H^{-1} g for a symmetric 3x3 (packed xx, xy, xz, yy, yz, zz)
 // with the reference fallbacks (src/solve.hpp:52-77).
 template <class R> EGG_HD void solve3(const R h[6], const R g[3], R x[3])
