@@ -143,9 +143,10 @@ def disk_oh(n: int = 65, frac: float = 0.25, seed: int = 0, half_width: float = 
 def grid_mindet(blocks, X, d=2) -> np.ndarray:
     """det A of every canonical corner sample (energy-stencil order)."""
     _, gc, gn, sg = _wire.cell_stencil(blocks, d)
-    c0 = sg[0][:, None] * (X[gn[0]] - X[gc])
-    c1 = sg[1][:, None] * (X[gn[1]] - X[gc])
-    return c0[:, 0] * c1[:, 1] - c1[:, 0] * c0[:, 1]
+    cols = [sg[k][:, None] * (X[gn[k]] - X[gc]) for k in range(d)]
+    if d == 2:
+        return cols[0][:, 0] * cols[1][:, 1] - cols[1][:, 0] * cols[0][:, 1]
+    return np.einsum("ij,ij->i", cols[0], np.cross(cols[1], cols[2]))
 
 
 def tangled_square(n: int = 1025, target: float = 0.05, seed: int = 0, batch: int | None = None) -> Grid:

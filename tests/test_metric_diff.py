@@ -1,0 +1,42 @@
+"""The metric difference forms used by the mixed-precision line search
+(dmu2 / dmu3 in egg_b200/csrc/metric*.cuh), compiled for the host: exact to
+fp64 round-off against extended-precision differences, and in fp32 far more
+accurate than subtracting two fp32 metric values, which loses the change
+entirely where mu ~ 1 (the size term at small cells)."""
+
+from __future__ import annotations
+
+import shutil
+import subprocess
+
+import pytest
+
+from tests.conftest import ROOT
+
+KIND = {0: "shape", 1: "untangle", 2: "shape_size"}
+
+
+@pytest.fixture(scope="module")
+def report(tmp_path_factory):
+    gxx = shutil.which("g++")
+    if gxx is None:
+        pytest.skip("no host C++ compiler")
+    exe = tmp_path_factory.mktemp("metric_diff") / "check"
+    subprocess.run([gxx, "-O1", "-std=c++17", f"-I{ROOT / 'egg_b200' / 'csrc'}",
+                    str(ROOT / "tests" / "native" / "metric_diff_check.cpp"), "-o", str(exe)], check=True)
+    out = subprocess.run([str(exe)], check=True, capture_output=True, text=True).stdout
+    rows = {}
+    for line in out.split("\n"):
+        if line.strip():
+            k, d, e64, e32, naive = line.split()
+            rows[(KIND[int(k)], int(d))] = (float(e64), float(e32), float(naive))
+    return rows
+
+
+@pytest.mark.parametrize("kind", list(KIND.values()))
+@pytest.mark.parametrize("dim", [2, 3])
+def test_difference_form_accuracy(report, kind, dim):
+    e64, e32, naive = report[(kind, dim)]
+    assert e64 < 1e-8
+    assert e32 < 0.1
+    assert naive > 10 * e32

@@ -221,3 +221,23 @@ def test_mixed_trajectory_tracks_fp64_reference(gpu, run):
     assert abs(E[-1] - e64) <= tol, (E[-1], e64, e32)
     assert np.abs(s.get_X() - _REF[key64 + "/Xn"]).max() <= 2e-3 * _hmin(g)
     assert np.sign(M[-1]) == np.sign(_REF[key64 + "/M"][-1])
+
+
+def test_mixed_shape_size_on_small_cells_tracks_fp64(gpu):
+    """With the identity target the size term makes mu ~ 1 on small cells and
+    a Newton step changes it by ~1e-12, below what fp32 resolves of mu itself;
+    the mixed line search accepts on exact metric differences and so tracks
+    the fp64 sweep (untangle, then shape+size with the mean-size target)."""
+    g = configs.tangled_square(257, target=0.05, seed=3)
+    w = configs.mean_size_w_inv(g.blocks, g.X)
+    res = {}
+    for prec in ("fp64", "mixed"):
+        a = driver.structured_session(g, compact=True, precision=prec)
+        md, _outer, _delta = driver.untangle(a)
+        assert md > 0
+        b = gpu.CppStructuredSweepSession(g.wire(compact=True, w_inv=w), g.structured(), a.get_X(),
+                                          precision=prec)
+        E, M = b.run(300, phase="shape_size", report_every=100)
+        assert M[-1] > 0
+        res[prec] = E
+    assert abs(res["mixed"][-1] - res["fp64"][-1]) <= 1e-3 * abs(res["fp64"][-1])
