@@ -40,10 +40,10 @@ UNIT = "vertex-updates/s"
 # memory; structure is synthesized, not read).
 BYTES_PER_UPDATE = 2 * 2 * 8
 # DRAM bytes (read + write) per moving-DOF update of the mixed interior
-# kernel, from one ncu capture at 4097^2 (522.9 MB per launch over
+# kernel, from one ncu capture at 4097^2 (523.8 MB per launch over
 # 16,769,025 DOFs; profiles/interior_tile_kernel_square4097.md).  Traffic
 # grows in proportion to the DOFs swept.
-DRAM_BYTES_PER_UPDATE = 522.86e6 / 16769025
+DRAM_BYTES_PER_UPDATE = 523.80e6 / 16769025
 
 
 def _peaks():
@@ -143,6 +143,14 @@ def _max_over_ranks(dist, x, device=None):
     t = torch.tensor([x], dtype=torch.float64, device=device)
     dist.all_reduce(t, op=dist.ReduceOp.MAX)
     return float(t.item())
+
+
+def replica_throughput(dist, updates_per_rank, dt_local, device=None):
+    """Whole-job updates/s of N independent replicas: every rank's updates
+    over the slowest rank's time (max over ranks). Returns (value, dt_max)."""
+    ws = dist.get_world_size() if dist is not None else 1
+    dt = _max_over_ranks(dist, dt_local, device=device)
+    return ws * updates_per_rank / dt, dt
 
 
 def _barrier(dist):
@@ -319,7 +327,7 @@ def main():
         launches = s.launch_count()
         stats = s.kernel_stats()
         s.set_profiling(False)
-        dt = _max_over_ranks(dist, dt, device=f"cuda:{local}")
+        _v, dt = replica_throughput(dist, F * sweeps * args.steps, dt, device=f"cuda:{local}")
         results[prec] = {"dt": dt, "E": float(E[-1]), "M": float(M[-1]), "stats": stats, "launches": launches,
                          "clocks": clk.summary(), "session": s, "variants": s.variants()}
 
@@ -348,8 +356,8 @@ def main():
         s.set_X(Xh)
         _e, _m = s.run(sweeps)
         Xout = s.get_X()
-    e2e_dt = _max_over_ranks(dist, time.perf_counter() - t0, device=f"cuda:{local}")
-    e2e_value = ws * F * sweeps * args.steps / e2e_dt
+    e2e_value, e2e_dt = replica_throughput(dist, F * sweeps * args.steps, time.perf_counter() - t0,
+                                           device=f"cuda:{local}")
 
     # Roofline of the dominant kernel (interior sweep), from the live events.
     k_ms, k_n = mixed["stats"]["interior_sweep"]
@@ -360,7 +368,7 @@ def main():
             "traffic": DRAM_BYTES_PER_UPDATE * F, "traffic_unit": "bytes per launch (ncu dram read+write)",
             "algorithmic_bytes": BYTES_PER_UPDATE * F, "kernel": "interior_tile_kernel (mixed)",
             "avg_launch_ms": avg_ms, "peak_source": peak_kind,
-            "note": "issue/latency-bound stencil (ncu: issue 57%, FMA 27%, XU 20%, DRAM 4%); "
+            "note": "issue/latency-bound stencil (ncu: issue 60%, FMA 33%, XU 16%, DRAM 4%); "
                     "frac states HBM use, not the binding roof"}
     total_ms = sum(v[0] for v in mixed["stats"].values())
     share = {k: v[0] / total_ms for k, v in mixed["stats"].items() if v[1]}
