@@ -384,23 +384,30 @@ __global__ void __launch_bounds__(CI* CJ, MINB)
             sm.det[a][tid] = C(1);
         }
         if (valid) {
+            // The cell's four edges.  Sample b's columns are the axis-0 edge on
+            // side (b & 1) and the axis-1 edge on side (b >> 1): the sample
+            // signs cancel the edge orientation exactly, so T is bitwise the
+            // per-sample s_k (n_k - c).
+            const double2 p00 = sm.P[ci * PW + cj], p01 = sm.P[ci * PW + cj + 1];
+            const double2 p10 = sm.P[(ci + 1) * PW + cj], p11 = sm.P[(ci + 1) * PW + cj + 1];
+            const double e0x[2] = {p10.x - p00.x, p11.x - p01.x}, e0y[2] = {p10.y - p00.y, p11.y - p01.y};
+            const double e1x[2] = {p01.x - p00.x, p11.x - p10.x}, e1y[2] = {p01.y - p00.y, p11.y - p10.y};
 #pragma unroll
             for (int b = 0; b < 4; ++b) {
                 const double s0 = (b & 2) ? -1.0 : 1.0;
                 const double s1 = (b & 1) ? -1.0 : 1.0;
-                const double2 pc = sm.P[(ci + (b >> 1)) * PW + cj + (b & 1)];
-                const double2 pn0 = sm.P[(ci + ((b ^ 2) >> 1)) * PW + cj + (b & 1)];
-                const double2 pn1 = sm.P[(ci + (b >> 1)) * PW + cj + ((b ^ 1) & 1)];
-                const double ax = s0 * (pn0.x - pc.x), bx = s1 * (pn1.x - pc.x);
-                const double ay = s0 * (pn0.y - pc.y), by = s1 * (pn1.y - pc.y);
+                const double ax = e0x[b & 1], bx = e1x[b >> 1];
+                const double ay = e0y[b & 1], by = e1y[b >> 1];
                 if constexpr (std::is_same_v<C, float>) {
-                    const double dd = ax * by - bx * ay;
-                    const double nn = (ax * ax + ay * ay) * (bx * bx + by * by);
-                    bad = bad || dd <= 0.0 || dd * dd < kBadCell * kBadCell * nn;
+                    // the fp32 / fp64 split needs only a coarse shape test
+                    const float fax = float(ax), fbx = float(bx), fay = float(ay), fby = float(by);
+                    const float dd = fax * fby - fbx * fay;
+                    const float nn = (fax * fax + fay * fay) * (fbx * fbx + fby * fby);
+                    bad = bad || !(dd > 0.0f) || dd * dd < float(kBadCell * kBadCell) * nn;
                 }
                 RoleOut<C> o;
                 sample_roles<KIND, C>(ax, bx, ay, by, s0, s1, delta, o);
-                sm.mu[b][tid] = o.mu;
+                if constexpr (std::is_same_v<C, double>) { sm.mu[b][tid] = o.mu; }  // fp32 accepts on differences
                 sm.det[b][tid] = o.det;
 #pragma unroll
                 for (int q = 0; q < 5; ++q) {
@@ -436,8 +443,10 @@ __global__ void __launch_bounds__(CI* CJ, MINB)
             hxx += sm.gh[a][2][cell];
             hxy += sm.gh[a][3][cell];
             hyy += sm.gh[a][4][cell];
-            e0 += (sm.mu[0][cell] + sm.mu[1][cell]) + (sm.mu[2][cell] + sm.mu[3][cell]);
-            econst += sm.mu[a ^ 3][cell];
+            if constexpr (std::is_same_v<C, double>) {  // energies: the fp64 accept test only
+                e0 += (sm.mu[0][cell] + sm.mu[1][cell]) + (sm.mu[2][cell] + sm.mu[3][cell]);
+                econst += sm.mu[a ^ 3][cell];
+            }
             mdconst = fmin(mdconst, sm.det[a ^ 3][cell]);
         }
     }

@@ -183,15 +183,18 @@ __device__ bool dof3_update(const Tile3Shared<TI, TJ, TK>& sm, int ti, int tj, i
     R alpha = R(1);
     if constexpr (std::is_same_v<R, float>) {
         // fp32: accept on the summed metric changes of the 32 samples the DOF
-        // moves (dmu3, free of the cancellation of e' - e0), with the fp64
-        // energy tolerance; near-degenerate trial samples are differenced in
-        // fp64 out of line.
+        // moves, with the fp64 energy tolerance.  The move is rank one along
+        // the line, so each sample reduces to a few coefficients
+        // (line_sample3) and every step length costs a few flops; two step
+        // lengths (alpha, alpha / 2) are tried per pass, in the reference's
+        // order.  Near-degenerate trial samples are differenced in fp64.
+        const float u[3] = {dl[0], dl[1], dl[2]};
 #pragma unroll 1
-        for (int it = 0; it < 10; ++it) {
-            const float df[3] = {alpha * dl[0], alpha * dl[1], alpha * dl[2]};
-            const double d[3] = {double(df[0]), double(df[1]), double(df[2])};
-            float dsum = 0.0f;
-            float md = mdconst;
+        for (int pass = 0; pass < 5; ++pass) {
+            const float al[2] = {alpha, 0.5f * alpha};
+            float dsum0 = 0.0f, dsum1 = 0.0f;
+            float md0 = mdconst, md1 = mdconst;
+            unsigned long long guard = 0ull;  // bit 2 * sample + trial
 #pragma unroll
             for (int r = 0; r < 4; ++r) {
 #pragma unroll 1
@@ -201,34 +204,67 @@ __device__ bool dof3_update(const Tile3Shared<TI, TJ, TK>& sm, int ti, int tj, i
                     const int b = r == 0 ? a : (a ^ bit3(r - 1));
                     double t[9];
                     edges3<TI, TJ, TK>(sm, ti + ci, tj + cj, tk + ck, b, -1, none, t);
-                    float tt[9], dt[9], tn[9];
+                    float tt[9], v[3];
 #pragma unroll
-                    for (int i = 0; i < 3; ++i) {
+                    for (int q = 0; q < 9; ++q) { tt[q] = float(t[q]); }
 #pragma unroll
-                        for (int k = 0; k < 3; ++k) {
-                            const float sk = (b & bit3(k)) ? -1.0f : 1.0f;
-                            tt[3 * i + k] = float(t[3 * i + k]);
-                            dt[3 * i + k] = r == 0 ? -sk * df[i] : (k == r - 1 ? sk * df[i] : 0.0f);
-                            tn[3 * i + k] = tt[3 * i + k] + dt[3 * i + k];
+                    for (int k = 0; k < 3; ++k) {
+                        const float sk = (b & bit3(k)) ? -1.0f : 1.0f;
+                        v[k] = r == 0 ? -sk : (k == r - 1 ? sk : 0.0f);
+                    }
+                    LineSample3<float> L;
+                    line_sample3<float>(tt, u, v, L);
+#pragma unroll
+                    for (int tr = 0; tr < 2; ++tr) {
+                        float dn;
+                        const float dm = dmu3_at<float>(KIND, L, al[tr], float(delta), dn);
+                        float nrm[3];
+                        line_norms3<float>(L, al[tr], nrm);
+                        if (!(fabsf(dn) > 0.0f) ||
+                            dn * dn < float(kGuard * kGuard) * nrm[0] * nrm[1] * nrm[2]) {
+                            guard |= 1ull << (2 * (r * 8 + cell) + tr);
+                        } else if (tr == 0) {
+                            dsum0 += dm;
+                            md0 = fminf(md0, dn);
+                        } else {
+                            dsum1 += dm;
+                            md1 = fminf(md1, dn);
                         }
                     }
-                    float dn;
-                    float dm = dmu3<float>(KIND, tt, dt, float(delta), dn);
-                    if (!(fabsf(dn) > 0.0f) || below3<float>(tn, fabsf(dn), float(kGuard))) {
-                        dm = dmu3_guard64<TI, TJ, TK, KIND>(sm, ti + ci, tj + cj, tk + ck, b, a, pos, d, delta, dn);
-                    }
-                    dsum += dm;
-                    md = fminf(md, dn);
                 }
             }
-            dsum -= float(tau[0]) * df[0] + float(tau[1]) * df[1] + float(tau[2]) * df[2];
-            if (isfinite(dsum) && dsum <= float(Tol<double>::energy) && (KIND == kUntangle || md > 0.0f)) {
-                out[0] = pos[0] + omega * d[0];
-                out[1] = pos[1] + omega * d[1];
-                out[2] = pos[2] + omega * d[2];
-                return true;
+#pragma unroll 1
+            for (int bit = 0; guard != 0ull && bit < 64; ++bit) {
+                if (!((guard >> bit) & 1ull)) { continue; }
+                const int si = bit >> 1, tr = bit & 1;
+                const int r = si >> 3, cell = si & 7;
+                const int ci = cell >> 2, cj = (cell >> 1) & 1, ck = cell & 1;
+                const int a = ((1 - ci) << 2) | ((1 - cj) << 1) | (1 - ck);
+                const int b = r == 0 ? a : (a ^ bit3(r - 1));
+                const double d3[3] = {double(al[tr] * u[0]), double(al[tr] * u[1]), double(al[tr] * u[2])};
+                float dn;
+                const float dm = dmu3_guard64<TI, TJ, TK, KIND>(sm, ti + ci, tj + cj, tk + ck, b, a, pos, d3, delta, dn);
+                if (tr == 0) {
+                    dsum0 += dm;
+                    md0 = fminf(md0, dn);
+                } else {
+                    dsum1 += dm;
+                    md1 = fminf(md1, dn);
+                }
             }
-            alpha *= 0.5f;
+#pragma unroll
+            for (int tr = 0; tr < 2; ++tr) {
+                const float d3[3] = {al[tr] * u[0], al[tr] * u[1], al[tr] * u[2]};
+                const float ds = tr == 0 ? dsum0 : dsum1, mdt = tr == 0 ? md0 : md1;
+                const float dd = ds - (float(tau[0]) * d3[0] + float(tau[1]) * d3[1] + float(tau[2]) * d3[2]);
+                if (isfinite(dd) && dd <= float(Tol<double>::energy) && (KIND == kUntangle || mdt > 0.0f)) {
+                    out[0] = pos[0] + omega * double(d3[0]);
+                    out[1] = pos[1] + omega * double(d3[1]);
+                    out[2] = pos[2] + omega * double(d3[2]);
+                    return true;
+                }
+            }
+            alpha *= 0.25f;
         }
     } else {
 #pragma unroll 1

@@ -288,6 +288,96 @@ template <class R> EGG_HD R dmu3(int kind, const R t[9], const R dt[9], R delta,
     return dm;
 }
 
+// A node move along a line changes T by the rank-one alpha u v^T (u the step
+// direction, v the node's role vector), so along the line
+//   det(T + a u v^T)    = D + a u.(C v)                   (exactly linear)
+//   |T + a u v^T|^2     = s + a 2 u.(T v) + a^2 |u|^2 |v|^2
+//   |cof(T + a u v^T)|^2 = q + a 2 C:N + a^2 |N|^2,  N = N(T, u v^T)
+// (cof of a rank-one matrix vanishes).  LineSample3 holds these coefficients
+// for one sample; dmu3_at gives mu(T + a u v^T) - mu(T) from them.
+template <class R> struct LineSample3 {
+    R D, D1, s, s1, s2, q, q1, q2;
+    R n0[3], n1[3], n2[3];  // column norms^2 of T along the line: n0 + a n1 + a^2 n2
+};
+
+template <class R> EGG_HD void line_sample3(const R t[9], const R u[3], const R v[3], LineSample3<R>& L)
+{
+    R C[9];
+    cof3<R>(t, C);
+    L.D = t[0] * C[0] + t[1] * C[1] + t[2] * C[2];
+    R s = R(0), q = R(0);
+#pragma unroll
+    for (int k = 0; k < 9; ++k) {
+        s += t[k] * t[k];
+        q += C[k] * C[k];
+    }
+    L.s = s;
+    L.q = q;
+    R Tv[3], Cv[3];
+#pragma unroll
+    for (int i = 0; i < 3; ++i) {
+        Tv[i] = t[3 * i] * v[0] + t[3 * i + 1] * v[1] + t[3 * i + 2] * v[2];
+        Cv[i] = C[3 * i] * v[0] + C[3 * i + 1] * v[1] + C[3 * i + 2] * v[2];
+    }
+    const R uu = u[0] * u[0] + u[1] * u[1] + u[2] * u[2];
+    const R vv = v[0] * v[0] + v[1] * v[1] + v[2] * v[2];
+    L.D1 = u[0] * Cv[0] + u[1] * Cv[1] + u[2] * Cv[2];
+    L.s1 = R(2) * (u[0] * Tv[0] + u[1] * Tv[1] + u[2] * Tv[2]);
+    L.s2 = uu * vv;
+    R cn = R(0), nn = R(0);
+#pragma unroll
+    for (int i = 0; i < 3; ++i) {
+        const int i1 = (i + 1) % 3, i2 = (i + 2) % 3;
+#pragma unroll
+        for (int j = 0; j < 3; ++j) {
+            const int j1 = (j + 1) % 3, j2 = (j + 2) % 3;
+            const R N = u[i1] * v[j1] * t[3 * i2 + j2] + t[3 * i1 + j1] * u[i2] * v[j2] -
+                        u[i1] * v[j2] * t[3 * i2 + j1] - t[3 * i1 + j2] * u[i2] * v[j1];
+            cn += C[3 * i + j] * N;
+            nn += N * N;
+        }
+    }
+    L.q1 = R(2) * cn;
+    L.q2 = nn;
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+        const R tk2 = t[k] * t[k] + t[3 + k] * t[3 + k] + t[6 + k] * t[6 + k];
+        const R ut = u[0] * t[k] + u[1] * t[3 + k] + u[2] * t[6 + k];
+        L.n0[k] = tk2;
+        L.n1[k] = R(2) * v[k] * ut;
+        L.n2[k] = v[k] * v[k] * uu;
+    }
+}
+
+// mu(T + a u v^T) - mu(T) (difference form, as dmu3) and the new det.
+template <class R> EGG_HD R dmu3_at(int kind, const LineSample3<R>& L, R a, R delta, R& dnew)
+{
+    const R dD = a * L.D1, ds = a * (L.s1 + a * L.s2), dq = a * (L.q1 + a * L.q2);
+    const R D = L.D, Dn = D + dD;
+    dnew = Dn;
+    R x = D, xn = Dn, dx = dD;
+    if (kind == kUntangle) {
+        const R d2 = R(4) * delta * delta;
+        const R r = sqrt(D * D + d2), rn = sqrt(Dn * Dn + d2);
+        x = untangle_dh_stable(D, r, delta);
+        xn = untangle_dh_stable(Dn, rn, delta);
+        dx = untangle_ddh(D, Dn, r, rn, dD, delta);
+    }
+    const R F = ls_div(R(1), x * x), Fn = ls_div(R(1), xn * xn);
+    const R dF = -dx * (x + xn) * F * Fn;
+    const R dsq = ds * L.q + L.s * dq + ds * dq;
+    R dm = (dsq * Fn + L.s * L.q * dF) * R(1.0 / 9.0);
+    if (kind == kShapeSize) { dm += dD * (Dn + D - R(2)); }
+    return dm;
+}
+
+// Column norms^2 of T + a u v^T (the guard's shape test).
+template <class R> EGG_HD void line_norms3(const LineSample3<R>& L, R a, R n[3])
+{
+#pragma unroll
+    for (int k = 0; k < 3; ++k) { n[k] = L.n0[k] + a * (L.n1[k] + a * L.n2[k]); }
+}
+
 // Newton step -H^{-1} g for a symmetric 3x3 (packed xx, xy, xz, yy, yz, zz)
 // with the reference fallbacks (src/solve.hpp:52-77).
 template <class R> EGG_HD void solve3(const R h[6], const R g[3], R x[3])

@@ -98,8 +98,10 @@ def test_fas_beats_jacobi_at_equal_fine_budget(gpu):
 def test_fas_falls_back_to_jacobi_without_levels(gpu):
     g = case_grid("square33")
     a = _session(gpu, g)
+    a.set_variant(1)  # the same kernel variant on both sides
     Ea, Ma = a.run_fas(3, nu_pre=2, nu_post=2, max_levels=1)
     b = _session(gpu, g)
+    b.set_variant(1)
     Eb, Mb = b.run(12, report_every=4)
     np.testing.assert_array_equal(Ea, Eb)
 
