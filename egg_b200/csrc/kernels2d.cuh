@@ -370,16 +370,18 @@ __global__ void __launch_bounds__(CI* CJ, MINB)
     __syncthreads();
 
     // Phase 2: cell (ci, cj) with base node window (ci, cj); thread = cell.
-    // Each thread owns column `tid` of the shared cell arrays and accumulates
-    // the role contributions of its four samples there (no register array).
+    // Each thread accumulates the role contributions of its cell's four
+    // samples per corner in registers and stores them once to column `tid`
+    // of the shared cell arrays.
     {
         const int ci = tid / CJ, cj = tid % CJ;
         const bool valid = (r0 + ci <= n0 - 2) && (c0 + cj <= n1 - 2);
         bool bad = false;
+        C acc[4][5];  // role contributions per cell corner, stored once below
 #pragma unroll
         for (int a = 0; a < 4; ++a) {
 #pragma unroll
-            for (int q = 0; q < 5; ++q) { sm.gh[a][q][tid] = C(0); }
+            for (int q = 0; q < 5; ++q) { acc[a][q] = C(0); }
             sm.mu[a][tid] = C(0);
             sm.det[a][tid] = C(1);
         }
@@ -411,11 +413,16 @@ __global__ void __launch_bounds__(CI* CJ, MINB)
                 sm.det[b][tid] = o.det;
 #pragma unroll
                 for (int q = 0; q < 5; ++q) {
-                    sm.gh[b][q][tid] += o.r[0][q];
-                    sm.gh[b ^ 2][q][tid] += o.r[1][q];
-                    sm.gh[b ^ 1][q][tid] += o.r[2][q];
+                    acc[b][q] += o.r[0][q];
+                    acc[b ^ 2][q] += o.r[1][q];
+                    acc[b ^ 1][q] += o.r[2][q];
                 }
             }
+        }
+#pragma unroll
+        for (int a = 0; a < 4; ++a) {
+#pragma unroll
+            for (int q = 0; q < 5; ++q) { sm.gh[a][q][tid] = acc[a][q]; }
         }
         sm.bad[tid] = bad ? 1 : 0;
     }
