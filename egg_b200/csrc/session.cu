@@ -134,6 +134,10 @@ struct Session : LevelData {
     int prec = EGG_B200_PREC_FP64;
     int device = 0;
     cudaStream_t stream = nullptr;
+    // side stream + fork/join events: the stored-patch sweep runs beside the
+    // interior tiles (both read the frozen snapshot, write disjoint slots)
+    cudaStream_t side = nullptr;
+    cudaEvent_t fork_ev = nullptr, join_ev = nullptr;
 
     int64_t M = 0;       // global nodes
     std::vector<int32_t> g2s;       // global -> owner slot (-1 if in no block)
@@ -217,6 +221,10 @@ struct Session : LevelData {
             event_pool.push_back(p.second.second);
         }
         for (cudaEvent_t e : event_pool) { cudaEventDestroy(e); }
+        if (side) { cudaStreamSynchronize(side); }
+        if (fork_ev) { cudaEventDestroy(fork_ev); }
+        if (join_ev) { cudaEventDestroy(join_ev); }
+        if (side) { cudaStreamDestroy(side); }
         if (stream) { cudaStreamDestroy(stream); }
     }
 
@@ -781,6 +789,9 @@ static Session* create_session(const egg_b200_session_desc& d)
     }
     EGG_CK(cudaGetDevice(&S->device));
     EGG_CK(cudaStreamCreateWithFlags(&S->stream, cudaStreamNonBlocking));
+    EGG_CK(cudaStreamCreateWithFlags(&S->side, cudaStreamNonBlocking));
+    EGG_CK(cudaEventCreateWithFlags(&S->fork_ev, cudaEventDisableTiming));
+    EGG_CK(cudaEventCreateWithFlags(&S->join_ev, cudaEventDisableTiming));
     configure_kernels(S->prec, S->dim);
 
     // ---- upload -----------------------------------------------------------
@@ -967,23 +978,24 @@ static StoredPatch2 stored_view(LevelData& S)
 
 template <int KIND>
 static void launch_stored(Session& S, LevelData& L, const double* xin, double* xout, const double* tau, double delta,
-                          double omega, double* gout = nullptr)
+                          double omega, double* gout = nullptr, cudaStream_t on = nullptr)
 {
     if (L.n_stored == 0) { return; }
+    const cudaStream_t st = on ? on : S.stream;
     if (S.dim == 3) {
         StoredPatch3 sp {L.n_stored, L.st_slot.p, L.st_off.p, L.st_gc.p,  L.st_gn0.p, L.st_gn1.p,
                          L.st_gn2.p, L.st_s0.p,   L.st_s1.p,  L.st_s2.p, L.st_role.p, L.st_W.p,
                          L.st_wstride, L.st_wt.p, L.st_wtstride};
         const unsigned grid = unsigned((L.n_stored + 127) / 128);
         S.timed(kKStored, [&] {
-            stored3_kernel<KIND><<<grid, 128, 0, S.stream>>>(sp, xin, xout, tau, delta, omega, gout);
+            stored3_kernel<KIND><<<grid, 128, 0, st>>>(sp, xin, xout, tau, delta, omega, gout);
         });
         return;
     }
     const StoredPatch2 sp = stored_view(L);
     const unsigned grid = unsigned((L.n_stored + 127) / 128);
     S.timed(kKStored, [&] {
-        stored_patch_kernel<KIND><<<grid, 128, 0, S.stream>>>(sp, reinterpret_cast<const double2*>(xin),
+        stored_patch_kernel<KIND><<<grid, 128, 0, st>>>(sp, reinterpret_cast<const double2*>(xin),
                                                               reinterpret_cast<double2*>(xout),
                                                               reinterpret_cast<const double2*>(tau), delta, omega,
                                                               reinterpret_cast<double2*>(gout));
@@ -1127,8 +1139,18 @@ template <int KIND> static void launch_report(Session& S, const double* x, doubl
 template <int KIND> static void sweep_once(Session& S, double* xin, double* xout, double delta, double omega)
 {
     launch_broadcast(S, S, xin);
-    launch_interior<KIND>(S, S, xin, xout, nullptr, delta, omega);
-    launch_stored<KIND>(S, S, xin, xout, nullptr, delta, omega);
+    if (S.n_stored > 0 && S.ntiles > 0 && !S.profiling) {
+        // fork: stored-patch DOFs on the side stream, interior tiles here, join
+        EGG_CK(cudaEventRecord(S.fork_ev, S.stream));
+        EGG_CK(cudaStreamWaitEvent(S.side, S.fork_ev, 0));
+        launch_stored<KIND>(S, S, xin, xout, nullptr, delta, omega, nullptr, S.side);
+        EGG_CK(cudaEventRecord(S.join_ev, S.side));
+        launch_interior<KIND>(S, S, xin, xout, nullptr, delta, omega);
+        EGG_CK(cudaStreamWaitEvent(S.stream, S.join_ev, 0));
+    } else {
+        launch_interior<KIND>(S, S, xin, xout, nullptr, delta, omega);
+        launch_stored<KIND>(S, S, xin, xout, nullptr, delta, omega);
+    }
     S.updates += S.n_interior + S.n_stored;
 }
 
