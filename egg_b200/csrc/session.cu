@@ -84,11 +84,11 @@ template <class T> struct DevBuf {
 struct Variant {
     int ci, cj, ck, minb;
 };
-constexpr int kNumVariants = 3;
-constexpr Variant kVar64[kNumVariants] = {{8, 32, 1, 1}, {8, 32, 1, 2}, {8, 16, 1, 4}};
-constexpr Variant kVar32[kNumVariants] = {{8, 32, 1, 2}, {8, 32, 1, 3}, {16, 32, 1, 1}};
-constexpr Variant kVar3_64[kNumVariants] = {{4, 8, 8, 1}, {4, 8, 8, 2}, {2, 8, 16, 2}};
-constexpr Variant kVar3_32[kNumVariants] = {{4, 8, 8, 1}, {4, 8, 8, 2}, {2, 8, 16, 2}};
+constexpr int kNumVariants = EGG_B200_NUM_VARIANTS;
+constexpr Variant kVar64[kNumVariants] = {{8, 32, 1, 2}, {8, 16, 1, 4}, {8, 16, 1, 5}, {8, 16, 1, 6}, {16, 16, 1, 3}};
+constexpr Variant kVar32[kNumVariants] = {{8, 32, 1, 3}, {8, 16, 1, 6}, {8, 16, 1, 8}, {16, 16, 1, 4}, {8, 16, 1, 7}};
+constexpr Variant kVar3_64[kNumVariants] = {{4, 8, 8, 1}, {4, 8, 8, 2}, {2, 8, 16, 2}, {2, 8, 16, 3}, {2, 4, 16, 4}};
+constexpr Variant kVar3_32[kNumVariants] = {{4, 8, 8, 1}, {4, 8, 8, 2}, {2, 8, 16, 2}, {2, 8, 16, 3}, {2, 4, 16, 4}};
 
 enum KernelId {
     kKInterior = 0,
@@ -327,10 +327,14 @@ static void configure_kernels(int prec, int dim)
         set_smem_attr<kVar64[0].ci, kVar64[0].cj, kVar64[0].minb, double>();
         set_smem_attr<kVar64[1].ci, kVar64[1].cj, kVar64[1].minb, double>();
         set_smem_attr<kVar64[2].ci, kVar64[2].cj, kVar64[2].minb, double>();
+        set_smem_attr<kVar64[3].ci, kVar64[3].cj, kVar64[3].minb, double>();
+        set_smem_attr<kVar64[4].ci, kVar64[4].cj, kVar64[4].minb, double>();
     } else {
         set_smem_attr<kVar32[0].ci, kVar32[0].cj, kVar32[0].minb, float>();
         set_smem_attr<kVar32[1].ci, kVar32[1].cj, kVar32[1].minb, float>();
         set_smem_attr<kVar32[2].ci, kVar32[2].cj, kVar32[2].minb, float>();
+        set_smem_attr<kVar32[3].ci, kVar32[3].cj, kVar32[3].minb, float>();
+        set_smem_attr<kVar32[4].ci, kVar32[4].cj, kVar32[4].minb, float>();
     }
 }
 
@@ -880,13 +884,17 @@ static void launch_interior(Session& S, LevelData& L, const double* xin, double*
             switch (S.variant) {
             case 0: EGG_V3(kVar3_64, double, 0); break;
             case 1: EGG_V3(kVar3_64, double, 1); break;
-            default: EGG_V3(kVar3_64, double, 2); break;
+            case 2: EGG_V3(kVar3_64, double, 2); break;
+            case 3: EGG_V3(kVar3_64, double, 3); break;
+            default: EGG_V3(kVar3_64, double, 4); break;
             }
         } else {
             switch (S.variant) {
             case 0: EGG_V3(kVar3_32, float, 0); break;
             case 1: EGG_V3(kVar3_32, float, 1); break;
-            default: EGG_V3(kVar3_32, float, 2); break;
+            case 2: EGG_V3(kVar3_32, float, 2); break;
+            case 3: EGG_V3(kVar3_32, float, 3); break;
+            default: EGG_V3(kVar3_32, float, 4); break;
             }
         }
         return;
@@ -896,13 +904,17 @@ static void launch_interior(Session& S, LevelData& L, const double* xin, double*
         switch (S.variant) {
         case 0: launch_tile<kVar64[0].ci, kVar64[0].cj, kVar64[0].minb, KIND, double>(S, L, xin, xout, tau, delta, omega, gout); break;
         case 1: launch_tile<kVar64[1].ci, kVar64[1].cj, kVar64[1].minb, KIND, double>(S, L, xin, xout, tau, delta, omega, gout); break;
-        default: launch_tile<kVar64[2].ci, kVar64[2].cj, kVar64[2].minb, KIND, double>(S, L, xin, xout, tau, delta, omega, gout); break;
+        case 2: launch_tile<kVar64[2].ci, kVar64[2].cj, kVar64[2].minb, KIND, double>(S, L, xin, xout, tau, delta, omega, gout); break;
+        case 3: launch_tile<kVar64[3].ci, kVar64[3].cj, kVar64[3].minb, KIND, double>(S, L, xin, xout, tau, delta, omega, gout); break;
+        default: launch_tile<kVar64[4].ci, kVar64[4].cj, kVar64[4].minb, KIND, double>(S, L, xin, xout, tau, delta, omega, gout); break;
         }
     } else {
         switch (S.variant) {
         case 0: launch_tile<kVar32[0].ci, kVar32[0].cj, kVar32[0].minb, KIND, float>(S, L, xin, xout, tau, delta, omega, gout); break;
         case 1: launch_tile<kVar32[1].ci, kVar32[1].cj, kVar32[1].minb, KIND, float>(S, L, xin, xout, tau, delta, omega, gout); break;
-        default: launch_tile<kVar32[2].ci, kVar32[2].cj, kVar32[2].minb, KIND, float>(S, L, xin, xout, tau, delta, omega, gout); break;
+        case 2: launch_tile<kVar32[2].ci, kVar32[2].cj, kVar32[2].minb, KIND, float>(S, L, xin, xout, tau, delta, omega, gout); break;
+        case 3: launch_tile<kVar32[3].ci, kVar32[3].cj, kVar32[3].minb, KIND, float>(S, L, xin, xout, tau, delta, omega, gout); break;
+        default: launch_tile<kVar32[4].ci, kVar32[4].cj, kVar32[4].minb, KIND, float>(S, L, xin, xout, tau, delta, omega, gout); break;
         }
     }
 }
