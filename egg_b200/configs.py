@@ -327,3 +327,26 @@ def batch_meshes(n_meshes: int = 256, seed: int = 0, **kw) -> list[Grid]:
     """Independent multi-block meshes for the batched sweep (mesh k uses seed
     seed * 100003 + k)."""
     return [multiblock_mesh(seed * 100003 + k, **kw) for k in range(n_meshes)]
+
+
+def two_squares(n_big: int = 17, n_small: int = 6, frac: float = 0.2, seed: int = 0) -> Grid:
+    """Two separate square blocks in one grid: [0, 4]^2 with n_big^2 nodes and
+    [6, 8] x [0, 2] with n_small^2 nodes (an even count cannot coarsen by 2).
+    Boundary nodes fixed, interior nodes carry seeded +-frac h noise."""
+    rng = np.random.default_rng(seed)
+    Xs, blocks, frees, off = [], [], [], 0
+    for n, x0, side in ((n_big, 0.0, 4.0), (n_small, 6.0, 2.0)):
+        t = np.linspace(0.0, side, n)
+        X = np.stack(np.meshgrid(t, t, indexing="ij"), axis=-1).reshape(-1, 2)
+        X[:, 0] += x0
+        free = np.zeros((n, n), dtype=bool)
+        free[1:-1, 1:-1] = True
+        free = free.reshape(-1)
+        h = side / (n - 1)
+        X[free] += rng.uniform(-frac * h, frac * h, size=(int(free.sum()), 2))
+        Xs.append(X)
+        frees.append(free)
+        blocks.append(off + np.arange(n * n, dtype=np.int64).reshape(n, n))
+        off += n * n
+    return Grid(f"two_squares{n_big}_{n_small}", 2, blocks, np.concatenate(Xs), np.concatenate(frees),
+                {"frac": frac, "seed": seed})

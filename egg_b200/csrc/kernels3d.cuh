@@ -189,8 +189,12 @@ __device__ bool dof3_update(const Tile3Shared<TI, TJ, TK>& sm, int ti, int tj, i
         // lengths (alpha, alpha / 2) are tried per pass, in the reference's
         // order.  Near-degenerate trial samples are differenced in fp64.
         const float u[3] = {dl[0], dl[1], dl[2]};
+        // pass 0 tries alpha = 1 alone (almost every DOF accepts it); later
+        // passes try two step lengths each, 10 in all in the reference's order
+        int tried = 0;
 #pragma unroll 1
-        for (int pass = 0; pass < 5; ++pass) {
+        for (int pass = 0; tried < 10; ++pass) {
+            const int nt = (pass == 0 || tried == 9) ? 1 : 2;
             const float al[2] = {alpha, 0.5f * alpha};
             float dsum0 = 0.0f, dsum1 = 0.0f;
             float md0 = mdconst, md1 = mdconst;
@@ -216,6 +220,7 @@ __device__ bool dof3_update(const Tile3Shared<TI, TJ, TK>& sm, int ti, int tj, i
                     line_sample3<float>(tt, u, v, L);
 #pragma unroll
                     for (int tr = 0; tr < 2; ++tr) {
+                        if (tr >= nt) { break; }
                         float dn;
                         const float dm = dmu3_at<float>(KIND, L, al[tr], float(delta), dn);
                         float nrm[3];
@@ -254,6 +259,7 @@ __device__ bool dof3_update(const Tile3Shared<TI, TJ, TK>& sm, int ti, int tj, i
             }
 #pragma unroll
             for (int tr = 0; tr < 2; ++tr) {
+                if (tr >= nt) { break; }
                 const float d3[3] = {al[tr] * u[0], al[tr] * u[1], al[tr] * u[2]};
                 const float ds = tr == 0 ? dsum0 : dsum1, mdt = tr == 0 ? md0 : md1;
                 const float dd = ds - (float(tau[0]) * d3[0] + float(tau[1]) * d3[1] + float(tau[2]) * d3[2]);
@@ -264,7 +270,8 @@ __device__ bool dof3_update(const Tile3Shared<TI, TJ, TK>& sm, int ti, int tj, i
                     return true;
                 }
             }
-            alpha *= 0.25f;
+            tried += nt;
+            alpha *= nt == 1 ? 0.5f : 0.25f;
         }
     } else {
 #pragma unroll 1

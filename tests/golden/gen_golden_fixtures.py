@@ -96,6 +96,7 @@ CASES = {
     "cube17": ("unit_cube", dict(n=17, frac=0.15, seed=14), None),
     "sphere_in_cube9": ("sphere_in_cube", dict(n=9, frac=0.1, seed=15), None),
     "square33f": ("unit_square", dict(n=33, frac=0.2, seed=22), None),
+    "two_squares": ("two_squares", dict(n_big=17, n_small=6, frac=0.2, seed=23), None),
 }
 RUNS = [
     # (case, phase, delta, omega, n_sweeps)
@@ -114,6 +115,7 @@ FAS_RUNS = [
     ("cube17", "barrier", 3, 2, 2, 32, 1.0, 32),
     ("sphere_in_cube9", "barrier", 3, 2, 2, 16, 0.8, 4),
     ("square33f", "barrier", 40, 2, 2, 32, 1.0, 32),
+    ("two_squares", "barrier", 6, 2, 2, 32, 0.8, 32),
 ]
 RUNS3 = [
     ("cube9", "barrier", 0.0, 1.0, 20),

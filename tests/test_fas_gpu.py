@@ -42,7 +42,9 @@ def test_fas_fp64_matches_reference(gpu, run):
     key = f"fp64/fas/{case}/{phase}/{ml}"
     s = _session(gpu, g)
     E, M = s.run_fas(nc, nu_pre=npre, nu_post=npost, nu_coarse=ncoarse, omega=omega, max_levels=ml, phase=phase)
-    np.testing.assert_allclose(E, _REF[key + "/E"], rtol=1e-8)
+    e_ref = _REF[key + "/E"]
+    # near the minimiser the energy is a sum of round-off: floor at 1e-12 of E0
+    np.testing.assert_allclose(E, e_ref, rtol=1e-8, atol=1e-12 * abs(e_ref[0]))
     np.testing.assert_allclose(M, _REF[key + "/M"], rtol=1e-7, atol=1e-16)
     assert np.abs(s.get_X() - _REF[key + "/X"]).max() <= 1e-8 * _hmin(g)
 

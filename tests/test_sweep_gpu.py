@@ -243,3 +243,30 @@ def test_mixed_shape_size_on_small_cells_tracks_fp64(gpu):
         assert M[-1] > 0
         res[prec] = E
     assert abs(res["mixed"][-1] - res["fp64"][-1]) <= 1e-3 * abs(res["fp64"][-1])
+
+
+def test_singular_owner_override_changes_nothing(gpu):
+    """sing_block / sing_logical pick which block's copy of a fan node the core
+    treats as its owner (the reference's singular-node host choice); the sweep
+    is the same whichever block owns it."""
+    g = case_grid("disk_oh17")
+    st = g.structured()
+    ids0 = g.blocks[0]
+    sb, sl = [], []
+    for gid in (ids0[0, 0], ids0[0, -1], ids0[-1, 0], ids0[-1, -1]):  # valence-3 nodes
+        for b in range(len(g.blocks) - 1, 0, -1):  # the highest block holding the node
+            hit = np.argwhere(g.blocks[b] == gid)
+            if hit.size:
+                sb.append(b)
+                sl.append(hit[0])
+                break
+    assert len(sb) == 4
+    st2 = dict(st, sing_block=np.asarray(sb, dtype=np.int32), sing_logical=np.asarray(sl, dtype=np.int32))
+    a = gpu.CppStructuredSweepSession(g.wire(), st, g.X_flat())
+    b = gpu.CppStructuredSweepSession(g.wire(), st2, g.X_flat())
+    a.set_variant(1)
+    b.set_variant(1)
+    Ea, Ma = a.run(6, report_every=2)
+    Eb, Mb = b.run(6, report_every=2)
+    np.testing.assert_array_equal(a.get_X(), b.get_X())
+    np.testing.assert_allclose(Ea, Eb, rtol=1e-14)
