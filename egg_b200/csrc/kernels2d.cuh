@@ -748,49 +748,124 @@ __device__ void stored_trial(const StoredPatch2& sp, const double2* X, int64_t d
     }
 }
 
+// Warp reductions by xor butterfly: every lane ends with the same value
+// (each step adds a pair in both orders, and fp addition commutes), so the
+// lanes of a warp take identical Newton steps and accept decisions.
+__device__ __forceinline__ double warp_sum(double v)
+{
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) { v += __shfl_xor_sync(0xffffffffu, v, o); }
+    return v;
+}
+
+__device__ __forceinline__ double warp_min(double v)
+{
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) { v = fmin(v, __shfl_xor_sync(0xffffffffu, v, o)); }
+    return v;
+}
+
+// Stored-patch sweep, one warp per DOF: the lanes split the DOF's samples
+// (gradient, contracted Hessian, energy; then each line-search trial) and
+// reduce across the warp, so a ragged patch of 16-64 gathered samples is a
+// few rounds of parallel work instead of one thread's serial loop.
 template <int KIND>
 __global__ void stored_patch_kernel(StoredPatch2 sp, const double2* __restrict__ Xin,
                                     double2* __restrict__ Xout, const double2* __restrict__ tau,
                                     double delta, double omega, double2* __restrict__ grad_out)
 {
-    const int64_t d = blockIdx.x * int64_t(blockDim.x) + threadIdx.x;
-    if (d >= sp.n) { return; }
-    const int32_t slot = sp.slot[d];
-    const double2 pos = Xin[slot];
-    double g[2], h[4], e0, md0;
-    stored_patch_eval<KIND>(sp, Xin, d, delta, g, h, e0, md0);
-    double tx = 0.0, ty = 0.0;
-    if (tau != nullptr) {
-        tx = tau[slot].x;
-        ty = tau[slot].y;
-        g[0] -= tx;
-        g[1] -= ty;
-        e0 -= tx * pos.x + ty * pos.y;
-    }
-    if (grad_out != nullptr) {
-        grad_out[slot] = make_double2(g[0], g[1]);
-        return;
-    }
-    double dl[2];
-    solve2<double>(h, g, dl);
-    double alpha = 1.0;
-    double2 cur = pos;
-    for (int it = 0; it < 10; ++it) {
-        const double2 trial = make_double2(pos.x + alpha * dl[0], pos.y + alpha * dl[1]);
-        double e, md;
-        stored_trial<KIND>(sp, Xin, d, slot, trial, delta, e, md);
-        e -= tx * trial.x + ty * trial.y;
-        if (isfinite(e) && e <= e0 + Tol<double>::energy && (KIND == kUntangle || md > 0.0)) {
-            cur = trial;
-            break;
+    const int lane = threadIdx.x & 31;
+    const int64_t nwarps = (int64_t(gridDim.x) * blockDim.x) >> 5;
+    for (int64_t d = (blockIdx.x * int64_t(blockDim.x) + threadIdx.x) >> 5; d < sp.n; d += nwarps) {
+        const int32_t slot = sp.slot[d];
+        const double2 pos = Xin[slot];
+        const int64_t p0 = sp.off[d], p1 = sp.off[d + 1];
+        double g0 = 0.0, g1 = 0.0, h00 = 0.0, h01 = 0.0, h10 = 0.0, h11 = 0.0, e0 = 0.0;
+        for (int64_t p = p0 + lane; p < p1; p += 32) {
+            const double* w = sp.W + p * sp.w_stride;
+            const double s0 = sp.s0[p], s1 = sp.s1[p];
+            double t[4], detA;
+            assemble_T(Xin[sp.gc[p]], Xin[sp.gn0[p]], Xin[sp.gn1[p]], s0, s1, w, t, detA);
+            const double wt = sp.wt[p * sp.wt_stride];
+            const int role = sp.role[p];
+            double mu, gg[4], H[16];
+            mu_eval<double>(KIND, t, delta, mu, gg, H);
+            e0 += wt * mu;
+            if (role < 0) { continue; }
+            double v[2];
+#pragma unroll
+            for (int c = 0; c < 2; ++c) {
+                v[c] = (role == 0) ? -(s0 * w[c] + s1 * w[2 + c]) : ((role == 1) ? s0 * w[c] : s1 * w[2 + c]);
+            }
+            double gl[2], hl[4];
+#pragma unroll
+            for (int i = 0; i < 2; ++i) {
+                gl[i] = gg[i * 2] * v[0] + gg[i * 2 + 1] * v[1];
+#pragma unroll
+                for (int j = 0; j < 2; ++j) {
+                    double acc = 0.0;
+#pragma unroll
+                    for (int c = 0; c < 2; ++c) {
+#pragma unroll
+                        for (int c2 = 0; c2 < 2; ++c2) { acc += v[c] * H[(i * 2 + c) * 4 + (j * 2 + c2)] * v[c2]; }
+                    }
+                    hl[i * 2 + j] = acc;
+                }
+            }
+            g0 += wt * gl[0];
+            g1 += wt * gl[1];
+            h00 += wt * hl[0];
+            h01 += wt * hl[1];
+            h10 += wt * hl[2];
+            h11 += wt * hl[3];
         }
-        alpha *= 0.5;
+        double g[2] = {warp_sum(g0), warp_sum(g1)};
+        const double h[4] = {warp_sum(h00), warp_sum(h01), warp_sum(h10), warp_sum(h11)};
+        e0 = warp_sum(e0);
+        double tx = 0.0, ty = 0.0;
+        if (tau != nullptr) {
+            tx = tau[slot].x;
+            ty = tau[slot].y;
+            g[0] -= tx;
+            g[1] -= ty;
+            e0 -= tx * pos.x + ty * pos.y;
+        }
+        if (grad_out != nullptr) {
+            if (lane == 0) { grad_out[slot] = make_double2(g[0], g[1]); }
+            continue;
+        }
+        double dl[2];
+        solve2<double>(h, g, dl);
+        double alpha = 1.0;
+        double2 cur = pos;
+        for (int it = 0; it < 10; ++it) {
+            const double2 trial = make_double2(pos.x + alpha * dl[0], pos.y + alpha * dl[1]);
+            double e = 0.0, md = INFINITY;
+            for (int64_t p = p0 + lane; p < p1; p += 32) {
+                const double* w = sp.W + p * sp.w_stride;
+                const int32_t ic = sp.gc[p], i0 = sp.gn0[p], i1 = sp.gn1[p];
+                const double2 c = (ic == slot) ? trial : Xin[ic];
+                const double2 n0 = (i0 == slot) ? trial : Xin[i0];
+                const double2 n1 = (i1 == slot) ? trial : Xin[i1];
+                double t[4], detA;
+                assemble_T(c, n0, n1, double(sp.s0[p]), double(sp.s1[p]), w, t, detA);
+                e += sp.wt[p * sp.wt_stride] * mu_value<double>(KIND, t, delta);
+                md = fmin(md, detA);
+            }
+            e = warp_sum(e) - (tx * trial.x + ty * trial.y);
+            md = warp_min(md);
+            if (isfinite(e) && e <= e0 + Tol<double>::energy && (KIND == kUntangle || md > 0.0)) {
+                cur = trial;
+                break;
+            }
+            alpha *= 0.5;
+        }
+        if (omega != 1.0) {
+            cur.x = pos.x + omega * (cur.x - pos.x);
+            cur.y = pos.y + omega * (cur.y - pos.y);
+        }
+        if (lane == 0) { Xout[slot] = cur; }
     }
-    if (omega != 1.0) {
-        cur.x = pos.x + omega * (cur.x - pos.x);
-        cur.y = pos.y + omega * (cur.y - pos.y);
-    }
-    Xout[slot] = cur;
 }
 
 // ---------------------------------------------------------------------------

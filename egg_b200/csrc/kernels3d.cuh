@@ -428,78 +428,93 @@ __device__ __forceinline__ void assemble_T3(const double* X, int32_t ic, const i
     }
 }
 
+// Stored-patch sweep, 3D, one warp per DOF (see stored_patch_kernel): the
+// lanes split the DOF's samples and reduce across the warp.
 template <int KIND>
 __global__ void stored3_kernel(StoredPatch3 sp, const double* __restrict__ Xin, double* __restrict__ Xout,
                                const double* __restrict__ tau, double delta, double omega, double* __restrict__ grad_out)
 {
-    const int64_t d = blockIdx.x * int64_t(blockDim.x) + threadIdx.x;
-    if (d >= sp.n) { return; }
-    const int32_t slot = sp.slot[d];
-    const double pos[3] = {Xin[3 * int64_t(slot)], Xin[3 * int64_t(slot) + 1], Xin[3 * int64_t(slot) + 2]};
-    double g[3] = {0, 0, 0}, h[6] = {0, 0, 0, 0, 0, 0}, e0 = 0.0;
+    const int lane = threadIdx.x & 31;
+    const int64_t nwarps = (int64_t(gridDim.x) * blockDim.x) >> 5;
     const double none[3] = {0, 0, 0};
-    for (int64_t p = sp.off[d]; p < sp.off[d + 1]; ++p) {
-        const double* w = sp.W + p * sp.w_stride;
-        const double s[3] = {double(sp.s0[p]), double(sp.s1[p]), double(sp.s2[p])};
-        const int32_t in[3] = {sp.gn0[p], sp.gn1[p], sp.gn2[p]};
-        double t[9], detA;
-        assemble_T3(Xin, sp.gc[p], in, s, w, -1, none, t, detA);
-        Shared3<double> S;
-        shared3<double>(KIND, t, delta, S);
-        const double wt = sp.wt[p * sp.wt_stride];
-        e0 += wt * mu3_from<double>(KIND, S);
-        const int role = sp.role[p];
-        if (role < 0) { continue; }
-        double v[3];
-#pragma unroll
-        for (int c = 0; c < 3; ++c) {
-            v[c] = role == 0 ? -(s[0] * w[c] + s[1] * w[3 + c] + s[2] * w[6 + c]) : s[role - 1] * w[3 * (role - 1) + c];
-        }
-        double gg[3], hh[6];
-        role3<double>(KIND, S, v, gg, hh);
-#pragma unroll
-        for (int q = 0; q < 3; ++q) { g[q] += wt * gg[q]; }
-#pragma unroll
-        for (int q = 0; q < 6; ++q) { h[q] += wt * hh[q]; }
-    }
-    double tv[3] = {0, 0, 0};
-    if (tau != nullptr) {
-        for (int q = 0; q < 3; ++q) { tv[q] = tau[3 * int64_t(slot) + q]; }
-        for (int q = 0; q < 3; ++q) {
-            g[q] -= tv[q];
-            e0 -= tv[q] * pos[q];
-        }
-    }
-    if (grad_out != nullptr) {
-        for (int q = 0; q < 3; ++q) { grad_out[3 * int64_t(slot) + q] = g[q]; }
-        return;
-    }
-    double dl[3];
-    solve3<double>(h, g, dl);
-    double alpha = 1.0;
-    double cur[3] = {pos[0], pos[1], pos[2]};
-    for (int it = 0; it < 10; ++it) {
-        const double tr[3] = {pos[0] + alpha * dl[0], pos[1] + alpha * dl[1], pos[2] + alpha * dl[2]};
-        double e = 0.0, md = INFINITY;
-        for (int64_t p = sp.off[d]; p < sp.off[d + 1]; ++p) {
+    for (int64_t d = (blockIdx.x * int64_t(blockDim.x) + threadIdx.x) >> 5; d < sp.n; d += nwarps) {
+        const int32_t slot = sp.slot[d];
+        const double pos[3] = {Xin[3 * int64_t(slot)], Xin[3 * int64_t(slot) + 1], Xin[3 * int64_t(slot) + 2]};
+        const int64_t p0 = sp.off[d], p1 = sp.off[d + 1];
+        double g[3] = {0, 0, 0}, h[6] = {0, 0, 0, 0, 0, 0}, e0 = 0.0;
+        for (int64_t p = p0 + lane; p < p1; p += 32) {
+            const double* w = sp.W + p * sp.w_stride;
             const double s[3] = {double(sp.s0[p]), double(sp.s1[p]), double(sp.s2[p])};
             const int32_t in[3] = {sp.gn0[p], sp.gn1[p], sp.gn2[p]};
             double t[9], detA;
-            assemble_T3(Xin, sp.gc[p], in, s, sp.W + p * sp.w_stride, slot, tr, t, detA);
-            double dd;
-            e += sp.wt[p * sp.wt_stride] * mu3_value<double>(KIND, t, delta, dd);
-            md = fmin(md, detA);
+            assemble_T3(Xin, sp.gc[p], in, s, w, -1, none, t, detA);
+            Shared3<double> S;
+            shared3<double>(KIND, t, delta, S);
+            const double wt = sp.wt[p * sp.wt_stride];
+            e0 += wt * mu3_from<double>(KIND, S);
+            const int role = sp.role[p];
+            if (role < 0) { continue; }
+            double v[3];
+#pragma unroll
+            for (int c = 0; c < 3; ++c) {
+                v[c] = role == 0 ? -(s[0] * w[c] + s[1] * w[3 + c] + s[2] * w[6 + c]) : s[role - 1] * w[3 * (role - 1) + c];
+            }
+            double gg[3], hh[6];
+            role3<double>(KIND, S, v, gg, hh);
+#pragma unroll
+            for (int q = 0; q < 3; ++q) { g[q] += wt * gg[q]; }
+#pragma unroll
+            for (int q = 0; q < 6; ++q) { h[q] += wt * hh[q]; }
         }
-        e -= tv[0] * tr[0] + tv[1] * tr[1] + tv[2] * tr[2];
-        if (isfinite(e) && e <= e0 + Tol<double>::energy && (KIND == kUntangle || md > 0.0)) {
-            cur[0] = tr[0];
-            cur[1] = tr[1];
-            cur[2] = tr[2];
-            break;
+#pragma unroll
+        for (int q = 0; q < 3; ++q) { g[q] = warp_sum(g[q]); }
+#pragma unroll
+        for (int q = 0; q < 6; ++q) { h[q] = warp_sum(h[q]); }
+        e0 = warp_sum(e0);
+        double tv[3] = {0, 0, 0};
+        if (tau != nullptr) {
+            for (int q = 0; q < 3; ++q) { tv[q] = tau[3 * int64_t(slot) + q]; }
+            for (int q = 0; q < 3; ++q) {
+                g[q] -= tv[q];
+                e0 -= tv[q] * pos[q];
+            }
         }
-        alpha *= 0.5;
+        if (grad_out != nullptr) {
+            if (lane == 0) {
+                for (int q = 0; q < 3; ++q) { grad_out[3 * int64_t(slot) + q] = g[q]; }
+            }
+            continue;
+        }
+        double dl[3];
+        solve3<double>(h, g, dl);
+        double alpha = 1.0;
+        double cur[3] = {pos[0], pos[1], pos[2]};
+        for (int it = 0; it < 10; ++it) {
+            const double tr[3] = {pos[0] + alpha * dl[0], pos[1] + alpha * dl[1], pos[2] + alpha * dl[2]};
+            double e = 0.0, md = INFINITY;
+            for (int64_t p = p0 + lane; p < p1; p += 32) {
+                const double s[3] = {double(sp.s0[p]), double(sp.s1[p]), double(sp.s2[p])};
+                const int32_t in[3] = {sp.gn0[p], sp.gn1[p], sp.gn2[p]};
+                double t[9], detA;
+                assemble_T3(Xin, sp.gc[p], in, s, sp.W + p * sp.w_stride, slot, tr, t, detA);
+                double dd;
+                e += sp.wt[p * sp.wt_stride] * mu3_value<double>(KIND, t, delta, dd);
+                md = fmin(md, detA);
+            }
+            e = warp_sum(e) - (tv[0] * tr[0] + tv[1] * tr[1] + tv[2] * tr[2]);
+            md = warp_min(md);
+            if (isfinite(e) && e <= e0 + Tol<double>::energy && (KIND == kUntangle || md > 0.0)) {
+                cur[0] = tr[0];
+                cur[1] = tr[1];
+                cur[2] = tr[2];
+                break;
+            }
+            alpha *= 0.5;
+        }
+        if (lane == 0) {
+            for (int q = 0; q < 3; ++q) { Xout[3 * int64_t(slot) + q] = pos[q] + omega * (cur[q] - pos[q]); }
+        }
     }
-    for (int q = 0; q < 3; ++q) { Xout[3 * int64_t(slot) + q] = pos[q] + omega * (cur[q] - pos[q]); }
 }
 
 // Owner -> non-owner copy refresh, three doubles per node.

@@ -998,14 +998,14 @@ static void launch_stored(Session& S, LevelData& L, const double* xin, double* x
         StoredPatch3 sp {L.n_stored, L.st_slot.p, L.st_off.p, L.st_gc.p,  L.st_gn0.p, L.st_gn1.p,
                          L.st_gn2.p, L.st_s0.p,   L.st_s1.p,  L.st_s2.p, L.st_role.p, L.st_W.p,
                          L.st_wstride, L.st_wt.p, L.st_wtstride};
-        const unsigned grid = unsigned((L.n_stored + 127) / 128);
+        const unsigned grid = unsigned(std::min<int64_t>((L.n_stored + 3) / 4, 148 * 16));  // a warp per DOF
         S.timed(kKStored, [&] {
             stored3_kernel<KIND><<<grid, 128, 0, st>>>(sp, xin, xout, tau, delta, omega, gout);
         });
         return;
     }
     const StoredPatch2 sp = stored_view(L);
-    const unsigned grid = unsigned((L.n_stored + 127) / 128);
+    const unsigned grid = unsigned(std::min<int64_t>((L.n_stored + 3) / 4, 148 * 16));  // a warp per DOF
     S.timed(kKStored, [&] {
         stored_patch_kernel<KIND><<<grid, 128, 0, st>>>(sp, reinterpret_cast<const double2*>(xin),
                                                               reinterpret_cast<double2*>(xout),
@@ -1148,21 +1148,30 @@ template <int KIND> static void launch_report(Session& S, const double* x, doubl
 
 // One block-Jacobi sweep xin -> xout (broadcast of the read buffer, then the
 // interior tiles and the stored-patch DOFs).
+// One relaxation of level L (or its gradient, gout): the interior tiles and
+// the stored-patch DOFs read the same snapshot and write disjoint slots, so
+// the stored-patch kernel forks onto the side stream beside the tiles.
+template <int KIND>
+static void relax_level(Session& S, LevelData& L, const double* xin, double* xout, const double* tau, double delta,
+                        double omega, double* gout = nullptr)
+{
+    if (L.n_stored > 0 && L.ntiles > 0 && !S.profiling) {
+        EGG_CK(cudaEventRecord(S.fork_ev, S.stream));
+        EGG_CK(cudaStreamWaitEvent(S.side, S.fork_ev, 0));
+        launch_stored<KIND>(S, L, xin, xout, tau, delta, omega, gout, S.side);
+        EGG_CK(cudaEventRecord(S.join_ev, S.side));
+        launch_interior<KIND>(S, L, xin, xout, tau, delta, omega, gout);
+        EGG_CK(cudaStreamWaitEvent(S.stream, S.join_ev, 0));
+    } else {
+        launch_interior<KIND>(S, L, xin, xout, tau, delta, omega, gout);
+        launch_stored<KIND>(S, L, xin, xout, tau, delta, omega, gout);
+    }
+}
+
 template <int KIND> static void sweep_once(Session& S, double* xin, double* xout, double delta, double omega)
 {
     launch_broadcast(S, S, xin);
-    if (S.n_stored > 0 && S.ntiles > 0 && !S.profiling) {
-        // fork: stored-patch DOFs on the side stream, interior tiles here, join
-        EGG_CK(cudaEventRecord(S.fork_ev, S.stream));
-        EGG_CK(cudaStreamWaitEvent(S.side, S.fork_ev, 0));
-        launch_stored<KIND>(S, S, xin, xout, nullptr, delta, omega, nullptr, S.side);
-        EGG_CK(cudaEventRecord(S.join_ev, S.side));
-        launch_interior<KIND>(S, S, xin, xout, nullptr, delta, omega);
-        EGG_CK(cudaStreamWaitEvent(S.stream, S.join_ev, 0));
-    } else {
-        launch_interior<KIND>(S, S, xin, xout, nullptr, delta, omega);
-        launch_stored<KIND>(S, S, xin, xout, nullptr, delta, omega);
-    }
+    relax_level<KIND>(S, S, xin, xout, nullptr, delta, omega);
     S.updates += S.n_interior + S.n_stored;
 }
 
