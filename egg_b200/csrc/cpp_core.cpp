@@ -444,14 +444,15 @@ class Session
 
     py::array_t<double> get_X()
     {
-        std::vector<double> X(size_t(M_ * dim_));
+        py::array_t<double> X(py::ssize_t(M_ * dim_));
+        double* out = X.mutable_data();
         int rc;
         {
             py::gil_scoped_release nogil;
-            rc = egg_b200_session_get_X(h_.get(), X.data(), int64_t(X.size()));
+            rc = egg_b200_session_get_X(h_.get(), out, int64_t(M_ * dim_));
         }
         check(rc);
-        return vec(X);
+        return X;
     }
 
     void set_X(const DArr& X)

@@ -21,6 +21,7 @@
 #include <mutex>
 #include <stdexcept>
 #include <string>
+#include <thread>
 #include <vector>
 
 namespace egg_b200
@@ -85,6 +86,8 @@ struct Variant {
     int ci, cj, ck, minb;
 };
 constexpr int kNumVariants = EGG_B200_NUM_VARIANTS;
+// Host threads that copy X between the caller's buffer and pinned staging.
+constexpr int kMaxCopyThreads = 16;
 constexpr Variant kVar64[kNumVariants] = {{8, 32, 1, 2}, {8, 16, 1, 4}, {8, 16, 1, 5}, {8, 16, 1, 6}, {16, 16, 1, 3}};
 constexpr Variant kVar32[kNumVariants] = {{8, 32, 1, 3}, {8, 16, 1, 6}, {8, 16, 1, 8}, {16, 16, 1, 4}, {8, 16, 1, 7}};
 constexpr Variant kVar3_64[kNumVariants] = {{4, 8, 8, 1}, {4, 8, 8, 2}, {2, 8, 16, 2}, {2, 8, 16, 3}, {2, 4, 16, 4}};
@@ -142,7 +145,15 @@ struct Session : LevelData {
     int64_t M = 0;       // global nodes
     std::vector<int32_t> g2s;       // global -> owner slot (-1 if in no block)
     std::vector<int32_t> slot_gid;  // store slot -> global id
-    std::vector<double> X_init;     // initial global X (for nodes in no block)
+    std::vector<int64_t> nb_gid;    // global nodes in no block: get_X returns
+    std::vector<double> nb_val;     // their last value set ([nb_gid.size() * dim])
+    // X transfers in global node order, allocated on first use: pinned host
+    // staging, a device copy in global order, the device remap tables and
+    // one event per host copy slice.
+    double* pin = nullptr;
+    DevBuf<double> Xg;
+    DevBuf<int32_t> g2s_d, slot_gid_d;
+    cudaEvent_t xfer_ev[kMaxCopyThreads] = {};
 
     DevBuf<double> Xbuf[2];
     int cur = 0;  // index of the canonical buffer
@@ -226,6 +237,10 @@ struct Session : LevelData {
         if (join_ev) { cudaEventDestroy(join_ev); }
         if (side) { cudaStreamDestroy(side); }
         if (stream) { cudaStreamDestroy(stream); }
+        for (cudaEvent_t e : xfer_ev) {
+            if (e) { cudaEventDestroy(e); }
+        }
+        if (pin) { cudaFreeHost(pin); }
     }
 
     cudaEvent_t take_event()
@@ -410,7 +425,6 @@ static Session* create_session(const egg_b200_session_desc& d)
     S->dim = D;
     S->prec = d.precision;
     S->M = M;
-    S->X_init.assign(d.X, d.X + M * D);
 
     // Host-side validation and remap come first, so malformed input is
     // rejected (ValueError) before any device is touched.
@@ -473,6 +487,11 @@ static Session* create_session(const egg_b200_session_desc& d)
         const int32_t g = S->slot_gid[bi.off + f];
         owner_block[g] = b;
         S->g2s[g] = int32_t(bi.off + f);
+    }
+    for (int64_t g = 0; g < M; ++g) {
+        if (S->g2s[g] >= 0) { continue; }
+        S->nb_gid.push_back(g);
+        for (int k = 0; k < D; ++k) { S->nb_val.push_back(d.X[g * D + k]); }
     }
     // Halo tables: validated (indices in the padded range); this core reads
     // cross-block neighbours from owner slots and needs no ghost fills.
@@ -1476,6 +1495,87 @@ struct egg_b200_session {
     Session* impl;
 };
 
+// ---------------------------------------------------------------------------
+// X in global node order <-> the packed store
+// ---------------------------------------------------------------------------
+// store slot i <- X[slot_gid[i]]: every copy of a node takes its value.
+template <int D>
+__global__ void gather_global_kernel(const double* __restrict__ Xg, const int32_t* __restrict__ slot_gid, int64_t n,
+                                     double* __restrict__ store)
+{
+    for (int64_t i = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; i < n; i += int64_t(gridDim.x) * blockDim.x) {
+        const int64_t g = slot_gid[i];
+        if constexpr (D == 2) {
+            reinterpret_cast<double2*>(store)[i] = reinterpret_cast<const double2*>(Xg)[g];
+        } else {
+#pragma unroll
+            for (int k = 0; k < D; ++k) { store[i * D + k] = Xg[g * D + k]; }
+        }
+    }
+}
+
+// X[g] <- store[g2s[g]] (the owner slot) for every node in a block; nodes in
+// no block are left for the host to fill.
+template <int D>
+__global__ void scatter_global_kernel(const double* __restrict__ store, const int32_t* __restrict__ g2s, int64_t M,
+                                      double* __restrict__ Xg)
+{
+    for (int64_t g = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; g < M; g += int64_t(gridDim.x) * blockDim.x) {
+        const int64_t s = g2s[g];
+        if (s < 0) { continue; }
+        if constexpr (D == 2) {
+            reinterpret_cast<double2*>(Xg)[g] = reinterpret_cast<const double2*>(store)[s];
+        } else {
+#pragma unroll
+            for (int k = 0; k < D; ++k) { Xg[g * D + k] = store[s * D + k]; }
+        }
+    }
+}
+
+// Host copy threads for a transfer of `bytes`: one per 4 MiB slice, at most
+// the hardware threads and kMaxCopyThreads.
+static int copy_threads(size_t bytes)
+{
+    const size_t hw = std::max(1u, std::thread::hardware_concurrency());
+    const size_t by_size = bytes >> 22;
+    return int(std::max<size_t>(1, std::min({hw, size_t(kMaxCopyThreads), by_size})));
+}
+
+// Runs body(t) for t in [0, T): slice 0 on the calling thread, the others on
+// new threads (inline when a thread cannot be started).  body must not throw.
+template <class F> static void run_slices(int T, F&& body)
+{
+    std::vector<std::thread> th;
+    th.reserve(size_t(std::max(T - 1, 0)));
+    int started = 1;
+    try {
+        for (; started < T; ++started) { th.emplace_back(body, started); }
+    } catch (...) {
+    }
+    for (int t = started; t < T; ++t) { body(t); }
+    body(0);
+    for (auto& x : th) { x.join(); }
+}
+
+// Slice t of T over n doubles.
+static inline size_t slice_begin(size_t n, int t, int T) { return n * size_t(t) / size_t(T); }
+
+static void ensure_xfer(Session& S)
+{
+    const size_t n = size_t(S.M) * S.dim;
+    if (!S.pin && n) {
+        EGG_CK(cudaHostAlloc(reinterpret_cast<void**>(&S.pin), n * sizeof(double), cudaHostAllocDefault));
+    }
+    if (S.Xg.n != n) { S.Xg.alloc(n); }
+    if (S.g2s_d.n != S.g2s.size()) { S.g2s_d.upload(S.g2s); }
+    if (S.slot_gid_d.n != S.slot_gid.size()) { S.slot_gid_d.upload(S.slot_gid); }
+    for (cudaEvent_t& e : S.xfer_ev) {
+        if (!e) { EGG_CK(cudaEventCreateWithFlags(&e, cudaEventDisableTiming)); }
+    }
+}
+
+static int remap_grid(int64_t n) { return int(std::max<int64_t>(1, std::min<int64_t>((n + 255) / 256, 148 * 8))); }
+
 extern "C" {
 
 int egg_b200_abi_version(void) { return EGG_B200_ABI_VERSION; }
@@ -1823,18 +1923,40 @@ int egg_b200_session_get_X(egg_b200_session* s, double* X, int64_t len)
         const int D = S.dim;
         if (len != S.M * D) { invalid("get_X: output length " + std::to_string(len) + " != num_nodes*dim"); }
         EGG_CK(cudaSetDevice(S.device));
-        std::vector<double> store(size_t(S.nstore) * D);
-        if (!store.empty()) {
-            EGG_CK(cudaMemcpyAsync(store.data(), S.X(S.cur), store.size() * sizeof(double), cudaMemcpyDeviceToHost,
-                                   S.stream));
+        ensure_xfer(S);
+        const size_t n = size_t(len);
+        if (S.M) {
+            if (D == 2) {
+                scatter_global_kernel<2><<<remap_grid(S.M), 256, 0, S.stream>>>(S.X(S.cur), S.g2s_d.p, S.M, S.Xg.p);
+            } else {
+                scatter_global_kernel<3><<<remap_grid(S.M), 256, 0, S.stream>>>(S.X(S.cur), S.g2s_d.p, S.M, S.Xg.p);
+            }
+            EGG_CK(cudaGetLastError());
+            ++S.launches;
+        }
+        // D2H slice by slice, each followed by its event; host thread t waits
+        // for slice t only, so the copy-out of early slices overlaps the DMA.
+        const int T = copy_threads(n * sizeof(double));
+        for (int t = 0; t < T; ++t) {
+            const size_t a = slice_begin(n, t, T), b = slice_begin(n, t + 1, T);
+            if (b > a) {
+                EGG_CK(cudaMemcpyAsync(S.pin + a, S.Xg.p + a, (b - a) * sizeof(double), cudaMemcpyDeviceToHost,
+                                       S.stream));
+            }
+            EGG_CK(cudaEventRecord(S.xfer_ev[t], S.stream));
+        }
+        cudaError_t err[kMaxCopyThreads] = {};
+        run_slices(T, [&](int t) {
+            const size_t a = slice_begin(n, t, T), b = slice_begin(n, t + 1, T);
+            err[t] = cudaSetDevice(S.device);
+            if (err[t] == cudaSuccess) { err[t] = cudaEventSynchronize(S.xfer_ev[t]); }
+            if (err[t] == cudaSuccess && b > a) { std::memcpy(X + a, S.pin + a, (b - a) * sizeof(double)); }
+        });
+        for (int t = 0; t < T; ++t) { EGG_CK(err[t]); }
+        for (size_t j = 0; j < S.nb_gid.size(); ++j) {
+            for (int k = 0; k < D; ++k) { X[S.nb_gid[j] * D + k] = S.nb_val[j * D + k]; }
         }
         S.sync();
-        for (int64_t g = 0; g < S.M; ++g) {
-            const int32_t slot = S.g2s[g];
-            for (int k = 0; k < D; ++k) {
-                X[g * D + k] = slot >= 0 ? store[size_t(slot) * D + k] : S.X_init[g * D + k];
-            }
-        }
     });
 }
 
@@ -1846,14 +1968,36 @@ int egg_b200_session_set_X(egg_b200_session* s, const double* X, int64_t len)
         const int D = S.dim;
         if (len != S.M * D) { invalid("set_X: input length != num_nodes*dim"); }
         EGG_CK(cudaSetDevice(S.device));
-        std::vector<double> store(size_t(S.nstore) * D);
-        for (int64_t i = 0; i < S.nstore; ++i) {
-            for (int k = 0; k < D; ++k) { store[i * D + k] = X[int64_t(S.slot_gid[i]) * D + k]; }
+        ensure_xfer(S);
+        const size_t n = size_t(len);
+        // Host thread t stages slice t in pinned memory and queues its H2D, so
+        // the DMA of early slices overlaps the staging of later ones.
+        const int T = copy_threads(n * sizeof(double));
+        cudaError_t err[kMaxCopyThreads] = {};
+        run_slices(T, [&](int t) {
+            const size_t a = slice_begin(n, t, T), b = slice_begin(n, t + 1, T);
+            if (b == a) { return; }
+            std::memcpy(S.pin + a, X + a, (b - a) * sizeof(double));
+            err[t] = cudaSetDevice(S.device);
+            if (err[t] == cudaSuccess) {
+                err[t] = cudaMemcpyAsync(S.Xg.p + a, S.pin + a, (b - a) * sizeof(double), cudaMemcpyHostToDevice,
+                                         S.stream);
+            }
+        });
+        for (int t = 0; t < T; ++t) { EGG_CK(err[t]); }
+        if (S.nstore) {
+            if (D == 2) {
+                gather_global_kernel<2><<<remap_grid(S.nstore), 256, 0, S.stream>>>(S.Xg.p, S.slot_gid_d.p, S.nstore,
+                                                                                 S.X(S.cur));
+            } else {
+                gather_global_kernel<3><<<remap_grid(S.nstore), 256, 0, S.stream>>>(S.Xg.p, S.slot_gid_d.p, S.nstore,
+                                                                                 S.X(S.cur));
+            }
+            EGG_CK(cudaGetLastError());
+            ++S.launches;
         }
-        S.X_init.assign(X, X + len);
-        if (!store.empty()) {
-            EGG_CK(cudaMemcpyAsync(S.X(S.cur), store.data(), store.size() * sizeof(double), cudaMemcpyHostToDevice,
-                                   S.stream));
+        for (size_t j = 0; j < S.nb_gid.size(); ++j) {
+            for (int k = 0; k < D; ++k) { S.nb_val[j * D + k] = X[S.nb_gid[j] * D + k]; }
         }
         S.sync();
     });

@@ -168,6 +168,44 @@ def test_set_get_roundtrip_and_restart(gpu):
     np.testing.assert_array_equal(e_a, e_b)
 
 
+def test_set_get_remap_copies_unblocked_nodes_and_slices(gpu):
+    """get_X/set_X remap between global node order and the packed store on the device.
+
+    Every copy of a node shared by blocks takes the value set, nodes in no block
+    return their last value set and sweeps leave them alone, and grids large
+    enough for several host copy slices round-trip bit for bit (2D and 3D).
+    """
+    g = case_grid("disk_oh17")
+    extra = np.array([0.9, 0.9, -0.9, 0.9, 0.1, -0.95])  # three nodes in no block
+    X = np.concatenate([g.X_flat(), extra])
+    s = gpu.CppStructuredSweepSession(g.wire(), g.structured(), X, precision="fp64")
+    s.set_variant(1)  # the same kernel variant as s2 below
+    np.testing.assert_array_equal(s.get_X(), X)
+    s.run(5)
+    np.testing.assert_array_equal(s.get_X()[-6:], extra)
+    rng = np.random.default_rng(3)
+    Xr = X + 1e-3 * rng.standard_normal(X.shape)
+    s.set_X(Xr)
+    np.testing.assert_array_equal(s.get_X(), Xr)
+    # every copy took the value: the next sweep equals a fresh session's
+    s.set_X(X)
+    e_a, _ = s.run(2, report_every=1)
+    s2 = gpu.CppStructuredSweepSession(g.wire(), g.structured(), X, precision="fp64")
+    s2.set_variant(1)
+    e_b, _ = s2.run(2, report_every=1)
+    np.testing.assert_array_equal(e_a, e_b)
+    np.testing.assert_array_equal(s.get_X(), s2.get_X())
+    for big in (configs.unit_square(1025, seed=4), configs.unit_cube(65, seed=4)):
+        b = gpu.CppStructuredSweepSession(big.wire(), big.structured(), big.X_flat(), dim=big.d, precision="mixed")
+        Xb = big.X_flat() + 1e-4 * rng.standard_normal(big.X_flat().shape)
+        b.set_X(Xb)
+        np.testing.assert_array_equal(b.get_X(), Xb)
+        b.run(1)
+        assert not np.array_equal(b.get_X(), Xb)
+        b.set_X(Xb)
+        np.testing.assert_array_equal(b.get_X(), Xb)
+
+
 def test_untangle_schedule_clears_folds_like_the_oracle(gpu):
     g = configs.tangled_square(33, seed=4)
     s = _session(gpu, g)
