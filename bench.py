@@ -199,6 +199,86 @@ def cpu_baseline(threads=None, target_s=12.0):
             "sample": f"1025x1025 unit square, +-0.3h noise, shape metric, {n} sweeps in {dt:.1f} s"}
 
 
+def _sweeps_to_tol(E, e_star, tol):
+    """Sweeps after which every reported energy stays within tol * |e_star|."""
+    out = np.nonzero(np.abs(np.asarray(E) - e_star) > tol * abs(e_star))[0]
+    if len(out) and out[-1] == len(E) - 1:
+        return None
+    return int(out[-1]) + 2 if len(out) else 1
+
+
+def _timed_run(torch, s, local, k):
+    """Device seconds of s.run(k) from the checkpoint, events on the session stream."""
+    stream = torch.cuda.ExternalStream(s.stream(), device=f"cuda:{local}")
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    s.restore()
+    torch.cuda.synchronize()
+    ev0.record(stream)
+    E, _ = s.run(k)
+    ev1.record(stream)
+    ev1.synchronize()
+    return ev0.elapsed_time(ev1) / 1e3, float(E[-1])
+
+
+def time_to_energy_tol(torch, cpp_core, local, sessions, sweeps, tol=1e-6, cpu=True):
+    """Time until the energy stays within tol (relative) of the fp64 energy
+    after `sweeps` sweeps.
+
+    `sessions` maps precision -> a session whose checkpoint holds the start
+    positions; each is traced with one report per sweep, then run(k) to the
+    first sweep k inside the band is timed on the device.  With cpu=True the
+    same is measured for the reference core (oracle/_ref, all host cores) on
+    a 1025^2 sample of the workload, whose band comes from a GPU fp64 trace of
+    that sample; the energy it reaches at k is reported beside its time.
+    """
+    from egg_b200 import configs
+
+    def measure(ss):
+        ss["fp64"].restore()
+        E64, _ = ss["fp64"].run(sweeps, report_every=1)
+        e_star = float(E64[-1])
+        res = {"e_fp64_final": e_star, "sweeps_to_tol": {}, "seconds": {}}
+        for prec, s in ss.items():
+            if prec == "fp64":
+                E = E64
+            else:
+                s.restore()
+                E, _ = s.run(sweeps, report_every=1)
+            k = _sweeps_to_tol(E, e_star, tol)
+            res["sweeps_to_tol"][prec] = k
+            if k is not None:
+                res["seconds"][prec], _e = _timed_run(torch, s, local, k)
+        return res
+
+    out = {"tol_rel": tol, "sweeps": sweeps,
+           "square4097": measure(sessions)}
+    g = configs.unit_square(1025, frac=FRAC, seed=SEED)
+    small = {}
+    for prec in ("fp64", "mixed"):
+        s = cpp_core.CppStructuredSweepSession(g.wire(compact=True), g.structured(), g.X_flat(),
+                                               device=f"cuda:{local}", precision=prec)
+        s.autotune("barrier", 3)
+        s.checkpoint()
+        small[prec] = s
+    r = measure(small)
+    from oracle import oracle
+
+    ref = oracle.load_ref("fp64") if cpu else None
+    k = r["sweeps_to_tol"].get("fp64")
+    if ref is not None and k is not None:
+        os.environ.setdefault("OMP_NUM_THREADS", str(os.cpu_count()))
+        rs = ref.CppStructuredSweepSession(g.wire(), g.structured(), g.X_flat(), device="cpu")
+        t0 = time.perf_counter()
+        E_ref, _ = rs.run(k)
+        r["seconds"]["reference_cpu"] = time.perf_counter() - t0
+        r["reference_cpu_energy_at_k"] = float(E_ref[-1])
+        r["reference_cpu_within_tol"] = bool(abs(float(E_ref[-1]) - r["e_fp64_final"])
+                                             <= tol * abs(r["e_fp64_final"]))
+        r["reference_cpu_cores"] = os.cpu_count()
+    out["square1025"] = r
+    return out
+
+
 def run_reference(args):
     """--impl reference: the reference's own CPU implementation, all host threads."""
     ws, rank, _ = _dist()
@@ -276,6 +356,8 @@ def main():
     ap.add_argument("--only", choices=["fp64", "mixed"], default=None,
                     help="time one precision only and skip e2e (profiling runs)")
     ap.add_argument("--n", type=int, default=N_SIDE, help="grid side (profiling runs)")
+    ap.add_argument("--variant", type=int, default=None,
+                    help="pin the interior-kernel variant instead of autotuning (profiling runs)")
     ap.add_argument("--workload", default="square4097",
                     help="square4097 (default), disk_oh65, untangle1025, sphere129_fas, batch256")
     args = ap.parse_args()
@@ -292,15 +374,22 @@ def main():
     from egg_b200 import cpp_core
 
     g = _grid(args.n)
+    t_setup = time.perf_counter()
     ctx = g.wire(compact=True)
     st = g.structured()
+    setup = {"wire_s": time.perf_counter() - t_setup}
     X0 = g.X_flat()
     F = g.num_free
     sweeps = args.sweeps
     results = {}
     for prec in ([args.only] if args.only else ["fp64", "mixed"]):
+        t_setup = time.perf_counter()
         s = cpp_core.CppStructuredSweepSession(ctx, st, X0, device=f"cuda:{local}", precision=prec)
-        s.autotune("barrier", 3)
+        setup[f"session_create_{prec}_s"] = time.perf_counter() - t_setup
+        if args.variant is None:
+            s.autotune("barrier", 3)
+        else:
+            s.set_variant(args.variant)
         s.checkpoint()
         for _ in range(args.warmup):
             s.restore()
@@ -359,6 +448,11 @@ def main():
     e2e_value, e2e_dt = replica_throughput(dist, F * sweeps * args.steps, time.perf_counter() - t0,
                                            device=f"cuda:{local}")
 
+    tte = None
+    if ws == 1:
+        tte = time_to_energy_tol(torch, cpp_core, local, {p: results[p]["session"] for p in ("fp64", "mixed")},
+                                 sweeps, cpu=not args.no_cpu_baseline)
+
     # Roofline of the dominant kernel (interior sweep), from the live events.
     k_ms, k_n = mixed["stats"]["interior_sweep"]
     hbm, peak_kind = _peaks()
@@ -396,6 +490,8 @@ def main():
                 "d2h_bytes_per_step": int(Xout.nbytes + 16)},
         "gpu_launches": int(mixed["launches"]),
         "clocks": mixed["clocks"],
+        "time_to_energy_tol": tte,
+        "setup": setup,
     }
     if not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline()

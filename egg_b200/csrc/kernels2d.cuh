@@ -122,11 +122,19 @@ __device__ __forceinline__ void sample_roles_c(C a, C b, C c, C d, C s0, C s1, C
         const int k = i * 4 + j;
         return (k == 3 || k == 12) ? C(1) : ((k == 6 || k == 9) ? C(-1) : C(0));
     };
+    // i, j are constants after inlining: the terms whose factor is an exact
+    // zero (off-diagonal 2f, P(i, j) = 0) are left out rather than multiplied
+    // by 0, which IEEE arithmetic would not let the compiler drop.
     auto H = [&](int i, int j) -> C {
-        const C h2 = (i == j ? C(2) * sf.f : C(0)) + C(2) * sf.fp * (t[i] * cof[j] + cof[i] * t[j]) +
-                     s * sf.fpp * cof[i] * cof[j] + s * sf.fp * P(i, j);
+        const C p = P(i, j);
+        C h2 = C(2) * sf.fp * (t[i] * cof[j] + cof[i] * t[j]);
+        if (i == j) { h2 = C(2) * sf.f + h2; }
+        h2 = h2 + s * sf.fpp * cof[i] * cof[j];
+        if (p != C(0)) { h2 = h2 + s * sf.fp * p; }
         if (KIND != kShapeSize) { return h2; }
-        return C(2) * g2[i] * g2[j] + C(2) * m * h2 + C(2) * cof[i] * cof[j] + C(2) * dm1 * P(i, j);
+        C h = C(2) * g2[i] * g2[j] + C(2) * m * h2 + C(2) * cof[i] * cof[j];
+        if (p != C(0)) { h = h + C(2) * dm1 * p; }
+        return h;
     };
     C g[4];
     if (KIND == kShapeSize) {
@@ -213,10 +221,15 @@ __global__ void broadcast2_kernel(double2* __restrict__ X, const int32_t* __rest
 // ---------------------------------------------------------------------------
 template <int CI, int CJ, class C> struct TileShared2 {
     static constexpr int NC = CI * CJ;
+    // fp32 cell edges, kept for the mixed line search (one slot otherwise)
+    static constexpr int NE = std::is_same_v<C, float> ? NC : 1;
+    // sample values: only the fp64 accept test reads them (one slot otherwise)
+    static constexpr int NM = std::is_same_v<C, double> ? NC : 1;
     double2 P[(CI + 1) * (CJ + 1)];
-    C mu[4][NC];
+    C mu[4][NM];
     C det[4][NC];
     C gh[4][5][NC];  // per local corner a: gx, gy, hxx, hxy, hyy
+    float2 E[4][NE];  // axis-0 edge at column side 0, 1; axis-1 edge at row side 0, 1
     uint8_t bad[NC]; // cell holds an inverted or badly shaped sample
 };
 
@@ -382,7 +395,7 @@ __global__ void __launch_bounds__(CI* CJ, MINB)
         for (int a = 0; a < 4; ++a) {
 #pragma unroll
             for (int q = 0; q < 5; ++q) { acc[a][q] = C(0); }
-            sm.mu[a][tid] = C(0);
+            if constexpr (std::is_same_v<C, double>) { sm.mu[a][tid] = C(0); }
             sm.det[a][tid] = C(1);
         }
         if (valid) {
@@ -394,6 +407,13 @@ __global__ void __launch_bounds__(CI* CJ, MINB)
             const double2 p10 = sm.P[(ci + 1) * PW + cj], p11 = sm.P[(ci + 1) * PW + cj + 1];
             const double e0x[2] = {p10.x - p00.x, p11.x - p01.x}, e0y[2] = {p10.y - p00.y, p11.y - p01.y};
             const double e1x[2] = {p01.x - p00.x, p11.x - p10.x}, e1y[2] = {p01.y - p00.y, p11.y - p10.y};
+            if constexpr (std::is_same_v<C, float>) {
+#pragma unroll
+                for (int k = 0; k < 2; ++k) {
+                    sm.E[k][tid] = make_float2(float(e0x[k]), float(e0y[k]));
+                    sm.E[2 + k][tid] = make_float2(float(e1x[k]), float(e1y[k]));
+                }
+            }
 #pragma unroll
             for (int b = 0; b < 4; ++b) {
                 const double s0 = (b & 2) ? -1.0 : 1.0;
@@ -517,33 +537,41 @@ __global__ void __launch_bounds__(CI* CJ, MINB)
 #pragma unroll
                 for (int cj = 0; cj < 2; ++cj) {
                     const int a = (1 - ci) * 2 + (1 - cj);
+                    const int cell = (ti + ci) * CJ + (tj + cj);
 #pragma unroll
                     for (int r = 0; r < 3; ++r) {
                         const int b = (r == 0) ? a : ((r == 1) ? (a ^ 2) : (a ^ 1));
-                        const int bn0 = b ^ 2, bn1 = b ^ 1;
-                        const int cu = ci + (b >> 1), cv = cj + (b & 1);
-                        const int u0 = ci + (bn0 >> 1), v0 = cj + (bn0 & 1);
-                        const int u1 = ci + (bn1 >> 1), v1 = cj + (bn1 & 1);
                         const float s0 = (b & 2) ? -1.0f : 1.0f;
                         const float s1 = (b & 1) ? -1.0f : 1.0f;
-                        const float t[4] = {s0 * (rx[u0][v0] - rx[cu][cv]), s1 * (rx[u1][v1] - rx[cu][cv]),
-                                            s0 * (ry[u0][v0] - ry[cu][cv]), s1 * (ry[u1][v1] - ry[cu][cv])};
-                        float dt[4] = {0.0f, 0.0f, 0.0f, 0.0f};
+                        // T of sample b: the cell's fp32 edges from phase 2
+                        // (each rounded once from its fp64 difference)
+                        const float2 ea = sm.E[b & 1][cell], eb = sm.E[2 + (b >> 1)][cell];
+                        const float t[4] = {ea.x, eb.x, ea.y, eb.y};
+                        // r = 0 moves both columns of T; r = 1 (2) moves column
+                        // 0 (1) only, whose change forms skip the zero entries.
+                        float dn, dm, ax, bx, ay, by;
                         if (r == 0) {
-                            dt[0] = -s0 * dx;
-                            dt[1] = -s1 * dx;
-                            dt[2] = -s0 * dy;
-                            dt[3] = -s1 * dy;
+                            const float dt[4] = {-s0 * dx, -s1 * dx, -s0 * dy, -s1 * dy};
+                            dm = dmu2<float>(KIND, t, dt, float(delta), dn);
+                            ax = t[0] + dt[0];
+                            bx = t[1] + dt[1];
+                            ay = t[2] + dt[2];
+                            by = t[3] + dt[3];
                         } else if (r == 1) {
-                            dt[0] = s0 * dx;
-                            dt[2] = s0 * dy;
+                            const float ex = s0 * dx, ey = s0 * dy;
+                            dm = dmu2_col<float, 0>(KIND, t, ex, ey, float(delta), dn);
+                            ax = t[0] + ex;
+                            bx = t[1];
+                            ay = t[2] + ey;
+                            by = t[3];
                         } else {
-                            dt[1] = s1 * dx;
-                            dt[3] = s1 * dy;
+                            const float ex = s1 * dx, ey = s1 * dy;
+                            dm = dmu2_col<float, 1>(KIND, t, ex, ey, float(delta), dn);
+                            ax = t[0];
+                            bx = t[1] + ex;
+                            ay = t[2];
+                            by = t[3] + ey;
                         }
-                        float dn;
-                        const float dm = dmu2<float>(KIND, t, dt, float(delta), dn);
-                        const float ax = t[0] + dt[0], bx = t[1] + dt[1], ay = t[2] + dt[2], by = t[3] + dt[3];
                         if (dn * dn < float(kGuard * kGuard) * (ax * ax + ay * ay) * (bx * bx + by * by)) {
                             guard |= 1u << (ci * 6 + cj * 3 + r);  // redone in fp64 below
                         } else {
@@ -748,40 +776,62 @@ __device__ void stored_trial(const StoredPatch2& sp, const double2* X, int64_t d
     }
 }
 
-// Warp reductions by xor butterfly: every lane ends with the same value
-// (each step adds a pair in both orders, and fp addition commutes), so the
-// lanes of a warp take identical Newton steps and accept decisions.
-__device__ __forceinline__ double warp_sum(double v)
+// Reductions over an aligned group of G lanes (G a power of two <= 32) by
+// xor butterfly: every lane of the group ends with the same value (each step
+// adds a pair in both orders, and fp addition commutes), so the lanes of a
+// group take identical Newton steps and accept decisions.
+template <int G> __device__ __forceinline__ unsigned group_mask()
+{
+    if constexpr (G == 32) {
+        return 0xffffffffu;
+    } else {
+        return ((1u << G) - 1u) << ((threadIdx.x & 31u) & ~unsigned(G - 1));
+    }
+}
+
+template <int G> __device__ __forceinline__ double group_sum(double v)
 {
 #pragma unroll
-    for (int o = 16; o > 0; o >>= 1) { v += __shfl_xor_sync(0xffffffffu, v, o); }
+    for (int o = G / 2; o > 0; o >>= 1) { v += __shfl_xor_sync(group_mask<G>(), v, o, G); }
     return v;
 }
 
-__device__ __forceinline__ double warp_min(double v)
+template <int G> __device__ __forceinline__ double group_min(double v)
 {
 #pragma unroll
-    for (int o = 16; o > 0; o >>= 1) { v = fmin(v, __shfl_xor_sync(0xffffffffu, v, o)); }
+    for (int o = G / 2; o > 0; o >>= 1) { v = fmin(v, __shfl_xor_sync(group_mask<G>(), v, o, G)); }
     return v;
 }
 
-// Stored-patch sweep, one warp per DOF: the lanes split the DOF's samples
+// Lanes per DOF of the stored-patch sweeps: the widest group (32, 8, 2 or 1)
+// whose threads over all stored DOFs stay within a budget.  Few stored DOFs
+// (a small multi-block mesh) get a warp each, so the patch is a few rounds of
+// parallel work; many (a batch of meshes) get narrow groups, which spend
+// fewer issue slots on per-lane redundancy (the solve, the reductions) while
+// the interior tiles run beside them.  A 3D patch has 64 samples to split,
+// so its budget is larger.  Measured on B200: 256 meshes with 139 k stored
+// DOFs run best at 2 lanes (a warp each: -15%); the 7-block 129^3 sphere's
+// FAS levels best at 8 lanes on the fine level.
+constexpr int64_t kStoredFillThreads2 = 148 * 4096;
+constexpr int64_t kStoredFillThreads3 = 148 * 16384;
+
+// Stored-patch sweep, G lanes per DOF: the lanes split the DOF's samples
 // (gradient, contracted Hessian, energy; then each line-search trial) and
-// reduce across the warp, so a ragged patch of 16-64 gathered samples is a
-// few rounds of parallel work instead of one thread's serial loop.
-template <int KIND>
+// reduce across the group, so a ragged patch of 16-64 gathered samples can be
+// a few rounds of parallel work instead of one thread's serial loop.
+template <int KIND, int G>
 __global__ void stored_patch_kernel(StoredPatch2 sp, const double2* __restrict__ Xin,
                                     double2* __restrict__ Xout, const double2* __restrict__ tau,
                                     double delta, double omega, double2* __restrict__ grad_out)
 {
-    const int lane = threadIdx.x & 31;
-    const int64_t nwarps = (int64_t(gridDim.x) * blockDim.x) >> 5;
-    for (int64_t d = (blockIdx.x * int64_t(blockDim.x) + threadIdx.x) >> 5; d < sp.n; d += nwarps) {
+    const int lane = threadIdx.x & (G - 1);
+    const int64_t ngroups = (int64_t(gridDim.x) * blockDim.x) / G;
+    for (int64_t d = (blockIdx.x * int64_t(blockDim.x) + threadIdx.x) / G; d < sp.n; d += ngroups) {
         const int32_t slot = sp.slot[d];
         const double2 pos = Xin[slot];
         const int64_t p0 = sp.off[d], p1 = sp.off[d + 1];
         double g0 = 0.0, g1 = 0.0, h00 = 0.0, h01 = 0.0, h10 = 0.0, h11 = 0.0, e0 = 0.0;
-        for (int64_t p = p0 + lane; p < p1; p += 32) {
+        for (int64_t p = p0 + lane; p < p1; p += G) {
             const double* w = sp.W + p * sp.w_stride;
             const double s0 = sp.s0[p], s1 = sp.s1[p];
             double t[4], detA;
@@ -819,9 +869,9 @@ __global__ void stored_patch_kernel(StoredPatch2 sp, const double2* __restrict__
             h10 += wt * hl[2];
             h11 += wt * hl[3];
         }
-        double g[2] = {warp_sum(g0), warp_sum(g1)};
-        const double h[4] = {warp_sum(h00), warp_sum(h01), warp_sum(h10), warp_sum(h11)};
-        e0 = warp_sum(e0);
+        double g[2] = {group_sum<G>(g0), group_sum<G>(g1)};
+        const double h[4] = {group_sum<G>(h00), group_sum<G>(h01), group_sum<G>(h10), group_sum<G>(h11)};
+        e0 = group_sum<G>(e0);
         double tx = 0.0, ty = 0.0;
         if (tau != nullptr) {
             tx = tau[slot].x;
@@ -841,7 +891,7 @@ __global__ void stored_patch_kernel(StoredPatch2 sp, const double2* __restrict__
         for (int it = 0; it < 10; ++it) {
             const double2 trial = make_double2(pos.x + alpha * dl[0], pos.y + alpha * dl[1]);
             double e = 0.0, md = INFINITY;
-            for (int64_t p = p0 + lane; p < p1; p += 32) {
+            for (int64_t p = p0 + lane; p < p1; p += G) {
                 const double* w = sp.W + p * sp.w_stride;
                 const int32_t ic = sp.gc[p], i0 = sp.gn0[p], i1 = sp.gn1[p];
                 const double2 c = (ic == slot) ? trial : Xin[ic];
@@ -852,8 +902,8 @@ __global__ void stored_patch_kernel(StoredPatch2 sp, const double2* __restrict__
                 e += sp.wt[p * sp.wt_stride] * mu_value<double>(KIND, t, delta);
                 md = fmin(md, detA);
             }
-            e = warp_sum(e) - (tx * trial.x + ty * trial.y);
-            md = warp_min(md);
+            e = group_sum<G>(e) - (tx * trial.x + ty * trial.y);
+            md = group_min<G>(md);
             if (isfinite(e) && e <= e0 + Tol<double>::energy && (KIND == kUntangle || md > 0.0)) {
                 cur = trial;
                 break;

@@ -69,6 +69,24 @@ __device__ __forceinline__ void edges3(const Tile3Shared<TI, TJ, TK>& sm, int bu
     }
 }
 
+// fp32 edge matrix of sample b from the window's fp32 forward edges
+// fe[(3k + i) * N + node] = (X[node + e_k] - X[node])_i.  Column k of T is
+// the forward edge along k at the corner with bit k cleared, so this is
+// bitwise the fp32 rounding of edges3's fp64 column: the cache saves each
+// sample 12 fp64 loads, 9 subtractions and 9 conversions.
+template <int TI, int TJ, int TK>
+__device__ __forceinline__ void edges3f(const float* __restrict__ fe, int bu, int bv, int bw, int b, float t[9])
+{
+    using W = Win3<TI, TJ, TK>;
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+        const int c = b & ~bit3(k);
+        const int id = W::idx(bu + (c >> 2), bv + ((c >> 1) & 1), bw + (c & 1));
+#pragma unroll
+        for (int i = 0; i < 3; ++i) { t[3 * i + k] = fe[(3 * k + i) * W::N + id]; }
+    }
+}
+
 template <class R> __device__ __forceinline__ bool below3(const R t[9], R det, R thr)
 {
     R n[3];
@@ -110,7 +128,8 @@ __device__ __noinline__ float dmu3_guard64(const Tile3Shared<TI, TJ, TK>& sm, in
 }
 
 template <int TI, int TJ, int TK, int KIND, class R>
-__device__ bool dof3_update(const Tile3Shared<TI, TJ, TK>& sm, int ti, int tj, int tk, const double tau[3],
+__device__ bool dof3_update(const Tile3Shared<TI, TJ, TK>& sm, const float* __restrict__ fe, int ti, int tj, int tk,
+                            const double tau[3],
                             double delta, double omega, double out[3], bool grad_only = false)
 {
     using W = Win3<TI, TJ, TK>;
@@ -129,10 +148,16 @@ __device__ bool dof3_update(const Tile3Shared<TI, TJ, TK>& sm, int ti, int tj, i
 #pragma unroll
         for (int x = 0; x < 4; ++x) {
             const int b = a ^ (x == 0 ? 7 : (x == 1 ? 6 : (x == 2 ? 5 : 3)));
-            double t[9];
-            edges3<TI, TJ, TK>(sm, ti + ci, tj + cj, tk + ck, b, -1, none, t);
             Shared3<R> S;
-            sample3_shared<KIND, R>(t, delta, S);
+            if constexpr (std::is_same_v<R, float>) {
+                float tf[9];
+                edges3f<TI, TJ, TK>(fe, ti + ci, tj + cj, tk + ck, b, tf);
+                shared3<float>(KIND, tf, float(delta), S);
+            } else {
+                double t[9];
+                edges3<TI, TJ, TK>(sm, ti + ci, tj + cj, tk + ck, b, -1, none, t);
+                sample3_shared<KIND, R>(t, delta, S);
+            }
             if constexpr (std::is_same_v<R, float>) {
                 if (below3<float>(S.t, S.D, float(kBadCell))) { return false; }
             }
@@ -148,10 +173,16 @@ __device__ bool dof3_update(const Tile3Shared<TI, TJ, TK>& sm, int ti, int tj, i
             const int ci = cell >> 2, cj = (cell >> 1) & 1, ck = cell & 1;
             const int a = ((1 - ci) << 2) | ((1 - cj) << 1) | (1 - ck);
             const int b = r == 0 ? a : (a ^ bit3(r - 1));
-            double t[9];
-            edges3<TI, TJ, TK>(sm, ti + ci, tj + cj, tk + ck, b, -1, none, t);
             Shared3<R> S;
-            sample3_shared<KIND, R>(t, delta, S);
+            if constexpr (std::is_same_v<R, float>) {
+                float tf[9];
+                edges3f<TI, TJ, TK>(fe, ti + ci, tj + cj, tk + ck, b, tf);
+                shared3<float>(KIND, tf, float(delta), S);
+            } else {
+                double t[9];
+                edges3<TI, TJ, TK>(sm, ti + ci, tj + cj, tk + ck, b, -1, none, t);
+                sample3_shared<KIND, R>(t, delta, S);
+            }
             if constexpr (std::is_same_v<R, float>) {
                 if (below3<float>(S.t, S.D, float(kBadCell))) { return false; }
             }
@@ -163,7 +194,7 @@ __device__ bool dof3_update(const Tile3Shared<TI, TJ, TK>& sm, int ti, int tj, i
                 v[k] = r == 0 ? -sk : (k == r - 1 ? sk : R(0));
             }
             R gg[3], hh[6];
-            role3<R>(KIND, S, v, gg, hh);
+            role3<R>(KIND, S, v, gg, hh, r - 1);  // r >= 1: v = sk e_(r-1)
 #pragma unroll
             for (int q = 0; q < 3; ++q) { g[q] += gg[q]; }
 #pragma unroll
@@ -206,25 +237,22 @@ __device__ bool dof3_update(const Tile3Shared<TI, TJ, TK>& sm, int ti, int tj, i
                     const int ci = cell >> 2, cj = (cell >> 1) & 1, ck = cell & 1;
                     const int a = ((1 - ci) << 2) | ((1 - cj) << 1) | (1 - ck);
                     const int b = r == 0 ? a : (a ^ bit3(r - 1));
-                    double t[9];
-                    edges3<TI, TJ, TK>(sm, ti + ci, tj + cj, tk + ck, b, -1, none, t);
                     float tt[9], v[3];
-#pragma unroll
-                    for (int q = 0; q < 9; ++q) { tt[q] = float(t[q]); }
+                    edges3f<TI, TJ, TK>(fe, ti + ci, tj + cj, tk + ck, b, tt);
 #pragma unroll
                     for (int k = 0; k < 3; ++k) {
                         const float sk = (b & bit3(k)) ? -1.0f : 1.0f;
                         v[k] = r == 0 ? -sk : (k == r - 1 ? sk : 0.0f);
                     }
                     LineSample3<float> L;
-                    line_sample3<float>(tt, u, v, L);
+                    line_sample3<float>(tt, u, v, L, r - 1);
 #pragma unroll
                     for (int tr = 0; tr < 2; ++tr) {
                         if (tr >= nt) { break; }
                         float dn;
                         const float dm = dmu3_at<float>(KIND, L, al[tr], float(delta), dn);
                         float nrm[3];
-                        line_norms3<float>(L, al[tr], nrm);
+                        line_norms3<float>(L, al[tr], nrm, r - 1);
                         if (!(fabsf(dn) > 0.0f) ||
                             dn * dn < float(kGuard * kGuard) * nrm[0] * nrm[1] * nrm[2]) {
                             guard |= 1ull << (2 * (r * 8 + cell) + tr);
@@ -331,6 +359,7 @@ __global__ void __launch_bounds__(TI* TJ* TK, MINB)
 {
     using W = Win3<TI, TJ, TK>;
     __shared__ Tile3Shared<TI, TJ, TK> sm;
+    __shared__ float fe[std::is_same_v<C, float> ? 9 * W::N : 1];  // fp32 forward edges (mixed)
     const Tile3 tile = tiles[blockIdx.x];
     const BlockInfo bi = blocks[tile.block];
     const int n0 = bi.n[0], n1 = bi.n[1], n2 = bi.n[2];
@@ -351,6 +380,22 @@ __global__ void __launch_bounds__(TI* TJ* TK, MINB)
         sm.P[2][id] = p2;
     }
     __syncthreads();
+    if constexpr (std::is_same_v<C, float>) {
+        // forward edge along k of every window node that has a +k neighbour
+        for (int id = threadIdx.x; id < W::N; id += NT) {
+            const int cu = id / (W::WJ * W::WK), cv = (id / W::WK) % W::WJ, cw = id % W::WK;
+            const bool has[3] = {cu + 1 < W::WI, cv + 1 < W::WJ, cw + 1 < W::WK};
+            const int step[3] = {W::WJ * W::WK, W::WK, 1};
+#pragma unroll
+            for (int k = 0; k < 3; ++k) {
+#pragma unroll
+                for (int i = 0; i < 3; ++i) {
+                    fe[(3 * k + i) * W::N + id] = has[k] ? float(sm.P[i][id + step[k]] - sm.P[i][id]) : 0.0f;
+                }
+            }
+        }
+        __syncthreads();
+    }
     const int ti = threadIdx.x / (TJ * TK), tj = (threadIdx.x / TK) % TJ, tk = threadIdx.x % TK;
     const int gi = tile.i0 + ti, gj = tile.j0 + tj, gk = tile.k0 + tk;
     if (gi > n0 - 2 || gj > n1 - 2 || gk > n2 - 2) { return; }
@@ -364,8 +409,8 @@ __global__ void __launch_bounds__(TI* TJ* TK, MINB)
     }
     double out[3];
     const bool go = grad_out != nullptr;
-    if (!dof3_update<TI, TJ, TK, KIND, C>(sm, ti, tj, tk, tv, delta, omega, out, go)) {
-        dof3_update<TI, TJ, TK, KIND, double>(sm, ti, tj, tk, tv, delta, omega, out, go);
+    if (!dof3_update<TI, TJ, TK, KIND, C>(sm, fe, ti, tj, tk, tv, delta, omega, out, go)) {
+        dof3_update<TI, TJ, TK, KIND, double>(sm, nullptr, ti, tj, tk, tv, delta, omega, out, go);
     }
     double* dst = go ? grad_out : Xout;
     dst[3 * slot] = out[0];
@@ -428,21 +473,21 @@ __device__ __forceinline__ void assemble_T3(const double* X, int32_t ic, const i
     }
 }
 
-// Stored-patch sweep, 3D, one warp per DOF (see stored_patch_kernel): the
-// lanes split the DOF's samples and reduce across the warp.
-template <int KIND>
+// Stored-patch sweep, 3D, G lanes per DOF (see stored_patch_kernel): the
+// lanes split the DOF's samples and reduce across the group.
+template <int KIND, int G>
 __global__ void stored3_kernel(StoredPatch3 sp, const double* __restrict__ Xin, double* __restrict__ Xout,
                                const double* __restrict__ tau, double delta, double omega, double* __restrict__ grad_out)
 {
-    const int lane = threadIdx.x & 31;
-    const int64_t nwarps = (int64_t(gridDim.x) * blockDim.x) >> 5;
+    const int lane = threadIdx.x & (G - 1);
+    const int64_t ngroups = (int64_t(gridDim.x) * blockDim.x) / G;
     const double none[3] = {0, 0, 0};
-    for (int64_t d = (blockIdx.x * int64_t(blockDim.x) + threadIdx.x) >> 5; d < sp.n; d += nwarps) {
+    for (int64_t d = (blockIdx.x * int64_t(blockDim.x) + threadIdx.x) / G; d < sp.n; d += ngroups) {
         const int32_t slot = sp.slot[d];
         const double pos[3] = {Xin[3 * int64_t(slot)], Xin[3 * int64_t(slot) + 1], Xin[3 * int64_t(slot) + 2]};
         const int64_t p0 = sp.off[d], p1 = sp.off[d + 1];
         double g[3] = {0, 0, 0}, h[6] = {0, 0, 0, 0, 0, 0}, e0 = 0.0;
-        for (int64_t p = p0 + lane; p < p1; p += 32) {
+        for (int64_t p = p0 + lane; p < p1; p += G) {
             const double* w = sp.W + p * sp.w_stride;
             const double s[3] = {double(sp.s0[p]), double(sp.s1[p]), double(sp.s2[p])};
             const int32_t in[3] = {sp.gn0[p], sp.gn1[p], sp.gn2[p]};
@@ -467,10 +512,10 @@ __global__ void stored3_kernel(StoredPatch3 sp, const double* __restrict__ Xin, 
             for (int q = 0; q < 6; ++q) { h[q] += wt * hh[q]; }
         }
 #pragma unroll
-        for (int q = 0; q < 3; ++q) { g[q] = warp_sum(g[q]); }
+        for (int q = 0; q < 3; ++q) { g[q] = group_sum<G>(g[q]); }
 #pragma unroll
-        for (int q = 0; q < 6; ++q) { h[q] = warp_sum(h[q]); }
-        e0 = warp_sum(e0);
+        for (int q = 0; q < 6; ++q) { h[q] = group_sum<G>(h[q]); }
+        e0 = group_sum<G>(e0);
         double tv[3] = {0, 0, 0};
         if (tau != nullptr) {
             for (int q = 0; q < 3; ++q) { tv[q] = tau[3 * int64_t(slot) + q]; }
@@ -492,7 +537,7 @@ __global__ void stored3_kernel(StoredPatch3 sp, const double* __restrict__ Xin, 
         for (int it = 0; it < 10; ++it) {
             const double tr[3] = {pos[0] + alpha * dl[0], pos[1] + alpha * dl[1], pos[2] + alpha * dl[2]};
             double e = 0.0, md = INFINITY;
-            for (int64_t p = p0 + lane; p < p1; p += 32) {
+            for (int64_t p = p0 + lane; p < p1; p += G) {
                 const double s[3] = {double(sp.s0[p]), double(sp.s1[p]), double(sp.s2[p])};
                 const int32_t in[3] = {sp.gn0[p], sp.gn1[p], sp.gn2[p]};
                 double t[9], detA;
@@ -501,8 +546,8 @@ __global__ void stored3_kernel(StoredPatch3 sp, const double* __restrict__ Xin, 
                 e += sp.wt[p * sp.wt_stride] * mu3_value<double>(KIND, t, delta, dd);
                 md = fmin(md, detA);
             }
-            e = warp_sum(e) - (tv[0] * tr[0] + tv[1] * tr[1] + tv[2] * tr[2]);
-            md = warp_min(md);
+            e = group_sum<G>(e) - (tv[0] * tr[0] + tv[1] * tr[1] + tv[2] * tr[2]);
+            md = group_min<G>(md);
             if (isfinite(e) && e <= e0 + Tol<double>::energy && (KIND == kUntangle || md > 0.0)) {
                 cur[0] = tr[0];
                 cur[1] = tr[1];

@@ -116,12 +116,17 @@ template <class R> EGG_HD void mu_eval(int kind, const R t[4], R delta, R& mu, R
     const R m = s * sf.f;  // s/(2D) (or s/(2Dh))
     R g2[4];
     for (int i = 0; i < 4; ++i) { g2[i] = R(2) * sf.f * t[i] + s * sf.fp * cof[i]; }
+    // Terms with an exact-zero factor (off-diagonal 2f, Pm = 0) are left out
+    // once the loops are unrolled, instead of being multiplied by 0.
     R H2[16];
     for (int i = 0; i < 4; ++i) {
         for (int j = 0; j < 4; ++j) {
-            H2[i * 4 + j] = (i == j ? R(2) * sf.f : R(0)) +
-                            R(2) * sf.fp * (t[i] * cof[j] + cof[i] * t[j]) +
-                            s * sf.fpp * cof[i] * cof[j] + s * sf.fp * Pm(i, j);
+            const R p = Pm(i, j);
+            R h = R(2) * sf.fp * (t[i] * cof[j] + cof[i] * t[j]);
+            if (i == j) { h = R(2) * sf.f + h; }
+            h = h + s * sf.fpp * cof[i] * cof[j];
+            if (p != R(0)) { h = h + s * sf.fp * p; }
+            H2[i * 4 + j] = h;
         }
     }
     if (kind != kShapeSize) {
@@ -136,8 +141,10 @@ template <class R> EGG_HD void mu_eval(int kind, const R t[4], R delta, R& mu, R
     for (int i = 0; i < 4; ++i) { g[i] = R(2) * m * g2[i] + R(2) * dm1 * cof[i]; }
     for (int i = 0; i < 4; ++i) {
         for (int j = 0; j < 4; ++j) {
-            H[i * 4 + j] = R(2) * g2[i] * g2[j] + R(2) * m * H2[i * 4 + j] + R(2) * cof[i] * cof[j] +
-                           R(2) * dm1 * Pm(i, j);
+            const R p = Pm(i, j);
+            R h = R(2) * g2[i] * g2[j] + R(2) * m * H2[i * 4 + j] + R(2) * cof[i] * cof[j];
+            if (p != R(0)) { h = h + R(2) * dm1 * p; }
+            H[i * 4 + j] = h;
         }
     }
 }
@@ -178,13 +185,9 @@ template <class R> EGG_HD R untangle_ddh(R D, R Dn, R r, R rn, R dD, R delta)
     return (Dn + D >= R(0)) ? R(0.5) * dD * (R(1) + q) : ls_div(R(2) * delta * delta * dD * (R(1) - q), (rn - Dn) * (r - D));
 }
 
-template <class R> EGG_HD R dmu2(int kind, const R t[4], const R dt[4], R delta, R& dnew)
+// The change from s, D and their exact increments ds, dD.
+template <class R> EGG_HD R dmu2_from(int kind, R s, R D, R ds, R dD, R delta, R& dnew)
 {
-    const R s = t[0] * t[0] + t[1] * t[1] + t[2] * t[2] + t[3] * t[3];
-    const R D = t[0] * t[3] - t[1] * t[2];
-    const R ds = R(2) * (t[0] * dt[0] + t[1] * dt[1] + t[2] * dt[2] + t[3] * dt[3]) +
-                 (dt[0] * dt[0] + dt[1] * dt[1] + dt[2] * dt[2] + dt[3] * dt[3]);
-    const R dD = (t[0] * dt[3] + dt[0] * t[3] - t[1] * dt[2] - dt[1] * t[2]) + (dt[0] * dt[3] - dt[1] * dt[2]);
     const R Dn = D + dD;
     dnew = Dn;
     if (kind == kUntangle) {
@@ -198,6 +201,35 @@ template <class R> EGG_HD R dmu2(int kind, const R t[4], const R dt[4], R delta,
     if (kind == kShape) { return dm; }
     const R m = ls_div(s, R(2) * D);
     return dm * (R(2) * m + dm) + dD * (Dn + D - R(2));
+}
+
+template <class R> EGG_HD R dmu2(int kind, const R t[4], const R dt[4], R delta, R& dnew)
+{
+    const R s = t[0] * t[0] + t[1] * t[1] + t[2] * t[2] + t[3] * t[3];
+    const R D = t[0] * t[3] - t[1] * t[2];
+    const R ds = R(2) * (t[0] * dt[0] + t[1] * dt[1] + t[2] * dt[2] + t[3] * dt[3]) +
+                 (dt[0] * dt[0] + dt[1] * dt[1] + dt[2] * dt[2] + dt[3] * dt[3]);
+    const R dD = (t[0] * dt[3] + dt[0] * t[3] - t[1] * dt[2] - dt[1] * t[2]) + (dt[0] * dt[3] - dt[1] * dt[2]);
+    return dmu2_from(kind, s, D, ds, dD, delta, dnew);
+}
+
+// dmu2 for a move of column COL of T = [t0 t1; t2 t3] by (ex, ey), the other
+// column fixed: the zero entries of dT are left out of the sums (IEEE
+// arithmetic keeps x * 0 and x + 0, so passing zeros would cost instructions),
+// and det(dT) = 0.
+template <class R, int COL> EGG_HD R dmu2_col(int kind, const R t[4], R ex, R ey, R delta, R& dnew)
+{
+    const R s = t[0] * t[0] + t[1] * t[1] + t[2] * t[2] + t[3] * t[3];
+    const R D = t[0] * t[3] - t[1] * t[2];
+    R ds, dD;
+    if constexpr (COL == 0) {
+        ds = R(2) * (t[0] * ex + t[2] * ey) + (ex * ex + ey * ey);
+        dD = ex * t[3] - t[1] * ey;
+    } else {
+        ds = R(2) * (t[1] * ex + t[3] * ey) + (ex * ex + ey * ey);
+        dD = t[0] * ey - ex * t[2];
+    }
+    return dmu2_from(kind, s, D, ds, dD, delta, dnew);
 }
 
 // Barrier accept policy: shape-type objectives never cross det A <= 0; the

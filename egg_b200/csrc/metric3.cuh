@@ -102,32 +102,71 @@ template <class R> EGG_HD R mu3_value(int kind, const R t[9], R delta, R& det)
     return mu3_from<R>(kind, S);
 }
 
+// x.v over the entries where v may be nonzero: all three, or only entry ax
+// when the caller knows v = v[ax] e_ax.  A known-zero entry is left out of
+// the sum rather than multiplied by 0, which IEEE arithmetic would not let
+// the compiler drop (ax is a constant once the caller's loop is unrolled).
+template <class R> EGG_HD R dot_ax(R x0, R x1, R x2, const R v[3], int ax)
+{
+    if (ax == 0) { return x0 * v[0]; }
+    if (ax == 1) { return x1 * v[1]; }
+    if (ax == 2) { return x2 * v[2]; }
+    return x0 * v[0] + x1 * v[1] + x2 * v[2];
+}
+
+// x.y with entry `skip` of y known to be zero (skip < 0: none).
+template <class R> EGG_HD R dot_skip(const R* x, const R* y, int skip)
+{
+    if (skip == 0) { return x[1] * y[1] + x[2] * y[2]; }
+    if (skip == 1) { return x[0] * y[0] + x[2] * y[2]; }
+    if (skip == 2) { return x[0] * y[0] + x[1] * y[1]; }
+    return x[0] * y[0] + x[1] * y[1] + x[2] * y[2];
+}
+
 // Node gradient g[3] and contracted Hessian h[6] = (xx, xy, xz, yy, yz, zz)
-// of one sample along the rank-one directions e_i v^T.
-template <class R> EGG_HD void role3(int kind, const Shared3<R>& S, const R v[3], R g[3], R h[6])
+// of one sample along the rank-one directions e_i v^T.  ax >= 0 states that
+// v = v[ax] e_ax (an axis neighbour with W_inv = I): then w_r = T_r x v has
+// a zero entry ax and the terms with zero factors are left out.
+template <class R> EGG_HD void role3(int kind, const Shared3<R>& S, const R v[3], R g[3], R h[6], int ax = -1)
 {
     const R* t = S.t;
     const R* C = S.C;
     R a[3], c[3], w[3][3];
 #pragma unroll
     for (int i = 0; i < 3; ++i) {
-        a[i] = t[3 * i] * v[0] + t[3 * i + 1] * v[1] + t[3 * i + 2] * v[2];
-        c[i] = C[3 * i] * v[0] + C[3 * i + 1] * v[1] + C[3 * i + 2] * v[2];
-        w[i][0] = t[3 * i + 1] * v[2] - t[3 * i + 2] * v[1];
-        w[i][1] = t[3 * i + 2] * v[0] - t[3 * i] * v[2];
-        w[i][2] = t[3 * i] * v[1] - t[3 * i + 1] * v[0];
+        const R* tr = t + 3 * i;
+        a[i] = dot_ax(tr[0], tr[1], tr[2], v, ax);
+        c[i] = dot_ax(C[3 * i], C[3 * i + 1], C[3 * i + 2], v, ax);
+        // w = T_r x v; with v = v[ax] e_ax, entry ax is zero and each other
+        // entry keeps its one term in v[ax]
+        if (ax == 0) {
+            w[i][0] = R(0);
+            w[i][1] = tr[2] * v[0];
+            w[i][2] = -(tr[1] * v[0]);
+        } else if (ax == 1) {
+            w[i][0] = -(tr[2] * v[1]);
+            w[i][1] = R(0);
+            w[i][2] = tr[0] * v[1];
+        } else if (ax == 2) {
+            w[i][0] = tr[1] * v[2];
+            w[i][1] = -(tr[0] * v[2]);
+            w[i][2] = R(0);
+        } else {
+            w[i][0] = tr[1] * v[2] - tr[2] * v[1];
+            w[i][1] = tr[2] * v[0] - tr[0] * v[2];
+            w[i][2] = tr[0] * v[1] - tr[1] * v[0];
+        }
     }
-    auto dot3 = [](const R* x, const R* y) { return x[0] * y[0] + x[1] * y[1] + x[2] * y[2]; };
     R k[3];
 #pragma unroll
     for (int i = 0; i < 3; ++i) {
         const int i1 = (i + 1) % 3, i2 = (i + 2) % 3;
-        k[i] = dot3(C + 3 * i1, w[i2]) - dot3(C + 3 * i2, w[i1]);
+        k[i] = dot_skip(C + 3 * i1, w[i2], ax) - dot_skip(C + 3 * i2, w[i1], ax);
     }
-    const R W00 = dot3(w[0], w[0]), W11 = dot3(w[1], w[1]), W22 = dot3(w[2], w[2]);
-    const R W01 = dot3(w[0], w[1]), W12 = dot3(w[1], w[2]), W02 = dot3(w[0], w[2]);
+    const R W00 = dot_skip(w[0], w[0], ax), W11 = dot_skip(w[1], w[1], ax), W22 = dot_skip(w[2], w[2], ax);
+    const R W01 = dot_skip(w[0], w[1], ax), W12 = dot_skip(w[1], w[2], ax), W02 = dot_skip(w[0], w[2], ax);
     const R m[3][3] = {{W11 + W22, -W01, -W02}, {-W01, W00 + W22, -W12}, {-W02, -W12, W00 + W11}};
-    const R vv = v[0] * v[0] + v[1] * v[1] + v[2] * v[2];
+    const R vv = dot_ax(v[0], v[1], v[2], v, ax);
     const R s = S.s, q = S.q, F = S.F, FD = S.FD, FDD = S.FDD;
     const R n9 = R(1.0 / 9.0);
     const R dm1x2 = R(2) * (S.D - R(1));
@@ -141,9 +180,10 @@ template <class R> EGG_HD void role3(int kind, const Shared3<R>& S, const R v[3]
     for (int i = 0; i < 3; ++i) {
 #pragma unroll
         for (int j = i; j < 3; ++j) {
-            R hij = (i == j ? R(2) * vv * q * F : R(0)) + R(2) * s * m[i][j] * F + s * q * FDD * c[i] * c[j] +
-                    R(4) * F * (a[i] * k[j] + a[j] * k[i]) + R(2) * q * FD * (a[i] * c[j] + a[j] * c[i]) +
-                    R(2) * s * FD * (k[i] * c[j] + k[j] * c[i]);
+            R hij = R(2) * s * m[i][j] * F;
+            if (i == j) { hij = R(2) * vv * q * F + hij; }
+            hij = hij + s * q * FDD * c[i] * c[j] + R(4) * F * (a[i] * k[j] + a[j] * k[i]) +
+                  R(2) * q * FD * (a[i] * c[j] + a[j] * c[i]) + R(2) * s * FD * (k[i] * c[j] + k[j] * c[i]);
             hij *= n9;
             if (kind == kShapeSize) { hij += R(2) * c[i] * c[j]; }
             h[e++] = hij;
@@ -300,7 +340,10 @@ template <class R> struct LineSample3 {
     R n0[3], n1[3], n2[3];  // column norms^2 of T along the line: n0 + a n1 + a^2 n2
 };
 
-template <class R> EGG_HD void line_sample3(const R t[9], const R u[3], const R v[3], LineSample3<R>& L)
+// ax >= 0 states that v = v[ax] e_ax (see role3): terms with zero factors
+// are left out, and N's column ax vanishes.
+template <class R>
+EGG_HD void line_sample3(const R t[9], const R u[3], const R v[3], LineSample3<R>& L, int ax = -1)
 {
     R C[9];
     cof3<R>(t, C);
@@ -316,25 +359,40 @@ template <class R> EGG_HD void line_sample3(const R t[9], const R u[3], const R 
     R Tv[3], Cv[3];
 #pragma unroll
     for (int i = 0; i < 3; ++i) {
-        Tv[i] = t[3 * i] * v[0] + t[3 * i + 1] * v[1] + t[3 * i + 2] * v[2];
-        Cv[i] = C[3 * i] * v[0] + C[3 * i + 1] * v[1] + C[3 * i + 2] * v[2];
+        Tv[i] = dot_ax(t[3 * i], t[3 * i + 1], t[3 * i + 2], v, ax);
+        Cv[i] = dot_ax(C[3 * i], C[3 * i + 1], C[3 * i + 2], v, ax);
     }
     const R uu = u[0] * u[0] + u[1] * u[1] + u[2] * u[2];
-    const R vv = v[0] * v[0] + v[1] * v[1] + v[2] * v[2];
+    const R vv = dot_ax(v[0], v[1], v[2], v, ax);
     L.D1 = u[0] * Cv[0] + u[1] * Cv[1] + u[2] * Cv[2];
     L.s1 = R(2) * (u[0] * Tv[0] + u[1] * Tv[1] + u[2] * Tv[2]);
     L.s2 = uu * vv;
     R cn = R(0), nn = R(0);
+    bool first = true;
 #pragma unroll
     for (int i = 0; i < 3; ++i) {
         const int i1 = (i + 1) % 3, i2 = (i + 2) % 3;
 #pragma unroll
         for (int j = 0; j < 3; ++j) {
+            if (ax == j) { continue; }  // N[i][ax] = 0
             const int j1 = (j + 1) % 3, j2 = (j + 2) % 3;
-            const R N = u[i1] * v[j1] * t[3 * i2 + j2] + t[3 * i1 + j1] * u[i2] * v[j2] -
-                        u[i1] * v[j2] * t[3 * i2 + j1] - t[3 * i1 + j2] * u[i2] * v[j1];
-            cn += C[3 * i + j] * N;
-            nn += N * N;
+            R N;
+            if (ax == j1) {
+                N = u[i1] * v[j1] * t[3 * i2 + j2] - t[3 * i1 + j2] * u[i2] * v[j1];
+            } else if (ax == j2) {
+                N = t[3 * i1 + j1] * u[i2] * v[j2] - u[i1] * v[j2] * t[3 * i2 + j1];
+            } else {
+                N = u[i1] * v[j1] * t[3 * i2 + j2] + t[3 * i1 + j1] * u[i2] * v[j2] -
+                    u[i1] * v[j2] * t[3 * i2 + j1] - t[3 * i1 + j2] * u[i2] * v[j1];
+            }
+            if (first) {
+                cn = C[3 * i + j] * N;
+                nn = N * N;
+                first = false;
+            } else {
+                cn += C[3 * i + j] * N;
+                nn += N * N;
+            }
         }
     }
     L.q1 = R(2) * cn;
@@ -342,8 +400,13 @@ template <class R> EGG_HD void line_sample3(const R t[9], const R u[3], const R 
 #pragma unroll
     for (int k = 0; k < 3; ++k) {
         const R tk2 = t[k] * t[k] + t[3 + k] * t[3 + k] + t[6 + k] * t[6 + k];
-        const R ut = u[0] * t[k] + u[1] * t[3 + k] + u[2] * t[6 + k];
         L.n0[k] = tk2;
+        if (ax >= 0 && k != ax) {  // column k of T does not move
+            L.n1[k] = R(0);
+            L.n2[k] = R(0);
+            continue;
+        }
+        const R ut = u[0] * t[k] + u[1] * t[3 + k] + u[2] * t[6 + k];
         L.n1[k] = R(2) * v[k] * ut;
         L.n2[k] = v[k] * v[k] * uu;
     }
@@ -371,11 +434,12 @@ template <class R> EGG_HD R dmu3_at(int kind, const LineSample3<R>& L, R a, R de
     return dm;
 }
 
-// Column norms^2 of T + a u v^T (the guard's shape test).
-template <class R> EGG_HD void line_norms3(const LineSample3<R>& L, R a, R n[3])
+// Column norms^2 of T + a u v^T (the guard's shape test); with ax >= 0 only
+// column ax moves.
+template <class R> EGG_HD void line_norms3(const LineSample3<R>& L, R a, R n[3], int ax = -1)
 {
 #pragma unroll
-    for (int k = 0; k < 3; ++k) { n[k] = L.n0[k] + a * (L.n1[k] + a * L.n2[k]); }
+    for (int k = 0; k < 3; ++k) { n[k] = (ax >= 0 && k != ax) ? L.n0[k] : L.n0[k] + a * (L.n1[k] + a * L.n2[k]); }
 }
 
 // Newton step -H^{-1} g for a symmetric 3x3 (packed xx, xy, xz, yy, yz, zz)

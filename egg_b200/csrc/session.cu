@@ -1007,29 +1007,56 @@ static StoredPatch2 stored_view(LevelData& S)
     return sp;
 }
 
+// Lanes per stored DOF (kStoredFillThreads2/3; EGG_B200_STORED_FILL
+// overrides the thread budget).
+static int stored_group(int64_t n, int dim)
+{
+    static const int64_t fill_env = [] {
+        const char* e = std::getenv("EGG_B200_STORED_FILL");
+        const long long v = e ? std::atoll(e) : 0;
+        return int64_t(v > 0 ? v : 0);
+    }();
+    const int64_t fill = fill_env > 0 ? fill_env : (dim == 3 ? kStoredFillThreads3 : kStoredFillThreads2);
+    for (int g : {32, 8, 2}) {
+        if (n * g <= fill) { return g; }
+    }
+    return 1;
+}
+
 template <int KIND>
 static void launch_stored(Session& S, LevelData& L, const double* xin, double* xout, const double* tau, double delta,
                           double omega, double* gout = nullptr, cudaStream_t on = nullptr)
 {
     if (L.n_stored == 0) { return; }
     const cudaStream_t st = on ? on : S.stream;
+    const int G = stored_group(L.n_stored, S.dim);
+    const unsigned grid = unsigned(std::min<int64_t>((L.n_stored * G + 127) / 128, 148 * 16));
     if (S.dim == 3) {
         StoredPatch3 sp {L.n_stored, L.st_slot.p, L.st_off.p, L.st_gc.p,  L.st_gn0.p, L.st_gn1.p,
                          L.st_gn2.p, L.st_s0.p,   L.st_s1.p,  L.st_s2.p, L.st_role.p, L.st_W.p,
                          L.st_wstride, L.st_wt.p, L.st_wtstride};
-        const unsigned grid = unsigned(std::min<int64_t>((L.n_stored + 3) / 4, 148 * 16));  // a warp per DOF
         S.timed(kKStored, [&] {
-            stored3_kernel<KIND><<<grid, 128, 0, st>>>(sp, xin, xout, tau, delta, omega, gout);
+            switch (G) {
+            case 32: stored3_kernel<KIND, 32><<<grid, 128, 0, st>>>(sp, xin, xout, tau, delta, omega, gout); break;
+            case 8: stored3_kernel<KIND, 8><<<grid, 128, 0, st>>>(sp, xin, xout, tau, delta, omega, gout); break;
+            case 2: stored3_kernel<KIND, 2><<<grid, 128, 0, st>>>(sp, xin, xout, tau, delta, omega, gout); break;
+            default: stored3_kernel<KIND, 1><<<grid, 128, 0, st>>>(sp, xin, xout, tau, delta, omega, gout); break;
+            }
         });
         return;
     }
     const StoredPatch2 sp = stored_view(L);
-    const unsigned grid = unsigned(std::min<int64_t>((L.n_stored + 3) / 4, 148 * 16));  // a warp per DOF
+    const auto* x2 = reinterpret_cast<const double2*>(xin);
+    auto* o2 = reinterpret_cast<double2*>(xout);
+    const auto* t2 = reinterpret_cast<const double2*>(tau);
+    auto* g2 = reinterpret_cast<double2*>(gout);
     S.timed(kKStored, [&] {
-        stored_patch_kernel<KIND><<<grid, 128, 0, st>>>(sp, reinterpret_cast<const double2*>(xin),
-                                                              reinterpret_cast<double2*>(xout),
-                                                              reinterpret_cast<const double2*>(tau), delta, omega,
-                                                              reinterpret_cast<double2*>(gout));
+        switch (G) {
+        case 32: stored_patch_kernel<KIND, 32><<<grid, 128, 0, st>>>(sp, x2, o2, t2, delta, omega, g2); break;
+        case 8: stored_patch_kernel<KIND, 8><<<grid, 128, 0, st>>>(sp, x2, o2, t2, delta, omega, g2); break;
+        case 2: stored_patch_kernel<KIND, 2><<<grid, 128, 0, st>>>(sp, x2, o2, t2, delta, omega, g2); break;
+        default: stored_patch_kernel<KIND, 1><<<grid, 128, 0, st>>>(sp, x2, o2, t2, delta, omega, g2); break;
+        }
     });
 }
 

@@ -40,3 +40,20 @@ def test_difference_form_accuracy(report, kind, dim):
     assert e64 < 1e-8
     assert e32 < 0.1
     assert naive > 10 * e32
+
+
+def test_forms_without_zero_terms_match_the_general_forms(tmp_path):
+    """dmu2_col, role3 / line_sample3 / line_norms3 with an axis hint leave
+    out terms with an exact-zero factor; they agree with the general forms to
+    rounding."""
+    gxx = shutil.which("g++")
+    if gxx is None:
+        pytest.skip("no host C++ compiler")
+    exe = tmp_path / "axis"
+    subprocess.run([gxx, "-O1", "-std=c++17", f"-I{ROOT / 'egg_b200' / 'csrc'}",
+                    str(ROOT / "tests" / "native" / "axis_forms_check.cpp"), "-o", str(exe)], check=True)
+    out = subprocess.run([str(exe)], check=True, capture_output=True, text=True).stdout
+    worst = {k: float(v) for k, v in (line.split() for line in out.strip().split("\n"))}
+    assert set(worst) == {"dmu2_col", "role3_ax", "line_sample3_ax", "line_norms3_ax"}
+    for name, w in worst.items():
+        assert w < 1e-13, (name, w)
