@@ -219,10 +219,16 @@ __global__ void broadcast2_kernel(double2* __restrict__ X, const int32_t* __rest
 // the omega blend and writes X_out.  Patch semantics follow
 // src/structured_patch.hpp:89-258 and src/sweep.hpp:1534-1650.
 // ---------------------------------------------------------------------------
-template <int CI, int CJ, class C> struct TileShared2 {
+// Whether the fp32 line search reads T from phase 2's cell edges.  Measured
+// on B200: faster for shape (+1-2%) and untangle; shape_size runs 4-5%
+// slower with it (its line search keeps more values live, and the hoisted
+// edge loads spill), so it forms T from the staged positions instead.
+template <int KIND, class C> constexpr bool kEdgeCache2 = std::is_same_v<C, float> && KIND != kShapeSize;
+
+template <int CI, int CJ, class C, int KIND> struct TileShared2 {
     static constexpr int NC = CI * CJ;
-    // fp32 cell edges, kept for the mixed line search (one slot otherwise)
-    static constexpr int NE = std::is_same_v<C, float> ? NC : 1;
+    // fp32 cell edges for the mixed line search (one slot otherwise)
+    static constexpr int NE = kEdgeCache2<KIND, C> ? NC : 1;
     // sample values: only the fp64 accept test reads them (one slot otherwise)
     static constexpr int NM = std::is_same_v<C, double> ? NC : 1;
     double2 P[(CI + 1) * (CJ + 1)];
@@ -361,7 +367,7 @@ __global__ void __launch_bounds__(CI* CJ, MINB)
                        double delta, double omega, double2* __restrict__ grad_out)
 {
     extern __shared__ __align__(16) unsigned char smem_raw[];
-    using S = TileShared2<CI, CJ, C>;
+    using S = TileShared2<CI, CJ, C, KIND>;
     S& sm = *reinterpret_cast<S*>(smem_raw);
     constexpr int NC = CI * CJ;
     constexpr int PW = CJ + 1;
@@ -407,7 +413,7 @@ __global__ void __launch_bounds__(CI* CJ, MINB)
             const double2 p10 = sm.P[(ci + 1) * PW + cj], p11 = sm.P[(ci + 1) * PW + cj + 1];
             const double e0x[2] = {p10.x - p00.x, p11.x - p01.x}, e0y[2] = {p10.y - p00.y, p11.y - p01.y};
             const double e1x[2] = {p01.x - p00.x, p11.x - p10.x}, e1y[2] = {p01.y - p00.y, p11.y - p10.y};
-            if constexpr (std::is_same_v<C, float>) {
+            if constexpr (kEdgeCache2<KIND, C>) {
 #pragma unroll
                 for (int k = 0; k < 2; ++k) {
                     sm.E[k][tid] = make_float2(float(e0x[k]), float(e0y[k]));
@@ -543,10 +549,25 @@ __global__ void __launch_bounds__(CI* CJ, MINB)
                         const int b = (r == 0) ? a : ((r == 1) ? (a ^ 2) : (a ^ 1));
                         const float s0 = (b & 2) ? -1.0f : 1.0f;
                         const float s1 = (b & 1) ? -1.0f : 1.0f;
-                        // T of sample b: the cell's fp32 edges from phase 2
-                        // (each rounded once from its fp64 difference)
-                        const float2 ea = sm.E[b & 1][cell], eb = sm.E[2 + (b >> 1)][cell];
-                        const float t[4] = {ea.x, eb.x, ea.y, eb.y};
+                        float t[4];
+                        if constexpr (kEdgeCache2<KIND, C>) {
+                            // T of sample b: the cell's fp32 edges from phase 2
+                            // (each rounded once from its fp64 difference)
+                            const float2 ea = sm.E[b & 1][cell], eb = sm.E[2 + (b >> 1)][cell];
+                            t[0] = ea.x;
+                            t[1] = eb.x;
+                            t[2] = ea.y;
+                            t[3] = eb.y;
+                        } else {
+                            const int bn0 = b ^ 2, bn1 = b ^ 1;
+                            const int cu = ci + (b >> 1), cv = cj + (b & 1);
+                            const int u0 = ci + (bn0 >> 1), v0 = cj + (bn0 & 1);
+                            const int u1 = ci + (bn1 >> 1), v1 = cj + (bn1 & 1);
+                            t[0] = s0 * (rx[u0][v0] - rx[cu][cv]);
+                            t[1] = s1 * (rx[u1][v1] - rx[cu][cv]);
+                            t[2] = s0 * (ry[u0][v0] - ry[cu][cv]);
+                            t[3] = s1 * (ry[u1][v1] - ry[cu][cv]);
+                        }
                         // r = 0 moves both columns of T; r = 1 (2) moves column
                         // 0 (1) only, whose change forms skip the zero entries.
                         float dn, dm, ax, bx, ay, by;

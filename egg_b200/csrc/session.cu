@@ -326,13 +326,15 @@ static bool rows_uniform(const double* W, int64_t rows, int width)
 // Opt the interior kernels into >48 KB of dynamic shared memory.
 template <int CI, int CJ, int MINB, class C> static void set_smem_attr()
 {
-    const int smem = int(sizeof(TileShared2<CI, CJ, C>));
     EGG_CK(cudaFuncSetAttribute(interior_tile_kernel<CI, CJ, MINB, kShape, C>,
-                                cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+                                cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                int(sizeof(TileShared2<CI, CJ, C, kShape>))));
     EGG_CK(cudaFuncSetAttribute(interior_tile_kernel<CI, CJ, MINB, kUntangle, C>,
-                                cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+                                cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                int(sizeof(TileShared2<CI, CJ, C, kUntangle>))));
     EGG_CK(cudaFuncSetAttribute(interior_tile_kernel<CI, CJ, MINB, kShapeSize, C>,
-                                cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+                                cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                int(sizeof(TileShared2<CI, CJ, C, kShapeSize>))));
 }
 
 static void configure_kernels(int prec, int dim)
@@ -871,7 +873,7 @@ template <int CI, int CJ, int MINB, int KIND, class C>
 static void launch_tile(Session& S, LevelData& L, const double* xin, double* xout, const double* tau, double delta,
                         double omega, double* gout)
 {
-    const size_t smem = sizeof(TileShared2<CI, CJ, C>);
+    const size_t smem = sizeof(TileShared2<CI, CJ, C, KIND>);
     const auto* xi = reinterpret_cast<const double2*>(xin);
     auto* xo = reinterpret_cast<double2*>(xout);
     const auto* tv = reinterpret_cast<const double2*>(tau);
