@@ -223,7 +223,7 @@ def sphere129_fas(torch, cpp_core, args, local):
                          "mindet_after": float(md_u)},
             "energy": {"initial": float(E0), "after_untangle": float(E1), "after_step": [float(x) for x in E],
                        "mindet": float(M[-1])},
-            "jacobi_updates_per_s": g.num_free * 8 / jac}
+            "jacobi_updates_per_s": g.num_free * 8 / jac, "autotune": s.variants()}
     ref = oracle.load_ref("fp64")
     if ref is not None and not args.no_cpu_baseline:
         _omp()
