@@ -30,7 +30,7 @@ from . import wire as _wire
 
 __all__ = [
     "Grid", "unit_square", "disk_oh", "tangled_square", "unit_cube", "two_cubes", "sphere_in_cube",
-    "grid_mindet", "mean_size_w_inv",
+    "grid_mindet", "mean_size_w_inv", "disk_on_curve", "square_sliding",
 ]
 
 
@@ -42,6 +42,8 @@ class Grid:
     X: np.ndarray  # (N, d) float64, global node order
     free: np.ndarray  # (N,) bool
     meta: dict = field(default_factory=dict)
+    # constrained boundary nodes: global id -> (entity tag, record)
+    constraints: dict = field(default_factory=dict)
 
     @property
     def num_nodes(self) -> int:
@@ -52,7 +54,8 @@ class Grid:
         return int(self.free.sum())
 
     def wire(self, *, w_inv=None, compact: bool = False) -> dict:
-        return _wire.flat_wire(self.blocks, self.free, self.d, w_inv=w_inv, compact=compact)
+        return _wire.flat_wire(self.blocks, self.free, self.d, w_inv=w_inv, compact=compact,
+                               constraints=self.constraints)
 
     def structured(self) -> dict:
         return _wire.structured_tables(self.blocks)
@@ -138,6 +141,62 @@ def disk_oh(n: int = 65, frac: float = 0.25, seed: int = 0, half_width: float = 
     noise = rng.uniform(-1.0, 1.0, size=(N, 2)) * (frac * h)[:, None]
     X = X + np.where(free[:, None], noise, 0.0)
     return Grid(f"disk_oh{n}", 2, blocks, X, free, {"frac": frac, "seed": seed, "half_width": a})
+
+
+def disk_on_curve(n: int = 17, frac: float = 0.25, slide: float = 0.3, off: float = 0.02, seed: int = 0,
+                  ry: float = 1.0) -> Grid:
+    """The 5-block O-H disk whose outer nodes slide on its boundary curve.
+
+    ``ry == 1``: the unit circle (Circle entity, tag 2).  Otherwise the disk is
+    squeezed to the axis-aligned ellipse with semi-axes (1, ry) (Ellipse
+    entity, tag 3).  Every boundary node is moved along the curve by up to
+    ``slide`` of its spacing and off it by up to ``off`` of the local edge
+    length, so the first sweep also projects.
+    """
+    g = disk_oh(n, frac=frac, seed=seed)
+    X = g.X.copy()
+    X[:, 1] *= ry
+    bnd = np.flatnonzero(~g.free)
+    rng = np.random.default_rng(seed + 101)
+    h = _min_edge(g.blocks, X)
+    th = np.arctan2(X[bnd, 1] / ry, X[bnd, 0])
+    th += rng.uniform(-slide, slide, bnd.size) * (0.5 * np.pi / (n - 1))
+    rad = 1.0 + rng.uniform(-off, off, bnd.size) * h[bnd]
+    X[bnd, 0] = rad * np.cos(th)
+    X[bnd, 1] = rad * ry * np.sin(th)
+    tag, rec = (2, (0.0, 0.0, 1.0)) if ry == 1.0 else (3, (0.0, 0.0, 1.0, ry))
+    cons = {int(b): (tag, rec) for b in bnd}
+    kind = "circle" if tag == 2 else "ellipse"
+    return Grid(f"disk_{kind}{n}", 2, g.blocks, X, g.free.copy(), {"frac": frac, "seed": seed, "ry": ry}, cons)
+
+
+def square_sliding(n: int = 17, frac: float = 0.25, slide: float = 0.3, seed: int = 0,
+                   rail_end: float = 0.6) -> Grid:
+    """Unit square whose side nodes slide: three sides on LineSeg entities
+    (tag 1), the top side on a LineRail (tag 15) from x = 0 to ``rail_end``,
+    so top nodes beyond it are released and move freely.  Corners stay fixed.
+    Side nodes move along their side by up to ``slide`` h; top nodes also sit
+    up to 0.05 h off the line."""
+    g = unit_square(n, frac=frac, seed=seed)
+    ids = g.blocks[0]
+    X = g.X.copy()
+    h = 1.0 / (n - 1)
+    rng = np.random.default_rng(seed + 202)
+    cons = {}
+    sides = [
+        (ids[1:-1, 0], 0, (1, (0.0, 0.0, 1.0, 0.0))),           # bottom, y = 0: x slides
+        (ids[-1, 1:-1], 1, (1, (1.0, 0.0, 1.0, 1.0))),          # right, x = 1: y slides
+        (ids[0, 1:-1], 1, (1, (0.0, 0.0, 0.0, 1.0))),           # left, x = 0
+        (ids[1:-1, -1], 0, (15, (0.0, 1.0, rail_end, 1.0))),    # top rail, y = 1
+    ]
+    for nodes, ax, ent in sides:
+        X[nodes, ax] += rng.uniform(-slide, slide, nodes.size) * h
+        if ent[0] == 15:
+            X[nodes, 1 - ax] += rng.uniform(-0.05, 0.05, nodes.size) * h
+        for v in nodes:
+            cons[int(v)] = ent
+    return Grid(f"square_slide{n}", 2, g.blocks, X, g.free.copy(),
+                {"frac": frac, "seed": seed, "rail_end": rail_end}, cons)
 
 
 def grid_mindet(blocks, X, d=2) -> np.ndarray:

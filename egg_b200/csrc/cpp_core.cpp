@@ -115,6 +115,7 @@ struct Desc {
     egg_b200_session_desc d {};
     Keep keep;
     std::vector<int32_t> shapes, bgd, tags;
+    std::vector<double> eparams;
 };
 
 // Fill the C-ABI descriptor from the reference's two dicts + X
@@ -199,19 +200,33 @@ void fill_desc(Desc& D, const py::dict& ctx, const py::dict& st, const DArr& X, 
         // Entity partitions: every DOF must be covered exactly once; non-Free
         // tags mark constrained boundary DOFs.
         D.tags.assign(size_t(d.ndof), -1);
+        bool constrained = false;
         if (g.contains("entities")) {
+            D.eparams.assign(size_t(d.ndof) * EGG_B200_ENTITY_FIELDS, 0.0);
             for (auto item : g["entities"].cast<py::dict>()) {
                 py::dict ed = item.second.cast<py::dict>();
                 if (!ed.contains("tag")) {
                     throw py::value_error("unpack_context: entities carries a '__blob__' group (unsupported)");
                 }
                 const int tag = ed["tag"].cast<int>();
+                const int kf = ed.contains("kFields") ? ed["kFields"].cast<int>() : 0;
                 IArr dl = IArr::ensure(ed["dof_local"]);
+                DArr rec = ed.contains("records") ? DArr::ensure(ed["records"]) : DArr();
+                if (tag != 0 && rec.size() != dl.size() * py::ssize_t(kf)) {
+                    throw py::value_error("validate_context: entity records size " + std::to_string(rec.size()) +
+                                          " != count*kFields " + std::to_string(dl.size() * kf));
+                }
                 for (py::ssize_t i = 0; i < dl.size(); ++i) {
                     const int32_t v = dl.data()[i];
                     if (v < 0 || v >= d.ndof) { throw py::value_error("validate_context: dof_local out of range"); }
                     if (D.tags[v] != -1) { throw py::value_error("validate_context: dof_local covered by more than one SoA partition"); }
                     D.tags[v] = tag;
+                    if (tag == 0) { continue; }
+                    constrained = true;
+                    // row i of the partition's (count, kFields) records
+                    for (int f = 0; f < std::min(kf, int(EGG_B200_ENTITY_FIELDS)); ++f) {
+                        D.eparams[size_t(v) * EGG_B200_ENTITY_FIELDS + f] = rec.data()[i * kf + f];
+                    }
                 }
             }
             for (int64_t i = 0; i < d.ndof; ++i) {
@@ -223,6 +238,7 @@ void fill_desc(Desc& D, const py::dict& ctx, const py::dict& st, const DArr& X, 
             std::fill(D.tags.begin(), D.tags.end(), 0);
         }
         d.entity_tag = D.tags.data();
+        d.entity_params = constrained ? D.eparams.data() : nullptr;
     }
 
     py::dict es = ctx["energy_stencil"].cast<py::dict>();
@@ -882,18 +898,43 @@ PYBIND11_MODULE(cpp_core, m)
 
     m.def(
       "newton_step",
-      [](const DArr& grad, const DArr& hess, const DArr& pos, int tag, const py::object&) {
-          if (tag != 0) {
-              PyErr_SetString(PyExc_NotImplementedError, "newton_step: constrained entity tags are not supported");
-              throw py::error_already_set();
-          }
+      [](const DArr& grad, const DArr& hess, const DArr& pos, int tag, const py::object& params) {
           if (grad.size() != 2 || hess.size() != 4 || pos.size() != 2) {
               throw py::value_error("newton_step: grad(2), hess(4), pos(2) expected");
           }
           std::vector<double> x(2);
-          check(egg_b200_newton_step(grad.data(), hess.data(), x.data()));
+          if (tag == 0) {
+              check(egg_b200_newton_step(grad.data(), hess.data(), x.data()));
+              return vec(x);
+          }
+          if (params.is_none()) { throw py::value_error("newton_step: a constrained tag needs its params"); }
+          DArr pr = DArr::ensure(params);
+          std::vector<double> rec(EGG_B200_ENTITY_FIELDS, 0.0);
+          for (py::ssize_t i = 0; i < std::min<py::ssize_t>(pr.size(), EGG_B200_ENTITY_FIELDS); ++i) {
+              rec[size_t(i)] = pr.data()[i];
+          }
+          std::vector<double> foot(2);
+          check(egg_b200_entity_step(tag, rec.data(), grad.data(), hess.data(), pos.data(), x.data(), foot.data()));
           return vec(x);
       },
       py::arg("grad"), py::arg("hess"), py::arg("pos"), py::arg("tag") = 0, py::arg("params") = py::none(),
-      "Free-DOF Newton step -H^{-1} g with the zero/non-finite fallbacks. Returns delta(2,).");
+      "Newton step: -H^{-1} g for a Free DOF (tag 0), or reduced onto the tangent of a 2D curve entity "
+      "(LineSeg, Circle, Ellipse, LineRail; params = its record). Returns delta(2,).");
+
+    m.def(
+      "entity_project",
+      [](const DArr& pos, int tag, const DArr& params) {
+          if (pos.size() != 2) { throw py::value_error("entity_project: pos(2) expected"); }
+          std::vector<double> rec(EGG_B200_ENTITY_FIELDS, 0.0);
+          for (py::ssize_t i = 0; i < std::min<py::ssize_t>(params.size(), EGG_B200_ENTITY_FIELDS); ++i) {
+              rec[size_t(i)] = params.data()[i];
+          }
+          const double g[2] = {0.0, 0.0}, h[4] = {1.0, 0.0, 0.0, 1.0};
+          double st[2];
+          std::vector<double> foot(2);
+          check(egg_b200_entity_step(tag, rec.data(), g, h, pos.data(), st, foot.data()));
+          return vec(foot);
+      },
+      py::arg("pos"), py::arg("tag"), py::arg("params"),
+      "Projection of pos onto a 2D curve entity (device evaluation). Returns foot(2,).");
 }

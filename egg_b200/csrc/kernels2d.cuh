@@ -12,6 +12,7 @@
 // Both sweep kernels read X_in (frozen snapshot) and write X_out.
 #pragma once
 
+#include "entity2.cuh"
 #include "metric.cuh"
 
 #include <cstdint>
@@ -723,6 +724,8 @@ struct StoredPatch2 {
     int32_t w_stride;       // 4 or 0
     const double* wt;       // [occ] or [1]
     int32_t wt_stride;      // 1 or 0
+    const int8_t* etag;     // [n] entity tag of each DOF, or NULL (all Free)
+    const double* epar;     // [n * EGG_B200_ENTITY_FIELDS] entity records (constrained DOFs)
 };
 
 __device__ __forceinline__ void assemble_T(const double2 c, const double2 n0, const double2 n1,
@@ -905,12 +908,25 @@ __global__ void stored_patch_kernel(StoredPatch2 sp, const double2* __restrict__
             if (lane == 0) { grad_out[slot] = make_double2(g[0], g[1]); }
             continue;
         }
+        // A constrained DOF (src/sweep.hpp:1286-1403): the Newton step reduced
+        // onto its entity's tangent, damped by omega before the line search,
+        // and every trial projected onto the entity, so the accepted point
+        // stays on the geometry.  A Free DOF: the full step, omega blend after.
+        const int etag = sp.etag != nullptr ? int(sp.etag[d]) : 0;
+        const double* er = sp.epar + (etag != 0 ? d * EGG_B200_ENTITY_FIELDS : 0);
         double dl[2];
-        solve2<double>(h, g, dl);
+        if (etag == 0) {
+            solve2<double>(h, g, dl);
+        } else {
+            entity_newton_step(etag, er, h, g, pos.x, pos.y, dl);
+            dl[0] *= omega;
+            dl[1] *= omega;
+        }
         double alpha = 1.0;
         double2 cur = pos;
         for (int it = 0; it < 10; ++it) {
-            const double2 trial = make_double2(pos.x + alpha * dl[0], pos.y + alpha * dl[1]);
+            double2 trial = make_double2(pos.x + alpha * dl[0], pos.y + alpha * dl[1]);
+            if (etag != 0) { entity_project(etag, er, trial.x, trial.y, trial.x, trial.y); }
             double e = 0.0, md = INFINITY;
             for (int64_t p = p0 + lane; p < p1; p += G) {
                 const double* w = sp.W + p * sp.w_stride;
@@ -931,7 +947,7 @@ __global__ void stored_patch_kernel(StoredPatch2 sp, const double2* __restrict__
             }
             alpha *= 0.5;
         }
-        if (omega != 1.0) {
+        if (etag == 0 && omega != 1.0) {
             cur.x = pos.x + omega * (cur.x - pos.x);
             cur.y = pos.y + omega * (cur.y - pos.y);
         }

@@ -31,6 +31,11 @@
 namespace egg_b200
 {
 
+#ifndef __CUDACC__
+// host builds (the tests' native checks): the C++ names of the CUDA math calls
+using std::isfinite;
+#endif
+
 enum ObjectiveKind : int { kShape = 0, kUntangle = 1, kShapeSize = 2 };
 
 // Line-search slack / zero-gradient guard of the working precision

@@ -125,6 +125,9 @@ struct LevelData {
     DevBuf<int8_t> st_s0, st_s1, st_s2;
     DevBuf<double> st_W, st_wt;
     int st_wstride = 0, st_wtstride = 0;
+    int64_t n_constrained = 0;  // stored DOFs on a boundary entity
+    DevBuf<int8_t> st_etag;     // [n_stored] entity tag (uploaded when n_constrained > 0)
+    DevBuf<double> st_epar;     // [n_stored * EGG_B200_ENTITY_FIELDS] entity records
     int64_t nshare = 0;
     DevBuf<int32_t> sh_src, sh_dst;
 };
@@ -569,7 +572,8 @@ static Session* create_session(const egg_b200_session_desc& d)
     std::vector<int64_t> st_off {0};
     std::vector<int32_t> st_gc, st_gn0, st_gn1, st_gn2, st_role;
     std::vector<int8_t> st_s0, st_s1, st_s2;
-    std::vector<double> st_W, st_wt;
+    std::vector<double> st_W, st_wt, st_epar;
+    std::vector<int8_t> st_etag;
     std::vector<uint8_t> seen_slot(off, 0);
     int64_t poff = 0;
     for (int64_t i = 0; i < ndof; ++i) {
@@ -581,9 +585,22 @@ static Session* create_session(const egg_b200_session_desc& d)
             invalid("validate_context: group[0] dof_idx index " + std::to_string(gid) + " out of range [0, " +
                     std::to_string(M) + ")");
         }
-        if (d.entity_tag && d.entity_tag[i] != 0) {
-            throw Error(EGG_B200_ENOTSUP,
-                        "egg_b200: constrained (non-Free) boundary DOFs are not supported by this core yet");
+        const int32_t etag = d.entity_tag ? d.entity_tag[i] : 0;
+        if (etag != 0) {
+            if (!entity_supported(D, etag)) {
+                throw Error(EGG_B200_ENOTSUP, "egg_b200: constrained entity tag " + std::to_string(etag) +
+                                                " is not supported in " + std::to_string(D) +
+                                                "D (this core relaxes the 2D LineSeg, Circle, Ellipse and LineRail)");
+            }
+            if (!d.entity_params) { invalid("validate_context: constrained DOF without entity_params"); }
+            for (int f = 0; f < EGG_B200_ENTITY_FIELDS; ++f) {
+                if (!std::isfinite(d.entity_params[i * EGG_B200_ENTITY_FIELDS + f])) {
+                    invalid("validate_context: entity record of DOF " + std::to_string(i) + " is not finite");
+                }
+            }
+            if (d.interior_block && d.interior_block[i] >= 0) {
+                throw Error(EGG_B200_ENOTSUP, "egg_b200: a constrained DOF on the structured-interior path");
+            }
         }
         const int32_t slot = S->g2s[gid];
         if (slot < 0) {
@@ -610,6 +627,11 @@ static Session* create_session(const egg_b200_session_desc& d)
             continue;
         }
         st_slot.push_back(slot);
+        st_etag.push_back(int8_t(etag));
+        for (int f = 0; f < EGG_B200_ENTITY_FIELDS; ++f) {
+            st_epar.push_back(etag != 0 ? d.entity_params[i * EGG_B200_ENTITY_FIELDS + f] : 0.0);
+        }
+        if (etag != 0) { S->n_constrained++; }
         for (int64_t p = p0; p < p0 + P; ++p) {
             auto remap = [&](int32_t g) {
                 const int32_t s = S->g2s[g];
@@ -840,6 +862,10 @@ static Session* create_session(const egg_b200_session_desc& d)
     set_tiles(*S, *S, variant_shape(*S, 0));
     S->st_slot.upload(st_slot);
     S->st_off.upload(st_off);
+    if (S->n_constrained) {
+        S->st_etag.upload(st_etag);
+        S->st_epar.upload(st_epar);
+    }
     S->st_gc.upload(st_gc);
     S->st_gn0.upload(st_gn0);
     S->st_gn1.upload(st_gn1);
@@ -1006,6 +1032,8 @@ static StoredPatch2 stored_view(LevelData& S)
     sp.w_stride = S.st_wstride;
     sp.wt = S.st_wt.p;
     sp.wt_stride = S.st_wtstride;
+    sp.etag = S.n_constrained ? S.st_etag.p : nullptr;
+    sp.epar = S.n_constrained ? S.st_epar.p : nullptr;
     return sp;
 }
 
@@ -1487,6 +1515,13 @@ template <int KIND> __global__ void patch_eval_kernel(StoredPatch2 sp, const dou
 
 __global__ void newton_step_kernel(const double* g, const double* h, double* out) { solve2<double>(h, g, out); }
 
+// in: record[4], grad[2], hess[4], pos[2]; out: step[2], foot[2]
+__global__ void entity_step_kernel(int tag, const double* in, double* out)
+{
+    entity_newton_step(tag, in, in + 6, in + 4, in[10], in[11], out);
+    entity_project(tag, in, in[10], in[11], out[2], out[3]);
+}
+
 template <class F> static int guarded(F&& f)
 {
     try {
@@ -1855,6 +1890,9 @@ int egg_b200_session_run_fas(egg_b200_session* s, int32_t n_cycles, int32_t nu_p
         Session& S = *s->impl;
         if (S.n_seg > 0) {
             throw Error(EGG_B200_ENOTSUP, "run_fas: FAS is not available on a batch session (one session per mesh)");
+        }
+        if (S.n_constrained > 0) {
+            throw Error(EGG_B200_ENOTSUP, "run_fas: FAS with constrained boundary DOFs is not supported by this core");
         }
         EGG_CK(cudaSetDevice(S.device));
         std::vector<double> E, Md;
@@ -2264,6 +2302,34 @@ int egg_b200_metric3_probe(int32_t objective, double delta, const double* t, con
         EGG_CK(cudaMemcpy(mu, dm.p, n * sizeof(double), cudaMemcpyDeviceToHost));
         EGG_CK(cudaMemcpy(grad9, dg.p, 9 * n * sizeof(double), cudaMemcpyDeviceToHost));
         EGG_CK(cudaMemcpy(hv, dh.p, 6 * n * sizeof(double), cudaMemcpyDeviceToHost));
+    });
+}
+
+int egg_b200_entity_step(int32_t tag, const double* record, const double* grad, const double* hess,
+                         const double* pos, double* step, double* foot)
+{
+    return guarded([&] {
+        if (!record || !grad || !hess || !pos || !step || !foot) { invalid("entity_step: NULL argument"); }
+        if (!entity_supported(2, tag)) {
+            throw Error(EGG_B200_ENOTSUP, "entity_step: entity tag " + std::to_string(tag) +
+                                            " is not supported (2D LineSeg, Circle, Ellipse and LineRail are)");
+        }
+        std::vector<double> in(12);
+        std::copy(record, record + EGG_B200_ENTITY_FIELDS, in.begin());
+        std::copy(grad, grad + 2, in.begin() + 4);
+        std::copy(hess, hess + 4, in.begin() + 6);
+        std::copy(pos, pos + 2, in.begin() + 10);
+        DevBuf<double> din, dout;
+        din.upload(in);
+        dout.alloc(4);
+        entity_step_kernel<<<1, 1>>>(tag, din.p, dout.p);
+        EGG_CK(cudaGetLastError());
+        double o[4];
+        EGG_CK(cudaMemcpy(o, dout.p, sizeof(o), cudaMemcpyDeviceToHost));
+        step[0] = o[0];
+        step[1] = o[1];
+        foot[0] = o[2];
+        foot[1] = o[3];
     });
 }
 

@@ -107,6 +107,12 @@ def free_mask_from_fixed(n_nodes: int, fixed_ids) -> np.ndarray:
     return m
 
 
+# Entity partitions of constrained DOFs: tag -> (partition name, kFields),
+# the reference's frozen tags and packed record widths (src/entity_soa.hpp:37-56,
+# src/geometry.hpp:1760-1928).
+ENTITY_KINDS = {1: ("line_seg", 4), 2: ("circle", 3), 3: ("ellipse", 4), 15: ("line_rail", 4)}
+
+
 def flat_wire(
     blocks: list[np.ndarray],
     free_mask: np.ndarray,
@@ -114,16 +120,25 @@ def flat_wire(
     *,
     w_inv: np.ndarray | None = None,
     compact: bool = False,
+    constraints: dict | None = None,
 ) -> dict:
-    """The ``{"groups", "energy_stencil"}`` wire for Free (unconstrained) DOFs.
+    """The ``{"groups", "energy_stencil"}`` wire for Free DOFs and, optionally,
+    constrained boundary DOFs.
 
     ``w_inv`` is one ``(d, d)`` inverse target shared by every sample (default
     identity) or ``(ns, d, d)`` per sample in canonical order.  Mirrors
-    ``build_flat_context`` (``egg/smoothing/flat_context.py:136-346``) for the
-    case without constraints, interface, curvature or directional terms.
+    ``build_flat_context`` (``egg/smoothing/flat_context.py:136-346``) without
+    interface, curvature or directional terms.  ``constraints`` maps a global
+    node id (not Free) to ``(tag, record)``: the node becomes a moving DOF on
+    that entity (``ENTITY_KINDS``), with a stored patch, in one SoA partition
+    per tag whose packed records follow the partition's ``dof_local`` order.
     ``compact`` drops the energy-stencil index arrays (see module docstring) and
     sends a uniform target as one shared row.
     """
+    constraints = constraints or {}
+    con_ids = np.array(sorted(constraints), dtype=np.int64)
+    if con_ids.size and np.asarray(free_mask)[con_ids].any():
+        raise ValueError("flat_wire: a constrained node is also marked Free")
     blocks = [np.asarray(b) for b in blocks]
     nc = 1 << d
     dd = d * d
@@ -149,7 +164,10 @@ def flat_wire(
             grids = np.meshgrid(*[np.arange(1, s - 1, dtype=np.int32) for s in sh], indexing="ij")
             node_block[inner] = bi
             node_logical[inner] = np.stack([g.reshape(-1) for g in grids], axis=1)
+    node_block[con_ids] = -1  # constrained nodes always take a stored patch
     node_interior = node_block >= 0
+    moving = np.asarray(free_mask, dtype=bool).copy()
+    moving[con_ids] = True
 
     C = cell_corner_ids(blocks, d)
     ncell = C.shape[0]
@@ -162,7 +180,7 @@ def flat_wire(
     # Membership only for stored-patch DOFs (moving, not interior-eligible):
     # restrict to cells that touch such a node, so large grids with few stored
     # DOFs never materialise the full node x sample table.
-    stored_node = free_mask & ~node_interior
+    stored_node = moving & ~node_interior
     touch = stored_node[C]  # (ncell, nc)
     cells = np.flatnonzero(touch.any(axis=1))
     Ct = C[cells]  # (m, nc)
@@ -192,7 +210,7 @@ def flat_wire(
         return out
 
     groups = []
-    dofs = np.flatnonzero(free_mask)
+    dofs = np.flatnonzero(moving)
     if dofs.size:
         P_of = np.zeros(dofs.size, dtype=np.int32)
         if m_node.size:
@@ -209,11 +227,19 @@ def flat_wire(
                 "free": {
                     "tag": 0,
                     "kFields": 0,
-                    "dof_local": np.arange(dofs.size, dtype=np.int32),
+                    "dof_local": np.flatnonzero(np.asarray(free_mask)[dofs]).astype(np.int32),
                     "records": np.zeros(0, dtype=np.float64),
                 }
             },
         }
+        for tag in sorted({int(constraints[int(n)][0]) for n in con_ids}):
+            name, kf = ENTITY_KINDS[tag]
+            nodes = [int(n) for n in con_ids if int(constraints[int(n)][0]) == tag]
+            local = np.searchsorted(dofs, np.array(nodes, dtype=np.int64)).astype(np.int32)
+            rec = np.array([np.asarray(constraints[n][1], dtype=np.float64)[:kf] for n in nodes])
+            g["entities"][name] = {"tag": tag, "kFields": kf, "dof_local": local,
+                                   "records": np.ascontiguousarray(rec.reshape(-1))}
+
         g.update(fields(m_sid, uniform_out=True))
         groups.append(g)
 

@@ -40,6 +40,16 @@ extern "C" {
 #define EGG_B200_PREC_FP64 0
 #define EGG_B200_PREC_MIXED 1
 
+/* Entity tags of constrained DOFs: the reference's frozen wire values
+ * (src/entity_soa.hpp:37-56 EntityTag).  This core relaxes the closed-form 2D
+ * curves below; other tags are rejected with EGG_B200_ENOTSUP. */
+#define EGG_B200_TAG_FREE 0
+#define EGG_B200_TAG_LINESEG 1   /* record (sx, sy, ex, ey): segment, projection clamped to it */
+#define EGG_B200_TAG_CIRCLE 2    /* record (cx, cy, r, -): radial projection */
+#define EGG_B200_TAG_ELLIPSE 3   /* record (cx, cy, rx, ry): axis-aligned, radial-scaling projection */
+#define EGG_B200_TAG_LINERAIL 15 /* record (sx, sy, ex, ey): open-ended segment, released beyond its ends */
+#define EGG_B200_ENTITY_FIELDS 4 /* reals per entity record in entity_params */
+
 typedef struct egg_b200_session egg_b200_session;
 
 /* Everything the reference's session constructor takes, flattened:
@@ -78,7 +88,7 @@ typedef struct egg_b200_session_desc {
     const int32_t* P_of;             /* [ndof] stored occurrences per DOF */
     const int32_t* interior_block;   /* [ndof] or NULL; -1 = stored patch */
     const int32_t* interior_logical; /* [ndof*dim] or NULL */
-    const int32_t* entity_tag;       /* [ndof] or NULL (all Free); non-zero = constrained */
+    const int32_t* entity_tag;       /* [ndof] or NULL (all Free); EGG_B200_TAG_*, non-zero = constrained */
     int64_t total_samples;           /* sum(P_of) */
     const int32_t* gc;               /* [total_samples] */
     const int32_t* gn[3];            /* [total_samples] each, first dim used */
@@ -100,6 +110,16 @@ typedef struct egg_b200_session_desc {
     int64_t es_W_inv_len;
     const double* es_weight; /* NULL, [1] or [es_num_samples] */
     int64_t es_weight_len;
+
+    /* Entity record of every constrained DOF, EGG_B200_ENTITY_FIELDS reals
+     * per DOF in group order (rows of Free DOFs are ignored): the DOF's row of
+     * its entity partition's packed SoA records (src/entity_soa.hpp:98-108,
+     * src/geometry.hpp:1760-1928 EntitySoA<E>::load), zero-padded.  NULL when
+     * every DOF is Free.  A constrained DOF takes the reference's
+     * boundary-kernel step (src/sweep.hpp:1286-1403): the Newton step reduced
+     * onto the entity tangent, damped by omega before the line search, every
+     * trial projected onto the entity. */
+    const double* entity_params; /* [ndof * EGG_B200_ENTITY_FIELDS] or NULL */
 } egg_b200_session_desc;
 
 /* Control-net wire for one block (src/control_net.hpp:72-87 ControlNetHostT;
@@ -335,6 +355,16 @@ int egg_b200_patch_eval(int32_t objective, double delta, const double* X, int64_
  * fallbacks, evaluated on the device (the oracle binding newton_step,
  * src/bindings.cpp:2100-2130, for the Free tag). grad[2], hess[4] -> step[2]. */
 int egg_b200_newton_step(const double* grad, const double* hess, double* step);
+
+/* Constrained-DOF Newton step and projection, evaluated on the device (the
+ * oracle binding newton_step, src/bindings.cpp:2103-2130, for an entity tag;
+ * src/patch.hpp:396-413 newton_delta): step = the Newton step reduced onto the
+ * entity tangent at pos (a rail released beyond its ends takes the full step),
+ * foot = the projection of pos onto the entity.  tag is one of the
+ * EGG_B200_TAG_* curves; record holds its EGG_B200_ENTITY_FIELDS reals.
+ * grad[2], hess[4] (row-major), pos[2] -> step[2], foot[2]. */
+int egg_b200_entity_step(int32_t tag, const double* record, const double* grad, const double* hess,
+                         const double* pos, double* step, double* foot);
 
 #ifdef __cplusplus
 }

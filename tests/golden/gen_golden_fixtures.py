@@ -13,7 +13,11 @@ Two sources, both from the reference checkout (run in a container that has it):
    energy / min-det trajectories), so the GPU tests can compare against the
    reference without the reference present.
 
-3. Control-net runs of the same reference core and of the reference's NumPy
+3. Constrained boundary runs of the same core (``ref_constrained.npz``):
+   sweeps with nodes sliding on Circle, Ellipse, LineSeg and LineRail
+   entities, and the entity Newton step / projection on random inputs.
+
+4. Control-net runs of the same reference core and of the reference's NumPy
    dense reduced-GN oracle (``egg.smoothing.control_ref``), with the control
    wires built by the reference's own builders -> ``ref_control.npz``.
 
@@ -126,11 +130,87 @@ RUNS3 = [
 ]
 
 
+# Constrained boundary DOFs (2D closed-form entities), reference fp64 core:
+# sweeps on grids whose boundary nodes slide on a Circle, an Ellipse, LineSegs
+# and a LineRail, plus the entity Newton step and projection on random inputs
+# -> ref_constrained.npz.
+CASES_CON = {
+    "disk_circle17": ("disk_on_curve", dict(n=17, seed=3)),
+    "disk_ellipse17": ("disk_on_curve", dict(n=17, seed=4, ry=0.6)),
+    "square_slide17": ("square_sliding", dict(n=17, seed=5)),
+    "disk_circle33": ("disk_on_curve", dict(n=33, seed=6)),
+}
+RUNS_CON = [
+    # (case, phase, delta, omega, n_sweeps)
+    ("disk_circle17", "barrier", 0.0, 1.0, 30),
+    ("disk_ellipse17", "barrier", 0.0, 0.8, 30),
+    ("square_slide17", "barrier", 0.0, 1.0, 30),
+    ("square_slide17", "shape_size", 0.0, 0.8, 20),
+    ("disk_circle33", "barrier", 0.0, 1.0, 30),
+    ("disk_circle17", "untangle", 1e-3, 0.5, 10),
+]
+ENTITY_RECORDS = {
+    1: (0.1, -0.2, 0.9, 0.4),
+    2: (0.2, -0.1, 0.7, 0.0),
+    3: (-0.1, 0.3, 0.8, 0.45),
+    15: (0.0, 0.0, 0.6, 0.3),
+}
+
+
 def case_grid(name: str):
     from egg_b200 import configs
 
+    if name in CASES_CON:
+        fn, kw = CASES_CON[name]
+        return getattr(configs, fn)(**kw)
     fn, kw, _ = CASES[name]
     return getattr(configs, fn)(**kw)
+
+
+def _constrained_runs() -> dict:
+    from oracle import oracle
+
+    ref = oracle.load_ref("fp64")
+    if ref is None:
+        raise SystemExit("oracle/_ref/fp64 missing: run oracle/build_ref.sh first")
+    out = {}
+    for case, phase, delta, omega, n in RUNS_CON:
+        g = case_grid(case)
+        ctx, st = g.wire(), g.structured()
+        X1, e1, m1 = ref.cpp_structured_sweep(ctx, st, g.X_flat(), 1, device="cpu", phase=phase,
+                                               delta=delta, omega=omega, report_every=1, dim=2)
+        Xn, en, mn = ref.cpp_structured_sweep(ctx, st, g.X_flat(), n, device="cpu", phase=phase,
+                                               delta=delta, omega=omega, report_every=1, dim=2)
+        key = f"{case}/{phase}/{omega}"
+        out[key + "/X1"] = X1
+        out[key + "/Xn"] = Xn
+        out[key + "/E"] = en
+        out[key + "/M"] = mn
+    rng = np.random.default_rng(31)
+    for tag, rec in ENTITY_RECORDS.items():
+        kf = 3 if tag == 2 else 4
+        params = np.array(rec[:kf])
+        G = rng.normal(size=(64, 2))
+        G[:4] *= 1e-17  # below the zero-gradient guard
+        H = rng.normal(size=(64, 2, 2))
+        H = H @ H.transpose(0, 2, 1) + 0.1 * np.eye(2)
+        H[4:8] = 0.0  # singular reduced system: the fallback step
+        P = rng.uniform(-1.2, 1.4, size=(64, 2))
+        steps = np.array([ref.newton_step(G[i], H[i].ravel(), P[i], tag, params) for i in range(64)])
+        feet = np.array([ref.geometry_project(P[i], tag, params) for i in range(64)])
+        out[f"entity/{tag}/params"] = params
+        out[f"entity/{tag}/grad"] = G
+        out[f"entity/{tag}/hess"] = H.reshape(64, 4)
+        out[f"entity/{tag}/pos"] = P
+        out[f"entity/{tag}/step"] = steps
+        out[f"entity/{tag}/foot"] = feet
+    return out
+
+
+def gen_reference_constrained() -> None:
+    out = _constrained_runs()
+    np.savez_compressed(HERE / "ref_constrained.npz", **out)
+    print(f"ref_constrained.npz: {len(out)} arrays")
 
 
 def _runs_for(prec: str) -> dict:
@@ -307,6 +387,10 @@ if __name__ == "__main__" and len(sys.argv) == 4 and sys.argv[1] == "--runs":
     np.savez(sys.argv[3], **_runs_for(sys.argv[2]))
     raise SystemExit(0)
 
+if __name__ == "__main__" and len(sys.argv) == 2 and sys.argv[1] == "--constrained":
+    gen_reference_constrained()
+    raise SystemExit(0)
+
 if __name__ == "__main__":
     args = [a for a in sys.argv[1:] if not a.startswith("--")]
     ref_root = Path(args[0]) if args else Path("/root/reference")
@@ -314,3 +398,4 @@ if __name__ == "__main__":
     gen_reference_runs()
     gen_reference_wire(ref_root)
     gen_reference_control(ref_root)
+    gen_reference_constrained()

@@ -1,0 +1,102 @@
+"""Constrained boundary DOFs on the GPU: nodes sliding on a Circle, an
+Ellipse, LineSegs and a LineRail relax exactly as the reference core relaxes
+them (first sweep and trajectory, fp64), the mixed path tracks that, every
+accepted boundary node lies on its entity, a batch of constrained meshes
+equals separate sessions, and FAS refuses them."""
+
+from __future__ import annotations
+
+import numpy as np
+import pytest
+
+from egg_b200 import configs
+from tests.conftest import GOLDEN
+from tests.golden.gen_golden_fixtures import ENTITY_RECORDS, RUNS_CON, case_grid
+
+pytestmark = pytest.mark.gpu
+
+_FX = np.load(GOLDEN / "ref_constrained.npz")
+
+
+def _hmin(g):
+    return float(configs._min_edge(g.blocks, g.X).min())
+
+
+def _session(core, g, precision="fp64", compact=False):
+    return core.CppStructuredSweepSession(g.wire(compact=compact), g.structured(), g.X_flat(), precision=precision)
+
+
+@pytest.mark.parametrize("tag", sorted(ENTITY_RECORDS))
+def test_entity_step_and_projection_match_reference(gpu, tag):
+    k = f"entity/{tag}/"
+    for i in range(len(_FX[k + "pos"])):
+        st = gpu.newton_step(_FX[k + "grad"][i], _FX[k + "hess"][i], _FX[k + "pos"][i], tag, _FX[k + "params"])
+        np.testing.assert_allclose(st, _FX[k + "step"][i], rtol=1e-12, atol=1e-15)
+        ft = gpu.entity_project(_FX[k + "pos"][i], tag, _FX[k + "params"])
+        np.testing.assert_allclose(ft, _FX[k + "foot"][i], rtol=1e-12, atol=1e-15)
+
+
+@pytest.mark.parametrize("run", RUNS_CON, ids=lambda r: f"{r[0]}-{r[1]}-{r[3]}")
+def test_constrained_sweeps_match_reference(gpu, run):
+    case, phase, delta, omega, n = run
+    g = case_grid(case)
+    key = f"{case}/{phase}/{omega}"
+    s = _session(gpu, g)
+    s.run(1, phase=phase, delta=delta, omega=omega)
+    assert np.abs(s.get_X() - _FX[key + "/X1"]).max() <= 1e-12 * _hmin(g)
+    s2 = _session(gpu, g)
+    E, M = s2.run(n, phase=phase, delta=delta, omega=omega, report_every=1)
+    np.testing.assert_allclose(E, _FX[key + "/E"], rtol=1e-9)
+    np.testing.assert_allclose(M, _FX[key + "/M"], rtol=1e-8, atol=1e-16)
+    assert np.abs(s2.get_X() - _FX[key + "/Xn"]).max() <= 1e-9 * _hmin(g)
+
+
+@pytest.mark.parametrize("case", ["disk_circle17", "disk_ellipse17", "square_slide17"])
+def test_accepted_boundary_nodes_lie_on_their_entity(gpu, case):
+    g = case_grid(case)
+    s = _session(gpu, g)
+    s.run(20)
+    X = s.get_X().reshape(-1, 2)
+    moved = 0
+    for v, (tag, rec) in g.constraints.items():
+        if np.allclose(X[v], g.X[v], rtol=0, atol=0):
+            continue  # never accepted a trial: still at its start
+        moved += 1
+        foot = gpu.entity_project(X[v], tag, np.asarray(rec, dtype=np.float64))
+        if tag == 15 and not np.allclose(foot, X[v]):
+            continue  # a released rail node
+        np.testing.assert_allclose(X[v], foot, rtol=0, atol=1e-14)
+    assert moved > len(g.constraints) // 2
+
+
+@pytest.mark.parametrize("case", ["disk_circle33", "square_slide17"])
+def test_constrained_mixed_tracks_fp64(gpu, case):
+    g = case_grid(case)
+    key = f"{case}/barrier/1.0"
+    s = _session(gpu, g, precision="mixed", compact=True)
+    s.run(1)
+    assert np.abs(s.get_X() - _FX[key + "/X1"]).max() <= 1e-5 * _hmin(g)
+    E, M = s.run(29, report_every=1)
+    np.testing.assert_allclose(E[-1], _FX[key + "/E"][-1], rtol=1e-5)
+    assert np.sign(M[-1]) == np.sign(_FX[key + "/M"][-1])
+
+
+def test_constrained_batch_equals_separate_sessions(gpu):
+    gs = [case_grid("disk_circle17"), case_grid("square_slide17"), case_grid("disk_ellipse17")]
+    b = gpu.CppBatchSweepSession([(g.wire(compact=True), g.structured(), g.X_flat()) for g in gs],
+                                 precision="mixed")
+    b.set_variant(1)
+    b.run(10)
+    Xb = b.get_X()
+    for m, g in enumerate(gs):
+        s = _session(gpu, g, precision="mixed", compact=True)
+        s.set_variant(1)
+        s.run(10)
+        np.testing.assert_array_equal(Xb[m], s.get_X())
+
+
+def test_fas_refuses_constrained_dofs(gpu):
+    g = case_grid("square_slide17")
+    s = _session(gpu, g)
+    with pytest.raises(NotImplementedError, match="constrained"):
+        s.run_fas(1)
