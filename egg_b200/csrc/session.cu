@@ -660,7 +660,13 @@ static Session* create_session(const egg_b200_session_desc& d)
     }
     S->n_stored = int64_t(st_slot.size());
     S->free_h.assign(off, 0);
-    for (int32_t sl : st_slot) { S->free_h[sl] = 1; }
+    // FAS masks: Free DOFs only.  Constrained DOFs relax in the fine smoothing
+    // but are frozen on the coarse levels and take no coarse correction, so
+    // the correction never pushes them off their geometry (src/fas.hpp:120-140
+    // masks_from_context, :380-384).
+    for (size_t k = 0; k < st_slot.size(); ++k) {
+        if (st_etag[k] == 0) { S->free_h[size_t(st_slot[k])] = 1; }
+    }
     for (int64_t i = 0; i < off; ++i) {
         if (active[i]) { S->free_h[i] = 1; }
     }
@@ -1890,9 +1896,6 @@ int egg_b200_session_run_fas(egg_b200_session* s, int32_t n_cycles, int32_t nu_p
         Session& S = *s->impl;
         if (S.n_seg > 0) {
             throw Error(EGG_B200_ENOTSUP, "run_fas: FAS is not available on a batch session (one session per mesh)");
-        }
-        if (S.n_constrained > 0) {
-            throw Error(EGG_B200_ENOTSUP, "run_fas: FAS with constrained boundary DOFs is not supported by this core");
         }
         EGG_CK(cudaSetDevice(S.device));
         std::vector<double> E, Md;

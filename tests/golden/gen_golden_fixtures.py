@@ -149,6 +149,12 @@ RUNS_CON = [
     ("disk_circle33", "barrier", 0.0, 1.0, 30),
     ("disk_circle17", "untangle", 1e-3, 0.5, 10),
 ]
+# FAS V-cycles on sliding-boundary grids: (case, phase, n_cycles, nu_pre, nu_post, nu_coarse, omega, max_levels)
+FAS_RUNS_CON = [
+    ("disk_circle33", "barrier", 4, 2, 2, 32, 0.8, 32),
+    ("square_slide17", "barrier", 4, 2, 2, 32, 1.0, 32),
+    ("disk_ellipse17", "barrier", 3, 2, 2, 32, 1.0, 3),
+]
 ENTITY_RECORDS = {
     1: (0.1, -0.2, 0.9, 0.4),
     2: (0.2, -0.1, 0.7, 0.0),
@@ -186,6 +192,15 @@ def _constrained_runs() -> dict:
         out[key + "/Xn"] = Xn
         out[key + "/E"] = en
         out[key + "/M"] = mn
+    for case, phase, nc, npre, npost, ncoarse, omega, ml in FAS_RUNS_CON:
+        g = case_grid(case)
+        sess = ref.CppStructuredSweepSession(g.wire(), g.structured(), g.X_flat(), device="cpu", dim=2)
+        E, M = sess.run_fas(nc, nu_pre=npre, nu_post=npost, nu_coarse=ncoarse, omega=omega, max_levels=ml,
+                            phase=phase)
+        key = f"fas/{case}/{phase}/{ml}"
+        out[key + "/E"] = E
+        out[key + "/M"] = M
+        out[key + "/X"] = sess.get_X()
     rng = np.random.default_rng(31)
     for tag, rec in ENTITY_RECORDS.items():
         kf = 3 if tag == 2 else 4

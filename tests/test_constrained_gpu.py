@@ -2,7 +2,7 @@
 Ellipse, LineSegs and a LineRail relax exactly as the reference core relaxes
 them (first sweep and trajectory, fp64), the mixed path tracks that, every
 accepted boundary node lies on its entity, a batch of constrained meshes
-equals separate sessions, and FAS refuses them."""
+equals separate sessions, and FAS V-cycles on such grids match the reference."""
 
 from __future__ import annotations
 
@@ -11,7 +11,7 @@ import pytest
 
 from egg_b200 import configs
 from tests.conftest import GOLDEN
-from tests.golden.gen_golden_fixtures import ENTITY_RECORDS, RUNS_CON, case_grid
+from tests.golden.gen_golden_fixtures import ENTITY_RECORDS, FAS_RUNS_CON, RUNS_CON, case_grid
 
 pytestmark = pytest.mark.gpu
 
@@ -95,8 +95,15 @@ def test_constrained_batch_equals_separate_sessions(gpu):
         np.testing.assert_array_equal(Xb[m], s.get_X())
 
 
-def test_fas_refuses_constrained_dofs(gpu):
-    g = case_grid("square_slide17")
+@pytest.mark.parametrize("run", FAS_RUNS_CON, ids=lambda r: f"{r[0]}-{r[1]}-{r[7]}")
+def test_fas_on_sliding_boundaries_matches_reference(gpu, run):
+    """FAS V-cycles: constrained DOFs relax in the fine smoothing, stay frozen
+    on the coarse levels and take no coarse correction, as in the reference."""
+    case, phase, nc, npre, npost, ncoarse, omega, ml = run
+    g = case_grid(case)
+    key = f"fas/{case}/{phase}/{ml}"
     s = _session(gpu, g)
-    with pytest.raises(NotImplementedError, match="constrained"):
-        s.run_fas(1)
+    E, M = s.run_fas(nc, nu_pre=npre, nu_post=npost, nu_coarse=ncoarse, omega=omega, max_levels=ml, phase=phase)
+    np.testing.assert_allclose(E, _FX[key + "/E"], rtol=1e-8)
+    np.testing.assert_allclose(M, _FX[key + "/M"], rtol=1e-7, atol=1e-16)
+    assert np.abs(s.get_X() - _FX[key + "/X"]).max() <= 1e-8 * _hmin(g)
