@@ -144,14 +144,18 @@ def disk_oh(n: int = 65, frac: float = 0.25, seed: int = 0, half_width: float = 
 
 
 def disk_on_curve(n: int = 17, frac: float = 0.25, slide: float = 0.3, off: float = 0.02, seed: int = 0,
-                  ry: float = 1.0) -> Grid:
+                  ry: float = 1.0, arcs: bool = False) -> Grid:
     """The 5-block O-H disk whose outer nodes slide on its boundary curve.
 
-    ``ry == 1``: the unit circle (Circle entity, tag 2).  Otherwise the disk is
-    squeezed to the axis-aligned ellipse with semi-axes (1, ry) (Ellipse
-    entity, tag 3).  Every boundary node is moved along the curve by up to
-    ``slide`` of its spacing and off it by up to ``off`` of the local edge
-    length, so the first sweep also projects.
+    ``ry == 1``: the unit circle (Circle entity, tag 2); with ``arcs`` each
+    outer block's quarter of it instead (CircleArc entities, tag 6, open,
+    angle ranges [-pi/4, pi/4], [pi/4, 3pi/4], [3pi/4, 5pi/4] (across the
+    +-pi seam) and [-3pi/4, -pi/4]; a node shared by two blocks takes the
+    first one's arc).  Otherwise the disk is squeezed to the axis-aligned
+    ellipse with semi-axes (1, ry) (Ellipse entity, tag 3).  Every boundary
+    node is moved along the curve by up to ``slide`` of its spacing and off it
+    by up to ``off`` of the local edge length, so the first sweep also
+    projects.
     """
     g = disk_oh(n, frac=frac, seed=seed)
     X = g.X.copy()
@@ -167,6 +171,14 @@ def disk_on_curve(n: int = 17, frac: float = 0.25, slide: float = 0.3, off: floa
     tag, rec = (2, (0.0, 0.0, 1.0)) if ry == 1.0 else (3, (0.0, 0.0, 1.0, ry))
     cons = {int(b): (tag, rec) for b in bnd}
     kind = "circle" if tag == 2 else "ellipse"
+    if arcs:
+        if ry != 1.0:
+            raise ValueError("disk_on_curve: arcs need the circle (ry == 1)")
+        cons = {}
+        for blk, t0 in zip(g.blocks[1:], (-0.25 * np.pi, 0.25 * np.pi, 0.75 * np.pi, -0.75 * np.pi)):
+            for v in blk[-1, :]:
+                cons.setdefault(int(v), (6, (0.0, 0.0, 1.0, t0, t0 + 0.5 * np.pi, 0.0)))
+        kind = "arcs"
     return Grid(f"disk_{kind}{n}", 2, g.blocks, X, g.free.copy(), {"frac": frac, "seed": seed, "ry": ry}, cons)
 
 

@@ -726,6 +726,7 @@ struct StoredPatch2 {
     int32_t wt_stride;      // 1 or 0
     const int8_t* etag;     // [n] entity tag of each DOF, or NULL (all Free)
     const double* epar;     // [n * EGG_B200_ENTITY_FIELDS] entity records (constrained DOFs)
+    int cold;               // first sweep of a run call: trimmed arcs project in world space
 };
 
 __device__ __forceinline__ void assemble_T(const double2 c, const double2 n0, const double2 n1,
@@ -912,11 +913,18 @@ __global__ void stored_patch_kernel(StoredPatch2 sp, const double2* __restrict__
         // onto its entity's tangent, damped by omega before the line search,
         // and every trial projected onto the entity, so the accepted point
         // stays on the geometry.  A Free DOF: the full step, omega blend after.
+        // A trimmed arc after the first sweep of a run call searches in its
+        // angle instead (src/sweep.hpp:1718-1876): trials q* + alpha dq,
+        // clamped onto the trim and evaluated on the arc.
         const int etag = sp.etag != nullptr ? int(sp.etag[d]) : 0;
         const double* er = sp.epar + (etag != 0 ? d * EGG_B200_ENTITY_FIELDS : 0);
-        double dl[2];
+        const bool warm_arc = etag == EGG_B200_TAG_CIRCLEARC && !sp.cold;
+        double dl[2] = {0.0, 0.0};
+        double qstar = 0.0, dq = 0.0;
         if (etag == 0) {
             solve2<double>(h, g, dl);
+        } else if (warm_arc) {
+            arc_warm_step(er, h, g, pos.x, pos.y, omega, qstar, dq);
         } else {
             entity_newton_step(etag, er, h, g, pos.x, pos.y, dl);
             dl[0] *= omega;
@@ -926,7 +934,11 @@ __global__ void stored_patch_kernel(StoredPatch2 sp, const double2* __restrict__
         double2 cur = pos;
         for (int it = 0; it < 10; ++it) {
             double2 trial = make_double2(pos.x + alpha * dl[0], pos.y + alpha * dl[1]);
-            if (etag != 0) { entity_project(etag, er, trial.x, trial.y, trial.x, trial.y); }
+            if (warm_arc) {
+                arc_eval(er, arc_clamp(er, qstar + alpha * dq), trial.x, trial.y);
+            } else if (etag != 0) {
+                entity_project(etag, er, trial.x, trial.y, trial.x, trial.y);
+            }
             double e = 0.0, md = INFINITY;
             for (int64_t p = p0 + lane; p < p1; p += G) {
                 const double* w = sp.W + p * sp.w_stride;

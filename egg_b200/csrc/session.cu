@@ -126,6 +126,7 @@ struct LevelData {
     DevBuf<double> st_W, st_wt;
     int st_wstride = 0, st_wtstride = 0;
     int64_t n_constrained = 0;  // stored DOFs on a boundary entity
+    int64_t n_arc = 0;          // of which on a trimmed arc (cold first sweep per run call)
     DevBuf<int8_t> st_etag;     // [n_stored] entity tag (uploaded when n_constrained > 0)
     DevBuf<double> st_epar;     // [n_stored * EGG_B200_ENTITY_FIELDS] entity records
     int64_t nshare = 0;
@@ -590,7 +591,7 @@ static Session* create_session(const egg_b200_session_desc& d)
             if (!entity_supported(D, etag)) {
                 throw Error(EGG_B200_ENOTSUP, "egg_b200: constrained entity tag " + std::to_string(etag) +
                                                 " is not supported in " + std::to_string(D) +
-                                                "D (this core relaxes the 2D LineSeg, Circle, Ellipse and LineRail)");
+                                                "D (this core relaxes the 2D LineSeg, Circle, Ellipse, CircleArc and LineRail)");
             }
             if (!d.entity_params) { invalid("validate_context: constrained DOF without entity_params"); }
             for (int f = 0; f < EGG_B200_ENTITY_FIELDS; ++f) {
@@ -632,6 +633,7 @@ static Session* create_session(const egg_b200_session_desc& d)
             st_epar.push_back(etag != 0 ? d.entity_params[i * EGG_B200_ENTITY_FIELDS + f] : 0.0);
         }
         if (etag != 0) { S->n_constrained++; }
+        if (etag == EGG_B200_TAG_CIRCLEARC) { S->n_arc++; }
         for (int64_t p = p0; p < p0 + P; ++p) {
             auto remap = [&](int32_t g) {
                 const int32_t s = S->g2s[g];
@@ -1040,6 +1042,7 @@ static StoredPatch2 stored_view(LevelData& S)
     sp.wt_stride = S.st_wtstride;
     sp.etag = S.n_constrained ? S.st_etag.p : nullptr;
     sp.epar = S.n_constrained ? S.st_epar.p : nullptr;
+    sp.cold = 0;
     return sp;
 }
 
@@ -1061,7 +1064,7 @@ static int stored_group(int64_t n, int dim)
 
 template <int KIND>
 static void launch_stored(Session& S, LevelData& L, const double* xin, double* xout, const double* tau, double delta,
-                          double omega, double* gout = nullptr, cudaStream_t on = nullptr)
+                          double omega, double* gout = nullptr, cudaStream_t on = nullptr, bool cold = false)
 {
     if (L.n_stored == 0) { return; }
     const cudaStream_t st = on ? on : S.stream;
@@ -1081,7 +1084,8 @@ static void launch_stored(Session& S, LevelData& L, const double* xin, double* x
         });
         return;
     }
-    const StoredPatch2 sp = stored_view(L);
+    StoredPatch2 sp = stored_view(L);
+    sp.cold = cold ? 1 : 0;
     const auto* x2 = reinterpret_cast<const double2*>(xin);
     auto* o2 = reinterpret_cast<double2*>(xout);
     const auto* t2 = reinterpret_cast<const double2*>(tau);
@@ -1235,25 +1239,26 @@ template <int KIND> static void launch_report(Session& S, const double* x, doubl
 // the stored-patch kernel forks onto the side stream beside the tiles.
 template <int KIND>
 static void relax_level(Session& S, LevelData& L, const double* xin, double* xout, const double* tau, double delta,
-                        double omega, double* gout = nullptr)
+                        double omega, double* gout = nullptr, bool cold = false)
 {
     if (L.n_stored > 0 && L.ntiles > 0 && !S.profiling) {
         EGG_CK(cudaEventRecord(S.fork_ev, S.stream));
         EGG_CK(cudaStreamWaitEvent(S.side, S.fork_ev, 0));
-        launch_stored<KIND>(S, L, xin, xout, tau, delta, omega, gout, S.side);
+        launch_stored<KIND>(S, L, xin, xout, tau, delta, omega, gout, S.side, cold);
         EGG_CK(cudaEventRecord(S.join_ev, S.side));
         launch_interior<KIND>(S, L, xin, xout, tau, delta, omega, gout);
         EGG_CK(cudaStreamWaitEvent(S.stream, S.join_ev, 0));
     } else {
         launch_interior<KIND>(S, L, xin, xout, tau, delta, omega, gout);
-        launch_stored<KIND>(S, L, xin, xout, tau, delta, omega, gout);
+        launch_stored<KIND>(S, L, xin, xout, tau, delta, omega, gout, nullptr, cold);
     }
 }
 
-template <int KIND> static void sweep_once(Session& S, double* xin, double* xout, double delta, double omega)
+template <int KIND>
+static void sweep_once(Session& S, double* xin, double* xout, double delta, double omega, bool cold = false)
 {
     launch_broadcast(S, S, xin);
-    relax_level<KIND>(S, S, xin, xout, nullptr, delta, omega);
+    relax_level<KIND>(S, S, xin, xout, nullptr, delta, omega, nullptr, cold);
     S.updates += S.n_interior + S.n_stored;
 }
 
@@ -1334,7 +1339,9 @@ template <int KIND> static void run_impl(Session& S, int n_sweeps, double delta,
     int s = 0;
     while (s < n_sweeps) {
         double* slot = S.red_out.p + 2 * width * ridx;
-        if (use_graphs && s + k <= n_sweeps) {
+        // With trimmed arcs the first sweep of the call is cold, so the first
+        // report chunk runs launch by launch; captured chunks are warm.
+        if (use_graphs && s % k == 0 && s + k <= n_sweeps && !(S.n_arc > 0 && s == 0)) {
             Session::ChunkGraph& g = chunk_graph<KIND>(S, k, per_mesh, delta, omega, xin, xout);
             EGG_CK(cudaGraphLaunch(g.exec, S.stream));
             S.launches += g.launches;
@@ -1349,7 +1356,7 @@ template <int KIND> static void run_impl(Session& S, int n_sweeps, double delta,
             ++ridx;
             continue;
         }
-        sweep_once<KIND>(S, xin, xout, delta, omega);
+        sweep_once<KIND>(S, xin, xout, delta, omega, s == 0);
         if ((s + 1) % k == 0 || s == n_sweeps - 1) {
             launch_broadcast(S, S, xout);
             launch_report<KIND>(S, xout, delta, per_mesh, slot);
@@ -1521,11 +1528,12 @@ template <int KIND> __global__ void patch_eval_kernel(StoredPatch2 sp, const dou
 
 __global__ void newton_step_kernel(const double* g, const double* h, double* out) { solve2<double>(h, g, out); }
 
-// in: record[4], grad[2], hess[4], pos[2]; out: step[2], foot[2]
+// in: record[EGG_B200_ENTITY_FIELDS], grad[2], hess[4], pos[2]; out: step[2], foot[2]
 __global__ void entity_step_kernel(int tag, const double* in, double* out)
 {
-    entity_newton_step(tag, in, in + 6, in + 4, in[10], in[11], out);
-    entity_project(tag, in, in[10], in[11], out[2], out[3]);
+    constexpr int R = EGG_B200_ENTITY_FIELDS;
+    entity_newton_step(tag, in, in + R + 2, in + R, in[R + 6], in[R + 7], out);
+    entity_project(tag, in, in[R + 6], in[R + 7], out[2], out[3]);
 }
 
 template <class F> static int guarded(F&& f)
@@ -2315,13 +2323,14 @@ int egg_b200_entity_step(int32_t tag, const double* record, const double* grad, 
         if (!record || !grad || !hess || !pos || !step || !foot) { invalid("entity_step: NULL argument"); }
         if (!entity_supported(2, tag)) {
             throw Error(EGG_B200_ENOTSUP, "entity_step: entity tag " + std::to_string(tag) +
-                                            " is not supported (2D LineSeg, Circle, Ellipse and LineRail are)");
+                                            " is not supported (2D LineSeg, Circle, Ellipse, CircleArc and LineRail are)");
         }
-        std::vector<double> in(12);
-        std::copy(record, record + EGG_B200_ENTITY_FIELDS, in.begin());
-        std::copy(grad, grad + 2, in.begin() + 4);
-        std::copy(hess, hess + 4, in.begin() + 6);
-        std::copy(pos, pos + 2, in.begin() + 10);
+        constexpr int R = EGG_B200_ENTITY_FIELDS;
+        std::vector<double> in(R + 8);
+        std::copy(record, record + R, in.begin());
+        std::copy(grad, grad + 2, in.begin() + R);
+        std::copy(hess, hess + 4, in.begin() + R + 2);
+        std::copy(pos, pos + 2, in.begin() + R + 6);
         DevBuf<double> din, dout;
         din.upload(in);
         dout.alloc(4);

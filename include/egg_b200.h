@@ -41,14 +41,15 @@ extern "C" {
 #define EGG_B200_PREC_MIXED 1
 
 /* Entity tags of constrained DOFs: the reference's frozen wire values
- * (src/entity_soa.hpp:37-56 EntityTag).  This core relaxes the closed-form 2D
- * curves below; other tags are rejected with EGG_B200_ENOTSUP. */
+ * (src/entity_soa.hpp:37-56 EntityTag).  This core relaxes the 2D curves
+ * below; other tags are rejected with EGG_B200_ENOTSUP. */
 #define EGG_B200_TAG_FREE 0
 #define EGG_B200_TAG_LINESEG 1   /* record (sx, sy, ex, ey): segment, projection clamped to it */
 #define EGG_B200_TAG_CIRCLE 2    /* record (cx, cy, r, -): radial projection */
 #define EGG_B200_TAG_ELLIPSE 3   /* record (cx, cy, rx, ry): axis-aligned, radial-scaling projection */
+#define EGG_B200_TAG_CIRCLEARC 6 /* record (cx, cy, r, t0, t1, closed): trimmed circular arc, angles in radians */
 #define EGG_B200_TAG_LINERAIL 15 /* record (sx, sy, ex, ey): open-ended segment, released beyond its ends */
-#define EGG_B200_ENTITY_FIELDS 4 /* reals per entity record in entity_params */
+#define EGG_B200_ENTITY_FIELDS 8 /* reals per entity record in entity_params */
 
 typedef struct egg_b200_session egg_b200_session;
 
@@ -114,11 +115,13 @@ typedef struct egg_b200_session_desc {
     /* Entity record of every constrained DOF, EGG_B200_ENTITY_FIELDS reals
      * per DOF in group order (rows of Free DOFs are ignored): the DOF's row of
      * its entity partition's packed SoA records (src/entity_soa.hpp:98-108,
-     * src/geometry.hpp:1760-1928 EntitySoA<E>::load), zero-padded.  NULL when
+     * src/geometry.hpp:1760-1965 EntitySoA<E>::load), zero-padded.  NULL when
      * every DOF is Free.  A constrained DOF takes the reference's
      * boundary-kernel step (src/sweep.hpp:1286-1403): the Newton step reduced
      * onto the entity tangent, damped by omega before the line search, every
-     * trial projected onto the entity. */
+     * trial projected onto the entity.  A trimmed arc does so on the first
+     * sweep of each run call; later sweeps search in its angle instead
+     * (src/sweep.hpp:1718-1876). */
     const double* entity_params; /* [ndof * EGG_B200_ENTITY_FIELDS] or NULL */
 } egg_b200_session_desc;
 

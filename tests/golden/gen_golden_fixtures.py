@@ -139,6 +139,7 @@ CASES_CON = {
     "disk_ellipse17": ("disk_on_curve", dict(n=17, seed=4, ry=0.6)),
     "square_slide17": ("square_sliding", dict(n=17, seed=5)),
     "disk_circle33": ("disk_on_curve", dict(n=33, seed=6)),
+    "disk_arcs17": ("disk_on_curve", dict(n=17, seed=7, arcs=True)),
 }
 RUNS_CON = [
     # (case, phase, delta, omega, n_sweeps)
@@ -148,18 +149,22 @@ RUNS_CON = [
     ("square_slide17", "shape_size", 0.0, 0.8, 20),
     ("disk_circle33", "barrier", 0.0, 1.0, 30),
     ("disk_circle17", "untangle", 1e-3, 0.5, 10),
+    ("disk_arcs17", "barrier", 0.0, 1.0, 30),
+    ("disk_arcs17", "barrier", 0.0, 0.8, 30),
 ]
 # FAS V-cycles on sliding-boundary grids: (case, phase, n_cycles, nu_pre, nu_post, nu_coarse, omega, max_levels)
 FAS_RUNS_CON = [
     ("disk_circle33", "barrier", 4, 2, 2, 32, 0.8, 32),
     ("square_slide17", "barrier", 4, 2, 2, 32, 1.0, 32),
     ("disk_ellipse17", "barrier", 3, 2, 2, 32, 1.0, 3),
+    ("disk_arcs17", "barrier", 3, 2, 2, 32, 1.0, 32),
 ]
 ENTITY_RECORDS = {
     1: (0.1, -0.2, 0.9, 0.4),
     2: (0.2, -0.1, 0.7, 0.0),
     3: (-0.1, 0.3, 0.8, 0.45),
     15: (0.0, 0.0, 0.6, 0.3),
+    6: (0.1, -0.05, 0.8, -2.6, 1.9, 0.0),
 }
 
 
@@ -201,9 +206,18 @@ def _constrained_runs() -> dict:
         out[key + "/E"] = E
         out[key + "/M"] = M
         out[key + "/X"] = sess.get_X()
+    # a session run in two calls: each call's first sweep projects cold
+    g = case_grid("disk_arcs17")
+    sess = ref.CppStructuredSweepSession(g.wire(), g.structured(), g.X_flat(), device="cpu", dim=2)
+    e_a, _ = sess.run(10, report_every=1)
+    e_b, _ = sess.run(20, report_every=1)
+    out["twocalls/disk_arcs17/E"] = np.concatenate([e_a, e_b])
+    out["twocalls/disk_arcs17/X"] = sess.get_X()
     rng = np.random.default_rng(31)
     for tag, rec in ENTITY_RECORDS.items():
-        kf = 3 if tag == 2 else 4
+        from egg_b200.wire import ENTITY_KINDS
+
+        kf = ENTITY_KINDS[tag][1]
         params = np.array(rec[:kf])
         G = rng.normal(size=(64, 2))
         G[:4] *= 1e-17  # below the zero-gradient guard

@@ -40,16 +40,17 @@ def test_wire_partitions_cover_every_dof_once(grid):
 def test_entity_geometry_matches_the_reference_core(tmp_path):
     """Newton step reduced onto the tangent (a released rail: the full step;
     zero gradient: no step; a singular reduced system: the -0.1 g/|g|
-    fallback) and the projection, for LineSeg, Circle, Ellipse, LineRail."""
+    fallback) and the projection, for LineSeg, Circle, Ellipse, CircleArc
+    (cold: the foot re-represented nearest the trim, then clamped) and LineRail."""
     gxx = shutil.which("g++")
     if gxx is None:
         pytest.skip("no host C++ compiler")
     exe = tmp_path / "entity"
     subprocess.run([gxx, "-O1", "-std=c++17", f"-I{ROOT / 'egg_b200' / 'csrc'}", f"-I{ROOT / 'include'}",
                     str(ROOT / "tests" / "native" / "entity_check.cpp"), "-o", str(exe)], check=True)
-    for tag in (1, 2, 3, 15):
+    for tag in (1, 2, 3, 6, 15):
         k = f"entity/{tag}/"
-        rec = np.zeros(4)
+        rec = np.zeros(8)
         rec[: len(_FX[k + "params"])] = _FX[k + "params"]
         lines = []
         for i in range(len(_FX[k + "pos"])):
@@ -79,9 +80,9 @@ def test_unsupported_entity_tag_is_rejected(core):
     g, ctx, st, X = _square()
     part = ctx["groups"][0]["entities"]["line_seg"]
     n = len(part["dof_local"])
-    ctx6 = _with_part(ctx, "line_seg", {"tag": 6, "kFields": 6, "records": np.zeros(6 * n)})  # CircleArc
-    with pytest.raises(NotImplementedError, match="tag 6"):
-        core.CppStructuredSweepSession(ctx6, st, X)
+    ctx7 = _with_part(ctx, "line_seg", {"tag": 7, "kFields": 8, "records": np.zeros(8 * n)})  # EllipseArc
+    with pytest.raises(NotImplementedError, match="tag 7"):
+        core.CppStructuredSweepSession(ctx7, st, X)
 
 
 def test_malformed_entity_records_are_rejected(core):

@@ -1,5 +1,5 @@
 """Constrained boundary DOFs on the GPU: nodes sliding on a Circle, an
-Ellipse, LineSegs and a LineRail relax exactly as the reference core relaxes
+Ellipse, trimmed CircleArcs, LineSegs and a LineRail relax exactly as the reference core relaxes
 them (first sweep and trajectory, fp64), the mixed path tracks that, every
 accepted boundary node lies on its entity, a batch of constrained meshes
 equals separate sessions, and FAS V-cycles on such grids match the reference."""
@@ -51,7 +51,7 @@ def test_constrained_sweeps_match_reference(gpu, run):
     assert np.abs(s2.get_X() - _FX[key + "/Xn"]).max() <= 1e-9 * _hmin(g)
 
 
-@pytest.mark.parametrize("case", ["disk_circle17", "disk_ellipse17", "square_slide17"])
+@pytest.mark.parametrize("case", ["disk_circle17", "disk_ellipse17", "square_slide17", "disk_arcs17"])
 def test_accepted_boundary_nodes_lie_on_their_entity(gpu, case):
     g = case_grid(case)
     s = _session(gpu, g)
@@ -69,6 +69,28 @@ def test_accepted_boundary_nodes_lie_on_their_entity(gpu, case):
     assert moved > len(g.constraints) // 2
 
 
+def test_arcs_cold_first_sweep_per_call_and_graph_chunks(gpu):
+    """Trimmed arcs project in world space on the first sweep of each run
+    call and search in their angle afterwards: reports every 5 sweeps (the
+    later chunks replay captured graphs) give the reference's trajectory, and
+    a session run in two calls (10 + 20 sweeps) follows the reference
+    session's two calls, which differ from one 30-sweep call."""
+    g = case_grid("disk_arcs17")
+    E30 = _FX["disk_arcs17/barrier/1.0/E"]
+    s = _session(gpu, g)
+    E, _ = s.run(30, report_every=5)
+    np.testing.assert_allclose(E, E30[4::5], rtol=1e-9)
+    assert np.abs(s.get_X() - _FX["disk_arcs17/barrier/1.0/Xn"]).max() <= 1e-9 * _hmin(g)
+    s2 = _session(gpu, g)
+    ea, _ = s2.run(10, report_every=1)
+    eb, _ = s2.run(20, report_every=4)
+    two = _FX["twocalls/disk_arcs17/E"]
+    np.testing.assert_allclose(ea, two[:10], rtol=1e-9)
+    np.testing.assert_allclose(eb, two[10:][3::4], rtol=1e-9)
+    assert np.abs(s2.get_X() - _FX["twocalls/disk_arcs17/X"]).max() <= 1e-9 * _hmin(g)
+    assert abs(two[-1] - E30[-1]) > 1e-6 * abs(E30[-1])
+
+
 @pytest.mark.parametrize("case", ["disk_circle33", "square_slide17"])
 def test_constrained_mixed_tracks_fp64(gpu, case):
     g = case_grid(case)
@@ -82,7 +104,8 @@ def test_constrained_mixed_tracks_fp64(gpu, case):
 
 
 def test_constrained_batch_equals_separate_sessions(gpu):
-    gs = [case_grid("disk_circle17"), case_grid("square_slide17"), case_grid("disk_ellipse17")]
+    gs = [case_grid("disk_circle17"), case_grid("square_slide17"), case_grid("disk_ellipse17"),
+          case_grid("disk_arcs17")]
     b = gpu.CppBatchSweepSession([(g.wire(compact=True), g.structured(), g.X_flat()) for g in gs],
                                  precision="mixed")
     b.set_variant(1)
