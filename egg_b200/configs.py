@@ -30,7 +30,7 @@ from . import wire as _wire
 
 __all__ = [
     "Grid", "unit_square", "disk_oh", "tangled_square", "unit_cube", "two_cubes", "sphere_in_cube",
-    "grid_mindet", "mean_size_w_inv", "disk_on_curve", "square_sliding",
+    "grid_mindet", "mean_size_w_inv", "disk_on_curve", "square_sliding", "cube_sliding",
 ]
 
 
@@ -267,6 +267,43 @@ def unit_cube(n: int, frac: float = 0.2, seed: int = 0) -> Grid:
     if frac > 0:
         X[free] += rng.uniform(-frac * h, frac * h, size=(int(free.sum()), 3))
     return Grid(f"cube{n}", 3, [ids], X, free, {"h": h, "frac": frac, "seed": seed})
+
+
+def cube_sliding(n: int = 9, frac: float = 0.2, slide: float = 0.3, off: float = 0.02, seed: int = 0,
+                 rail_end: float = 0.6) -> Grid:
+    """Unit cube whose face nodes slide on their planes (Plane entities, tag 5)
+    on four faces: x = 0, x = 1, y = 0, and z = 1 with in-plane axes rotated
+    by 0.3 rad.  The nodes of the edge y = z = 0 slide on a LineRail3 (tag 16)
+    from x = 0 to ``rail_end``, so those beyond it are released.  The faces
+    y = 1 and z = 0 and the other edges stay fixed.  Face and edge nodes move
+    along their entity by up to ``slide`` h and off it by up to ``off`` h."""
+    g = unit_cube(n, frac=frac, seed=seed)
+    ids = g.blocks[0]
+    X = g.X.copy()
+    h = 1.0 / (n - 1)
+    rng = np.random.default_rng(seed + 303)
+    c, sn = np.cos(0.3), np.sin(0.3)
+    inner = slice(1, -1)
+    faces = [
+        (ids[0, inner, inner], 0, (0.0, 0, 0, 0, 1, 0, 0, 0, 1)),
+        (ids[-1, inner, inner], 0, (1.0, 0, 0, 0, 1, 0, 0, 0, 1)),
+        (ids[inner, 0, inner], 1, (0.0, 0, 0, 1, 0, 0, 0, 0, 1)),
+        (ids[inner, inner, -1], 2, (0.0, 0, 1, c, sn, 0, -sn, c, 0)),
+    ]
+    cons = {}
+    for nodes, normal, rec in faces:
+        nodes = nodes.reshape(-1)
+        for ax in range(3):
+            amp = off if ax == normal else slide
+            X[nodes, ax] += rng.uniform(-amp, amp, nodes.size) * h
+        for v in nodes:
+            cons[int(v)] = (5, tuple(float(x) for x in rec))
+    edge = ids[inner, 0, 0].reshape(-1)
+    X[edge, 0] += rng.uniform(-slide, slide, edge.size) * h
+    X[edge, 1:] += rng.uniform(-off, off, (edge.size, 2)) * h
+    for v in edge:
+        cons[int(v)] = (16, (0.0, 0.0, 0.0, rail_end, 0.0, 0.0))
+    return Grid(f"cube_slide{n}", 3, g.blocks, X, g.free.copy(), {"frac": frac, "seed": seed}, cons)
 
 
 def two_cubes(n: int, frac: float = 0.2, seed: int = 0) -> Grid:

@@ -126,7 +126,7 @@ struct LevelData {
     DevBuf<double> st_W, st_wt;
     int st_wstride = 0, st_wtstride = 0;
     int64_t n_constrained = 0;  // stored DOFs on a boundary entity
-    int64_t n_arc = 0;          // of which on a trimmed arc (cold first sweep per run call)
+    int64_t n_arc = 0;          // of which on a parametric entity (arc, plane: cold first sweep per run call)
     DevBuf<int8_t> st_etag;     // [n_stored] entity tag (uploaded when n_constrained > 0)
     DevBuf<double> st_epar;     // [n_stored * EGG_B200_ENTITY_FIELDS] entity records
     int64_t nshare = 0;
@@ -591,7 +591,7 @@ static Session* create_session(const egg_b200_session_desc& d)
             if (!entity_supported(D, etag)) {
                 throw Error(EGG_B200_ENOTSUP, "egg_b200: constrained entity tag " + std::to_string(etag) +
                                                 " is not supported in " + std::to_string(D) +
-                                                "D (this core relaxes the 2D LineSeg, Circle, Ellipse, CircleArc and LineRail)");
+                                                "D (this core relaxes the 2D LineSeg, Circle, Ellipse, CircleArc, LineRail and the 3D Plane, LineRail3)");
             }
             if (!d.entity_params) { invalid("validate_context: constrained DOF without entity_params"); }
             for (int f = 0; f < EGG_B200_ENTITY_FIELDS; ++f) {
@@ -633,7 +633,7 @@ static Session* create_session(const egg_b200_session_desc& d)
             st_epar.push_back(etag != 0 ? d.entity_params[i * EGG_B200_ENTITY_FIELDS + f] : 0.0);
         }
         if (etag != 0) { S->n_constrained++; }
-        if (etag == EGG_B200_TAG_CIRCLEARC) { S->n_arc++; }
+        if (etag == EGG_B200_TAG_CIRCLEARC || etag == EGG_B200_TAG_PLANE) { S->n_arc++; }
         for (int64_t p = p0; p < p0 + P; ++p) {
             auto remap = [&](int32_t g) {
                 const int32_t s = S->g2s[g];
@@ -1073,7 +1073,9 @@ static void launch_stored(Session& S, LevelData& L, const double* xin, double* x
     if (S.dim == 3) {
         StoredPatch3 sp {L.n_stored, L.st_slot.p, L.st_off.p, L.st_gc.p,  L.st_gn0.p, L.st_gn1.p,
                          L.st_gn2.p, L.st_s0.p,   L.st_s1.p,  L.st_s2.p, L.st_role.p, L.st_W.p,
-                         L.st_wstride, L.st_wt.p, L.st_wtstride};
+                         L.st_wstride, L.st_wt.p, L.st_wtstride,
+                         L.n_constrained ? L.st_etag.p : nullptr, L.n_constrained ? L.st_epar.p : nullptr,
+                         cold ? 1 : 0};
         S.timed(kKStored, [&] {
             switch (G) {
             case 32: stored3_kernel<KIND, 32><<<grid, 128, 0, st>>>(sp, xin, xout, tau, delta, omega, gout); break;
@@ -1339,7 +1341,7 @@ template <int KIND> static void run_impl(Session& S, int n_sweeps, double delta,
     int s = 0;
     while (s < n_sweeps) {
         double* slot = S.red_out.p + 2 * width * ridx;
-        // With trimmed arcs the first sweep of the call is cold, so the first
+        // With arcs or planes the first sweep of the call is cold, so the first
         // report chunk runs launch by launch; captured chunks are warm.
         if (use_graphs && s % k == 0 && s + k <= n_sweeps && !(S.n_arc > 0 && s == 0)) {
             Session::ChunkGraph& g = chunk_graph<KIND>(S, k, per_mesh, delta, omega, xin, xout);

@@ -41,7 +41,7 @@ extern "C" {
 #define EGG_B200_PREC_MIXED 1
 
 /* Entity tags of constrained DOFs: the reference's frozen wire values
- * (src/entity_soa.hpp:37-56 EntityTag).  This core relaxes the 2D curves
+ * (src/entity_soa.hpp:37-56 EntityTag).  This core relaxes the entities
  * below; other tags are rejected with EGG_B200_ENOTSUP. */
 #define EGG_B200_TAG_FREE 0
 #define EGG_B200_TAG_LINESEG 1   /* record (sx, sy, ex, ey): segment, projection clamped to it */
@@ -49,7 +49,9 @@ extern "C" {
 #define EGG_B200_TAG_ELLIPSE 3   /* record (cx, cy, rx, ry): axis-aligned, radial-scaling projection */
 #define EGG_B200_TAG_CIRCLEARC 6 /* record (cx, cy, r, t0, t1, closed): trimmed circular arc, angles in radians */
 #define EGG_B200_TAG_LINERAIL 15 /* record (sx, sy, ex, ey): open-ended segment, released beyond its ends */
-#define EGG_B200_ENTITY_FIELDS 8 /* reals per entity record in entity_params */
+#define EGG_B200_TAG_PLANE 5     /* 3D record (o(3), ax(3), ay(3)): untrimmed plane, orthonormal in-plane axes */
+#define EGG_B200_TAG_LINERAIL3 16 /* 3D record (s(3), e(3)): open-ended segment, released beyond its ends */
+#define EGG_B200_ENTITY_FIELDS 10 /* reals per entity record in entity_params */
 
 typedef struct egg_b200_session egg_b200_session;
 

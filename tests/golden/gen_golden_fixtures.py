@@ -140,6 +140,7 @@ CASES_CON = {
     "square_slide17": ("square_sliding", dict(n=17, seed=5)),
     "disk_circle33": ("disk_on_curve", dict(n=33, seed=6)),
     "disk_arcs17": ("disk_on_curve", dict(n=17, seed=7, arcs=True)),
+    "cube_slide9": ("cube_sliding", dict(n=9, seed=8)),
 }
 RUNS_CON = [
     # (case, phase, delta, omega, n_sweeps)
@@ -151,6 +152,9 @@ RUNS_CON = [
     ("disk_circle17", "untangle", 1e-3, 0.5, 10),
     ("disk_arcs17", "barrier", 0.0, 1.0, 30),
     ("disk_arcs17", "barrier", 0.0, 0.8, 30),
+    ("cube_slide9", "barrier", 0.0, 1.0, 20),
+    ("cube_slide9", "barrier", 0.0, 0.8, 20),
+    ("cube_slide9", "shape_size", 0.0, 1.0, 10),
 ]
 # FAS V-cycles on sliding-boundary grids: (case, phase, n_cycles, nu_pre, nu_post, nu_coarse, omega, max_levels)
 FAS_RUNS_CON = [
@@ -158,6 +162,7 @@ FAS_RUNS_CON = [
     ("square_slide17", "barrier", 4, 2, 2, 32, 1.0, 32),
     ("disk_ellipse17", "barrier", 3, 2, 2, 32, 1.0, 3),
     ("disk_arcs17", "barrier", 3, 2, 2, 32, 1.0, 32),
+    ("cube_slide9", "barrier", 3, 2, 2, 16, 1.0, 32),
 ]
 ENTITY_RECORDS = {
     1: (0.1, -0.2, 0.9, 0.4),
@@ -189,9 +194,9 @@ def _constrained_runs() -> dict:
         g = case_grid(case)
         ctx, st = g.wire(), g.structured()
         X1, e1, m1 = ref.cpp_structured_sweep(ctx, st, g.X_flat(), 1, device="cpu", phase=phase,
-                                               delta=delta, omega=omega, report_every=1, dim=2)
+                                               delta=delta, omega=omega, report_every=1, dim=g.d)
         Xn, en, mn = ref.cpp_structured_sweep(ctx, st, g.X_flat(), n, device="cpu", phase=phase,
-                                               delta=delta, omega=omega, report_every=1, dim=2)
+                                               delta=delta, omega=omega, report_every=1, dim=g.d)
         key = f"{case}/{phase}/{omega}"
         out[key + "/X1"] = X1
         out[key + "/Xn"] = Xn
@@ -199,13 +204,14 @@ def _constrained_runs() -> dict:
         out[key + "/M"] = mn
     for case, phase, nc, npre, npost, ncoarse, omega, ml in FAS_RUNS_CON:
         g = case_grid(case)
-        sess = ref.CppStructuredSweepSession(g.wire(), g.structured(), g.X_flat(), device="cpu", dim=2)
+        sess = ref.CppStructuredSweepSession(g.wire(), g.structured(), g.X_flat(), device="cpu", dim=g.d)
         E, M = sess.run_fas(nc, nu_pre=npre, nu_post=npost, nu_coarse=ncoarse, omega=omega, max_levels=ml,
                             phase=phase)
         key = f"fas/{case}/{phase}/{ml}"
         out[key + "/E"] = E
         out[key + "/M"] = M
         out[key + "/X"] = sess.get_X()
+    rng3 = np.random.default_rng(37)
     # a session run in two calls: each call's first sweep projects cold
     g = case_grid("disk_arcs17")
     sess = ref.CppStructuredSweepSession(g.wire(), g.structured(), g.X_flat(), device="cpu", dim=2)
@@ -213,6 +219,20 @@ def _constrained_runs() -> dict:
     e_b, _ = sess.run(20, report_every=1)
     out["twocalls/disk_arcs17/E"] = np.concatenate([e_a, e_b])
     out["twocalls/disk_arcs17/X"] = sess.get_X()
+    g = case_grid("cube_slide9")
+    sess = ref.CppStructuredSweepSession(g.wire(), g.structured(), g.X_flat(), device="cpu", dim=3)
+    e_a, _ = sess.run(5, report_every=1)
+    e_b, _ = sess.run(10, report_every=1)
+    out["twocalls/cube_slide9/E"] = np.concatenate([e_a, e_b])
+    out["twocalls/cube_slide9/X"] = sess.get_X()
+    # 3D projections: the reference's own batched projection
+    c, sn = np.cos(0.4), np.sin(0.4)
+    for tag, rec in ((5, (0.1, -0.2, 0.3, c, sn, 0.0, 0.0, 0.0, 1.0)), (16, (0.1, 0.0, -0.1, 0.7, 0.3, 0.2))):
+        Q = rng3.uniform(-0.5, 1.2, size=(64, 3))
+        feet, _basis = ref.geometry_project_batch(Q, tag, np.array(rec), [])
+        out[f"entity3/{tag}/params"] = np.array(rec)
+        out[f"entity3/{tag}/pos"] = Q
+        out[f"entity3/{tag}/foot"] = np.asarray(feet)
     rng = np.random.default_rng(31)
     for tag, rec in ENTITY_RECORDS.items():
         from egg_b200.wire import ENTITY_KINDS

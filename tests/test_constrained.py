@@ -19,7 +19,8 @@ _FX = np.load(GOLDEN / "ref_constrained.npz")
 
 
 @pytest.mark.parametrize("grid", [configs.disk_on_curve(9), configs.disk_on_curve(9, ry=0.6),
-                                  configs.square_sliding(9)], ids=lambda g: g.name)
+                                  configs.disk_on_curve(9, arcs=True), configs.square_sliding(9),
+                                  configs.cube_sliding(5)], ids=lambda g: g.name)
 def test_wire_partitions_cover_every_dof_once(grid):
     grp = grid.wire()["groups"][0]
     seen = np.zeros(grp["D"], dtype=int)
@@ -61,6 +62,27 @@ def test_entity_geometry_matches_the_reference_core(tmp_path):
         got = np.array([[float(x) for x in ln.split()] for ln in out.strip().split("\n")])
         np.testing.assert_allclose(got[:, :2], _FX[k + "step"], rtol=1e-12, atol=1e-15)
         np.testing.assert_allclose(got[:, 2:], _FX[k + "foot"], rtol=1e-12, atol=1e-15)
+
+
+def test_entity3_projection_matches_the_reference_core(tmp_path):
+    """Plane (in-plane coordinates, then evaluated) and LineRail3 (released
+    beyond its ends) projections against the reference's batched projection."""
+    gxx = shutil.which("g++")
+    if gxx is None:
+        pytest.skip("no host C++ compiler")
+    exe = tmp_path / "entity3"
+    subprocess.run([gxx, "-O1", "-std=c++17", f"-I{ROOT / 'egg_b200' / 'csrc'}", f"-I{ROOT / 'include'}",
+                    str(ROOT / "tests" / "native" / "entity3_check.cpp"), "-o", str(exe)], check=True)
+    for tag in (5, 16):
+        k = f"entity3/{tag}/"
+        rec = np.zeros(10)
+        rec[: len(_FX[k + "params"])] = _FX[k + "params"]
+        lines = [" ".join([str(tag), *(repr(float(v)) for v in rec), *(repr(float(v)) for v in q)])
+                 for q in _FX[k + "pos"]]
+        out = subprocess.run([str(exe)], input="\n".join(lines) + "\n", capture_output=True, text=True,
+                             check=True).stdout
+        got = np.array([[float(x) for x in ln.split()] for ln in out.strip().split("\n")])
+        np.testing.assert_allclose(got, _FX[k + "foot"], rtol=1e-12, atol=1e-15)
 
 
 def _square():

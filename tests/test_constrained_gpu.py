@@ -1,5 +1,6 @@
 """Constrained boundary DOFs on the GPU: nodes sliding on a Circle, an
-Ellipse, trimmed CircleArcs, LineSegs and a LineRail relax exactly as the reference core relaxes
+Ellipse, trimmed CircleArcs, LineSegs, a LineRail, Planes and a LineRail3
+relax exactly as the reference core relaxes
 them (first sweep and trajectory, fp64), the mixed path tracks that, every
 accepted boundary node lies on its entity, a batch of constrained meshes
 equals separate sessions, and FAS V-cycles on such grids match the reference."""
@@ -23,7 +24,8 @@ def _hmin(g):
 
 
 def _session(core, g, precision="fp64", compact=False):
-    return core.CppStructuredSweepSession(g.wire(compact=compact), g.structured(), g.X_flat(), precision=precision)
+    return core.CppStructuredSweepSession(g.wire(compact=compact), g.structured(), g.X_flat(), dim=g.d,
+                                          precision=precision)
 
 
 @pytest.mark.parametrize("tag", sorted(ENTITY_RECORDS))
@@ -91,14 +93,43 @@ def test_arcs_cold_first_sweep_per_call_and_graph_chunks(gpu):
     assert abs(two[-1] - E30[-1]) > 1e-6 * abs(E30[-1])
 
 
-@pytest.mark.parametrize("case", ["disk_circle33", "square_slide17"])
+def test_cube_faces_and_edge_stay_on_their_entities_and_restart_cold(gpu):
+    """3D: nodes on Plane faces stay in their planes, nodes on the LineRail3
+    edge stay on its line (or are released beyond its end), and a session run
+    in two calls follows the reference session's two calls (each call's
+    first sweep projects cold)."""
+    g = case_grid("cube_slide9")
+    s = _session(gpu, g)
+    ea, _ = s.run(5, report_every=1)
+    eb, _ = s.run(10, report_every=5)
+    two = _FX["twocalls/cube_slide9/E"]
+    np.testing.assert_allclose(ea, two[:5], rtol=1e-9)
+    np.testing.assert_allclose(eb, two[5:][4::5], rtol=1e-9)
+    X = s.get_X().reshape(-1, 3)
+    assert np.abs(X.ravel() - _FX["twocalls/cube_slide9/X"]).max() <= 1e-9 * _hmin(g)
+    for v, (tag, rec) in g.constraints.items():
+        if np.array_equal(X[v], g.X[v]):
+            continue
+        rec = np.asarray(rec)
+        if tag == 5:
+            nrm = np.cross(rec[3:6], rec[6:9])
+            assert abs(np.dot(X[v] - rec[:3], nrm)) <= 1e-14
+        else:
+            t = np.dot(X[v] - rec[:3], rec[3:6] - rec[:3]) / np.dot(rec[3:6] - rec[:3], rec[3:6] - rec[:3])
+            if 0.0 <= t <= 1.0:
+                np.testing.assert_allclose(X[v], rec[:3] + t * (rec[3:6] - rec[:3]), rtol=0, atol=1e-14)
+
+
+@pytest.mark.parametrize("case", ["disk_circle33", "square_slide17", "cube_slide9"])
 def test_constrained_mixed_tracks_fp64(gpu, case):
     g = case_grid(case)
     key = f"{case}/barrier/1.0"
+    n = len(_FX[key + "/E"])
     s = _session(gpu, g, precision="mixed", compact=True)
     s.run(1)
     assert np.abs(s.get_X() - _FX[key + "/X1"]).max() <= 1e-5 * _hmin(g)
-    E, M = s.run(29, report_every=1)
+    s2 = _session(gpu, g, precision="mixed", compact=True)  # one call: planes restart cold per call
+    E, M = s2.run(n, report_every=1)
     np.testing.assert_allclose(E[-1], _FX[key + "/E"][-1], rtol=1e-5)
     assert np.sign(M[-1]) == np.sign(_FX[key + "/M"][-1])
 
@@ -116,6 +147,17 @@ def test_constrained_batch_equals_separate_sessions(gpu):
         s.set_variant(1)
         s.run(10)
         np.testing.assert_array_equal(Xb[m], s.get_X())
+    g3 = [case_grid("cube_slide9"), configs.cube_sliding(7, seed=11)]
+    b3 = gpu.CppBatchSweepSession([(g.wire(compact=True), g.structured(), g.X_flat()) for g in g3], dim=3,
+                                  precision="mixed")
+    b3.set_variant(1)
+    b3.run(6)
+    Xb3 = b3.get_X()
+    for m, g in enumerate(g3):
+        s = _session(gpu, g, precision="mixed", compact=True)
+        s.set_variant(1)
+        s.run(6)
+        np.testing.assert_array_equal(Xb3[m], s.get_X())
 
 
 @pytest.mark.parametrize("run", FAS_RUNS_CON, ids=lambda r: f"{r[0]}-{r[1]}-{r[7]}")
