@@ -30,7 +30,7 @@ from . import wire as _wire
 
 __all__ = [
     "Grid", "unit_square", "disk_oh", "tangled_square", "unit_cube", "two_cubes", "sphere_in_cube",
-    "grid_mindet", "mean_size_w_inv", "disk_on_curve", "square_sliding", "cube_sliding",
+    "grid_mindet", "mean_size_w_inv", "disk_on_curve", "square_sliding", "cube_sliding", "square_bezier",
 ]
 
 
@@ -151,7 +151,8 @@ def disk_on_curve(n: int = 17, frac: float = 0.25, slide: float = 0.3, off: floa
     outer block's quarter of it instead (CircleArc entities, tag 6, open,
     angle ranges [-pi/4, pi/4], [pi/4, 3pi/4], [3pi/4, 5pi/4] (across the
     +-pi seam) and [-3pi/4, -pi/4]; a node shared by two blocks takes the
-    first one's arc).  Otherwise the disk is squeezed to the axis-aligned
+    first one's arc; with ``ry != 1`` EllipseArc quarters, tag 7, the last
+    one [5pi/4, 7pi/4]).  Otherwise the disk is squeezed to the axis-aligned
     ellipse with semi-axes (1, ry) (Ellipse entity, tag 3).  Every boundary
     node is moved along the curve by up to ``slide`` of its spacing and off it
     by up to ``off`` of the local edge length, so the first sweep also
@@ -172,13 +173,18 @@ def disk_on_curve(n: int = 17, frac: float = 0.25, slide: float = 0.3, off: floa
     cons = {int(b): (tag, rec) for b in bnd}
     kind = "circle" if tag == 2 else "ellipse"
     if arcs:
-        if ry != 1.0:
-            raise ValueError("disk_on_curve: arcs need the circle (ry == 1)")
         cons = {}
-        for blk, t0 in zip(g.blocks[1:], (-0.25 * np.pi, 0.25 * np.pi, 0.75 * np.pi, -0.75 * np.pi)):
+        if ry == 1.0:  # CircleArc quarters
+            starts = (-0.25 * np.pi, 0.25 * np.pi, 0.75 * np.pi, -0.75 * np.pi)
+            ent = lambda t0: (6, (0.0, 0.0, 1.0, t0, t0 + 0.5 * np.pi, 0.0))
+            kind = "arcs"
+        else:  # EllipseArc quarters, parametric angle in [0, 2 pi) except the first
+            starts = (-0.25 * np.pi, 0.25 * np.pi, 0.75 * np.pi, 1.25 * np.pi)
+            ent = lambda t0: (7, (0.0, 0.0, 1.0, ry, 0.0, t0, t0 + 0.5 * np.pi, 0.0))
+            kind = "earcs"
+        for blk, t0 in zip(g.blocks[1:], starts):
             for v in blk[-1, :]:
-                cons.setdefault(int(v), (6, (0.0, 0.0, 1.0, t0, t0 + 0.5 * np.pi, 0.0)))
-        kind = "arcs"
+                cons.setdefault(int(v), ent(t0))
     return Grid(f"disk_{kind}{n}", 2, g.blocks, X, g.free.copy(), {"frac": frac, "seed": seed, "ry": ry}, cons)
 
 
@@ -267,6 +273,35 @@ def unit_cube(n: int, frac: float = 0.2, seed: int = 0) -> Grid:
     if frac > 0:
         X[free] += rng.uniform(-frac * h, frac * h, size=(int(free.sum()), 3))
     return Grid(f"cube{n}", 3, [ids], X, free, {"h": h, "frac": frac, "seed": seed})
+
+
+def _bezier(P: np.ndarray, t: np.ndarray) -> np.ndarray:
+    n = len(P) - 1
+    from math import comb
+
+    return sum(comb(n, i) * ((1 - t) ** (n - i) * t**i)[:, None] * P[i] for i in range(n + 1))
+
+
+def square_bezier(n: int = 17, frac: float = 0.2, slide: float = 0.3, seed: int = 0) -> Grid:
+    """Unit square whose bottom side bends into the quadratic Bezier
+    (0,0)-(0.5,-0.12)-(1,0) (QuadBezier, tag 8) and whose top side into the
+    cubic (0,1)-(0.3,1.15)-(0.7,0.9)-(1,1) (CubicBezier, tag 9), both trimmed
+    to [0, 1]; their nodes sit on the curves at parameters i/(n-1), moved by up
+    to ``slide`` of a step, and slide along them.  Corners stay fixed."""
+    g = unit_square(n, frac=frac, seed=seed)
+    ids = g.blocks[0]
+    X = g.X.copy()
+    rng = np.random.default_rng(seed + 404)
+    t = np.linspace(0.0, 1.0, n)[1:-1] + rng.uniform(-slide, slide, n - 2) / (n - 1)
+    quad = np.array([[0.0, 0.0], [0.5, -0.12], [1.0, 0.0]])
+    cub = np.array([[0.0, 1.0], [0.3, 1.15], [0.7, 0.9], [1.0, 1.0]])
+    cons = {}
+    for nodes, P, tag in ((ids[1:-1, 0], quad, 8), (ids[1:-1, -1], cub, 9)):
+        X[nodes] = _bezier(P, t)
+        rec = tuple(float(x) for x in P.ravel()) + (0.0, 1.0)
+        for v in nodes:
+            cons[int(v)] = (tag, rec)
+    return Grid(f"square_bezier{n}", 2, g.blocks, X, g.free.copy(), {"frac": frac, "seed": seed}, cons)
 
 
 def cube_sliding(n: int = 9, frac: float = 0.2, slide: float = 0.3, off: float = 0.02, seed: int = 0,

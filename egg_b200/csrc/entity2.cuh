@@ -4,8 +4,8 @@
 //   LineRail  (sx, sy, ex, ey)  open-ended: identity beyond its ends :322-360
 //   Circle    (cx, cy, r)       radial projection                   :398-430
 //   Ellipse   (cx, cy, rx, ry)  radial-scaling projection           :432-472
-//   CircleArc (cx, cy, r, t0, t1, closed)  trimmed arc: angle foot,
-//             period re-representation, trim clamp       :129-140,195-229,562-579
+//   trimmed curves (CircleArc, EllipseArc, QuadBezier, CubicBezier): foot,
+//             period re-representation, trim clamp   :129-140,195-229,498-672
 // and the tangent-reduced Newton step of a curve DOF (tangent dimension 1):
 // M = b^T H b, r = b^T g, y = solve1x1(M, r), delta = b y
 // (src/patch.hpp:355-413 newton_step_from_basis / newton_delta,
@@ -31,10 +31,33 @@ EGG_HD double seg_foot(const double* e, double px, double py)
     return ((px - e[0]) * abx + (py - e[1]) * aby) / fmax(ab_sq, kGeomTiny);
 }
 
-// ---- trimmed circular arc, record (cx, cy, r, t0, t1, closed) ---------------
+// ---- trimmed parametric curves -------------------------------------------
+//   CircleArc    (cx, cy, r, t0, t1, closed)           foot: polar angle
+//   EllipseArc   (cx, cy, a, b, phi, t0, t1, closed)    foot: grid + Newton on [0, 2 pi]
+//   QuadBezier   (p0, p1, p2, t0, t1)                   foot: grid + Newton on [0, 1]
+//   CubicBezier  (p0, p1, p2, p3, t0, t1)               foot: grid + Newton on [0, 1]
+// (src/geometry.hpp:498-672, records :1929-2095).  The arcs' angle is
+// periodic: the cold foot takes the representative nearest the trim.
 constexpr double kArcPeriod = 6.283185307179586;  // 2 pi, the angle's period
 
-// Wrap x into [a, b) (a closed arc); unchanged when b <= a.
+EGG_HD bool is_tcurve(int tag)
+{
+    return tag == EGG_B200_TAG_CIRCLEARC || tag == EGG_B200_TAG_ELLIPSEARC || tag == EGG_B200_TAG_QUADBEZIER ||
+           tag == EGG_B200_TAG_CUBICBEZIER;
+}
+
+// Trim (t0, t1, closed) of a curve record.
+EGG_HD void tc_trim(int tag, const double* e, double& t0, double& t1, bool& closed)
+{
+    switch (tag) {
+    case EGG_B200_TAG_CIRCLEARC: t0 = e[3], t1 = e[4], closed = e[5] != 0.0; return;
+    case EGG_B200_TAG_ELLIPSEARC: t0 = e[5], t1 = e[6], closed = e[7] != 0.0; return;
+    case EGG_B200_TAG_QUADBEZIER: t0 = e[6], t1 = e[7], closed = false; return;
+    default: t0 = e[8], t1 = e[9], closed = false; return;
+    }
+}
+
+// Wrap x into [a, b) (a closed curve); unchanged when b <= a.
 EGG_HD double arc_wrap(double x, double a, double b)
 {
     const double L = b - a;
@@ -44,28 +67,132 @@ EGG_HD double arc_wrap(double x, double a, double b)
     return a + t;
 }
 
-EGG_HD bool arc_contains(const double* e, double q) { return e[5] != 0.0 || (q >= e[3] && q <= e[4]); }
-
-EGG_HD double arc_clamp(const double* e, double q)
+EGG_HD bool tc_contains(int tag, const double* e, double q)
 {
-    if (e[5] != 0.0) { return arc_wrap(q, e[3], e[4]); }
-    return q < e[3] ? e[3] : (q > e[4] ? e[4] : q);
+    double t0, t1;
+    bool closed;
+    tc_trim(tag, e, t0, t1, closed);
+    return closed || (q >= t0 && q <= t1);
 }
 
-// Raw foot angle of (px, py): one branch representative.
-EGG_HD double arc_invert(const double* e, double px, double py) { return atan2(py - e[1], px - e[0]); }
-
-EGG_HD void arc_eval(const double* e, double q, double& x, double& y)
+EGG_HD double tc_clamp(int tag, const double* e, double q)
 {
-    x = e[0] + e[2] * cos(q);
-    y = e[1] + e[2] * sin(q);
+    double t0, t1;
+    bool closed;
+    tc_trim(tag, e, t0, t1, closed);
+    if (closed) { return arc_wrap(q, t0, t1); }
+    return q < t0 ? t0 : (q > t1 ? t1 : q);
 }
 
-// Raw tangent column r (-sin q, cos q).
-EGG_HD void arc_frame(const double* e, double q, double& jx, double& jy)
+// Position (nd = 0), first (nd = 1) or second (nd = 2) derivative at t.
+EGG_HD void tc_eval(int tag, const double* e, double t, int nd, double& x, double& y)
 {
-    jx = -e[2] * sin(q);
-    jy = e[2] * cos(q);
+    if (tag == EGG_B200_TAG_CIRCLEARC) {
+        const double c = cos(t), s = sin(t);
+        if (nd == 0) {
+            x = e[0] + e[2] * c;
+            y = e[1] + e[2] * s;
+        } else if (nd == 1) {
+            x = -e[2] * s;
+            y = e[2] * c;
+        } else {
+            x = -e[2] * c;
+            y = -e[2] * s;
+        }
+        return;
+    }
+    if (tag == EGG_B200_TAG_ELLIPSEARC) {
+        const double cp = cos(e[4]), sp = sin(e[4]);
+        double u, v;
+        if (nd == 0) {
+            u = e[2] * cos(t);
+            v = e[3] * sin(t);
+            x = (e[0] + cp * u) - sp * v;
+            y = (e[1] + sp * u) + cp * v;
+            return;
+        }
+        if (nd == 1) {
+            u = -e[2] * sin(t);
+            v = e[3] * cos(t);
+        } else {
+            u = -e[2] * cos(t);
+            v = -e[3] * sin(t);
+        }
+        x = cp * u - sp * v;
+        y = sp * u + cp * v;
+        return;
+    }
+    const double w = 1.0 - t;
+    if (tag == EGG_B200_TAG_QUADBEZIER) {
+        if (nd == 0) {
+            const double b0 = w * w, b1 = 2.0 * w * t, b2 = t * t;
+            x = (b0 * e[0] + b1 * e[2]) + b2 * e[4];
+            y = (b0 * e[1] + b1 * e[3]) + b2 * e[5];
+        } else if (nd == 1) {
+            const double c0 = 2.0 * w, c1 = 2.0 * t;
+            x = c0 * (e[2] - e[0]) + c1 * (e[4] - e[2]);
+            y = c0 * (e[3] - e[1]) + c1 * (e[5] - e[3]);
+        } else {
+            x = 2.0 * ((e[4] - 2.0 * e[2]) + e[0]);
+            y = 2.0 * ((e[5] - 2.0 * e[3]) + e[1]);
+        }
+        return;
+    }
+    // cubic
+    if (nd == 0) {
+        const double b0 = w * w * w, b1 = 3.0 * w * w * t, b2 = 3.0 * w * t * t, b3 = t * t * t;
+        x = ((b0 * e[0] + b1 * e[2]) + b2 * e[4]) + b3 * e[6];
+        y = ((b0 * e[1] + b1 * e[3]) + b2 * e[5]) + b3 * e[7];
+    } else if (nd == 1) {
+        const double c0 = 3.0 * w * w, c1 = 6.0 * w * t, c2 = 3.0 * t * t;
+        x = (c0 * (e[2] - e[0]) + c1 * (e[4] - e[2])) + c2 * (e[6] - e[4]);
+        y = (c0 * (e[3] - e[1]) + c1 * (e[5] - e[3])) + c2 * (e[7] - e[5]);
+    } else {
+        const double c0 = 6.0 * w, c1 = 6.0 * t;
+        x = c0 * ((e[4] - 2.0 * e[2]) + e[0]) + c1 * ((e[6] - 2.0 * e[4]) + e[2]);
+        y = c0 * ((e[5] - 2.0 * e[3]) + e[1]) + c1 * ((e[7] - 2.0 * e[5]) + e[3]);
+    }
+}
+
+// Nearest-foot parameter on [lo, hi]: the best of 17 grid samples, then 8
+// Newton steps on (C(t) - q).C'(t) (src/geometry.hpp:518-560 project_param).
+EGG_HD double tc_grid_newton(int tag, const double* e, double qx, double qy, double lo, double hi)
+{
+    double best_t = lo, best_d = INFINITY;
+    for (int i = 0; i <= 16; ++i) {
+        const double tc = lo + ((hi - lo) * double(i)) / 16.0;
+        double x, y;
+        tc_eval(tag, e, tc, 0, x, y);
+        const double dx = x - qx, dy = y - qy;
+        const double dd = dx * dx + dy * dy;
+        if (dd < best_d) {
+            best_d = dd;
+            best_t = tc;
+        }
+    }
+    double t = best_t;
+    for (int it = 0; it < 8; ++it) {
+        double x, y, d1x, d1y, d2x, d2y;
+        tc_eval(tag, e, t, 0, x, y);
+        tc_eval(tag, e, t, 1, d1x, d1y);
+        tc_eval(tag, e, t, 2, d2x, d2y);
+        const double dx = x - qx, dy = y - qy;
+        const double f = dx * d1x + dy * d1y;
+        const double fp = (d1x * d1x + d1y * d1y) + (dx * d2x + dy * d2y);
+        if (fabs(fp) < kGeomTiny) { break; }
+        t -= f / fp;
+    }
+    return t;
+}
+
+// Raw foot parameter of (px, py): one representative for the arcs.
+EGG_HD double tc_invert(int tag, const double* e, double px, double py)
+{
+    switch (tag) {
+    case EGG_B200_TAG_CIRCLEARC: return atan2(py - e[1], px - e[0]);
+    case EGG_B200_TAG_ELLIPSEARC: return tc_grid_newton(tag, e, px, py, 0.0, kArcPeriod);
+    default: return tc_grid_newton(tag, e, px, py, 0.0, 1.0);
+    }
 }
 
 // Unit vector (1/n) v, or e_0 below the zero-vector guard.
@@ -82,29 +209,32 @@ EGG_HD void unit_or_e0(double vx, double vy, double& ux, double& uy)
     uy = inv * vy;
 }
 
-// Cold foot: the representative nearest the trim interval (open arcs), then
-// clamped onto it.
-EGG_HD double arc_cold_foot(const double* e, double px, double py)
+// Cold foot: for the arcs the representative nearest the trim interval (open
+// trims), then clamped onto the trim.
+EGG_HD double tc_cold_foot(int tag, const double* e, double px, double py)
 {
-    double q = arc_invert(e, px, py);
-    if (e[5] == 0.0) {
-        const double mid = 0.5 * (e[3] + e[4]);
+    double q = tc_invert(tag, e, px, py);
+    double t0, t1;
+    bool closed;
+    tc_trim(tag, e, t0, t1, closed);
+    if ((tag == EGG_B200_TAG_CIRCLEARC || tag == EGG_B200_TAG_ELLIPSEARC) && !closed) {
+        const double mid = 0.5 * (t0 + t1);
         q = mid + remainder(q - mid, kArcPeriod);
     }
-    if (!arc_contains(e, q)) { q = arc_clamp(e, q); }
+    if (!tc_contains(tag, e, q)) { q = tc_clamp(tag, e, q); }
     return q;
 }
 
-// Warm step of an arc DOF (sweeps after the first of a run call): the Newton
-// step on the tangent at the raw foot q*, reduced to an angle step
+// Warm step of a curve DOF (sweeps after the first of a run call): the Newton
+// step on the tangent at the raw foot q*, reduced to a parameter step
 // dq = (J.J)^-1 J.delta and damped by omega; trials are q* + alpha dq,
 // clamped onto the trim and evaluated.
-EGG_HD void arc_warm_step(const double* e, const double H[4], const double g[2], double px, double py, double omega,
-                          double& qstar, double& dq)
+EGG_HD void tc_warm_step(int tag, const double* e, const double H[4], const double g[2], double px, double py,
+                         double omega, double& qstar, double& dq)
 {
-    qstar = arc_invert(e, px, py);
+    qstar = tc_invert(tag, e, px, py);
     double jx, jy, bx, by;
-    arc_frame(e, qstar, jx, jy);
+    tc_eval(tag, e, qstar, 1, jx, jy);
     unit_or_e0(jx, jy, bx, by);
     const double hb0 = H[0] * bx + H[1] * by;
     const double hb1 = H[2] * bx + H[3] * by;
@@ -126,8 +256,8 @@ EGG_HD void arc_warm_step(const double* e, const double H[4], const double g[2],
 // Projection of (px, py) onto the entity.
 EGG_HD void entity_project(int tag, const double* e, double px, double py, double& qx, double& qy)
 {
-    if (tag == EGG_B200_TAG_CIRCLEARC) {
-        arc_eval(e, arc_cold_foot(e, px, py), qx, qy);
+    if (is_tcurve(tag)) {
+        tc_eval(tag, e, tc_cold_foot(tag, e, px, py), 0, qx, qy);
         return;
     }
     if (tag == EGG_B200_TAG_LINESEG || tag == EGG_B200_TAG_LINERAIL) {
@@ -176,9 +306,9 @@ EGG_HD void entity_project(int tag, const double* e, double px, double py, doubl
 // Unit tangent of the entity at (px, py).
 EGG_HD void entity_tangent(int tag, const double* e, double px, double py, double& tx, double& ty)
 {
-    if (tag == EGG_B200_TAG_CIRCLEARC) {  // at the cold foot
+    if (is_tcurve(tag)) {  // at the cold foot
         double jx, jy;
-        arc_frame(e, arc_cold_foot(e, px, py), jx, jy);
+        tc_eval(tag, e, tc_cold_foot(tag, e, px, py), 1, jx, jy);
         unit_or_e0(jx, jy, tx, ty);
         return;
     }
@@ -252,8 +382,7 @@ EGG_HD bool entity_supported(int dim, int tag)
 {
     if (dim == 3) { return tag == EGG_B200_TAG_PLANE || tag == EGG_B200_TAG_LINERAIL3; }
     return dim == 2 && (tag == EGG_B200_TAG_LINESEG || tag == EGG_B200_TAG_CIRCLE ||
-                        tag == EGG_B200_TAG_ELLIPSE || tag == EGG_B200_TAG_LINERAIL ||
-                        tag == EGG_B200_TAG_CIRCLEARC);
+                        tag == EGG_B200_TAG_ELLIPSE || tag == EGG_B200_TAG_LINERAIL || is_tcurve(tag));
 }
 
 }  // namespace egg_b200

@@ -913,18 +913,18 @@ __global__ void stored_patch_kernel(StoredPatch2 sp, const double2* __restrict__
         // onto its entity's tangent, damped by omega before the line search,
         // and every trial projected onto the entity, so the accepted point
         // stays on the geometry.  A Free DOF: the full step, omega blend after.
-        // A trimmed arc after the first sweep of a run call searches in its
-        // angle instead (src/sweep.hpp:1718-1876): trials q* + alpha dq,
-        // clamped onto the trim and evaluated on the arc.
+        // A trimmed curve after the first sweep of a run call searches in its
+        // parameter instead (src/sweep.hpp:1718-1876): trials q* + alpha dq,
+        // clamped onto the trim and evaluated on the curve.
         const int etag = sp.etag != nullptr ? int(sp.etag[d]) : 0;
         const double* er = sp.epar + (etag != 0 ? d * EGG_B200_ENTITY_FIELDS : 0);
-        const bool warm_arc = etag == EGG_B200_TAG_CIRCLEARC && !sp.cold;
+        const bool warm_arc = is_tcurve(etag) && !sp.cold;
         double dl[2] = {0.0, 0.0};
         double qstar = 0.0, dq = 0.0;
         if (etag == 0) {
             solve2<double>(h, g, dl);
         } else if (warm_arc) {
-            arc_warm_step(er, h, g, pos.x, pos.y, omega, qstar, dq);
+            tc_warm_step(etag, er, h, g, pos.x, pos.y, omega, qstar, dq);
         } else {
             entity_newton_step(etag, er, h, g, pos.x, pos.y, dl);
             dl[0] *= omega;
@@ -935,7 +935,7 @@ __global__ void stored_patch_kernel(StoredPatch2 sp, const double2* __restrict__
         for (int it = 0; it < 10; ++it) {
             double2 trial = make_double2(pos.x + alpha * dl[0], pos.y + alpha * dl[1]);
             if (warm_arc) {
-                arc_eval(er, arc_clamp(er, qstar + alpha * dq), trial.x, trial.y);
+                tc_eval(etag, er, tc_clamp(etag, er, qstar + alpha * dq), 0, trial.x, trial.y);
             } else if (etag != 0) {
                 entity_project(etag, er, trial.x, trial.y, trial.x, trial.y);
             }

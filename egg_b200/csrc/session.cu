@@ -591,7 +591,8 @@ static Session* create_session(const egg_b200_session_desc& d)
             if (!entity_supported(D, etag)) {
                 throw Error(EGG_B200_ENOTSUP, "egg_b200: constrained entity tag " + std::to_string(etag) +
                                                 " is not supported in " + std::to_string(D) +
-                                                "D (this core relaxes the 2D LineSeg, Circle, Ellipse, CircleArc, LineRail and the 3D Plane, LineRail3)");
+                                                "D (this core relaxes the 2D LineSeg, Circle, Ellipse, CircleArc, EllipseArc, QuadBezier, CubicBezier, "
+                                                "LineRail and the 3D Plane, LineRail3)");
             }
             if (!d.entity_params) { invalid("validate_context: constrained DOF without entity_params"); }
             for (int f = 0; f < EGG_B200_ENTITY_FIELDS; ++f) {
@@ -633,7 +634,7 @@ static Session* create_session(const egg_b200_session_desc& d)
             st_epar.push_back(etag != 0 ? d.entity_params[i * EGG_B200_ENTITY_FIELDS + f] : 0.0);
         }
         if (etag != 0) { S->n_constrained++; }
-        if (etag == EGG_B200_TAG_CIRCLEARC || etag == EGG_B200_TAG_PLANE) { S->n_arc++; }
+        if (is_tcurve(etag) || etag == EGG_B200_TAG_PLANE) { S->n_arc++; }
         for (int64_t p = p0; p < p0 + P; ++p) {
             auto remap = [&](int32_t g) {
                 const int32_t s = S->g2s[g];
@@ -2325,7 +2326,8 @@ int egg_b200_entity_step(int32_t tag, const double* record, const double* grad, 
         if (!record || !grad || !hess || !pos || !step || !foot) { invalid("entity_step: NULL argument"); }
         if (!entity_supported(2, tag)) {
             throw Error(EGG_B200_ENOTSUP, "entity_step: entity tag " + std::to_string(tag) +
-                                            " is not supported (2D LineSeg, Circle, Ellipse, CircleArc and LineRail are)");
+                                            " is not supported (the 2D curves LineSeg, Circle, Ellipse, CircleArc, EllipseArc, QuadBezier, "
+                                            "CubicBezier and LineRail are)");
         }
         constexpr int R = EGG_B200_ENTITY_FIELDS;
         std::vector<double> in(R + 8);

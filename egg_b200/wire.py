@@ -111,7 +111,8 @@ def free_mask_from_fixed(n_nodes: int, fixed_ids) -> np.ndarray:
 # the reference's frozen tags and packed record widths (src/entity_soa.hpp:37-56,
 # src/geometry.hpp:1760-1928).
 ENTITY_KINDS = {1: ("line_seg", 4), 2: ("circle", 3), 3: ("ellipse", 4), 5: ("plane", 9), 6: ("circle_arc", 6),
-                15: ("line_rail", 4), 16: ("line_rail3", 6)}
+                7: ("ellipse_arc", 8), 8: ("quad_bezier", 8), 9: ("cubic_bezier", 10), 15: ("line_rail", 4),
+                16: ("line_rail3", 6)}
 
 
 def flat_wire(

@@ -48,6 +48,9 @@ extern "C" {
 #define EGG_B200_TAG_CIRCLE 2    /* record (cx, cy, r, -): radial projection */
 #define EGG_B200_TAG_ELLIPSE 3   /* record (cx, cy, rx, ry): axis-aligned, radial-scaling projection */
 #define EGG_B200_TAG_CIRCLEARC 6 /* record (cx, cy, r, t0, t1, closed): trimmed circular arc, angles in radians */
+#define EGG_B200_TAG_ELLIPSEARC 7 /* record (cx, cy, a, b, phi, t0, t1, closed): rotated elliptic arc */
+#define EGG_B200_TAG_QUADBEZIER 8 /* record (p0, p1, p2, t0, t1): quadratic Bezier, trimmed to [t0, t1] */
+#define EGG_B200_TAG_CUBICBEZIER 9 /* record (p0, p1, p2, p3, t0, t1): cubic Bezier, trimmed to [t0, t1] */
 #define EGG_B200_TAG_LINERAIL 15 /* record (sx, sy, ex, ey): open-ended segment, released beyond its ends */
 #define EGG_B200_TAG_PLANE 5     /* 3D record (o(3), ax(3), ay(3)): untrimmed plane, orthonormal in-plane axes */
 #define EGG_B200_TAG_LINERAIL3 16 /* 3D record (s(3), e(3)): open-ended segment, released beyond its ends */

@@ -141,6 +141,8 @@ CASES_CON = {
     "disk_circle33": ("disk_on_curve", dict(n=33, seed=6)),
     "disk_arcs17": ("disk_on_curve", dict(n=17, seed=7, arcs=True)),
     "cube_slide9": ("cube_sliding", dict(n=9, seed=8)),
+    "disk_earcs17": ("disk_on_curve", dict(n=17, seed=9, ry=0.6, arcs=True)),
+    "square_bezier17": ("square_bezier", dict(n=17, seed=10)),
 }
 RUNS_CON = [
     # (case, phase, delta, omega, n_sweeps)
@@ -155,6 +157,9 @@ RUNS_CON = [
     ("cube_slide9", "barrier", 0.0, 1.0, 20),
     ("cube_slide9", "barrier", 0.0, 0.8, 20),
     ("cube_slide9", "shape_size", 0.0, 1.0, 10),
+    ("disk_earcs17", "barrier", 0.0, 1.0, 30),
+    ("square_bezier17", "barrier", 0.0, 1.0, 30),
+    ("square_bezier17", "barrier", 0.0, 0.8, 30),
 ]
 # FAS V-cycles on sliding-boundary grids: (case, phase, n_cycles, nu_pre, nu_post, nu_coarse, omega, max_levels)
 FAS_RUNS_CON = [
@@ -163,6 +168,7 @@ FAS_RUNS_CON = [
     ("disk_ellipse17", "barrier", 3, 2, 2, 32, 1.0, 3),
     ("disk_arcs17", "barrier", 3, 2, 2, 32, 1.0, 32),
     ("cube_slide9", "barrier", 3, 2, 2, 16, 1.0, 32),
+    ("square_bezier17", "barrier", 3, 2, 2, 32, 1.0, 32),
 ]
 ENTITY_RECORDS = {
     1: (0.1, -0.2, 0.9, 0.4),
@@ -170,6 +176,9 @@ ENTITY_RECORDS = {
     3: (-0.1, 0.3, 0.8, 0.45),
     15: (0.0, 0.0, 0.6, 0.3),
     6: (0.1, -0.05, 0.8, -2.6, 1.9, 0.0),
+    7: (0.05, 0.1, 0.9, 0.5, 0.4, -1.0, 2.2, 0.0),
+    8: (-0.2, 0.1, 0.4, 0.9, 1.0, -0.1, 0.1, 0.95),
+    9: (-0.3, -0.2, 0.0, 0.8, 0.7, -0.6, 1.1, 0.3, 0.0, 1.0),
 }
 
 

@@ -19,7 +19,8 @@ _FX = np.load(GOLDEN / "ref_constrained.npz")
 
 
 @pytest.mark.parametrize("grid", [configs.disk_on_curve(9), configs.disk_on_curve(9, ry=0.6),
-                                  configs.disk_on_curve(9, arcs=True), configs.square_sliding(9),
+                                  configs.disk_on_curve(9, arcs=True), configs.disk_on_curve(9, ry=0.6, arcs=True),
+                                  configs.square_sliding(9), configs.square_bezier(9),
                                   configs.cube_sliding(5)], ids=lambda g: g.name)
 def test_wire_partitions_cover_every_dof_once(grid):
     grp = grid.wire()["groups"][0]
@@ -41,17 +42,18 @@ def test_wire_partitions_cover_every_dof_once(grid):
 def test_entity_geometry_matches_the_reference_core(tmp_path):
     """Newton step reduced onto the tangent (a released rail: the full step;
     zero gradient: no step; a singular reduced system: the -0.1 g/|g|
-    fallback) and the projection, for LineSeg, Circle, Ellipse, CircleArc
-    (cold: the foot re-represented nearest the trim, then clamped) and LineRail."""
+    fallback) and the projection, for LineSeg, Circle, Ellipse, LineRail and
+    the trimmed curves CircleArc, EllipseArc, QuadBezier, CubicBezier (cold:
+    the foot re-represented nearest the trim, then clamped)."""
     gxx = shutil.which("g++")
     if gxx is None:
         pytest.skip("no host C++ compiler")
     exe = tmp_path / "entity"
     subprocess.run([gxx, "-O1", "-std=c++17", f"-I{ROOT / 'egg_b200' / 'csrc'}", f"-I{ROOT / 'include'}",
                     str(ROOT / "tests" / "native" / "entity_check.cpp"), "-o", str(exe)], check=True)
-    for tag in (1, 2, 3, 6, 15):
+    for tag in (1, 2, 3, 6, 7, 8, 9, 15):
         k = f"entity/{tag}/"
-        rec = np.zeros(8)
+        rec = np.zeros(10)
         rec[: len(_FX[k + "params"])] = _FX[k + "params"]
         lines = []
         for i in range(len(_FX[k + "pos"])):
@@ -102,9 +104,9 @@ def test_unsupported_entity_tag_is_rejected(core):
     g, ctx, st, X = _square()
     part = ctx["groups"][0]["entities"]["line_seg"]
     n = len(part["dof_local"])
-    ctx7 = _with_part(ctx, "line_seg", {"tag": 7, "kFields": 8, "records": np.zeros(8 * n)})  # EllipseArc
-    with pytest.raises(NotImplementedError, match="tag 7"):
-        core.CppStructuredSweepSession(ctx7, st, X)
+    ctx4 = _with_part(ctx, "line_seg", {"tag": 4, "kFields": 10, "records": np.zeros(10 * n)})  # Sphere
+    with pytest.raises(NotImplementedError, match="tag 4"):
+        core.CppStructuredSweepSession(ctx4, st, X)
 
 
 def test_malformed_entity_records_are_rejected(core):

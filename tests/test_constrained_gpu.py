@@ -1,6 +1,6 @@
 """Constrained boundary DOFs on the GPU: nodes sliding on a Circle, an
-Ellipse, trimmed CircleArcs, LineSegs, a LineRail, Planes and a LineRail3
-relax exactly as the reference core relaxes
+Ellipse, trimmed CircleArcs, EllipseArcs and Beziers, LineSegs, a LineRail,
+Planes and a LineRail3 relax exactly as the reference core relaxes
 them (first sweep and trajectory, fp64), the mixed path tracks that, every
 accepted boundary node lies on its entity, a batch of constrained meshes
 equals separate sessions, and FAS V-cycles on such grids match the reference."""
@@ -30,12 +30,16 @@ def _session(core, g, precision="fp64", compact=False):
 
 @pytest.mark.parametrize("tag", sorted(ENTITY_RECORDS))
 def test_entity_step_and_projection_match_reference(gpu, tag):
+    # The elliptic arc and the Beziers find their foot by 8 Newton iterations,
+    # whose rounding follows each compiler's FMA contraction: 1e-10 there,
+    # 1e-12 for the closed forms.
+    rtol = 1e-10 if tag in (7, 8, 9) else 1e-12
     k = f"entity/{tag}/"
     for i in range(len(_FX[k + "pos"])):
         st = gpu.newton_step(_FX[k + "grad"][i], _FX[k + "hess"][i], _FX[k + "pos"][i], tag, _FX[k + "params"])
-        np.testing.assert_allclose(st, _FX[k + "step"][i], rtol=1e-12, atol=1e-15)
+        np.testing.assert_allclose(st, _FX[k + "step"][i], rtol=rtol, atol=1e-15)
         ft = gpu.entity_project(_FX[k + "pos"][i], tag, _FX[k + "params"])
-        np.testing.assert_allclose(ft, _FX[k + "foot"][i], rtol=1e-12, atol=1e-15)
+        np.testing.assert_allclose(ft, _FX[k + "foot"][i], rtol=rtol, atol=1e-15)
 
 
 @pytest.mark.parametrize("run", RUNS_CON, ids=lambda r: f"{r[0]}-{r[1]}-{r[3]}")
@@ -53,7 +57,8 @@ def test_constrained_sweeps_match_reference(gpu, run):
     assert np.abs(s2.get_X() - _FX[key + "/Xn"]).max() <= 1e-9 * _hmin(g)
 
 
-@pytest.mark.parametrize("case", ["disk_circle17", "disk_ellipse17", "square_slide17", "disk_arcs17"])
+@pytest.mark.parametrize("case", ["disk_circle17", "disk_ellipse17", "square_slide17", "disk_arcs17",
+                                  "disk_earcs17", "square_bezier17"])
 def test_accepted_boundary_nodes_lie_on_their_entity(gpu, case):
     g = case_grid(case)
     s = _session(gpu, g)
@@ -67,7 +72,7 @@ def test_accepted_boundary_nodes_lie_on_their_entity(gpu, case):
         foot = gpu.entity_project(X[v], tag, np.asarray(rec, dtype=np.float64))
         if tag == 15 and not np.allclose(foot, X[v]):
             continue  # a released rail node
-        np.testing.assert_allclose(X[v], foot, rtol=0, atol=1e-14)
+        np.testing.assert_allclose(X[v], foot, rtol=0, atol=1e-13)
     assert moved > len(g.constraints) // 2
 
 
