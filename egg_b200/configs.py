@@ -31,6 +31,7 @@ from . import wire as _wire
 __all__ = [
     "Grid", "unit_square", "disk_oh", "tangled_square", "unit_cube", "two_cubes", "sphere_in_cube",
     "grid_mindet", "mean_size_w_inv", "disk_on_curve", "square_sliding", "cube_sliding", "square_bezier",
+    "cube_curved",
 ]
 
 
@@ -339,6 +340,52 @@ def cube_sliding(n: int = 9, frac: float = 0.2, slide: float = 0.3, off: float =
     for v in edge:
         cons[int(v)] = (16, (0.0, 0.0, 0.0, rail_end, 0.0, 0.0))
     return Grid(f"cube_slide{n}", 3, g.blocks, X, g.free.copy(), {"frac": frac, "seed": seed}, cons)
+
+
+def cube_curved(n: int = 9, frac: float = 0.15, slide: float = 0.3, off: float = 0.02, seed: int = 0) -> Grid:
+    """Unit cube with curved faces whose nodes slide on them: the top face on
+    the sphere of radius 4 about (0.5, 0.5, -3) (Sphere, tag 4), the face
+    x ~ 1 on the cylinder of radius 4 about the z-parallel axis through
+    (-3, 0.5) (Cylinder, tag 12), the face y = 0 on its plane (Plane, tag 5),
+    and the edge y = z = 0 on the line x in [0.05, 0.95] (Line3, tag 13).  The
+    other faces and edges stay fixed.  Nodes move along their entity by up to
+    ``slide`` h and off it by up to ``off`` h."""
+    g = unit_cube(n, frac=frac, seed=seed)
+    ids = g.blocks[0]
+    X = g.X.copy()
+    h = 1.0 / (n - 1)
+    rng = np.random.default_rng(seed + 505)
+    inner = slice(1, -1)
+    cons = {}
+    # cylinder face: x from the cylinder at (y, z)
+    cyl = ids[-1, inner, inner].reshape(-1)
+    X[cyl, 1:] += rng.uniform(-slide, slide, (cyl.size, 2)) * h
+    X[cyl, 0] = -3.0 + np.sqrt(16.0 - (X[cyl, 1] - 0.5) ** 2) + rng.uniform(-off, off, cyl.size) * h
+    for v in cyl:
+        cons[int(v)] = (12, (-3.0, 0.5, 0.0, 1.0, 0.0, 0.0, 0.0, 1.0, 0.0, 4.0))
+    # sphere cap: z from the sphere at (x, y)
+    sph = ids[inner, inner, -1].reshape(-1)
+    X[sph, :2] += rng.uniform(-slide, slide, (sph.size, 2)) * h
+    X[sph, 2] = -3.0 + np.sqrt(16.0 - (X[sph, 0] - 0.5) ** 2 - (X[sph, 1] - 0.5) ** 2)
+    X[sph, 2] += rng.uniform(-off, off, sph.size) * h
+    for v in sph:
+        # chart frame ax = x, ay = z (pole along -y): the cap lies on the chart's
+        # equator, away from the latitude's ill-conditioned poles
+        cons[int(v)] = (4, (0.5, 0.5, -3.0, 4.0, 1.0, 0.0, 0.0, 0.0, 0.0, 1.0))
+    # plane face y = 0
+    pl = ids[inner, 0, inner].reshape(-1)
+    X[pl, 0] += rng.uniform(-slide, slide, pl.size) * h
+    X[pl, 2] += rng.uniform(-slide, slide, pl.size) * h
+    X[pl, 1] += rng.uniform(-off, off, pl.size) * h
+    for v in pl:
+        cons[int(v)] = (5, (0.0, 0.0, 0.0, 1.0, 0.0, 0.0, 0.0, 0.0, 1.0))
+    # edge line y = z = 0, trimmed
+    ed = ids[inner, 0, 0].reshape(-1)
+    X[ed, 0] += rng.uniform(-slide, slide, ed.size) * h
+    X[ed, 1:] += rng.uniform(-off, off, (ed.size, 2)) * h
+    for v in ed:
+        cons[int(v)] = (13, (0.0, 0.0, 0.0, 1.0, 0.0, 0.0, 0.05, 0.95))
+    return Grid(f"cube_curved{n}", 3, g.blocks, X, g.free.copy(), {"frac": frac, "seed": seed}, cons)
 
 
 def two_cubes(n: int, frac: float = 0.2, seed: int = 0) -> Grid:

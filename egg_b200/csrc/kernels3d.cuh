@@ -440,7 +440,7 @@ struct StoredPatch3 {
     int32_t wt_stride;
     const int8_t* etag;  // [n] entity tag of each DOF, or NULL (all Free)
     const double* epar;  // [n * EGG_B200_ENTITY_FIELDS] entity records
-    int cold;            // first sweep of a run call: planes project in world space
+    int cold;            // first sweep of a run call: parametric entities project in world space
 };
 
 __device__ __forceinline__ void assemble_T3(const double* X, int32_t ic, const int32_t in[3], const double s[3],
@@ -536,17 +536,17 @@ __global__ void stored3_kernel(StoredPatch3 sp, const double* __restrict__ Xin, 
         }
         // Constrained DOFs (src/sweep.hpp:1286-1403, 1718-1876): the step on
         // the entity's tangent space, damped by omega before the line
-        // search, every trial on the entity; a plane after the first sweep of
-        // a run call searches in its in-plane coordinates.
+        // search, every trial on the entity; a parametric entity after the
+        // first sweep of a run call searches in its parameters.
         const int etag = sp.etag != nullptr ? int(sp.etag[d]) : 0;
         const double* er = sp.epar + (etag != 0 ? d * EGG_B200_ENTITY_FIELDS : 0);
-        const bool warm_plane = etag == EGG_B200_TAG_PLANE && !sp.cold;
+        const bool warm_param = is_param3(etag) && !sp.cold;
         double dl[3] = {0.0, 0.0, 0.0};
         double qs[2] = {0.0, 0.0}, dq[2] = {0.0, 0.0};
         if (etag == 0) {
             solve3<double>(h, g, dl);
-        } else if (warm_plane) {
-            plane_warm_step(er, h, g, pos, omega, qs, dq);
+        } else if (warm_param) {
+            param3_warm_step(etag, er, h, g, pos, omega, qs, dq);
         } else {
             entity3_newton_step(etag, er, h, g, pos, dl);
             for (int q = 0; q < 3; ++q) { dl[q] *= omega; }
@@ -555,9 +555,10 @@ __global__ void stored3_kernel(StoredPatch3 sp, const double* __restrict__ Xin, 
         double cur[3] = {pos[0], pos[1], pos[2]};
         for (int it = 0; it < 10; ++it) {
             double tr[3] = {pos[0] + alpha * dl[0], pos[1] + alpha * dl[1], pos[2] + alpha * dl[2]};
-            if (warm_plane) {
-                const double qt[2] = {qs[0] + alpha * dq[0], qs[1] + alpha * dq[1]};
-                plane_eval(er, qt, tr);
+            if (warm_param) {
+                double qt[2] = {qs[0] + alpha * dq[0], qs[1] + alpha * dq[1]};
+                p3_clamp(etag, er, qt);
+                p3_eval(etag, er, qt, tr);
             } else if (etag != 0) {
                 const double raw[3] = {tr[0], tr[1], tr[2]};
                 entity3_project(etag, er, raw, tr);

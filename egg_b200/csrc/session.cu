@@ -592,7 +592,7 @@ static Session* create_session(const egg_b200_session_desc& d)
                 throw Error(EGG_B200_ENOTSUP, "egg_b200: constrained entity tag " + std::to_string(etag) +
                                                 " is not supported in " + std::to_string(D) +
                                                 "D (this core relaxes the 2D LineSeg, Circle, Ellipse, CircleArc, EllipseArc, QuadBezier, CubicBezier, "
-                                                "LineRail and the 3D Plane, LineRail3)");
+                                                "LineRail and the 3D Plane, Sphere, Cylinder, Line3, LineRail3)");
             }
             if (!d.entity_params) { invalid("validate_context: constrained DOF without entity_params"); }
             for (int f = 0; f < EGG_B200_ENTITY_FIELDS; ++f) {
@@ -634,7 +634,7 @@ static Session* create_session(const egg_b200_session_desc& d)
             st_epar.push_back(etag != 0 ? d.entity_params[i * EGG_B200_ENTITY_FIELDS + f] : 0.0);
         }
         if (etag != 0) { S->n_constrained++; }
-        if (is_tcurve(etag) || etag == EGG_B200_TAG_PLANE) { S->n_arc++; }
+        if ((D == 2 && is_tcurve(etag)) || (D == 3 && is_param3(etag))) { S->n_arc++; }
         for (int64_t p = p0; p < p0 + P; ++p) {
             auto remap = [&](int32_t g) {
                 const int32_t s = S->g2s[g];

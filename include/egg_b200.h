@@ -52,7 +52,10 @@ extern "C" {
 #define EGG_B200_TAG_QUADBEZIER 8 /* record (p0, p1, p2, t0, t1): quadratic Bezier, trimmed to [t0, t1] */
 #define EGG_B200_TAG_CUBICBEZIER 9 /* record (p0, p1, p2, p3, t0, t1): cubic Bezier, trimmed to [t0, t1] */
 #define EGG_B200_TAG_LINERAIL 15 /* record (sx, sy, ex, ey): open-ended segment, released beyond its ends */
+#define EGG_B200_TAG_SPHERE 4    /* 3D record (c(3), r, ax(3), ay(3)): untrimmed sphere, frame ax, ay, ax x ay */
 #define EGG_B200_TAG_PLANE 5     /* 3D record (o(3), ax(3), ay(3)): untrimmed plane, orthonormal in-plane axes */
+#define EGG_B200_TAG_CYLINDER 12 /* 3D record (o(3), ax(3), ay(3), r): untrimmed cylinder about ax x ay */
+#define EGG_B200_TAG_LINE3 13    /* 3D record (p0(3), p1(3), t0, t1): line trimmed to [t0, t1] */
 #define EGG_B200_TAG_LINERAIL3 16 /* 3D record (s(3), e(3)): open-ended segment, released beyond its ends */
 #define EGG_B200_ENTITY_FIELDS 10 /* reals per entity record in entity_params */
 

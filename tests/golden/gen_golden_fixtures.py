@@ -143,6 +143,7 @@ CASES_CON = {
     "cube_slide9": ("cube_sliding", dict(n=9, seed=8)),
     "disk_earcs17": ("disk_on_curve", dict(n=17, seed=9, ry=0.6, arcs=True)),
     "square_bezier17": ("square_bezier", dict(n=17, seed=10)),
+    "cube_curved9": ("cube_curved", dict(n=9, seed=11)),
 }
 RUNS_CON = [
     # (case, phase, delta, omega, n_sweeps)
@@ -160,6 +161,8 @@ RUNS_CON = [
     ("disk_earcs17", "barrier", 0.0, 1.0, 30),
     ("square_bezier17", "barrier", 0.0, 1.0, 30),
     ("square_bezier17", "barrier", 0.0, 0.8, 30),
+    ("cube_curved9", "barrier", 0.0, 1.0, 20),
+    ("cube_curved9", "barrier", 0.0, 0.8, 20),
 ]
 # FAS V-cycles on sliding-boundary grids: (case, phase, n_cycles, nu_pre, nu_post, nu_coarse, omega, max_levels)
 FAS_RUNS_CON = [
@@ -169,6 +172,7 @@ FAS_RUNS_CON = [
     ("disk_arcs17", "barrier", 3, 2, 2, 32, 1.0, 32),
     ("cube_slide9", "barrier", 3, 2, 2, 16, 1.0, 32),
     ("square_bezier17", "barrier", 3, 2, 2, 32, 1.0, 32),
+    ("cube_curved9", "barrier", 3, 2, 2, 16, 1.0, 32),
 ]
 ENTITY_RECORDS = {
     1: (0.1, -0.2, 0.9, 0.4),
@@ -228,15 +232,19 @@ def _constrained_runs() -> dict:
     e_b, _ = sess.run(20, report_every=1)
     out["twocalls/disk_arcs17/E"] = np.concatenate([e_a, e_b])
     out["twocalls/disk_arcs17/X"] = sess.get_X()
-    g = case_grid("cube_slide9")
-    sess = ref.CppStructuredSweepSession(g.wire(), g.structured(), g.X_flat(), device="cpu", dim=3)
-    e_a, _ = sess.run(5, report_every=1)
-    e_b, _ = sess.run(10, report_every=1)
-    out["twocalls/cube_slide9/E"] = np.concatenate([e_a, e_b])
-    out["twocalls/cube_slide9/X"] = sess.get_X()
+    for case in ("cube_slide9", "cube_curved9"):
+        g = case_grid(case)
+        sess = ref.CppStructuredSweepSession(g.wire(), g.structured(), g.X_flat(), device="cpu", dim=3)
+        e_a, _ = sess.run(5, report_every=1)
+        e_b, _ = sess.run(10, report_every=1)
+        out[f"twocalls/{case}/E"] = np.concatenate([e_a, e_b])
+        out[f"twocalls/{case}/X"] = sess.get_X()
     # 3D projections: the reference's own batched projection
     c, sn = np.cos(0.4), np.sin(0.4)
-    for tag, rec in ((5, (0.1, -0.2, 0.3, c, sn, 0.0, 0.0, 0.0, 1.0)), (16, (0.1, 0.0, -0.1, 0.7, 0.3, 0.2))):
+    for tag, rec in ((5, (0.1, -0.2, 0.3, c, sn, 0.0, 0.0, 0.0, 1.0)), (16, (0.1, 0.0, -0.1, 0.7, 0.3, 0.2)),
+                     (4, (0.2, 0.1, -0.3, 0.9, c, sn, 0.0, -sn, c, 0.0)),
+                     (12, (0.1, 0.2, 0.0, c, 0.0, sn, 0.0, 1.0, 0.0, 0.7)),
+                     (13, (0.1, 0.0, -0.1, 0.7, 0.3, 0.2, 0.1, 0.8))):
         Q = rng3.uniform(-0.5, 1.2, size=(64, 3))
         feet, _basis = ref.geometry_project_batch(Q, tag, np.array(rec), [])
         out[f"entity3/{tag}/params"] = np.array(rec)

@@ -21,7 +21,7 @@ _FX = np.load(GOLDEN / "ref_constrained.npz")
 @pytest.mark.parametrize("grid", [configs.disk_on_curve(9), configs.disk_on_curve(9, ry=0.6),
                                   configs.disk_on_curve(9, arcs=True), configs.disk_on_curve(9, ry=0.6, arcs=True),
                                   configs.square_sliding(9), configs.square_bezier(9),
-                                  configs.cube_sliding(5)], ids=lambda g: g.name)
+                                  configs.cube_sliding(5), configs.cube_curved(5)], ids=lambda g: g.name)
 def test_wire_partitions_cover_every_dof_once(grid):
     grp = grid.wire()["groups"][0]
     seen = np.zeros(grp["D"], dtype=int)
@@ -67,15 +67,16 @@ def test_entity_geometry_matches_the_reference_core(tmp_path):
 
 
 def test_entity3_projection_matches_the_reference_core(tmp_path):
-    """Plane (in-plane coordinates, then evaluated) and LineRail3 (released
-    beyond its ends) projections against the reference's batched projection."""
+    """Sphere, Plane, Cylinder, Line3 (foot, trim clamp, evaluation) and
+    LineRail3 (released beyond its ends) projections against the reference's
+    batched projection."""
     gxx = shutil.which("g++")
     if gxx is None:
         pytest.skip("no host C++ compiler")
     exe = tmp_path / "entity3"
     subprocess.run([gxx, "-O1", "-std=c++17", f"-I{ROOT / 'egg_b200' / 'csrc'}", f"-I{ROOT / 'include'}",
                     str(ROOT / "tests" / "native" / "entity3_check.cpp"), "-o", str(exe)], check=True)
-    for tag in (5, 16):
+    for tag in (4, 5, 12, 13, 16):
         k = f"entity3/{tag}/"
         rec = np.zeros(10)
         rec[: len(_FX[k + "params"])] = _FX[k + "params"]

@@ -1,6 +1,6 @@
 """Constrained boundary DOFs on the GPU: nodes sliding on a Circle, an
 Ellipse, trimmed CircleArcs, EllipseArcs and Beziers, LineSegs, a LineRail,
-Planes and a LineRail3 relax exactly as the reference core relaxes
+Planes, a Sphere, a Cylinder, a Line3 and a LineRail3 relax exactly as the reference core relaxes
 them (first sweep and trajectory, fp64), the mixed path tracks that, every
 accepted boundary node lies on its entity, a batch of constrained meshes
 equals separate sessions, and FAS V-cycles on such grids match the reference."""
@@ -42,19 +42,27 @@ def test_entity_step_and_projection_match_reference(gpu, tag):
         np.testing.assert_allclose(ft, _FX[k + "foot"][i], rtol=rtol, atol=1e-15)
 
 
+# Position tolerances (first sweep, trajectory) in units of the smallest edge,
+# per case where the default (1e-12, 1e-9) is too tight: none at present (a
+# sphere's latitude chart is ill-conditioned at its poles, so the curved cube
+# keeps its cap on the chart's equator instead).
+_XTOL: dict = {}
+
+
 @pytest.mark.parametrize("run", RUNS_CON, ids=lambda r: f"{r[0]}-{r[1]}-{r[3]}")
 def test_constrained_sweeps_match_reference(gpu, run):
     case, phase, delta, omega, n = run
     g = case_grid(case)
     key = f"{case}/{phase}/{omega}"
+    t1, tn = _XTOL.get(case, (1e-12, 1e-9))
     s = _session(gpu, g)
     s.run(1, phase=phase, delta=delta, omega=omega)
-    assert np.abs(s.get_X() - _FX[key + "/X1"]).max() <= 1e-12 * _hmin(g)
+    assert np.abs(s.get_X() - _FX[key + "/X1"]).max() <= t1 * _hmin(g)
     s2 = _session(gpu, g)
     E, M = s2.run(n, phase=phase, delta=delta, omega=omega, report_every=1)
     np.testing.assert_allclose(E, _FX[key + "/E"], rtol=1e-9)
     np.testing.assert_allclose(M, _FX[key + "/M"], rtol=1e-8, atol=1e-16)
-    assert np.abs(s2.get_X() - _FX[key + "/Xn"]).max() <= 1e-9 * _hmin(g)
+    assert np.abs(s2.get_X() - _FX[key + "/Xn"]).max() <= tn * _hmin(g)
 
 
 @pytest.mark.parametrize("case", ["disk_circle17", "disk_ellipse17", "square_slide17", "disk_arcs17",
@@ -98,6 +106,19 @@ def test_arcs_cold_first_sweep_per_call_and_graph_chunks(gpu):
     assert abs(two[-1] - E30[-1]) > 1e-6 * abs(E30[-1])
 
 
+def test_curved_cube_restarts_cold_per_call(gpu):
+    """Sphere, Cylinder, Plane and Line3 DOFs in a session run in two calls
+    follow the reference session's two calls."""
+    g = case_grid("cube_curved9")
+    s = _session(gpu, g)
+    ea, _ = s.run(5, report_every=1)
+    eb, _ = s.run(10, report_every=5)
+    two = _FX["twocalls/cube_curved9/E"]
+    np.testing.assert_allclose(ea, two[:5], rtol=1e-9)
+    np.testing.assert_allclose(eb, two[5:][4::5], rtol=1e-9)
+    assert np.abs(s.get_X() - _FX["twocalls/cube_curved9/X"]).max() <= 1e-9 * _hmin(g)
+
+
 def test_cube_faces_and_edge_stay_on_their_entities_and_restart_cold(gpu):
     """3D: nodes on Plane faces stay in their planes, nodes on the LineRail3
     edge stay on its line (or are released beyond its end), and a session run
@@ -125,7 +146,7 @@ def test_cube_faces_and_edge_stay_on_their_entities_and_restart_cold(gpu):
                 np.testing.assert_allclose(X[v], rec[:3] + t * (rec[3:6] - rec[:3]), rtol=0, atol=1e-14)
 
 
-@pytest.mark.parametrize("case", ["disk_circle33", "square_slide17", "cube_slide9"])
+@pytest.mark.parametrize("case", ["disk_circle33", "square_slide17", "cube_slide9", "cube_curved9"])
 def test_constrained_mixed_tracks_fp64(gpu, case):
     g = case_grid(case)
     key = f"{case}/barrier/1.0"
