@@ -31,7 +31,7 @@ from . import wire as _wire
 __all__ = [
     "Grid", "unit_square", "disk_oh", "tangled_square", "unit_cube", "two_cubes", "sphere_in_cube",
     "grid_mindet", "mean_size_w_inv", "disk_on_curve", "square_sliding", "cube_sliding", "square_bezier",
-    "cube_curved",
+    "cube_curved", "square_bspline",
 ]
 
 
@@ -303,6 +303,41 @@ def square_bezier(n: int = 17, frac: float = 0.2, slide: float = 0.3, seed: int 
         for v in nodes:
             cons[int(v)] = (tag, rec)
     return Grid(f"square_bezier{n}", 2, g.blocks, X, g.free.copy(), {"frac": frac, "seed": seed}, cons)
+
+
+def _nurbs_points(deg, knots, ctrl, w, t):
+    from scipy.interpolate import BSpline
+
+    ctrl = np.asarray(ctrl, dtype=np.float64)
+    w = np.ones(len(ctrl)) if w is None else np.asarray(w, dtype=np.float64)
+    num = BSpline(np.asarray(knots), ctrl * w[:, None], deg)(t)
+    den = BSpline(np.asarray(knots), w, deg)(t)
+    return num / den[:, None]
+
+
+def square_bspline(n: int = 17, frac: float = 0.2, slide: float = 0.3, seed: int = 0) -> Grid:
+    """Unit square whose top side is a clamped cubic B-spline through six
+    control points and whose bottom side is a rational quadratic NURBS
+    (B-spline entities, tag 10, trimmed to [0, 1]); their nodes sit on the
+    curves at parameters i/(n-1), moved by up to ``slide`` of a step, and
+    slide along them.  Corners stay fixed."""
+    g = unit_square(n, frac=frac, seed=seed)
+    ids = g.blocks[0]
+    X = g.X.copy()
+    rng = np.random.default_rng(seed + 606)
+    t = np.linspace(0.0, 1.0, n)[1:-1] + rng.uniform(-slide, slide, n - 2) / (n - 1)
+    top = (3, [0, 0, 0, 0, 1 / 3, 2 / 3, 1, 1, 1, 1],
+           [[0, 1], [0.2, 1.1], [0.4, 0.95], [0.6, 1.08], [0.8, 0.97], [1, 1]], None)
+    bot = (2, [0, 0, 0, 0.5, 1, 1, 1], [[0, 0], [0.3, -0.12], [0.7, -0.08], [1, 0]], [1.0, 0.8, 1.2, 1.0])
+    cons = {}
+    for nodes, (deg, knots, ctrl, w) in ((ids[1:-1, -1], top), (ids[1:-1, 0], bot)):
+        X[nodes] = _nurbs_points(deg, knots, ctrl, w, t)
+        rec = (float(deg), float(len(ctrl)), 0.0, 1.0, 0.0, 0.0 if w is None else 1.0)
+        seg = (np.asarray(knots, dtype=np.float64), np.asarray(ctrl, dtype=np.float64).ravel(),
+               np.zeros(0) if w is None else np.asarray(w, dtype=np.float64))
+        for v in nodes:
+            cons[int(v)] = (10, rec, seg)
+    return Grid(f"square_bspline{n}", 2, g.blocks, X, g.free.copy(), {"frac": frac, "seed": seed}, cons)
 
 
 def cube_sliding(n: int = 9, frac: float = 0.2, slide: float = 0.3, off: float = 0.02, seed: int = 0,

@@ -115,7 +115,7 @@ struct Desc {
     egg_b200_session_desc d {};
     Keep keep;
     std::vector<int32_t> shapes, bgd, tags;
-    std::vector<double> eparams;
+    std::vector<double> eparams, arena;
 };
 
 // Fill the C-ABI descriptor from the reference's two dicts + X
@@ -216,6 +216,32 @@ void fill_desc(Desc& D, const py::dict& ctx, const py::dict& st, const DArr& X, 
                     throw py::value_error("validate_context: entity records size " + std::to_string(rec.size()) +
                                           " != count*kFields " + std::to_string(dl.size() * kf));
                 }
+                // Segmented fields ({data, off} CSR per field: B-spline knots,
+                // control points, weights) go to the entity arena; a B-spline
+                // record then addresses its slices by arena offset.
+                std::vector<int64_t> seg_base;
+                std::vector<IArr> seg_off;
+                if (ed.contains("seg")) {
+                    for (auto sv : ed["seg"].cast<py::list>()) {
+                        py::dict sd = sv.cast<py::dict>();
+                        DArr data = DArr::ensure(sd["data"]);
+                        IArr off = IArr::ensure(sd["off"]);
+                        if (off.size() != dl.size() + 1) {
+                            throw py::value_error("validate_context: entity seg off size != count + 1");
+                        }
+                        for (py::ssize_t r = 0; r + 1 < off.size(); ++r) {
+                            if (off.data()[r] < 0 || off.data()[r] > off.data()[r + 1] || off.data()[r + 1] > data.size()) {
+                                throw py::value_error("validate_context: entity seg off out of range");
+                            }
+                        }
+                        seg_base.push_back(int64_t(D.arena.size()));
+                        D.arena.insert(D.arena.end(), data.data(), data.data() + data.size());
+                        seg_off.push_back(off);
+                    }
+                }
+                if (tag == EGG_B200_TAG_BSPLINE && seg_off.size() < 2) {
+                    throw py::value_error("validate_context: a B-spline partition needs its knots and ctrl seg fields");
+                }
                 for (py::ssize_t i = 0; i < dl.size(); ++i) {
                     const int32_t v = dl.data()[i];
                     if (v < 0 || v >= d.ndof) { throw py::value_error("validate_context: dof_local out of range"); }
@@ -224,8 +250,12 @@ void fill_desc(Desc& D, const py::dict& ctx, const py::dict& st, const DArr& X, 
                     if (tag == 0) { continue; }
                     constrained = true;
                     // row i of the partition's (count, kFields) records
-                    for (int f = 0; f < std::min(kf, int(EGG_B200_ENTITY_FIELDS)); ++f) {
-                        D.eparams[size_t(v) * EGG_B200_ENTITY_FIELDS + f] = rec.data()[i * kf + f];
+                    double* er = &D.eparams[size_t(v) * EGG_B200_ENTITY_FIELDS];
+                    for (int f = 0; f < std::min(kf, int(EGG_B200_ENTITY_FIELDS)); ++f) { er[f] = rec.data()[i * kf + f]; }
+                    if (tag == EGG_B200_TAG_BSPLINE) {
+                        for (size_t k = 0; k < 3 && k < seg_off.size(); ++k) {
+                            er[6 + k] = double(seg_base[k] + seg_off[k].data()[i]);
+                        }
                     }
                 }
             }
@@ -239,6 +269,8 @@ void fill_desc(Desc& D, const py::dict& ctx, const py::dict& st, const DArr& X, 
         }
         d.entity_tag = D.tags.data();
         d.entity_params = constrained ? D.eparams.data() : nullptr;
+        d.entity_arena = D.arena.empty() ? nullptr : D.arena.data();
+        d.entity_arena_len = int64_t(D.arena.size());
     }
 
     py::dict es = ctx["energy_stencil"].cast<py::dict>();

@@ -253,6 +253,266 @@ EGG_HD void tc_warm_step(int tag, const double* e, const double H[4], const doub
     dq *= omega;
 }
 
+// ---- B-spline / NURBS curve (tag 10) ----------------------------------------
+// Record (degree, n_ctrl, t0, t1, closed, has_w, knots_at, ctrl_at, w_at): the
+// last three are offsets into the session's entity arena (knots: n_ctrl +
+// degree + 1 reals, control points: 2 n_ctrl, weights: n_ctrl when has_w).
+// Basis functions and derivatives by the triangular recurrences of Piegl and
+// Tiller, "The NURBS Book", algorithms A2.1 (span) and A2.3 (derivatives);
+// the rational form by the quotient rule (src/geometry.hpp:720-965).
+constexpr int kBSplineMaxDegree = 7;  // the reference's default curve degree cap
+constexpr int kBSplineCap = kBSplineMaxDegree + 1;
+
+struct BSplineCurve {
+    int p, n;  // degree, control points
+    const double* knots;
+    const double* ctrl;
+    const double* w;  // NULL: polynomial
+    double t0, t1;
+    bool closed;
+};
+
+EGG_HD BSplineCurve bspline_view(const double* e, const double* arena)
+{
+    BSplineCurve c;
+    c.p = int(e[0]);
+    c.n = int(e[1]);
+    c.t0 = e[2];
+    c.t1 = e[3];
+    c.closed = e[4] != 0.0;
+    c.knots = arena + int64_t(e[6]);
+    c.ctrl = arena + int64_t(e[7]);
+    c.w = e[5] != 0.0 ? arena + int64_t(e[8]) : nullptr;
+    return c;
+}
+
+// Knot span of u: the last knot interval [k_i, k_i+1) that holds it, clamped
+// to [degree, n_ctrl - 1].
+EGG_HD int bspline_span(const BSplineCurve& c, double u)
+{
+    const int last = c.n - 1;
+    if (u >= c.knots[last + 1]) { return last; }
+    if (u <= c.knots[c.p]) { return c.p; }
+    int lo = c.p, hi = last + 1;
+    int mid = (lo + hi) / 2;
+    while (u < c.knots[mid] || u >= c.knots[mid + 1]) {
+        if (u < c.knots[mid]) {
+            hi = mid;
+        } else {
+            lo = mid;
+        }
+        mid = (lo + hi) / 2;
+    }
+    return mid;
+}
+
+// der[k][j]: k-th derivative (k <= nd <= 2) of the j-th nonzero basis
+// function at u in span.
+EGG_HD void bspline_basis(const BSplineCurve& c, int span, double u, int nd, double der[3][kBSplineCap])
+{
+    const int p = c.p;
+    double tab[kBSplineCap][kBSplineCap];  // lower: knot differences, upper: basis values
+    double lft[kBSplineCap], rgt[kBSplineCap];
+    tab[0][0] = 1.0;
+    for (int j = 1; j <= p; ++j) {
+        lft[j] = u - c.knots[span + 1 - j];
+        rgt[j] = c.knots[span + j] - u;
+        double carry = 0.0;
+        for (int r = 0; r < j; ++r) {
+            tab[j][r] = rgt[r + 1] + lft[j - r];
+            const double q = tab[r][j - 1] / tab[j][r];
+            tab[r][j] = carry + rgt[r + 1] * q;
+            carry = lft[j - r] * q;
+        }
+        tab[j][j] = carry;
+    }
+    for (int j = 0; j <= p; ++j) { der[0][j] = tab[j][p]; }
+    double co[2][kBSplineCap];
+    for (int r = 0; r <= p; ++r) {
+        int cur = 0, nxt = 1;
+        co[0][0] = 1.0;
+        for (int k = 1; k <= nd; ++k) {
+            double acc = 0.0;
+            const int rk = r - k, pk = p - k;
+            if (r >= k) {
+                co[nxt][0] = co[cur][0] / tab[pk + 1][rk];
+                acc = co[nxt][0] * tab[rk][pk];
+            }
+            const int jlo = rk >= -1 ? 1 : -rk;
+            const int jhi = r - 1 <= pk ? k - 1 : p - r;
+            for (int j = jlo; j <= jhi; ++j) {
+                co[nxt][j] = (co[cur][j] - co[cur][j - 1]) / tab[pk + 1][rk + j];
+                acc += co[nxt][j] * tab[rk + j][pk];
+            }
+            if (r <= pk) {
+                co[nxt][k] = -co[cur][k - 1] / tab[pk + 1][r];
+                acc += co[nxt][k] * tab[r][pk];
+            }
+            der[k][r] = acc;
+            const int t = cur;
+            cur = nxt;
+            nxt = t;
+        }
+    }
+    double f = double(p);  // scale row k by p! / (p - k)!
+    for (int k = 1; k <= nd; ++k) {
+        for (int j = 0; j <= p; ++j) { der[k][j] *= f; }
+        f *= double(p - k);
+    }
+}
+
+// Curve point (order 0) or its first / second derivative at u.
+EGG_HD void bspline_point(const BSplineCurve& c, double u, int order, double& x, double& y)
+{
+    const int span = bspline_span(c, u);
+    double der[3][kBSplineCap];
+    bspline_basis(c, span, u, order, der);
+    if (c.w == nullptr) {
+        double ax = 0.0, ay = 0.0;
+        for (int j = 0; j <= c.p; ++j) {
+            const int i = span - c.p + j;
+            ax = ax + der[order][j] * c.ctrl[2 * i];
+            ay = ay + der[order][j] * c.ctrl[2 * i + 1];
+        }
+        x = ax;
+        y = ay;
+        return;
+    }
+    // rational: A^(k) = sum N^(k) w P, w^(k) = sum N^(k) w; C = A / w,
+    // C' = (A' - w' C) / w, C'' = (A'' - 2 w' C' - w'' C) / w
+    double Ax[3] = {0.0, 0.0, 0.0}, Ay[3] = {0.0, 0.0, 0.0}, W[3] = {0.0, 0.0, 0.0};
+    for (int k = 0; k <= order; ++k) {
+        for (int j = 0; j <= c.p; ++j) {
+            const int i = span - c.p + j;
+            const double nw = der[k][j] * c.w[i];
+            Ax[k] = Ax[k] + nw * c.ctrl[2 * i];
+            Ay[k] = Ay[k] + nw * c.ctrl[2 * i + 1];
+            W[k] += nw;
+        }
+    }
+    const double iw = 1.0 / W[0];
+    double Cx[3], Cy[3];
+    Cx[0] = iw * Ax[0];
+    Cy[0] = iw * Ay[0];
+    if (order >= 1) {
+        Cx[1] = iw * (Ax[1] - W[1] * Cx[0]);
+        Cy[1] = iw * (Ay[1] - W[1] * Cy[0]);
+    }
+    if (order >= 2) {
+        Cx[2] = iw * ((Ax[2] - 2.0 * W[1] * Cx[1]) - W[2] * Cx[0]);
+        Cy[2] = iw * ((Ay[2] - 2.0 * W[1] * Cy[1]) - W[2] * Cy[0]);
+    }
+    x = Cx[order];
+    y = Cy[order];
+}
+
+// Seeded nearest-foot parameter on the live domain [knots[p], knots[n]]:
+// from the clamped seed when it is finite, else the best of 17 grid samples;
+// then 8 Newton steps (src/geometry.hpp:518-560 project_param_seeded).
+EGG_HD double bspline_foot(const BSplineCurve& c, double qx, double qy, double seed)
+{
+    const double lo = c.knots[c.p], hi = c.knots[c.n];
+    double t;
+    if (isfinite(seed)) {
+        t = seed < lo ? lo : (seed > hi ? hi : seed);
+    } else {
+        double best_t = lo, best_d = INFINITY;
+        for (int i = 0; i <= 16; ++i) {
+            const double tc = lo + ((hi - lo) * double(i)) / 16.0;
+            double x, y;
+            bspline_point(c, tc, 0, x, y);
+            const double dx = x - qx, dy = y - qy;
+            const double dd = dx * dx + dy * dy;
+            if (dd < best_d) {
+                best_d = dd;
+                best_t = tc;
+            }
+        }
+        t = best_t;
+    }
+    for (int it = 0; it < 8; ++it) {
+        double x, y, d1x, d1y, d2x, d2y;
+        bspline_point(c, t, 0, x, y);
+        bspline_point(c, t, 1, d1x, d1y);
+        bspline_point(c, t, 2, d2x, d2y);
+        const double dx = x - qx, dy = y - qy;
+        const double f = dx * d1x + dy * d1y;
+        const double fp = (d1x * d1x + d1y * d1y) + (dx * d2x + dy * d2y);
+        if (fabs(fp) < kGeomTiny) { break; }
+        t -= f / fp;
+    }
+    return t;
+}
+
+EGG_HD double bspline_clamp(const BSplineCurve& c, double q)
+{
+    if (c.closed) { return arc_wrap(q, c.t0, c.t1); }
+    return q < c.t0 ? c.t0 : (q > c.t1 ? c.t1 : q);
+}
+
+EGG_HD bool bspline_inside(const BSplineCurve& c, double q) { return c.closed || (q >= c.t0 && q <= c.t1); }
+
+// Seeded projection (cold path, one trial): foot from the seed, stored back
+// unclamped, clamped onto the trim and evaluated.
+EGG_HD void bspline_project_seeded(const BSplineCurve& c, double px, double py, double& seed, double& qx, double& qy)
+{
+    double q = bspline_foot(c, px, py, seed);
+    seed = q;
+    if (!bspline_inside(c, q)) { q = bspline_clamp(c, q); }
+    bspline_point(c, q, 0, qx, qy);
+}
+
+// Cold Newton step: the tangent at the seeded foot of pos (seed updated).
+EGG_HD void bspline_cold_step(const BSplineCurve& c, const double H[4], const double g[2], double px, double py,
+                              double& seed, double out[2])
+{
+    double q = bspline_foot(c, px, py, seed);
+    seed = q;
+    if (!bspline_inside(c, q)) { q = bspline_clamp(c, q); }
+    double jx, jy, bx, by;
+    bspline_point(c, q, 1, jx, jy);
+    unit_or_e0(jx, jy, bx, by);
+    const double hb0 = H[0] * bx + H[1] * by;
+    const double hb1 = H[2] * bx + H[3] * by;
+    const double M = bx * hb0 + by * hb1;
+    const double r = bx * g[0] + by * g[1];
+    double y = 0.0;
+    const double rn = fabs(r);
+    if (!(rn < kGeomZnorm)) {
+        y = -r / M;
+        if (!isfinite(y)) { y = -0.1 * r / rn; }
+    }
+    out[0] = bx * y;
+    out[1] = by * y;
+}
+
+// Warm step: seeded foot q* of pos (stored as the seed), the step on the raw
+// tangent there, dq = (J.J)^-1 J.delta damped by omega.
+EGG_HD void bspline_warm_step(const BSplineCurve& c, const double H[4], const double g[2], double px, double py,
+                              double omega, double& seed, double& qstar, double& dq)
+{
+    qstar = bspline_foot(c, px, py, seed);
+    seed = qstar;
+    double jx, jy, bx, by;
+    bspline_point(c, qstar, 1, jx, jy);
+    unit_or_e0(jx, jy, bx, by);
+    const double hb0 = H[0] * bx + H[1] * by;
+    const double hb1 = H[2] * bx + H[3] * by;
+    const double M = bx * hb0 + by * hb1;
+    const double r = bx * g[0] + by * g[1];
+    double y = 0.0;
+    const double rn = fabs(r);
+    if (!(rn < kGeomZnorm)) {
+        y = -r / M;
+        if (!isfinite(y)) { y = -0.1 * r / rn; }
+    }
+    const double dx = bx * y, dy = by * y;
+    const double jtj = jx * jx + jy * jy;
+    const double jtd = jx * dx + jy * dy;
+    dq = (fabs(jtj) > kGeomTiny) ? jtd / jtj : 0.0;
+    dq *= omega;
+}
+
 // Projection of (px, py) onto the entity.
 EGG_HD void entity_project(int tag, const double* e, double px, double py, double& qx, double& qy)
 {
@@ -385,7 +645,8 @@ EGG_HD bool entity_supported(int dim, int tag)
                tag == EGG_B200_TAG_LINE3 || tag == EGG_B200_TAG_LINERAIL3;
     }
     return dim == 2 && (tag == EGG_B200_TAG_LINESEG || tag == EGG_B200_TAG_CIRCLE ||
-                        tag == EGG_B200_TAG_ELLIPSE || tag == EGG_B200_TAG_LINERAIL || is_tcurve(tag));
+                        tag == EGG_B200_TAG_ELLIPSE || tag == EGG_B200_TAG_LINERAIL || is_tcurve(tag) ||
+                        tag == EGG_B200_TAG_BSPLINE);
 }
 
 }  // namespace egg_b200

@@ -727,6 +727,8 @@ struct StoredPatch2 {
     const int8_t* etag;     // [n] entity tag of each DOF, or NULL (all Free)
     const double* epar;     // [n * EGG_B200_ENTITY_FIELDS] entity records (constrained DOFs)
     int cold;               // first sweep of a run call: trimmed arcs project in world space
+    const double* arena;    // entity arena (B-spline knots, control points, weights)
+    double* seeds;          // [n] last foot parameter of each B-spline DOF (NaN: none)
 };
 
 __device__ __forceinline__ void assemble_T(const double2 c, const double2 n0, const double2 n1,
@@ -919,10 +921,25 @@ __global__ void stored_patch_kernel(StoredPatch2 sp, const double2* __restrict__
         const int etag = sp.etag != nullptr ? int(sp.etag[d]) : 0;
         const double* er = sp.epar + (etag != 0 ? d * EGG_B200_ENTITY_FIELDS : 0);
         const bool warm_arc = is_tcurve(etag) && !sp.cold;
+        // B-spline DOFs carry a seed (their last foot parameter): every seeded
+        // projection starts its Newton solve there and stores its result
+        // (src/sweep.hpp:1219-1265).
+        const bool bsp = etag == EGG_B200_TAG_BSPLINE;
+        double seed = bsp ? sp.seeds[d] : 0.0;
+        BSplineCurve bc {};
+        if (bsp) { bc = bspline_view(er, sp.arena); }
         double dl[2] = {0.0, 0.0};
         double qstar = 0.0, dq = 0.0;
         if (etag == 0) {
             solve2<double>(h, g, dl);
+        } else if (bsp) {
+            if (sp.cold) {
+                bspline_cold_step(bc, h, g, pos.x, pos.y, seed, dl);
+                dl[0] *= omega;
+                dl[1] *= omega;
+            } else {
+                bspline_warm_step(bc, h, g, pos.x, pos.y, omega, seed, qstar, dq);
+            }
         } else if (warm_arc) {
             tc_warm_step(etag, er, h, g, pos.x, pos.y, omega, qstar, dq);
         } else {
@@ -934,7 +951,13 @@ __global__ void stored_patch_kernel(StoredPatch2 sp, const double2* __restrict__
         double2 cur = pos;
         for (int it = 0; it < 10; ++it) {
             double2 trial = make_double2(pos.x + alpha * dl[0], pos.y + alpha * dl[1]);
-            if (warm_arc) {
+            if (bsp) {
+                if (sp.cold) {
+                    bspline_project_seeded(bc, trial.x, trial.y, seed, trial.x, trial.y);
+                } else {
+                    bspline_point(bc, bspline_clamp(bc, qstar + alpha * dq), 0, trial.x, trial.y);
+                }
+            } else if (warm_arc) {
                 tc_eval(etag, er, tc_clamp(etag, er, qstar + alpha * dq), 0, trial.x, trial.y);
             } else if (etag != 0) {
                 entity_project(etag, er, trial.x, trial.y, trial.x, trial.y);
@@ -963,6 +986,7 @@ __global__ void stored_patch_kernel(StoredPatch2 sp, const double2* __restrict__
             cur.x = pos.x + omega * (cur.x - pos.x);
             cur.y = pos.y + omega * (cur.y - pos.y);
         }
+        if (bsp && lane == 0) { sp.seeds[d] = seed; }
         if (lane == 0) { Xout[slot] = cur; }
     }
 }

@@ -127,6 +127,9 @@ struct LevelData {
     int st_wstride = 0, st_wtstride = 0;
     int64_t n_constrained = 0;  // stored DOFs on a boundary entity
     int64_t n_arc = 0;          // of which on a parametric entity (arc, plane: cold first sweep per run call)
+    int64_t n_bspline = 0;      // of which on a B-spline curve (seeded projection)
+    DevBuf<double> arena;       // entity arena (B-spline knots, control points, weights)
+    DevBuf<double> seeds;       // [n_stored] last foot parameter of each B-spline DOF
     DevBuf<int8_t> st_etag;     // [n_stored] entity tag (uploaded when n_constrained > 0)
     DevBuf<double> st_epar;     // [n_stored * EGG_B200_ENTITY_FIELDS] entity records
     int64_t nshare = 0;
@@ -591,7 +594,7 @@ static Session* create_session(const egg_b200_session_desc& d)
             if (!entity_supported(D, etag)) {
                 throw Error(EGG_B200_ENOTSUP, "egg_b200: constrained entity tag " + std::to_string(etag) +
                                                 " is not supported in " + std::to_string(D) +
-                                                "D (this core relaxes the 2D LineSeg, Circle, Ellipse, CircleArc, EllipseArc, QuadBezier, CubicBezier, "
+                                                "D (this core relaxes the 2D LineSeg, Circle, Ellipse, CircleArc, EllipseArc, QuadBezier, CubicBezier, BSpline, "
                                                 "LineRail and the 3D Plane, Sphere, Cylinder, Line3, LineRail3)");
             }
             if (!d.entity_params) { invalid("validate_context: constrained DOF without entity_params"); }
@@ -602,6 +605,21 @@ static Session* create_session(const egg_b200_session_desc& d)
             }
             if (d.interior_block && d.interior_block[i] >= 0) {
                 throw Error(EGG_B200_ENOTSUP, "egg_b200: a constrained DOF on the structured-interior path");
+            }
+            if (etag == EGG_B200_TAG_BSPLINE) {
+                const double* r = d.entity_params + i * EGG_B200_ENTITY_FIELDS;
+                const int64_t deg = int64_t(r[0]), nc = int64_t(r[1]);
+                if (double(deg) != r[0] || deg < 1 || deg > kBSplineMaxDegree || double(nc) != r[1] || nc < deg + 1) {
+                    invalid("validate_context: B-spline degree must be 1.." + std::to_string(kBSplineMaxDegree) +
+                            " with n_ctrl > degree");
+                }
+                auto within = [&](double at, int64_t len) {
+                    return at >= 0.0 && double(int64_t(at)) == at && int64_t(at) + len <= d.entity_arena_len;
+                };
+                if (!d.entity_arena || !within(r[6], nc + deg + 1) || !within(r[7], 2 * nc) ||
+                    (r[5] != 0.0 && !within(r[8], nc))) {
+                    invalid("validate_context: B-spline knots / control points / weights outside entity_arena");
+                }
             }
         }
         const int32_t slot = S->g2s[gid];
@@ -634,7 +652,10 @@ static Session* create_session(const egg_b200_session_desc& d)
             st_epar.push_back(etag != 0 ? d.entity_params[i * EGG_B200_ENTITY_FIELDS + f] : 0.0);
         }
         if (etag != 0) { S->n_constrained++; }
-        if ((D == 2 && is_tcurve(etag)) || (D == 3 && is_param3(etag))) { S->n_arc++; }
+        if ((D == 2 && (is_tcurve(etag) || etag == EGG_B200_TAG_BSPLINE)) || (D == 3 && is_param3(etag))) {
+            S->n_arc++;
+        }
+        if (etag == EGG_B200_TAG_BSPLINE) { S->n_bspline++; }
         for (int64_t p = p0; p < p0 + P; ++p) {
             auto remap = [&](int32_t g) {
                 const int32_t s = S->g2s[g];
@@ -875,6 +896,11 @@ static Session* create_session(const egg_b200_session_desc& d)
         S->st_etag.upload(st_etag);
         S->st_epar.upload(st_epar);
     }
+    if (S->n_bspline) {
+        S->arena.upload(std::vector<double>(d.entity_arena, d.entity_arena + d.entity_arena_len));
+        S->seeds.alloc(size_t(S->n_stored));
+        EGG_CK(cudaMemset(S->seeds.p, 0xFF, size_t(S->n_stored) * sizeof(double)));  // all-ones: NaN
+    }
     S->st_gc.upload(st_gc);
     S->st_gn0.upload(st_gn0);
     S->st_gn1.upload(st_gn1);
@@ -1044,6 +1070,8 @@ static StoredPatch2 stored_view(LevelData& S)
     sp.etag = S.n_constrained ? S.st_etag.p : nullptr;
     sp.epar = S.n_constrained ? S.st_epar.p : nullptr;
     sp.cold = 0;
+    sp.arena = S.n_bspline ? S.arena.p : nullptr;
+    sp.seeds = S.n_bspline ? S.seeds.p : nullptr;
     return sp;
 }
 
@@ -1655,6 +1683,15 @@ static void ensure_xfer(Session& S)
     }
 }
 
+// The B-spline seeds after a position reset: NaN (the next projection seeds
+// from its coarse grid), as the reference's upload_X does (src/sweep.hpp:592-597).
+static void reset_seeds(Session& S)
+{
+    if (S.n_bspline) {
+        EGG_CK(cudaMemsetAsync(S.seeds.p, 0xFF, size_t(S.n_stored) * sizeof(double), S.stream));
+    }
+}
+
 static int remap_grid(int64_t n) { return int(std::max<int64_t>(1, std::min<int64_t>((n + 255) / 256, 148 * 8))); }
 
 extern "C" {
@@ -2080,6 +2117,7 @@ int egg_b200_session_set_X(egg_b200_session* s, const double* X, int64_t len)
         for (size_t j = 0; j < S.nb_gid.size(); ++j) {
             for (int k = 0; k < D; ++k) { S.nb_val[j * D + k] = X[S.nb_gid[j] * D + k]; }
         }
+        reset_seeds(S);  // new positions: B-spline projections start cold
         S.sync();
     });
 }
@@ -2138,6 +2176,7 @@ int egg_b200_session_restore(egg_b200_session* s)
         EGG_CK(cudaSetDevice(S.device));
         const size_t n = size_t(S.nstore) * S.dim;
         if (n) { EGG_CK(cudaMemcpyAsync(S.X(S.cur), S.ckpt.p, n * sizeof(double), cudaMemcpyDeviceToDevice, S.stream)); }
+        reset_seeds(S);
         S.sync();
     });
 }

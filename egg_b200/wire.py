@@ -112,7 +112,8 @@ def free_mask_from_fixed(n_nodes: int, fixed_ids) -> np.ndarray:
 # src/geometry.hpp:1760-1928).
 ENTITY_KINDS = {1: ("line_seg", 4), 2: ("circle", 3), 3: ("ellipse", 4), 5: ("plane", 9), 6: ("circle_arc", 6),
                 7: ("ellipse_arc", 8), 8: ("quad_bezier", 8), 9: ("cubic_bezier", 10), 15: ("line_rail", 4),
-                16: ("line_rail3", 6), 4: ("sphere", 10), 12: ("cylinder", 10), 13: ("line3", 8)}
+                16: ("line_rail3", 6), 4: ("sphere", 10), 12: ("cylinder", 10), 13: ("line3", 8),
+                10: ("bspline", 6)}
 
 
 def flat_wire(
@@ -131,7 +132,9 @@ def flat_wire(
     identity) or ``(ns, d, d)`` per sample in canonical order.  Mirrors
     ``build_flat_context`` (``egg/smoothing/flat_context.py:136-346``) without
     interface, curvature or directional terms.  ``constraints`` maps a global
-    node id (not Free) to ``(tag, record)``: the node becomes a moving DOF on
+    node id (not Free) to ``(tag, record)`` or ``(tag, record, seg)``, seg the
+    entity's variable-length fields (a B-spline's knots, control points and
+    weights), sent as one ``{data, off}`` CSR field each: the node becomes a moving DOF on
     that entity (``ENTITY_KINDS``), with a stored patch, in one SoA partition
     per tag whose packed records follow the partition's ``dof_local`` order.
     ``compact`` drops the energy-stencil index arrays (see module docstring) and
@@ -241,6 +244,13 @@ def flat_wire(
             rec = np.array([np.asarray(constraints[n][1], dtype=np.float64)[:kf] for n in nodes])
             g["entities"][name] = {"tag": tag, "kFields": kf, "dof_local": local,
                                    "records": np.ascontiguousarray(rec.reshape(-1))}
+            if len(constraints[nodes[0]]) > 2:  # segmented fields: (knots, ctrl, weights) per node
+                seg = []
+                for k in range(len(constraints[nodes[0]][2])):
+                    parts = [np.asarray(constraints[n][2][k], dtype=np.float64).ravel() for n in nodes]
+                    off = np.concatenate([[0], np.cumsum([len(x) for x in parts])]).astype(np.int32)
+                    seg.append({"data": np.concatenate(parts) if parts else np.zeros(0), "off": off})
+                g["entities"][name]["seg"] = seg
 
         g.update(fields(m_sid, uniform_out=True))
         groups.append(g)

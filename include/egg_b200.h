@@ -51,6 +51,9 @@ extern "C" {
 #define EGG_B200_TAG_ELLIPSEARC 7 /* record (cx, cy, a, b, phi, t0, t1, closed): rotated elliptic arc */
 #define EGG_B200_TAG_QUADBEZIER 8 /* record (p0, p1, p2, t0, t1): quadratic Bezier, trimmed to [t0, t1] */
 #define EGG_B200_TAG_CUBICBEZIER 9 /* record (p0, p1, p2, p3, t0, t1): cubic Bezier, trimmed to [t0, t1] */
+#define EGG_B200_TAG_BSPLINE 10  /* record (degree, n_ctrl, t0, t1, closed, has_w, knots_at, ctrl_at, w_at):
+                                  * B-spline / NURBS curve, degree <= 7; the *_at fields are offsets into
+                                  * entity_arena (knots n_ctrl+degree+1, ctrl 2 n_ctrl, weights n_ctrl) */
 #define EGG_B200_TAG_LINERAIL 15 /* record (sx, sy, ex, ey): open-ended segment, released beyond its ends */
 #define EGG_B200_TAG_SPHERE 4    /* 3D record (c(3), r, ax(3), ay(3)): untrimmed sphere, frame ax, ay, ax x ay */
 #define EGG_B200_TAG_PLANE 5     /* 3D record (o(3), ax(3), ay(3)): untrimmed plane, orthonormal in-plane axes */
@@ -131,6 +134,13 @@ typedef struct egg_b200_session_desc {
      * sweep of each run call; later sweeps search in its angle instead
      * (src/sweep.hpp:1718-1876). */
     const double* entity_params; /* [ndof * EGG_B200_ENTITY_FIELDS] or NULL */
+    /* Variable-length entity data (B-spline knots, control points, weights),
+     * addressed by offsets in the records.  A session with B-spline DOFs keeps
+     * a per-DOF seed (the last foot parameter) for their iterative projection,
+     * as the reference does (src/sweep.hpp:325-336): cold at creation and after
+     * set_X / restore. */
+    const double* entity_arena; /* [entity_arena_len] or NULL */
+    int64_t entity_arena_len;
 } egg_b200_session_desc;
 
 /* Control-net wire for one block (src/control_net.hpp:72-87 ControlNetHostT;

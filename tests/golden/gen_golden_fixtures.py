@@ -144,6 +144,7 @@ CASES_CON = {
     "disk_earcs17": ("disk_on_curve", dict(n=17, seed=9, ry=0.6, arcs=True)),
     "square_bezier17": ("square_bezier", dict(n=17, seed=10)),
     "cube_curved9": ("cube_curved", dict(n=9, seed=11)),
+    "square_bspline17": ("square_bspline", dict(n=17, seed=12)),
 }
 RUNS_CON = [
     # (case, phase, delta, omega, n_sweeps)
@@ -163,6 +164,9 @@ RUNS_CON = [
     ("square_bezier17", "barrier", 0.0, 0.8, 30),
     ("cube_curved9", "barrier", 0.0, 1.0, 20),
     ("cube_curved9", "barrier", 0.0, 0.8, 20),
+    ("square_bspline17", "barrier", 0.0, 1.0, 30),
+    ("square_bspline17", "barrier", 0.0, 0.8, 30),
+    ("square_bspline17", "shape_size", 0.0, 1.0, 20),
 ]
 # FAS V-cycles on sliding-boundary grids: (case, phase, n_cycles, nu_pre, nu_post, nu_coarse, omega, max_levels)
 FAS_RUNS_CON = [
@@ -173,6 +177,7 @@ FAS_RUNS_CON = [
     ("cube_slide9", "barrier", 3, 2, 2, 16, 1.0, 32),
     ("square_bezier17", "barrier", 3, 2, 2, 32, 1.0, 32),
     ("cube_curved9", "barrier", 3, 2, 2, 16, 1.0, 32),
+    ("square_bspline17", "barrier", 3, 2, 2, 32, 1.0, 32),
 ]
 ENTITY_RECORDS = {
     1: (0.1, -0.2, 0.9, 0.4),
@@ -232,6 +237,16 @@ def _constrained_runs() -> dict:
     e_b, _ = sess.run(20, report_every=1)
     out["twocalls/disk_arcs17/E"] = np.concatenate([e_a, e_b])
     out["twocalls/disk_arcs17/X"] = sess.get_X()
+    # B-spline seeds: two run calls, then a fresh session from the positions
+    # reached (positions uploaded anew: seeds cold) and a third call
+    g = case_grid("square_bspline17")
+    sess = ref.CppStructuredSweepSession(g.wire(), g.structured(), g.X_flat(), device="cpu", dim=2)
+    e_a, _ = sess.run(7, report_every=1)
+    e_b, _ = sess.run(12, report_every=1)
+    sess = ref.CppStructuredSweepSession(g.wire(), g.structured(), sess.get_X(), device="cpu", dim=2)
+    e_c, _ = sess.run(6, report_every=1)
+    out["seeds/square_bspline17/E"] = np.concatenate([e_a, e_b, e_c])
+    out["seeds/square_bspline17/X"] = sess.get_X()
     for case in ("cube_slide9", "cube_curved9"):
         g = case_grid(case)
         sess = ref.CppStructuredSweepSession(g.wire(), g.structured(), g.X_flat(), device="cpu", dim=3)

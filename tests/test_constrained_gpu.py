@@ -1,5 +1,5 @@
 """Constrained boundary DOFs on the GPU: nodes sliding on a Circle, an
-Ellipse, trimmed CircleArcs, EllipseArcs and Beziers, LineSegs, a LineRail,
+Ellipse, trimmed CircleArcs, EllipseArcs, Beziers and B-splines, LineSegs, a LineRail,
 Planes, a Sphere, a Cylinder, a Line3 and a LineRail3 relax exactly as the reference core relaxes
 them (first sweep and trajectory, fp64), the mixed path tracks that, every
 accepted boundary node lies on its entity, a batch of constrained meshes
@@ -66,7 +66,7 @@ def test_constrained_sweeps_match_reference(gpu, run):
 
 
 @pytest.mark.parametrize("case", ["disk_circle17", "disk_ellipse17", "square_slide17", "disk_arcs17",
-                                  "disk_earcs17", "square_bezier17"])
+                                  "disk_earcs17", "square_bezier17"])  # (B-splines: see the seeds test)
 def test_accepted_boundary_nodes_lie_on_their_entity(gpu, case):
     g = case_grid(case)
     s = _session(gpu, g)
@@ -104,6 +104,24 @@ def test_arcs_cold_first_sweep_per_call_and_graph_chunks(gpu):
     np.testing.assert_allclose(eb, two[10:][3::4], rtol=1e-9)
     assert np.abs(s2.get_X() - _FX["twocalls/disk_arcs17/X"]).max() <= 1e-9 * _hmin(g)
     assert abs(two[-1] - E30[-1]) > 1e-6 * abs(E30[-1])
+
+
+def test_bspline_seeds_persist_across_calls_and_reset_on_set_x(gpu):
+    """B-spline DOFs warm-start their projection from the last foot
+    parameter: it persists across run calls (7 + 12 sweeps) and resets when
+    set_X replaces the positions, so the last 6 sweeps equal a fresh reference
+    session started from the positions reached."""
+    g = case_grid("square_bspline17")
+    s = _session(gpu, g)
+    ea, _ = s.run(7, report_every=1)
+    eb, _ = s.run(12, report_every=4)
+    s.set_X(s.get_X())
+    ec, _ = s.run(6, report_every=1)
+    ref = _FX["seeds/square_bspline17/E"]
+    np.testing.assert_allclose(ea, ref[:7], rtol=1e-9)
+    np.testing.assert_allclose(eb, ref[7:19][3::4], rtol=1e-9)
+    np.testing.assert_allclose(ec, ref[19:], rtol=1e-9)
+    assert np.abs(s.get_X() - _FX["seeds/square_bspline17/X"]).max() <= 1e-9 * _hmin(g)
 
 
 def test_curved_cube_restarts_cold_per_call(gpu):
@@ -162,7 +180,7 @@ def test_constrained_mixed_tracks_fp64(gpu, case):
 
 def test_constrained_batch_equals_separate_sessions(gpu):
     gs = [case_grid("disk_circle17"), case_grid("square_slide17"), case_grid("disk_ellipse17"),
-          case_grid("disk_arcs17")]
+          case_grid("disk_arcs17"), case_grid("square_bspline17"), configs.square_bspline(13, seed=21)]
     b = gpu.CppBatchSweepSession([(g.wire(compact=True), g.structured(), g.X_flat()) for g in gs],
                                  precision="mixed")
     b.set_variant(1)
