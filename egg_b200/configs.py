@@ -31,7 +31,7 @@ from . import wire as _wire
 __all__ = [
     "Grid", "unit_square", "disk_oh", "tangled_square", "unit_cube", "two_cubes", "sphere_in_cube",
     "grid_mindet", "mean_size_w_inv", "disk_on_curve", "square_sliding", "cube_sliding", "square_bezier",
-    "cube_curved", "square_bspline",
+    "cube_curved", "square_bspline", "square_composite",
 ]
 
 
@@ -338,6 +338,48 @@ def square_bspline(n: int = 17, frac: float = 0.2, slide: float = 0.3, seed: int
         for v in nodes:
             cons[int(v)] = (10, rec, seg)
     return Grid(f"square_bspline{n}", 2, g.blocks, X, g.free.copy(), {"frac": frac, "seed": seed}, cons)
+
+
+def _composite_block(segs) -> np.ndarray:
+    """Composite segment records: [tag, params...] padded to 13 reals each."""
+    out = np.zeros((len(segs), 13))
+    for k, (tag, params) in enumerate(segs):
+        out[k, 0] = tag
+        out[k, 1 : 1 + len(params)] = params
+    return out.ravel()
+
+
+def square_composite(n: int = 17, frac: float = 0.2, slide: float = 0.3, seed: int = 0) -> Grid:
+    """Unit square whose bottom and top sides are composite paths (tag 11):
+    bottom = LineSeg (0,0)-(0.3,0), QuadBezier (0.3,0)-(0.5,-0.05)-(0.7,0),
+    LineSeg (0.7,0)-(1,0); top = CubicBezier (0,1)-(0.2,1.05)-(0.4,1.03)-(0.5,1)
+    then a shallow arc of the ellipse about (0.75, 1.27) with semi-axes
+    (0.25 / sqrt(0.19), 0.3) from (0.5, 1) to (1, 1) (EllipseArc).  Side nodes sit on their
+    path at x = i/(n-1) moved by up to ``slide`` of a step, and slide along
+    it.  Corners stay fixed."""
+    g = unit_square(n, frac=frac, seed=seed)
+    ids = g.blocks[0]
+    X = g.X.copy()
+    rng = np.random.default_rng(seed + 707)
+    x = np.linspace(0.0, 1.0, n)[1:-1] + rng.uniform(-slide, slide, n - 2) / (n - 1)
+    bot = [(1, (0.0, 0.0, 0.3, 0.0)), (8, (0.3, 0.0, 0.5, -0.05, 0.7, 0.0, 0.0, 1.0)), (1, (0.7, 0.0, 1.0, 0.0))]
+    ea = 0.25 / np.sqrt(0.19)
+    t0, t1 = np.arctan2(-0.9, -0.25 / ea) % (2 * np.pi), np.arctan2(-0.9, 0.25 / ea) % (2 * np.pi)
+    top = [(9, (0.0, 1.0, 0.2, 1.05, 0.4, 1.03, 0.5, 1.0, 0.0, 1.0)),
+           (7, (0.75, 1.27, ea, 0.3, 0.0, t0, t1, 0.0))]
+    yb = np.where((x > 0.3) & (x < 0.7), 2 * (1 - (x - 0.3) / 0.4) * ((x - 0.3) / 0.4) * -0.05, 0.0)
+    X[ids[1:-1, 0]] = np.stack([x, yb], axis=1)
+    tt = np.clip(x / 0.5, 0.0, 1.0)
+    cub = _bezier(np.array(top[0][1][:8]).reshape(4, 2), tt)
+    ang = t0 + (t1 - t0) * np.clip((x - 0.5) / 0.5, 0.0, 1.0)
+    ell = np.stack([0.75 + ea * np.cos(ang), 1.27 + 0.3 * np.sin(ang)], axis=1)
+    X[ids[1:-1, -1]] = np.where((x <= 0.5)[:, None], cub, ell)
+    cons = {}
+    for nodes, segs in ((ids[1:-1, 0], bot), (ids[1:-1, -1], top)):
+        blk = _composite_block(segs)
+        for v in nodes:
+            cons[int(v)] = (11, (float(len(segs)), 0.0), (blk,))
+    return Grid(f"square_composite{n}", 2, g.blocks, X, g.free.copy(), {"frac": frac, "seed": seed}, cons)
 
 
 def cube_sliding(n: int = 9, frac: float = 0.2, slide: float = 0.3, off: float = 0.02, seed: int = 0,

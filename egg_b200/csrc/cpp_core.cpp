@@ -242,6 +242,9 @@ void fill_desc(Desc& D, const py::dict& ctx, const py::dict& st, const DArr& X, 
                 if (tag == EGG_B200_TAG_BSPLINE && seg_off.size() < 2) {
                     throw py::value_error("validate_context: a B-spline partition needs its knots and ctrl seg fields");
                 }
+                if (tag == EGG_B200_TAG_COMPOSITE && seg_off.empty()) {
+                    throw py::value_error("validate_context: a composite partition needs its arena seg field");
+                }
                 for (py::ssize_t i = 0; i < dl.size(); ++i) {
                     const int32_t v = dl.data()[i];
                     if (v < 0 || v >= d.ndof) { throw py::value_error("validate_context: dof_local out of range"); }
@@ -256,6 +259,9 @@ void fill_desc(Desc& D, const py::dict& ctx, const py::dict& st, const DArr& X, 
                         for (size_t k = 0; k < 3 && k < seg_off.size(); ++k) {
                             er[6 + k] = double(seg_base[k] + seg_off[k].data()[i]);
                         }
+                    }
+                    if (tag == EGG_B200_TAG_COMPOSITE && !seg_off.empty()) {  // the entity's arena slice
+                        er[6] = double(seg_base[0] + seg_off[0].data()[i]);
                     }
                 }
             }

@@ -637,6 +637,64 @@ EGG_HD void entity_newton_step(int tag, const double* e, const double H[4], cons
     out[1] = by * y;
 }
 
+// ---- composite path (tag 11) -------------------------------------------------
+// Record (n_segs, rec_off, .., slice_at): segment records of kCompositeRec
+// reals each, [tag, params...] with the positional params of that tag, at
+// arena[slice_at + rec_off ...].  A point projects onto every segment and
+// keeps the nearest (strictly closer wins; the first on a tie); the tangent is
+// that segment's (src/geometry.hpp:955-981, 2587-2617).
+constexpr int kCompositeRec = 13;
+
+EGG_HD bool composite_segment_ok(int tag)
+{
+    return tag == EGG_B200_TAG_LINESEG || tag == EGG_B200_TAG_CIRCLE || tag == EGG_B200_TAG_ELLIPSE ||
+           tag == EGG_B200_TAG_LINERAIL || is_tcurve(tag);
+}
+
+EGG_HD void composite_frame(const double* recs, int n_segs, double px, double py, double& qx, double& qy,
+                            double& tx, double& ty)
+{
+    qx = px;
+    qy = py;
+    tx = 1.0;
+    ty = 0.0;
+    double best = INFINITY;
+    for (int k = 0; k < n_segs; ++k) {
+        const double* rec = recs + k * kCompositeRec;
+        const int tag = int(rec[0]);
+        if (!composite_segment_ok(tag)) { continue; }
+        double fx, fy;
+        entity_project(tag, rec + 1, px, py, fx, fy);
+        const double dx = fx - px, dy = fy - py;
+        const double dd = dx * dx + dy * dy;
+        if (dd < best) {
+            best = dd;
+            qx = fx;
+            qy = fy;
+            entity_tangent(tag, rec + 1, px, py, tx, ty);
+        }
+    }
+}
+
+EGG_HD void composite_newton_step(const double* recs, int n_segs, const double H[4], const double g[2], double px,
+                                  double py, double out[2])
+{
+    double qx, qy, bx, by;
+    composite_frame(recs, n_segs, px, py, qx, qy, bx, by);
+    const double hb0 = H[0] * bx + H[1] * by;
+    const double hb1 = H[2] * bx + H[3] * by;
+    const double M = bx * hb0 + by * hb1;
+    const double r = bx * g[0] + by * g[1];
+    double y = 0.0;
+    const double rn = fabs(r);
+    if (!(rn < kGeomZnorm)) {
+        y = -r / M;
+        if (!isfinite(y)) { y = -0.1 * r / rn; }
+    }
+    out[0] = bx * y;
+    out[1] = by * y;
+}
+
 // Tags this core relaxes in dimension dim.
 EGG_HD bool entity_supported(int dim, int tag)
 {
@@ -646,7 +704,7 @@ EGG_HD bool entity_supported(int dim, int tag)
     }
     return dim == 2 && (tag == EGG_B200_TAG_LINESEG || tag == EGG_B200_TAG_CIRCLE ||
                         tag == EGG_B200_TAG_ELLIPSE || tag == EGG_B200_TAG_LINERAIL || is_tcurve(tag) ||
-                        tag == EGG_B200_TAG_BSPLINE);
+                        tag == EGG_B200_TAG_BSPLINE || tag == EGG_B200_TAG_COMPOSITE);
 }
 
 }  // namespace egg_b200

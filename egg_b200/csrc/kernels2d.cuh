@@ -925,6 +925,9 @@ __global__ void stored_patch_kernel(StoredPatch2 sp, const double2* __restrict__
         // projection starts its Newton solve there and stores its result
         // (src/sweep.hpp:1219-1265).
         const bool bsp = etag == EGG_B200_TAG_BSPLINE;
+        const bool comp = etag == EGG_B200_TAG_COMPOSITE;
+        const double* crec = comp ? sp.arena + int64_t(er[6]) + int64_t(er[1]) : nullptr;
+        const int cseg = comp ? int(er[0]) : 0;
         double seed = bsp ? sp.seeds[d] : 0.0;
         BSplineCurve bc {};
         if (bsp) { bc = bspline_view(er, sp.arena); }
@@ -932,6 +935,10 @@ __global__ void stored_patch_kernel(StoredPatch2 sp, const double2* __restrict__
         double qstar = 0.0, dq = 0.0;
         if (etag == 0) {
             solve2<double>(h, g, dl);
+        } else if (comp) {  // one path for every sweep: step on the nearest segment's tangent
+            composite_newton_step(crec, cseg, h, g, pos.x, pos.y, dl);
+            dl[0] *= omega;
+            dl[1] *= omega;
         } else if (bsp) {
             if (sp.cold) {
                 bspline_cold_step(bc, h, g, pos.x, pos.y, seed, dl);
@@ -951,7 +958,10 @@ __global__ void stored_patch_kernel(StoredPatch2 sp, const double2* __restrict__
         double2 cur = pos;
         for (int it = 0; it < 10; ++it) {
             double2 trial = make_double2(pos.x + alpha * dl[0], pos.y + alpha * dl[1]);
-            if (bsp) {
+            if (comp) {
+                double tx, ty;
+                composite_frame(crec, cseg, trial.x, trial.y, trial.x, trial.y, tx, ty);
+            } else if (bsp) {
                 if (sp.cold) {
                     bspline_project_seeded(bc, trial.x, trial.y, seed, trial.x, trial.y);
                 } else {

@@ -128,6 +128,7 @@ struct LevelData {
     int64_t n_constrained = 0;  // stored DOFs on a boundary entity
     int64_t n_arc = 0;          // of which on a parametric entity (arc, plane: cold first sweep per run call)
     int64_t n_bspline = 0;      // of which on a B-spline curve (seeded projection)
+    int64_t n_composite = 0;    // of which on a composite path
     DevBuf<double> arena;       // entity arena (B-spline knots, control points, weights)
     DevBuf<double> seeds;       // [n_stored] last foot parameter of each B-spline DOF
     DevBuf<int8_t> st_etag;     // [n_stored] entity tag (uploaded when n_constrained > 0)
@@ -606,6 +607,21 @@ static Session* create_session(const egg_b200_session_desc& d)
             if (d.interior_block && d.interior_block[i] >= 0) {
                 throw Error(EGG_B200_ENOTSUP, "egg_b200: a constrained DOF on the structured-interior path");
             }
+            if (etag == EGG_B200_TAG_COMPOSITE) {
+                const double* r = d.entity_params + i * EGG_B200_ENTITY_FIELDS;
+                const int64_t ns = int64_t(r[0]), ro = int64_t(r[1]), at = int64_t(r[6]);
+                if (double(ns) != r[0] || ns < 1 || double(ro) != r[1] || ro < 0 || double(at) != r[6] || at < 0 ||
+                    !d.entity_arena || at + ro + ns * kCompositeRec > d.entity_arena_len) {
+                    invalid("validate_context: composite segment records outside entity_arena");
+                }
+                for (int64_t k = 0; k < ns; ++k) {
+                    const int st = int(d.entity_arena[at + ro + k * kCompositeRec]);
+                    if (st != 0 && st != EGG_B200_TAG_COMPOSITE && !composite_segment_ok(st)) {
+                        throw Error(EGG_B200_ENOTSUP, "egg_b200: composite segment tag " + std::to_string(st) +
+                                                        " is not supported (fixed-size 2D curves are)");
+                    }
+                }
+            }
             if (etag == EGG_B200_TAG_BSPLINE) {
                 const double* r = d.entity_params + i * EGG_B200_ENTITY_FIELDS;
                 const int64_t deg = int64_t(r[0]), nc = int64_t(r[1]);
@@ -656,6 +672,7 @@ static Session* create_session(const egg_b200_session_desc& d)
             S->n_arc++;
         }
         if (etag == EGG_B200_TAG_BSPLINE) { S->n_bspline++; }
+        if (etag == EGG_B200_TAG_COMPOSITE) { S->n_composite++; }
         for (int64_t p = p0; p < p0 + P; ++p) {
             auto remap = [&](int32_t g) {
                 const int32_t s = S->g2s[g];
@@ -896,8 +913,10 @@ static Session* create_session(const egg_b200_session_desc& d)
         S->st_etag.upload(st_etag);
         S->st_epar.upload(st_epar);
     }
-    if (S->n_bspline) {
+    if (S->n_bspline || S->n_composite) {
         S->arena.upload(std::vector<double>(d.entity_arena, d.entity_arena + d.entity_arena_len));
+    }
+    if (S->n_bspline) {
         S->seeds.alloc(size_t(S->n_stored));
         EGG_CK(cudaMemset(S->seeds.p, 0xFF, size_t(S->n_stored) * sizeof(double)));  // all-ones: NaN
     }
@@ -1070,7 +1089,7 @@ static StoredPatch2 stored_view(LevelData& S)
     sp.etag = S.n_constrained ? S.st_etag.p : nullptr;
     sp.epar = S.n_constrained ? S.st_epar.p : nullptr;
     sp.cold = 0;
-    sp.arena = S.n_bspline ? S.arena.p : nullptr;
+    sp.arena = (S.n_bspline || S.n_composite) ? S.arena.p : nullptr;
     sp.seeds = S.n_bspline ? S.seeds.p : nullptr;
     return sp;
 }

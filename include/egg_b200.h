@@ -54,6 +54,9 @@ extern "C" {
 #define EGG_B200_TAG_BSPLINE 10  /* record (degree, n_ctrl, t0, t1, closed, has_w, knots_at, ctrl_at, w_at):
                                   * B-spline / NURBS curve, degree <= 7; the *_at fields are offsets into
                                   * entity_arena (knots n_ctrl+degree+1, ctrl 2 n_ctrl, weights n_ctrl) */
+#define EGG_B200_TAG_COMPOSITE 11 /* record (n_segs, rec_off, 0, 0, 0, 0, slice_at): a path of segment records
+                                   * [tag, 12 params] at entity_arena[slice_at + rec_off ...]; segments are the
+                                   * fixed-size 2D curves (tags 1, 2, 3, 6, 7, 8, 9, 15) */
 #define EGG_B200_TAG_LINERAIL 15 /* record (sx, sy, ex, ey): open-ended segment, released beyond its ends */
 #define EGG_B200_TAG_SPHERE 4    /* 3D record (c(3), r, ax(3), ay(3)): untrimmed sphere, frame ax, ay, ax x ay */
 #define EGG_B200_TAG_PLANE 5     /* 3D record (o(3), ax(3), ay(3)): untrimmed plane, orthonormal in-plane axes */

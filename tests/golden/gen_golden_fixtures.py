@@ -145,6 +145,7 @@ CASES_CON = {
     "square_bezier17": ("square_bezier", dict(n=17, seed=10)),
     "cube_curved9": ("cube_curved", dict(n=9, seed=11)),
     "square_bspline17": ("square_bspline", dict(n=17, seed=12)),
+    "square_composite17": ("square_composite", dict(n=17, seed=13)),
 }
 RUNS_CON = [
     # (case, phase, delta, omega, n_sweeps)
@@ -167,6 +168,8 @@ RUNS_CON = [
     ("square_bspline17", "barrier", 0.0, 1.0, 30),
     ("square_bspline17", "barrier", 0.0, 0.8, 30),
     ("square_bspline17", "shape_size", 0.0, 1.0, 20),
+    ("square_composite17", "barrier", 0.0, 1.0, 30),
+    ("square_composite17", "barrier", 0.0, 0.8, 30),
 ]
 # FAS V-cycles on sliding-boundary grids: (case, phase, n_cycles, nu_pre, nu_post, nu_coarse, omega, max_levels)
 FAS_RUNS_CON = [
@@ -178,6 +181,7 @@ FAS_RUNS_CON = [
     ("square_bezier17", "barrier", 3, 2, 2, 32, 1.0, 32),
     ("cube_curved9", "barrier", 3, 2, 2, 16, 1.0, 32),
     ("square_bspline17", "barrier", 3, 2, 2, 32, 1.0, 32),
+    ("square_composite17", "barrier", 3, 2, 2, 32, 1.0, 32),
 ]
 ENTITY_RECORDS = {
     1: (0.1, -0.2, 0.9, 0.4),

@@ -21,7 +21,8 @@ _FX = np.load(GOLDEN / "ref_constrained.npz")
 @pytest.mark.parametrize("grid", [configs.disk_on_curve(9), configs.disk_on_curve(9, ry=0.6),
                                   configs.disk_on_curve(9, arcs=True), configs.disk_on_curve(9, ry=0.6, arcs=True),
                                   configs.square_sliding(9), configs.square_bezier(9),
-                                  configs.cube_sliding(5), configs.cube_curved(5), configs.square_bspline(9)],
+                                  configs.cube_sliding(5), configs.cube_curved(5), configs.square_bspline(9),
+                                  configs.square_composite(9)],
                          ids=lambda g: g.name)
 def test_wire_partitions_cover_every_dof_once(grid):
     grp = grid.wire()["groups"][0]
