@@ -16,6 +16,15 @@
 #include "egg_b200.h"
 #include "metric.cuh"
 
+// Out-of-line on the device: the iterative curve routines (grid + Newton
+// feet, B-spline evaluation, composite search) are called from many sites and
+// only for constrained DOFs, so inlining them would only grow the kernels.
+#ifdef __CUDACC__
+#define EGG_OUTLINE __host__ __device__ __noinline__
+#else
+#define EGG_OUTLINE inline
+#endif
+
 namespace egg_b200
 {
 
@@ -85,7 +94,7 @@ EGG_HD double tc_clamp(int tag, const double* e, double q)
 }
 
 // Position (nd = 0), first (nd = 1) or second (nd = 2) derivative at t.
-EGG_HD void tc_eval(int tag, const double* e, double t, int nd, double& x, double& y)
+EGG_OUTLINE void tc_eval(int tag, const double* e, double t, int nd, double& x, double& y)
 {
     if (tag == EGG_B200_TAG_CIRCLEARC) {
         const double c = cos(t), s = sin(t);
@@ -156,7 +165,7 @@ EGG_HD void tc_eval(int tag, const double* e, double t, int nd, double& x, doubl
 
 // Nearest-foot parameter on [lo, hi]: the best of 17 grid samples, then 8
 // Newton steps on (C(t) - q).C'(t) (src/geometry.hpp:518-560 project_param).
-EGG_HD double tc_grid_newton(int tag, const double* e, double qx, double qy, double lo, double hi)
+EGG_OUTLINE double tc_grid_newton(int tag, const double* e, double qx, double qy, double lo, double hi)
 {
     double best_t = lo, best_d = INFINITY;
     for (int i = 0; i <= 16; ++i) {
@@ -362,7 +371,7 @@ EGG_HD void bspline_basis(const BSplineCurve& c, int span, double u, int nd, dou
 }
 
 // Curve point (order 0) or its first / second derivative at u.
-EGG_HD void bspline_point(const BSplineCurve& c, double u, int order, double& x, double& y)
+EGG_OUTLINE void bspline_point(const BSplineCurve& c, double u, int order, double& x, double& y)
 {
     const int span = bspline_span(c, u);
     double der[3][kBSplineCap];
@@ -409,7 +418,7 @@ EGG_HD void bspline_point(const BSplineCurve& c, double u, int order, double& x,
 // Seeded nearest-foot parameter on the live domain [knots[p], knots[n]]:
 // from the clamped seed when it is finite, else the best of 17 grid samples;
 // then 8 Newton steps (src/geometry.hpp:518-560 project_param_seeded).
-EGG_HD double bspline_foot(const BSplineCurve& c, double qx, double qy, double seed)
+EGG_OUTLINE double bspline_foot(const BSplineCurve& c, double qx, double qy, double seed)
 {
     const double lo = c.knots[c.p], hi = c.knots[c.n];
     double t;
@@ -651,7 +660,7 @@ EGG_HD bool composite_segment_ok(int tag)
            tag == EGG_B200_TAG_LINERAIL || is_tcurve(tag);
 }
 
-EGG_HD void composite_frame(const double* recs, int n_segs, double px, double py, double& qx, double& qy,
+EGG_OUTLINE void composite_frame(const double* recs, int n_segs, double px, double py, double& qx, double& qy,
                             double& tx, double& ty)
 {
     qx = px;

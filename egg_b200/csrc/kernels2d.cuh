@@ -846,7 +846,7 @@ constexpr int64_t kStoredFillThreads3 = 148 * 16384;
 // (gradient, contracted Hessian, energy; then each line-search trial) and
 // reduce across the group, so a ragged patch of 16-64 gathered samples can be
 // a few rounds of parallel work instead of one thread's serial loop.
-template <int KIND, int G>
+template <int KIND, int G, bool CON>
 __global__ void stored_patch_kernel(StoredPatch2 sp, const double2* __restrict__ Xin,
                                     double2* __restrict__ Xout, const double2* __restrict__ tau,
                                     double delta, double omega, double2* __restrict__ grad_out)
@@ -918,7 +918,8 @@ __global__ void stored_patch_kernel(StoredPatch2 sp, const double2* __restrict__
         // A trimmed curve after the first sweep of a run call searches in its
         // parameter instead (src/sweep.hpp:1718-1876): trials q* + alpha dq,
         // clamped onto the trim and evaluated on the curve.
-        const int etag = sp.etag != nullptr ? int(sp.etag[d]) : 0;
+        // CON = false (a level without constrained DOFs) compiles none of it.
+        const int etag = (CON && sp.etag != nullptr) ? int(sp.etag[d]) : 0;
         const double* er = sp.epar + (etag != 0 ? d * EGG_B200_ENTITY_FIELDS : 0);
         const bool warm_arc = is_tcurve(etag) && !sp.cold;
         // B-spline DOFs carry a seed (their last foot parameter): every seeded

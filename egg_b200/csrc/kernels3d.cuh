@@ -479,7 +479,7 @@ __device__ __forceinline__ void assemble_T3(const double* X, int32_t ic, const i
 
 // Stored-patch sweep, 3D, G lanes per DOF (see stored_patch_kernel): the
 // lanes split the DOF's samples and reduce across the group.
-template <int KIND, int G>
+template <int KIND, int G, bool CON>
 __global__ void stored3_kernel(StoredPatch3 sp, const double* __restrict__ Xin, double* __restrict__ Xout,
                                const double* __restrict__ tau, double delta, double omega, double* __restrict__ grad_out)
 {
@@ -538,7 +538,8 @@ __global__ void stored3_kernel(StoredPatch3 sp, const double* __restrict__ Xin, 
         // the entity's tangent space, damped by omega before the line
         // search, every trial on the entity; a parametric entity after the
         // first sweep of a run call searches in its parameters.
-        const int etag = sp.etag != nullptr ? int(sp.etag[d]) : 0;
+        // CON = false (a level without constrained DOFs) compiles none of it.
+        const int etag = (CON && sp.etag != nullptr) ? int(sp.etag[d]) : 0;
         const double* er = sp.epar + (etag != 0 ? d * EGG_B200_ENTITY_FIELDS : 0);
         const bool warm_param = is_param3(etag) && !sp.cold;
         double dl[3] = {0.0, 0.0, 0.0};

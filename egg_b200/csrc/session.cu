@@ -1124,12 +1124,20 @@ static void launch_stored(Session& S, LevelData& L, const double* xin, double* x
                          L.st_wstride, L.st_wt.p, L.st_wtstride,
                          L.n_constrained ? L.st_etag.p : nullptr, L.n_constrained ? L.st_epar.p : nullptr,
                          cold ? 1 : 0};
-        S.timed(kKStored, [&] {
+        auto go3 = [&](auto con) {
+            constexpr bool C = decltype(con)::value;
             switch (G) {
-            case 32: stored3_kernel<KIND, 32><<<grid, 128, 0, st>>>(sp, xin, xout, tau, delta, omega, gout); break;
-            case 8: stored3_kernel<KIND, 8><<<grid, 128, 0, st>>>(sp, xin, xout, tau, delta, omega, gout); break;
-            case 2: stored3_kernel<KIND, 2><<<grid, 128, 0, st>>>(sp, xin, xout, tau, delta, omega, gout); break;
-            default: stored3_kernel<KIND, 1><<<grid, 128, 0, st>>>(sp, xin, xout, tau, delta, omega, gout); break;
+            case 32: stored3_kernel<KIND, 32, C><<<grid, 128, 0, st>>>(sp, xin, xout, tau, delta, omega, gout); break;
+            case 8: stored3_kernel<KIND, 8, C><<<grid, 128, 0, st>>>(sp, xin, xout, tau, delta, omega, gout); break;
+            case 2: stored3_kernel<KIND, 2, C><<<grid, 128, 0, st>>>(sp, xin, xout, tau, delta, omega, gout); break;
+            default: stored3_kernel<KIND, 1, C><<<grid, 128, 0, st>>>(sp, xin, xout, tau, delta, omega, gout); break;
+            }
+        };
+        S.timed(kKStored, [&] {
+            if (L.n_constrained) {
+                go3(std::true_type {});
+            } else {
+                go3(std::false_type {});
             }
         });
         return;
@@ -1140,12 +1148,22 @@ static void launch_stored(Session& S, LevelData& L, const double* xin, double* x
     auto* o2 = reinterpret_cast<double2*>(xout);
     const auto* t2 = reinterpret_cast<const double2*>(tau);
     auto* g2 = reinterpret_cast<double2*>(gout);
-    S.timed(kKStored, [&] {
+    auto go2 = [&](auto con) {
+        constexpr bool C = decltype(con)::value;
         switch (G) {
-        case 32: stored_patch_kernel<KIND, 32><<<grid, 128, 0, st>>>(sp, x2, o2, t2, delta, omega, g2); break;
-        case 8: stored_patch_kernel<KIND, 8><<<grid, 128, 0, st>>>(sp, x2, o2, t2, delta, omega, g2); break;
-        case 2: stored_patch_kernel<KIND, 2><<<grid, 128, 0, st>>>(sp, x2, o2, t2, delta, omega, g2); break;
-        default: stored_patch_kernel<KIND, 1><<<grid, 128, 0, st>>>(sp, x2, o2, t2, delta, omega, g2); break;
+        case 32: stored_patch_kernel<KIND, 32, C><<<grid, 128, 0, st>>>(sp, x2, o2, t2, delta, omega, g2); break;
+        case 8: stored_patch_kernel<KIND, 8, C><<<grid, 128, 0, st>>>(sp, x2, o2, t2, delta, omega, g2); break;
+        case 2: stored_patch_kernel<KIND, 2, C><<<grid, 128, 0, st>>>(sp, x2, o2, t2, delta, omega, g2); break;
+        default: stored_patch_kernel<KIND, 1, C><<<grid, 128, 0, st>>>(sp, x2, o2, t2, delta, omega, g2); break;
+        }
+    };
+    // Levels without constrained DOFs (every coarse FAS level, most meshes)
+    // launch the instantiation that carries no entity code.
+    S.timed(kKStored, [&] {
+        if (L.n_constrained) {
+            go2(std::true_type {});
+        } else {
+            go2(std::false_type {});
         }
     });
 }
