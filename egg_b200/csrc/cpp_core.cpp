@@ -593,14 +593,15 @@ class Session
 
     py::dict variants()
     {
-        int32_t v = 0, shape[4 * EGG_B200_NUM_VARIANTS];
+        int32_t v = 0, shape[5 * EGG_B200_NUM_VARIANTS];
         double t[EGG_B200_NUM_VARIANTS];
         check(egg_b200_session_variant_info(h_.get(), &v, shape, t, EGG_B200_NUM_VARIANTS));
         py::dict d;
         d["variant"] = v;
         py::list lst;
         for (int i = 0; i < EGG_B200_NUM_VARIANTS; ++i) {
-            lst.append(py::make_tuple(shape[4 * i], shape[4 * i + 1], shape[4 * i + 2], shape[4 * i + 3], t[i]));
+            lst.append(py::make_tuple(shape[5 * i], shape[5 * i + 1], shape[5 * i + 2], shape[5 * i + 3],
+                                      shape[5 * i + 4], t[i]));
         }
         d["table"] = lst;
         return d;

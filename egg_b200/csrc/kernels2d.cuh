@@ -360,7 +360,7 @@ __device__ float dmu2_guard64(double2 qc, double2 q0, double2 q1, int role, doub
     return float(m1 - m0);
 }
 
-template <int CI, int CJ, int MINB, int KIND, class C>
+template <int CI, int CJ, int MINB, int KIND, class C, int FD>
 __global__ void __launch_bounds__(CI* CJ, MINB)
   interior_tile_kernel(const double2* __restrict__ Xin, double2* __restrict__ Xout,
                        const Tile2* __restrict__ tiles, const BlockInfo* __restrict__ blocks,
@@ -368,10 +368,15 @@ __global__ void __launch_bounds__(CI* CJ, MINB)
                        double delta, double omega, double2* __restrict__ grad_out)
 {
     extern __shared__ __align__(16) unsigned char smem_raw[];
-    using S = TileShared2<CI, CJ, C, KIND>;
+    // FD = 0: CI x CJ cells per CTA, one per thread, for their (CI-1) x (CJ-1)
+    // interior DOFs.  FD = 1: CI x CJ DOFs per CTA, one per thread, over the
+    // (CI+1) x (CJ+1) cells around them, so no thread idles in phase 3.
+    constexpr int NT = CI * CJ;
+    constexpr int CH = FD ? CI + 1 : CI, CW = FD ? CJ + 1 : CJ;  // cells staged
+    using S = TileShared2<CH, CW, C, KIND>;
     S& sm = *reinterpret_cast<S*>(smem_raw);
-    constexpr int NC = CI * CJ;
-    constexpr int PW = CJ + 1;
+    constexpr int NC = CH * CW;
+    constexpr int PW = CW + 1;
 
     const Tile2 tile = tiles[blockIdx.x];
     const BlockInfo bi = blocks[tile.block];
@@ -380,7 +385,7 @@ __global__ void __launch_bounds__(CI* CJ, MINB)
     const int tid = threadIdx.x;
 
     // Phase 1: node window.
-    for (int k = tid; k < (CI + 1) * (CJ + 1); k += NC) {
+    for (int k = tid; k < (CH + 1) * PW; k += NT) {
         const int r = k / PW, c = k % PW;
         const int gi = r0 + r, gj = c0 + c;
         double2 v = make_double2(0.0, 0.0);
@@ -389,12 +394,13 @@ __global__ void __launch_bounds__(CI* CJ, MINB)
     }
     __syncthreads();
 
-    // Phase 2: cell (ci, cj) with base node window (ci, cj); thread = cell.
-    // Each thread accumulates the role contributions of its cell's four
-    // samples per corner in registers and stores them once to column `tid`
-    // of the shared cell arrays.
-    {
-        const int ci = tid / CJ, cj = tid % CJ;
+    // Phase 2: cell (ci, cj) with base node window (ci, cj); thread = cell
+    // (a second round for the extra cells of an FD tile).  Each thread
+    // accumulates the role contributions of its cell's four samples per
+    // corner in registers and stores them once to column `cell` of the shared
+    // cell arrays.
+    for (int cell = tid; cell < NC; cell += NT) {
+        const int ci = cell / CW, cj = cell % CW;
         const bool valid = (r0 + ci <= n0 - 2) && (c0 + cj <= n1 - 2);
         bool bad = false;
         C acc[4][5];  // role contributions per cell corner, stored once below
@@ -402,8 +408,8 @@ __global__ void __launch_bounds__(CI* CJ, MINB)
         for (int a = 0; a < 4; ++a) {
 #pragma unroll
             for (int q = 0; q < 5; ++q) { acc[a][q] = C(0); }
-            if constexpr (std::is_same_v<C, double>) { sm.mu[a][tid] = C(0); }
-            sm.det[a][tid] = C(1);
+            if constexpr (std::is_same_v<C, double>) { sm.mu[a][cell] = C(0); }
+            sm.det[a][cell] = C(1);
         }
         if (valid) {
             // The cell's four edges.  Sample b's columns are the axis-0 edge on
@@ -417,8 +423,8 @@ __global__ void __launch_bounds__(CI* CJ, MINB)
             if constexpr (kEdgeCache2<KIND, C>) {
 #pragma unroll
                 for (int k = 0; k < 2; ++k) {
-                    sm.E[k][tid] = make_float2(float(e0x[k]), float(e0y[k]));
-                    sm.E[2 + k][tid] = make_float2(float(e1x[k]), float(e1y[k]));
+                    sm.E[k][cell] = make_float2(float(e0x[k]), float(e0y[k]));
+                    sm.E[2 + k][cell] = make_float2(float(e1x[k]), float(e1y[k]));
                 }
             }
 #pragma unroll
@@ -436,8 +442,8 @@ __global__ void __launch_bounds__(CI* CJ, MINB)
                 }
                 RoleOut<C> o;
                 sample_roles<KIND, C>(ax, bx, ay, by, s0, s1, delta, o);
-                if constexpr (std::is_same_v<C, double>) { sm.mu[b][tid] = o.mu; }  // fp32 accepts on differences
-                sm.det[b][tid] = o.det;
+                if constexpr (std::is_same_v<C, double>) { sm.mu[b][cell] = o.mu; }  // fp32 accepts on differences
+                sm.det[b][cell] = o.det;
 #pragma unroll
                 for (int q = 0; q < 5; ++q) {
                     acc[b][q] += o.r[0][q];
@@ -449,14 +455,14 @@ __global__ void __launch_bounds__(CI* CJ, MINB)
 #pragma unroll
         for (int a = 0; a < 4; ++a) {
 #pragma unroll
-            for (int q = 0; q < 5; ++q) { sm.gh[a][q][tid] = acc[a][q]; }
+            for (int q = 0; q < 5; ++q) { sm.gh[a][q][cell] = acc[a][q]; }
         }
-        sm.bad[tid] = bad ? 1 : 0;
+        sm.bad[cell] = bad ? 1 : 0;
     }
     __syncthreads();
 
     // Phase 3: DOFs.
-    constexpr int DI = CI - 1, DJ = CJ - 1;
+    constexpr int DI = FD ? CI : CI - 1, DJ = FD ? CJ : CJ - 1;
     if (tid >= DI * DJ) { return; }
     const int ti = tid / DJ, tj = tid % DJ;
     const int gi = tile.i0 + ti, gj = tile.j0 + tj;
@@ -470,7 +476,7 @@ __global__ void __launch_bounds__(CI* CJ, MINB)
     for (int ci = 0; ci < 2; ++ci) {
 #pragma unroll
         for (int cj = 0; cj < 2; ++cj) {
-            const int cell = (ti + ci) * CJ + (tj + cj);
+            const int cell = (ti + ci) * CW + (tj + cj);
             const int a = (1 - ci) * 2 + (1 - cj);
             g0 += sm.gh[a][0][cell];
             g1 += sm.gh[a][1][cell];
@@ -494,8 +500,8 @@ __global__ void __launch_bounds__(CI* CJ, MINB)
         ty = C(tv.y);
     }
     if constexpr (std::is_same_v<C, float>) {
-        const int c00 = ti * CJ + tj;
-        if (sm.bad[c00] | sm.bad[c00 + 1] | sm.bad[c00 + CJ] | sm.bad[c00 + CJ + 1]) {
+        const int c00 = ti * CW + tj;
+        if (sm.bad[c00] | sm.bad[c00 + 1] | sm.bad[c00 + CW] | sm.bad[c00 + CW + 1]) {
             if (grad_out != nullptr) {
                 dof_update_fp64<KIND>(sm.P, PW, ti, tj, txd, tyd, delta, omega, grad_out + slot);
             } else {
@@ -544,7 +550,7 @@ __global__ void __launch_bounds__(CI* CJ, MINB)
 #pragma unroll
                 for (int cj = 0; cj < 2; ++cj) {
                     const int a = (1 - ci) * 2 + (1 - cj);
-                    const int cell = (ti + ci) * CJ + (tj + cj);
+                    const int cell = (ti + ci) * CW + (tj + cj);
 #pragma unroll
                     for (int r = 0; r < 3; ++r) {
                         const int b = (r == 0) ? a : ((r == 1) ? (a ^ 2) : (a ^ 1));

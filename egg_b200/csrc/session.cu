@@ -81,15 +81,16 @@ template <class T> struct DevBuf {
 // minimum resident CTAs per SM requested from the register allocator.  The
 // session's autotuner times each on the session's own data and keeps the
 // fastest (egg_b200_session_autotune).
-// 2D: (ci, cj) cells per CTA; 3D: (ci, cj, ck) DOFs per CTA.
+// 2D: (ci, cj) cells per CTA, or with fd = 1 (ci, cj) DOFs per CTA over the
+// (ci+1) x (cj+1) cells around them; 3D: (ci, cj, ck) DOFs per CTA.
 struct Variant {
-    int ci, cj, ck, minb;
+    int ci, cj, ck, minb, fd = 0;
 };
 constexpr int kNumVariants = EGG_B200_NUM_VARIANTS;
 // Host threads that copy X between the caller's buffer and pinned staging.
 constexpr int kMaxCopyThreads = 16;
 constexpr Variant kVar64[kNumVariants] = {{8, 32, 1, 2}, {8, 16, 1, 4}, {8, 16, 1, 5}, {8, 16, 1, 6}, {16, 16, 1, 3}};
-constexpr Variant kVar32[kNumVariants] = {{8, 32, 1, 3}, {8, 16, 1, 6}, {8, 16, 1, 8}, {16, 16, 1, 4}, {8, 16, 1, 7}};
+constexpr Variant kVar32[kNumVariants] = {{8, 16, 1, 6, 1}, {8, 16, 1, 6}, {8, 16, 1, 8}, {8, 16, 1, 7, 1}, {8, 16, 1, 7}};
 constexpr Variant kVar3_64[kNumVariants] = {{4, 8, 8, 1}, {4, 8, 8, 2}, {2, 8, 16, 2}, {2, 8, 16, 3}, {2, 4, 16, 4}};
 constexpr Variant kVar3_32[kNumVariants] = {{4, 8, 8, 1}, {4, 8, 8, 2}, {2, 8, 16, 2}, {2, 8, 16, 3}, {2, 4, 16, 4}};
 
@@ -118,7 +119,7 @@ struct LevelData {
     DevBuf<Tile2> tiles_d;   // 2D tiles of the current variant's shape
     DevBuf<Tile3> tiles3_d;  // 3D tiles of the current variant's shape
     int64_t ntiles = 0;
-    int tile_ci = 0, tile_cj = 0, tile_ck = 0;
+    int tile_ci = 0, tile_cj = 0, tile_ck = 0, tile_fd = 0;
     int64_t n_stored = 0;
     DevBuf<int32_t> st_slot, st_gc, st_gn0, st_gn1, st_gn2, st_role;
     DevBuf<int64_t> st_off;
@@ -332,34 +333,38 @@ static bool rows_uniform(const double* W, int64_t rows, int width)
 }
 
 // Opt the interior kernels into >48 KB of dynamic shared memory.
-template <int CI, int CJ, int MINB, class C> static void set_smem_attr()
+template <int CI, int CJ, int FD, int KIND, class C> constexpr size_t tile_smem2()
 {
-    EGG_CK(cudaFuncSetAttribute(interior_tile_kernel<CI, CJ, MINB, kShape, C>,
+    return sizeof(TileShared2<CI + FD, CJ + FD, C, KIND>);
+}
+
+template <int CI, int CJ, int MINB, class C, int FD> static void set_smem_attr()
+{
+    EGG_CK(cudaFuncSetAttribute(interior_tile_kernel<CI, CJ, MINB, kShape, C, FD>,
+                                cudaFuncAttributeMaxDynamicSharedMemorySize, int(tile_smem2<CI, CJ, FD, kShape, C>())));
+    EGG_CK(cudaFuncSetAttribute(interior_tile_kernel<CI, CJ, MINB, kUntangle, C, FD>,
                                 cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                int(sizeof(TileShared2<CI, CJ, C, kShape>))));
-    EGG_CK(cudaFuncSetAttribute(interior_tile_kernel<CI, CJ, MINB, kUntangle, C>,
+                                int(tile_smem2<CI, CJ, FD, kUntangle, C>())));
+    EGG_CK(cudaFuncSetAttribute(interior_tile_kernel<CI, CJ, MINB, kShapeSize, C, FD>,
                                 cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                int(sizeof(TileShared2<CI, CJ, C, kUntangle>))));
-    EGG_CK(cudaFuncSetAttribute(interior_tile_kernel<CI, CJ, MINB, kShapeSize, C>,
-                                cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                int(sizeof(TileShared2<CI, CJ, C, kShapeSize>))));
+                                int(tile_smem2<CI, CJ, FD, kShapeSize, C>())));
 }
 
 static void configure_kernels(int prec, int dim)
 {
     if (dim == 3) { return; }  // 3D kernels use < 48 KB of static shared memory
     if (prec == EGG_B200_PREC_FP64) {
-        set_smem_attr<kVar64[0].ci, kVar64[0].cj, kVar64[0].minb, double>();
-        set_smem_attr<kVar64[1].ci, kVar64[1].cj, kVar64[1].minb, double>();
-        set_smem_attr<kVar64[2].ci, kVar64[2].cj, kVar64[2].minb, double>();
-        set_smem_attr<kVar64[3].ci, kVar64[3].cj, kVar64[3].minb, double>();
-        set_smem_attr<kVar64[4].ci, kVar64[4].cj, kVar64[4].minb, double>();
+        set_smem_attr<kVar64[0].ci, kVar64[0].cj, kVar64[0].minb, double, kVar64[0].fd>();
+        set_smem_attr<kVar64[1].ci, kVar64[1].cj, kVar64[1].minb, double, kVar64[1].fd>();
+        set_smem_attr<kVar64[2].ci, kVar64[2].cj, kVar64[2].minb, double, kVar64[2].fd>();
+        set_smem_attr<kVar64[3].ci, kVar64[3].cj, kVar64[3].minb, double, kVar64[3].fd>();
+        set_smem_attr<kVar64[4].ci, kVar64[4].cj, kVar64[4].minb, double, kVar64[4].fd>();
     } else {
-        set_smem_attr<kVar32[0].ci, kVar32[0].cj, kVar32[0].minb, float>();
-        set_smem_attr<kVar32[1].ci, kVar32[1].cj, kVar32[1].minb, float>();
-        set_smem_attr<kVar32[2].ci, kVar32[2].cj, kVar32[2].minb, float>();
-        set_smem_attr<kVar32[3].ci, kVar32[3].cj, kVar32[3].minb, float>();
-        set_smem_attr<kVar32[4].ci, kVar32[4].cj, kVar32[4].minb, float>();
+        set_smem_attr<kVar32[0].ci, kVar32[0].cj, kVar32[0].minb, float, kVar32[0].fd>();
+        set_smem_attr<kVar32[1].ci, kVar32[1].cj, kVar32[1].minb, float, kVar32[1].fd>();
+        set_smem_attr<kVar32[2].ci, kVar32[2].cj, kVar32[2].minb, float, kVar32[2].fd>();
+        set_smem_attr<kVar32[3].ci, kVar32[3].cj, kVar32[3].minb, float, kVar32[3].fd>();
+        set_smem_attr<kVar32[4].ci, kVar32[4].cj, kVar32[4].minb, float, kVar32[4].fd>();
     }
 }
 
@@ -371,12 +376,14 @@ static Variant variant_shape(const Session& S, int v)
 
 // Tile list of the interior kernel for variant v over every block's
 // structured interior, keeping tiles that hold a moving DOF.  2D: CI x CJ
-// cells, (CI-1) x (CJ-1) DOFs per tile; 3D: CI x CJ x CK DOFs per tile.
+// cells, (CI-1) x (CJ-1) DOFs per tile (CI x CJ DOFs with fd); 3D: CI x CJ x
+// CK DOFs per tile.
 static void set_tiles(Session& S, LevelData& L, Variant v)
 {
-    if (L.tile_ci == v.ci && L.tile_cj == v.cj && L.tile_ck == v.ck) { return; }
+    if (L.tile_ci == v.ci && L.tile_cj == v.cj && L.tile_ck == v.ck && L.tile_fd == v.fd) { return; }
     S.drop_graphs();
-    const int di = S.dim == 2 ? v.ci - 1 : v.ci, dj = S.dim == 2 ? v.cj - 1 : v.cj, dk = S.dim == 2 ? 1 : v.ck;
+    const int shrink = (S.dim == 2 && !v.fd) ? 1 : 0;
+    const int di = v.ci - shrink, dj = v.cj - shrink, dk = S.dim == 2 ? 1 : v.ck;
     std::vector<Tile2> tiles2;
     std::vector<Tile3> tiles3;
     for (int b = 0; b < int(L.blocks_h.size()); ++b) {
@@ -418,6 +425,7 @@ static void set_tiles(Session& S, LevelData& L, Variant v)
     L.tile_ci = v.ci;
     L.tile_cj = v.cj;
     L.tile_ck = v.ck;
+    L.tile_fd = v.fd;
 }
 
 static Session* create_session(const egg_b200_session_desc& d)
@@ -949,16 +957,16 @@ static Session* create_session(const egg_b200_session_desc& d)
 // ---------------------------------------------------------------------------
 // Sweep driver
 // ---------------------------------------------------------------------------
-template <int CI, int CJ, int MINB, int KIND, class C>
+template <int CI, int CJ, int MINB, int KIND, class C, int FD>
 static void launch_tile(Session& S, LevelData& L, const double* xin, double* xout, const double* tau, double delta,
                         double omega, double* gout)
 {
-    const size_t smem = sizeof(TileShared2<CI, CJ, C, KIND>);
+    const size_t smem = tile_smem2<CI, CJ, FD, KIND, C>();
     const auto* xi = reinterpret_cast<const double2*>(xin);
     auto* xo = reinterpret_cast<double2*>(xout);
     const auto* tv = reinterpret_cast<const double2*>(tau);
     S.timed(kKInterior, [&] {
-        interior_tile_kernel<CI, CJ, MINB, KIND, C><<<unsigned(L.ntiles), CI * CJ, smem, S.stream>>>(
+        interior_tile_kernel<CI, CJ, MINB, KIND, C, FD><<<unsigned(L.ntiles), CI * CJ, smem, S.stream>>>(
           xi, xo, L.tiles_d.p, L.blocks_d.p, L.active_d.p, tv, delta, omega, reinterpret_cast<double2*>(gout));
     });
 }
@@ -1003,19 +1011,19 @@ static void launch_interior(Session& S, LevelData& L, const double* xin, double*
 #undef EGG_V3
     if (S.prec == EGG_B200_PREC_FP64) {
         switch (S.variant) {
-        case 0: launch_tile<kVar64[0].ci, kVar64[0].cj, kVar64[0].minb, KIND, double>(S, L, xin, xout, tau, delta, omega, gout); break;
-        case 1: launch_tile<kVar64[1].ci, kVar64[1].cj, kVar64[1].minb, KIND, double>(S, L, xin, xout, tau, delta, omega, gout); break;
-        case 2: launch_tile<kVar64[2].ci, kVar64[2].cj, kVar64[2].minb, KIND, double>(S, L, xin, xout, tau, delta, omega, gout); break;
-        case 3: launch_tile<kVar64[3].ci, kVar64[3].cj, kVar64[3].minb, KIND, double>(S, L, xin, xout, tau, delta, omega, gout); break;
-        default: launch_tile<kVar64[4].ci, kVar64[4].cj, kVar64[4].minb, KIND, double>(S, L, xin, xout, tau, delta, omega, gout); break;
+        case 0: launch_tile<kVar64[0].ci, kVar64[0].cj, kVar64[0].minb, KIND, double, kVar64[0].fd>(S, L, xin, xout, tau, delta, omega, gout); break;
+        case 1: launch_tile<kVar64[1].ci, kVar64[1].cj, kVar64[1].minb, KIND, double, kVar64[1].fd>(S, L, xin, xout, tau, delta, omega, gout); break;
+        case 2: launch_tile<kVar64[2].ci, kVar64[2].cj, kVar64[2].minb, KIND, double, kVar64[2].fd>(S, L, xin, xout, tau, delta, omega, gout); break;
+        case 3: launch_tile<kVar64[3].ci, kVar64[3].cj, kVar64[3].minb, KIND, double, kVar64[3].fd>(S, L, xin, xout, tau, delta, omega, gout); break;
+        default: launch_tile<kVar64[4].ci, kVar64[4].cj, kVar64[4].minb, KIND, double, kVar64[4].fd>(S, L, xin, xout, tau, delta, omega, gout); break;
         }
     } else {
         switch (S.variant) {
-        case 0: launch_tile<kVar32[0].ci, kVar32[0].cj, kVar32[0].minb, KIND, float>(S, L, xin, xout, tau, delta, omega, gout); break;
-        case 1: launch_tile<kVar32[1].ci, kVar32[1].cj, kVar32[1].minb, KIND, float>(S, L, xin, xout, tau, delta, omega, gout); break;
-        case 2: launch_tile<kVar32[2].ci, kVar32[2].cj, kVar32[2].minb, KIND, float>(S, L, xin, xout, tau, delta, omega, gout); break;
-        case 3: launch_tile<kVar32[3].ci, kVar32[3].cj, kVar32[3].minb, KIND, float>(S, L, xin, xout, tau, delta, omega, gout); break;
-        default: launch_tile<kVar32[4].ci, kVar32[4].cj, kVar32[4].minb, KIND, float>(S, L, xin, xout, tau, delta, omega, gout); break;
+        case 0: launch_tile<kVar32[0].ci, kVar32[0].cj, kVar32[0].minb, KIND, float, kVar32[0].fd>(S, L, xin, xout, tau, delta, omega, gout); break;
+        case 1: launch_tile<kVar32[1].ci, kVar32[1].cj, kVar32[1].minb, KIND, float, kVar32[1].fd>(S, L, xin, xout, tau, delta, omega, gout); break;
+        case 2: launch_tile<kVar32[2].ci, kVar32[2].cj, kVar32[2].minb, KIND, float, kVar32[2].fd>(S, L, xin, xout, tau, delta, omega, gout); break;
+        case 3: launch_tile<kVar32[3].ci, kVar32[3].cj, kVar32[3].minb, KIND, float, kVar32[3].fd>(S, L, xin, xout, tau, delta, omega, gout); break;
+        default: launch_tile<kVar32[4].ci, kVar32[4].cj, kVar32[4].minb, KIND, float, kVar32[4].fd>(S, L, xin, xout, tau, delta, omega, gout); break;
         }
     }
 }
@@ -2258,10 +2266,11 @@ int egg_b200_session_variant_info(egg_b200_session* s, int32_t* variant, int32_t
         for (int v = 0; v < n && v < kNumVariants; ++v) {
             const Variant vs = variant_shape(S, v);
             if (shape) {
-                shape[4 * v] = vs.ci;
-                shape[4 * v + 1] = vs.cj;
-                shape[4 * v + 2] = vs.ck;
-                shape[4 * v + 3] = vs.minb;
+                shape[5 * v] = vs.ci;
+                shape[5 * v + 1] = vs.cj;
+                shape[5 * v + 2] = vs.ck;
+                shape[5 * v + 3] = vs.minb;
+                shape[5 * v + 4] = vs.fd;
             }
             if (times_ms) { times_ms[v] = S.variant_ms[v]; }
         }

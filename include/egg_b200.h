@@ -334,9 +334,10 @@ int egg_b200_session_restore(egg_b200_session* s);
  * reference (AdaptiveCpp picks launch shapes itself). */
 int egg_b200_session_autotune(egg_b200_session* s, int32_t objective, int32_t reps, int32_t* chosen);
 int egg_b200_session_set_variant(egg_b200_session* s, int32_t variant);
-/* Current variant, per-variant shape (ci, cj, ck, min CTAs/SM) [4*n] -- 2D:
- * cells per CTA, 3D: DOFs per CTA -- and the tuned times in ms [n], for the
- * first n <= EGG_B200_NUM_VARIANTS variants. */
+/* Current variant, per-variant shape (ci, cj, ck, min CTAs/SM, full_dof)
+ * [5*n] -- 2D: cells per CTA, or DOFs per CTA when full_dof = 1; 3D: DOFs per
+ * CTA -- and the tuned times in ms [n], for the first n <=
+ * EGG_B200_NUM_VARIANTS variants. */
 #define EGG_B200_NUM_VARIANTS 5
 int egg_b200_session_variant_info(egg_b200_session* s, int32_t* variant, int32_t* shape, double* times_ms,
                                   int32_t n);

@@ -88,6 +88,28 @@ def test_trajectory_fp64_matches_reference(gpu, run):
     assert np.sign(M[-1]) == np.sign(_REF[key + "/M"][-1])
 
 
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+@pytest.mark.parametrize("case", ["disk_oh33", "square65"])
+def test_every_launch_variant_matches_reference(gpu, case, precision):
+    """Each interior-kernel variant (cell tiles and full-DOF tiles, whose
+    edges fall on different nodes of these 33- and 65-node blocks) relaxes
+    the first sweep and the trajectory as the reference does."""
+    phase, omega, n = "barrier", 0.8, 40
+    g = case_grid(case)
+    key = f"fp64/{case}/{phase}/{omega}"
+    t1 = 1e-12 if precision == "fp64" else 1e-5
+    nv = len(_session(gpu, g).variants()["table"])
+    for v in range(nv):
+        s = _session(gpu, g, precision=precision)
+        s.set_variant(v)
+        s.run(1, phase=phase, omega=omega)
+        dx = np.abs(s.get_X() - _REF[key + "/X1"]).max()
+        assert dx <= t1 * _hmin(g), (v, dx / _hmin(g))
+        E, M = s.run(n - 1, phase=phase, omega=omega, report_every=n - 1)
+        np.testing.assert_allclose(E[-1], _REF[key + "/E"][-1], rtol=1e-9 if precision == "fp64" else 1e-4)
+        assert np.sign(M[-1]) == np.sign(_REF[key + "/M"][-1])
+
+
 @pytest.mark.parametrize("run", RUNS, ids=lambda r: f"{r[0]}-{r[1]}-{r[3]}")
 def test_first_sweep_mixed_within_1e5_h(gpu, run):
     case, phase, delta, omega, n = run
