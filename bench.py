@@ -40,10 +40,9 @@ UNIT = "vertex-updates/s"
 # memory; structure is synthesized, not read).
 BYTES_PER_UPDATE = 2 * 2 * 8
 # DRAM bytes (read + write) per moving-DOF update of the mixed interior
-# kernel, from one ncu capture at 4097^2 (527.6 MB per launch over
-# 16,769,025 DOFs).  Traffic
-# grows in proportion to the DOFs swept.
-DRAM_BYTES_PER_UPDATE = 527.6e6 / 16769025
+# kernel, from one ncu capture at 4097^2 (527.0 MB per launch over
+# 16,769,025 DOFs).  Traffic grows in proportion to the DOFs swept.
+DRAM_BYTES_PER_UPDATE = 527.0e6 / 16769025
 
 
 def _peaks():
@@ -462,7 +461,7 @@ def main():
             "traffic": DRAM_BYTES_PER_UPDATE * F, "traffic_unit": "bytes per launch (ncu dram read+write)",
             "algorithmic_bytes": BYTES_PER_UPDATE * F, "kernel": "interior_tile_kernel (mixed)",
             "avg_launch_ms": avg_ms, "peak_source": peak_kind,
-            "note": "issue-bound stencil (ncu: issue 69%, FMA 40%, ALU 24%, XU 15%, DRAM 5%); "
+            "note": "issue-bound stencil (ncu: issue 66%, FMA 38%, ALU 23%, XU 15%, DRAM 5%); "
                     "frac states HBM use, not the binding roof"}
     total_ms = sum(v[0] for v in mixed["stats"].values())
     share = {k: v[0] / total_ms for k, v in mixed["stats"].items() if v[1]}
