@@ -45,6 +45,8 @@ class Grid:
     meta: dict = field(default_factory=dict)
     # constrained boundary nodes: global id -> (entity tag, record)
     constraints: dict = field(default_factory=dict)
+    # soft terms: optional "directional" and "curvature" tables (wire.flat_wire)
+    soft: dict = field(default_factory=dict)
 
     @property
     def num_nodes(self) -> int:
@@ -56,7 +58,8 @@ class Grid:
 
     def wire(self, *, w_inv=None, compact: bool = False) -> dict:
         return _wire.flat_wire(self.blocks, self.free, self.d, w_inv=w_inv, compact=compact,
-                               constraints=self.constraints)
+                               constraints=self.constraints, directional=self.soft.get("directional"),
+                               curvature=self.soft.get("curvature"))
 
     def structured(self) -> dict:
         return _wire.structured_tables(self.blocks)
@@ -617,3 +620,68 @@ def two_squares(n_big: int = 17, n_small: int = 6, frac: float = 0.2, seed: int 
         off += n * n
     return Grid(f"two_squares{n_big}_{n_small}", 2, blocks, np.concatenate(Xs), np.concatenate(frees),
                 {"frac": frac, "seed": seed})
+
+
+def with_soft_terms(g: Grid, seed: int = 0, *, n_dir: int = 36, n_curv: int = 24, weight: float = 0.3,
+                    block: int = 0) -> Grid:
+    """Attaches seeded soft terms to a grid, on grid lines of one block:
+    directional samples of every kind (parallel: two consecutive nodes, ref
+    the unit normal of their initial segment, tilted; line: three
+    consecutive nodes; stem: a node and its neighbour across the line, ref the
+    line's unit direction) and, in 2D, curvature windows of four consecutive
+    nodes.  Weights are drawn around ``weight``; some tuples reach the block
+    boundary, whose fixed or constrained nodes stay frozen partners."""
+    rng = np.random.default_rng(seed)
+    ids = np.asarray(g.blocks[block])
+    d = g.d
+    sh = ids.shape
+
+    def line(length: int):
+        ax = int(rng.integers(d))
+        start = [int(rng.integers(0, sh[k] - (length - 1 if k == ax else 0))) for k in range(d)]
+        nodes = []
+        for m in range(length):
+            q = list(start)
+            q[ax] += m
+            nodes.append(int(ids[tuple(q)]))
+        return ax, start, nodes
+
+    def unit(v):
+        return v / np.linalg.norm(v)
+
+    nodes, kind, ref, axis, w = [], [], [], [], []
+    for t in range(n_dir):
+        k = t % 3
+        if k == 1:  # line: a, c, b
+            _ax, _st, nd = line(3)
+            r = np.zeros(d)
+        else:
+            ax, st, nd = line(2)
+            u = unit(g.X[nd[1]] - g.X[nd[0]])
+            if k == 0:  # parallel: the segment's normal, tilted
+                nrm = np.array([-u[1], u[0]]) if d == 2 else unit(np.cross(u, rng.normal(size=3)))
+                r = unit(nrm + 0.3 * rng.normal(size=d))
+            else:  # stem: n across the line at c, ref the line's direction
+                other = (ax + 1 + int(rng.integers(d - 1))) % d
+                c = list(st)
+                c[other] = min(max(c[other], 1), sh[other] - 2)
+                n = list(c)
+                n[other] += 1 if rng.random() < 0.5 else -1
+                nd = [int(ids[tuple(n)]), int(ids[tuple(c)])]
+                r = unit(u + 0.2 * rng.normal(size=d))
+        nodes.append(nd + [-1] * (4 - len(nd)))
+        kind.append(k)
+        ref.append(r)
+        axis.append(np.zeros(d))
+        w.append(weight * rng.uniform(0.5, 1.5))
+    soft = {"directional": {"nodes": np.array(nodes, dtype=np.int32), "kind": np.array(kind, dtype=np.int32),
+                            "ref": np.array(ref), "axis": np.array(axis), "weight": np.array(w), "eps": 1e-12}}
+    if d == 2 and n_curv:
+        cn, cw = [], []
+        for _ in range(n_curv):
+            cn.append(line(4)[2])
+            cw.append(weight * rng.uniform(0.5, 1.5))
+        soft["curvature"] = {"nodes": np.array(cn, dtype=np.int64), "weight": np.array(cw)}
+    g.soft = soft
+    g.name = g.name + "+soft"
+    return g

@@ -277,6 +277,43 @@ void fill_desc(Desc& D, const py::dict& ctx, const py::dict& st, const DArr& X, 
         d.entity_params = constrained ? D.eparams.data() : nullptr;
         d.entity_arena = D.arena.empty() ? nullptr : D.arena.data();
         d.entity_arena_len = int64_t(D.arena.size());
+        // Soft terms (src/bindings.cpp:380-410): per-DOF fixed-K tables with
+        // global node ids; the core remaps them to owner slots.
+        auto sized = [&](const char* key, int64_t want, bool real) -> const void* {
+            int64_t got = 0;
+            const void* ptr = real ? static_cast<const void*>(D.keep.reals(g[key], &got))
+                                   : static_cast<const void*>(D.keep.ints(g[key], &got));
+            if (got != want) {
+                throw py::value_error(std::string("validate_context: group[0] ") + key + " size " + std::to_string(got) +
+                                      " != " + std::to_string(want));
+            }
+            return ptr;
+        };
+        if (g.contains("curv_k")) {
+            const int k = g["curv_k"].cast<int>();
+            if (k < 0) { throw py::value_error("validate_context: group[0] curv_k < 0"); }
+            if (k > 0) {
+                d.curv_k = k;
+                d.curv_nodes = static_cast<const int32_t*>(sized("curv_nodes", d.ndof * k * 4, false));
+                d.curv_slot = static_cast<const int32_t*>(sized("curv_slot", d.ndof * k, false));
+                d.curv_weight = static_cast<const double*>(sized("curv_weight", d.ndof * k, true));
+            }
+        }
+        if (g.contains("dir_k")) {
+            const int k = g["dir_k"].cast<int>();
+            if (k < 0) { throw py::value_error("validate_context: group[0] dir_k < 0"); }
+            if (k > 0) {
+                d.dir_k = k;
+                d.dir_eps = g["dir_eps"].cast<double>();
+                d.dir_nodes = static_cast<const int32_t*>(sized("dir_nodes", d.ndof * k * 4, false));
+                d.dir_slot = static_cast<const int32_t*>(sized("dir_slot", d.ndof * k, false));
+                d.dir_kind = static_cast<const int32_t*>(sized("dir_kind", d.ndof * k, false));
+                d.dir_ref = static_cast<const double*>(sized("dir_ref", d.ndof * k * dim, true));
+                d.dir_weight = static_cast<const double*>(sized("dir_weight", d.ndof * k, true));
+                // dir_axis (the 3D-only kinds' projector) is read by no kind yet
+                if (g.contains("dir_axis")) { sized("dir_axis", d.ndof * k * dim, true); }
+            }
+        }
     }
 
     py::dict es = ctx["energy_stencil"].cast<py::dict>();
@@ -295,6 +332,21 @@ void fill_desc(Desc& D, const py::dict& ctx, const py::dict& st, const DArr& X, 
     }
     d.es_W_inv = D.keep.reals(es["W_inv"], &d.es_W_inv_len);
     if (es.contains("weight")) { d.es_weight = D.keep.reals(es["weight"], &d.es_weight_len); }
+    // Whole-sample directional table (src/bindings.cpp:471-480).
+    if (es.contains("dir_num") && es["dir_num"].cast<int64_t>() > 0) {
+        const int64_t nd = es["dir_num"].cast<int64_t>();
+        d.es_dir_num = nd;
+        d.es_dir_eps = es["dir_eps"].cast<double>();
+        int64_t n = 0;
+        d.es_dir_nodes = D.keep.ints(es["dir_nodes"], &n);
+        if (n != nd * 4) { throw py::value_error("validate_context: energy_stencil dir_nodes size mismatch"); }
+        d.es_dir_kind = D.keep.ints(es["dir_kind"], &n);
+        if (n != nd) { throw py::value_error("validate_context: energy_stencil dir_kind size mismatch"); }
+        d.es_dir_ref = D.keep.reals(es["dir_ref"], &n);
+        if (n != nd * dim) { throw py::value_error("validate_context: energy_stencil dir_ref size mismatch"); }
+        d.es_dir_weight = D.keep.reals(es["dir_weight"], &n);
+        if (n != nd) { throw py::value_error("validate_context: energy_stencil dir_weight size mismatch"); }
+    }
 }
 
 py::array_t<double> vec(const std::vector<double>& v)

@@ -14,6 +14,7 @@
 
 #include "entity2.cuh"
 #include "metric.cuh"
+#include "soft.cuh"
 
 #include <cstdint>
 #include <cuda_runtime.h>
@@ -735,6 +736,7 @@ struct StoredPatch2 {
     int cold;               // first sweep of a run call: trimmed arcs project in world space
     const double* arena;    // entity arena (B-spline knots, control points, weights)
     double* seeds;          // [n] last foot parameter of each B-spline DOF (NaN: none)
+    SoftTable soft;         // directional / curvature terms per DOF (off == NULL: none)
 };
 
 __device__ __forceinline__ void assemble_T(const double2 c, const double2 n0, const double2 n1,
@@ -903,8 +905,14 @@ __global__ void stored_patch_kernel(StoredPatch2 sp, const double2* __restrict__
             h11 += wt * hl[3];
         }
         double g[2] = {group_sum<G>(g0), group_sum<G>(g1)};
-        const double h[4] = {group_sum<G>(h00), group_sum<G>(h01), group_sum<G>(h10), group_sum<G>(h11)};
+        double h[4] = {group_sum<G>(h00), group_sum<G>(h01), group_sum<G>(h10), group_sum<G>(h11)};
         e0 = group_sum<G>(e0);
+        // Soft terms fold into the Newton system and the baseline energy
+        // (src/sweep.hpp:1461-1512; constrained DOFs take the directional
+        // samples only, src/sweep.hpp:1307-1327).  Every lane of the group
+        // adds them alike.
+        const int etag = (CON && sp.etag != nullptr) ? int(sp.etag[d]) : 0;
+        soft_dof_accumulate<2>(sp.soft, d, etag == 0, reinterpret_cast<const double*>(Xin), g, h, e0);
         double tx = 0.0, ty = 0.0;
         if (tau != nullptr) {
             tx = tau[slot].x;
@@ -925,7 +933,6 @@ __global__ void stored_patch_kernel(StoredPatch2 sp, const double2* __restrict__
         // parameter instead (src/sweep.hpp:1718-1876): trials q* + alpha dq,
         // clamped onto the trim and evaluated on the curve.
         // CON = false (a level without constrained DOFs) compiles none of it.
-        const int etag = (CON && sp.etag != nullptr) ? int(sp.etag[d]) : 0;
         const double* er = sp.epar + (etag != 0 ? d * EGG_B200_ENTITY_FIELDS : 0);
         const bool warm_arc = is_tcurve(etag) && !sp.cold;
         // B-spline DOFs carry a seed (their last foot parameter): every seeded
@@ -991,7 +998,12 @@ __global__ void stored_patch_kernel(StoredPatch2 sp, const double2* __restrict__
                 e += sp.wt[p * sp.wt_stride] * mu_value<double>(KIND, t, delta);
                 md = fmin(md, detA);
             }
-            e = group_sum<G>(e) - (tx * trial.x + ty * trial.y);
+            e = group_sum<G>(e);
+            if (sp.soft.off != nullptr) {
+                const double tr[2] = {trial.x, trial.y};
+                e += soft_dof_trial<2>(sp.soft, d, etag == 0, reinterpret_cast<const double*>(Xin), tr);
+            }
+            e -= tx * trial.x + ty * trial.y;
             md = group_min<G>(md);
             if (isfinite(e) && e <= e0 + Tol<double>::energy && (KIND == kUntangle || md > 0.0)) {
                 cur = trial;
@@ -1196,6 +1208,24 @@ __global__ void reduce_finalize_kernel(const double* part_s, const double* part_
         *out_e = acc.s + acc.c;
         *out_m = mn;
     }
+}
+
+// Adds the whole-sample directional total to a finished energy report
+// (src/directional.hpp:281-299, src/sweep.hpp:1921): one CTA, compensated,
+// fixed order, so the reported energy is the composed objective.
+template <int D>
+__global__ void soft_energy_add_kernel(const SoftTerm* __restrict__ terms, int64_t n, double eps,
+                                       const double* __restrict__ X, double* out_e)
+{
+    Comp acc {0.0, 0.0};
+    double mn = INFINITY;
+    for (int64_t i = threadIdx.x; i < n; i += blockDim.x) {
+        const SoftTerm t = terms[i];
+        double p[4][3];
+        soft_load<D>(t, X, p);
+        comp_add(acc, soft_energy<D>(t, p, eps));
+    }
+    if (block_reduce(acc, mn)) { *out_e += acc.s + acc.c; }
 }
 
 // Segmented final pass: CTA m folds partials [m n, (m+1) n) into

@@ -441,6 +441,7 @@ struct StoredPatch3 {
     const int8_t* etag;  // [n] entity tag of each DOF, or NULL (all Free)
     const double* epar;  // [n * EGG_B200_ENTITY_FIELDS] entity records
     int cold;            // first sweep of a run call: parametric entities project in world space
+    SoftTable soft;      // directional terms per DOF (off == NULL: none)
 };
 
 __device__ __forceinline__ void assemble_T3(const double* X, int32_t ic, const int32_t in[3], const double s[3],
@@ -520,6 +521,19 @@ __global__ void stored3_kernel(StoredPatch3 sp, const double* __restrict__ Xin, 
 #pragma unroll
         for (int q = 0; q < 6; ++q) { h[q] = group_sum<G>(h[q]); }
         e0 = group_sum<G>(e0);
+        // Directional soft terms (src/sweep.hpp:1307-1327,1491-1512), added
+        // entry by entry to the full 3x3 Hessian.
+        const int etag = (CON && sp.etag != nullptr) ? int(sp.etag[d]) : 0;
+        if (sp.soft.off != nullptr) {
+            double H9[9] = {h[0], h[1], h[2], h[1], h[3], h[4], h[2], h[4], h[5]};
+            soft_dof_accumulate<3>(sp.soft, d, false, Xin, g, H9, e0);
+            h[0] = H9[0];
+            h[1] = H9[1];
+            h[2] = H9[2];
+            h[3] = H9[4];
+            h[4] = H9[5];
+            h[5] = H9[8];
+        }
         double tv[3] = {0, 0, 0};
         if (tau != nullptr) {
             for (int q = 0; q < 3; ++q) { tv[q] = tau[3 * int64_t(slot) + q]; }
@@ -539,7 +553,6 @@ __global__ void stored3_kernel(StoredPatch3 sp, const double* __restrict__ Xin, 
         // search, every trial on the entity; a parametric entity after the
         // first sweep of a run call searches in its parameters.
         // CON = false (a level without constrained DOFs) compiles none of it.
-        const int etag = (CON && sp.etag != nullptr) ? int(sp.etag[d]) : 0;
         const double* er = sp.epar + (etag != 0 ? d * EGG_B200_ENTITY_FIELDS : 0);
         const bool warm_param = is_param3(etag) && !sp.cold;
         double dl[3] = {0.0, 0.0, 0.0};
@@ -574,7 +587,9 @@ __global__ void stored3_kernel(StoredPatch3 sp, const double* __restrict__ Xin, 
                 e += sp.wt[p * sp.wt_stride] * mu3_value<double>(KIND, t, delta, dd);
                 md = fmin(md, detA);
             }
-            e = group_sum<G>(e) - (tv[0] * tr[0] + tv[1] * tr[1] + tv[2] * tr[2]);
+            e = group_sum<G>(e);
+            if (sp.soft.off != nullptr) { e += soft_dof_trial<3>(sp.soft, d, false, Xin, tr); }
+            e -= tv[0] * tr[0] + tv[1] * tr[1] + tv[2] * tr[2];
             md = group_min<G>(md);
             if (isfinite(e) && e <= e0 + Tol<double>::energy && (KIND == kUntangle || md > 0.0)) {
                 cur[0] = tr[0];

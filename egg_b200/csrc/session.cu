@@ -115,6 +115,9 @@ struct LevelData {
     DevBuf<BlockInfo> blocks_d;
     int64_t n_interior = 0;
     std::vector<uint8_t> active_h;
+    // structured-interior DOF slots (the tile kernel's plus those relaxed as
+    // stored DOFs for their soft terms): the FAS coarsening's interior set
+    std::vector<uint8_t> interior_h;
     DevBuf<uint8_t> active_d;
     DevBuf<Tile2> tiles_d;   // 2D tiles of the current variant's shape
     DevBuf<Tile3> tiles3_d;  // 3D tiles of the current variant's shape
@@ -134,6 +137,10 @@ struct LevelData {
     DevBuf<double> seeds;       // [n_stored] last foot parameter of each B-spline DOF
     DevBuf<int8_t> st_etag;     // [n_stored] entity tag (uploaded when n_constrained > 0)
     DevBuf<double> st_epar;     // [n_stored * EGG_B200_ENTITY_FIELDS] entity records
+    int64_t n_soft = 0;          // soft terms over the stored DOFs (0: none)
+    DevBuf<int32_t> soft_off;    // [n_stored + 1] term ranges
+    DevBuf<SoftTerm> soft_terms;
+    double soft_eps = 0.0;
     int64_t nshare = 0;
     DevBuf<int32_t> sh_src, sh_dst;
 };
@@ -189,6 +196,10 @@ struct Session : LevelData {
     DevBuf<int8_t> es_s0, es_s1, es_s2;
     DevBuf<double> es_W, es_wt;
     int es_wstride = 0, es_wtstride = 0;
+    // whole-sample directional table: its total joins every reported energy
+    int64_t es_dir_n = 0;
+    DevBuf<SoftTerm> es_dir;
+    double es_dir_eps = 0.0;
     // reductions
     int red_grid = 0;
     DevBuf<double> part;      // [3 * red_grid]
@@ -580,7 +591,95 @@ static Session* create_session(const egg_b200_session_desc& d)
         for (int k = 0; k < D; ++k) { chk(d.gn[k][p], ("gn" + std::to_string(k)).c_str()); }
     }
 
-    std::vector<uint8_t> active(off, 0);
+    // ---- soft terms --------------------------------------------------------
+    // Per-DOF directional samples (2D, 3D) and curvature windows (2D; the
+    // reference reads them in 2D only, src/sweep.hpp:1464).  A structured-
+    // interior DOF that carries a term leaves the tile path and relaxes as a
+    // stored DOF with the synthesized patch's identity target and unit weight
+    // (src/structured_patch.hpp:183-185), so its terms join its Newton system.
+    if (d.dir_k < 0 || d.curv_k < 0) { invalid("validate_context: negative dir_k / curv_k"); }
+    const int64_t dk = d.dir_k, ck = D == 2 ? d.curv_k : 0;
+    if (dk) {
+        require_ptr(d.dir_nodes, ndof * dk * 4, "dir_nodes");
+        require_ptr(d.dir_slot, ndof * dk, "dir_slot");
+        require_ptr(d.dir_kind, ndof * dk, "dir_kind");
+        require_ptr(d.dir_ref, ndof * dk * D, "dir_ref");
+        require_ptr(d.dir_weight, ndof * dk, "dir_weight");
+        if (!std::isfinite(d.dir_eps)) { invalid("validate_context: dir_eps is not finite"); }
+    }
+    if (ck) {
+        require_ptr(d.curv_nodes, ndof * ck * 4, "curv_nodes");
+        require_ptr(d.curv_slot, ndof * ck, "curv_slot");
+        require_ptr(d.curv_weight, ndof * ck, "curv_weight");
+    }
+    auto dir_arity = [](int32_t kind) { return (kind >= 0 && kind <= kSoftStem) ? soft_arity(kind) : 0; };
+    auto soft_node = [&](int32_t g, const char* what) {
+        const int32_t sl = (g >= 0 && g < M) ? S->g2s[g] : -1;
+        if (sl < 0) {
+            invalid(std::string("structured: a ") + what + " node references a global node absent from every block's interior map");
+        }
+        return sl;
+    };
+    std::vector<uint8_t> has_soft(size_t(ndof), 0);
+    for (int64_t i = 0; i < ndof; ++i) {
+        for (int64_t j = 0; j < ck; ++j) {
+            const int32_t sl = d.curv_slot[i * ck + j];
+            if (sl < -1 || sl > 3) { invalid("validate_context: curv_slot out of range [-1, 3]"); }
+            if (sl >= 0) { has_soft[i] = 1; }
+        }
+        for (int64_t j = 0; j < dk; ++j) {
+            const int32_t sl = d.dir_slot[i * dk + j];
+            const int ar = dir_arity(d.dir_kind[i * dk + j]);
+            if (sl < -1 || (sl >= 0 && ar > 0 && sl >= ar)) { invalid("validate_context: dir_slot out of range"); }
+            if (sl >= 0 && ar > 0) { has_soft[i] = 1; }
+        }
+    }
+    bool any_demote = false;
+    for (int64_t i = 0; i < ndof; ++i) {
+        if (has_soft[i] && d.interior_block && d.interior_block[i] >= 0) { any_demote = true; }
+    }
+    auto is_identity = [&](const double* w) {
+        for (int a = 0; a < D; ++a) {
+            for (int b = 0; b < D; ++b) {
+                if (w[a * D + b] != (a == b ? 1.0 : 0.0)) { return false; }
+            }
+        }
+        return true;
+    };
+    const bool per_row_W = !w_uniform || (any_demote && !is_identity(d.W_inv));
+    const bool per_row_wt = d.weight_len > 1 || (any_demote && d.weight_len == 1 && d.weight[0] != 1.0);
+    std::vector<SoftTerm> soft_terms;
+    std::vector<int32_t> soft_off {0};
+    auto soft_terms_of = [&](int64_t i) {
+        for (int64_t j = 0; j < ck; ++j) {
+            const int32_t sl = d.curv_slot[i * ck + j];
+            if (sl < 0) { continue; }
+            SoftTerm t {};
+            for (int m = 0; m < 4; ++m) { t.node[m] = soft_node(d.curv_nodes[(i * ck + j) * 4 + m], "curvature-window"); }
+            t.slot = sl;
+            t.kind = kSoftCurv;
+            t.w = d.curv_weight[i * ck + j];
+            soft_terms.push_back(t);
+        }
+        for (int64_t j = 0; j < dk; ++j) {
+            const int32_t sl = d.dir_slot[i * dk + j], kind = d.dir_kind[i * dk + j];
+            const int ar = dir_arity(kind);
+            if (sl < 0 || ar == 0) { continue; }
+            SoftTerm t {};
+            for (int m = 0; m < 4; ++m) {
+                t.node[m] = m < ar ? soft_node(d.dir_nodes[(i * dk + j) * 4 + m], "directional-sample") : -1;
+            }
+            t.slot = sl;
+            t.kind = kind;
+            for (int k = 0; k < D; ++k) { t.ref[k] = d.dir_ref[(i * dk + j) * D + k]; }
+            t.w = d.dir_weight[i * dk + j];
+            soft_terms.push_back(t);
+        }
+        if (soft_terms.size() > size_t(INT32_MAX)) { invalid("validate_context: too many soft terms"); }
+        soft_off.push_back(int32_t(soft_terms.size()));
+    };
+
+    std::vector<uint8_t> active(off, 0), interior(off, 0);
     std::vector<int32_t> st_slot;
     std::vector<int64_t> st_off {0};
     std::vector<int32_t> st_gc, st_gn0, st_gn1, st_gn2, st_role;
@@ -666,10 +765,14 @@ static Session* create_session(const egg_b200_session_desc& d)
             if (S->slot_gid[bi.off + f] != gid) {
                 invalid("structured: interior_block/interior_logical does not name the DOF's node");
             }
-            active[bi.off + f] = 1;
-            S->n_interior++;
-            continue;
+            interior[bi.off + f] = 1;
+            if (!has_soft[i]) {
+                active[bi.off + f] = 1;
+                S->n_interior++;
+                continue;
+            }
         }
+        const bool synth_target = ib >= 0;  // a structured-interior DOF carrying soft terms
         st_slot.push_back(slot);
         st_etag.push_back(int8_t(etag));
         for (int f = 0; f < EGG_B200_ENTITY_FIELDS; ++f) {
@@ -681,7 +784,55 @@ static Session* create_session(const egg_b200_session_desc& d)
         }
         if (etag == EGG_B200_TAG_BSPLINE) { S->n_bspline++; }
         if (etag == EGG_B200_TAG_COMPOSITE) { S->n_composite++; }
-        for (int64_t p = p0; p < p0 + P; ++p) {
+        if (synth_target) {
+            // The synthesized interior patch (src/structured_patch.hpp:89-130):
+            // every sample of the 2^D cells around the node, identity target,
+            // unit weight, node slots in the DOF's block.  Wire rows of such a
+            // DOF (none on the reference's wire) are not read.
+            const BlockInfo& bi = S->blocks_h[ib];
+            const int nz = D == 3 ? bi.n[2] : 1;
+            int32_t l[3] = {0, 0, 0};
+            for (int k = 0; k < D; ++k) { l[k] = d.interior_logical[i * D + k]; }
+            const int nco = 1 << D;
+            for (int cell = 0; cell < nco; ++cell) {
+                int base[3] = {0, 0, 0};
+                for (int k = 0; k < D; ++k) { base[k] = l[k] - 1 + ((cell >> (D - 1 - k)) & 1); }
+                auto corner = [&](int a) {
+                    int q[3] = {0, 0, 0};
+                    for (int k = 0; k < D; ++k) { q[k] = base[k] + ((a >> (D - 1 - k)) & 1); }
+                    return int32_t(bi.off + (int64_t(q[0]) * bi.n[1] + q[1]) * nz + q[2]);
+                };
+                for (int b = 0; b < nco; ++b) {
+                    const int32_t c = corner(b);
+                    int32_t nbr[3] = {0, 0, 0};
+                    int8_t sg[3] = {1, 1, 1};
+                    int32_t role = c == slot ? 0 : -1;
+                    for (int k = 0; k < D; ++k) {
+                        const int bit = 1 << (D - 1 - k);
+                        nbr[k] = corner(b ^ bit);
+                        sg[k] = (b & bit) ? int8_t(-1) : int8_t(1);
+                        if (nbr[k] == slot) { role = k + 1; }
+                    }
+                    st_gc.push_back(c);
+                    st_gn0.push_back(nbr[0]);
+                    st_gn1.push_back(nbr[1]);
+                    st_s0.push_back(sg[0]);
+                    st_s1.push_back(sg[1]);
+                    if (D == 3) {
+                        st_gn2.push_back(nbr[2]);
+                        st_s2.push_back(sg[2]);
+                    }
+                    st_role.push_back(role);
+                    if (per_row_W) {
+                        for (int a = 0; a < D; ++a) {
+                            for (int e = 0; e < D; ++e) { st_W.push_back(a == e ? 1.0 : 0.0); }
+                        }
+                    }
+                    if (per_row_wt) { st_wt.push_back(1.0); }
+                }
+            }
+        }
+        for (int64_t p = p0; p < (synth_target ? p0 : p0 + P); ++p) {
             auto remap = [&](int32_t g) {
                 const int32_t s = S->g2s[g];
                 if (s < 0) {
@@ -700,12 +851,16 @@ static Session* create_session(const egg_b200_session_desc& d)
                 st_s2.push_back(d.s[2][p] < 0 ? int8_t(-1) : int8_t(1));
             }
             st_role.push_back(d.role[p]);
-            if (!w_uniform) {
-                for (int e = 0; e < D * D; ++e) { st_W.push_back(d.W_inv[p * D * D + e]); }
+            if (per_row_W) {
+                const double* w = w_uniform ? d.W_inv : d.W_inv + p * D * D;
+                for (int a = 0; a < D; ++a) {
+                    for (int b = 0; b < D; ++b) { st_W.push_back(synth_target ? (a == b ? 1.0 : 0.0) : w[a * D + b]); }
+                }
             }
-            if (d.weight_len > 1) { st_wt.push_back(d.weight[p]); }
+            if (per_row_wt) { st_wt.push_back(synth_target ? 1.0 : d.weight[d.weight_len > 1 ? p : 0]); }
         }
         st_off.push_back(int64_t(st_gc.size()));
+        soft_terms_of(i);
     }
     S->n_stored = int64_t(st_slot.size());
     S->free_h.assign(off, 0);
@@ -730,7 +885,7 @@ static Session* create_session(const egg_b200_session_desc& d)
         S->halo.sp.push_back(sp);
         S->halo.dp.push_back(dp);
     }
-    if (w_uniform || st_W.empty()) {
+    if (!per_row_W || st_W.empty()) {
         st_W.assign(d.W_inv, d.W_inv + (w_uniform ? D * D : 0));
         if (st_W.empty()) { st_W = identity_row(D); }
         S->st_wstride = 0;
@@ -878,6 +1033,7 @@ static Session* create_session(const egg_b200_session_desc& d)
     }
 
     S->active_h = std::move(active);
+    S->interior_h = std::move(interior);
 
     // ---- device --------------------------------------------------------------
     int ndev = 0;
@@ -899,6 +1055,33 @@ static Session* create_session(const egg_b200_session_desc& d)
     // ---- upload -----------------------------------------------------------
     S->es_W.upload(es_W_h);
     S->es_wt.upload(es_wt_h);
+    // Whole-sample directional table (src/bindings.cpp:471-480, remapped to
+    // owner slots as src/bindings.cpp:1053-1066 does); reserved kinds drop.
+    if (d.es_dir_num < 0) { invalid("validate_context: energy_stencil negative dir_num"); }
+    if (d.es_dir_num > 0) {
+        const int64_t nd = d.es_dir_num;
+        require_ptr(d.es_dir_nodes, nd * 4, "energy_stencil dir_nodes");
+        require_ptr(d.es_dir_kind, nd, "energy_stencil dir_kind");
+        require_ptr(d.es_dir_ref, nd * D, "energy_stencil dir_ref");
+        require_ptr(d.es_dir_weight, nd, "energy_stencil dir_weight");
+        if (!std::isfinite(d.es_dir_eps)) { invalid("validate_context: energy_stencil dir_eps is not finite"); }
+        std::vector<SoftTerm> es_dir;
+        for (int64_t q = 0; q < nd; ++q) {
+            const int32_t kind = d.es_dir_kind[q];
+            const int ar = dir_arity(kind);
+            if (ar == 0) { continue; }
+            SoftTerm t {};
+            for (int m = 0; m < 4; ++m) { t.node[m] = m < ar ? soft_node(d.es_dir_nodes[q * 4 + m], "directional-sample") : -1; }
+            t.slot = -1;
+            t.kind = kind;
+            for (int k = 0; k < D; ++k) { t.ref[k] = d.es_dir_ref[q * D + k]; }
+            t.w = d.es_dir_weight[q];
+            es_dir.push_back(t);
+        }
+        S->es_dir_n = int64_t(es_dir.size());
+        S->es_dir.upload(es_dir);
+        S->es_dir_eps = d.es_dir_eps;
+    }
     if (structured) {
         S->es_cell_off.upload(cell_off);
     } else {
@@ -938,6 +1121,12 @@ static Session* create_session(const egg_b200_session_desc& d)
     S->st_s2.upload(st_s2);
     S->st_W.upload(st_W);
     S->st_wt.upload(st_wt);
+    S->n_soft = int64_t(soft_terms.size());
+    if (S->n_soft) {
+        S->soft_off.upload(soft_off);
+        S->soft_terms.upload(soft_terms);
+        S->soft_eps = d.dir_eps;
+    }
     S->sh_src.upload(sh_src);
     S->sh_dst.upload(sh_dst);
     std::vector<double> Xs(off * D);
@@ -1078,6 +1267,11 @@ static bool autotune_enabled()
     return !(v && std::string(v) == "0");
 }
 
+static SoftTable soft_view(LevelData& L)
+{
+    return SoftTable {L.n_soft ? L.soft_off.p : nullptr, L.n_soft ? L.soft_terms.p : nullptr, L.soft_eps};
+}
+
 static StoredPatch2 stored_view(LevelData& S)
 {
     StoredPatch2 sp;
@@ -1099,6 +1293,7 @@ static StoredPatch2 stored_view(LevelData& S)
     sp.cold = 0;
     sp.arena = (S.n_bspline || S.n_composite) ? S.arena.p : nullptr;
     sp.seeds = S.n_bspline ? S.seeds.p : nullptr;
+    sp.soft = soft_view(S);
     return sp;
 }
 
@@ -1131,7 +1326,7 @@ static void launch_stored(Session& S, LevelData& L, const double* xin, double* x
                          L.st_gn2.p, L.st_s0.p,   L.st_s1.p,  L.st_s2.p, L.st_role.p, L.st_W.p,
                          L.st_wstride, L.st_wt.p, L.st_wtstride,
                          L.n_constrained ? L.st_etag.p : nullptr, L.n_constrained ? L.st_epar.p : nullptr,
-                         cold ? 1 : 0};
+                         cold ? 1 : 0, soft_view(L)};
         auto go3 = [&](auto con) {
             constexpr bool C = decltype(con)::value;
             switch (G) {
@@ -1189,6 +1384,19 @@ static void launch_broadcast(Session& S, LevelData& L, double* x)
     });
 }
 
+// The whole-sample directional total, added onto *out_e (no-op without one).
+static void launch_soft_energy(Session& S, const double* x, double* out_e)
+{
+    if (S.es_dir_n == 0) { return; }
+    S.timed(kKFinal, [&] {
+        if (S.dim == 3) {
+            soft_energy_add_kernel<3><<<1, 256, 0, S.stream>>>(S.es_dir.p, S.es_dir_n, S.es_dir_eps, x, out_e);
+        } else {
+            soft_energy_add_kernel<2><<<1, 256, 0, S.stream>>>(S.es_dir.p, S.es_dir_n, S.es_dir_eps, x, out_e);
+        }
+    });
+}
+
 template <int KIND> static void launch_reduce(Session& S, const double* x, double delta, double* out_e, double* out_m)
 {
     double* ps = S.part.p;
@@ -1237,6 +1445,7 @@ template <int KIND> static void launch_reduce(Session& S, const double* x, doubl
         });
     }
     S.timed(kKFinal, [&] { reduce_finalize_kernel<<<1, 1024, 0, S.stream>>>(ps, pc, pm, S.red_grid, out_e, out_m); });
+    launch_soft_energy(S, x, out_e);
 }
 
 // Per-mesh energy / min det of a batch session: CTA row m reduces mesh m's
@@ -1553,6 +1762,15 @@ static void energy_noalloc_impl(Session& S, double delta, int grid, double* scra
     reduce_finalize_kernel<<<1, 1024, 0, S.stream>>>(ps, pc, pm, grid, out, out + 1);
     EGG_CK(cudaGetLastError());
     S.launches += 2;
+    if (S.es_dir_n) {
+        if (S.dim == 3) {
+            soft_energy_add_kernel<3><<<1, 256, 0, S.stream>>>(S.es_dir.p, S.es_dir_n, S.es_dir_eps, x, out);
+        } else {
+            soft_energy_add_kernel<2><<<1, 256, 0, S.stream>>>(S.es_dir.p, S.es_dir_n, S.es_dir_eps, x, out);
+        }
+        EGG_CK(cudaGetLastError());
+        ++S.launches;
+    }
     double buf[2];
     EGG_CK(cudaMemcpyAsync(buf, out, sizeof(buf), cudaMemcpyDeviceToHost, S.stream));
     EGG_CK(cudaStreamSynchronize(S.stream));

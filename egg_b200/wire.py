@@ -124,6 +124,8 @@ def flat_wire(
     w_inv: np.ndarray | None = None,
     compact: bool = False,
     constraints: dict | None = None,
+    directional: dict | None = None,
+    curvature: dict | None = None,
 ) -> dict:
     """The ``{"groups", "energy_stencil"}`` wire for Free DOFs and, optionally,
     constrained boundary DOFs.
@@ -139,6 +141,9 @@ def flat_wire(
     per tag whose packed records follow the partition's ``dof_local`` order.
     ``compact`` drops the energy-stencil index arrays (see module docstring) and
     sends a uniform target as one shared row.
+    ``directional`` (``nodes`` (n, 4) -1 padded, ``kind``, ``ref`` (n, d),
+    ``axis`` (n, d), ``weight``, ``eps``) and ``curvature`` (``nodes`` (W, 4),
+    ``weight``) add the soft-term tables (``soft_tables``).
     """
     constraints = constraints or {}
     con_ids = np.array(sorted(constraints), dtype=np.int64)
@@ -253,6 +258,7 @@ def flat_wire(
                 g["entities"][name]["seg"] = seg
 
         g.update(fields(m_sid, uniform_out=True))
+        g.update(soft_tables(moving, d, directional=directional, curvature=curvature))
         groups.append(g)
 
     if compact:
@@ -262,7 +268,88 @@ def flat_wire(
     else:
         es = {"num_samples": int(ns)}
         es.update(fields(np.arange(ns, dtype=np.int64), uniform_out=True))
+    if directional is not None and len(directional["kind"]):
+        es.update({
+            "dir_num": int(len(directional["kind"])),
+            "dir_eps": float(directional["eps"]),
+            "dir_nodes": np.ascontiguousarray(np.asarray(directional["nodes"], dtype=np.int32)),
+            "dir_kind": np.ascontiguousarray(np.asarray(directional["kind"], dtype=np.int32)),
+            "dir_ref": np.ascontiguousarray(np.asarray(directional["ref"], dtype=np.float64)),
+            "dir_axis": np.ascontiguousarray(np.asarray(directional["axis"], dtype=np.float64)),
+            "dir_weight": np.ascontiguousarray(np.asarray(directional["weight"], dtype=np.float64)),
+        })
     return {"groups": groups, "energy_stencil": es}
+
+
+DIR_ARITY = {0: 2, 1: 3, 2: 2}  # parallel, line, stem; other kinds are reserved (arity 0)
+
+
+def soft_tables(moving: np.ndarray, d: int, *, directional: dict | None = None,
+                curvature: dict | None = None) -> dict:
+    """Per-DOF fixed-K soft-term tables of the group (wire layout of
+    ``egg/smoothing/directional.py:381-437`` and
+    ``egg/smoothing/interface_c2.py:233-279``).
+
+    For each moving DOF in ascending order, every term it takes part in is
+    listed with the DOF's slot in the term, in term order, padded to the
+    widest DOF's count K with slot -1.  Node ids stay global.  Returns
+    ``curv_k``/``curv_nodes`` (ndof, K, 4)/``curv_slot``/``curv_weight`` and
+    ``dir_k``/``dir_eps``/``dir_nodes`` (ndof, K, 4)/``dir_slot``/``dir_kind``/
+    ``dir_ref`` and ``dir_axis`` (ndof, K, d)/``dir_weight``; nothing for an
+    absent or empty term set.
+    """
+    moving = np.asarray(moving, dtype=bool)
+    dofs = np.flatnonzero(moving)
+    pos = np.full(moving.shape[0], -1, dtype=np.int64)
+    pos[dofs] = np.arange(dofs.size)
+    out: dict = {}
+
+    def listing(nodes: np.ndarray, arity) -> list:
+        per = [[] for _ in range(dofs.size)]
+        for t in range(nodes.shape[0]):
+            for slot in range(arity(t)):
+                nd = int(nodes[t, slot])
+                if nd >= 0 and moving[nd]:
+                    per[int(pos[nd])].append((t, slot))
+        return per
+
+    if curvature is not None and len(curvature["weight"]) and dofs.size:
+        cn = np.asarray(curvature["nodes"], dtype=np.int64).reshape(-1, 4)
+        cw = np.asarray(curvature["weight"], dtype=np.float64)
+        per = listing(cn, lambda t: 4)
+        K = max(len(e) for e in per)
+        if K:
+            nodes = np.full((dofs.size, K, 4), -1, dtype=np.int32)
+            slot = np.full((dofs.size, K), -1, dtype=np.int32)
+            w = np.zeros((dofs.size, K))
+            for i, e in enumerate(per):
+                for j, (t, sl) in enumerate(e):
+                    nodes[i, j], slot[i, j], w[i, j] = cn[t], sl, cw[t]
+            out.update({"curv_k": int(K), "curv_nodes": nodes.reshape(-1), "curv_slot": slot.reshape(-1),
+                        "curv_weight": w.reshape(-1)})
+    if directional is not None and len(directional["kind"]) and dofs.size:
+        dn = np.asarray(directional["nodes"], dtype=np.int64).reshape(-1, 4)
+        dk = np.asarray(directional["kind"], dtype=np.int64)
+        dr = np.asarray(directional["ref"], dtype=np.float64).reshape(-1, d)
+        da = np.asarray(directional["axis"], dtype=np.float64).reshape(-1, d)
+        dw = np.asarray(directional["weight"], dtype=np.float64)
+        per = listing(dn, lambda t: DIR_ARITY.get(int(dk[t]), 0))
+        K = max(len(e) for e in per)
+        if K:
+            nodes = np.full((dofs.size, K, 4), -1, dtype=np.int32)
+            slot = np.full((dofs.size, K), -1, dtype=np.int32)
+            kind = np.zeros((dofs.size, K), dtype=np.int32)
+            ref = np.zeros((dofs.size, K, d))
+            axis = np.zeros((dofs.size, K, d))
+            w = np.zeros((dofs.size, K))
+            for i, e in enumerate(per):
+                for j, (t, sl) in enumerate(e):
+                    nodes[i, j], slot[i, j], kind[i, j] = dn[t], sl, dk[t]
+                    ref[i, j], axis[i, j], w[i, j] = dr[t], da[t], dw[t]
+            out.update({"dir_k": int(K), "dir_eps": float(directional["eps"]), "dir_nodes": nodes.reshape(-1),
+                        "dir_slot": slot.reshape(-1), "dir_kind": kind.reshape(-1), "dir_ref": ref.reshape(-1),
+                        "dir_axis": axis.reshape(-1), "dir_weight": w.reshape(-1)})
+    return out
 
 
 def structured_tables(blocks: list[np.ndarray]) -> dict:

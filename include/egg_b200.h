@@ -144,6 +144,35 @@ typedef struct egg_b200_session_desc {
      * set_X / restore. */
     const double* entity_arena; /* [entity_arena_len] or NULL */
     int64_t entity_arena_len;
+
+    /* Soft energy terms added to the shape objective (the group's curv_* and
+     * dir_* tables and the energy stencil's dir_* table, src/bindings.cpp:
+     * 380-410,471-480).  Per DOF in group order, K fixed slots each; a slot
+     * of -1 pads.  Node ids are global.  Every moving DOF with a used slot
+     * folds its terms into its Newton system and line search
+     * (src/sweep.hpp:1307-1327,1461-1512,1600-1630, src/directional.hpp:
+     * 221-279, src/curvature.hpp:113-183); reports add the whole-sample
+     * directional total (src/sweep.hpp:1921, src/directional.hpp:281-299).
+     * A curvature window is the 2D block-interface C2 term over four nodes;
+     * a directional sample is kind 0 parallel (2 nodes), 1 line (3), 2 stem
+     * (2); other kinds contribute nothing, as in the reference. */
+    int32_t dir_k;             /* directional samples per DOF, 0 = none */
+    int32_t curv_k;            /* curvature windows per DOF (2D), 0 = none */
+    double dir_eps;            /* regularisation of the unit directions */
+    const int32_t* dir_nodes;  /* [ndof*dir_k*4] */
+    const int32_t* dir_slot;   /* [ndof*dir_k] the DOF's place in the sample */
+    const int32_t* dir_kind;   /* [ndof*dir_k] */
+    const double* dir_ref;     /* [ndof*dir_k*dim] frozen reference vector */
+    const double* dir_weight;  /* [ndof*dir_k] */
+    const int32_t* curv_nodes; /* [ndof*curv_k*4] */
+    const int32_t* curv_slot;  /* [ndof*curv_k] */
+    const double* curv_weight; /* [ndof*curv_k] */
+    int64_t es_dir_num;        /* whole-sample directional table, 0 = none */
+    double es_dir_eps;
+    const int32_t* es_dir_nodes; /* [es_dir_num*4] */
+    const int32_t* es_dir_kind;  /* [es_dir_num] */
+    const double* es_dir_ref;    /* [es_dir_num*dim] */
+    const double* es_dir_weight; /* [es_dir_num] */
 } egg_b200_session_desc;
 
 /* Control-net wire for one block (src/control_net.hpp:72-87 ControlNetHostT;

@@ -21,6 +21,10 @@ Two sources, both from the reference checkout (run in a container that has it):
    dense reduced-GN oracle (``egg.smoothing.control_ref``), with the control
    wires built by the reference's own builders -> ``ref_control.npz``.
 
+5. Soft-term runs of the same core (``ref_soft.npz``): sweeps and FAS cycles
+   on grids carrying directional samples and curvature windows, and the
+   reference's own soft-term wire tables for the same terms.
+
 Usage: python tests/golden/gen_golden_fixtures.py [REFERENCE_ROOT]
 """
 
@@ -183,6 +187,29 @@ FAS_RUNS_CON = [
     ("square_bspline17", "barrier", 3, 2, 2, 32, 1.0, 32),
     ("square_composite17", "barrier", 3, 2, 2, 32, 1.0, 32),
 ]
+# Soft terms (directional samples, 2D curvature windows) on seeded grids:
+# name -> (configs builder, kwargs, with_soft_terms kwargs) -> ref_soft.npz.
+CASES_SOFT = {
+    "square_soft17": ("unit_square", dict(n=17, frac=0.25, seed=11), dict(seed=21)),
+    "disk_oh_soft17": ("disk_oh", dict(n=17, frac=0.25, seed=12), dict(seed=22, block=1)),
+    "slide_soft17": ("square_sliding", dict(n=17, seed=13), dict(seed=23)),
+    "cube_soft7": ("unit_cube", dict(n=7, frac=0.15, seed=14), dict(seed=24, n_dir=30)),
+    "square_soft33": ("unit_square", dict(n=33, frac=0.25, seed=15), dict(seed=25, n_dir=60, n_curv=40)),
+}
+RUNS_SOFT = [
+    ("square_soft17", "barrier", 0.0, 1.0, 30),
+    ("square_soft17", "barrier", 0.0, 0.8, 30),
+    ("square_soft17", "shape_size", 0.0, 1.0, 20),
+    ("square_soft17", "untangle", 1e-3, 0.5, 10),
+    ("disk_oh_soft17", "barrier", 0.0, 1.0, 30),
+    ("slide_soft17", "barrier", 0.0, 1.0, 30),
+    ("cube_soft7", "barrier", 0.0, 1.0, 15),
+    ("cube_soft7", "barrier", 0.0, 0.8, 15),
+]
+FAS_RUNS_SOFT = [
+    ("square_soft33", "barrier", 3, 2, 2, 32, 1.0, 32),
+    ("disk_oh_soft17", "barrier", 3, 2, 2, 32, 0.8, 32),
+]
 ENTITY_RECORDS = {
     1: (0.1, -0.2, 0.9, 0.4),
     2: (0.2, -0.1, 0.7, 0.0),
@@ -198,6 +225,9 @@ ENTITY_RECORDS = {
 def case_grid(name: str):
     from egg_b200 import configs
 
+    if name in CASES_SOFT:
+        fn, kw, skw = CASES_SOFT[name]
+        return configs.with_soft_terms(getattr(configs, fn)(**kw), **skw)
     if name in CASES_CON:
         fn, kw = CASES_CON[name]
         return getattr(configs, fn)(**kw)
@@ -290,6 +320,63 @@ def _constrained_runs() -> dict:
         out[f"entity/{tag}/step"] = steps
         out[f"entity/{tag}/foot"] = feet
     return out
+
+
+def _soft_runs(ref_root: Path) -> dict:
+    """Reference-core sweeps and FAS cycles on the soft-term grids, plus the
+    reference's own per-DOF and whole-sample tables for the wire check."""
+    sys.path.insert(0, str(ref_root))
+    from egg.smoothing.directional import DirectionalSamples, directional_dof_table, directional_energy_table
+    from egg.smoothing.interface_c2 import CurvatureWindows, curvature_dof_table
+
+    from oracle import oracle
+
+    ref = oracle.load_ref("fp64")
+    if ref is None:
+        raise SystemExit("oracle/_ref/fp64 missing: run oracle/build_ref.sh first")
+    out = {}
+    for case in CASES_SOFT:
+        g = case_grid(case)
+        moving = g.free.copy()
+        moving[list(g.constraints)] = True
+        ds = g.soft["directional"]
+        smp = DirectionalSamples(nodes=ds["nodes"], kind=ds["kind"], ref=ds["ref"], axis=ds["axis"],
+                                 weight=ds["weight"], eps=ds["eps"])
+        tabs = {"dof": directional_dof_table(moving, smp), "es": directional_energy_table(smp)}
+        if "curvature" in g.soft:
+            cw = g.soft["curvature"]
+            tabs["dof_curv"] = curvature_dof_table(moving, CurvatureWindows(nodes=cw["nodes"], weight=cw["weight"]))
+        for part, t in tabs.items():
+            for k, v in t.items():
+                out[f"table/{case}/{part}/{k}"] = np.asarray(v)
+    for case, phase, delta, omega, n in RUNS_SOFT:
+        g = case_grid(case)
+        ctx, st = g.wire(), g.structured()
+        X1, _e1, _m1 = ref.cpp_structured_sweep(ctx, st, g.X_flat(), 1, device="cpu", phase=phase,
+                                                 delta=delta, omega=omega, report_every=1, dim=g.d)
+        Xn, en, mn = ref.cpp_structured_sweep(ctx, st, g.X_flat(), n, device="cpu", phase=phase,
+                                               delta=delta, omega=omega, report_every=1, dim=g.d)
+        key = f"{case}/{phase}/{omega}"
+        out[key + "/X1"] = X1
+        out[key + "/Xn"] = Xn
+        out[key + "/E"] = en
+        out[key + "/M"] = mn
+    for case, phase, nc, npre, npost, ncoarse, omega, ml in FAS_RUNS_SOFT:
+        g = case_grid(case)
+        sess = ref.CppStructuredSweepSession(g.wire(), g.structured(), g.X_flat(), device="cpu", dim=g.d)
+        E, M = sess.run_fas(nc, nu_pre=npre, nu_post=npost, nu_coarse=ncoarse, omega=omega, max_levels=ml,
+                            phase=phase)
+        key = f"fas/{case}/{phase}/{ml}"
+        out[key + "/E"] = E
+        out[key + "/M"] = M
+        out[key + "/X"] = sess.get_X()
+    return out
+
+
+def gen_reference_soft(ref_root: Path) -> None:
+    out = _soft_runs(ref_root)
+    np.savez_compressed(HERE / "ref_soft.npz", **out)
+    print(f"ref_soft.npz: {len(out)} arrays")
 
 
 def gen_reference_constrained() -> None:
@@ -472,6 +559,10 @@ if __name__ == "__main__" and len(sys.argv) == 4 and sys.argv[1] == "--runs":
     np.savez(sys.argv[3], **_runs_for(sys.argv[2]))
     raise SystemExit(0)
 
+if __name__ == "__main__" and len(sys.argv) in (2, 3) and sys.argv[1] == "--soft":
+    gen_reference_soft(Path(sys.argv[2]) if len(sys.argv) == 3 else Path("/root/reference"))
+    raise SystemExit(0)
+
 if __name__ == "__main__" and len(sys.argv) == 2 and sys.argv[1] == "--constrained":
     gen_reference_constrained()
     raise SystemExit(0)
@@ -484,3 +575,4 @@ if __name__ == "__main__":
     gen_reference_wire(ref_root)
     gen_reference_control(ref_root)
     gen_reference_constrained()
+    gen_reference_soft(ref_root)
