@@ -27,6 +27,9 @@ Python package.  Conventions (kept identical because the wire is an interface):
   block, target a uniform multiple of the identity) carry no stored samples:
   ``interior_block``/``interior_logical`` name them and ``P_of`` is 0
   (``egg/smoothing/flat_context.py:211-238``).
+* Soft terms ride as per-DOF fixed-K tables on the group (``curv_*``,
+  ``dir_*``) and as one whole-sample directional table on the energy stencil
+  (``egg/smoothing/flat_context.py:293-345``); node ids stay global.
 
 Extension (accepted by this repository's core only): ``compact=True`` emits the
 energy stencil as ``{"num_samples": ns, "structured": 1, "W_inv": row}`` with no
@@ -133,7 +136,7 @@ def flat_wire(
     ``w_inv`` is one ``(d, d)`` inverse target shared by every sample (default
     identity) or ``(ns, d, d)`` per sample in canonical order.  Mirrors
     ``build_flat_context`` (``egg/smoothing/flat_context.py:136-346``) without
-    interface, curvature or directional terms.  ``constraints`` maps a global
+    interface samples.  ``constraints`` maps a global
     node id (not Free) to ``(tag, record)`` or ``(tag, record, seg)``, seg the
     entity's variable-length fields (a B-spline's knots, control points and
     weights), sent as one ``{data, off}`` CSR field each: the node becomes a moving DOF on
