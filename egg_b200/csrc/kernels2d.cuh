@@ -1228,6 +1228,23 @@ __global__ void soft_energy_add_kernel(const SoftTerm* __restrict__ terms, int64
     if (block_reduce(acc, mn)) { *out_e += acc.s + acc.c; }
 }
 
+// Per-mesh directional totals of a batch: CTA m adds the sum over terms
+// [seg[m], seg[m+1]) to out[2m], the mesh's reported energy.
+template <int D>
+__global__ void soft_energy_add_seg_kernel(const SoftTerm* __restrict__ terms, const int64_t* __restrict__ seg,
+                                           double eps, const double* __restrict__ X, double* out)
+{
+    Comp acc {0.0, 0.0};
+    double mn = INFINITY;
+    for (int64_t i = seg[blockIdx.x] + threadIdx.x; i < seg[blockIdx.x + 1]; i += blockDim.x) {
+        const SoftTerm t = terms[i];
+        double p[4][3];
+        soft_load<D>(t, X, p);
+        comp_add(acc, soft_energy<D>(t, p, eps));
+    }
+    if (block_reduce(acc, mn)) { out[2 * int64_t(blockIdx.x)] += acc.s + acc.c; }
+}
+
 // Segmented final pass: CTA m folds partials [m n, (m+1) n) into
 // out[2m] = energy and out[2m+1] = min det of segment m.
 __global__ void reduce_finalize_seg_kernel(const double* part_s, const double* part_c,

@@ -200,6 +200,7 @@ struct Session : LevelData {
     int64_t es_dir_n = 0;
     DevBuf<SoftTerm> es_dir;
     double es_dir_eps = 0.0;
+    DevBuf<int64_t> es_dir_seg;  // batch: [n_seg + 1] each mesh's range of es_dir
     // reductions
     int red_grid = 0;
     DevBuf<double> part;      // [3 * red_grid]
@@ -1504,6 +1505,17 @@ template <int KIND> static void launch_reduce_seg(Session& S, const double* x, d
     S.timed(kKFinal, [&] {
         reduce_finalize_seg_kernel<<<unsigned(S.n_seg), 256, 0, S.stream>>>(ps, pc, pm, S.seg_gx, out);
     });
+    if (S.es_dir_n) {
+        S.timed(kKFinal, [&] {
+            if (S.dim == 3) {
+                soft_energy_add_seg_kernel<3><<<unsigned(S.n_seg), 256, 0, S.stream>>>(S.es_dir.p, S.es_dir_seg.p,
+                                                                                       S.es_dir_eps, x, out);
+            } else {
+                soft_energy_add_seg_kernel<2><<<unsigned(S.n_seg), 256, 0, S.stream>>>(S.es_dir.p, S.es_dir_seg.p,
+                                                                                       S.es_dir_eps, x, out);
+            }
+        });
+    }
 }
 
 // One report's reduction: the whole store (2 doubles) or every mesh of a

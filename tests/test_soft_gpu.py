@@ -3,8 +3,8 @@ line, stem; 2D and 3D) and 2D curvature windows relax exactly as the reference
 core relaxes them (first sweep and trajectory, fp64, the reported energy being
 the composed objective), structured-interior DOFs with terms leave the tile
 path, sliding boundary DOFs take the directional samples only, FAS V-cycles
-match the reference's, the mixed path tracks fp64, and batch sessions with
-soft terms are refused."""
+match the reference's, the mixed path tracks fp64, and batch sessions relax
+each mesh's terms as the reference does."""
 
 from __future__ import annotations
 
@@ -96,7 +96,27 @@ def test_soft_mixed_tracks_fp64(gpu, case):
     assert np.sign(M[-1]) == np.sign(_FX[key + "/M"][-1])
 
 
-def test_batch_with_soft_terms_is_refused(gpu):
-    g = case_grid("square_soft17")
-    with pytest.raises(NotImplementedError, match="soft terms"):
-        gpu.CppBatchSweepSession([(g.wire(compact=True), g.structured(), g.X_flat())], precision="mixed")
+def test_soft_batch_matches_reference_per_mesh(gpu):
+    """A batch of meshes with different soft-term widths (and one without
+    terms) relaxes each mesh as the reference does, and reports each mesh's
+    composed objective."""
+    plain = case_grid("square_soft17")
+    plain.soft = {}
+    gs = [case_grid("square_soft17"), case_grid("slide_soft17"), case_grid("disk_oh_soft17"), plain]
+    b = gpu.CppBatchSweepSession([(g.wire(), g.structured(), g.X_flat()) for g in gs], precision="fp64")
+    E, M = b.run(30, report_every=1)
+    Xb = b.get_X()
+    for m, case in enumerate(["square_soft17", "slide_soft17", "disk_oh_soft17"]):
+        key = f"{case}/barrier/1.0"
+        np.testing.assert_allclose(E[m], _FX[key + "/E"], rtol=1e-9)
+        np.testing.assert_allclose(M[m], _FX[key + "/M"], rtol=1e-8, atol=1e-16)
+        assert np.abs(Xb[m] - _FX[key + "/Xn"]).max() <= 1e-9 * _hmin(gs[m])
+    s = _session(gpu, plain)
+    Ep, _ = s.run(30, report_every=1)
+    np.testing.assert_allclose(E[3], Ep, rtol=1e-12)
+    Ee, _ = b.energy()
+    np.testing.assert_allclose(Ee, E[:, -1], rtol=1e-12)
+    g3 = [case_grid("cube_soft7"), configs.unit_cube(5, seed=3)]
+    b3 = gpu.CppBatchSweepSession([(g.wire(), g.structured(), g.X_flat()) for g in g3], dim=3, precision="fp64")
+    E3, _ = b3.run(15, report_every=1)
+    np.testing.assert_allclose(E3[0], _FX["cube_soft7/barrier/1.0/E"], rtol=1e-9)
