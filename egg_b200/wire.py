@@ -301,6 +301,8 @@ def soft_tables(moving: np.ndarray, d: int, *, directional: dict | None = None,
     ``dir_ref`` and ``dir_axis`` (ndof, K, d)/``dir_weight``; nothing for an
     absent or empty term set.
     """
+    if (directional is None or not len(directional["kind"])) and (curvature is None or not len(curvature["weight"])):
+        return {}
     moving = np.asarray(moving, dtype=bool)
     dofs = np.flatnonzero(moving)
     pos = np.full(moving.shape[0], -1, dtype=np.int64)
