@@ -183,6 +183,39 @@ template <int D> __device__ __forceinline__ void role_dir(int role, const double
     }
 }
 
+// The directional soft terms' nodal gradient added into the net-node
+// gradient y (src/directional.hpp:343-379, src/control_solve.hpp:556-559):
+// every node of every sample, at its owner slot; a slot inside a net's block
+// adds to that net's node.  The control's Newton model and preconditioner
+// stay the shape term's, as in the reference.
+template <int D>
+__global__ void ctl_dir_scatter_kernel(CtlTables T, const SoftTerm* __restrict__ terms, int64_t n, double eps,
+                                       const double* __restrict__ X, double* __restrict__ y)
+{
+    for (int64_t i = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; i < n; i += int64_t(gridDim.x) * blockDim.x) {
+        SoftTerm t = terms[i];
+        const int ar = soft_arity(t.kind);
+        for (int m = 0; m < ar; ++m) {
+            const int64_t slot = t.node[m];
+            int ni = -1;
+            for (int q = 0; q < T.n_nets && ni < 0; ++q) {
+                if (slot >= T.nets[q].node_off && slot < T.nets[q].node_off + T.nets[q].n_nodes) { ni = q; }
+            }
+            if (ni < 0) { continue; }
+            t.slot = m;
+            double g[D], H[D * D], e = 0.0;
+#pragma unroll
+            for (int k = 0; k < D; ++k) { g[k] = 0.0; }
+#pragma unroll
+            for (int k = 0; k < D * D; ++k) { H[k] = 0.0; }
+            soft_accumulate<D>(t, X, eps, g, H, e);
+            const int64_t row = T.nets[ni].n_off + (slot - T.nets[ni].node_off);
+#pragma unroll
+            for (int k = 0; k < D; ++k) { atomicAdd(&y[row * D + k], g[k]); }
+        }
+    }
+}
+
 // Per-node gradient / Hessian-vector product / contracted Hessian over the
 // block's canonical cell stencil (see the file comment).
 template <int D, int KIND, int MODE>

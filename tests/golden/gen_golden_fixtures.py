@@ -206,6 +206,8 @@ RUNS_SOFT = [
     ("cube_soft7", "barrier", 0.0, 1.0, 15),
     ("cube_soft7", "barrier", 0.0, 0.8, 15),
 ]
+# control nets on soft-term grids: (case, block, ctrl shape, n_outer)
+CONTROL_SOFT = [("square_soft17", 0, (6, 6), 8), ("disk_oh_soft17", 1, (6, 6), 8)]
 FAS_RUNS_SOFT = [
     ("square_soft33", "barrier", 3, 2, 2, 32, 1.0, 32),
     ("disk_oh_soft17", "barrier", 3, 2, 2, 32, 0.8, 32),
@@ -361,6 +363,29 @@ def _soft_runs(ref_root: Path) -> dict:
         out[key + "/Xn"] = Xn
         out[key + "/E"] = en
         out[key + "/M"] = mn
+    from egg.geometry.control_net import tensor_map
+    from egg.smoothing.control_backend import build_control_wire
+    from egg.smoothing.control_ref import boolean_sum_b, boundary_ctrl_mask, fit_control_net
+
+    for case, blk, ctrl, n_outer in CONTROL_SOFT:
+        g = case_grid(case)
+        ids = g.blocks[blk]
+        X0b = g.X[ids.reshape(-1)].reshape(ids.shape + (g.d,))
+        cmap = tensor_map(ids.shape, ctrl, degree=3)
+        C0 = fit_control_net(cmap, X0b)
+        wire = build_control_wire(cmap, C0, ~boundary_ctrl_mask(tuple(ctrl)), boolean_sum_b(cmap, C0, X0b),
+                                  block=blk)
+        for k, v in wire.items():
+            out[f"control/{case}/wire/{k}"] = np.asarray(v)
+        sess = ref.CppStructuredSweepSession(g.wire(), g.structured(), g.X_flat(), device="cpu", dim=g.d,
+                                             control=wire)
+        rep = sess.run_control(n_outer)
+        for k in ("energies", "mindets", "alphas", "pcg_iters"):
+            out[f"control/{case}/{k}"] = np.asarray(rep[k], dtype=float)
+        out[f"control/{case}/iters"] = np.int64(rep["iters"])
+        out[f"control/{case}/X"] = np.asarray(sess.get_X())
+        out[f"control/{case}/C"] = np.asarray(sess.get_C())
+        print(case, "control iters", rep["iters"], "E", rep["energies"][0], "->", rep["energies"][-1])
     for case, phase, nc, npre, npost, ncoarse, omega, ml in FAS_RUNS_SOFT:
         g = case_grid(case)
         sess = ref.CppStructuredSweepSession(g.wire(), g.structured(), g.X_flat(), device="cpu", dim=g.d)

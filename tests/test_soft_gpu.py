@@ -3,8 +3,9 @@ line, stem; 2D and 3D) and 2D curvature windows relax exactly as the reference
 core relaxes them (first sweep and trajectory, fp64, the reported energy being
 the composed objective), structured-interior DOFs with terms leave the tile
 path, sliding boundary DOFs take the directional samples only, FAS V-cycles
-match the reference's, the mixed path tracks fp64, and batch sessions relax
-each mesh's terms as the reference does."""
+match the reference's, the mixed path tracks fp64, batch sessions relax
+each mesh's terms as the reference does, and control nets take the
+directional gradient and the composed objective."""
 
 from __future__ import annotations
 
@@ -13,7 +14,7 @@ import pytest
 
 from egg_b200 import configs
 from tests.conftest import GOLDEN
-from tests.golden.gen_golden_fixtures import FAS_RUNS_SOFT, RUNS_SOFT, case_grid
+from tests.golden.gen_golden_fixtures import CONTROL_SOFT, FAS_RUNS_SOFT, RUNS_SOFT, case_grid
 
 pytestmark = pytest.mark.gpu
 
@@ -120,3 +121,25 @@ def test_soft_batch_matches_reference_per_mesh(gpu):
     b3 = gpu.CppBatchSweepSession([(g.wire(), g.structured(), g.X_flat()) for g in g3], dim=3, precision="fp64")
     E3, _ = b3.run(15, report_every=1)
     np.testing.assert_allclose(E3[0], _FX["cube_soft7/barrier/1.0/E"], rtol=1e-9)
+
+
+@pytest.mark.parametrize("case, blk, ctrl, n_outer", CONTROL_SOFT, ids=lambda v: str(v))
+def test_soft_control_net_matches_reference(gpu, case, blk, ctrl, n_outer):
+    """A control net on a grid with soft terms: the reduced gradient takes
+    the directional samples' nodal gradient, every accept energy the
+    composed objective (the net's block holds the terms in both cases)."""
+    g = case_grid(case)
+    pre = f"control/{case}/"
+    w = {k[len(pre + "wire/"):]: _FX[k] for k in _FX.files if k.startswith(pre + "wire/")}
+    w["block"] = int(w["block"])
+    w["k_supp"] = int(w["k_supp"])
+    s = gpu.CppStructuredSweepSession(g.wire(), g.structured(), g.X_flat(), dim=g.d, control=w)
+    rep = s.run_control(n_outer)
+    assert rep["iters"] == int(_FX[pre + "iters"])
+    e_ref = _FX[pre + "energies"]
+    np.testing.assert_allclose(rep["energies"], e_ref, rtol=1e-9, atol=1e-12 * abs(e_ref[0]))
+    np.testing.assert_allclose(rep["mindets"], _FX[pre + "mindets"], rtol=1e-8)
+    np.testing.assert_array_equal(rep["alphas"], _FX[pre + "alphas"])
+    scale = np.abs(g.X).max()
+    np.testing.assert_allclose(s.get_X(), _FX[pre + "X"], rtol=0, atol=1e-8 * scale)
+    np.testing.assert_allclose(s.get_C(), _FX[pre + "C"], rtol=0, atol=1e-8 * scale)
