@@ -385,6 +385,68 @@ def square_composite(n: int = 17, frac: float = 0.2, slide: float = 0.3, seed: i
     return Grid(f"square_composite{n}", 2, g.blocks, X, g.free.copy(), {"frac": frac, "seed": seed}, cons)
 
 
+def _composite_slice(segs) -> np.ndarray:
+    """A composite path's arena slice: the segment records ([tag, params...]
+    padded to 13 reals) followed by each B-spline segment's knots, control
+    points and weights.  A B-spline segment is given as
+    ``(10, (degree, knots, ctrl, weights or None, t0, t1))`` and its record
+    blob becomes [degree, n_ctrl, knot_off, ctrl_off, t0, t1, w_off, has_w]
+    with offsets into the slice (``src/geometry.hpp:1524-1550``)."""
+    recs = np.zeros((len(segs), 13))
+    data: list[np.ndarray] = []
+    at = recs.size
+    for k, (tag, params) in enumerate(segs):
+        recs[k, 0] = tag
+        if tag != 10:
+            recs[k, 1 : 1 + len(params)] = params
+            continue
+        deg, knots, ctrl, w, t0, t1 = params
+        knots = np.asarray(knots, dtype=np.float64)
+        ctrl = np.asarray(ctrl, dtype=np.float64).ravel()
+        ko, co = at, at + knots.size
+        at = co + ctrl.size
+        data += [knots, ctrl]
+        wo = at
+        if w is not None:
+            data.append(np.asarray(w, dtype=np.float64))
+            at += len(w)
+        recs[k, 1:9] = (deg, ctrl.size // 2, ko, co, t0, t1, wo, 0.0 if w is None else 1.0)
+    return np.concatenate([recs.ravel()] + data)
+
+
+def square_composite_bspline(n: int = 17, frac: float = 0.2, slide: float = 0.3, seed: int = 0) -> Grid:
+    """Unit square whose bottom and top sides are composite paths with
+    B-spline segments: bottom = LineSeg (0,0)-(0.3,0), a clamped cubic
+    B-spline from (0.3,0) to (0.7,0) dipping below the side, LineSeg
+    (0.7,0)-(1,0); top = a rational quadratic NURBS from (0,1) to (0.6,1),
+    then LineSeg (0.6,1)-(1,1).  Side nodes sit on their path (on the
+    spline at the parameter their x maps to), moved by up to ``slide`` of a
+    step, and slide along it.  Corners stay fixed."""
+    g = unit_square(n, frac=frac, seed=seed)
+    ids = g.blocks[0]
+    X = g.X.copy()
+    rng = np.random.default_rng(seed + 808)
+    x = np.linspace(0.0, 1.0, n)[1:-1] + rng.uniform(-slide, slide, n - 2) / (n - 1)
+    b_sp = (3, [0, 0, 0, 0, 0.5, 1, 1, 1, 1], [[0.3, 0], [0.4, -0.06], [0.5, 0.02], [0.6, -0.05], [0.7, 0]], None,
+            0.0, 1.0)
+    t_sp = (2, [0, 0, 0, 1 / 3, 2 / 3, 1, 1, 1], [[0, 1], [0.15, 1.06], [0.3, 0.98], [0.45, 1.04], [0.6, 1]],
+            [1.0, 0.8, 1.2, 0.9, 1.0], 0.0, 1.0)
+    bot = [(1, (0.0, 0.0, 0.3, 0.0)), (10, b_sp), (1, (0.7, 0.0, 1.0, 0.0))]
+    top = [(10, t_sp), (1, (0.6, 1.0, 1.0, 1.0))]
+    tb = np.clip((x - 0.3) / 0.4, 0.0, 1.0)
+    pb = _nurbs_points(b_sp[0], b_sp[1], b_sp[2], b_sp[3], tb)
+    X[ids[1:-1, 0]] = np.where(((x > 0.3) & (x < 0.7))[:, None], pb, np.stack([x, np.zeros_like(x)], axis=1))
+    tt = np.clip(x / 0.6, 0.0, 1.0)
+    pt = _nurbs_points(t_sp[0], t_sp[1], t_sp[2], t_sp[3], tt)
+    X[ids[1:-1, -1]] = np.where((x < 0.6)[:, None], pt, np.stack([x, np.ones_like(x)], axis=1))
+    cons = {}
+    for nodes, segs in ((ids[1:-1, 0], bot), (ids[1:-1, -1], top)):
+        sl = _composite_slice(segs)
+        for v in nodes:
+            cons[int(v)] = (11, (float(len(segs)), 0.0), (sl,))
+    return Grid(f"square_compbsp{n}", 2, g.blocks, X, g.free.copy(), {"frac": frac, "seed": seed}, cons)
+
+
 def cube_sliding(n: int = 9, frac: float = 0.2, slide: float = 0.3, off: float = 0.02, seed: int = 0,
                  rail_end: float = 0.6) -> Grid:
     """Unit cube whose face nodes slide on their planes (Plane entities, tag 5)

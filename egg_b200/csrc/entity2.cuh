@@ -657,11 +657,32 @@ constexpr int kCompositeRec = 13;
 EGG_HD bool composite_segment_ok(int tag)
 {
     return tag == EGG_B200_TAG_LINESEG || tag == EGG_B200_TAG_CIRCLE || tag == EGG_B200_TAG_ELLIPSE ||
-           tag == EGG_B200_TAG_LINERAIL || is_tcurve(tag);
+           tag == EGG_B200_TAG_LINERAIL || tag == EGG_B200_TAG_BSPLINE || is_tcurve(tag);
 }
 
-EGG_OUTLINE void composite_frame(const double* recs, int n_segs, double px, double py, double& qx, double& qy,
-                            double& tx, double& ty)
+// A B-spline segment of a composite path: blob [degree, n_ctrl, knot_off,
+// ctrl_off, t0, t1, w_off, has_w], offsets into the path's arena slice, an
+// open trim (src/geometry.hpp:1524-1550).
+EGG_HD BSplineCurve composite_bspline(const double* b, const double* slice)
+{
+    BSplineCurve c;
+    c.p = int(b[0]);
+    c.n = int(b[1]);
+    c.knots = slice + int64_t(b[2]);
+    c.ctrl = slice + int64_t(b[3]);
+    c.t0 = b[4];
+    c.t1 = b[5];
+    c.closed = false;
+    c.w = b[7] != 0.0 ? slice + int64_t(b[6]) : nullptr;
+    return c;
+}
+
+// Nearest segment of a composite path (src/geometry.hpp:2587-2617): every
+// segment projects cold (a B-spline from its grid, unseeded) and the closest
+// foot wins, with its segment's unit tangent.  `slice` is the path's arena
+// slice (B-spline data offsets are relative to it), `recs` its records.
+EGG_OUTLINE void composite_frame(const double* slice, const double* recs, int n_segs, double px, double py,
+                                 double& qx, double& qy, double& tx, double& ty)
 {
     qx = px;
     qy = py;
@@ -673,6 +694,23 @@ EGG_OUTLINE void composite_frame(const double* recs, int n_segs, double px, doub
         const int tag = int(rec[0]);
         if (!composite_segment_ok(tag)) { continue; }
         double fx, fy;
+        if (tag == EGG_B200_TAG_BSPLINE) {
+            const BSplineCurve c = composite_bspline(rec + 1, slice);
+            double q = bspline_foot(c, px, py, INFINITY);
+            if (!bspline_inside(c, q)) { q = bspline_clamp(c, q); }
+            bspline_point(c, q, 0, fx, fy);
+            const double dx = fx - px, dy = fy - py;
+            const double dd = dx * dx + dy * dy;
+            if (dd < best) {
+                best = dd;
+                qx = fx;
+                qy = fy;
+                double jx, jy;
+                bspline_point(c, q, 1, jx, jy);
+                unit_or_e0(jx, jy, tx, ty);
+            }
+            continue;
+        }
         entity_project(tag, rec + 1, px, py, fx, fy);
         const double dx = fx - px, dy = fy - py;
         const double dd = dx * dx + dy * dy;
@@ -685,11 +723,11 @@ EGG_OUTLINE void composite_frame(const double* recs, int n_segs, double px, doub
     }
 }
 
-EGG_HD void composite_newton_step(const double* recs, int n_segs, const double H[4], const double g[2], double px,
-                                  double py, double out[2])
+EGG_HD void composite_newton_step(const double* slice, const double* recs, int n_segs, const double H[4],
+                                  const double g[2], double px, double py, double out[2])
 {
     double qx, qy, bx, by;
-    composite_frame(recs, n_segs, px, py, qx, qy, bx, by);
+    composite_frame(slice, recs, n_segs, px, py, qx, qy, bx, by);
     const double hb0 = H[0] * bx + H[1] * by;
     const double hb1 = H[2] * bx + H[3] * by;
     const double M = bx * hb0 + by * hb1;

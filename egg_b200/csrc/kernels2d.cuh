@@ -940,7 +940,8 @@ __global__ void stored_patch_kernel(StoredPatch2 sp, const double2* __restrict__
         // (src/sweep.hpp:1219-1265).
         const bool bsp = etag == EGG_B200_TAG_BSPLINE;
         const bool comp = etag == EGG_B200_TAG_COMPOSITE;
-        const double* crec = comp ? sp.arena + int64_t(er[6]) + int64_t(er[1]) : nullptr;
+        const double* cslice = comp ? sp.arena + int64_t(er[6]) : nullptr;  // the path's arena slice
+        const double* crec = comp ? cslice + int64_t(er[1]) : nullptr;
         const int cseg = comp ? int(er[0]) : 0;
         double seed = bsp ? sp.seeds[d] : 0.0;
         BSplineCurve bc {};
@@ -950,7 +951,7 @@ __global__ void stored_patch_kernel(StoredPatch2 sp, const double2* __restrict__
         if (etag == 0) {
             solve2<double>(h, g, dl);
         } else if (comp) {  // one path for every sweep: step on the nearest segment's tangent
-            composite_newton_step(crec, cseg, h, g, pos.x, pos.y, dl);
+            composite_newton_step(cslice, crec, cseg, h, g, pos.x, pos.y, dl);
             dl[0] *= omega;
             dl[1] *= omega;
         } else if (bsp) {
@@ -974,7 +975,7 @@ __global__ void stored_patch_kernel(StoredPatch2 sp, const double2* __restrict__
             double2 trial = make_double2(pos.x + alpha * dl[0], pos.y + alpha * dl[1]);
             if (comp) {
                 double tx, ty;
-                composite_frame(crec, cseg, trial.x, trial.y, trial.x, trial.y, tx, ty);
+                composite_frame(cslice, crec, cseg, trial.x, trial.y, trial.x, trial.y, tx, ty);
             } else if (bsp) {
                 if (sp.cold) {
                     bspline_project_seeded(bc, trial.x, trial.y, seed, trial.x, trial.y);

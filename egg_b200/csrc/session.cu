@@ -723,10 +723,23 @@ static Session* create_session(const egg_b200_session_desc& d)
                     invalid("validate_context: composite segment records outside entity_arena");
                 }
                 for (int64_t k = 0; k < ns; ++k) {
-                    const int st = int(d.entity_arena[at + ro + k * kCompositeRec]);
+                    const double* sr = d.entity_arena + at + ro + k * kCompositeRec;
+                    const int st = int(sr[0]);
                     if (st != 0 && st != EGG_B200_TAG_COMPOSITE && !composite_segment_ok(st)) {
                         throw Error(EGG_B200_ENOTSUP, "egg_b200: composite segment tag " + std::to_string(st) +
-                                                        " is not supported (fixed-size 2D curves are)");
+                                                        " is not supported (2D curves are)");
+                    }
+                    if (st == EGG_B200_TAG_BSPLINE) {  // blob [degree, n_ctrl, knots, ctrl, t0, t1, w, has_w]
+                        const double* b = sr + 1;
+                        const int64_t deg = int64_t(b[0]), nc = int64_t(b[1]);
+                        auto in_slice = [&](double o, int64_t len) {
+                            return o >= 0.0 && double(int64_t(o)) == o && at + int64_t(o) + len <= d.entity_arena_len;
+                        };
+                        if (double(deg) != b[0] || deg < 1 || deg > kBSplineMaxDegree || double(nc) != b[1] ||
+                            nc < deg + 1 || !in_slice(b[2], nc + deg + 1) || !in_slice(b[3], 2 * nc) ||
+                            (b[7] != 0.0 && !in_slice(b[6], nc))) {
+                            invalid("validate_context: a composite B-spline segment's data lies outside entity_arena");
+                        }
                     }
                 }
             }

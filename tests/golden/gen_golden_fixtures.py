@@ -150,6 +150,7 @@ CASES_CON = {
     "cube_curved9": ("cube_curved", dict(n=9, seed=11)),
     "square_bspline17": ("square_bspline", dict(n=17, seed=12)),
     "square_composite17": ("square_composite", dict(n=17, seed=13)),
+    "square_compbsp17": ("square_composite_bspline", dict(n=17, seed=14)),
 }
 RUNS_CON = [
     # (case, phase, delta, omega, n_sweeps)
@@ -174,6 +175,9 @@ RUNS_CON = [
     ("square_bspline17", "shape_size", 0.0, 1.0, 20),
     ("square_composite17", "barrier", 0.0, 1.0, 30),
     ("square_composite17", "barrier", 0.0, 0.8, 30),
+    ("square_compbsp17", "barrier", 0.0, 1.0, 30),
+    ("square_compbsp17", "barrier", 0.0, 0.8, 30),
+    ("square_compbsp17", "shape_size", 0.0, 1.0, 20),
 ]
 # FAS V-cycles on sliding-boundary grids: (case, phase, n_cycles, nu_pre, nu_post, nu_coarse, omega, max_levels)
 FAS_RUNS_CON = [
@@ -186,6 +190,7 @@ FAS_RUNS_CON = [
     ("cube_curved9", "barrier", 3, 2, 2, 16, 1.0, 32),
     ("square_bspline17", "barrier", 3, 2, 2, 32, 1.0, 32),
     ("square_composite17", "barrier", 3, 2, 2, 32, 1.0, 32),
+    ("square_compbsp17", "barrier", 3, 2, 2, 32, 1.0, 32),
 ]
 # Soft terms (directional samples, 2D curvature windows) on seeded grids:
 # name -> (configs builder, kwargs, with_soft_terms kwargs) -> ref_soft.npz.

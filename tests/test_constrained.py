@@ -22,7 +22,7 @@ _FX = np.load(GOLDEN / "ref_constrained.npz")
                                   configs.disk_on_curve(9, arcs=True), configs.disk_on_curve(9, ry=0.6, arcs=True),
                                   configs.square_sliding(9), configs.square_bezier(9),
                                   configs.cube_sliding(5), configs.cube_curved(5), configs.square_bspline(9),
-                                  configs.square_composite(9)],
+                                  configs.square_composite(9), configs.square_composite_bspline(9)],
                          ids=lambda g: g.name)
 def test_wire_partitions_cover_every_dof_once(grid):
     grp = grid.wire()["groups"][0]

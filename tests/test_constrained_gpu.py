@@ -1,6 +1,6 @@
 """Constrained boundary DOFs on the GPU: nodes sliding on a Circle, an
 Ellipse, trimmed CircleArcs, EllipseArcs, Beziers and B-splines, composite
-paths, LineSegs, a LineRail,
+paths (of fixed-size curves and of B-spline segments), LineSegs, a LineRail,
 Planes, a Sphere, a Cylinder, a Line3 and a LineRail3 relax exactly as the reference core relaxes
 them (first sweep and trajectory, fp64), the mixed path tracks that, every
 accepted boundary node lies on its entity, a batch of constrained meshes
@@ -182,7 +182,7 @@ def test_constrained_mixed_tracks_fp64(gpu, case):
 def test_constrained_batch_equals_separate_sessions(gpu):
     gs = [case_grid("disk_circle17"), case_grid("square_slide17"), case_grid("disk_ellipse17"),
           case_grid("disk_arcs17"), case_grid("square_bspline17"), configs.square_bspline(13, seed=21),
-          case_grid("square_composite17")]
+          case_grid("square_composite17"), case_grid("square_compbsp17")]
     b = gpu.CppBatchSweepSession([(g.wire(compact=True), g.structured(), g.X_flat()) for g in gs],
                                  precision="mixed")
     b.set_variant(1)
