@@ -43,3 +43,25 @@ def test_soft_tables_absent_without_terms():
     w = g.wire()
     assert "dir_k" not in w["groups"][0] and "curv_k" not in w["groups"][0]
     assert "dir_num" not in w["energy_stencil"]
+
+
+@pytest.mark.parametrize("key, cut", [("dir_nodes", 1), ("dir_ref", 2), ("dir_weight", 1), ("curv_slot", 1),
+                                      ("curv_weight", 3)])
+def test_malformed_soft_tables_are_refused_before_the_device(core, key, cut):
+    g = case_grid("square_soft17")
+    w = g.wire()
+    w["groups"][0][key] = w["groups"][0][key][:-cut]
+    with pytest.raises(ValueError, match=key):
+        core.CppStructuredSweepSession(w, g.structured(), g.X_flat())
+
+
+def test_malformed_whole_sample_table_is_refused(core):
+    g = case_grid("square_soft17")
+    w = g.wire()
+    w["energy_stencil"]["dir_kind"] = w["energy_stencil"]["dir_kind"][:-1]
+    with pytest.raises(ValueError, match="dir_kind"):
+        core.CppStructuredSweepSession(w, g.structured(), g.X_flat())
+    w = g.wire()
+    w["groups"][0]["dir_k"] = -1
+    with pytest.raises(ValueError, match="dir_k"):
+        core.CppStructuredSweepSession(w, g.structured(), g.X_flat())
