@@ -503,6 +503,9 @@ CONTROL_CASES = {
     "wavy13ss": ("wavy", dict(n=13), (6, 6), 0, "shape_size", 12, {}, False),
     "cube9c": ("unit_cube", dict(n=9, frac=0.15, seed=31), (5, 5, 5), 0, "barrier", 8, {}, False),
     "disk17c": ("disk_oh", dict(n=17, frac=0.25, seed=2), (6, 6), 0, "barrier", 8, {}, False),
+    # sessions with constrained boundary DOFs (sliding sides; a circle outside the net's block)
+    "slide17c": ("square_sliding", dict(n=17, seed=5), (6, 6), 0, "barrier", 8, {}, False),
+    "circle17c": ("disk_on_curve", dict(n=17, seed=3), (6, 6), 0, "barrier", 8, {}, False),
 }
 
 
