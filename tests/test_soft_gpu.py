@@ -143,3 +143,26 @@ def test_soft_control_net_matches_reference(gpu, case, blk, ctrl, n_outer):
     scale = np.abs(g.X).max()
     np.testing.assert_allclose(s.get_X(), _FX[pre + "X"], rtol=0, atol=1e-8 * scale)
     np.testing.assert_allclose(s.get_C(), _FX[pre + "C"], rtol=0, atol=1e-8 * scale)
+
+
+def test_soft_batch_of_control_nets_matches_reference(gpu):
+    """Two soft-term meshes with one net each, solved together: each mesh's
+    reduced gradient takes only its own directional samples."""
+    cases = [c for c, *_ in CONTROL_SOFT]
+    gs = [case_grid(c) for c in cases]
+    wires = []
+    for c in cases:
+        pre = f"control/{c}/wire/"
+        w = {k[len(pre):]: _FX[k] for k in _FX.files if k.startswith(pre)}
+        w["block"] = int(w["block"])
+        w["k_supp"] = int(w["k_supp"])
+        wires.append(w)
+    bs = gpu.CppBatchSweepSession([(g.wire(compact=True), g.structured(), g.X_flat()) for g in gs], control=wires)
+    reps = bs.run_control(CONTROL_SOFT[0][3])
+    Xb = bs.get_X()
+    for m, (c, g) in enumerate(zip(cases, gs)):
+        pre = f"control/{c}/"
+        assert reps[m]["iters"] == int(_FX[pre + "iters"])
+        e_ref = _FX[pre + "energies"]
+        np.testing.assert_allclose(reps[m]["energies"], e_ref, rtol=1e-9, atol=1e-12 * abs(e_ref[0]))
+        np.testing.assert_allclose(Xb[m], _FX[pre + "X"], rtol=0, atol=1e-8 * np.abs(g.X).max())
