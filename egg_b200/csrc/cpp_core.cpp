@@ -111,6 +111,11 @@ int64_t checked_num_nodes(const DArr& X, int d)
     return int64_t(buf.shape[0]) / d;
 }
 
+struct PinnedBuf {
+    void* p;
+    int64_t bytes;
+};
+
 struct Desc {
     egg_b200_session_desc d {};
     Keep keep;
@@ -550,7 +555,23 @@ class Session
 
     py::array_t<double> get_X()
     {
-        py::array_t<double> X(py::ssize_t(M_ * dim_));
+        // A page-locked buffer from the pool when one can be had, so the
+        // device writes straight into the result; it returns to the pool when
+        // the array is freed.  Otherwise ordinary numpy memory.
+        const int64_t n = int64_t(M_ * dim_), bytes = n * int64_t(sizeof(double));
+        void* pin = nullptr;
+        py::array_t<double> X;
+        if (bytes > 0 && egg_b200_pinned_acquire(bytes, &pin) == EGG_B200_OK && pin) {
+            auto* rec = new PinnedBuf {pin, bytes};
+            py::capsule owner(rec, [](void* r) {
+                auto* b = static_cast<PinnedBuf*>(r);
+                egg_b200_pinned_release(b->p, b->bytes);
+                delete b;
+            });
+            X = py::array_t<double>({py::ssize_t(n)}, {py::ssize_t(sizeof(double))}, static_cast<double*>(pin), owner);
+        } else {
+            X = py::array_t<double>(py::ssize_t(n));
+        }
         double* out = X.mutable_data();
         int rc;
         {

@@ -2340,9 +2340,18 @@ int egg_b200_session_get_X(egg_b200_session* s, double* X, int64_t len)
             EGG_CK(cudaGetLastError());
             ++S.launches;
         }
-        // D2H slice by slice, each followed by its event; host thread t waits
-        // for slice t only, so the copy-out of early slices overlaps the DMA.
-        const int T = copy_threads(n * sizeof(double));
+        // Page-locked output: one DMA straight into it.
+        cudaPointerAttributes attr {};
+        const bool pinned = cudaPointerGetAttributes(&attr, X) == cudaSuccess && attr.type == cudaMemoryTypeHost;
+        cudaGetLastError();
+        if (pinned && n) {
+            EGG_CK(cudaMemcpyAsync(X, S.Xg.p, n * sizeof(double), cudaMemcpyDeviceToHost, S.stream));
+            EGG_CK(cudaStreamSynchronize(S.stream));
+        }
+        // Otherwise D2H slice by slice, each followed by its event; host thread
+        // t waits for slice t only, so the copy-out of early slices overlaps
+        // the DMA.
+        const int T = pinned ? 0 : copy_threads(n * sizeof(double));
         for (int t = 0; t < T; ++t) {
             const size_t a = slice_begin(n, t, T), b = slice_begin(n, t + 1, T);
             if (b > a) {
@@ -2352,12 +2361,14 @@ int egg_b200_session_get_X(egg_b200_session* s, double* X, int64_t len)
             EGG_CK(cudaEventRecord(S.xfer_ev[t], S.stream));
         }
         cudaError_t err[kMaxCopyThreads] = {};
-        run_slices(T, [&](int t) {
-            const size_t a = slice_begin(n, t, T), b = slice_begin(n, t + 1, T);
-            err[t] = cudaSetDevice(S.device);
-            if (err[t] == cudaSuccess) { err[t] = cudaEventSynchronize(S.xfer_ev[t]); }
-            if (err[t] == cudaSuccess && b > a) { std::memcpy(X + a, S.pin + a, (b - a) * sizeof(double)); }
-        });
+        if (T > 0) {
+            run_slices(T, [&](int t) {
+                const size_t a = slice_begin(n, t, T), b = slice_begin(n, t + 1, T);
+                err[t] = cudaSetDevice(S.device);
+                if (err[t] == cudaSuccess) { err[t] = cudaEventSynchronize(S.xfer_ev[t]); }
+                if (err[t] == cudaSuccess && b > a) { std::memcpy(X + a, S.pin + a, (b - a) * sizeof(double)); }
+            });
+        }
         for (int t = 0; t < T; ++t) { EGG_CK(err[t]); }
         for (size_t j = 0; j < S.nb_gid.size(); ++j) {
             for (int k = 0; k < D; ++k) { X[S.nb_gid[j] * D + k] = S.nb_val[j * D + k]; }
@@ -2689,6 +2700,51 @@ int egg_b200_newton_step(const double* grad, const double* hess, double* step)
         EGG_CK(cudaGetLastError());
         EGG_CK(cudaMemcpy(step, ds.p, 2 * sizeof(double), cudaMemcpyDeviceToHost));
     });
+}
+
+namespace {
+struct PinnedPool {
+    std::mutex m;
+    std::unordered_multimap<int64_t, void*> free;
+};
+PinnedPool& pinned_pool()
+{
+    static PinnedPool* p = new PinnedPool;  // outlives every array that holds a buffer
+    return *p;
+}
+}  // namespace
+
+int egg_b200_pinned_acquire(int64_t bytes, void** out)
+{
+    return guarded([&] {
+        if (!out || bytes <= 0) { invalid("pinned_acquire: bad arguments"); }
+        *out = nullptr;
+        PinnedPool& P = pinned_pool();
+        {
+            std::lock_guard<std::mutex> lk(P.m);
+            const auto it = P.free.find(bytes);
+            if (it != P.free.end()) {
+                *out = it->second;
+                P.free.erase(it);
+                return;
+            }
+        }
+        EGG_CK(cudaHostAlloc(out, size_t(bytes), cudaHostAllocPortable));
+    });
+}
+
+void egg_b200_pinned_release(void* p, int64_t bytes)
+{
+    if (!p) { return; }
+    PinnedPool& P = pinned_pool();
+    {
+        std::lock_guard<std::mutex> lk(P.m);
+        if (P.free.count(bytes) < 4) {
+            P.free.emplace(bytes, p);
+            return;
+        }
+    }
+    cudaFreeHost(p);
 }
 
 }  // extern "C"

@@ -56,7 +56,8 @@ extern "C" {
                                   * entity_arena (knots n_ctrl+degree+1, ctrl 2 n_ctrl, weights n_ctrl) */
 #define EGG_B200_TAG_COMPOSITE 11 /* record (n_segs, rec_off, 0, 0, 0, 0, slice_at): a path of segment records
                                    * [tag, 12 params] at entity_arena[slice_at + rec_off ...]; segments are the
-                                   * fixed-size 2D curves (tags 1, 2, 3, 6, 7, 8, 9, 15) */
+                                   * 2D curves (tags 1, 2, 3, 6, 7, 8, 9, 10, 15); a B-spline segment's blob
+                                   * (degree, n_ctrl, knots, ctrl, t0, t1, w, has_w) offsets into the slice */
 #define EGG_B200_TAG_LINERAIL 15 /* record (sx, sy, ex, ey): open-ended segment, released beyond its ends */
 #define EGG_B200_TAG_SPHERE 4    /* 3D record (c(3), r, ax(3), ay(3)): untrimmed sphere, frame ax, ay, ax x ay */
 #define EGG_B200_TAG_PLANE 5     /* 3D record (o(3), ax(3), ay(3)): untrimmed plane, orthonormal in-plane axes */
@@ -327,6 +328,13 @@ int egg_b200_session_energy_noalloc(egg_b200_session* s, int32_t objective, doub
 
 /* Download the resident positions in GLOBAL node order ([num_nodes*dim]).
  * Replaces CppStructuredSweepSession::get_X (src/bindings.cpp:1359-1376). */
+/* Page-locked host buffers from a process-wide pool (no counterpart in the
+ * reference).  get_X into such a buffer is one DMA, with no staging copy.
+ * release returns the buffer to the pool, which keeps up to four buffers
+ * per size and frees the rest.  acquire returns EGG_B200_ERUNTIME when the
+ * page-lock fails; the caller then uses ordinary memory. */
+int egg_b200_pinned_acquire(int64_t bytes, void** out);
+void egg_b200_pinned_release(void* p, int64_t bytes);
 int egg_b200_session_get_X(egg_b200_session* s, double* X, int64_t len);
 
 /* Upload positions in global node order, scattered into every copy.
