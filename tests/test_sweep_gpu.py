@@ -330,3 +330,26 @@ def test_singular_owner_override_changes_nothing(gpu):
     Eb, Mb = b.run(6, report_every=2)
     np.testing.assert_array_equal(a.get_X(), b.get_X())
     np.testing.assert_allclose(Ea, Eb, rtol=1e-14)
+
+
+def test_get_x_results_are_independent_pooled_arrays(gpu):
+    """get_X hands out page-locked pooled buffers: every result is its own
+    array (no aliasing between live results), and a buffer recycled after its
+    array is freed carries the new positions."""
+    g = case_grid("square33")
+    s = _session(gpu, g)
+    a = s.get_X()
+    s.run(2)
+    b = s.get_X()
+    assert not np.shares_memory(a, b)
+    np.testing.assert_array_equal(a, g.X_flat())
+    b_copy = b.copy()
+    a[:] = -1.0
+    np.testing.assert_array_equal(b, b_copy)
+    del a
+    s.run(1)
+    c = s.get_X()
+    assert not np.shares_memory(b, c)
+    assert not np.array_equal(c, b_copy)
+    s.set_X(c)
+    np.testing.assert_array_equal(s.get_X(), c)
