@@ -39,13 +39,19 @@ void check(int st)
     if (st != EGG_B200_OK) { raise_status(st); }
 }
 
-// Default arithmetic of new sessions: EGG_B200_PRECISION=mixed selects fp32
-// bulk; anything else (or unset) is plain fp64, the reference's double build.
+// Default arithmetic of sessions created without `precision=` (every session
+// a reference caller creates): EGG_B200_PRECISION=mixed selects fp32 bulk;
+// anything else (or unset) is plain fp64, the reference's double build.  Read
+// once, at the first use (module import), so that REAL_IS_FLOAT -- the
+// reference's "this core computes in float" -- holds for every such session.
 int default_precision()
 {
-    const char* v = std::getenv("EGG_B200_PRECISION");
-    if (v && (std::string(v) == "mixed" || std::string(v) == "fp32")) { return EGG_B200_PREC_MIXED; }
-    return EGG_B200_PREC_FP64;
+    static const int prec = [] {
+        const char* v = std::getenv("EGG_B200_PRECISION");
+        if (v && (std::string(v) == "mixed" || std::string(v) == "fp32")) { return int(EGG_B200_PREC_MIXED); }
+        return int(EGG_B200_PREC_FP64);
+    }();
+    return prec;
 }
 
 int parse_precision(const py::object& p)
@@ -565,7 +571,7 @@ class Session
             auto* rec = new PinnedBuf {pin, bytes};
             py::capsule owner(rec, [](void* r) {
                 auto* b = static_cast<PinnedBuf*>(r);
-                egg_b200_pinned_release(b->p, b->bytes);
+                egg_b200_pinned_release(b->p);
                 delete b;
             });
             X = py::array_t<double>({py::ssize_t(n)}, {py::ssize_t(sizeof(double))}, static_cast<double*>(pin), owner);

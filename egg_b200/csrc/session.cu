@@ -2,6 +2,7 @@
 // state, the block-Jacobi driver, and the C-ABI declared in include/egg_b200.h.
 #include "egg_b200.h"
 #include "kernels2d.cuh"
+#include "kernels2d_x2.cuh"
 #include "kernels3d.cuh"
 #include "fas.cuh"
 #include "control.cuh"
@@ -82,7 +83,9 @@ template <class T> struct DevBuf {
 // session's autotuner times each on the session's own data and keeps the
 // fastest (egg_b200_session_autotune).
 // 2D: (ci, cj) cells per CTA, or with fd = 1 (ci, cj) DOFs per CTA over the
-// (ci+1) x (cj+1) cells around them; 3D: (ci, cj, ck) DOFs per CTA.
+// (ci+1) x (cj+1) cells around them; fd = 2 is the same full-DOF tile on the
+// packed two-lane fp32 kernel (interior_x2_kernel, mixed precision only);
+// 3D: (ci, cj, ck) DOFs per CTA.
 struct Variant {
     int ci, cj, ck, minb, fd = 0;
 };
@@ -90,7 +93,7 @@ constexpr int kNumVariants = EGG_B200_NUM_VARIANTS;
 // Host threads that copy X between the caller's buffer and pinned staging.
 constexpr int kMaxCopyThreads = 16;
 constexpr Variant kVar64[kNumVariants] = {{8, 16, 1, 5, 1}, {8, 16, 1, 4}, {8, 16, 1, 5}, {8, 16, 1, 6}, {8, 16, 1, 4, 1}};
-constexpr Variant kVar32[kNumVariants] = {{8, 16, 1, 6, 1}, {8, 16, 1, 6}, {8, 16, 1, 8}, {8, 16, 1, 7, 1}, {8, 16, 1, 7}};
+constexpr Variant kVar32[kNumVariants] = {{8, 16, 1, 5, 2}, {8, 16, 1, 6, 2}, {8, 16, 1, 7, 2}, {16, 16, 1, 3, 2}, {8, 16, 1, 7, 1}};
 constexpr Variant kVar3_64[kNumVariants] = {{4, 8, 8, 1}, {4, 8, 8, 2}, {2, 8, 16, 2}, {2, 8, 16, 3}, {2, 4, 16, 4}};
 constexpr Variant kVar3_32[kNumVariants] = {{4, 8, 8, 1}, {4, 8, 8, 2}, {2, 8, 16, 2}, {2, 8, 16, 3}, {2, 4, 16, 4}};
 
@@ -347,11 +350,25 @@ static bool rows_uniform(const double* W, int64_t rows, int width)
 // Opt the interior kernels into >48 KB of dynamic shared memory.
 template <int CI, int CJ, int FD, int KIND, class C> constexpr size_t tile_smem2()
 {
-    return sizeof(TileShared2<CI + FD, CJ + FD, C, KIND>);
+    if constexpr (FD == 2) {
+        return sizeof(TileSharedX2<CI, CJ>);
+    } else {
+        return sizeof(TileShared2<CI + FD, CJ + FD, C, KIND>);
+    }
 }
 
 template <int CI, int CJ, int MINB, class C, int FD> static void set_smem_attr()
 {
+    if constexpr (FD == 2) {
+        static_assert(std::is_same_v<C, float>, "the packed kernel is the mixed-precision path");
+        EGG_CK(cudaFuncSetAttribute(interior_x2_kernel<CI, CJ, MINB, kShape>,
+                                    cudaFuncAttributeMaxDynamicSharedMemorySize, int(sizeof(TileSharedX2<CI, CJ>))));
+        EGG_CK(cudaFuncSetAttribute(interior_x2_kernel<CI, CJ, MINB, kUntangle>,
+                                    cudaFuncAttributeMaxDynamicSharedMemorySize, int(sizeof(TileSharedX2<CI, CJ>))));
+        EGG_CK(cudaFuncSetAttribute(interior_x2_kernel<CI, CJ, MINB, kShapeSize>,
+                                    cudaFuncAttributeMaxDynamicSharedMemorySize, int(sizeof(TileSharedX2<CI, CJ>))));
+        return;
+    } else {
     EGG_CK(cudaFuncSetAttribute(interior_tile_kernel<CI, CJ, MINB, kShape, C, FD>,
                                 cudaFuncAttributeMaxDynamicSharedMemorySize, int(tile_smem2<CI, CJ, FD, kShape, C>())));
     EGG_CK(cudaFuncSetAttribute(interior_tile_kernel<CI, CJ, MINB, kUntangle, C, FD>,
@@ -360,6 +377,7 @@ template <int CI, int CJ, int MINB, class C, int FD> static void set_smem_attr()
     EGG_CK(cudaFuncSetAttribute(interior_tile_kernel<CI, CJ, MINB, kShapeSize, C, FD>,
                                 cudaFuncAttributeMaxDynamicSharedMemorySize,
                                 int(tile_smem2<CI, CJ, FD, kShapeSize, C>())));
+    }
 }
 
 static void configure_kernels(int prec, int dim)
@@ -1169,8 +1187,13 @@ static void launch_tile(Session& S, LevelData& L, const double* xin, double* xou
     auto* xo = reinterpret_cast<double2*>(xout);
     const auto* tv = reinterpret_cast<const double2*>(tau);
     S.timed(kKInterior, [&] {
-        interior_tile_kernel<CI, CJ, MINB, KIND, C, FD><<<unsigned(L.ntiles), CI * CJ, smem, S.stream>>>(
-          xi, xo, L.tiles_d.p, L.blocks_d.p, L.active_d.p, tv, delta, omega, reinterpret_cast<double2*>(gout));
+        if constexpr (FD == 2) {
+            interior_x2_kernel<CI, CJ, MINB, KIND><<<unsigned(L.ntiles), CI * CJ, smem, S.stream>>>(
+              xi, xo, L.tiles_d.p, L.blocks_d.p, L.active_d.p, tv, delta, omega, reinterpret_cast<double2*>(gout));
+        } else {
+            interior_tile_kernel<CI, CJ, MINB, KIND, C, FD><<<unsigned(L.ntiles), CI * CJ, smem, S.stream>>>(
+              xi, xo, L.tiles_d.p, L.blocks_d.p, L.active_d.p, tv, delta, omega, reinterpret_cast<double2*>(gout));
+        }
     });
 }
 
@@ -2703,9 +2726,16 @@ int egg_b200_newton_step(const double* grad, const double* hess, double* step)
 }
 
 namespace {
+// Buffers handed out (pointer -> size) and idle buffers kept for reuse
+// (size -> pointer).  Idle bytes are capped; release frees what would exceed
+// the cap, and trim frees every idle buffer.
+constexpr int64_t kPinnedIdleCap = int64_t(1) << 30;
+constexpr size_t kPinnedIdlePerSize = 2;
 struct PinnedPool {
     std::mutex m;
-    std::unordered_multimap<int64_t, void*> free;
+    std::unordered_map<void*, int64_t> out;
+    std::unordered_multimap<int64_t, void*> idle;
+    int64_t idle_bytes = 0;
 };
 PinnedPool& pinned_pool()
 {
@@ -2722,29 +2752,56 @@ int egg_b200_pinned_acquire(int64_t bytes, void** out)
         PinnedPool& P = pinned_pool();
         {
             std::lock_guard<std::mutex> lk(P.m);
-            const auto it = P.free.find(bytes);
-            if (it != P.free.end()) {
+            const auto it = P.idle.find(bytes);
+            if (it != P.idle.end()) {
                 *out = it->second;
-                P.free.erase(it);
+                P.idle.erase(it);
+                P.idle_bytes -= bytes;
+                P.out.emplace(*out, bytes);
                 return;
             }
         }
         EGG_CK(cudaHostAlloc(out, size_t(bytes), cudaHostAllocPortable));
+        std::lock_guard<std::mutex> lk(P.m);
+        P.out.emplace(*out, bytes);
     });
 }
 
-void egg_b200_pinned_release(void* p, int64_t bytes)
+int egg_b200_pinned_release(void* p)
 {
-    if (!p) { return; }
-    PinnedPool& P = pinned_pool();
-    {
-        std::lock_guard<std::mutex> lk(P.m);
-        if (P.free.count(bytes) < 4) {
-            P.free.emplace(bytes, p);
-            return;
+    return guarded([&] {
+        if (!p) { return; }
+        PinnedPool& P = pinned_pool();
+        {
+            std::lock_guard<std::mutex> lk(P.m);
+            const auto it = P.out.find(p);
+            if (it == P.out.end()) { invalid("pinned_release: pointer did not come from pinned_acquire"); }
+            const int64_t bytes = it->second;
+            P.out.erase(it);
+            if (P.idle.count(bytes) < kPinnedIdlePerSize && P.idle_bytes + bytes <= kPinnedIdleCap) {
+                P.idle.emplace(bytes, p);
+                P.idle_bytes += bytes;
+                return;
+            }
         }
+        EGG_CK(cudaFreeHost(p));
+    });
+}
+
+int64_t egg_b200_pinned_trim(void)
+{
+    std::vector<void*> drop;
+    int64_t freed = 0;
+    {
+        PinnedPool& P = pinned_pool();
+        std::lock_guard<std::mutex> lk(P.m);
+        for (const auto& kv : P.idle) { drop.push_back(kv.second); }
+        freed = P.idle_bytes;
+        P.idle.clear();
+        P.idle_bytes = 0;
     }
-    cudaFreeHost(p);
+    for (void* p : drop) { cudaFreeHost(p); }
+    return freed;
 }
 
 }  // extern "C"

@@ -319,22 +319,30 @@ int egg_b200_session_energy(egg_b200_session* s, int32_t objective, double delta
  * or negative values fail with EGG_B200_EINVAL.  Every call on a device
  * shares the one array: calls whose GPU work overlaps (concurrent host
  * threads, or sessions on different streams) race on it.  Each call
- * returns only after its own result has reached the host.
+ * returns only after its own result has reached the host.  The first call
+ * on a device looks up the array's device address and keeps it for the
+ * process; after cudaDeviceReset that address is stale, so a process that
+ * resets a device must not call this entry point on it again.
  * No counterpart in the reference: it exists for callers that must not
  * allocate device memory per call. */
 #define EGG_B200_NOALLOC_MAX_PARTIALS 4096
 int egg_b200_session_energy_noalloc(egg_b200_session* s, int32_t objective, double delta,
                                     int32_t n_partials, double* energy, double* mindet);
 
-/* Download the resident positions in GLOBAL node order ([num_nodes*dim]).
- * Replaces CppStructuredSweepSession::get_X (src/bindings.cpp:1359-1376). */
 /* Page-locked host buffers from a process-wide pool (no counterpart in the
  * reference).  get_X into such a buffer is one DMA, with no staging copy.
- * release returns the buffer to the pool, which keeps up to four buffers
- * per size and frees the rest.  acquire returns EGG_B200_ERUNTIME when the
- * page-lock fails; the caller then uses ordinary memory. */
+ * acquire returns EGG_B200_ERUNTIME when the page-lock fails; the caller
+ * then uses ordinary memory.  release takes a pointer that acquire returned
+ * (anything else fails with EGG_B200_EINVAL) and returns it to the pool; the
+ * pool keeps at most two idle buffers per size and 1 GiB of idle buffers in
+ * all, and frees the rest.  trim frees every idle buffer and returns the
+ * bytes it freed. */
 int egg_b200_pinned_acquire(int64_t bytes, void** out);
-void egg_b200_pinned_release(void* p, int64_t bytes);
+int egg_b200_pinned_release(void* p);
+int64_t egg_b200_pinned_trim(void);
+
+/* Download the resident positions in GLOBAL node order ([num_nodes*dim]).
+ * Replaces CppStructuredSweepSession::get_X (src/bindings.cpp:1359-1376). */
 int egg_b200_session_get_X(egg_b200_session* s, double* X, int64_t len);
 
 /* Upload positions in global node order, scattered into every copy.

@@ -4,10 +4,14 @@
 # SYCL / mdspan shims in oracle/shim/.  Outputs go to oracle/_ref/ only:
 #   oracle/_ref/fp64/cpp_core<EXT>   (egg::real = double)
 #   oracle/_ref/fp32/cpp_core<EXT>   (egg::real = float, -DEGG_REAL_IS_FP32=1)
-# Usage: oracle/build_ref.sh [REFERENCE_ROOT]   (default: /root/reference)
+# Usage: oracle/build_ref.sh REFERENCE_ROOT   (or set EGG_REFERENCE_ROOT)
 set -euo pipefail
 HERE="$(cd "$(dirname "${BASH_SOURCE[0]}")" && pwd)"
-REF="${1:-/root/reference}"
+REF="${1:-${EGG_REFERENCE_ROOT:-}}"
+if [ -z "$REF" ]; then
+  echo "usage: build_ref.sh REFERENCE_ROOT (or set EGG_REFERENCE_ROOT)" >&2
+  exit 2
+fi
 if [ ! -f "$REF/src/bindings.cpp" ]; then
   echo "build_ref.sh: reference sources not found under $REF" >&2
   exit 2

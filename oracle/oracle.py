@@ -18,6 +18,7 @@ from __future__ import annotations
 
 import ctypes as C
 import importlib.util
+import os
 import subprocess
 import sysconfig
 from pathlib import Path
@@ -242,6 +243,16 @@ def energy(X, stencil, *, phase="barrier", delta=0.0):
 
 def ref_path(precision: str = "fp64") -> Path:
     return HERE / "_ref" / precision / f"cpp_core{sysconfig.get_config_var('EXT_SUFFIX')}"
+
+
+def reference_root() -> Path | None:
+    """The reference checkout that the recipes read: ``$EGG_REFERENCE_ROOT``, or
+    a checkout named ``reference`` beside this repository.  None when neither
+    holds the reference's ``src/bindings.cpp`` (the GPU hosts never have it;
+    they use what was built here)."""
+    env = os.environ.get("EGG_REFERENCE_ROOT")
+    cand = Path(env) if env else HERE.parent.parent / "reference"
+    return cand if (cand / "src" / "bindings.cpp").exists() else None
 
 
 _ref_loaded: dict = {}

@@ -44,6 +44,17 @@ sys.path.insert(0, str(ROOT))
 _NUM = r"[+-]?(?:\d+\.?\d*|\.\d+)(?:[eE][+-]?\d+)?"
 
 
+def _ref_root() -> Path:
+    """The reference checkout to read (``$EGG_REFERENCE_ROOT`` or a sibling
+    ``reference/`` of this repository); the script needs it."""
+    from oracle import oracle
+
+    root = oracle.reference_root()
+    if root is None:
+        raise SystemExit("reference checkout not found: pass its path or set EGG_REFERENCE_ROOT")
+    return root
+
+
 def _blocks(text: str) -> list[str]:
     """Top-level ``{ ... }`` records of the kSamples initializer."""
     start = text.index("= {{") + 4
@@ -593,7 +604,7 @@ if __name__ == "__main__" and len(sys.argv) == 4 and sys.argv[1] == "--runs":
     raise SystemExit(0)
 
 if __name__ == "__main__" and len(sys.argv) in (2, 3) and sys.argv[1] == "--soft":
-    gen_reference_soft(Path(sys.argv[2]) if len(sys.argv) == 3 else Path("/root/reference"))
+    gen_reference_soft(Path(sys.argv[2]) if len(sys.argv) == 3 else _ref_root())
     raise SystemExit(0)
 
 if __name__ == "__main__" and len(sys.argv) == 2 and sys.argv[1] == "--constrained":
@@ -602,7 +613,7 @@ if __name__ == "__main__" and len(sys.argv) == 2 and sys.argv[1] == "--constrain
 
 if __name__ == "__main__":
     args = [a for a in sys.argv[1:] if not a.startswith("--")]
-    ref_root = Path(args[0]) if args else Path("/root/reference")
+    ref_root = Path(args[0]) if args else _ref_root()
     gen_reference_vectors(ref_root)
     gen_reference_runs()
     gen_reference_wire(ref_root)
