@@ -219,38 +219,45 @@ def _timed_run(torch, s, local, k):
     return ev0.elapsed_time(ev1) / 1e3, float(E[-1])
 
 
-def time_to_energy_tol(torch, cpp_core, local, sessions, sweeps, tol=1e-6, cpu=True):
-    """Time until the energy stays within tol (relative) of the fp64 energy
-    after `sweeps` sweeps.
+def time_to_energy_tol(torch, cpp_core, local, sessions, long_sweeps=2000, every=10, tol=1e-6, cpu=True):
+    """Time until the energy stays within tol (relative) of the converged fp64
+    energy.
 
-    `sessions` maps precision -> a session whose checkpoint holds the start
-    positions; each is traced with one report per sweep, then run(k) to the
-    first sweep k inside the band is timed on the device.  With cpu=True the
-    same is measured for the reference core (oracle/_ref, all host cores) on
-    a 1025^2 sample of the workload, whose band comes from a GPU fp64 trace of
-    that sample; the energy it reaches at k is reported beside its time.
+    The converged energy e* is the fp64 energy after `long_sweeps` sweeps (far
+    past the job's 200); `sessions` maps precision -> a session whose
+    checkpoint holds the start positions.  Each precision is traced to
+    `long_sweeps` with a report every `every` sweeps; k is the first report
+    after which the energy stays inside the band, and run(k) from the start is
+    then timed on the device.  The fp64 energy's change over the trace's last
+    quarter is reported beside e* (how converged e* itself is).  With cpu=True
+    the reference core (oracle/_ref, all host cores) runs the fp64 k on a
+    1025^2 sample of the workload whose band comes from the GPU fp64 trace of
+    that sample; its energy at k is reported beside its time.
     """
     from egg_b200 import configs
 
     def measure(ss):
         ss["fp64"].restore()
-        E64, _ = ss["fp64"].run(sweeps, report_every=1)
+        E64, _ = ss["fp64"].run(long_sweeps, report_every=every)
         e_star = float(E64[-1])
-        res = {"e_fp64_final": e_star, "sweeps_to_tol": {}, "seconds": {}}
+        q = len(E64) // 4
+        res = {"e_star_fp64": e_star, "long_sweeps": long_sweeps,
+               "fp64_change_last_quarter_rel": abs(float(E64[-1] - E64[-1 - q])) / abs(e_star),
+               "sweeps_to_tol": {}, "seconds": {}, "energy_at_k": {}}
         for prec, s in ss.items():
             if prec == "fp64":
                 E = E64
             else:
                 s.restore()
-                E, _ = s.run(sweeps, report_every=1)
+                E, _ = s.run(long_sweeps, report_every=every)
             k = _sweeps_to_tol(E, e_star, tol)
+            k = None if k is None else every * k
             res["sweeps_to_tol"][prec] = k
             if k is not None:
-                res["seconds"][prec], _e = _timed_run(torch, s, local, k)
+                res["seconds"][prec], res["energy_at_k"][prec] = _timed_run(torch, s, local, k)
         return res
 
-    out = {"tol_rel": tol, "sweeps": sweeps,
-           "square4097": measure(sessions)}
+    out = {"tol_rel": tol, "square4097": measure(sessions)}
     g = configs.unit_square(1025, frac=FRAC, seed=SEED)
     small = {}
     for prec in ("fp64", "mixed"):
@@ -264,17 +271,62 @@ def time_to_energy_tol(torch, cpp_core, local, sessions, sweeps, tol=1e-6, cpu=T
 
     ref = oracle.load_ref("fp64") if cpu else None
     k = r["sweeps_to_tol"].get("fp64")
-    if ref is not None and k is not None:
+    if ref is not None and k is not None and k <= 1000:
         os.environ.setdefault("OMP_NUM_THREADS", str(os.cpu_count()))
         rs = ref.CppStructuredSweepSession(g.wire(), g.structured(), g.X_flat(), device="cpu")
         t0 = time.perf_counter()
         E_ref, _ = rs.run(k)
         r["seconds"]["reference_cpu"] = time.perf_counter() - t0
         r["reference_cpu_energy_at_k"] = float(E_ref[-1])
-        r["reference_cpu_within_tol"] = bool(abs(float(E_ref[-1]) - r["e_fp64_final"])
-                                             <= tol * abs(r["e_fp64_final"]))
+        r["reference_cpu_within_tol"] = bool(abs(float(E_ref[-1]) - r["e_star_fp64"])
+                                             <= tol * abs(r["e_star_fp64"]))
         r["reference_cpu_cores"] = os.cpu_count()
     out["square1025"] = r
+    return out
+
+
+def _error_stats(X, E, M, Xr, Er, Mr, h):
+    """The north star's error figures of a result against an fp64 oracle."""
+    return {"max_dx_over_h": float(np.abs(np.asarray(X) - np.asarray(Xr)).max() / h),
+            "rel_energy": abs(float(E) - float(Er)) / abs(float(Er)),
+            "mindet": float(M), "mindet_oracle": float(Mr),
+            "same_untangle_status": bool((float(M) > 0) == (float(Mr) > 0))}
+
+
+def error_vs_fp64_oracle(g, sessions, sweeps, cpu=True, ref_sweeps=2):
+    """Errors of both GPU paths against fp64 oracles on the bench grid.
+
+    * reference_core: `ref_sweeps` sweeps from the start positions by the
+      reference core itself (oracle/_ref, fp64), against the same sweeps on
+      each GPU path;
+    * gpu_fp64: the mixed path after the job's `sweeps` sweeps against the
+      plain fp64 GPU path (pinned to the reference core on every parity case).
+    h is the grid's nominal spacing.
+    """
+    h = 1.0 / (int(round(np.sqrt(g.num_nodes))) - 1)
+    out = {"h": h}
+    runs = {}
+    for prec, s in sessions.items():
+        s.restore()
+        E, M = s.run(sweeps)
+        runs[prec] = (s.get_X(), float(E[-1]), float(M[-1]))
+    Xf, Ef, Mf = runs["fp64"]
+    Xm, Em, Mm = runs["mixed"]
+    out["gpu_fp64"] = {"sweeps": sweeps, "mixed": _error_stats(Xm, Em, Mm, Xf, Ef, Mf, h)}
+    if cpu:
+        from oracle import oracle
+
+        ref = oracle.load_ref("fp64")
+        if ref is not None:
+            os.environ.setdefault("OMP_NUM_THREADS", str(os.cpu_count()))
+            Xr, Er, Mr = ref.cpp_structured_sweep(g.wire(), g.structured(), g.X_flat(), ref_sweeps, device="cpu",
+                                                  phase="barrier", report_every=ref_sweeps)
+            res = {"sweeps": ref_sweeps, "cores": os.cpu_count()}
+            for prec, s in sessions.items():
+                s.restore()
+                E, M = s.run(ref_sweeps)
+                res[prec] = _error_stats(s.get_X(), E[-1], M[-1], Xr, Er[-1], Mr[-1], h)
+            out["reference_core"] = res
     return out
 
 
@@ -449,10 +501,11 @@ def main():
     e2e_value, e2e_dt = replica_throughput(dist, F * sweeps * args.steps, time.perf_counter() - t0,
                                            device=f"cuda:{local}")
 
-    tte = None
+    tte = err = None
     if ws == 1:
-        tte = time_to_energy_tol(torch, cpp_core, local, {p: results[p]["session"] for p in ("fp64", "mixed")},
-                                 sweeps, cpu=not args.no_cpu_baseline)
+        sess = {p: results[p]["session"] for p in ("fp64", "mixed")}
+        err = error_vs_fp64_oracle(g, sess, sweeps, cpu=not args.no_cpu_baseline)
+        tte = time_to_energy_tol(torch, cpp_core, local, sess, cpu=not args.no_cpu_baseline)
 
     # Roofline of the dominant kernel (interior sweep), from the live events.
     k_ms, k_n = mixed["stats"]["interior_sweep"]
@@ -491,6 +544,7 @@ def main():
                 "d2h_bytes_per_step": int(Xout.nbytes + 16)},
         "gpu_launches": int(mixed["launches"]),
         "clocks": mixed["clocks"],
+        "error_vs_fp64_oracle": err,
         "time_to_energy_tol": tte,
         "setup": setup,
     }

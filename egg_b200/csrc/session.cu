@@ -126,6 +126,9 @@ struct LevelData {
     DevBuf<Tile3> tiles3_d;  // 3D tiles of the current variant's shape
     int64_t ntiles = 0;
     int tile_ci = 0, tile_cj = 0, tile_ck = 0, tile_fd = 0;
+    // the coarsest FAS level of a mixed-precision session sweeps its
+    // interior with the fp64 kernels (tiles of the first fp64 variant)
+    bool fp64_tiles = false;
     int64_t n_stored = 0;
     DevBuf<int32_t> st_slot, st_gc, st_gn0, st_gn1, st_gn2, st_role;
     DevBuf<int64_t> st_off;
@@ -395,6 +398,8 @@ static void configure_kernels(int prec, int dim)
         set_smem_attr<kVar32[2].ci, kVar32[2].cj, kVar32[2].minb, float, kVar32[2].fd>();
         set_smem_attr<kVar32[3].ci, kVar32[3].cj, kVar32[3].minb, float, kVar32[3].fd>();
         set_smem_attr<kVar32[4].ci, kVar32[4].cj, kVar32[4].minb, float, kVar32[4].fd>();
+        // the coarsest FAS level of a mixed session runs the first fp64 variant
+        set_smem_attr<kVar64[0].ci, kVar64[0].cj, kVar64[0].minb, double, kVar64[0].fd>();
     }
 }
 
@@ -1212,6 +1217,16 @@ static void launch_interior(Session& S, LevelData& L, const double* xin, double*
                             double omega, double* gout = nullptr)
 {
     if (L.ntiles == 0) { return; }
+    if (L.fp64_tiles && S.prec != EGG_B200_PREC_FP64) {
+        if (S.dim == 3) {
+            launch_tile3<kVar3_64[0].ci, kVar3_64[0].cj, kVar3_64[0].ck, kVar3_64[0].minb, KIND, double>(
+              S, L, xin, xout, tau, delta, omega, gout);
+        } else {
+            launch_tile<kVar64[0].ci, kVar64[0].cj, kVar64[0].minb, KIND, double, kVar64[0].fd>(S, L, xin, xout, tau,
+                                                                                               delta, omega, gout);
+        }
+        return;
+    }
 #define EGG_V3(T, C, i) \
     launch_tile3<T[i].ci, T[i].cj, T[i].ck, T[i].minb, KIND, C>(S, L, xin, xout, tau, delta, omega, gout)
     if (S.dim == 3) {

@@ -595,6 +595,113 @@ def gen_reference_control(ref_root: Path) -> None:
     print(f"ref_control.npz: {len(out)} arrays")
 
 
+# ---------------------------------------------------------------------------
+# The benchmark configurations at their own sizes, run by the reference core
+# (fp64 build): C1 exactly, C3 at 1025^2 (untangle schedule, then shape+size),
+# C4 as the 7-block sphere-in-cube at 33^3 (untangle, FAS V(2,2), 4 levels),
+# C5 as 32 batched multi-block meshes.  Positions of the larger cases are kept
+# at every CONFIG_STRIDE-th node to keep the fixture small.
+# ---------------------------------------------------------------------------
+CONFIG_STRIDE = {"c3": 101, "c4": 47, "c5": 151}
+C3_SHAPE_SIZE_SWEEPS = 100
+C4_CYCLES = 4
+C5_MESHES = 32
+
+
+def _ref_untangle(make_session, X, mindet0, *, sweeps_per_delta=20, delta0_factor=2.0, shrink=0.8, max_outer=60,
+                  margin=1e-9, omega=0.5):
+    """The delta-continuation schedule of egg/smoothing/cpp_backend.py:773-848
+    on a reference-core session; returns (session, per-step min det, deltas)."""
+    mds, deltas = [], []
+    if mindet0 > margin:
+        return None, mds, deltas
+    sess = make_session(X)
+    delta = delta0_factor * max(abs(mindet0), 1e-12)
+    for _ in range(max_outer):
+        _e, m = sess.run(sweeps_per_delta, phase="untangle", delta=delta, omega=omega)
+        mds.append(float(np.asarray(m)[-1]))
+        deltas.append(delta)
+        if mds[-1] > margin:
+            break
+        delta *= shrink
+    return sess, mds, deltas
+
+
+def _config_runs() -> dict:
+    import time
+
+    from egg_b200 import configs
+    from oracle import oracle
+
+    ref = oracle.load_ref("fp64")
+    if ref is None:
+        raise SystemExit("oracle/_ref/fp64 missing: run oracle/build_ref.sh first")
+    out = {}
+    t0 = time.perf_counter()
+    # C1: disk O-H 5 x 65^2, +-0.25h, shape, 40 sweeps
+    g = configs.disk_oh(65, frac=0.25, seed=0)
+    ctx, st = g.wire(), g.structured()
+    X1, e1, _ = ref.cpp_structured_sweep(ctx, st, g.X_flat(), 1, device="cpu", phase="barrier", report_every=1, dim=2)
+    Xn, E, M = ref.cpp_structured_sweep(ctx, st, g.X_flat(), 40, device="cpu", phase="barrier", report_every=1,
+                                        dim=2)
+    out.update({"c1/X1": X1, "c1/E1": e1, "c1/X40": Xn, "c1/E": E, "c1/M": M})
+    print(f"C1 {time.perf_counter() - t0:.1f}s", flush=True)
+    # C3: 1025^2, ~5% inverted: untangle schedule, then shape+size (mean-size target)
+    g = configs.tangled_square(1025, target=0.05, seed=0)
+    md0 = float(configs.grid_mindet(g.blocks, g.X).min())
+    sa, mds, deltas = _ref_untangle(
+        lambda X: ref.CppStructuredSweepSession(g.wire(), g.structured(), X, device="cpu"), g.X_flat(),
+        md0)
+    Xu = sa.get_X()
+    sb = ref.CppStructuredSweepSession(g.wire(w_inv=configs.mean_size_w_inv(g.blocks, g.X)),
+                                       g.structured(), Xu, device="cpu")
+    E, M = sb.run(C3_SHAPE_SIZE_SWEEPS, phase="shape_size", report_every=10)
+    k = CONFIG_STRIDE["c3"]
+    out.update({"c3/mindet0": np.array(md0), "c3/untangle_mindets": np.array(mds), "c3/deltas": np.array(deltas),
+                "c3/Xu": Xu.reshape(-1, 2)[::k].copy(), "c3/E": E, "c3/M": M,
+                "c3/X": sb.get_X().reshape(-1, 2)[::k].copy()})
+    print(f"C3 {time.perf_counter() - t0:.1f}s, {len(mds)} delta steps", flush=True)
+    # C4: 7-block sphere-in-cube 33^3, +-0.2h: untangle, then FAS V(2,2), 4 levels
+    g = configs.sphere_in_cube(33, frac=0.2, seed=0)
+    md0 = float(configs.grid_mindet(g.blocks, g.X, 3).min())
+
+    def make(X):
+        return ref.CppStructuredSweepSession(g.wire(), g.structured(), X, device="cpu", dim=3)
+
+    sa, mds, deltas = _ref_untangle(make, g.X_flat(), md0)
+    Xu = sa.get_X() if sa is not None else g.X_flat()
+    sf = make(Xu)
+    E, M = sf.run_fas(C4_CYCLES, nu_pre=2, nu_post=2, max_levels=4)
+    k = CONFIG_STRIDE["c4"]
+    lv = sf.mg_levels()
+    out.update({"c4/mindet0": np.array(md0), "c4/untangle_mindets": np.array(mds), "c4/deltas": np.array(deltas),
+                "c4/E": E, "c4/M": M, "c4/X": sf.get_X().reshape(-1, 3)[::k].copy(),
+                "c4/levels": np.array([[list(t) for t in x] for x in lv], dtype=np.int32).reshape(len(lv), -1)})
+    print(f"C4 {time.perf_counter() - t0:.1f}s, {len(mds)} delta steps", flush=True)
+    # C5: 32 multi-block meshes, 20 sweeps, each by its own reference session
+    Es, Ms, Xs = [], [], []
+    for gm in configs.batch_meshes(C5_MESHES, seed=0):
+        Xo, E, M = ref.cpp_structured_sweep(gm.wire(), gm.structured(), gm.X_flat(), 20, device="cpu",
+                                            phase="barrier", report_every=10, dim=2)
+        Es.append(E)
+        Ms.append(M)
+        Xs.append(Xo.reshape(-1, 2))
+    k = CONFIG_STRIDE["c5"]
+    out.update({"c5/E": np.array(Es), "c5/M": np.array(Ms), "c5/X": np.concatenate(Xs)[::k].copy()})
+    print(f"C5 {time.perf_counter() - t0:.1f}s", flush=True)
+    return out
+
+
+def gen_reference_configs() -> None:
+    out = _config_runs()
+    np.savez_compressed(HERE / "ref_configs.npz", **out)
+    print(f"ref_configs.npz: {len(out)} arrays")
+
+
+if __name__ == "__main__" and len(sys.argv) == 2 and sys.argv[1] == "--configs":
+    gen_reference_configs()
+    raise SystemExit(0)
+
 if __name__ == "__main__" and len(sys.argv) == 4 and sys.argv[1] == "--control":
     np.savez(sys.argv[3], **_control_runs(Path(sys.argv[2])))
     raise SystemExit(0)
@@ -620,3 +727,4 @@ if __name__ == "__main__":
     gen_reference_control(ref_root)
     gen_reference_constrained()
     gen_reference_soft(ref_root)
+    gen_reference_configs()
