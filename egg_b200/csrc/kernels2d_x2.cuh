@@ -9,11 +9,14 @@
 //            the rest, so an edge (hi_b - hi_a) + (lo_b - lo_a) is the fp64
 //            edge rounded once more -- no fp64 arithmetic or conversion per
 //            edge;
-//   phase 2  one thread per cell evaluates the cell's four samples as two
-//            lane pairs (samples 0|1 and 2|3 share their axis-0 edges) and
-//            stores the role contributions per corner, lane pairs (0,1) and
-//            (2,3), plus the sample dets and the forward edges of its base
-//            node for phase 3;
+//   phase 2  one thread per cell (the CTA has one thread per cell, rounded
+//            up to whole warps, so the cells take one round) evaluates the
+//            cell's four samples as two lane pairs (samples 0|1 and 2|3 share
+//            their axis-0 edges) and stores the role contributions per
+//            corner, the sample dets and the forward edges of its base node
+//            for phase 3 -- the corner values in a layout shifted by one cell
+//            (below) so that a DOF gathers each row of its cells with one
+//            64-bit load;
 //   phase 3  one thread per DOF sums its 4 corners, solves, and line-searches
 //            its 12 moving samples as 6 lane pairs (cells (ci, 0) | (ci, 1),
 //            same role), accepting on summed exact metric changes with the
@@ -35,12 +38,19 @@ template <int CI, int CJ> struct TileSharedX2 {
     static constexpr int NC = CH * CW;
     static constexpr int PW = CW + 1;                // window row length (nodes)
     static constexpr int NN = (CH + 1) * PW;         // window nodes
+    static constexpr int NT = (NC + 31) / 32 * 32;   // threads: one per cell, whole warps
     double2 P[NN];                                   // fp64 window
     float hx[NN], hy[NN], lx[NN], ly[NN];            // offsets from the first node, hi + lo
     float f0x[NN], f0y[NN], f1x[NN], f1y[NN];        // forward edges along axis 0 / axis 1
-    float2 g[2][5][NC];  // corner pairs (0,1), (2,3): gx, gy, hxx, hxy, hyy
-    float2 det[2][NC];   // sample dets (0,1), (2,3)
-    uint8_t bad[NC];
+    // Corner values of cell c, shifted: g[p][q][c] = (corner 2p+1 of cell c,
+    // corner 2p of cell c+1), q = gx, gy, hxx, hxy, hyy; a DOF whose cells
+    // are c00, c01 (row 0) and c10, c11 (row 1) takes corners 3 | 2 from
+    // g[1][q][c00] and 1 | 0 from g[0][q][c10].
+    float2 g[2][5][NC];
+    // Sample dets, shifted alike: det[p][c] = (sample 2p of cell c, sample
+    // 2p+1 of cell c+1); -inf for a cell with an inverted or badly shaped
+    // sample, which sends every DOF around it to the fp64 path.
+    float2 det[2][NC];
 };
 
 // hi = the fp64 value with its mantissa cut to 24 bits (exact in fp32), lo =
@@ -53,7 +63,7 @@ __device__ __forceinline__ void split_hl(double v, float& hi, float& lo)
 }
 
 template <int CI, int CJ, int MINB, int KIND>
-__global__ void __launch_bounds__(CI* CJ, MINB)
+__global__ void __launch_bounds__(TileSharedX2<CI, CJ>::NT, MINB)
   interior_x2_kernel(const double2* __restrict__ Xin, double2* __restrict__ Xout, const Tile2* __restrict__ tiles,
                      const BlockInfo* __restrict__ blocks, const uint8_t* __restrict__ active,
                      const double2* __restrict__ tau, double delta, double omega, double2* __restrict__ grad_out)
@@ -61,7 +71,7 @@ __global__ void __launch_bounds__(CI* CJ, MINB)
     using S = TileSharedX2<CI, CJ>;
     extern __shared__ __align__(16) unsigned char smem_raw[];
     S& sm = *reinterpret_cast<S*>(smem_raw);
-    constexpr int NT = CI * CJ;
+    constexpr int NT = S::NT;
     constexpr int CW = S::CW, NC = S::NC, PW = S::PW, NN = S::NN;
     const float fdelta = float(delta);
 
@@ -86,7 +96,8 @@ __global__ void __launch_bounds__(CI* CJ, MINB)
 
     // Phase 2: cells.  Samples b = 0..3 of a cell: axis-0 edge on side (b & 1),
     // axis-1 edge on side (b >> 1); signs s0 = -1 iff b & 2, s1 = -1 iff b & 1.
-    for (int cell = tid; cell < NC; cell += NT) {
+    if (tid < NC) {
+        const int cell = tid;
         const int ci = cell / CW, cj = cell % CW;
         const bool valid = (r0 + ci <= n0 - 2) && (c0 + cj <= n1 - 2);
         const int a = ci * PW + cj, b = a + 1, c = a + PW, d = c + 1;  // nodes 00, 01, 10, 11
@@ -113,22 +124,32 @@ __global__ void __launch_bounds__(CI* CJ, MINB)
             sm.f1x[c] = e1x.y;
             sm.f1y[c] = e1y.y;
         }
+        // shifted stores: lane y of pair p goes to slot cell (.x), lane x to
+        // slot cell - 1 (.y), which no DOF reads when cj = 0
+        float* gs = reinterpret_cast<float*>(&sm.g[0][0][0]);
+        float* ds = reinterpret_cast<float*>(&sm.det[0][0]);
+        auto put_g = [&](int p, int q, float2 v) {
+            gs[2 * ((p * 5 + q) * NC + cell)] = v.y;
+            if (cj > 0) { gs[2 * ((p * 5 + q) * NC + cell - 1) + 1] = v.x; }
+        };
+        auto put_det = [&](int p, float2 v) {
+            ds[2 * (p * NC + cell)] = v.x;
+            if (cj > 0) { ds[2 * (p * NC + cell - 1) + 1] = v.y; }
+        };
         if (!valid) {
 #pragma unroll
             for (int q = 0; q < 5; ++q) {
-                sm.g[0][q][cell] = p2(0.0f);
-                sm.g[1][q][cell] = p2(0.0f);
+                put_g(0, q, p2(0.0f));
+                put_g(1, q, p2(0.0f));
             }
-            sm.det[0][cell] = p2(1.0f);
-            sm.det[1][cell] = p2(1.0f);
-            sm.bad[cell] = 0;
-            continue;
-        }
+            put_det(0, p2(1.0f));
+            put_det(1, p2(1.0f));
+        } else {
         // corner c receives sample c in role 0, sample c^2 in role 1 and
         // sample c^1 in role 2.  Samples 0 | 1 first, folded at once into the
         // corner pairs 0 | 1 and 2 | 3 so that fewer values stay live.
         const float kb = float(kBadCell * kBadCell);
-        float2 G01[5], G23[5];
+        float2 G01[5], G23[5], D01, D23;
         bool bad;
         {
             Roles2 P;  // columns (axis-0 side 0 | 1, axis-1 side 0)
@@ -141,40 +162,48 @@ __global__ void __launch_bounds__(CI* CJ, MINB)
             // inverted or badly shaped sample (sine of a corner below kBadCell)
             const float2 bp = fma2(P.D, P.D, neg2(mul2(p2(kb), mul2(P.n0, P.n1))));
             bad = !(P.D.x > 0.0f) || !(P.D.y > 0.0f) || bp.x < 0.0f || bp.y < 0.0f;
-            sm.det[0][cell] = P.D;
+            D01 = P.D;
         }
         {
             Roles2 Q;  // samples 2 | 3: columns (axis-0 side 0 | 1, axis-1 side 1)
             roles2<KIND>(e0x, p2(e1x.y), e0y, p2(e1y.y), p2(-1.0f), make_float2(1.0f, -1.0f), fdelta, Q);
 #pragma unroll
             for (int q = 0; q < 5; ++q) {
-                sm.g[0][q][cell] = add2(G01[q], Q.r1[q]);
+                put_g(0, q, add2(G01[q], Q.r1[q]));
                 const float2 B = add2(G23[q], Q.r0[q]);
-                sm.g[1][q][cell] = make_float2(B.x + Q.r2[q].y, B.y + Q.r2[q].x);
+                put_g(1, q, make_float2(B.x + Q.r2[q].y, B.y + Q.r2[q].x));
             }
             const float2 bq = fma2(Q.D, Q.D, neg2(mul2(p2(kb), mul2(Q.n0, Q.n1))));
             bad = bad || !(Q.D.x > 0.0f) || !(Q.D.y > 0.0f) || bq.x < 0.0f || bq.y < 0.0f;
-            sm.det[1][cell] = Q.D;
+            D23 = Q.D;
         }
-        sm.bad[cell] = bad ? 1 : 0;
+        put_det(0, bad ? p2(-INFINITY) : D01);
+        put_det(1, bad ? p2(-INFINITY) : D23);
+        }
     }
     __syncthreads();
 
-    // Phase 3: one DOF per thread, at window node (ti + 1, tj + 1).
+    // Phase 3: one DOF per thread, at window node (ti + 1, tj + 1); the
+    // threads beyond the tile's DOFs are done.
+    if (tid >= CI * CJ) { return; }
     const int ti = tid / CJ, tj = tid % CJ;
     const int gi = tile.i0 + ti, gj = tile.j0 + tj;
     if (gi > n0 - 2 || gj > n1 - 2) { return; }
     const int64_t slot = bi.off + int64_t(gi) * n1 + gj;
     if (!active[slot]) { return; }
 
-    const int c00 = ti * CW + tj, c01 = c00 + 1, c10 = c00 + CW, c11 = c10 + 1;
+    const int c00 = ti * CW + tj, c10 = c00 + CW;
     double txd = 0.0, tyd = 0.0;
     if (tau != nullptr) {
         const double2 tv = tau[slot];
         txd = tv.x;
         tyd = tv.y;
     }
-    if (sm.bad[c00] | sm.bad[c01] | sm.bad[c10] | sm.bad[c11]) {
+    // min det of the four samples the DOF does not move (sample a^3 of the
+    // cell whose corner a it is); -inf flags a bad cell
+    const float2 d0 = sm.det[0][c00], d1 = sm.det[1][c10];
+    const float mdconst = fminf(fminf(d0.x, d0.y), fminf(d1.x, d1.y));
+    if (mdconst == -INFINITY) {
         if (grad_out != nullptr) {
             dof_update_fp64<KIND>(sm.P, PW, ti, tj, txd, tyd, delta, omega, grad_out + slot);
         } else {
@@ -186,10 +215,9 @@ __global__ void __launch_bounds__(CI* CJ, MINB)
     float gsum[5];
 #pragma unroll
     for (int q = 0; q < 5; ++q) {
-        gsum[q] = (sm.g[1][q][c00].y + sm.g[1][q][c01].x) + (sm.g[0][q][c10].y + sm.g[0][q][c11].x);
+        const float2 v = add2(sm.g[1][q][c00], sm.g[0][q][c10]);
+        gsum[q] = v.x + v.y;
     }
-    // min det of the four samples the DOF does not move (sample a^3 of each cell)
-    const float mdconst = fminf(fminf(sm.det[0][c00].x, sm.det[0][c01].y), fminf(sm.det[1][c10].x, sm.det[1][c11].y));
     const float tx = float(txd), ty = float(tyd);
     const float gv[2] = {gsum[0] - tx, gsum[1] - ty};
     if (grad_out != nullptr) {

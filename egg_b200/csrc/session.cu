@@ -93,7 +93,7 @@ constexpr int kNumVariants = EGG_B200_NUM_VARIANTS;
 // Host threads that copy X between the caller's buffer and pinned staging.
 constexpr int kMaxCopyThreads = 16;
 constexpr Variant kVar64[kNumVariants] = {{8, 16, 1, 5, 1}, {8, 16, 1, 4}, {8, 16, 1, 5}, {8, 16, 1, 6}, {8, 16, 1, 4, 1}};
-constexpr Variant kVar32[kNumVariants] = {{8, 16, 1, 5, 2}, {8, 16, 1, 6, 2}, {8, 16, 1, 7, 2}, {16, 16, 1, 3, 2}, {8, 16, 1, 7, 1}};
+constexpr Variant kVar32[kNumVariants] = {{8, 16, 1, 4, 2}, {8, 16, 1, 5, 2}, {8, 16, 1, 6, 2}, {16, 16, 1, 2, 2}, {8, 16, 1, 7, 1}};
 constexpr Variant kVar3_64[kNumVariants] = {{4, 8, 8, 1}, {4, 8, 8, 2}, {2, 8, 16, 2}, {2, 8, 16, 3}, {2, 4, 16, 4}};
 constexpr Variant kVar3_32[kNumVariants] = {{4, 8, 8, 1}, {4, 8, 8, 2}, {2, 8, 16, 2}, {2, 8, 16, 3}, {2, 4, 16, 4}};
 
@@ -1193,7 +1193,7 @@ static void launch_tile(Session& S, LevelData& L, const double* xin, double* xou
     const auto* tv = reinterpret_cast<const double2*>(tau);
     S.timed(kKInterior, [&] {
         if constexpr (FD == 2) {
-            interior_x2_kernel<CI, CJ, MINB, KIND><<<unsigned(L.ntiles), CI * CJ, smem, S.stream>>>(
+            interior_x2_kernel<CI, CJ, MINB, KIND><<<unsigned(L.ntiles), TileSharedX2<CI, CJ>::NT, smem, S.stream>>>(
               xi, xo, L.tiles_d.p, L.blocks_d.p, L.active_d.p, tv, delta, omega, reinterpret_cast<double2*>(gout));
         } else {
             interior_tile_kernel<CI, CJ, MINB, KIND, C, FD><<<unsigned(L.ntiles), CI * CJ, smem, S.stream>>>(
