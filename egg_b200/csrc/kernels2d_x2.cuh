@@ -33,13 +33,14 @@
 namespace egg_b200
 {
 
-template <int CI, int CJ> struct TileSharedX2 {
+template <int CI, int CJ, int NB = 1> struct TileSharedX2 {
     static constexpr int CH = CI + 1, CW = CJ + 1;  // cells staged
     static constexpr int NC = CH * CW;
     static constexpr int PW = CW + 1;                // window row length (nodes)
-    static constexpr int NN = (CH + 1) * PW;         // window nodes
+    static constexpr int PH = CH + 1;                // window rows
+    static constexpr int NN = PH * PW;               // window nodes
     static constexpr int NT = (NC + 31) / 32 * 32;   // threads: one per cell, whole warps
-    double2 P[NN];                                   // fp64 window
+    double2 P[NB][NN];                               // fp64 window(s)
     float hx[NN], hy[NN], lx[NN], ly[NN];            // offsets from the first node, hi + lo
     float f0x[NN], f0y[NN], f1x[NN], f1y[NN];        // forward edges along axis 0 / axis 1
     // Corner values of cell c, shifted: g[p][q][c] = (corner 2p+1 of cell c,
@@ -51,6 +52,7 @@ template <int CI, int CJ> struct TileSharedX2 {
     // 2p+1 of cell c+1); -inf for a cell with an inverted or badly shaped
     // sample, which sends every DOF around it to the fp64 path.
     float2 det[2][NC];
+    uint64_t bar[NB];  // window-copy completion (persistent kernel)
 };
 
 // hi = the fp64 value with its mantissa cut to 24 bits (exact in fp32), lo =
@@ -62,40 +64,13 @@ __device__ __forceinline__ void split_hl(double v, float& hi, float& lo)
     lo = __double2float_rn(v - h);
 }
 
-template <int CI, int CJ, int MINB, int KIND>
-__global__ void __launch_bounds__(TileSharedX2<CI, CJ>::NT, MINB)
-  interior_x2_kernel(const double2* __restrict__ Xin, double2* __restrict__ Xout, const Tile2* __restrict__ tiles,
-                     const BlockInfo* __restrict__ blocks, const uint8_t* __restrict__ active,
-                     const double2* __restrict__ tau, double delta, double omega, double2* __restrict__ grad_out)
+// Phase 2 of a tile: one thread per cell (threads 0 .. NC-1).  The cell
+// (ci, cj) has its base at window node (ci, cj); (r0, c0) is the window's
+// first node in the block, (n0, n1) the block's node counts.
+template <class S, int KIND>
+__device__ __forceinline__ void x2_cells(S& sm, int tid, int r0, int c0, int n0, int n1, float fdelta)
 {
-    using S = TileSharedX2<CI, CJ>;
-    extern __shared__ __align__(16) unsigned char smem_raw[];
-    S& sm = *reinterpret_cast<S*>(smem_raw);
-    constexpr int NT = S::NT;
-    constexpr int CW = S::CW, NC = S::NC, PW = S::PW, NN = S::NN;
-    const float fdelta = float(delta);
-
-    const Tile2 tile = tiles[blockIdx.x];
-    const BlockInfo bi = blocks[tile.block];
-    const int n0 = bi.n[0], n1 = bi.n[1];
-    const int r0 = tile.i0 - 1, c0 = tile.j0 - 1;  // window origin (always inside the block)
-    const int tid = threadIdx.x;
-
-    // Phase 1: window, fp64 and as fp32 offsets from its first node.
-    const double2 org = Xin[bi.off + int64_t(r0) * n1 + c0];
-    for (int k = tid; k < NN; k += NT) {
-        const int r = k / PW, c = k % PW;
-        const int gi = r0 + r, gj = c0 + c;
-        double2 v = org;  // outside the block: never part of a valid cell
-        if (gi < n0 && gj < n1) { v = Xin[bi.off + int64_t(gi) * n1 + gj]; }
-        sm.P[k] = v;
-        split_hl(v.x - org.x, sm.hx[k], sm.lx[k]);
-        split_hl(v.y - org.y, sm.hy[k], sm.ly[k]);
-    }
-    __syncthreads();
-
-    // Phase 2: cells.  Samples b = 0..3 of a cell: axis-0 edge on side (b & 1),
-    // axis-1 edge on side (b >> 1); signs s0 = -1 iff b & 2, s1 = -1 iff b & 1.
+    constexpr int CW = S::CW, NC = S::NC, PW = S::PW;
     if (tid < NC) {
         const int cell = tid;
         const int ci = cell / CW, cj = cell % CW;
@@ -181,33 +156,28 @@ __global__ void __launch_bounds__(TileSharedX2<CI, CJ>::NT, MINB)
         put_det(1, bad ? p2(-INFINITY) : D23);
         }
     }
-    __syncthreads();
+}
 
-    // Phase 3: one DOF per thread, at window node (ti + 1, tj + 1); the
-    // threads beyond the tile's DOFs are done.
-    if (tid >= CI * CJ) { return; }
-    const int ti = tid / CJ, tj = tid % CJ;
-    const int gi = tile.i0 + ti, gj = tile.j0 + tj;
-    if (gi > n0 - 2 || gj > n1 - 2) { return; }
-    const int64_t slot = bi.off + int64_t(gi) * n1 + gj;
-    if (!active[slot]) { return; }
-
+// Phase 3 of a tile: the DOF at window node (ti + 1, tj + 1), store slot
+// `slot`, from the tile's cell values and its fp64 window P; (txd, tyd) is
+// its FAS shift tau (zero outside FAS).  Writes Xout[slot], or the gradient
+// to grad_out[slot] in gradient-only mode.
+template <class S, int KIND>
+__device__ __forceinline__ void x2_dof(S& sm, const double2* __restrict__ P, int ti, int tj, int64_t slot,
+                                       double txd, double tyd, double delta, double omega, float fdelta,
+                                       double2* __restrict__ Xout, double2* __restrict__ grad_out)
+{
+    constexpr int CW = S::CW, PW = S::PW;
     const int c00 = ti * CW + tj, c10 = c00 + CW;
-    double txd = 0.0, tyd = 0.0;
-    if (tau != nullptr) {
-        const double2 tv = tau[slot];
-        txd = tv.x;
-        tyd = tv.y;
-    }
     // min det of the four samples the DOF does not move (sample a^3 of the
     // cell whose corner a it is); -inf flags a bad cell
     const float2 d0 = sm.det[0][c00], d1 = sm.det[1][c10];
     const float mdconst = fminf(fminf(d0.x, d0.y), fminf(d1.x, d1.y));
     if (mdconst == -INFINITY) {
         if (grad_out != nullptr) {
-            dof_update_fp64<KIND>(sm.P, PW, ti, tj, txd, tyd, delta, omega, grad_out + slot);
+            dof_update_fp64<KIND>(P, PW, ti, tj, txd, tyd, delta, omega, grad_out + slot);
         } else {
-            Xout[slot] = dof_update_fp64<KIND>(sm.P, PW, ti, tj, txd, tyd, delta, omega);
+            Xout[slot] = dof_update_fp64<KIND>(P, PW, ti, tj, txd, tyd, delta, omega);
         }
         return;
     }
@@ -324,9 +294,9 @@ __global__ void __launch_bounds__(TileSharedX2<CI, CJ>::NT, MINB)
             const int b = (r == 0) ? a : ((r == 1) ? (a ^ 2) : (a ^ 1));
             const int bn0 = b ^ 2, bn1 = b ^ 1;
             float dn;
-            dsum += dmu2_guard64<KIND>(sm.P[(ti + ci + (b >> 1)) * PW + (tj + cj + (b & 1))],
-                                       sm.P[(ti + ci + (bn0 >> 1)) * PW + (tj + cj + (bn0 & 1))],
-                                       sm.P[(ti + ci + (bn1 >> 1)) * PW + (tj + cj + (bn1 & 1))], r, double(dx),
+            dsum += dmu2_guard64<KIND>(P[(ti + ci + (b >> 1)) * PW + (tj + cj + (b & 1))],
+                                       P[(ti + ci + (bn0 >> 1)) * PW + (tj + cj + (bn0 & 1))],
+                                       P[(ti + ci + (bn1 >> 1)) * PW + (tj + cj + (bn1 & 1))], r, double(dx),
                                        double(dy), (b & 2) ? -1.0 : 1.0, (b & 1) ? -1.0 : 1.0, delta, dn);
             md = fminf(md, dn);
         }
@@ -339,12 +309,202 @@ __global__ void __launch_bounds__(TileSharedX2<CI, CJ>::NT, MINB)
             alpha *= 0.5f;
         }
     }
-    double2 out = sm.P[(ti + 1) * PW + (tj + 1)];
+    double2 out = P[(ti + 1) * PW + (tj + 1)];
     if (accepted) {
         out.x += omega * double(ax_acc);
         out.y += omega * double(ay_acc);
     }
     Xout[slot] = out;
+}
+
+// The tile's window: fp64 into P and, relative to its first node, the fp32
+// hi + lo planes (threads stride NT over the window nodes).
+template <class S>
+__device__ __forceinline__ void x2_planes(S& sm, const double2* P, int tid)
+{
+    const double2 org = P[0];
+    for (int k = tid; k < S::NN; k += S::NT) {
+        const double2 v = P[k];
+        split_hl(v.x - org.x, sm.hx[k], sm.lx[k]);
+        split_hl(v.y - org.y, sm.hy[k], sm.ly[k]);
+    }
+}
+
+template <int CI, int CJ, int MINB, int KIND>
+__global__ void __launch_bounds__(TileSharedX2<CI, CJ>::NT, MINB)
+  interior_x2_kernel(const double2* __restrict__ Xin, double2* __restrict__ Xout, const Tile2* __restrict__ tiles,
+                     const BlockInfo* __restrict__ blocks, const uint8_t* __restrict__ active,
+                     const double2* __restrict__ tau, double delta, double omega, double2* __restrict__ grad_out)
+{
+    using S = TileSharedX2<CI, CJ>;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    S& sm = *reinterpret_cast<S*>(smem_raw);
+    constexpr int NT = S::NT, PW = S::PW, NN = S::NN;
+    const float fdelta = float(delta);
+
+    const Tile2 tile = tiles[blockIdx.x];
+    const BlockInfo bi = blocks[tile.block];
+    const int n0 = bi.n[0], n1 = bi.n[1];
+    const int r0 = tile.i0 - 1, c0 = tile.j0 - 1;  // window origin (always inside the block)
+    const int tid = threadIdx.x;
+    // This thread's DOF, its active flag and tau, read up front so that their
+    // latency hides behind phases 1 and 2.
+    const int ti = tid / CJ, tj = tid % CJ;
+    const int gi = tile.i0 + ti, gj = tile.j0 + tj;
+    const int64_t slot = bi.off + int64_t(gi) * n1 + gj;
+    const bool mine = tid < CI * CJ && gi <= n0 - 2 && gj <= n1 - 2 && active[slot];
+    double2 tv = make_double2(0.0, 0.0);
+    if (mine && tau != nullptr) { tv = tau[slot]; }
+
+    // Phase 1: window, fp64 and as fp32 offsets from its first node.
+    const double2 org = Xin[bi.off + int64_t(r0) * n1 + c0];
+    for (int k = tid; k < NN; k += NT) {
+        const int r = k / PW, c = k % PW;
+        const int wi = r0 + r, wj = c0 + c;
+        double2 v = org;  // outside the block: never part of a valid cell
+        if (wi < n0 && wj < n1) { v = Xin[bi.off + int64_t(wi) * n1 + wj]; }
+        sm.P[0][k] = v;
+        split_hl(v.x - org.x, sm.hx[k], sm.lx[k]);
+        split_hl(v.y - org.y, sm.hy[k], sm.ly[k]);
+    }
+    __syncthreads();
+    x2_cells<S, KIND>(sm, tid, r0, c0, n0, n1, fdelta);
+    __syncthreads();
+    if (mine) { x2_dof<S, KIND>(sm, sm.P[0], ti, tj, slot, tv.x, tv.y, delta, omega, fdelta, Xout, grad_out); }
+}
+
+// ---------------------------------------------------------------------------
+// Persistent variant: each CTA walks the tile list with stride gridDim.x and
+// double-buffers the fp64 window.  While a tile is computed, the TMA engine
+// copies the next tile's window rows (cp.async.bulk, one per row, no tensor
+// map: rows are contiguous in the store) into the other buffer, completing on
+// that buffer's mbarrier.  Every wait is bounded: past kX2WaitLimit polls the
+// kernel sets *err, drains its copies in flight (bounded as well) and stops.
+// ---------------------------------------------------------------------------
+constexpr long long kX2WaitLimit = 1ll << 24;
+
+__device__ __forceinline__ uint32_t smem_addr(const void* p) { return uint32_t(__cvta_generic_to_shared(p)); }
+
+__device__ __forceinline__ void mbar_init(uint64_t* bar, uint32_t count)
+{
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_addr(bar)), "r"(count) : "memory");
+}
+
+__device__ __forceinline__ void mbar_expect_tx(uint64_t* bar, uint32_t bytes)
+{
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_addr(bar)), "r"(bytes)
+                 : "memory");
+}
+
+__device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t parity)
+{
+    uint32_t ok;
+    asm volatile(
+      "{\n\t.reg .pred p;\n\tmbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\tselp.u32 %0, 1, 0, p;\n\t}"
+      : "=r"(ok)
+      : "r"(smem_addr(bar)), "r"(parity)
+      : "memory");
+    return ok != 0;
+}
+
+// Polls until the phase with `parity` completes, at most kX2WaitLimit times.
+__device__ __forceinline__ bool mbar_wait_bounded(uint64_t* bar, uint32_t parity)
+{
+    for (long long it = 0; it < kX2WaitLimit; ++it) {
+        if (mbar_try_wait(bar, parity)) { return true; }
+    }
+    return false;
+}
+
+// One bulk copy global -> this CTA's shared memory, completing `bytes` on bar.
+__device__ __forceinline__ void bulk_copy_g2s(void* dst, const void* src, uint32_t bytes, uint64_t* bar)
+{
+    asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+                   smem_addr(dst)),
+                 "l"(src), "r"(bytes), "r"(smem_addr(bar))
+                 : "memory");
+}
+
+// Thread 0: the window rows of tile t into buffer b.  Rows and columns past
+// the block's last node are not copied (they feed only invalid cells).  Every
+// row starts on a node (16 bytes) and copies whole nodes, as the bulk copy
+// requires.
+template <class S>
+__device__ __forceinline__ void x2_issue_window(S& sm, int b, const double2* Xin, const Tile2* tiles,
+                                                const BlockInfo* blocks, int t)
+{
+    const Tile2 tile = tiles[t];
+    const BlockInfo bi = blocks[tile.block];
+    const int r0 = tile.i0 - 1, c0 = tile.j0 - 1;
+    const int rows = min(S::PH, bi.n[0] - r0), cols = min(S::PW, bi.n[1] - c0);
+    const uint32_t row_bytes = uint32_t(cols) * uint32_t(sizeof(double2));
+    // order this CTA's earlier generic reads of the buffer before the async writes
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+    mbar_expect_tx(&sm.bar[b], row_bytes * uint32_t(rows));
+    for (int r = 0; r < rows; ++r) {
+        bulk_copy_g2s(&sm.P[b][r * S::PW], Xin + bi.off + int64_t(r0 + r) * bi.n[1] + c0, row_bytes, &sm.bar[b]);
+    }
+}
+
+template <int CI, int CJ, int MINB, int KIND>
+__global__ void __launch_bounds__(TileSharedX2<CI, CJ, 2>::NT, MINB)
+  interior_x2p_kernel(const double2* __restrict__ Xin, double2* __restrict__ Xout, const Tile2* __restrict__ tiles,
+                      int ntiles, const BlockInfo* __restrict__ blocks, const uint8_t* __restrict__ active,
+                      const double2* __restrict__ tau, double delta, double omega, double2* __restrict__ grad_out,
+                      int* __restrict__ err)
+{
+    using S = TileSharedX2<CI, CJ, 2>;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    S& sm = *reinterpret_cast<S*>(smem_raw);
+    const float fdelta = float(delta);
+    const int tid = threadIdx.x;
+    const int ti = tid / CJ, tj = tid % CJ;
+
+    if (tid == 0) {
+        mbar_init(&sm.bar[0], 1);
+        mbar_init(&sm.bar[1], 1);
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    __syncthreads();
+    int t = blockIdx.x;
+    if (tid == 0 && t < ntiles) { x2_issue_window(sm, 0, Xin, tiles, blocks, t); }
+    bool ok = true;
+    int k = 0;
+    for (; t < ntiles; t += gridDim.x, ++k) {
+        const int b = k & 1;
+        // the other buffer was released by the barrier that ended the last tile
+        if (tid == 0 && t + int(gridDim.x) < ntiles) {
+            x2_issue_window(sm, b ^ 1, Xin, tiles, blocks, t + gridDim.x);
+        }
+        const Tile2 tile = tiles[t];
+        const BlockInfo bi = blocks[tile.block];
+        const int n0 = bi.n[0], n1 = bi.n[1];
+        const int gi = tile.i0 + ti, gj = tile.j0 + tj;
+        const int64_t slot = bi.off + int64_t(gi) * n1 + gj;
+        const bool mine = tid < CI * CJ && gi <= n0 - 2 && gj <= n1 - 2 && active[slot];
+        double2 tv = make_double2(0.0, 0.0);
+        if (mine && tau != nullptr) { tv = tau[slot]; }
+        const bool landed = mbar_wait_bounded(&sm.bar[b], uint32_t(k >> 1) & 1u);
+        if (landed) { x2_planes(sm, sm.P[b], tid); }
+        // one decision for the whole CTA (a thread whose wait ran out must not
+        // leave the others at a barrier)
+        if (!__syncthreads_and(landed)) {
+            ok = false;
+            break;
+        }
+        x2_cells<S, KIND>(sm, tid, tile.i0 - 1, tile.j0 - 1, n0, n1, fdelta);
+        __syncthreads();
+        if (mine) { x2_dof<S, KIND>(sm, sm.P[b], ti, tj, slot, tv.x, tv.y, delta, omega, fdelta, Xout, grad_out); }
+        __syncthreads();
+    }
+    if (!ok) {
+        // a window copy did not complete: flag it and wait (bounded) for the
+        // copies this CTA still has in flight before leaving
+        if (tid == 0) { atomicExch(err, 1); }
+        const int b = k & 1;
+        mbar_wait_bounded(&sm.bar[b], uint32_t(k >> 1) & 1u);
+        if (t + int(gridDim.x) < ntiles) { mbar_wait_bounded(&sm.bar[b ^ 1], uint32_t((k + 1) >> 1) & 1u); }
+    }
 }
 
 }  // namespace egg_b200

@@ -84,7 +84,8 @@ template <class T> struct DevBuf {
 // fastest (egg_b200_session_autotune).
 // 2D: (ci, cj) cells per CTA, or with fd = 1 (ci, cj) DOFs per CTA over the
 // (ci+1) x (cj+1) cells around them; fd = 2 is the same full-DOF tile on the
-// packed two-lane fp32 kernel (interior_x2_kernel, mixed precision only);
+// packed two-lane fp32 kernel (interior_x2_kernel, mixed precision only), fd
+// = 3 its persistent form with TMA window prefetch (interior_x2p_kernel);
 // 3D: (ci, cj, ck) DOFs per CTA.
 struct Variant {
     int ci, cj, ck, minb, fd = 0;
@@ -93,7 +94,7 @@ constexpr int kNumVariants = EGG_B200_NUM_VARIANTS;
 // Host threads that copy X between the caller's buffer and pinned staging.
 constexpr int kMaxCopyThreads = 16;
 constexpr Variant kVar64[kNumVariants] = {{8, 16, 1, 5, 1}, {8, 16, 1, 4}, {8, 16, 1, 5}, {8, 16, 1, 6}, {8, 16, 1, 4, 1}};
-constexpr Variant kVar32[kNumVariants] = {{8, 16, 1, 4, 2}, {8, 16, 1, 5, 2}, {8, 16, 1, 6, 2}, {16, 16, 1, 2, 2}, {8, 16, 1, 7, 1}};
+constexpr Variant kVar32[kNumVariants] = {{8, 16, 1, 6, 2}, {8, 16, 1, 5, 2}, {8, 16, 1, 6, 3}, {8, 16, 1, 5, 3}, {8, 16, 1, 4, 3}};
 constexpr Variant kVar3_64[kNumVariants] = {{4, 8, 8, 1}, {4, 8, 8, 2}, {2, 8, 16, 2}, {2, 8, 16, 3}, {2, 4, 16, 4}};
 constexpr Variant kVar3_32[kNumVariants] = {{4, 8, 8, 1}, {4, 8, 8, 2}, {2, 8, 16, 2}, {2, 8, 16, 3}, {2, 4, 16, 4}};
 
@@ -158,6 +159,10 @@ struct Session : LevelData {
     int dim = 2;
     int prec = EGG_B200_PREC_FP64;
     int device = 0;
+    int num_sms = 148;
+    // error flag of kernels with bounded waits (set on device, checked at sync)
+    DevBuf<int> kerr;
+    bool kerr_armed = false;
     cudaStream_t stream = nullptr;
     // side stream + fork/join events: the stored-patch sweep runs beside the
     // interior tiles (both read the frozen snapshot, write disjoint slots)
@@ -315,6 +320,20 @@ struct Session : LevelData {
     {
         EGG_CK(cudaStreamSynchronize(stream));
         harvest();
+        check_kerr();
+    }
+
+    // A kernel whose bounded wait ran out set kerr: report it once as an error.
+    void check_kerr()
+    {
+        if (!kerr_armed || kerr.p == nullptr) { return; }
+        kerr_armed = false;
+        int e = 0;
+        EGG_CK(cudaMemcpy(&e, kerr.p, sizeof(int), cudaMemcpyDeviceToHost));
+        if (e != 0) {
+            EGG_CK(cudaMemset(kerr.p, 0, sizeof(int)));
+            throw Error(EGG_B200_ERUNTIME, "interior sweep: a window copy did not complete within its wait limit");
+        }
     }
 
     double* X(int i) { return Xbuf[i].p; }
@@ -355,6 +374,8 @@ template <int CI, int CJ, int FD, int KIND, class C> constexpr size_t tile_smem2
 {
     if constexpr (FD == 2) {
         return sizeof(TileSharedX2<CI, CJ>);
+    } else if constexpr (FD == 3) {
+        return sizeof(TileSharedX2<CI, CJ, 2>);
     } else {
         return sizeof(TileShared2<CI + FD, CJ + FD, C, KIND>);
     }
@@ -362,7 +383,17 @@ template <int CI, int CJ, int FD, int KIND, class C> constexpr size_t tile_smem2
 
 template <int CI, int CJ, int MINB, class C, int FD> static void set_smem_attr()
 {
-    if constexpr (FD == 2) {
+    if constexpr (FD == 3) {
+        static_assert(std::is_same_v<C, float>, "the packed kernel is the mixed-precision path");
+        constexpr int sz = int(sizeof(TileSharedX2<CI, CJ, 2>));
+        EGG_CK(cudaFuncSetAttribute(interior_x2p_kernel<CI, CJ, MINB, kShape>,
+                                    cudaFuncAttributeMaxDynamicSharedMemorySize, sz));
+        EGG_CK(cudaFuncSetAttribute(interior_x2p_kernel<CI, CJ, MINB, kUntangle>,
+                                    cudaFuncAttributeMaxDynamicSharedMemorySize, sz));
+        EGG_CK(cudaFuncSetAttribute(interior_x2p_kernel<CI, CJ, MINB, kShapeSize>,
+                                    cudaFuncAttributeMaxDynamicSharedMemorySize, sz));
+        return;
+    } else if constexpr (FD == 2) {
         static_assert(std::is_same_v<C, float>, "the packed kernel is the mixed-precision path");
         EGG_CK(cudaFuncSetAttribute(interior_x2_kernel<CI, CJ, MINB, kShape>,
                                     cudaFuncAttributeMaxDynamicSharedMemorySize, int(sizeof(TileSharedX2<CI, CJ>))));
@@ -1088,6 +1119,8 @@ static Session* create_session(const egg_b200_session_desc& d)
     EGG_CK(cudaEventCreateWithFlags(&S->fork_ev, cudaEventDisableTiming));
     EGG_CK(cudaEventCreateWithFlags(&S->join_ev, cudaEventDisableTiming));
     configure_kernels(S->prec, S->dim);
+    EGG_CK(cudaDeviceGetAttribute(&S->num_sms, cudaDevAttrMultiProcessorCount, S->device));
+    S->kerr.upload(std::vector<int> {0});
 
     // ---- upload -----------------------------------------------------------
     S->es_W.upload(es_W_h);
@@ -1192,7 +1225,21 @@ static void launch_tile(Session& S, LevelData& L, const double* xin, double* xou
     auto* xo = reinterpret_cast<double2*>(xout);
     const auto* tv = reinterpret_cast<const double2*>(tau);
     S.timed(kKInterior, [&] {
-        if constexpr (FD == 2) {
+        if constexpr (FD == 3) {
+            // persistent: as many CTAs as fit on the device at once
+            static const int per_sm = [] {
+                int nb = 0;
+                EGG_CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(
+                  &nb, interior_x2p_kernel<CI, CJ, MINB, KIND>, TileSharedX2<CI, CJ, 2>::NT,
+                  sizeof(TileSharedX2<CI, CJ, 2>)));
+                return std::max(nb, 1);
+            }();
+            const int grid = int(std::min<int64_t>(L.ntiles, int64_t(per_sm) * S.num_sms));
+            interior_x2p_kernel<CI, CJ, MINB, KIND><<<unsigned(grid), TileSharedX2<CI, CJ, 2>::NT, smem, S.stream>>>(
+              xi, xo, L.tiles_d.p, int(L.ntiles), L.blocks_d.p, L.active_d.p, tv, delta, omega,
+              reinterpret_cast<double2*>(gout), S.kerr.p);
+            S.kerr_armed = true;
+        } else if constexpr (FD == 2) {
             interior_x2_kernel<CI, CJ, MINB, KIND><<<unsigned(L.ntiles), TileSharedX2<CI, CJ>::NT, smem, S.stream>>>(
               xi, xo, L.tiles_d.p, L.blocks_d.p, L.active_d.p, tv, delta, omega, reinterpret_cast<double2*>(gout));
         } else {
