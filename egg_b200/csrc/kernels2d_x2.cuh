@@ -9,8 +9,9 @@
 //            the rest, so an edge (hi_b - hi_a) + (lo_b - lo_a) is the fp64
 //            edge rounded once more -- no fp64 arithmetic or conversion per
 //            edge;
-//   phase 2  one thread per cell (the CTA has one thread per cell, rounded
-//            up to whole warps, so the cells take one round) evaluates the
+//   phase 2  one thread per cell (a second, partial round covers the cells
+//            beyond the CTA's CI x CJ threads; one thread per cell in whole
+//            warps measured slower, fewer CTAs fitting per SM) evaluates the
 //            cell's four samples as two lane pairs (samples 0|1 and 2|3 share
 //            their axis-0 edges) and stores the role contributions per
 //            corner, the sample dets and the forward edges of its base node
@@ -39,7 +40,7 @@ template <int CI, int CJ, int NB = 1> struct TileSharedX2 {
     static constexpr int PW = CW + 1;                // window row length (nodes)
     static constexpr int PH = CH + 1;                // window rows
     static constexpr int NN = PH * PW;               // window nodes
-    static constexpr int NT = (NC + 31) / 32 * 32;   // threads: one per cell, whole warps
+    static constexpr int NT = CI * CJ;                // threads: one per DOF
     double2 P[NB][NN];                               // fp64 window(s)
     float hx[NN], hy[NN], lx[NN], ly[NN];            // offsets from the first node, hi + lo
     float f0x[NN], f0y[NN], f1x[NN], f1y[NN];        // forward edges along axis 0 / axis 1
@@ -64,15 +65,14 @@ __device__ __forceinline__ void split_hl(double v, float& hi, float& lo)
     lo = __double2float_rn(v - h);
 }
 
-// Phase 2 of a tile: one thread per cell (threads 0 .. NC-1).  The cell
+// Phase 2 of a tile: thread t takes cells t, t + NT, ...  The cell
 // (ci, cj) has its base at window node (ci, cj); (r0, c0) is the window's
 // first node in the block, (n0, n1) the block's node counts.
 template <class S, int KIND>
 __device__ __forceinline__ void x2_cells(S& sm, int tid, int r0, int c0, int n0, int n1, float fdelta)
 {
     constexpr int CW = S::CW, NC = S::NC, PW = S::PW;
-    if (tid < NC) {
-        const int cell = tid;
+    for (int cell = tid; cell < NC; cell += S::NT) {
         const int ci = cell / CW, cj = cell % CW;
         const bool valid = (r0 + ci <= n0 - 2) && (c0 + cj <= n1 - 2);
         const int a = ci * PW + cj, b = a + 1, c = a + PW, d = c + 1;  // nodes 00, 01, 10, 11
@@ -158,6 +158,22 @@ __device__ __forceinline__ void x2_cells(S& sm, int tid, int r0, int c0, int n0,
     }
 }
 
+// The fp64 fallbacks, out of line: they run for few DOFs, and inlined their
+// fp64 temporaries would raise the register demand of the whole kernel.
+template <int KIND>
+__device__ __noinline__ double2 x2_dof_fp64(const double2* P, int PW, int ti, int tj, double tx, double ty,
+                                            double delta, double omega, double2* gout)
+{
+    return dof_update_fp64<KIND>(P, PW, ti, tj, tx, ty, delta, omega, gout);
+}
+
+template <int KIND>
+__device__ __noinline__ float x2_guard64(double2 qc, double2 q0, double2 q1, int role, double dx, double dy, double s0,
+                                         double s1, double delta, float& dn)
+{
+    return dmu2_guard64<KIND>(qc, q0, q1, role, dx, dy, s0, s1, delta, dn);
+}
+
 // Phase 3 of a tile: the DOF at window node (ti + 1, tj + 1), store slot
 // `slot`, from the tile's cell values and its fp64 window P; (txd, tyd) is
 // its FAS shift tau (zero outside FAS).  Writes Xout[slot], or the gradient
@@ -175,9 +191,9 @@ __device__ __forceinline__ void x2_dof(S& sm, const double2* __restrict__ P, int
     const float mdconst = fminf(fminf(d0.x, d0.y), fminf(d1.x, d1.y));
     if (mdconst == -INFINITY) {
         if (grad_out != nullptr) {
-            dof_update_fp64<KIND>(P, PW, ti, tj, txd, tyd, delta, omega, grad_out + slot);
+            x2_dof_fp64<KIND>(P, PW, ti, tj, txd, tyd, delta, omega, grad_out + slot);
         } else {
-            Xout[slot] = dof_update_fp64<KIND>(P, PW, ti, tj, txd, tyd, delta, omega);
+            Xout[slot] = x2_dof_fp64<KIND>(P, PW, ti, tj, txd, tyd, delta, omega, nullptr);
         }
         return;
     }
@@ -294,7 +310,7 @@ __device__ __forceinline__ void x2_dof(S& sm, const double2* __restrict__ P, int
             const int b = (r == 0) ? a : ((r == 1) ? (a ^ 2) : (a ^ 1));
             const int bn0 = b ^ 2, bn1 = b ^ 1;
             float dn;
-            dsum += dmu2_guard64<KIND>(P[(ti + ci + (b >> 1)) * PW + (tj + cj + (b & 1))],
+            dsum += x2_guard64<KIND>(P[(ti + ci + (b >> 1)) * PW + (tj + cj + (b & 1))],
                                        P[(ti + ci + (bn0 >> 1)) * PW + (tj + cj + (bn0 & 1))],
                                        P[(ti + ci + (bn1 >> 1)) * PW + (tj + cj + (bn1 & 1))], r, double(dx),
                                        double(dy), (b & 2) ? -1.0 : 1.0, (b & 1) ? -1.0 : 1.0, delta, dn);

@@ -94,7 +94,7 @@ constexpr int kNumVariants = EGG_B200_NUM_VARIANTS;
 // Host threads that copy X between the caller's buffer and pinned staging.
 constexpr int kMaxCopyThreads = 16;
 constexpr Variant kVar64[kNumVariants] = {{8, 16, 1, 5, 1}, {8, 16, 1, 4}, {8, 16, 1, 5}, {8, 16, 1, 6}, {8, 16, 1, 4, 1}};
-constexpr Variant kVar32[kNumVariants] = {{8, 16, 1, 6, 2}, {8, 16, 1, 5, 2}, {8, 16, 1, 6, 3}, {8, 16, 1, 5, 3}, {8, 16, 1, 4, 3}};
+constexpr Variant kVar32[kNumVariants] = {{8, 16, 1, 7, 2}, {8, 16, 1, 8, 2}, {8, 16, 1, 6, 2}, {8, 16, 1, 5, 2}, {8, 16, 1, 7, 3}};
 constexpr Variant kVar3_64[kNumVariants] = {{4, 8, 8, 1}, {4, 8, 8, 2}, {2, 8, 16, 2}, {2, 8, 16, 3}, {2, 4, 16, 4}};
 constexpr Variant kVar3_32[kNumVariants] = {{4, 8, 8, 1}, {4, 8, 8, 2}, {2, 8, 16, 2}, {2, 8, 16, 3}, {2, 4, 16, 4}};
 

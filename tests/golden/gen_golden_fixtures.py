@@ -702,6 +702,107 @@ if __name__ == "__main__" and len(sys.argv) == 2 and sys.argv[1] == "--configs":
     gen_reference_configs()
     raise SystemExit(0)
 
+# ---------------------------------------------------------------------------
+# The reference core's remaining free functions (src/bindings.cpp:1819-2100):
+# geometry_tangent on the closed-form curves, geometry_project_batch on one
+# entity row of every constrained test grid, energy_mindet on the golden
+# patches, directional_eval on seeded sample tables (2D and 3D).
+# ---------------------------------------------------------------------------
+FREE_BATCH_CASES = ["disk_arcs17", "disk_earcs17", "square_slide17", "square_bezier17", "square_bspline17",
+                    "square_composite17", "square_compbsp17", "cube_slide9", "cube_curved9", "disk_circle17",
+                    "disk_ellipse17"]
+
+
+def _entity_rows(g):
+    """(tag, record row, per-row seg list) of the first DOF of every entity
+    partition of a grid's wire, in the reference's single-row encoding."""
+    out = []
+    for name, ed in g.wire()["groups"][0]["entities"].items():
+        tag = int(ed["tag"])
+        if tag == 0:
+            continue
+        kf = int(ed["kFields"])
+        rec = np.asarray(ed["records"], dtype=np.float64).reshape(-1, kf)[0]
+        seg = []
+        for sd in ed.get("seg", []):
+            off = np.asarray(sd["off"])
+            seg.append({"data": np.asarray(sd["data"], dtype=np.float64)[off[0]:off[1]].copy(),
+                        "off": np.array([0, off[1] - off[0]], dtype=np.int32)})
+        out.append((name, tag, rec, seg))
+    return out
+
+
+def _free_runs() -> dict:
+    from egg_b200.wire import ENTITY_KINDS
+    from oracle import oracle
+
+    ref = oracle.load_ref("fp64")
+    if ref is None:
+        raise SystemExit("oracle/_ref/fp64 missing: run oracle/build_ref.sh first")
+    rng = np.random.default_rng(21)
+    out = {}
+    for tag, rec in ENTITY_RECORDS.items():
+        params = np.array(rec[: ENTITY_KINDS[tag][1]])
+        P = rng.uniform(-1.2, 1.4, size=(48, 2))
+        out[f"tangent/{tag}/params"] = params
+        out[f"tangent/{tag}/pos"] = P
+        out[f"tangent/{tag}/t"] = np.array([ref.geometry_tangent(P[i], tag, params) for i in range(len(P))])
+    k = 0
+    for case in FREE_BATCH_CASES:
+        g = case_grid(case)
+        lo, hi = g.X.min(axis=0), g.X.max(axis=0)
+        for name, tag, rec, seg in _entity_rows(g):
+            q = lo + (hi - lo) * rng.uniform(-0.1, 1.1, size=(40, g.d))
+            feet, basis = ref.geometry_project_batch(q, tag, rec, seg)
+            key = f"batch/{k}/"
+            out[key + "case"] = np.array(case)
+            out[key + "tag"] = np.array(tag)
+            out[key + "rec"] = rec
+            for j, sd in enumerate(seg):
+                out[key + f"seg{j}_data"] = sd["data"]
+                out[key + f"seg{j}_off"] = sd["off"]
+            out[key + "nseg"] = np.array(len(seg))
+            out[key + "q"] = q
+            out[key + "feet"] = np.asarray(feet)
+            out[key + "basis"] = np.asarray(basis)
+            k += 1
+    out["batch/count"] = np.array(k)
+    patches = json.loads((HERE / "golden_patch.json").read_text())["records"]
+    em = []
+    for r in patches:
+        P, n = int(r["P"]), int(r["n_nodes"])
+        em.append(ref.energy_mindet(np.array(r["X"][: 2 * n]), np.array(r["gc"][:P], dtype=np.int32),
+                                    np.array(r["gn0"][:P], dtype=np.int32), np.array(r["gn1"][:P], dtype=np.int32),
+                                    np.array(r["s0"][:P]), np.array(r["s1"][:P]), np.array(r["W_inv"][: 4 * P])))
+    out["energy_mindet"] = np.array(em)
+    for d in (2, 3):
+        nn, ns = 40, 60
+        X = rng.normal(size=(nn, d))
+        kind = rng.integers(0, 3, size=ns).astype(np.int32)
+        nodes = np.full((ns, 4), -1, dtype=np.int32)
+        for i in range(ns):
+            ar = 3 if kind[i] == 1 else 2
+            nodes[i, :ar] = rng.choice(nn, size=ar, replace=False)
+        refv = rng.normal(size=(ns, d))
+        refv /= np.linalg.norm(refv, axis=1, keepdims=True)
+        w = rng.uniform(0.1, 2.0, size=ns)
+        e, gr = ref.directional_eval(X, nodes, kind, refv, w, 1e-3)
+        key = f"dir{d}/"
+        out.update({key + "X": X, key + "nodes": nodes, key + "kind": kind, key + "ref": refv, key + "w": w,
+                    key + "e": np.array(e), key + "g": np.asarray(gr)})
+    return out
+
+
+def gen_reference_free() -> None:
+    out = _free_runs()
+    np.savez_compressed(HERE / "ref_free.npz", **out)
+    print(f"ref_free.npz: {len(out)} arrays")
+
+
+if __name__ == "__main__" and len(sys.argv) == 2 and sys.argv[1] == "--free":
+    gen_reference_free()
+    raise SystemExit(0)
+
 if __name__ == "__main__" and len(sys.argv) == 4 and sys.argv[1] == "--control":
     np.savez(sys.argv[3], **_control_runs(Path(sys.argv[2])))
     raise SystemExit(0)
@@ -728,3 +829,4 @@ if __name__ == "__main__":
     gen_reference_constrained()
     gen_reference_soft(ref_root)
     gen_reference_configs()
+    gen_reference_free()
