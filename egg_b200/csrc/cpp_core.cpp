@@ -1055,4 +1055,117 @@ PYBIND11_MODULE(cpp_core, m)
       },
       py::arg("pos"), py::arg("tag"), py::arg("params"),
       "Projection of pos onto a 2D curve entity (device evaluation). Returns foot(2,).");
+
+    // A 2D curve's record from its parameter blob, padded to the record width.
+    auto record_of = [](const DArr& params) {
+        std::vector<double> rec(EGG_B200_ENTITY_FIELDS, 0.0);
+        for (py::ssize_t i = 0; i < std::min<py::ssize_t>(params.size(), EGG_B200_ENTITY_FIELDS); ++i) {
+            rec[size_t(i)] = params.data()[i];
+        }
+        return rec;
+    };
+    m.def(
+      "geometry_project",
+      [record_of](const DArr& p, int tag, const DArr& params) {
+          if (p.size() != 2) { throw py::value_error("geometry_project: p(2) expected"); }
+          const std::vector<double> rec = record_of(params);
+          std::vector<double> foot(2), tang(2);
+          check(egg_b200_entity_frame(2, tag, rec.data(), nullptr, 0, p.data(), 1, foot.data(), tang.data()));
+          return vec(foot);
+      },
+      py::arg("p"), py::arg("tag"), py::arg("params"), "Project point onto entity (device evaluation). Returns proj(2,).");
+    m.def(
+      "geometry_tangent",
+      [record_of](const DArr& p, int tag, const DArr& params) {
+          if (p.size() != 2) { throw py::value_error("geometry_tangent: p(2) expected"); }
+          const std::vector<double> rec = record_of(params);
+          std::vector<double> foot(2), tang(2);
+          check(egg_b200_entity_frame(2, tag, rec.data(), nullptr, 0, p.data(), 1, foot.data(), tang.data()));
+          return vec(tang);
+      },
+      py::arg("p"), py::arg("tag"), py::arg("params"),
+      "Tangent direction at point on entity (device evaluation). Returns tang(2,).");
+    m.def(
+      "geometry_project_batch",
+      [](const py::array_t<double, py::array::c_style | py::array::forcecast>& q, int tag, const DArr& records,
+         const py::list& seg) {
+          if (q.ndim() != 2 || (q.shape(1) != 2 && q.shape(1) != 3)) {
+              throw std::invalid_argument("geometry_project_batch: q must be (n, 2) or (n, 3)");
+          }
+          const int d = int(q.shape(1));
+          const py::ssize_t n = q.shape(0);
+          // One wire row: its kFields reals, and the row's slice of each
+          // segmented field appended to an arena that the record addresses.
+          std::vector<double> rec(EGG_B200_ENTITY_FIELDS, 0.0), arena;
+          for (py::ssize_t i = 0; i < std::min<py::ssize_t>(records.size(), EGG_B200_ENTITY_FIELDS); ++i) {
+              rec[size_t(i)] = records.data()[i];
+          }
+          int k = 0;
+          for (auto item : seg) {
+              py::dict sd = item.cast<py::dict>();
+              DArr data = DArr::ensure(sd["data"]);
+              IArr off = IArr::ensure(sd["off"]);
+              if (!data || !off || off.size() < 2 || off.data()[0] < 0 || off.data()[1] > data.size() ||
+                  off.data()[0] > off.data()[1]) {
+                  throw std::invalid_argument("geometry_project_batch: seg slot " + std::to_string(k) + " is malformed");
+              }
+              const double base = double(arena.size());
+              if (tag == EGG_B200_TAG_BSPLINE && k < 3) { rec[size_t(6 + k)] = base; }
+              if (tag == EGG_B200_TAG_COMPOSITE && k == 0) { rec[6] = base; }
+              arena.insert(arena.end(), data.data() + off.data()[0], data.data() + off.data()[1]);
+              ++k;
+          }
+          const bool surf = d == 3 && (tag == EGG_B200_TAG_PLANE || tag == EGG_B200_TAG_SPHERE ||
+                                       tag == EGG_B200_TAG_CYLINDER);
+          const int K = surf ? 2 : 1;
+          py::array_t<double> feet({n, py::ssize_t(d)});
+          py::array_t<double> basis({n, py::ssize_t(d), py::ssize_t(K)});
+          check(egg_b200_entity_frame(d, tag, rec.data(), arena.empty() ? nullptr : arena.data(), int64_t(arena.size()),
+                                      q.data(), int64_t(n), feet.mutable_data(), basis.mutable_data()));
+          return std::make_tuple(feet, basis);
+      },
+      py::arg("q"), py::arg("tag"), py::arg("records"), py::arg("seg"),
+      "Batched projection onto ONE entity in its wire (SoA) encoding, on the device. q is (n, d), d in {2, 3}; "
+      "returns (feet(n, d), basis(n, d, tdim)): the projected points and the orthonormal tangent basis at each foot.");
+    m.def(
+      "energy_mindet",
+      [](const DArr& X, const IArr& gc, const IArr& gn0, const IArr& gn1, const DArr& s0, const DArr& s1,
+         const DArr& W) {
+          const int P = int(gc.size());
+          if (gn0.size() != P || gn1.size() != P || s0.size() != P || s1.size() != P || W.size() != 4 * P) {
+              throw py::value_error("energy_mindet: inconsistent patch array sizes");
+          }
+          // every occurrence in role -1: the patch's energy and min det A, no gradient
+          std::vector<int32_t> role(size_t(P), -1);
+          std::vector<double> g(2), h(4), st(2);
+          double e = 0, md = 0;
+          check(egg_b200_patch_eval(EGG_B200_OBJ_SHAPE, 0.0, X.data(), int64_t(X.size() / 2), P, gc.data(), gn0.data(),
+                                    gn1.data(), s0.data(), s1.data(), W.data(), role.data(), g.data(), h.data(), &e,
+                                    &md, st.data()));
+          return std::make_tuple(e, md);
+      },
+      py::arg("X"), py::arg("gc"), py::arg("gn0"), py::arg("gn1"), py::arg("s0"), py::arg("s1"), py::arg("W_inv"),
+      "Patch energy and min det A only, on the GPU. Returns (energy, mindet).");
+    m.def(
+      "directional_eval",
+      [](const py::array_t<double, py::array::c_style | py::array::forcecast>& X, const IArr& nodes, const IArr& kind,
+         const py::array_t<double, py::array::c_style | py::array::forcecast>& ref, const DArr& weight, double eps) {
+          if (X.ndim() != 2 || (X.shape(1) != 2 && X.shape(1) != 3)) {
+              throw py::value_error("directional_eval: X must be (n_nodes, 2) or (n_nodes, 3)");
+          }
+          const int d = int(X.shape(1));
+          const py::ssize_t n = weight.size();
+          auto nb = nodes.request();
+          if (nb.ndim != 2 || nb.shape[1] != 4 || nb.shape[0] != n || kind.size() != n || ref.ndim() != 2 ||
+              ref.shape(0) != n || ref.shape(1) != d) {
+              throw py::value_error("directional_eval: inconsistent sample-table shapes");
+          }
+          py::array_t<double> grad({X.shape(0), py::ssize_t(d)});
+          double e = 0.0;
+          check(egg_b200_directional_eval(d, X.data(), int64_t(X.shape(0)), int64_t(n), nodes.data(), kind.data(),
+                                          ref.data(), weight.data(), eps, &e, grad.mutable_data()));
+          return std::make_tuple(e, grad);
+      },
+      py::arg("X"), py::arg("nodes"), py::arg("kind"), py::arg("ref"), py::arg("weight"), py::arg("eps") = 1e-12,
+      "Directional soft-energy total and gradient over a sample table, on the GPU. Returns (energy, grad (n_nodes, d)).");
 }

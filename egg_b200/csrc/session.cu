@@ -1940,6 +1940,84 @@ __global__ void entity_step_kernel(int tag, const double* in, double* out)
     entity_project(tag, in, in[R + 6], in[R + 7], out[2], out[3]);
 }
 
+// Foot and orthonormal tangent basis of n points on one entity: 2D curves
+// (the unit tangent at the cold foot, as the sweep's cold path takes it), 3D
+// surfaces (two Gram-Schmidt columns of the raw frame at the foot) and lines
+// (one column).  basis is packed (point, component, column).
+__global__ void entity_frame_kernel(int dim, int tag, const double* __restrict__ e, const double* __restrict__ arena,
+                                    const double* __restrict__ q, int64_t n, double* __restrict__ foot,
+                                    double* __restrict__ basis)
+{
+    const int64_t i = blockIdx.x * int64_t(blockDim.x) + threadIdx.x;
+    if (i >= n) { return; }
+    if (dim == 2) {
+        const double px = q[2 * i], py = q[2 * i + 1];
+        double fx, fy, tx, ty;
+        if (tag == EGG_B200_TAG_COMPOSITE) {
+            const double* slice = arena + int64_t(e[6]);
+            composite_frame(slice, slice + int64_t(e[1]), int(e[0]), px, py, fx, fy, tx, ty);
+        } else if (tag == EGG_B200_TAG_BSPLINE) {
+            const BSplineCurve c = bspline_view(e, arena);
+            double t = bspline_foot(c, px, py, NAN);
+            if (!bspline_inside(c, t)) { t = bspline_clamp(c, t); }
+            bspline_point(c, t, 0, fx, fy);
+            double jx, jy;
+            bspline_point(c, t, 1, jx, jy);
+            unit_or_e0(jx, jy, tx, ty);
+        } else {
+            entity_project(tag, e, px, py, fx, fy);
+            entity_tangent(tag, e, px, py, tx, ty);
+        }
+        foot[2 * i] = fx;
+        foot[2 * i + 1] = fy;
+        basis[2 * i] = tx;
+        basis[2 * i + 1] = ty;
+        return;
+    }
+    const double* p = q + 3 * i;
+    entity3_project(tag, e, p, foot + 3 * i);
+    double B[2][3] = {{1.0, 0.0, 0.0}, {0.0, 1.0, 0.0}};
+    if (is_param3(tag)) {
+        double qq[2], J[2][3];
+        p3_invert(tag, e, p, qq);
+        p3_clamp(tag, e, qq);
+        p3_frame(tag, e, qq, J);
+        p3_basis(tag, J, B);
+    } else {  // rail: its direction
+        const double d[3] = {e[3] - e[0], e[4] - e[1], e[5] - e[2]};
+        const double norm = sqrt(dot3v(d, d));
+        if (!(norm < kGeomZnorm)) {
+            for (int k = 0; k < 3; ++k) { B[0][k] = d[k] / norm; }
+        }
+    }
+    const int K = is_surf3(tag) ? 2 : 1;
+    for (int k = 0; k < 3; ++k) {
+        for (int c = 0; c < K; ++c) { basis[(3 * i + k) * K + c] = B[c][k]; }
+    }
+}
+
+// Directional soft terms over a sample table: each thread one sample's
+// energy and its gradient on each of the sample's nodes (slot order); the
+// host sums them in table order.
+template <int D>
+__global__ void directional_eval_kernel(const double* __restrict__ X, const SoftTerm* __restrict__ terms, int64_t n,
+                                        double eps, double* __restrict__ energy, double* __restrict__ grad)
+{
+    const int64_t i = blockIdx.x * int64_t(blockDim.x) + threadIdx.x;
+    if (i >= n) { return; }
+    SoftTerm t = terms[i];
+    double p[4][3];
+    soft_load<D>(t, X, p);
+    energy[i] = soft_energy<D>(t, p, eps);
+    const int ar = soft_arity(t.kind);
+    for (int m = 0; m < ar; ++m) {
+        t.slot = m;
+        double g[D] = {}, H[D * D] = {}, e0 = 0.0;
+        soft_accumulate<D>(t, X, eps, g, H, e0);
+        for (int k = 0; k < D; ++k) { grad[(i * 4 + m) * D + k] = g[k]; }
+    }
+}
+
 template <class F> static int guarded(F&& f)
 {
     try {
@@ -2770,6 +2848,97 @@ int egg_b200_entity_step(int32_t tag, const double* record, const double* grad, 
         step[1] = o[1];
         foot[0] = o[2];
         foot[1] = o[3];
+    });
+}
+
+int egg_b200_entity_frame(int32_t dim, int32_t tag, const double* record, const double* arena, int64_t arena_len,
+                          const double* q, int64_t n, double* foot, double* basis)
+{
+    return guarded([&] {
+        if (dim != 2 && dim != 3) { invalid("entity_frame: dim must be 2 or 3"); }
+        if (!entity_supported(dim, tag) || tag == EGG_B200_TAG_FREE) {
+            invalid("entity_frame: tag " + std::to_string(tag) + " is not a projectable curve/surface entity in dimension " +
+                    std::to_string(dim));
+        }
+        if (!record || n < 0 || (n > 0 && (!q || !foot || !basis)) || arena_len < 0 || (arena_len > 0 && !arena)) {
+            invalid("entity_frame: bad arguments");
+        }
+        const bool segd = tag == EGG_B200_TAG_BSPLINE || tag == EGG_B200_TAG_COMPOSITE;
+        if (segd && arena_len == 0) { invalid("entity_frame: a B-spline or composite entity needs its arena"); }
+        if (n == 0) { return; }
+        const int K = (dim == 3 && (tag == EGG_B200_TAG_PLANE || tag == EGG_B200_TAG_SPHERE ||
+                                    tag == EGG_B200_TAG_CYLINDER)) ? 2 : 1;
+        DevBuf<double> de, da, dq, df, db;
+        de.upload(std::vector<double>(record, record + EGG_B200_ENTITY_FIELDS));
+        da.upload(arena_len ? std::vector<double>(arena, arena + arena_len) : std::vector<double> {0.0});
+        dq.upload(std::vector<double>(q, q + n * dim));
+        df.alloc(size_t(n * dim));
+        db.alloc(size_t(n * dim * K));
+        entity_frame_kernel<<<unsigned((n + 127) / 128), 128>>>(dim, tag, de.p, da.p, dq.p, n, df.p, db.p);
+        EGG_CK(cudaGetLastError());
+        EGG_CK(cudaMemcpy(foot, df.p, size_t(n * dim) * sizeof(double), cudaMemcpyDeviceToHost));
+        EGG_CK(cudaMemcpy(basis, db.p, size_t(n * dim * K) * sizeof(double), cudaMemcpyDeviceToHost));
+    });
+}
+
+int egg_b200_directional_eval(int32_t dim, const double* X, int64_t n_nodes, int64_t n, const int32_t* nodes,
+                              const int32_t* kind, const double* ref, const double* weight, double eps,
+                              double* energy, double* grad)
+{
+    return guarded([&] {
+        if (dim != 2 && dim != 3) { invalid("directional_eval: dim must be 2 or 3"); }
+        if (n < 0 || n_nodes < 0 || (n > 0 && (!X || !nodes || !kind || !ref || !weight)) || !energy ||
+            (n_nodes > 0 && !grad)) {
+            invalid("directional_eval: bad arguments");
+        }
+        std::vector<SoftTerm> terms(static_cast<size_t>(n));
+        for (int64_t i = 0; i < n; ++i) {
+            SoftTerm& t = terms[size_t(i)];
+            t.kind = kind[i];
+            const int ar = soft_arity(t.kind);
+            if (ar == 0 || t.kind == kSoftCurv) {
+                invalid("directional_eval: unsupported sample kind " + std::to_string(kind[i]));
+            }
+            for (int m = 0; m < 4; ++m) {
+                const int32_t v = nodes[i * 4 + m];
+                if (m < ar && (v < 0 || v >= n_nodes)) { invalid("directional_eval: node index out of range"); }
+                t.node[m] = m < ar ? v : -1;
+            }
+            t.slot = 0;
+            for (int k = 0; k < 3; ++k) { t.ref[k] = k < dim ? ref[i * dim + k] : 0.0; }
+            t.w = weight[i];
+        }
+        std::fill(grad, grad + n_nodes * dim, 0.0);
+        *energy = 0.0;
+        if (n == 0) { return; }
+        DevBuf<double> dX, de, dg;
+        DevBuf<SoftTerm> dt;
+        dX.upload(std::vector<double>(X, X + n_nodes * dim));
+        dt.upload(terms);
+        de.alloc(size_t(n));
+        dg.alloc(size_t(n) * 4 * dim);
+        const unsigned grid = unsigned((n + 127) / 128);
+        if (dim == 2) {
+            directional_eval_kernel<2><<<grid, 128>>>(dX.p, dt.p, n, eps, de.p, dg.p);
+        } else {
+            directional_eval_kernel<3><<<grid, 128>>>(dX.p, dt.p, n, eps, de.p, dg.p);
+        }
+        EGG_CK(cudaGetLastError());
+        std::vector<double> e(static_cast<size_t>(n)), g(static_cast<size_t>(n) * 4 * dim);
+        EGG_CK(cudaMemcpy(e.data(), de.p, e.size() * sizeof(double), cudaMemcpyDeviceToHost));
+        EGG_CK(cudaMemcpy(g.data(), dg.p, g.size() * sizeof(double), cudaMemcpyDeviceToHost));
+        // sums in table order, as the reference's host loop adds them
+        double et = 0.0;
+        for (int64_t i = 0; i < n; ++i) {
+            et += e[size_t(i)];
+            const int ar = soft_arity(terms[size_t(i)].kind);
+            for (int m = 0; m < ar; ++m) {
+                for (int k = 0; k < dim; ++k) {
+                    grad[int64_t(terms[size_t(i)].node[m]) * dim + k] += g[(size_t(i) * 4 + m) * dim + k];
+                }
+            }
+        }
+        *energy = et;
     });
 }
 

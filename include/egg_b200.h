@@ -436,6 +436,28 @@ int egg_b200_newton_step(const double* grad, const double* hess, double* step);
 int egg_b200_entity_step(int32_t tag, const double* record, const double* grad, const double* hess,
                          const double* pos, double* step, double* foot);
 
+/* Projection of n points onto one constrained-boundary entity, with the
+ * orthonormal tangent basis at each foot, evaluated on the device (the GPU
+ * twin of the reference's oracle bindings geometry_project_batch,
+ * src/bindings.cpp:1891-1990, and -- for a 2D curve and n = 1 --
+ * geometry_project / geometry_tangent, src/bindings.cpp:1859-1889).
+ * dim 2: a curve tag, basis [n*2] (the unit tangent at the foot); dim 3: a
+ * surface (Plane, Sphere, Cylinder: basis [n*3*2]) or a line (Line3,
+ * LineRail3: basis [n*3]), packed (point, component, column).  record holds
+ * EGG_B200_ENTITY_FIELDS reals as in entity_params; B-spline and composite
+ * records address `arena` by offset.  q [n*dim] -> foot [n*dim]. */
+int egg_b200_entity_frame(int32_t dim, int32_t tag, const double* record, const double* arena, int64_t arena_len,
+                          const double* q, int64_t n, double* foot, double* basis);
+
+/* Directional soft-term total and its gradient over a sample table,
+ * evaluated on the device (the GPU twin of the oracle binding
+ * directional_eval, src/bindings.cpp:1819-1857).  X [n_nodes*dim]; per
+ * sample nodes [4] (-1 pads), kind (parallel 0, line 1, stem 2), ref [dim],
+ * weight.  Out: energy, grad [n_nodes*dim]. */
+int egg_b200_directional_eval(int32_t dim, const double* X, int64_t n_nodes, int64_t n, const int32_t* nodes,
+                              const int32_t* kind, const double* ref, const double* weight, double eps,
+                              double* energy, double* grad);
+
 #ifdef __cplusplus
 }
 #endif

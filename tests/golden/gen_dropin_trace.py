@@ -1,0 +1,216 @@
+"""Record the reference's own Python drivers talking to a cpp_core module.
+
+The reference's smoothing drivers (``egg/smoothing/cpp_backend.py``:
+``CppStructuredSweepSession``, ``cpp_structured_sweep``, ``cpp_untangle``;
+``egg/pipeline.py:510-527`` ``_cpp_reduce``) reach the compiled core only
+through ``egg._cpp.cpp_core``.  This script runs them, unmodified, from the
+reference checkout with ``egg._cpp.cpp_core`` replaced by a recording proxy
+around the reference core built from source (``oracle/_ref/fp64``).  Every
+call that crosses the module boundary -- its arguments exactly as the driver
+built them, and the reference core's results -- goes to
+``tests/golden/ref_dropin.pkl.gz``.
+
+``tests/test_dropin_gpu.py`` replays that trace against ``egg_b200.cpp_core``
+on the GPU: the drop-in boundary is then exercised by the very calls the
+reference's drivers make, which the GPU host cannot generate itself (the
+reference's Python does not travel there).
+
+    python tests/golden/gen_dropin_trace.py [REFERENCE_ROOT]
+
+(default: ``$EGG_REFERENCE_ROOT`` or a ``reference`` checkout beside this
+repository).  Test infrastructure only.
+"""
+
+from __future__ import annotations
+
+import gzip
+import pickle
+import sys
+import types
+from pathlib import Path
+
+import numpy as np
+
+HERE = Path(__file__).resolve().parent
+ROOT = HERE.parent.parent
+sys.path.insert(0, str(ROOT))
+
+TRACE = HERE / "ref_dropin.pkl.gz"
+
+
+def _copy(v):
+    """Deep copy of an argument or result (numpy arrays, dicts, lists, tuples)."""
+    if isinstance(v, np.ndarray):
+        return v.copy()
+    if isinstance(v, dict):
+        return {k: _copy(x) for k, x in v.items()}
+    if isinstance(v, list):
+        return [_copy(x) for x in v]
+    if isinstance(v, tuple):
+        return tuple(_copy(x) for x in v)
+    if isinstance(v, (np.floating, np.integer)):
+        return v.item()
+    return v
+
+
+class Recorder:
+    """Builds the proxy module and collects the trace."""
+
+    def __init__(self, ref):
+        self.ref = ref
+        self.events: list[dict] = []
+        self.scenario = ""
+        self._next_sid = 0
+
+    def log(self, **ev):
+        ev["scenario"] = self.scenario
+        self.events.append(ev)
+
+    def module(self) -> types.ModuleType:
+        rec = self
+        ref = self.ref
+        mod = types.ModuleType("egg._cpp.cpp_core")
+        for name in dir(ref):
+            if name.startswith("_") or name == "CppStructuredSweepSession":
+                continue
+            obj = getattr(ref, name)
+            if callable(obj):
+
+                def fn(*args, _name=name, _obj=obj, **kwargs):
+                    out = _obj(*args, **kwargs)
+                    rec.log(op="fn", name=_name, args=_copy(args), kwargs=_copy(kwargs), result=_copy(out))
+                    return out
+
+                setattr(mod, name, fn)
+            else:
+                setattr(mod, name, obj)
+
+        class CppStructuredSweepSession:
+            def __init__(self, *args, **kwargs):
+                self._s = ref.CppStructuredSweepSession(*args, **kwargs)
+                self._sid = rec._next_sid
+                rec._next_sid += 1
+                rec.log(op="new", sid=self._sid, args=_copy(args), kwargs=_copy(kwargs))
+
+            def __getattr__(self, name):
+                attr = getattr(self._s, name)
+                if not callable(attr):
+                    return attr
+
+                def method(*args, **kwargs):
+                    out = attr(*args, **kwargs)
+                    rec.log(op="call", sid=self._sid, name=name, args=_copy(args), kwargs=_copy(kwargs),
+                            result=_copy(out))
+                    return out
+
+                return method
+
+        mod.CppStructuredSweepSession = CppStructuredSweepSession
+        return mod
+
+
+def _perturb(grid, seed: int, scale: float) -> np.ndarray:
+    """Seeded normal noise on the free nodes that carry no boundary
+    constraint, written back into the grid's global and per-block views."""
+    rng = np.random.default_rng(seed)
+    X = np.array(grid.global_nodes, dtype=np.float64)
+    free = np.asarray(grid.free_mask, dtype=bool)
+    movable = [i for i in range(X.shape[0]) if free[i] and i not in grid.dof_constraints]
+    X[movable] += rng.normal(0.0, scale, size=(len(movable), X.shape[1]))
+    grid.global_nodes = X
+    for bi, blk in enumerate(grid.blocks):
+        blk.nodes[...] = X[grid.block_dof_maps[bi]]
+    return X.copy()
+
+
+def record(ref_root: Path) -> list[dict]:
+    from oracle import oracle
+
+    ref = oracle.load_ref("fp64")
+    if ref is None:
+        raise SystemExit("oracle/_ref/fp64 missing: run oracle/build_ref.sh first")
+    sys.path.insert(0, str(ref_root))
+    sys.path.insert(0, str(ref_root / "examples" / "2D" / "circles"))
+    import egg._cpp  # noqa: F401  (the package only; its compiled module is the proxy)
+
+    rec = Recorder(ref)
+    proxy = rec.module()
+    sys.modules["egg._cpp.cpp_core"] = proxy
+    sys.modules["egg._cpp"].cpp_core = proxy
+
+    from topologies import build_circle_in_rectangle
+
+    from egg.pipeline import _cpp_reduce
+    from egg.smoothing.cpp_backend import (CppStructuredSweepSession, build_block_structured_context,
+                                           cpp_structured_sweep, cpp_untangle)
+    from egg.smoothing.solver import build_sweep_context
+    from egg.smoothing.targets import IdentityTarget
+    from egg.topology.builder import TopologyBuilder
+
+    # 1. The 12-block circle-in-rectangle O-grid (singular fans): the
+    #    one-shot structured sweep, reporting every 5 sweeps.
+    rec.scenario = "ogrid_sweep"
+    topo, _ = build_circle_in_rectangle(rough=False, R=1)
+    grid = topo.initialize_grid()
+    ctx = build_sweep_context(grid, IdentityTarget(d=topo.d))
+    X0 = _perturb(grid, seed=3, scale=0.01)
+    cpp_structured_sweep(ctx, grid, X0, 50, device="auto", report_every=5)
+
+    # 2. Two conforming blocks through the driver's session wrapper: sweeps,
+    #    shape+size, positions, FAS and its hierarchy.
+    rec.scenario = "lr_session"
+    b = TopologyBuilder(d=2)
+    for name, pos in [("A", (0.0, 0.0)), ("D", (0.0, 2.0)), ("B", (2.0, 0.0)), ("C", (2.0, 2.0)),
+                      ("E", (4.0, 0.0)), ("F", (4.0, 2.0))]:
+        b.add_corner(name, pos, fixed=True)
+    b.add_block("L", ("A", "D", "B", "C"), (16, 16))
+    b.add_block("R", ("B", "C", "E", "F"), (16, 16))
+    b.connect("L", 0, 1, "R", 0, 0)
+    grid = b.build().initialize_grid()
+    X0 = _perturb(grid, seed=5, scale=0.02)
+    ctx = build_sweep_context(grid, IdentityTarget(2))
+    s = CppStructuredSweepSession(ctx, build_block_structured_context(grid), X0, device="auto")
+    s.run(20, report_every=1)
+    s.run(10, phase="shape_size", omega=1.0, report_every=5)
+    s._session.get_X()
+    s.run_fas(3, omega=1.0)
+    s._session.mg_levels()
+    s._session.get_X()
+
+    # 3. The delta-continuation untangle driver on a mildly folded O-grid
+    #    (halfway between the valid and the rough initial grids).
+    rec.scenario = "untangle"
+    topo, _ = build_circle_in_rectangle(rough=True, R=3)
+    grid = topo.initialize_grid()
+    X_fold = grid.global_nodes.copy()
+    X_ok = build_circle_in_rectangle(rough=False, R=3)[0].initialize_grid().global_nodes.copy()
+    X0 = 0.5 * X_fold + 0.5 * X_ok
+    grid.global_nodes = X0
+    for bi, blk in enumerate(grid.blocks):
+        blk.nodes[...] = X0[grid.block_dof_maps[bi]]
+    ctx = build_sweep_context(grid, IdentityTarget(d=topo.d))
+    cpp_untangle(ctx, grid, X0.copy(), device="auto", sweeps_per_delta=40, max_outer=60, margin=1e-9, omega=0.5)
+
+    # 4. The pipeline's energy probe: one omega = 0 sweep as a reduction.
+    rec.scenario = "pipeline_probe"
+    topo, _ = build_circle_in_rectangle(rough=False, R=1)
+    grid = topo.initialize_grid()
+    ctx = build_sweep_context(grid, IdentityTarget(d=topo.d))
+    _cpp_reduce(grid, ctx, "auto")
+    _cpp_reduce(grid, ctx, "auto", phase="shape_size")
+    return rec.events
+
+
+if __name__ == "__main__":
+    from oracle import oracle
+
+    root = Path(sys.argv[1]) if len(sys.argv) > 1 else oracle.reference_root()
+    if root is None:
+        raise SystemExit("reference checkout not found: pass its path or set EGG_REFERENCE_ROOT")
+    events = record(root)
+    with gzip.open(TRACE, "wb") as f:
+        pickle.dump({"events": events}, f, protocol=4)
+    counts = {}
+    for ev in events:
+        counts[ev["scenario"]] = counts.get(ev["scenario"], 0) + 1
+    print(f"{TRACE.name}: {len(events)} calls {counts}")

@@ -33,8 +33,31 @@ def test_cpp_core_surface(core):
     assert core.REAL_IS_FLOAT in (True, False)
     for m in ("run", "run_fas", "mg_levels", "get_X", "run_control", "get_C", "set_C"):
         assert hasattr(core.CppStructuredSweepSession, m)
-    for f in ("cpp_structured_sweep", "metric_eval", "patch_eval", "newton_step"):
+    for f in ("cpp_structured_sweep", "metric_eval", "metric_eval_3d", "patch_eval", "newton_step", "energy_mindet",
+              "directional_eval", "geometry_project", "geometry_project_batch", "geometry_tangent"):
         assert hasattr(core, f)
+
+
+def test_cpp_core_covers_the_reference_module_surface(core):
+    """Every public name of the reference's cpp_core module (built from its
+    sources into oracle/_ref) exists here, with the same keyword names."""
+    import json
+    import subprocess
+    import sys
+
+    from oracle import oracle
+
+    if not oracle.ref_path("fp64").exists():
+        pytest.skip("oracle/_ref not built in this environment")
+    code = ("import json,sys,inspect; sys.path.insert(0, %r); from oracle import oracle; m = oracle.load_ref('fp64');"
+            "print(json.dumps({n: getattr(m, n).__doc__ or '' for n in dir(m) if not n.startswith('_')}))"
+            % str(oracle.HERE.parent))
+    out = subprocess.run([sys.executable, "-c", code], check=True, capture_output=True, text=True).stdout
+    ref = json.loads(out.strip().splitlines()[-1])
+    missing = [n for n in ref if not hasattr(core, n)]
+    assert not missing, missing
+    for cls in ("CppStructuredSweepSession",):
+        assert hasattr(core, cls)
 
 
 def _inputs(n=9):
