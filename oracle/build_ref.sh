@@ -4,6 +4,8 @@
 # SYCL / mdspan shims in oracle/shim/.  Outputs go to oracle/_ref/ only:
 #   oracle/_ref/fp64/cpp_core<EXT>   (egg::real = double)
 #   oracle/_ref/fp32/cpp_core<EXT>   (egg::real = float, -DEGG_REAL_IS_FP32=1)
+#   oracle/_ref/fp64snap/cpp_core<EXT> (fp64, parallel loops run serially with the
+#                                     shared-node refreshes before the ghost fills)
 # Usage: oracle/build_ref.sh REFERENCE_ROOT   (or set EGG_REFERENCE_ROOT)
 set -euo pipefail
 HERE="$(cd "$(dirname "${BASH_SOURCE[0]}")" && pwd)"
@@ -24,11 +26,15 @@ EXT="$($PY -c 'import sysconfig;print(sysconfig.get_config_var("EXT_SUFFIX"))')"
 # (AVX2/FMA) so the binary also runs on the GPU hosts' CPUs.
 FLAGS=(-std=c++23 -O3 -march=x86-64-v3 -ffp-contract=off -fopenmp -shared -fPIC -w
        -I"$HERE/shim" -I"$REF/src" -I"$PYINC" -I"$PBINC")
-mkdir -p "$HERE/_ref/fp64" "$HERE/_ref/fp32"
+mkdir -p "$HERE/_ref/fp64" "$HERE/_ref/fp32" "$HERE/_ref/fp64snap"
 g++ "${FLAGS[@]}" "$REF/src/bindings.cpp" -o "$HERE/_ref/fp64/cpp_core$EXT" &
 p1=$!
 g++ "${FLAGS[@]}" -DEGG_REAL_IS_FP32=1 "$REF/src/bindings.cpp" -o "$HERE/_ref/fp32/cpp_core$EXT" &
 p2=$!
+# serial, race-free ordering of the shim's parallel loops (see oracle/shim/sycl/sycl.hpp)
+g++ "${FLAGS[@]}" -DEGG_SHIM_SNAPSHOT=1 "$REF/src/bindings.cpp" -o "$HERE/_ref/fp64snap/cpp_core$EXT" &
+p3=$!
 wait $p1
 wait $p2
-echo "built $HERE/_ref/{fp64,fp32}/cpp_core$EXT"
+wait $p3
+echo "built $HERE/_ref/{fp64,fp32,fp64snap}/cpp_core$EXT"

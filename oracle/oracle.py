@@ -259,7 +259,10 @@ _ref_loaded: dict = {}
 
 
 def load_ref(precision: str = "fp64"):
-    """The reference core built from source (oracle/_ref), or None if absent.
+    """The reference core built from source (oracle/_ref), or None if absent:
+    "fp64", "fp32", or "fp64snap" (fp64 with the shim's parallel loops run
+    serially, shared-node refreshes before ghost fills: the race-free
+    ordering of the reference's halo launch).
 
     Only one precision can be loaded per process (both builds are extension
     modules named ``cpp_core``); asking for the other one raises."""

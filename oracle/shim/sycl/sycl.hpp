@@ -5,6 +5,7 @@
 //
 // Semantics kept from SYCL:
 //   * queue::parallel_for(range<1>, f(id<1>))         -> OpenMP static loop
+//     (with EGG_SHIM_SNAPSHOT: serial, last item first -- see parallel_for)
 //   * queue::parallel_for(range<1>, red..., f(id, r&...)) -> serial loop with
 //     reducers (deterministic order; the reference does not rely on any
 //     particular reduction order)
@@ -185,8 +186,20 @@ class queue
     template <class F> event parallel_for(range<1> r, F&& f)
     {
         const long long n = static_cast<long long>(r[0]);
+#ifdef EGG_SHIM_SNAPSHOT
+        // Serial, last item first.  The reference's fused ghost-fill +
+        // shared-node broadcast launch (src/structured_halo.hpp:215-236) puts
+        // the ghost copies first and the owner -> copy refreshes last; when a
+        // ghost's source is itself a non-owner copy, a parallel run races and
+        // its result depends on the thread count.  Running the refreshes
+        // before the ghost fills gives every ghost the refreshed value: the
+        // race-free snapshot that the launch's own comment describes.  Every
+        // other kernel writes disjoint slots, so its order does not matter.
+        for (long long i = n - 1; i >= 0; --i) { f(id<1>(static_cast<std::size_t>(i))); }
+#else
 #pragma omp parallel for schedule(static)
         for (long long i = 0; i < n; ++i) { f(id<1>(static_cast<std::size_t>(i))); }
+#endif
         return {};
     }
 

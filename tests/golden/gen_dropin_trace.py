@@ -5,7 +5,13 @@ The reference's smoothing drivers (``egg/smoothing/cpp_backend.py``:
 ``egg/pipeline.py:510-527`` ``_cpp_reduce``) reach the compiled core only
 through ``egg._cpp.cpp_core``.  This script runs them, unmodified, from the
 reference checkout with ``egg._cpp.cpp_core`` replaced by a recording proxy
-around the reference core built from source (``oracle/_ref/fp64``).  Every
+around the reference core built from source with its parallel loops run
+serially in the race-free order (``oracle/_ref/fp64snap``).  The plain OpenMP
+build is not a usable recorder here: on these multi-block grids the
+reference's fused ghost-fill + shared-node-refresh launch
+(``src/structured_halo.hpp:215-236``) reads non-owner copies while they are
+refreshed, and its positions after two sweeps on the O-grid differ by 2.2e-5
+between 8 threads and 1 or 2 threads.  Every
 call that crosses the module boundary -- its arguments exactly as the driver
 built them, and the reference core's results -- goes to
 ``tests/golden/ref_dropin.pkl.gz``.
@@ -126,9 +132,9 @@ def _perturb(grid, seed: int, scale: float) -> np.ndarray:
 def record(ref_root: Path) -> list[dict]:
     from oracle import oracle
 
-    ref = oracle.load_ref("fp64")
+    ref = oracle.load_ref("fp64snap")
     if ref is None:
-        raise SystemExit("oracle/_ref/fp64 missing: run oracle/build_ref.sh first")
+        raise SystemExit("oracle/_ref/fp64snap missing: run oracle/build_ref.sh first")
     sys.path.insert(0, str(ref_root))
     sys.path.insert(0, str(ref_root / "examples" / "2D" / "circles"))
     import egg._cpp  # noqa: F401  (the package only; its compiled module is the proxy)

@@ -115,3 +115,36 @@ def test_oracle3_matches_recorded_reference(run):
     Xn, E, M = oracle.run3(g.X, pt, sc, n, phase=phase, delta=delta, omega=omega, report_every=1)
     np.testing.assert_allclose(E, _REF[key + "/E"], rtol=1e-10)
     np.testing.assert_allclose(M, _REF[key + "/M"], rtol=1e-9, atol=1e-15)
+
+
+def _ref_sweep_energy(build: str, threads: int) -> float:
+    """Energy after two sweeps of the recorded O-grid call, by one reference
+    build in a fresh process (one cpp_core per process)."""
+    import os
+    import subprocess
+    import sys
+
+    code = (
+        "import gzip,pickle,sys; sys.path.insert(0, %r); from oracle import oracle;"
+        "ev=[e for e in pickle.load(gzip.open(%r))['events'] if e.get('name')=='cpp_structured_sweep'][0];"
+        "ctx,st,X=ev['args'][:3]; kw=dict(ev['kwargs']); kw.update(device='cpu', report_every=2);"
+        "print(repr(float(oracle.load_ref(%r).cpp_structured_sweep(ctx,st,X,2,**kw)[1][-1])))"
+        % (str(oracle.HERE.parent), str(oracle.HERE.parent / "tests" / "golden" / "ref_dropin.pkl.gz"), build))
+    env = dict(os.environ, OMP_NUM_THREADS=str(threads))
+    out = subprocess.run([sys.executable, "-c", code], check=True, capture_output=True, text=True, env=env).stdout
+    return float(out.strip().splitlines()[-1])
+
+
+def test_reference_halo_launch_order_matters_and_the_snapshot_build_is_fixed():
+    """On the reference's 12-block O-grid the order inside its fused
+    ghost-fill + shared-node-refresh launch changes the result: the serial
+    forward order (one OpenMP thread: ghost fills first, from non-owner copies
+    not yet refreshed) differs from the snapshot order (refreshes first),
+    which is the same for any thread count.  With several threads the OpenMP
+    build's result varies from run to run between the two."""
+    if not (oracle.ref_path("fp64").exists() and oracle.ref_path("fp64snap").exists()):
+        pytest.skip("oracle/_ref not built in this environment")
+    e1 = _ref_sweep_energy("fp64", 1)
+    s1, s8 = _ref_sweep_energy("fp64snap", 1), _ref_sweep_energy("fp64snap", 8)
+    assert s1 == s8
+    assert abs(s1 - e1) > 1e-7 * abs(s1)  # 7e-7 here; equivalent orderings agree to ~1e-15
