@@ -39,10 +39,15 @@ UNIT = "vertex-updates/s"
 # fp64 position once, write it once (neighbours are reused through shared
 # memory; structure is synthesized, not read).
 BYTES_PER_UPDATE = 2 * 2 * 8
-# DRAM bytes (read + write) per moving-DOF update of the mixed interior
-# kernel, from one ncu capture at 4097^2 (527.0 MB per launch over
-# 16,769,025 DOFs).  Traffic grows in proportion to the DOFs swept.
+# DRAM bytes (read + write) and thread instructions per moving-DOF update of
+# the mixed interior kernel (interior_x2_kernel<8,16,7>), from one ncu capture
+# of a 2049^2 launch (4,190,209 DOFs; the store exceeds L2): traffic and
+# instructions grow in proportion to the DOFs swept.
 DRAM_BYTES_PER_UPDATE = 527.0e6 / 16769025
+INSTR_PER_UPDATE = 1271.0
+# Issue roof: 148 SMs x 4 schedulers x 32 lanes, one warp instruction per
+# scheduler per cycle.
+ISSUE_LANES = 148 * 4 * 32
 
 
 def _peaks():
@@ -206,55 +211,60 @@ def _sweeps_to_tol(E, e_star, tol):
     return int(out[-1]) + 2 if len(out) else 1
 
 
-def _timed_run(torch, s, local, k):
-    """Device seconds of s.run(k) from the checkpoint, events on the session stream."""
-    stream = torch.cuda.ExternalStream(s.stream(), device=f"cuda:{local}")
-    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    s.restore()
-    torch.cuda.synchronize()
-    ev0.record(stream)
-    E, _ = s.run(k)
-    ev1.record(stream)
-    ev1.synchronize()
-    return ev0.elapsed_time(ev1) / 1e3, float(E[-1])
-
-
-def time_to_energy_tol(torch, cpp_core, local, sessions, long_sweeps=2000, every=10, tol=1e-6, cpu=True):
+def time_to_energy_tol(torch, cpp_core, local, sessions, tol=1e-6, fas_cycles=60, jacobi_sweeps=2000, every=10,
+                       cpu=True):
     """Time until the energy stays within tol (relative) of the converged fp64
-    energy.
+    energy, for block-Jacobi and for FAS V(2,2) cycles, both precisions.
 
-    The converged energy e* is the fp64 energy after `long_sweeps` sweeps (far
-    past the job's 200); `sessions` maps precision -> a session whose
-    checkpoint holds the start positions.  Each precision is traced to
-    `long_sweeps` with a report every `every` sweeps; k is the first report
-    after which the energy stays inside the band, and run(k) from the start is
-    then timed on the device.  The fp64 energy's change over the trace's last
-    quarter is reported beside e* (how converged e* itself is).  With cpu=True
-    the reference core (oracle/_ref, all host cores) runs the fp64 k on a
-    1025^2 sample of the workload whose band comes from the GPU fp64 trace of
-    that sample; its energy at k is reported beside its time.
+    The converged energy e* is the fp64 session's energy after `fas_cycles`
+    FAS V(2,2) cycles (the cycle-to-cycle change at the end is reported; the
+    Jacobi energy alone still moves by ~3e-5 relative over its last 500 of
+    2000 sweeps at 4097^2).  `sessions` maps precision -> a session whose
+    checkpoint holds the start positions.  Each solver is traced (Jacobi to
+    `jacobi_sweeps` with a report every `every` sweeps, FAS per cycle); k is
+    the first report after which the energy stays inside the band, and the
+    solver's k steps from the start are then timed on the device.  With
+    cpu=True the reference core (oracle/_ref, all host cores) times its FAS
+    to the same band on a 1025^2 sample of the workload.
     """
     from egg_b200 import configs
 
+    def fas(s, k):
+        return s.run_fas(k, nu_pre=2, nu_post=2)
+
+    def timed(s, fn, k):
+        stream = torch.cuda.ExternalStream(s.stream(), device=f"cuda:{local}")
+        ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        s.restore()
+        torch.cuda.synchronize()
+        ev0.record(stream)
+        E, _ = fn(s, k)
+        ev1.record(stream)
+        ev1.synchronize()
+        return ev0.elapsed_time(ev1) / 1e3, float(E[-1])
+
     def measure(ss):
         ss["fp64"].restore()
-        E64, _ = ss["fp64"].run(long_sweeps, report_every=every)
-        e_star = float(E64[-1])
-        q = len(E64) // 4
-        res = {"e_star_fp64": e_star, "long_sweeps": long_sweeps,
-               "fp64_change_last_quarter_rel": abs(float(E64[-1] - E64[-1 - q])) / abs(e_star),
-               "sweeps_to_tol": {}, "seconds": {}, "energy_at_k": {}}
+        Ef, _ = fas(ss["fp64"], fas_cycles)
+        e_star = float(Ef[-1])
+        res = {"e_star_fp64_fas": e_star, "fas_cycles": fas_cycles,
+               "fas_last_cycle_change_rel": abs(float(Ef[-1] - Ef[-2])) / abs(e_star),
+               "jacobi": {"sweeps_to_tol": {}, "seconds": {}, "rel_gap_at_end": {}},
+               "fas": {"cycles_to_tol": {}, "seconds": {}}}
         for prec, s in ss.items():
-            if prec == "fp64":
-                E = E64
-            else:
-                s.restore()
-                E, _ = s.run(long_sweeps, report_every=every)
+            s.restore()
+            E, _ = s.run(jacobi_sweeps, report_every=every)
             k = _sweeps_to_tol(E, e_star, tol)
-            k = None if k is None else every * k
-            res["sweeps_to_tol"][prec] = k
+            res["jacobi"]["rel_gap_at_end"][prec] = abs(float(E[-1]) - e_star) / abs(e_star)
+            res["jacobi"]["sweeps_to_tol"][prec] = None if k is None else every * k
             if k is not None:
-                res["seconds"][prec], res["energy_at_k"][prec] = _timed_run(torch, s, local, k)
+                res["jacobi"]["seconds"][prec] = timed(s, lambda t, n: t.run(n), every * k)[0]
+            s.restore()
+            E, _ = fas(s, fas_cycles)
+            k = _sweeps_to_tol(E, e_star, tol)
+            res["fas"]["cycles_to_tol"][prec] = k
+            if k is not None:
+                res["fas"]["seconds"][prec] = timed(s, fas, k)[0]
         return res
 
     out = {"tol_rel": tol, "square4097": measure(sessions)}
@@ -270,17 +280,17 @@ def time_to_energy_tol(torch, cpp_core, local, sessions, long_sweeps=2000, every
     from oracle import oracle
 
     ref = oracle.load_ref("fp64") if cpu else None
-    k = r["sweeps_to_tol"].get("fp64")
-    if ref is not None and k is not None and k <= 1000:
+    k = r["fas"]["cycles_to_tol"].get("fp64")
+    if ref is not None and k is not None:
         os.environ.setdefault("OMP_NUM_THREADS", str(os.cpu_count()))
         rs = ref.CppStructuredSweepSession(g.wire(), g.structured(), g.X_flat(), device="cpu")
         t0 = time.perf_counter()
-        E_ref, _ = rs.run(k)
-        r["seconds"]["reference_cpu"] = time.perf_counter() - t0
-        r["reference_cpu_energy_at_k"] = float(E_ref[-1])
-        r["reference_cpu_within_tol"] = bool(abs(float(E_ref[-1]) - r["e_star_fp64"])
-                                             <= tol * abs(r["e_star_fp64"]))
-        r["reference_cpu_cores"] = os.cpu_count()
+        E_ref, _ = rs.run_fas(k, nu_pre=2, nu_post=2)
+        r["fas"]["seconds"]["reference_cpu"] = time.perf_counter() - t0
+        r["fas"]["reference_cpu_energy_at_k"] = float(E_ref[-1])
+        r["fas"]["reference_cpu_within_tol"] = bool(abs(float(E_ref[-1]) - r["e_star_fp64_fas"])
+                                                    <= tol * abs(r["e_star_fp64_fas"]))
+        r["fas"]["reference_cpu_cores"] = os.cpu_count()
     out["square1025"] = r
     return out
 
@@ -514,10 +524,15 @@ def main():
     achieved = BYTES_PER_UPDATE * F / (avg_ms / 1e3) / 1e9
     roof = {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s", "frac": achieved / hbm,
             "traffic": DRAM_BYTES_PER_UPDATE * F, "traffic_unit": "bytes per launch (ncu dram read+write)",
-            "algorithmic_bytes": BYTES_PER_UPDATE * F, "kernel": "interior_tile_kernel (mixed)",
+            "algorithmic_bytes": BYTES_PER_UPDATE * F, "kernel": "interior_x2_kernel (mixed)",
             "avg_launch_ms": avg_ms, "peak_source": peak_kind,
-            "note": "issue-bound stencil (ncu: issue 66%, FMA 38%, ALU 23%, XU 15%, DRAM 5%); "
-                    "frac states HBM use, not the binding roof"}
+            "note": "frac states HBM use; the binding roof is instruction issue (see issue)"}
+    mhz = mixed["clocks"].get("sm_mhz") or 1965.0
+    upd_rate = F / (avg_ms / 1e3)
+    roof["issue"] = {"thread_instructions_per_update": INSTR_PER_UPDATE,
+                     "achieved": INSTR_PER_UPDATE * upd_rate, "peak": ISSUE_LANES * mhz * 1e6,
+                     "unit": "thread instructions/s", "frac": INSTR_PER_UPDATE * upd_rate / (ISSUE_LANES * mhz * 1e6),
+                     "sm_mhz": mhz, "source": "instructions per update from ncu (profiles/), rate from live events"}
     total_ms = sum(v[0] for v in mixed["stats"].values())
     share = {k: v[0] / total_ms for k, v in mixed["stats"].items() if v[1]}
 
