@@ -373,7 +373,8 @@ void fill_control(egg_b200_control_desc& c, Keep& keep, const py::dict& w, int d
 {
     if (w.contains("blocks")) {
         PyErr_SetString(PyExc_NotImplementedError,
-                        "egg_b200: multi-block control topologies (control['blocks']) are not supported");
+                        "egg_b200: a multi-block control topology (control['blocks']) attaches to one "
+                        "CppStructuredSweepSession; a batch takes one single-block net per mesh");
         throw py::error_already_set();
     }
     if (w.contains("walls") && py::len(w["walls"]) > 0) {
@@ -411,6 +412,91 @@ void fill_control(egg_b200_control_desc& c, Keep& keep, const py::dict& w, int d
     c.b = keep.reals(w["b"], &c.b_len);
 }
 
+// The reference's multi-block control wire (src/bindings.cpp:596-690
+// unpack_control_topo, built by egg/smoothing/control_backend.py
+// run_control_topo) -> egg_b200_control_topo_desc.  Per-block X0 (used only
+// by the sliding-wall frames) is checked for size and otherwise unused.
+struct TopoWire {
+    std::vector<egg_b200_control_desc> nets;
+    egg_b200_control_topo_desc d {};
+};
+
+void fill_control_topo(TopoWire& t, Keep& keep, const py::dict& w, int dim)
+{
+    if (w.contains("slide")) {
+        PyErr_SetString(PyExc_NotImplementedError,
+                        "egg_b200: sliding-wall control frames (control['slide']) are not supported");
+        throw py::error_already_set();
+    }
+    int64_t n_stack = 0;
+    for (const py::handle item : w["blocks"].cast<py::list>()) {
+        const py::dict bd = item.cast<py::dict>();
+        egg_b200_control_desc c {};
+        c.block = bd["block"].cast<int32_t>();
+        int64_t ncs = 0;
+        const int32_t* cs = keep.ints(bd["ctrl_shape"], &ncs);
+        if (ncs != dim) { throw py::value_error("control topo: ctrl_shape must have D entries"); }
+        int64_t n_ctrl = 1, n_nodes = 1;
+        for (int k = 0; k < dim; ++k) {
+            c.ctrl_shape[k] = cs[k];
+            if (cs[k] < 2) { throw py::value_error("control topo: each ctrl_shape entry must be >= 2"); }
+            n_ctrl *= cs[k];
+        }
+        c.k_supp = bd["k_supp"].cast<int32_t>();
+        if (c.k_supp < 1) { throw py::value_error("control topo: k_supp must be >= 1"); }
+        for (int k = 0; k < dim; ++k) {
+            const std::string ok = "off" + std::to_string(k), wk = "wt" + std::to_string(k);
+            int64_t nw = 0;
+            c.off[k] = keep.ints(bd[ok.c_str()], &c.off_len[k]);
+            c.wt[k] = keep.reals(bd[wk.c_str()], &nw);
+            if (nw != c.off_len[k] * int64_t(c.k_supp)) {
+                throw py::value_error("control topo: wt" + std::to_string(k) + " size != off size * k_supp");
+            }
+            for (int64_t i = 0; i < c.off_len[k]; ++i) {
+                if (c.off[k][i] < 0 || c.off[k][i] + c.k_supp > c.ctrl_shape[k]) {
+                    throw py::value_error("control topo: off" + std::to_string(k) +
+                                          " support window out of the control lattice");
+                }
+            }
+            n_nodes *= c.off_len[k];
+        }
+        c.b = keep.reals(bd["b"], &c.b_len);
+        if (c.b_len != n_nodes * dim) { throw py::value_error("control topo: b size != prod(node_shape) * D"); }
+        if (bd.contains("X0")) {
+            int64_t nx = 0;
+            keep.reals(bd["X0"], &nx);
+            if (nx != n_nodes * dim) { throw py::value_error("control topo: X0 size != prod(node_shape) * D"); }
+        }
+        n_stack += n_ctrl;
+        t.nets.push_back(c);
+    }
+    egg_b200_control_topo_desc& d = t.d;
+    d = egg_b200_control_topo_desc {};
+    d.n_nets = int32_t(t.nets.size());
+    d.nets = t.nets.data();
+    d.C0 = keep.reals(w["C0"], &d.C0_len);
+    if (d.C0_len != n_stack * dim) { throw py::value_error("control topo: C0 size != total controls * D"); }
+    d.nq = w["nq"].cast<int64_t>();
+    int64_t ncol = 0;
+    d.r_off = keep.ints(w["r_off"], &d.r_off_len);
+    d.r_col = keep.ints(w["r_col"], &ncol);
+    d.r_coef = keep.reals(w["r_coef"], &d.r_nnz);
+    if (d.r_off_len != n_stack * dim + 1 || ncol != d.r_nnz || d.r_off[d.r_off_len - 1] != ncol) {
+        throw py::value_error("control topo: malformed reduction CSR");
+    }
+    if (w.contains("p_off")) {
+        int64_t pcol = 0;
+        d.p_off = keep.ints(w["p_off"], &d.p_off_len);
+        d.p_col = keep.ints(w["p_col"], &pcol);
+        d.p_coef = keep.reals(w["p_coef"], &d.p_nnz);
+        d.p_w = keep.reals(w["p_w"], &d.p_w_len);
+        if (pcol != d.p_nnz || (d.p_off_len == 0 ? pcol != 0 : d.p_off[d.p_off_len - 1] != pcol) ||
+            (d.p_off_len != 0 && d.p_w_len != d.p_off_len - 1)) {
+            throw py::value_error("control topo: malformed penalty CSR");
+        }
+    }
+}
+
 py::dict control_report(int n_outer, const std::vector<double>& E, const std::vector<double>& M,
                         const std::vector<double>& A, const std::vector<double>& PI, const std::vector<double>& PR,
                         const int64_t* cnt, int32_t iters, int32_t conv)
@@ -442,7 +528,13 @@ class Session
         fill_desc(D, ctx, st, X, dim, parse_precision(precision), device_of(device));
         Keep ckeep;
         egg_b200_control_desc cdesc;
-        if (!control.is_none()) { fill_control(cdesc, ckeep, control.cast<py::dict>(), dim); }
+        TopoWire topo;
+        const bool is_topo = !control.is_none() && control.cast<py::dict>().contains("blocks");
+        if (is_topo) {
+            fill_control_topo(topo, ckeep, control.cast<py::dict>(), dim);
+        } else if (!control.is_none()) {
+            fill_control(cdesc, ckeep, control.cast<py::dict>(), dim);
+        }
         egg_b200_session* h = nullptr;
         {
             py::gil_scoped_release nogil;
@@ -455,7 +547,35 @@ class Session
         h_.reset(h);
         M_ = D.d.num_nodes;
         nblocks_ = D.d.num_blocks;
-        if (!control.is_none()) { check(egg_b200_session_attach_control(h_.get(), &cdesc)); }
+        if (is_topo) {
+            check(egg_b200_session_attach_control_topo(h_.get(), &topo.d));
+        } else if (!control.is_none()) {
+            check(egg_b200_session_attach_control(h_.get(), &cdesc));
+        }
+    }
+
+    void set_control_reduction(int64_t nq, const IArr& off, const IArr& col, const DArr& coef)
+    {
+        if (col.size() != coef.size()) { throw py::value_error("control topo: malformed reduction CSR"); }
+        check(egg_b200_session_set_control_reduction(h_.get(), nq, off.data(), int64_t(off.size()), col.data(),
+                                                     coef.data(), int64_t(coef.size())));
+    }
+
+    void set_control_penalty(const IArr& off, const IArr& col, const DArr& coef, const DArr& w)
+    {
+        if (col.size() != coef.size()) { throw py::value_error("control topo: malformed penalty CSR"); }
+        check(egg_b200_session_set_control_penalty(h_.get(), off.data(), int64_t(off.size()), col.data(), coef.data(),
+                                                   int64_t(coef.size()), w.data(), int64_t(w.size())));
+    }
+
+    void set_control_b(int block_index, const DArr& b)
+    {
+        int rc;
+        {
+            py::gil_scoped_release nogil;
+            rc = egg_b200_session_set_control_b(h_.get(), block_index, b.data(), int64_t(b.size()));
+        }
+        check(rc);
     }
 
     py::dict run_control(int n_outer, const std::string& phase, double grad_tol, double alpha_min, double lm0,
@@ -911,7 +1031,13 @@ PYBIND11_MODULE(cpp_core, m)
            py::arg("pcg_rtol") = 1e-10, py::arg("pcg_forcing") = true, py::arg("model_db") = true,
            "Damped reduced Gauss-Newton on the control net; returns the reference's report dict.")
       .def("get_C", &Session::get_C, "The resident control lattice, flat (n_ctrl * dim,).")
-      .def("set_C", &Session::set_C, py::arg("C"), "Upload a control lattice and evaluate X = M C + b.");
+      .def("set_C", &Session::set_C, py::arg("C"), "Upload a control lattice and evaluate X = M C + b.")
+      .def("set_control_reduction", &Session::set_control_reduction, py::arg("nq"), py::arg("off"), py::arg("col"),
+           py::arg("coef"), "Replace the multi-block reduction CSR dC = R dq.")
+      .def("set_control_penalty", &Session::set_control_penalty, py::arg("off"), py::arg("col"), py::arg("coef"),
+           py::arg("w"), "Replace the multi-block penalty rows (1/2 sum_j w_j (P_j C)^2); empty off removes them.")
+      .def("set_control_b", &Session::set_control_b, py::arg("block_index"), py::arg("b"),
+           "Replace one net's Boolean-sum offset b and re-evaluate X.");
 
     py::class_<Batch, Session>(m, "CppBatchSweepSession",
                                "Several independent meshes swept together in one device-resident session.")

@@ -6,6 +6,7 @@
 #include "kernels3d.cuh"
 #include "fas.cuh"
 #include "control.cuh"
+#include "control_topo.cuh"
 
 #include <algorithm>
 #include <array>
@@ -2043,6 +2044,7 @@ static void check_objective(int obj)
 }
 
 #include "control_host.inc"
+#include "control_topo_host.inc"
 
 }  // namespace egg_b200
 
@@ -2254,6 +2256,53 @@ int egg_b200_session_attach_control(egg_b200_session* s, const egg_b200_control_
         Session& S = *s->impl;
         if (S.n_seg > 0) { invalid("attach_control: a batch session takes one net per mesh (batch_attach_controls)"); }
         attach_control(S, desc, 1, nullptr, nullptr);
+    });
+}
+
+int egg_b200_session_attach_control_topo(egg_b200_session* s, const egg_b200_control_topo_desc* desc)
+{
+    return guarded([&] {
+        if (!s || !desc) { invalid("attach_control_topo: NULL argument"); }
+        Session& S = *s->impl;
+        if (S.n_seg > 0) { invalid("attach_control_topo: a batch session takes one net per mesh"); }
+        EGG_CK(cudaSetDevice(S.device));
+        attach_control_topo(S, *desc);
+    });
+}
+
+static Session& topo_session(egg_b200_session* s, const char* what)
+{
+    if (!s) { invalid(std::string(what) + ": NULL session"); }
+    Session& S = *s->impl;
+    if (!S.ctl || !S.ctl->topo) { invalid(std::string(what) + ": session has no multi-block control wire"); }
+    EGG_CK(cudaSetDevice(S.device));
+    return S;
+}
+
+int egg_b200_session_set_control_reduction(egg_b200_session* s, int64_t nq, const int32_t* off, int64_t off_len,
+                                           const int32_t* col, const double* coef, int64_t nnz)
+{
+    return guarded([&] {
+        Session& S = topo_session(s, "set_control_reduction");
+        topo_set_reduction(S, nq, off, off_len, col, coef, nnz);
+    });
+}
+
+int egg_b200_session_set_control_penalty(egg_b200_session* s, const int32_t* off, int64_t off_len,
+                                         const int32_t* col, const double* coef, int64_t nnz, const double* w,
+                                         int64_t w_len)
+{
+    return guarded([&] {
+        Session& S = topo_session(s, "set_control_penalty");
+        topo_set_penalty(S, off, off_len, col, coef, nnz, w, w_len);
+    });
+}
+
+int egg_b200_session_set_control_b(egg_b200_session* s, int32_t net_index, const double* b, int64_t len)
+{
+    return guarded([&] {
+        Session& S = topo_session(s, "set_control_b");
+        topo_set_b(S, net_index, b, len);
     });
 }
 

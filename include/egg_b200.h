@@ -266,9 +266,64 @@ int egg_b200_session_run_control(egg_b200_session* s, int32_t n_outer, int32_t o
                                  double* pcg_iters, double* pcg_relres, int64_t* counts, int32_t* iters,
                                  int32_t* converged);
 
+/* Multi-block control topology wire (src/control_net.hpp ControlTopoHostT;
+ * src/bindings.cpp:596-690 unpack_control_topo; built by
+ * egg/smoothing/control_backend.py run_control_topo): one net per block,
+ * stacked in wire order (nets[i].C0, free_idx and n_free are ignored: every
+ * control is free and C0 is the stacked lattice), the reduction CSR dC = R dq
+ * over the nsd = total controls * dim stacked components (r_off has nsd + 1
+ * entries, columns < nq), and optional penalty rows 1/2 sum_j w_j (P_j C)^2
+ * (p_off_len == 0 for none; columns < nsd).  The sliding-wall frame wire
+ * (control['slide']) has no counterpart here. */
+typedef struct egg_b200_control_topo_desc {
+    int32_t n_nets;
+    int32_t reserved;
+    const egg_b200_control_desc* nets; /* [n_nets] */
+    const double* C0;                  /* [C0_len = total controls * dim] */
+    int64_t C0_len;
+    int64_t nq;
+    const int32_t* r_off;
+    int64_t r_off_len;
+    const int32_t* r_col;
+    const double* r_coef;
+    int64_t r_nnz;
+    const int32_t* p_off;
+    int64_t p_off_len;
+    const int32_t* p_col;
+    const double* p_coef;
+    int64_t p_nnz;
+    const double* p_w;
+    int64_t p_w_len;
+} egg_b200_control_topo_desc;
+
+/* Attach a multi-block control topology (the reference builds it inside the
+ * session constructor when control['blocks'] is present, src/bindings.cpp:
+ * 1181-1235 -> ControlTopoSessionT, src/control_solve.hpp:1585).  The alias
+ * groups of shared nodes come from the session's own owner / copy tables.
+ * Validation messages as the reference's ("control topo: ...", EINVAL);
+ * ENOTSUP when a block carries no net or the energy stencil is not the
+ * canonical cell stencil of the blocks.  Evaluates X = M C + b and refreshes
+ * the copies.  egg_b200_session_run_control then runs the topology's single
+ * reduced problem (one report); get_C / set_C use the stacked lattice. */
+int egg_b200_session_attach_control_topo(egg_b200_session* s, const egg_b200_control_topo_desc* desc);
+/* Replace the reduction CSR (src/control_solve.hpp:2057 set_reduction;
+ * binding src/bindings.cpp:1474-1495 set_control_reduction). */
+int egg_b200_session_set_control_reduction(egg_b200_session* s, int64_t nq, const int32_t* off, int64_t off_len,
+                                           const int32_t* col, const double* coef, int64_t nnz);
+/* Replace the penalty rows; off_len == 0 removes them (src/control_solve.hpp:
+ * 2120 set_penalty; binding src/bindings.cpp:1497-1516). */
+int egg_b200_session_set_control_penalty(egg_b200_session* s, const int32_t* off, int64_t off_len,
+                                         const int32_t* col, const double* coef, int64_t nnz, const double* w,
+                                         int64_t w_len);
+/* Replace net `net_index`'s Boolean-sum offset b (node count * dim reals) and
+ * re-evaluate X (src/control_solve.hpp:2172 set_b; binding
+ * src/bindings.cpp:1518-1530 set_control_b). */
+int egg_b200_session_set_control_b(egg_b200_session* s, int32_t net_index, const double* b, int64_t len);
+
 /* The resident control lattice (prod(ctrl_shape) * dim reals; stacked over
- * the meshes of a batch): size, download, and upload followed by the
- * evaluation X = M C + b into the store (src/bindings.cpp:1441-1480). */
+ * the meshes of a batch or the nets of a topology): size, download, and
+ * upload followed by the evaluation X = M C + b into the store
+ * (src/bindings.cpp:1441-1480). */
 int egg_b200_session_control_size(egg_b200_session* s, int64_t* n_reals);
 int egg_b200_session_get_C(egg_b200_session* s, double* C, int64_t len);
 int egg_b200_session_set_C(egg_b200_session* s, const double* C, int64_t len);

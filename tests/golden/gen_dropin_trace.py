@@ -21,7 +21,8 @@ on the GPU: the drop-in boundary is then exercised by the very calls the
 reference's drivers make, which the GPU host cannot generate itself (the
 reference's Python does not travel there).
 
-    python tests/golden/gen_dropin_trace.py [REFERENCE_ROOT]
+    python tests/golden/gen_dropin_trace.py [REFERENCE_ROOT]          # ref_dropin.pkl.gz
+    python tests/golden/gen_dropin_trace.py --topo [REFERENCE_ROOT]   # ref_dropin_topo.pkl.gz
 
 (default: ``$EGG_REFERENCE_ROOT`` or a ``reference`` checkout beside this
 repository).  Test infrastructure only.
@@ -207,16 +208,64 @@ def record(ref_root: Path) -> list[dict]:
     return rec.events
 
 
-if __name__ == "__main__":
+TRACE_TOPO = HERE / "ref_dropin_topo.pkl.gz"
+
+
+def record_topo(ref_root: Path) -> list[dict]:
+    """``run_control_topo`` (``egg/smoothing/control_backend.py:646``) on the
+    reference's own multi-block control test grids: a two-block seam with a
+    wavy edge, a 2 x 2 crossing and a valence-3 fan, with C1 seams and fan
+    penalty rows, plus a seam-orthogonality penalty run (per-iteration
+    penalty uploads) and a C2-penalty run."""
     from oracle import oracle
 
-    root = Path(sys.argv[1]) if len(sys.argv) > 1 else oracle.reference_root()
-    if root is None:
-        raise SystemExit("reference checkout not found: pass its path or set EGG_REFERENCE_ROOT")
-    events = record(root)
-    with gzip.open(TRACE, "wb") as f:
+    ref = oracle.load_ref("fp64snap")
+    if ref is None:
+        raise SystemExit("oracle/_ref/fp64snap missing: run oracle/build_ref.sh first")
+    sys.path.insert(0, str(ref_root))
+    import egg._cpp  # noqa: F401
+
+    rec = Recorder(ref)
+    proxy = rec.module()
+    sys.modules["egg._cpp.cpp_core"] = proxy
+    sys.modules["egg._cpp"].cpp_core = proxy
+
+    from egg.smoothing.control_backend import run_control_topo
+    from egg.smoothing.targets import IdentityTarget
+    from tests.smoothing.test_control_topology import _fan_grid, _lr_grid, _perturb, _quad_grid
+
+    exact = dict(pcg_forcing=False, pcg_rtol=1e-12, pcg_max_iter=2000)
+    cases = [("seam", lambda: _lr_grid(wave=0.3), {}), ("crossing", _quad_grid, {}), ("fan", _fan_grid, {}),
+             ("seam_c2", lambda: _lr_grid(wave=0.3), dict(c2_weight=0.5)),
+             ("seam_ortho", lambda: _lr_grid(shear=0.3), dict(ortho="penalty", ortho_weight=1.0)),
+             ("crossing_inexact", _quad_grid, dict(pcg_forcing=True, pcg_rtol=1e-10))]
+    for name, make, kw in cases:
+        rec.scenario = name
+        grid = make()
+        _perturb(grid)
+        opts = dict(exact)
+        opts.update(kw)
+        run_control_topo(grid, IdentityTarget(2), device="auto", **opts)
+    return rec.events
+
+
+def _save(path: Path, events: list[dict]) -> None:
+    with gzip.open(path, "wb") as f:
         pickle.dump({"events": events}, f, protocol=4)
     counts = {}
     for ev in events:
         counts[ev["scenario"]] = counts.get(ev["scenario"], 0) + 1
-    print(f"{TRACE.name}: {len(events)} calls {counts}")
+    print(f"{path.name}: {len(events)} calls {counts}")
+
+
+if __name__ == "__main__":
+    from oracle import oracle
+
+    args = [a for a in sys.argv[1:] if not a.startswith("--")]
+    root = Path(args[0]) if args else oracle.reference_root()
+    if root is None:
+        raise SystemExit("reference checkout not found: pass its path or set EGG_REFERENCE_ROOT")
+    if "--topo" in sys.argv:
+        _save(TRACE_TOPO, record_topo(root))
+    else:
+        _save(TRACE, record(root))

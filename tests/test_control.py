@@ -81,12 +81,53 @@ def test_malformed_wire_is_refused_before_the_device(core, bad, match):
         core.CppStructuredSweepSession(ctx, st, X, control=bad(_wire("wavy9")))
 
 
-def test_walls_and_topologies_are_not_supported(core):
+def test_walls_are_not_supported(core):
     g, (ctx, st, X) = _session_args("wavy9")
     with pytest.raises(NotImplementedError, match="walls"):
         core.CppStructuredSweepSession(ctx, st, X, control={**_wire("wavy9"), "walls": [object()]})
-    with pytest.raises(NotImplementedError, match="blocks"):
-        core.CppStructuredSweepSession(ctx, st, X, control={"blocks": []})
+
+
+def _topo_new():
+    """The constructor call the reference's run_control_topo made for its
+    two-block seam grid (tests/golden/ref_dropin_topo.pkl.gz)."""
+    import gzip
+    import pickle
+
+    from tests.conftest import GOLDEN
+
+    with gzip.open(GOLDEN / "ref_dropin_topo.pkl.gz", "rb") as f:
+        ev = next(e for e in pickle.load(f)["events"] if e["scenario"] == "seam" and e["op"] == "new")
+    return ev["args"], ev["kwargs"]
+
+
+def _with_block(ctl, i, **kv):
+    blocks = [dict(b) for b in ctl["blocks"]]
+    blocks[i].update(kv)
+    return {**ctl, "blocks": blocks}
+
+
+@pytest.mark.parametrize("bad, exc, match", [
+    (lambda c: _with_block(c, 1, ctrl_shape=np.array([1, 6], dtype=np.int32)), ValueError, "ctrl_shape entry"),
+    (lambda c: _with_block(c, 0, wt0=np.asarray(c["blocks"][0]["wt0"])[:-1]), ValueError, "wt0 size"),
+    (lambda c: _with_block(c, 0, k_supp=0), ValueError, "k_supp"),
+    (lambda c: _with_block(c, 1, b=np.asarray(c["blocks"][1]["b"])[:-2]), ValueError, "b size"),
+    (lambda c: _with_block(c, 1, X0=np.zeros(3)), ValueError, "X0 size"),
+    (lambda c: {**c, "C0": np.asarray(c["C0"])[:-2]}, ValueError, "C0 size"),
+    (lambda c: {**c, "r_off": np.asarray(c["r_off"])[:-1]}, ValueError, "malformed reduction CSR"),
+    (lambda c: {**c, "p_off": np.array([0, 1]), "p_col": np.array([0]), "p_coef": np.array([1.0]),
+                "p_w": np.array([1.0, 1.0])}, ValueError, "malformed penalty CSR"),
+    (lambda c: {**c, "slide": []}, NotImplementedError, "slide"),
+])
+def test_malformed_topology_wire_is_refused_before_the_device(core, bad, exc, match):
+    args, kwargs = _topo_new()
+    with pytest.raises(exc, match=match):
+        core.CppStructuredSweepSession(*args, **{**kwargs, "control": bad(kwargs["control"])})
+
+
+def test_batch_refuses_a_topology_wire(core):
+    args, kwargs = _topo_new()
+    with pytest.raises(NotImplementedError, match="batch"):
+        core.CppBatchSweepSession([tuple(args)], dim=kwargs["dim"], control=[kwargs["control"]])
 
 
 # ---------------------------------------------------------------- GPU ----
