@@ -1,6 +1,7 @@
-// Multi-block control topology: the layer that couples per-block nets
-// (src/control_solve.hpp:1585-2610 ControlTopoSessionT, src/control_net.hpp:
-// 776-1106).  The per-net kernels of control.cuh evaluate every net, gather
+// Reduced control solves: the layer that couples per-block nets in a
+// multi-block topology (src/control_solve.hpp:1585-2610 ControlTopoSessionT,
+// src/control_net.hpp:776-1106) and carries a single net's sliding walls
+// (src/control_solve.hpp:820-1545).  The per-net kernels of control.cuh evaluate every net, gather
 // per-node gradients / Hessian-vector products / Hessian blocks over each
 // block's own cells and pull them back onto that net's lattice; here:
 //   * alias sums over the copies of a shared node (the owner's net node takes
@@ -19,6 +20,8 @@
 #include <cstdint>
 #include <cuda_runtime.h>
 
+#include "control.cuh"
+
 namespace egg_b200
 {
 
@@ -32,6 +35,20 @@ struct TopoPcg {
     double b_norm2, stop2, r_norm2, rz, alpha, beta, rtol, pad;
     int32_t it, its, done, max_iter;
 };
+
+// out[f] = C[lattice(f)] over the stacked free controls (D reals each).
+template <int D>
+__global__ void ctl_gather_free_kernel(CtlTables T, int64_t total_free, const double* __restrict__ C,
+                                       double* __restrict__ out)
+{
+    for (int64_t g = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; g < total_free;
+         g += int64_t(gridDim.x) * blockDim.x) {
+        const int ni = net_of(T.free_pfx, T.n_nets, g);
+        const int64_t ci = T.nets[ni].c_off + T.free_idx[g];
+#pragma unroll
+        for (int c = 0; c < D; ++c) { out[g * D + c] = C[ci * D + c]; }
+    }
+}
 
 // out[i] = sum_e coef[e] v[col[e]] over row i's entries.
 __global__ void topo_csr_apply_kernel(int64_t n_rows, const int32_t* __restrict__ off, const int32_t* __restrict__ col,

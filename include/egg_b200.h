@@ -302,8 +302,9 @@ typedef struct egg_b200_control_topo_desc {
  * groups of shared nodes come from the session's own owner / copy tables.
  * Validation messages as the reference's ("control topo: ...", EINVAL);
  * ENOTSUP when a block carries no net or the energy stencil is not the
- * canonical cell stencil of the blocks.  Evaluates X = M C + b and refreshes
- * the copies.  egg_b200_session_run_control then runs the topology's single
+ * canonical cell stencil of the blocks.  X is left as it is (a run, set_C or
+ * set_control_b evaluates X = M C + b and refreshes the copies).
+ * egg_b200_session_run_control then runs the topology's single
  * reduced problem (one report); get_C / set_C use the stacked lattice. */
 int egg_b200_session_attach_control_topo(egg_b200_session* s, const egg_b200_control_topo_desc* desc);
 /* Replace the reduction CSR (src/control_solve.hpp:2057 set_reduction;

@@ -81,8 +81,11 @@ def _topo_session(gpu, scenario="seam"):
 def test_set_control_b_moves_only_that_net(gpu):
     ev, s = _topo_session(gpu)
     ctl = ev["kwargs"]["control"]
-    X0 = s.get_X().copy()
+    X_wire = s.get_X().copy()
     b0 = np.asarray(ctl["blocks"][1]["b"], dtype=np.float64)
+    s.set_control_b(1, b0 + 0.0)  # evaluates the nets: X = M C0 + b
+    X0 = s.get_X().copy()
+    assert np.abs(X0 - X_wire).max() > 0  # the constructor left the wire's X
     s.set_control_b(1, b0 + 0.0)
     np.testing.assert_array_equal(s.get_X(), X0)
     s.set_control_b(1, b0 + 1e-3)
