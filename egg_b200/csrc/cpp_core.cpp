@@ -377,10 +377,6 @@ void fill_control(egg_b200_control_desc& c, Keep& keep, const py::dict& w, int d
                         "CppStructuredSweepSession; a batch takes one single-block net per mesh");
         throw py::error_already_set();
     }
-    if (w.contains("walls") && py::len(w["walls"]) > 0) {
-        PyErr_SetString(PyExc_NotImplementedError, "egg_b200: control walls (sliding boundary controls) are not supported");
-        throw py::error_already_set();
-    }
     for (const char* k : {"block", "ctrl_shape", "k_supp", "C0", "free_idx", "b"}) {
         if (!w.contains(k)) { throw py::value_error(std::string("control: missing key '") + k + "'"); }
     }
@@ -497,6 +493,52 @@ void fill_control_topo(TopoWire& t, Keep& keep, const py::dict& w, int dim)
     }
 }
 
+// The walls of a single-block control wire (src/bindings.cpp:557-590): the
+// exact node field X0 and one record per wall face.
+struct WallWire {
+    std::vector<egg_b200_control_wall> walls;
+    const double* X0 = nullptr;
+    int64_t X0_len = 0;
+    bool present = false;
+};
+
+void fill_walls(WallWire& ww, Keep& keep, const py::dict& w, const egg_b200_control_desc& c, int dim)
+{
+    if (!w.contains("walls")) { return; }
+    ww.present = true;
+    if (!w.contains("X0")) { throw py::value_error("control: walls require X0"); }
+    ww.X0 = keep.reals(w["X0"], &ww.X0_len);
+    int64_t n_nodes = 1;
+    for (int k = 0; k < dim; ++k) { n_nodes *= c.off_len[k]; }
+    if (ww.X0_len != n_nodes * dim) { throw py::value_error("control: X0 size != prod(node_shape) * D"); }
+    int64_t n_ctrl = 1;
+    for (int k = 0; k < dim; ++k) { n_ctrl *= c.ctrl_shape[k]; }
+    for (const py::handle item : w["walls"].cast<py::list>()) {
+        const py::dict wd = item.cast<py::dict>();
+        egg_b200_control_wall x {};
+        x.axis = wd["axis"].cast<int32_t>();
+        x.side = wd["side"].cast<int32_t>();
+        x.mode = wd["mode"].cast<int32_t>();
+        if (x.axis < 0 || x.axis >= dim || (x.side != 0 && x.side != 1) || x.mode < 0 || x.mode > 2) {
+            throw py::value_error("control: wall axis/side/mode out of range");
+        }
+        int64_t nw = 0, n0 = 0, n1 = 0;
+        x.weight = keep.reals(wd["weight"], &nw);
+        x.p0 = keep.ints(wd["p0"], &n0);
+        x.p1 = keep.ints(wd["p1"], &n1);
+        if (n0 != n1 || nw != n0) { throw py::value_error("control: wall p0/p1/weight length mismatch"); }
+        x.n_legs = n0;
+        for (int64_t j = 0; j < n0; ++j) {
+            if (x.p0[j] < 0 || x.p0[j] >= n_ctrl || x.p1[j] < 0 || x.p1[j] >= n_ctrl) {
+                throw py::value_error("control: wall control id out of range");
+            }
+        }
+        x.tag = wd["tag"].cast<int32_t>();
+        x.params = keep.reals(wd["params"], &x.params_len);
+        ww.walls.push_back(x);
+    }
+}
+
 py::dict control_report(int n_outer, const std::vector<double>& E, const std::vector<double>& M,
                         const std::vector<double>& A, const std::vector<double>& PI, const std::vector<double>& PR,
                         const int64_t* cnt, int32_t iters, int32_t conv)
@@ -529,11 +571,13 @@ class Session
         Keep ckeep;
         egg_b200_control_desc cdesc;
         TopoWire topo;
+        WallWire walls;
         const bool is_topo = !control.is_none() && control.cast<py::dict>().contains("blocks");
         if (is_topo) {
             fill_control_topo(topo, ckeep, control.cast<py::dict>(), dim);
         } else if (!control.is_none()) {
             fill_control(cdesc, ckeep, control.cast<py::dict>(), dim);
+            fill_walls(walls, ckeep, control.cast<py::dict>(), cdesc, dim);
         }
         egg_b200_session* h = nullptr;
         {
@@ -549,6 +593,9 @@ class Session
         nblocks_ = D.d.num_blocks;
         if (is_topo) {
             check(egg_b200_session_attach_control_topo(h_.get(), &topo.d));
+        } else if (!walls.walls.empty()) {
+            check(egg_b200_session_attach_control_walls(h_.get(), &cdesc, walls.X0, walls.X0_len,
+                                                        int32_t(walls.walls.size()), walls.walls.data()));
         } else if (!control.is_none()) {
             check(egg_b200_session_attach_control(h_.get(), &cdesc));
         }
@@ -858,7 +905,16 @@ class Batch : public Session
             py::sequence cl = control.cast<py::sequence>();
             if (size_t(py::len(cl)) != n) { throw py::value_error("control: one wire per mesh is required"); }
             cds.resize(n);
-            for (size_t m = 0; m < n; ++m) { fill_control(cds[m], ckeep, cl[m].cast<py::dict>(), dim); }
+            for (size_t m = 0; m < n; ++m) {
+                const py::dict wm = cl[m].cast<py::dict>();
+                if (wm.contains("walls") && py::len(wm["walls"]) > 0) {
+                    PyErr_SetString(PyExc_NotImplementedError,
+                                    "egg_b200: control walls attach to one CppStructuredSweepSession; a batch takes "
+                                    "plain nets");
+                    throw py::error_already_set();
+                }
+                fill_control(cds[m], ckeep, wm, dim);
+            }
         }
         egg_b200_session* h = nullptr;
         int rc;

@@ -77,6 +77,13 @@ template <class T> struct DevBuf {
         alloc(h.size());
         if (n) { EGG_CK(cudaMemcpy(p, h.data(), n * sizeof(T), cudaMemcpyHostToDevice)); }
     }
+    // upload() that keeps an allocation of the same size; only for buffers
+    // that no queued work still reads (the caller has synchronised).
+    void put(const std::vector<T>& h)
+    {
+        if (h.size() != n) { alloc(h.size()); }
+        if (n) { EGG_CK(cudaMemcpy(p, h.data(), n * sizeof(T), cudaMemcpyHostToDevice)); }
+    }
 };
 
 // Launch variants of the interior kernel: cells per CTA (CI x CJ) and the
@@ -2045,6 +2052,7 @@ static void check_objective(int obj)
 
 #include "control_host.inc"
 #include "control_topo_host.inc"
+#include "control_walls_host.inc"
 
 }  // namespace egg_b200
 
@@ -2259,6 +2267,18 @@ int egg_b200_session_attach_control(egg_b200_session* s, const egg_b200_control_
     });
 }
 
+int egg_b200_session_attach_control_walls(egg_b200_session* s, const egg_b200_control_desc* desc, const double* X0,
+                                          int64_t X0_len, int32_t n_walls, const egg_b200_control_wall* walls)
+{
+    return guarded([&] {
+        if (!s || !desc) { invalid("attach_control_walls: NULL argument"); }
+        Session& S = *s->impl;
+        if (S.n_seg > 0) { invalid("attach_control_walls: a batch session takes plain nets (batch_attach_controls)"); }
+        EGG_CK(cudaSetDevice(S.device));
+        attach_control_walls(S, *desc, X0, X0_len, n_walls, walls);
+    });
+}
+
 int egg_b200_session_attach_control_topo(egg_b200_session* s, const egg_b200_control_topo_desc* desc)
 {
     return guarded([&] {
@@ -2274,7 +2294,9 @@ static Session& topo_session(egg_b200_session* s, const char* what)
 {
     if (!s) { invalid(std::string(what) + ": NULL session"); }
     Session& S = *s->impl;
-    if (!S.ctl || !S.ctl->topo) { invalid(std::string(what) + ": session has no multi-block control wire"); }
+    if (!S.ctl || !S.ctl->topo || S.ctl->walls) {
+        invalid(std::string(what) + ": session has no multi-block control wire");
+    }
     EGG_CK(cudaSetDevice(S.device));
     return S;
 }

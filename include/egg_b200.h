@@ -266,6 +266,38 @@ int egg_b200_session_run_control(egg_b200_session* s, int32_t n_outer, int32_t o
                                  double* pcg_iters, double* pcg_relres, int64_t* counts, int32_t* iters,
                                  int32_t* converged);
 
+/* One wall face of a single control net (src/control_net.hpp
+ * ControlWallHost; wire src/bindings.cpp:557-590, built by
+ * egg/smoothing/control_backend.py:137-175 from
+ * egg/smoothing/control_wall.py WallSpec): the net's face `axis`/`side`
+ * lies on a codim-1 entity (a 2D curve or a 3D surface with a fixed-size
+ * record: tags 1-3, 6-9, 15 in 2D; 4, 5, 12 in 3D).  Leg j pairs the
+ * wall-row control p0[j], which slides on the entity, with its inward
+ * neighbour p1[j]; mode 0 leaves p1 free, 1 adds the penalty
+ * weight[j] / |leg|^2 on the leg's tangential components, 2 holds p1 on the
+ * wall normal through p0 (one height unknown). */
+typedef struct egg_b200_control_wall {
+    int32_t axis, side, mode, tag;
+    int64_t n_legs;
+    const int32_t* p0;     /* [n_legs] lattice ids (free controls) */
+    const int32_t* p1;     /* [n_legs] */
+    const double* weight;  /* [n_legs] */
+    const double* params;  /* entity record, params_len <= EGG_B200_ENTITY_FIELDS reals */
+    int64_t params_len;
+} egg_b200_control_wall;
+
+/* Attach a control net with walls (the reference builds it inside the
+ * session constructor when the control wire carries "walls": ControlSessionT
+ * with init_walls, src/control_solve.hpp:498,828).  X0 [node count * dim] is
+ * the block's exact node field; its non-wall boundary rows anchor the
+ * Boolean-sum re-extension.  egg_b200_session_run_control then rebuilds the
+ * wall frame before every outer iteration and once at the end
+ * (src/control_solve.hpp:1331 run_walls).  EINVAL on the reference's
+ * validation failures; ENOTSUP for segmented wall entities (B-spline,
+ * composite), which the reference's wire builder refuses too. */
+int egg_b200_session_attach_control_walls(egg_b200_session* s, const egg_b200_control_desc* desc, const double* X0,
+                                          int64_t X0_len, int32_t n_walls, const egg_b200_control_wall* walls);
+
 /* Multi-block control topology wire (src/control_net.hpp ControlTopoHostT;
  * src/bindings.cpp:596-690 unpack_control_topo; built by
  * egg/smoothing/control_backend.py run_control_topo): one net per block,

@@ -23,6 +23,7 @@ reference's Python does not travel there).
 
     python tests/golden/gen_dropin_trace.py [REFERENCE_ROOT]          # ref_dropin.pkl.gz
     python tests/golden/gen_dropin_trace.py --topo [REFERENCE_ROOT]   # ref_dropin_topo.pkl.gz
+    python tests/golden/gen_dropin_trace.py --walls [REFERENCE_ROOT]  # ref_dropin_walls.pkl.gz
 
 (default: ``$EGG_REFERENCE_ROOT`` or a ``reference`` checkout beside this
 repository).  Test infrastructure only.
@@ -61,7 +62,9 @@ def _copy(v):
 
 
 class Recorder:
-    """Builds the proxy module and collects the trace."""
+    """Builds the proxy module and collects the trace.  A session that the
+    driver opens on the reference's host device (``device="cpu"``) is
+    recorded with ``device="auto"``: the replay runs it on the GPU."""
 
     def __init__(self, ref):
         self.ref = ref
@@ -97,7 +100,10 @@ class Recorder:
                 self._s = ref.CppStructuredSweepSession(*args, **kwargs)
                 self._sid = rec._next_sid
                 rec._next_sid += 1
-                rec.log(op="new", sid=self._sid, args=_copy(args), kwargs=_copy(kwargs))
+                kw = _copy(kwargs)
+                if kw.get("device") == "cpu":
+                    kw["device"] = "auto"
+                rec.log(op="new", sid=self._sid, args=_copy(args), kwargs=kw)
 
             def __getattr__(self, name):
                 attr = getattr(self._s, name)
@@ -249,6 +255,66 @@ def record_topo(ref_root: Path) -> list[dict]:
     return rec.events
 
 
+TRACE_WALLS = HERE / "ref_dropin_walls.pkl.gz"
+
+
+def record_walls(ref_root: Path) -> list[dict]:
+    """Single-block control nets with sliding walls, through the reference's
+    own wall-session helpers (``tests/smoothing/test_control_wall_cpp.py``,
+    wire ``egg/smoothing/control_backend.py:137-175``): an arc wall with the
+    orthogonality dial off, a sheared arc wall in the three modes (off,
+    penalty, hard) with exact PCG solves and once more in hard mode with the
+    default inexact solves, and a 3D cube whose bottom face slides on a
+    sphere (off and hard)."""
+    from oracle import oracle
+
+    ref = oracle.load_ref("fp64snap")
+    if ref is None:
+        raise SystemExit("oracle/_ref/fp64snap missing: run oracle/build_ref.sh first")
+    sys.path.insert(0, str(ref_root))
+    import egg._cpp  # noqa: F401
+
+    rec = Recorder(ref)
+    proxy = rec.module()
+    sys.modules["egg._cpp.cpp_core"] = proxy
+    sys.modules["egg._cpp"].cpp_core = proxy
+
+    from tests.smoothing.test_control_wall import _make_arc_grid, _make_sheared_arc_grid
+    from tests.smoothing.test_control_wall_cpp import (
+        _make_sphere_cube_grid,
+        _make_wall_session,
+        _make_wall_session_3d,
+    )
+
+    def finish(sess):
+        sess.get_C()
+        sess.get_X()
+
+    rec.scenario = "arc_off"
+    grid, arc = _make_arc_grid()
+    sess, _ = _make_wall_session(grid, arc, "off")
+    sess.run_control(20)
+    finish(sess)
+    for ortho, weight in (("off", 0.0), ("penalty", 10.0), ("hard", 0.0)):
+        rec.scenario = f"sheared_{ortho}"
+        grid, arc = _make_sheared_arc_grid()
+        sess, _ = _make_wall_session(grid, arc, ortho, weight=weight)
+        sess.run_control(12, pcg_max_iter=500, pcg_rtol=1e-12, pcg_forcing=False)
+        finish(sess)
+    rec.scenario = "sheared_hard_inexact"
+    grid, arc = _make_sheared_arc_grid()
+    sess, _ = _make_wall_session(grid, arc, "hard")
+    sess.run_control(25)
+    finish(sess)
+    for ortho in ("off", "hard"):
+        rec.scenario = f"sphere_{ortho}"
+        grid, sphere = _make_sphere_cube_grid()
+        sess, _ = _make_wall_session_3d(grid, sphere, ortho)
+        sess.run_control(10)
+        finish(sess)
+    return rec.events
+
+
 def _save(path: Path, events: list[dict]) -> None:
     with gzip.open(path, "wb") as f:
         pickle.dump({"events": events}, f, protocol=4)
@@ -267,5 +333,7 @@ if __name__ == "__main__":
         raise SystemExit("reference checkout not found: pass its path or set EGG_REFERENCE_ROOT")
     if "--topo" in sys.argv:
         _save(TRACE_TOPO, record_topo(root))
+    elif "--walls" in sys.argv:
+        _save(TRACE_WALLS, record_walls(root))
     else:
         _save(TRACE, record(root))

@@ -81,10 +81,41 @@ def test_malformed_wire_is_refused_before_the_device(core, bad, match):
         core.CppStructuredSweepSession(ctx, st, X, control=bad(_wire("wavy9")))
 
 
-def test_walls_are_not_supported(core):
-    g, (ctx, st, X) = _session_args("wavy9")
+def _walls_new():
+    """The constructor call of the reference's arc-wall session
+    (tests/golden/ref_dropin_walls.pkl.gz)."""
+    import gzip
+    import pickle
+
+    from tests.conftest import GOLDEN
+
+    with gzip.open(GOLDEN / "ref_dropin_walls.pkl.gz", "rb") as f:
+        ev = next(e for e in pickle.load(f)["events"] if e["scenario"] == "arc_off" and e["op"] == "new")
+    return ev["args"], ev["kwargs"]
+
+
+def _with_wall(ctl, **kv):
+    return {**ctl, "walls": [dict(ctl["walls"][0], **kv)]}
+
+
+@pytest.mark.parametrize("bad, match", [
+    (lambda c: {k: v for k, v in c.items() if k != "X0"}, "walls require X0"),
+    (lambda c: {**c, "X0": np.asarray(c["X0"])[:-2]}, "X0 size"),
+    (lambda c: _with_wall(c, axis=2), "axis/side/mode"),
+    (lambda c: _with_wall(c, mode=3), "axis/side/mode"),
+    (lambda c: _with_wall(c, weight=np.zeros(1)), "p0/p1/weight length mismatch"),
+    (lambda c: _with_wall(c, p1=np.full(len(c["walls"][0]["p1"]), 10**6, dtype=np.int32)), "control id out of range"),
+])
+def test_malformed_wall_wire_is_refused_before_the_device(core, bad, match):
+    args, kwargs = _walls_new()
+    with pytest.raises(ValueError, match=match):
+        core.CppStructuredSweepSession(*args, **{**kwargs, "control": bad(kwargs["control"])})
+
+
+def test_batch_refuses_walls(core):
+    args, kwargs = _walls_new()
     with pytest.raises(NotImplementedError, match="walls"):
-        core.CppStructuredSweepSession(ctx, st, X, control={**_wire("wavy9"), "walls": [object()]})
+        core.CppBatchSweepSession([tuple(args)], dim=kwargs["dim"], control=[kwargs["control"]])
 
 
 def _topo_new():
