@@ -6,10 +6,10 @@ A trace is a list of events recorded by tests/golden/gen_dropin_trace.py:
 its arguments and the reference core's result).  Reports of ``run_control``
 are compared field by field: energies, min dets, step lengths, iteration
 count and convergence at the trajectory tolerances of the other fp64 control
-tests.  A PCG solve that stops at rtol may take an iteration or two more or
+tests.  A PCG solve that stops at rtol may take a few iterations more or
 fewer when its dot products round differently, so its iteration count is
-compared to within two and its final relative residual to within one
-decade.
+compared to within two or 5%, whichever is larger, and its final relative
+residual to within one decade.
 """
 
 from __future__ import annotations
@@ -38,7 +38,7 @@ def check_report(got, want, what, rtol=RTOL, atol=ATOL):
     assert len(got["frame_jumps"]) == len(want["frame_jumps"]) == 0
     gi, wi = np.asarray(got["pcg_iters"]), np.asarray(want["pcg_iters"])
     assert gi.shape == wi.shape, (what, gi, wi)
-    assert np.all(np.abs(gi - wi) <= 2), (what, gi, wi)
+    assert np.all(np.abs(gi - wi) <= np.maximum(2, 0.05 * wi)), (what, gi, wi)
     gr, wr = np.asarray(got["pcg_relres"]), np.asarray(want["pcg_relres"])
     assert gr.shape == wr.shape
     pos = wr > 0
