@@ -414,17 +414,79 @@ void fill_control(egg_b200_control_desc& c, Keep& keep, const py::dict& w, int d
 // by the sliding-wall frames) is checked for size and otherwise unused.
 struct TopoWire {
     std::vector<egg_b200_control_desc> nets;
+    std::vector<egg_b200_control_slide> slide;
+    std::vector<egg_b200_control_wall_face> wall_faces;
+    std::vector<int32_t> seam;
+    std::vector<double> X0;
     egg_b200_control_topo_desc d {};
 };
 
+// The sliding-wall frame wire of a topology (src/bindings.cpp:681-722,
+// egg/smoothing/control_backend.py:472-560): sliding roots, CAD wall faces,
+// per-net seam flags, the entity arena and every net's X0.
+void fill_topo_slides(TopoWire& t, Keep& keep, const py::dict& w, int dim, const std::vector<int64_t>& n_nodes)
+{
+    if (w.contains("arena")) { t.d.arena = keep.reals(w["arena"], &t.d.arena_len); }
+    for (const py::handle item : w["slide"].cast<py::list>()) {
+        const py::dict sd = item.cast<py::dict>();
+        egg_b200_control_slide r {};
+        r.rep_row = sd["rep_row"].cast<int32_t>();
+        int64_t nc = 0, nk = 0, ncomp = 0, nb = 0;
+        r.members = keep.ints(sd["members"], &r.n_members);
+        r.member_coef = keep.reals(sd["member_coef"], &nc);
+        r.tag = sd["tag"].cast<int32_t>();
+        r.params = keep.reals(sd["params"], &r.params_len);
+        r.r_entry = keep.ints(sd["r_entry"], &r.n_entries);
+        r.comp = keep.ints(sd["comp"], &ncomp);
+        r.kt = keep.ints(sd["kt"], &nk);
+        r.base = keep.reals(sd["base"], &nb);
+        if (nc != r.n_members || ncomp != r.n_entries || nk != r.n_entries || nb != r.n_entries) {
+            throw py::value_error("control topo: slide list length mismatch");
+        }
+        t.slide.push_back(r);
+    }
+    for (const py::handle item : w["wall_faces"].cast<py::list>()) {
+        const py::dict wd = item.cast<py::dict>();
+        egg_b200_control_wall_face f {};
+        f.net = wd["block"].cast<int32_t>();
+        f.axis = wd["axis"].cast<int32_t>();
+        f.side = wd["side"].cast<int32_t>();
+        f.tag = wd["tag"].cast<int32_t>();
+        f.params = keep.reals(wd["params"], &f.params_len);
+        t.wall_faces.push_back(f);
+    }
+    const py::list seams = w["seam_face"].cast<py::list>();
+    if (size_t(py::len(seams)) != t.nets.size()) {
+        throw py::value_error("control topo: seam_face flags must cover every net");
+    }
+    for (const py::handle item : seams) {
+        int64_t nf = 0;
+        const int32_t* fl = keep.ints(item, &nf);
+        if (nf != 2 * dim) { throw py::value_error("control topo: seam_face flags must have 2*D entries"); }
+        for (int64_t k = 0; k < nf; ++k) { t.seam.push_back(fl[k] != 0 ? 1 : 0); }
+    }
+    const py::list blocks = w["blocks"].cast<py::list>();
+    for (size_t i = 0; i < t.nets.size(); ++i) {
+        const py::dict bd = blocks[i].cast<py::dict>();
+        if (!bd.contains("X0")) { throw py::value_error("control topo: the slide wire requires per-block X0"); }
+        int64_t nx = 0;
+        const double* x0 = keep.reals(bd["X0"], &nx);
+        if (nx != n_nodes[i] * dim) { throw py::value_error("control topo: X0 size != prod(node_shape) * D"); }
+        t.X0.insert(t.X0.end(), x0, x0 + nx);
+    }
+    t.d.n_slide = int32_t(t.slide.size());
+    t.d.n_wall_faces = int32_t(t.wall_faces.size());
+    t.d.slide = t.slide.data();
+    t.d.wall_faces = t.wall_faces.data();
+    t.d.seam_face = t.seam.data();
+    t.d.X0 = t.X0.data();
+    t.d.X0_len = int64_t(t.X0.size());
+}
+
 void fill_control_topo(TopoWire& t, Keep& keep, const py::dict& w, int dim)
 {
-    if (w.contains("slide")) {
-        PyErr_SetString(PyExc_NotImplementedError,
-                        "egg_b200: sliding-wall control frames (control['slide']) are not supported");
-        throw py::error_already_set();
-    }
     int64_t n_stack = 0;
+    std::vector<int64_t> net_nodes;
     for (const py::handle item : w["blocks"].cast<py::list>()) {
         const py::dict bd = item.cast<py::dict>();
         egg_b200_control_desc c {};
@@ -464,6 +526,7 @@ void fill_control_topo(TopoWire& t, Keep& keep, const py::dict& w, int dim)
             if (nx != n_nodes * dim) { throw py::value_error("control topo: X0 size != prod(node_shape) * D"); }
         }
         n_stack += n_ctrl;
+        net_nodes.push_back(n_nodes);
         t.nets.push_back(c);
     }
     egg_b200_control_topo_desc& d = t.d;
@@ -491,6 +554,7 @@ void fill_control_topo(TopoWire& t, Keep& keep, const py::dict& w, int dim)
             throw py::value_error("control topo: malformed penalty CSR");
         }
     }
+    if (w.contains("slide")) { fill_topo_slides(t, keep, w, dim, net_nodes); }
 }
 
 // The walls of a single-block control wire (src/bindings.cpp:557-590): the
@@ -628,21 +692,24 @@ class Session
     py::dict run_control(int n_outer, const std::string& phase, double grad_tol, double alpha_min, double lm0,
                          int pcg_max_iter, double pcg_rtol, bool pcg_forcing, bool model_db)
     {
-        (void)model_db;  // frozen-frame d b / d C modelling applies to sliding walls only
         const int64_t ce = int64_t(n_outer) + 1, ca = std::max(n_outer, 1), cp = 8 * ca;
         std::vector<double> E(static_cast<size_t>(ce)), M(static_cast<size_t>(ce)), A(static_cast<size_t>(ca));
-        std::vector<double> PI(static_cast<size_t>(cp)), PR(static_cast<size_t>(cp));
-        int64_t cnt[3] = {0, 0, 0};
+        std::vector<double> PI(static_cast<size_t>(cp)), PR(static_cast<size_t>(cp)), FJ(static_cast<size_t>(ca));
+        int64_t cnt[3] = {0, 0, 0}, nfj = 0;
         int32_t iters = 0, conv = 0;
         int rc;
         {
             py::gil_scoped_release nogil;
-            rc = egg_b200_session_run_control(h_.get(), n_outer, objective_of(phase), grad_tol, alpha_min, lm0,
-                                              pcg_max_iter, pcg_rtol, pcg_forcing ? 1 : 0, E.data(), M.data(),
-                                              A.data(), PI.data(), PR.data(), cnt, &iters, &conv);
+            rc = egg_b200_session_run_control_ex(h_.get(), n_outer, objective_of(phase), grad_tol, alpha_min, lm0,
+                                                 pcg_max_iter, pcg_rtol, pcg_forcing ? 1 : 0, model_db ? 1 : 0,
+                                                 E.data(), M.data(), A.data(), PI.data(), PR.data(), cnt, &iters,
+                                                 &conv, FJ.data(), &nfj);
         }
         check(rc);
-        return control_report(n_outer, E, M, A, PI, PR, cnt, iters, conv);
+        py::dict out = control_report(n_outer, E, M, A, PI, PR, cnt, iters, conv);
+        FJ.resize(static_cast<size_t>(nfj));
+        out["frame_jumps"] = vec(FJ);
+        return out;
     }
 
     py::array_t<double> get_C()

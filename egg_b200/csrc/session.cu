@@ -2364,6 +2364,20 @@ int egg_b200_session_run_control(egg_b200_session* s, int32_t n_outer, int32_t o
     });
 }
 
+int egg_b200_session_run_control_ex(egg_b200_session* s, int32_t n_outer, int32_t objective, double grad_tol,
+                                    double alpha_min, double lm0, int32_t pcg_max_iter, double pcg_rtol,
+                                    int32_t pcg_forcing, int32_t model_db, double* energies, double* mindets,
+                                    double* alphas, double* pcg_iters, double* pcg_relres, int64_t* counts,
+                                    int32_t* iters, int32_t* converged, double* frame_jumps, int64_t* n_frame_jumps)
+{
+    return guarded([&] {
+        if (!s) { invalid("run_control: NULL session"); }
+        run_control_abi(*s->impl, n_outer, objective, grad_tol, alpha_min, lm0, pcg_max_iter, pcg_rtol, pcg_forcing,
+                        energies, mindets, alphas, pcg_iters, pcg_relres, counts, iters, converged, false, model_db,
+                        frame_jumps, n_frame_jumps);
+    });
+}
+
 int egg_b200_batch_run_control(egg_b200_session* s, int32_t n_outer, int32_t objective, double grad_tol,
                                double alpha_min, double lm0, int32_t pcg_max_iter, double pcg_rtol,
                                int32_t pcg_forcing, double* energies, double* mindets, double* alphas,

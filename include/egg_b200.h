@@ -305,8 +305,44 @@ int egg_b200_session_attach_control_walls(egg_b200_session* s, const egg_b200_co
  * control is free and C0 is the stacked lattice), the reduction CSR dC = R dq
  * over the nsd = total controls * dim stacked components (r_off has nsd + 1
  * entries, columns < nq), and optional penalty rows 1/2 sum_j w_j (P_j C)^2
- * (p_off_len == 0 for none; columns < nsd).  The sliding-wall frame wire
- * (control['slide']) has no counterpart here. */
+ * (p_off_len == 0 for none; columns < nsd), and optionally the
+ * sliding-wall frames (egg_b200_control_slide): run_control then rebuilds
+ * the frame before every outer iteration and once at the end
+ * (src/control_solve.hpp:2771 rebuild_frame) and reports each rebuild's
+ * energy jump. */
+/* Sliding-wall frames of a topology (src/control_net.hpp ControlTopoHostT
+ * slide / wall_faces / seam_face; wire built by
+ * egg/smoothing/control_backend.py:472-560 _attach_slide_wire).  A sliding
+ * root is a reduced unknown riding an entity: its representative stacked
+ * control rep_row is projected every outer iteration, the tangent frame at
+ * the foot rewrites the reduction entries r_entry[e] = base[e] *
+ * t[kt[e]][comp[e]], and every member row moves by member_coef * (foot -
+ * rep).  Entity records are the reference's decode blobs: the fixed-size
+ * records of the constrained-boundary tags, a 2D B-spline curve as
+ * (degree, n_ctrl, knot_off, ctrl_off, t0, t1, w_off, has_w) and a 2D
+ * composite path as (n_segs, rec_off), offsets into `arena`. */
+typedef struct egg_b200_control_slide {
+    int32_t rep_row, tag;
+    int64_t n_members;
+    const int32_t* members;     /* [n_members] stacked control rows */
+    const double* member_coef;  /* [n_members] */
+    const double* params;       /* entity blob, params_len reals */
+    int64_t params_len;
+    int64_t n_entries;
+    const int32_t* r_entry;     /* [n_entries] reduction CSR entries */
+    const int32_t* comp;        /* [n_entries] component 0..dim-1 */
+    const int32_t* kt;          /* [n_entries] tangent slot 0..dim-2 */
+    const double* base;         /* [n_entries] frame-free coefficient */
+} egg_b200_control_slide;
+
+/* A wall face of a net: its nodes on `axis`/`side` are re-extended against
+ * the entity's projection of the spline every frame. */
+typedef struct egg_b200_control_wall_face {
+    int32_t net, axis, side, tag;
+    const double* params; /* entity blob */
+    int64_t params_len;
+} egg_b200_control_wall_face;
+
 typedef struct egg_b200_control_topo_desc {
     int32_t n_nets;
     int32_t reserved;
@@ -326,6 +362,16 @@ typedef struct egg_b200_control_topo_desc {
     int64_t p_nnz;
     const double* p_w;
     int64_t p_w_len;
+    /* sliding-wall frames (n_slide == 0: none; the rest is then unread) */
+    int32_t n_slide;
+    int32_t n_wall_faces;
+    const egg_b200_control_slide* slide;          /* [n_slide] */
+    const egg_b200_control_wall_face* wall_faces; /* [n_wall_faces] */
+    const int32_t* seam_face; /* [n_nets * 2 * dim]: face (axis, side) of each net lies on a seam */
+    const double* X0;         /* every net's exact node field, concatenated in net order */
+    int64_t X0_len;
+    const double* arena;      /* variable-length entity payloads */
+    int64_t arena_len;
 } egg_b200_control_topo_desc;
 
 /* Attach a multi-block control topology (the reference builds it inside the
@@ -352,6 +398,17 @@ int egg_b200_session_set_control_penalty(egg_b200_session* s, const int32_t* off
  * re-evaluate X (src/control_solve.hpp:2172 set_b; binding
  * src/bindings.cpp:1518-1530 set_control_b). */
 int egg_b200_session_set_control_b(egg_b200_session* s, int32_t net_index, const double* b, int64_t len);
+
+/* egg_b200_session_run_control with the options of the reference's full
+ * ControlOptions (src/control_solve.hpp:308-330): model_db switches the
+ * db/dC linearisation of a topology's sliding-wall frames, and frame_jumps
+ * (capacity n_outer) receives the energy jump of each frame rebuild
+ * (*n_frame_jumps entries; none without sliding-wall frames). */
+int egg_b200_session_run_control_ex(egg_b200_session* s, int32_t n_outer, int32_t objective, double grad_tol,
+                                    double alpha_min, double lm0, int32_t pcg_max_iter, double pcg_rtol,
+                                    int32_t pcg_forcing, int32_t model_db, double* energies, double* mindets,
+                                    double* alphas, double* pcg_iters, double* pcg_relres, int64_t* counts,
+                                    int32_t* iters, int32_t* converged, double* frame_jumps, int64_t* n_frame_jumps);
 
 /* The resident control lattice (prod(ctrl_shape) * dim reals; stacked over
  * the meshes of a batch or the nets of a topology): size, download, and

@@ -35,7 +35,11 @@ def check_report(got, want, what, rtol=RTOL, atol=ATOL):
         assert g.shape == w.shape, (what, k, g, w)
         np.testing.assert_allclose(g, w, rtol=rtol, atol=atol, err_msg=f"{what}.{k}")
     assert got["iters"] == want["iters"] and bool(got["converged"]) == bool(want["converged"]), (what, got, want)
-    assert len(got["frame_jumps"]) == len(want["frame_jumps"]) == 0
+    fg, fw = np.asarray(got["frame_jumps"]), np.asarray(want["frame_jumps"])
+    assert fg.shape == fw.shape, (what, fg, fw)
+    # a frame's jump is a difference of two energies: absolute at their scale
+    scale = float(np.abs(np.asarray(want["energies"])).max()) if len(want["energies"]) else 1.0
+    np.testing.assert_allclose(fg, fw, rtol=0, atol=rtol * scale + atol, err_msg=f"{what}.frame_jumps")
     gi, wi = np.asarray(got["pcg_iters"]), np.asarray(want["pcg_iters"])
     assert gi.shape == wi.shape, (what, gi, wi)
     assert np.all(np.abs(gi - wi) <= np.maximum(2, 0.05 * wi)), (what, gi, wi)
@@ -46,13 +50,31 @@ def check_report(got, want, what, rtol=RTOL, atol=ATOL):
     assert np.all(np.abs(np.log10(gr[pos] / wr[pos])) <= 1.0), (what, gr, wr)
 
 
+def _close(got, want, what, rtol, atol):
+    if isinstance(want, (tuple, list)):
+        assert isinstance(got, (tuple, list)) and len(got) == len(want), (what, got, want)
+        for i, (g, w) in enumerate(zip(got, want)):
+            _close(g, w, f"{what}[{i}]", rtol, atol)
+        return
+    g, w = np.asarray(got, dtype=np.float64), np.asarray(want, dtype=np.float64)
+    assert g.shape == w.shape, (what, g.shape, w.shape)
+    np.testing.assert_allclose(g, w, rtol=rtol, atol=atol, err_msg=what)
+
+
 def replay(core, events, scenario, rtol=RTOL, atol=ATOL, x_atol=1e-10):
-    """Replay one scenario's calls on `core`; returns the number compared."""
+    """Replay one scenario's calls on `core`; returns the number compared.
+    Free-function calls of the driver (entity projections) are compared at
+    the entity tests' 1e-10."""
     sessions = {}
     n = 0
     for ev in (e for e in events if e["scenario"] == scenario):
         if ev["op"] == "new":
             sessions[ev["sid"]] = core.CppStructuredSweepSession(*ev["args"], **ev["kwargs"])
+            continue
+        if ev["op"] == "fn":
+            got = getattr(core, ev["name"])(*ev["args"], **ev["kwargs"])
+            _close(got, ev["result"], f"{scenario}:{ev['name']}#{n}", 1e-10, 1e-12)
+            n += 1
             continue
         got = getattr(sessions[ev["sid"]], ev["name"])(*ev["args"], **ev["kwargs"])
         what = f"{scenario}:{ev['name']}#{n}"

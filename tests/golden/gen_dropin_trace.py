@@ -24,6 +24,7 @@ reference's Python does not travel there).
     python tests/golden/gen_dropin_trace.py [REFERENCE_ROOT]          # ref_dropin.pkl.gz
     python tests/golden/gen_dropin_trace.py --topo [REFERENCE_ROOT]   # ref_dropin_topo.pkl.gz
     python tests/golden/gen_dropin_trace.py --walls [REFERENCE_ROOT]  # ref_dropin_walls.pkl.gz
+    python tests/golden/gen_dropin_trace.py --slides [REFERENCE_ROOT] # ref_dropin_slides.pkl.gz
 
 (default: ``$EGG_REFERENCE_ROOT`` or a ``reference`` checkout beside this
 repository).  Test infrastructure only.
@@ -315,6 +316,40 @@ def record_walls(ref_root: Path) -> list[dict]:
     return rec.events
 
 
+TRACE_SLIDES = HERE / "ref_dropin_slides.pkl.gz"
+
+
+def record_slides(ref_root: Path) -> list[dict]:
+    """Topologies with sliding-wall frames and a 3D topology, through the
+    reference's own tests of its multi-block driver
+    (``tests/smoothing/test_control_topo_cpp.py``): a two-block seam whose
+    bottom rides a line segment (then the same grid with fixed walls), a
+    single block whose bottom rides a cubic B-spline, and a rotated 3D
+    two-block slab.  Each test runs as written (its assertions check the
+    reference core); the recorder keeps the calls."""
+    from oracle import oracle
+
+    ref = oracle.load_ref("fp64snap")
+    if ref is None:
+        raise SystemExit("oracle/_ref/fp64snap missing: run oracle/build_ref.sh first")
+    sys.path.insert(0, str(ref_root))
+    import egg._cpp  # noqa: F401
+
+    rec = Recorder(ref)
+    proxy = rec.module()
+    sys.modules["egg._cpp.cpp_core"] = proxy
+    sys.modules["egg._cpp"].cpp_core = proxy
+
+    from tests.smoothing import test_control_topo_cpp as t
+
+    for name, fn in (("line_seam", t.test_device_sliding_wall_roots),
+                     ("bspline_block", t.test_single_block_segmented_wall),
+                     ("slab3_rotated", t.test_device_3d_two_block_run)):
+        rec.scenario = name
+        fn()
+    return rec.events
+
+
 def _save(path: Path, events: list[dict]) -> None:
     with gzip.open(path, "wb") as f:
         pickle.dump({"events": events}, f, protocol=4)
@@ -335,5 +370,7 @@ if __name__ == "__main__":
         _save(TRACE_TOPO, record_topo(root))
     elif "--walls" in sys.argv:
         _save(TRACE_WALLS, record_walls(root))
+    elif "--slides" in sys.argv:
+        _save(TRACE_SLIDES, record_slides(root))
     else:
         _save(TRACE, record(root))

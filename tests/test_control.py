@@ -147,7 +147,7 @@ def _with_block(ctl, i, **kv):
     (lambda c: {**c, "r_off": np.asarray(c["r_off"])[:-1]}, ValueError, "malformed reduction CSR"),
     (lambda c: {**c, "p_off": np.array([0, 1]), "p_col": np.array([0]), "p_coef": np.array([1.0]),
                 "p_w": np.array([1.0, 1.0])}, ValueError, "malformed penalty CSR"),
-    (lambda c: {**c, "slide": []}, NotImplementedError, "slide"),
+    (lambda c: {**c, "slide": [], "wall_faces": [], "seam_face": [np.zeros(4, np.int32)]}, ValueError, "seam_face"),
 ])
 def test_malformed_topology_wire_is_refused_before_the_device(core, bad, exc, match):
     args, kwargs = _topo_new()
