@@ -25,6 +25,14 @@ _EVENTS = control_replay.load("ref_dropin_slides.pkl.gz")
 SCENARIOS = sorted({ev["scenario"] for ev in _EVENTS})
 
 
+# The B-spline wall's feet come from Newton iterations that round with each
+# compiler's FMA contraction (the entity tests hold them to 1e-10): the
+# lattice then agrees to ~1e-11 and the min det, a minimum over the samples
+# next to the wall, to ~1e-8 relative; energies and frame jumps to ~1e-14.
+_TOL = {"bspline_block": (1e-7, 1e-10)}
+
+
 @pytest.mark.parametrize("scenario", SCENARIOS)
 def test_reference_sliding_topology_replay(gpu, scenario):
-    assert control_replay.replay(gpu, _EVENTS, scenario) > 0
+    rtol, x_atol = _TOL.get(scenario, (control_replay.RTOL, 1e-10))
+    assert control_replay.replay(gpu, _EVENTS, scenario, rtol=rtol, x_atol=x_atol) > 0
