@@ -530,6 +530,91 @@ def cube_curved(n: int = 9, frac: float = 0.15, slide: float = 0.3, off: float =
     return Grid(f"cube_curved{n}", 3, g.blocks, X, g.free.copy(), {"frac": frac, "seed": seed}, cons)
 
 
+def _bsurf_points(pu, pv, ku, kv, ctrl, w, u, v):
+    """Points of a tensor-product B-spline / NURBS surface at (u[i], v[i])."""
+    from scipy.interpolate import BSpline
+
+    ctrl = np.asarray(ctrl, dtype=np.float64)
+    nu, nv = ctrl.shape[:2]
+    w = np.ones((nu, nv)) if w is None else np.asarray(w, dtype=np.float64).reshape(nu, nv)
+    Nu = BSpline.design_matrix(np.asarray(u), np.asarray(ku, dtype=np.float64), pu).toarray()
+    Nv = BSpline.design_matrix(np.asarray(v), np.asarray(kv, dtype=np.float64), pv).toarray()
+    num = np.einsum("pi,pj,ijc->pc", Nu, Nv, ctrl * w[..., None])
+    den = np.einsum("pi,pj,ij->p", Nu, Nv, w)
+    return num / den[:, None]
+
+
+def _bsurf_entity(pu, pv, ku, kv, ctrl, w=None, trim=None):
+    """(tag, record, seg) of a B-spline surface in the wire's SoA form
+    (tag 14: (pu, pv, nu, nv, 0, 0, 0, 0, has_w) and the knots_u, knots_v,
+    control net, weights, trim vertices and trim loop offsets fields)."""
+    ctrl = np.asarray(ctrl, dtype=np.float64)
+    nu, nv = ctrl.shape[:2]
+    rec = (float(pu), float(pv), float(nu), float(nv), 0.0, 0.0, 0.0, 0.0, 0.0 if w is None else 1.0)
+    verts = np.zeros(0) if trim is None else np.concatenate([np.asarray(lp, float).ravel() for lp in trim])
+    loops = np.zeros(0) if trim is None else np.concatenate([[0], np.cumsum([len(lp) for lp in trim])]).astype(float)
+    seg = (np.asarray(ku, dtype=np.float64), np.asarray(kv, dtype=np.float64), ctrl.reshape(-1),
+           np.zeros(0) if w is None else np.asarray(w, dtype=np.float64).reshape(-1), verts, loops)
+    return 14, rec, seg
+
+
+# The two surfaces of cube_bsurf: a bicubic bump over the top face and a
+# rational biquadratic (NURBS) sheet over the face x ~ 1, each spanning its
+# face with a margin.
+BSURF_TOP = dict(pu=3, pv=3, ku=[0, 0, 0, 0, 0.5, 1, 1, 1, 1], kv=[0, 0, 0, 0, 0.5, 1, 1, 1, 1])
+BSURF_SIDE = dict(pu=2, pv=2, ku=[0, 0, 0, 0.5, 1, 1, 1], kv=[0, 0, 0, 0.5, 1, 1, 1])
+
+
+def bsurf_nets():
+    g = np.linspace(-0.1, 1.1, 5)
+    top = np.zeros((5, 5, 3))
+    top[..., 0], top[..., 1] = np.meshgrid(g, g, indexing="ij")
+    bump = np.array([[0.0, 0.01, 0.02, 0.01, 0.0], [0.01, 0.05, 0.07, 0.04, 0.0], [0.02, 0.06, 0.1, 0.06, 0.02],
+                     [0.0, 0.03, 0.05, 0.04, 0.01], [0.0, 0.0, 0.02, 0.01, 0.0]])
+    top[..., 2] = 1.0 + bump
+    h = np.linspace(-0.1, 1.1, 4)
+    side = np.zeros((4, 4, 3))
+    side[..., 1], side[..., 2] = np.meshgrid(h, h, indexing="ij")
+    side[..., 0] = 1.0 + np.array([[0.0, 0.02, 0.02, 0.0], [0.01, 0.05, 0.04, 0.0],
+                                   [0.0, 0.04, 0.06, 0.01], [0.0, 0.0, 0.01, 0.0]])
+    w = np.array([[1.0, 0.9, 1.1, 1.0], [1.0, 1.2, 0.8, 1.0], [1.0, 0.85, 1.15, 1.0], [1.0, 1.0, 1.0, 1.0]])
+    return top, side, w
+
+
+def cube_bsurf(n: int = 9, frac: float = 0.15, slide: float = 0.3, off: float = 0.02, seed: int = 0) -> Grid:
+    """Unit cube whose top face slides on a bicubic B-spline surface (a bump
+    of up to 0.1 over z = 1) and whose face x ~ 1 slides on a rational
+    biquadratic NURBS sheet (B-spline surfaces, tag 14).  Face nodes sit on
+    the surfaces near their grid positions, moved along them by up to
+    ``slide`` h and off them by up to ``off`` h; the other faces and all edges
+    stay fixed."""
+    g = unit_cube(n, frac=frac, seed=seed)
+    ids = g.blocks[0]
+    X = g.X.copy()
+    h = 1.0 / (n - 1)
+    rng = np.random.default_rng(seed + 707)
+    inner = slice(1, -1)
+    top, side, w = bsurf_nets()
+    cons = {}
+    t = BSURF_TOP
+    nodes = ids[inner, inner, -1].reshape(-1)
+    uv = (X[nodes, :2] + 0.1) / 1.2 + rng.uniform(-slide, slide, (nodes.size, 2)) * h / 1.2
+    X[nodes] = _bsurf_points(t["pu"], t["pv"], t["ku"], t["kv"], top, None, uv[:, 0], uv[:, 1])
+    X[nodes, 2] += rng.uniform(-off, off, nodes.size) * h
+    ent = _bsurf_entity(t["pu"], t["pv"], t["ku"], t["kv"], top)
+    for v in nodes:
+        cons[int(v)] = ent
+    t = BSURF_SIDE
+    nodes = ids[-1, inner, inner].reshape(-1)
+    uv = (X[nodes, 1:] + 0.1) / 1.2 + rng.uniform(-slide, slide, (nodes.size, 2)) * h / 1.2
+    X[nodes] = _bsurf_points(t["pu"], t["pv"], t["ku"], t["kv"], side, w, uv[:, 0], uv[:, 1])
+    X[nodes, 0] += rng.uniform(-off, off, nodes.size) * h
+    ent = _bsurf_entity(t["pu"], t["pv"], t["ku"], t["kv"], side, w)
+    for v in nodes:
+        cons[int(v)] = ent
+    return Grid(f"cube_bsurf{n}", 3, g.blocks, X, g.free.copy(), {"frac": frac, "seed": seed}, cons)
+
+
 def two_cubes(n: int, frac: float = 0.2, seed: int = 0) -> Grid:
     """Two n^3 unit cubes sharing the x = 1 face (conforming 3D interface)."""
     t = np.linspace(0.0, 1.0, n)

@@ -347,6 +347,11 @@ __device__ void frame_entity(int tag, const double* rec, const double* arena, co
         foot[1] = fy;
         t[0][0] = tx;
         t[0][1] = ty;
+    } else if (tag == EGG_B200_TAG_BSPLINESURF) {
+        const BSplineSurf bs = bsurf_view(rec, arena);
+        double B[2][3], g2[3];
+        bsurf_project_frame(bs, p, foot, B);
+        bsurf_project_frame(bs, foot, g2, t);
     } else {
         entity3_project(tag, rec, p, foot);
         if (is_surf3(tag)) {

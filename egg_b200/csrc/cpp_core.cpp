@@ -256,6 +256,10 @@ void fill_desc(Desc& D, const py::dict& ctx, const py::dict& st, const DArr& X, 
                 if (tag == EGG_B200_TAG_COMPOSITE && seg_off.empty()) {
                     throw py::value_error("validate_context: a composite partition needs its arena seg field");
                 }
+                if (tag == EGG_B200_TAG_BSPLINESURF && seg_off.size() < 3) {
+                    throw py::value_error(
+                      "validate_context: a B-spline surface partition needs its knots_u, knots_v and ctrl seg fields");
+                }
                 for (py::ssize_t i = 0; i < dl.size(); ++i) {
                     const int32_t v = dl.data()[i];
                     if (v < 0 || v >= d.ndof) { throw py::value_error("validate_context: dof_local out of range"); }
@@ -273,6 +277,23 @@ void fill_desc(Desc& D, const py::dict& ctx, const py::dict& st, const DArr& X, 
                     }
                     if (tag == EGG_B200_TAG_COMPOSITE && !seg_off.empty()) {  // the entity's arena slice
                         er[6] = double(seg_base[0] + seg_off[0].data()[i]);
+                    }
+                    if (tag == EGG_B200_TAG_BSPLINESURF) {
+                        // knots_u, knots_v, ctrl, weights by arena offset; the UV
+                        // trim (vertices, loop offsets) through a header
+                        for (size_t k = 0; k < 4 && k < seg_off.size(); ++k) {
+                            er[4 + k] = double(seg_base[k] + seg_off[k].data()[i]);
+                        }
+                        er[9] = -1.0;
+                        if (seg_off.size() >= 6) {
+                            const int64_t nl = seg_off[5].data()[i + 1] - seg_off[5].data()[i];
+                            if (nl >= 2) {
+                                er[9] = double(D.arena.size());
+                                D.arena.push_back(double(nl));
+                                D.arena.push_back(double(seg_base[5] + seg_off[5].data()[i]));
+                                D.arena.push_back(double(seg_base[4] + seg_off[4].data()[i]));
+                            }
+                        }
                     }
                 }
             }
@@ -414,6 +435,8 @@ void fill_control(egg_b200_control_desc& c, Keep& keep, const py::dict& w, int d
 // by the sliding-wall frames) is checked for size and otherwise unused.
 struct TopoWire {
     std::vector<egg_b200_control_desc> nets;
+    std::vector<double> arena;                  // the wire's arena plus B-spline-surface trim headers
+    std::vector<std::vector<double>> surf_rec;  // converted B-spline-surface records
     std::vector<egg_b200_control_slide> slide;
     std::vector<egg_b200_control_wall_face> wall_faces;
     std::vector<int32_t> seam;
@@ -426,7 +449,31 @@ struct TopoWire {
 // per-net seam flags, the entity arena and every net's X0.
 void fill_topo_slides(TopoWire& t, Keep& keep, const py::dict& w, int dim, const std::vector<int64_t>& n_nodes)
 {
-    if (w.contains("arena")) { t.d.arena = keep.reals(w["arena"], &t.d.arena_len); }
+    if (w.contains("arena")) {
+        int64_t na = 0;
+        const double* a = keep.reals(w["arena"], &na);
+        t.arena.assign(a, a + na);
+    }
+    // A 3D B-spline surface blob (pu, pv, nu, nv, ku_off, kv_off, ctrl_off,
+    // w_off, has_w, trim_v_off, trim_l_off, n_trim_loop_entries;
+    // egg/smoothing/control_backend.py _encode_frame_entity) becomes this
+    // core's record, its trim reached through a header in the arena.
+    auto record = [&](int tag, const double* params, int64_t& len) -> const double* {
+        if (dim != 3 || tag != EGG_B200_TAG_BSPLINESURF) { return params; }
+        if (len < 9) { throw py::value_error("control topo: B-spline surface blob too short"); }
+        std::vector<double> r(EGG_B200_ENTITY_FIELDS, 0.0);
+        for (int k = 0; k < 9; ++k) { r[size_t(k)] = params[k]; }
+        r[9] = -1.0;
+        if (len >= 12 && params[11] >= 2) {
+            r[9] = double(t.arena.size());
+            t.arena.push_back(params[11]);
+            t.arena.push_back(params[10]);
+            t.arena.push_back(params[9]);
+        }
+        t.surf_rec.push_back(std::move(r));  // moving the outer vector keeps each record's buffer
+        len = EGG_B200_ENTITY_FIELDS;
+        return t.surf_rec.back().data();
+    };
     for (const py::handle item : w["slide"].cast<py::list>()) {
         const py::dict sd = item.cast<py::dict>();
         egg_b200_control_slide r {};
@@ -436,6 +483,7 @@ void fill_topo_slides(TopoWire& t, Keep& keep, const py::dict& w, int dim, const
         r.member_coef = keep.reals(sd["member_coef"], &nc);
         r.tag = sd["tag"].cast<int32_t>();
         r.params = keep.reals(sd["params"], &r.params_len);
+        r.params = record(r.tag, r.params, r.params_len);
         r.r_entry = keep.ints(sd["r_entry"], &r.n_entries);
         r.comp = keep.ints(sd["comp"], &ncomp);
         r.kt = keep.ints(sd["kt"], &nk);
@@ -453,6 +501,7 @@ void fill_topo_slides(TopoWire& t, Keep& keep, const py::dict& w, int dim, const
         f.side = wd["side"].cast<int32_t>();
         f.tag = wd["tag"].cast<int32_t>();
         f.params = keep.reals(wd["params"], &f.params_len);
+        f.params = record(f.tag, f.params, f.params_len);
         t.wall_faces.push_back(f);
     }
     const py::list seams = w["seam_face"].cast<py::list>();
@@ -481,6 +530,8 @@ void fill_topo_slides(TopoWire& t, Keep& keep, const py::dict& w, int dim, const
     t.d.seam_face = t.seam.data();
     t.d.X0 = t.X0.data();
     t.d.X0_len = int64_t(t.X0.size());
+    t.d.arena = t.arena.empty() ? nullptr : t.arena.data();
+    t.d.arena_len = int64_t(t.arena.size());
 }
 
 void fill_control_topo(TopoWire& t, Keep& keep, const py::dict& w, int dim)
@@ -1350,6 +1401,7 @@ PYBIND11_MODULE(cpp_core, m)
               rec[size_t(i)] = records.data()[i];
           }
           int k = 0;
+          std::vector<double> seg_at, seg_len;
           for (auto item : seg) {
               py::dict sd = item.cast<py::dict>();
               DArr data = DArr::ensure(sd["data"]);
@@ -1361,11 +1413,23 @@ PYBIND11_MODULE(cpp_core, m)
               const double base = double(arena.size());
               if (tag == EGG_B200_TAG_BSPLINE && k < 3) { rec[size_t(6 + k)] = base; }
               if (tag == EGG_B200_TAG_COMPOSITE && k == 0) { rec[6] = base; }
+              if (tag == EGG_B200_TAG_BSPLINESURF && k < 4) { rec[size_t(4 + k)] = base; }
+              seg_at.push_back(base);
+              seg_len.push_back(double(off.data()[1] - off.data()[0]));
               arena.insert(arena.end(), data.data() + off.data()[0], data.data() + off.data()[1]);
               ++k;
           }
+          if (tag == EGG_B200_TAG_BSPLINESURF) {  // the UV trim through its header
+              rec[9] = -1.0;
+              if (seg_at.size() >= 6 && seg_len[5] >= 2) {
+                  rec[9] = double(arena.size());
+                  arena.push_back(seg_len[5]);
+                  arena.push_back(seg_at[5]);
+                  arena.push_back(seg_at[4]);
+              }
+          }
           const bool surf = d == 3 && (tag == EGG_B200_TAG_PLANE || tag == EGG_B200_TAG_SPHERE ||
-                                       tag == EGG_B200_TAG_CYLINDER);
+                                       tag == EGG_B200_TAG_CYLINDER || tag == EGG_B200_TAG_BSPLINESURF);
           const int K = surf ? 2 : 1;
           py::array_t<double> feet({n, py::ssize_t(d)});
           py::array_t<double> basis({n, py::ssize_t(d), py::ssize_t(K)});

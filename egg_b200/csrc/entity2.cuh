@@ -747,7 +747,7 @@ EGG_HD bool entity_supported(int dim, int tag)
 {
     if (dim == 3) {
         return tag == EGG_B200_TAG_PLANE || tag == EGG_B200_TAG_SPHERE || tag == EGG_B200_TAG_CYLINDER ||
-               tag == EGG_B200_TAG_LINE3 || tag == EGG_B200_TAG_LINERAIL3;
+               tag == EGG_B200_TAG_LINE3 || tag == EGG_B200_TAG_LINERAIL3 || tag == EGG_B200_TAG_BSPLINESURF;
     }
     return dim == 2 && (tag == EGG_B200_TAG_LINESEG || tag == EGG_B200_TAG_CIRCLE ||
                         tag == EGG_B200_TAG_ELLIPSE || tag == EGG_B200_TAG_LINERAIL || is_tcurve(tag) ||

@@ -304,4 +304,434 @@ EGG_HD void param3_warm_step(int tag, const double* e, const double h[6], const 
     dq[1] *= omega;
 }
 
+// ---- B-spline / NURBS surfaces (tag 14) -------------------------------------
+// Record: (pu, pv, nu, nv, ku_at, kv_at, ctrl_at, w_at, has_w, trim_at), the
+// *_at fields arena offsets of the knot vectors (nu + pu + 1, nv + pv + 1),
+// the control net (3 nu nv, u-major) and the weights (nu nv); trim_at < 0
+// for an untrimmed surface, else the offset of (n_loop_entries, loops_at,
+// verts_at): the UV trim polygon's loop offsets [0, n0, n0 + n1, ..., total]
+// and its vertices (u, v) (src/geometry.hpp:1095-1420, decode :1616-1650,
+// trim :144-191).  Evaluation by the tensor product of the curve bases
+// (The NURBS Book A2.3 in each direction, the rational form by the
+// quotient rule); the foot by Newton on ((S - p) . S_u, (S - p) . S_v) = 0:
+// Gauss-Newton from a seed (the DOF's last foot), else from the 4 best of a
+// 9 x 9 parameter grid polished by damped Newton (Levenberg-Marquardt with
+// residual backtracking), the nearest foot winning.
+constexpr double kSurfTiny = 1e-30;    // det / denominator floor
+constexpr double kSurfNewton = 1e-9;   // |dq| break of the foot iterations
+
+struct BSplineSurf {
+    BSplineCurve u, v;  // degree, count and knots per direction
+    int nu, nv;
+    const double* ctrl;
+    const double* w;       // NULL: polynomial
+    const double* loops;   // NULL: untrimmed
+    const double* verts;
+    int n_loop;
+};
+
+// Host check of a tag-14 record against its arena: integral degrees in
+// 1..kBSplineMaxDegree with more controls than the degree, and every
+// addressed span (knots, net, weights, trim header, loops, vertices) inside
+// the arena, the loop offsets non-decreasing from 0.
+inline bool bsurf_record_ok(const double* e, const double* arena, int64_t len)
+{
+    auto integral = [](double x) { return std::isfinite(x) && double(int64_t(x)) == x; };
+    auto span_ok = [&](double at, double n) { return integral(at) && at >= 0.0 && n >= 0.0 && at + n <= double(len); };
+    for (int k = 0; k < 9; ++k) {
+        if (k != 8 && !integral(e[k])) { return false; }
+    }
+    const double pu = e[0], pv = e[1], nu = e[2], nv = e[3];
+    if (pu < 1 || pu > kBSplineMaxDegree || pv < 1 || pv > kBSplineMaxDegree || nu < pu + 1 || nv < pv + 1 ||
+        nu * nv > 1e9) {
+        return false;
+    }
+    if (!arena || !span_ok(e[4], nu + pu + 1) || !span_ok(e[5], nv + pv + 1) || !span_ok(e[6], 3 * nu * nv) ||
+        (e[8] != 0.0 && !span_ok(e[7], nu * nv))) {
+        return false;
+    }
+    if (!(e[9] >= 0.0)) { return true; }
+    if (!span_ok(e[9], 3)) { return false; }
+    const double* h = arena + int64_t(e[9]);
+    const double nl = h[0];
+    if (!integral(nl) || nl < 2 || !span_ok(h[1], nl)) { return false; }
+    const double* loops = arena + int64_t(h[1]);
+    if (loops[0] != 0.0) { return false; }
+    for (int64_t l = 0; l + 1 < int64_t(nl); ++l) {
+        if (!integral(loops[l + 1]) || loops[l + 1] < loops[l]) { return false; }
+    }
+    return span_ok(h[2], 2.0 * loops[int64_t(nl) - 1]);
+}
+
+EGG_HD BSplineSurf bsurf_view(const double* e, const double* arena)
+{
+    BSplineSurf s;
+    s.u.p = int(e[0]);
+    s.v.p = int(e[1]);
+    s.nu = s.u.n = int(e[2]);
+    s.nv = s.v.n = int(e[3]);
+    s.u.knots = arena + int64_t(e[4]);
+    s.v.knots = arena + int64_t(e[5]);
+    s.u.ctrl = s.v.ctrl = nullptr;
+    s.u.w = s.v.w = nullptr;
+    s.ctrl = arena + int64_t(e[6]);
+    s.w = e[8] != 0.0 ? arena + int64_t(e[7]) : nullptr;
+    s.loops = s.verts = nullptr;
+    s.n_loop = 0;
+    if (e[9] >= 0.0) {
+        const double* h = arena + int64_t(e[9]);
+        s.n_loop = int(h[0]);
+        s.loops = arena + int64_t(h[1]);
+        s.verts = arena + int64_t(h[2]);
+    }
+    return s;
+}
+
+// Surface partials S00, S10, S01, S20, S02, S11 (rows 0..5) up to order nd.
+EGG_OUTLINE void bsurf_ders(const BSplineSurf& s, const double q[2], int nd, double S[6][3])
+{
+    const int su = bspline_span(s.u, q[0]), sv = bspline_span(s.v, q[1]);
+    double du[3][kBSplineCap], dv[3][kBSplineCap];
+    bspline_basis(s.u, su, q[0], nd, du);
+    bspline_basis(s.v, sv, q[1], nd, dv);
+    double A[6][3] = {}, wsum[6] = {};
+    for (int i = 0; i <= s.u.p; ++i) {
+        const int iu = su - s.u.p + i;
+        for (int j = 0; j <= s.v.p; ++j) {
+            const int iv = sv - s.v.p + j;
+            const int64_t c = int64_t(iu) * s.nv + iv;
+            const double wt = s.w ? s.w[c] : 1.0;
+            const double Pw[3] = {wt * s.ctrl[3 * c], wt * s.ctrl[3 * c + 1], wt * s.ctrl[3 * c + 2]};
+            double n[6];
+            n[0] = du[0][i] * dv[0][j];
+            if (nd >= 1) {
+                n[1] = du[1][i] * dv[0][j];
+                n[2] = du[0][i] * dv[1][j];
+            }
+            if (nd >= 2) {
+                n[5] = du[1][i] * dv[1][j];
+                n[3] = du[2][i] * dv[0][j];
+                n[4] = du[0][i] * dv[2][j];
+            }
+            const int rows = nd == 0 ? 1 : (nd == 1 ? 3 : 6);
+            for (int r = 0; r < rows; ++r) {
+                for (int k = 0; k < 3; ++k) { A[r][k] = A[r][k] + n[r] * Pw[k]; }
+                wsum[r] += n[r] * wt;
+            }
+        }
+    }
+    if (!s.w) {
+        for (int r = 0; r < 6; ++r) {
+            for (int k = 0; k < 3; ++k) { S[r][k] = A[r][k]; }
+        }
+        return;
+    }
+    const double iw = 1.0 / wsum[0];
+    for (int k = 0; k < 3; ++k) { S[0][k] = iw * A[0][k]; }
+    if (nd >= 1) {
+        for (int k = 0; k < 3; ++k) {
+            S[1][k] = iw * (A[1][k] - wsum[1] * S[0][k]);
+            S[2][k] = iw * (A[2][k] - wsum[2] * S[0][k]);
+        }
+    }
+    if (nd >= 2) {
+        for (int k = 0; k < 3; ++k) {
+            S[5][k] = iw * (A[5][k] - wsum[1] * S[2][k] - wsum[2] * S[1][k] - wsum[5] * S[0][k]);
+            S[3][k] = iw * (A[3][k] - 2.0 * wsum[1] * S[1][k] - wsum[3] * S[0][k]);
+            S[4][k] = iw * (A[4][k] - 2.0 * wsum[2] * S[2][k] - wsum[4] * S[0][k]);
+        }
+    }
+}
+
+EGG_HD void bsurf_eval(const BSplineSurf& s, const double q[2], double out[3])
+{
+    double S[6][3];
+    bsurf_ders(s, q, 0, S);
+    for (int k = 0; k < 3; ++k) { out[k] = S[0][k]; }
+}
+
+EGG_HD void bsurf_domain(const BSplineSurf& s, double& u0, double& u1, double& v0, double& v1)
+{
+    u0 = s.u.knots[s.u.p];
+    u1 = s.u.knots[s.nu];
+    v0 = s.v.knots[s.v.p];
+    v1 = s.v.knots[s.nv];
+}
+
+EGG_HD double clampd(double x, double lo, double hi) { return x < lo ? lo : (x > hi ? hi : x); }
+
+// Even-odd test of (u, v) against the trim loops; untrimmed contains all.
+EGG_HD bool bsurf_contains(const BSplineSurf& s, const double q[2])
+{
+    if (s.n_loop < 2) { return true; }
+    bool inside = false;
+    for (int l = 0; l + 1 < s.n_loop; ++l) {
+        const int lo = int(s.loops[l]), hi = int(s.loops[l + 1]);
+        for (int i = lo, j = hi - 1; i < hi; j = i++) {
+            const double au = s.verts[2 * i], av = s.verts[2 * i + 1], bu = s.verts[2 * j], bv = s.verts[2 * j + 1];
+            if ((av > q[1]) != (bv > q[1]) && q[0] < ((bu - au) * (q[1] - av) / (bv - av)) + au) { inside = !inside; }
+        }
+    }
+    return inside;
+}
+
+// Nearest point of the trim loops' polylines (closed loops); untrimmed: q.
+EGG_HD void bsurf_trim_clamp(const BSplineSurf& s, double q[2])
+{
+    double bu = q[0], bv = q[1], best = INFINITY;
+    for (int l = 0; l + 1 < s.n_loop; ++l) {
+        const int lo = int(s.loops[l]), hi = int(s.loops[l + 1]);
+        for (int i = lo, j = hi - 1; i < hi; j = i++) {
+            const double au = s.verts[2 * j], av = s.verts[2 * j + 1];
+            const double eu = s.verts[2 * i] - au, ev = s.verts[2 * i + 1] - av;
+            const double ab = eu * eu + ev * ev;
+            double t = ab > kSurfTiny ? ((q[0] - au) * eu + (q[1] - av) * ev) / ab : 0.0;
+            t = clampd(t, 0.0, 1.0);
+            const double pu = au + t * eu, pv = av + t * ev;
+            const double du = pu - q[0], dv = pv - q[1];
+            const double dd = du * du + dv * dv;
+            if (dd < best) {
+                best = dd;
+                bu = pu;
+                bv = pv;
+            }
+        }
+    }
+    q[0] = bu;
+    q[1] = bv;
+}
+
+// Newton on the foot conditions from q, iterates clamped to the domain,
+// stopping when the clamped iterate moves less than kSurfNewton or the
+// Jacobian is singular.  EXACT adds the curvature terms (d . S_uv...).  J
+// receives the raw frame (S_u, S_v) of the last iterate evaluated.
+EGG_OUTLINE void bsurf_newton(const BSplineSurf& s, const double* p, double q[2], bool exact, double J[2][3])
+{
+    double u0, u1, v0, v1;
+    bsurf_domain(s, u0, u1, v0, v1);
+    for (int it = 0; it < 12; ++it) {
+        double S[6][3];
+        bsurf_ders(s, q, exact ? 2 : 1, S);
+        for (int k = 0; k < 3; ++k) {
+            J[0][k] = S[1][k];
+            J[1][k] = S[2][k];
+        }
+        const double d[3] = {S[0][0] - p[0], S[0][1] - p[1], S[0][2] - p[2]};
+        const double f1 = dot3v(d, S[1]), f2 = dot3v(d, S[2]);
+        double j11 = dot3v(S[1], S[1]), j12 = dot3v(S[1], S[2]), j22 = dot3v(S[2], S[2]);
+        if (exact) {
+            j11 += dot3v(d, S[3]);
+            j12 += dot3v(d, S[5]);
+            j22 += dot3v(d, S[4]);
+        }
+        const double det = j11 * j22 - j12 * j12;
+        if (fabs(det) < kSurfTiny) { break; }
+        const double qu = clampd(q[0] - (j22 * f1 - j12 * f2) / det, u0, u1);
+        const double qv = clampd(q[1] - (-j12 * f1 + j11 * f2) / det, v0, v1);
+        const bool done = fabs(qu - q[0]) + fabs(qv - q[1]) < kSurfNewton;
+        q[0] = qu;
+        q[1] = qv;
+        if (done) { break; }
+    }
+}
+
+// Damped Newton from one seed (cold multi-start only): the damping bridges
+// Gauss-Newton and gradient descent, and a step is kept only if it lowers
+// |S - p|^2 (up to 6 damping increases per iteration).
+EGG_OUTLINE void bsurf_newton_lm(const BSplineSurf& s, const double* p, double q[2], double J[2][3])
+{
+    double u0, u1, v0, v1;
+    bsurf_domain(s, u0, u1, v0, v1);
+    q[0] = clampd(q[0], u0, u1);
+    q[1] = clampd(q[1], v0, v1);
+    double S[6][3];
+    bsurf_ders(s, q, 2, S);
+    double d[3] = {S[0][0] - p[0], S[0][1] - p[1], S[0][2] - p[2]};
+    double r = dot3v(d, d);
+    double lambda = 1e-3 * (dot3v(S[1], S[1]) + dot3v(S[2], S[2]) + kSurfTiny);
+    for (int it = 0; it < 16; ++it) {
+        const double f1 = dot3v(d, S[1]), f2 = dot3v(d, S[2]);
+        const double j11 = dot3v(S[1], S[1]) + dot3v(d, S[3]);
+        const double j12 = dot3v(S[1], S[2]) + dot3v(d, S[5]);
+        const double j22 = dot3v(S[2], S[2]) + dot3v(d, S[4]);
+        double du = 0.0, dv = 0.0;
+        bool accepted = false;
+        for (int bt = 0; bt < 6; ++bt) {
+            const double a11 = j11 + lambda, a22 = j22 + lambda;
+            const double det = a11 * a22 - j12 * j12;
+            if (fabs(det) < kSurfTiny) {
+                lambda *= 4.0;
+                continue;
+            }
+            du = -((a22 * f1 - j12 * f2) / det);
+            dv = -((-j12 * f1 + a11 * f2) / det);
+            const double qn[2] = {clampd(q[0] + du, u0, u1), clampd(q[1] + dv, v0, v1)};
+            double e[3];
+            bsurf_eval(s, qn, e);
+            const double dn[3] = {e[0] - p[0], e[1] - p[1], e[2] - p[2]};
+            const double rn = dot3v(dn, dn);
+            if (rn < r) {
+                q[0] = qn[0];
+                q[1] = qn[1];
+                r = rn;
+                bsurf_ders(s, q, 2, S);
+                for (int k = 0; k < 3; ++k) { d[k] = S[0][k] - p[k]; }
+                lambda = fmax(lambda * 0.3, kSurfTiny);
+                accepted = true;
+                break;
+            }
+            lambda *= 4.0;
+        }
+        if (!accepted || fabs(du) + fabs(dv) < kSurfNewton) { break; }
+    }
+    for (int k = 0; k < 3; ++k) {
+        J[0][k] = S[1][k];
+        J[1][k] = S[2][k];
+    }
+}
+
+// Foot parameter of p (src/geometry.hpp:1342-1420 invert_seeded): from the
+// seed when there is one (Gauss-Newton), else the multi-start search; J is
+// the raw frame the chosen iteration saw last.
+EGG_OUTLINE void bsurf_invert(const BSplineSurf& s, const double* p, const double seed[2], bool has_seed, double q[2],
+                              double J[2][3])
+{
+    double u0, u1, v0, v1;
+    bsurf_domain(s, u0, u1, v0, v1);
+    if (has_seed) {
+        q[0] = clampd(seed[0], u0, u1);
+        q[1] = clampd(seed[1], v0, v1);
+        bsurf_newton(s, p, q, false, J);
+        return;
+    }
+    constexpr int kGrid = 8, kStarts = 4;
+    double bestd[kStarts], bestq[kStarts][2];
+    for (int k = 0; k < kStarts; ++k) {
+        bestd[k] = INFINITY;
+        bestq[k][0] = u0;
+        bestq[k][1] = v0;
+    }
+    for (int i = 0; i <= kGrid; ++i) {
+        for (int j = 0; j <= kGrid; ++j) {
+            const double t[2] = {u0 + ((u1 - u0) * i) / kGrid, v0 + ((v1 - v0) * j) / kGrid};
+            double e[3];
+            bsurf_eval(s, t, e);
+            const double dx[3] = {e[0] - p[0], e[1] - p[1], e[2] - p[2]};
+            const double dd = dot3v(dx, dx);
+            if (dd < bestd[kStarts - 1]) {
+                int k = kStarts - 1;
+                for (; k > 0 && dd < bestd[k - 1]; --k) {
+                    bestd[k] = bestd[k - 1];
+                    bestq[k][0] = bestq[k - 1][0];
+                    bestq[k][1] = bestq[k - 1][1];
+                }
+                bestd[k] = dd;
+                bestq[k][0] = t[0];
+                bestq[k][1] = t[1];
+            }
+        }
+    }
+    q[0] = u0;
+    q[1] = v0;
+    double best = INFINITY;
+    for (int k = 0; k < kStarts; ++k) {
+        if (bestd[k] == INFINITY) { continue; }
+        double f[2] = {bestq[k][0], bestq[k][1]}, Jk[2][3];
+        bsurf_newton_lm(s, p, f, Jk);
+        double e[3];
+        bsurf_eval(s, f, e);
+        const double dx[3] = {e[0] - p[0], e[1] - p[1], e[2] - p[2]};
+        const double dd = dot3v(dx, dx);
+        if (dd < best) {
+            best = dd;
+            q[0] = f[0];
+            q[1] = f[1];
+            for (int a = 0; a < 2; ++a) {
+                for (int c = 0; c < 3; ++c) { J[a][c] = Jk[a][c]; }
+            }
+        }
+    }
+}
+
+// Seeded projection / tangent basis of a constrained DOF (the seed becomes
+// the unclamped foot; a foot outside the trim is clamped onto it): the
+// world-space path of the first sweep of a run call and of cold trials
+// (src/geometry.hpp:230-260).
+EGG_OUTLINE void bsurf_foot_seeded(const BSplineSurf& s, const double* p, double seed[2], double q[2])
+{
+    const bool has = isfinite(seed[0]);
+    double J[2][3];
+    bsurf_invert(s, p, seed, has, q, J);
+    seed[0] = q[0];
+    seed[1] = q[1];
+    if (!bsurf_contains(s, q)) { bsurf_trim_clamp(s, q); }
+}
+
+EGG_HD void bsurf_project_seeded(const BSplineSurf& s, const double* p, double seed[2], double out[3])
+{
+    double q[2];
+    bsurf_foot_seeded(s, p, seed, q);
+    bsurf_eval(s, q, out);
+}
+
+EGG_HD void bsurf_basis_at(const BSplineSurf& s, const double q[2], double B[2][3])
+{
+    double S[6][3];
+    bsurf_ders(s, q, 1, S);
+    const double J[2][3] = {{S[1][0], S[1][1], S[1][2]}, {S[2][0], S[2][1], S[2][2]}};
+    p3_basis(EGG_B200_TAG_PLANE, J, B);
+}
+
+// Warm step of a B-spline-surface DOF (src/sweep.hpp:1785-1832): foot q* and
+// raw frame J from Gauss-Newton off the seed (the seed becomes q*), the
+// Newton step on the orthonormalised J, reduced to dq = (J^T J)^-1 J^T delta
+// and damped by omega.
+EGG_HD void bsurf_warm_step(const BSplineSurf& s, const double h[6], const double g[3], const double* pos,
+                            double omega, double seed[2], double qstar[2], double dq[2])
+{
+    double J[2][3], B[2][3], d[3];
+    bsurf_invert(s, pos, seed, true, qstar, J);
+    seed[0] = qstar[0];
+    seed[1] = qstar[1];
+    const double H[9] = {h[0], h[1], h[2], h[1], h[3], h[4], h[2], h[4], h[5]};
+    p3_basis(EGG_B200_TAG_PLANE, J, B);
+    step_from_basis3<2>(g, H, B, d);
+    double M[4], b[2];
+    for (int a = 0; a < 2; ++a) {
+        for (int c = 0; c < 2; ++c) { M[a * 2 + c] = dot3v(J[a], J[c]); }
+        b[a] = dot3v(J[a], d);
+    }
+    dq[0] = dq[1] = 0.0;
+    const double det = M[0] * M[3] - M[1] * M[2];
+    if (!(fabs(det) < kGeomTiny)) {
+        const double inv = 1.0 / det;
+        dq[0] = inv * (M[3] * b[0] - M[1] * b[1]);
+        dq[1] = inv * (-M[2] * b[0] + M[0] * b[1]);
+    }
+    dq[0] *= omega;
+    dq[1] *= omega;
+}
+
+// Cold step of a B-spline-surface DOF (the first sweep of a run call): the
+// seeded foot's orthonormal frame (the seed becomes the foot), the Newton
+// step on it.
+EGG_HD void bsurf_cold_step(const BSplineSurf& s, const double h[6], const double g[3], const double* pos,
+                            double seed[2], double d[3])
+{
+    double q[2], B[2][3];
+    bsurf_foot_seeded(s, pos, seed, q);
+    bsurf_basis_at(s, q, B);
+    const double H[9] = {h[0], h[1], h[2], h[1], h[3], h[4], h[2], h[4], h[5]};
+    step_from_basis3<2>(g, H, B, d);
+}
+
+// Cold projection without a seed and its basis (src/geometry.hpp:204-222).
+EGG_HD void bsurf_project_frame(const BSplineSurf& s, const double* p, double foot[3], double B[2][3])
+{
+    double seed[2] = {NAN, NAN}, q[2];
+    bsurf_foot_seeded(s, p, seed, q);
+    bsurf_eval(s, q, foot);
+    bsurf_basis_at(s, q, B);
+}
+
 }  // namespace egg_b200

@@ -442,6 +442,8 @@ struct StoredPatch3 {
     const double* epar;  // [n * EGG_B200_ENTITY_FIELDS] entity records
     int cold;            // first sweep of a run call: parametric entities project in world space
     SoftTable soft;      // directional terms per DOF (off == NULL: none)
+    const double* arena; // entity arena (B-spline surfaces)
+    double* seeds;       // [n * 2] last foot parameter of each B-spline-surface DOF (NaN: none)
 };
 
 __device__ __forceinline__ void assemble_T3(const double* X, int32_t ic, const int32_t in[3], const double s[3],
@@ -554,11 +556,30 @@ __global__ void stored3_kernel(StoredPatch3 sp, const double* __restrict__ Xin, 
         // first sweep of a run call searches in its parameters.
         // CON = false (a level without constrained DOFs) compiles none of it.
         const double* er = sp.epar + (etag != 0 ? d * EGG_B200_ENTITY_FIELDS : 0);
-        const bool warm_param = is_param3(etag) && !sp.cold;
+        // A B-spline surface carries its foot parameter from sweep to sweep
+        // (src/sweep.hpp:1221-1265): the first sweep of a run call steps on
+        // the seeded foot's frame and projects every trial from the seed,
+        // which each projection advances; later sweeps search in its
+        // parameters, every trial clamped onto the trim polygon
+        // (src/sweep.hpp:1820-1832: the clamp applies inside the trim too).
+        const bool bsurf = etag == EGG_B200_TAG_BSPLINESURF;
+        BSplineSurf bs {};
+        double seed[2] = {NAN, NAN};
+        if (bsurf) {
+            bs = bsurf_view(er, sp.arena);
+            seed[0] = sp.seeds[2 * d];
+            seed[1] = sp.seeds[2 * d + 1];
+        }
+        const bool warm_param = (is_param3(etag) || (bsurf && isfinite(seed[0]))) && !sp.cold;
         double dl[3] = {0.0, 0.0, 0.0};
         double qs[2] = {0.0, 0.0}, dq[2] = {0.0, 0.0};
         if (etag == 0) {
             solve3<double>(h, g, dl);
+        } else if (bsurf && warm_param) {
+            bsurf_warm_step(bs, h, g, pos, omega, seed, qs, dq);
+        } else if (bsurf) {
+            bsurf_cold_step(bs, h, g, pos, seed, dl);
+            for (int q = 0; q < 3; ++q) { dl[q] *= omega; }
         } else if (warm_param) {
             param3_warm_step(etag, er, h, g, pos, omega, qs, dq);
         } else {
@@ -569,7 +590,14 @@ __global__ void stored3_kernel(StoredPatch3 sp, const double* __restrict__ Xin, 
         double cur[3] = {pos[0], pos[1], pos[2]};
         for (int it = 0; it < 10; ++it) {
             double tr[3] = {pos[0] + alpha * dl[0], pos[1] + alpha * dl[1], pos[2] + alpha * dl[2]};
-            if (warm_param) {
+            if (bsurf && warm_param) {
+                double qt[2] = {qs[0] + alpha * dq[0], qs[1] + alpha * dq[1]};
+                bsurf_trim_clamp(bs, qt);
+                bsurf_eval(bs, qt, tr);
+            } else if (bsurf) {
+                const double raw[3] = {tr[0], tr[1], tr[2]};
+                bsurf_project_seeded(bs, raw, seed, tr);
+            } else if (warm_param) {
                 double qt[2] = {qs[0] + alpha * dq[0], qs[1] + alpha * dq[1]};
                 p3_clamp(etag, er, qt);
                 p3_eval(etag, er, qt, tr);
@@ -602,6 +630,10 @@ __global__ void stored3_kernel(StoredPatch3 sp, const double* __restrict__ Xin, 
         if (lane == 0) {
             for (int q = 0; q < 3; ++q) {
                 Xout[3 * int64_t(slot) + q] = etag != 0 ? cur[q] : pos[q] + omega * (cur[q] - pos[q]);
+            }
+            if (bsurf) {
+                sp.seeds[2 * d] = seed[0];
+                sp.seeds[2 * d + 1] = seed[1];
             }
         }
     }

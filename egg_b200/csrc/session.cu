@@ -766,7 +766,7 @@ static Session* create_session(const egg_b200_session_desc& d)
                 throw Error(EGG_B200_ENOTSUP, "egg_b200: constrained entity tag " + std::to_string(etag) +
                                                 " is not supported in " + std::to_string(D) +
                                                 "D (this core relaxes the 2D LineSeg, Circle, Ellipse, CircleArc, EllipseArc, QuadBezier, CubicBezier, BSpline, "
-                                                "LineRail and the 3D Plane, Sphere, Cylinder, Line3, LineRail3)");
+                                                "LineRail and the 3D Plane, Sphere, Cylinder, Line3, LineRail3, BSplineSurface)");
             }
             if (!d.entity_params) { invalid("validate_context: constrained DOF without entity_params"); }
             for (int f = 0; f < EGG_B200_ENTITY_FIELDS; ++f) {
@@ -803,6 +803,13 @@ static Session* create_session(const egg_b200_session_desc& d)
                             invalid("validate_context: a composite B-spline segment's data lies outside entity_arena");
                         }
                     }
+                }
+            }
+            if (etag == EGG_B200_TAG_BSPLINESURF) {
+                const double* r = d.entity_params + i * EGG_B200_ENTITY_FIELDS;
+                if (!bsurf_record_ok(r, d.entity_arena, d.entity_arena_len)) {
+                    invalid("validate_context: B-spline surface degrees (1.." + std::to_string(kBSplineMaxDegree) +
+                            "), control net, knots, weights or trim polygon outside entity_arena");
                 }
             }
             if (etag == EGG_B200_TAG_BSPLINE) {
@@ -858,7 +865,7 @@ static Session* create_session(const egg_b200_session_desc& d)
         if ((D == 2 && (is_tcurve(etag) || etag == EGG_B200_TAG_BSPLINE)) || (D == 3 && is_param3(etag))) {
             S->n_arc++;
         }
-        if (etag == EGG_B200_TAG_BSPLINE) { S->n_bspline++; }
+        if (etag == EGG_B200_TAG_BSPLINE || etag == EGG_B200_TAG_BSPLINESURF) { S->n_bspline++; }
         if (etag == EGG_B200_TAG_COMPOSITE) { S->n_composite++; }
         if (synth_target) {
             // The synthesized interior patch (src/structured_patch.hpp:89-130):
@@ -1185,9 +1192,9 @@ static Session* create_session(const egg_b200_session_desc& d)
     if (S->n_bspline || S->n_composite) {
         S->arena.upload(std::vector<double>(d.entity_arena, d.entity_arena + d.entity_arena_len));
     }
-    if (S->n_bspline) {
-        S->seeds.alloc(size_t(S->n_stored));
-        EGG_CK(cudaMemset(S->seeds.p, 0xFF, size_t(S->n_stored) * sizeof(double)));  // all-ones: NaN
+    if (S->n_bspline) {  // D - 1 foot parameters per stored DOF
+        S->seeds.alloc(size_t(S->n_stored) * size_t(D - 1));
+        EGG_CK(cudaMemset(S->seeds.p, 0xFF, S->seeds.n * sizeof(double)));  // all-ones: NaN
     }
     S->st_gc.upload(st_gc);
     S->st_gn0.upload(st_gn0);
@@ -1433,7 +1440,8 @@ static void launch_stored(Session& S, LevelData& L, const double* xin, double* x
                          L.st_gn2.p, L.st_s0.p,   L.st_s1.p,  L.st_s2.p, L.st_role.p, L.st_W.p,
                          L.st_wstride, L.st_wt.p, L.st_wtstride,
                          L.n_constrained ? L.st_etag.p : nullptr, L.n_constrained ? L.st_epar.p : nullptr,
-                         cold ? 1 : 0, soft_view(L)};
+                         cold ? 1 : 0, soft_view(L), L.n_bspline ? L.arena.p : nullptr,
+                         L.n_bspline ? L.seeds.p : nullptr};
         auto go3 = [&](auto con) {
             constexpr bool C = decltype(con)::value;
             switch (G) {
@@ -1983,6 +1991,15 @@ __global__ void entity_frame_kernel(int dim, int tag, const double* __restrict__
         return;
     }
     const double* p = q + 3 * i;
+    if (tag == EGG_B200_TAG_BSPLINESURF) {
+        double B[2][3];
+        bsurf_project_frame(bsurf_view(e, arena), p, foot + 3 * i, B);
+        for (int k = 0; k < 3; ++k) {
+            basis[(3 * i + k) * 2] = B[0][k];
+            basis[(3 * i + k) * 2 + 1] = B[1][k];
+        }
+        return;
+    }
     entity3_project(tag, e, p, foot + 3 * i);
     double B[2][3] = {{1.0, 0.0, 0.0}, {0.0, 1.0, 0.0}};
     if (is_param3(tag)) {
@@ -2148,9 +2165,7 @@ static void ensure_xfer(Session& S)
 // from its coarse grid), as the reference's upload_X does (src/sweep.hpp:592-597).
 static void reset_seeds(Session& S)
 {
-    if (S.n_bspline) {
-        EGG_CK(cudaMemsetAsync(S.seeds.p, 0xFF, size_t(S.n_stored) * sizeof(double), S.stream));
-    }
+    if (S.n_bspline) { EGG_CK(cudaMemsetAsync(S.seeds.p, 0xFF, S.seeds.n * sizeof(double), S.stream)); }
 }
 
 static int remap_grid(int64_t n) { return int(std::max<int64_t>(1, std::min<int64_t>((n + 255) / 256, 148 * 8))); }
@@ -2948,11 +2963,15 @@ int egg_b200_entity_frame(int32_t dim, int32_t tag, const double* record, const 
         if (!record || n < 0 || (n > 0 && (!q || !foot || !basis)) || arena_len < 0 || (arena_len > 0 && !arena)) {
             invalid("entity_frame: bad arguments");
         }
-        const bool segd = tag == EGG_B200_TAG_BSPLINE || tag == EGG_B200_TAG_COMPOSITE;
+        const bool segd = tag == EGG_B200_TAG_BSPLINE || tag == EGG_B200_TAG_COMPOSITE ||
+                          tag == EGG_B200_TAG_BSPLINESURF;
         if (segd && arena_len == 0) { invalid("entity_frame: a B-spline or composite entity needs its arena"); }
+        if (tag == EGG_B200_TAG_BSPLINESURF && !bsurf_record_ok(record, arena, arena_len)) {
+            invalid("entity_frame: B-spline surface record outside its arena");
+        }
         if (n == 0) { return; }
         const int K = (dim == 3 && (tag == EGG_B200_TAG_PLANE || tag == EGG_B200_TAG_SPHERE ||
-                                    tag == EGG_B200_TAG_CYLINDER)) ? 2 : 1;
+                                    tag == EGG_B200_TAG_CYLINDER || tag == EGG_B200_TAG_BSPLINESURF)) ? 2 : 1;
         DevBuf<double> de, da, dq, df, db;
         de.upload(std::vector<double>(record, record + EGG_B200_ENTITY_FIELDS));
         da.upload(arena_len ? std::vector<double>(arena, arena + arena_len) : std::vector<double> {0.0});

@@ -116,7 +116,7 @@ def free_mask_from_fixed(n_nodes: int, fixed_ids) -> np.ndarray:
 ENTITY_KINDS = {1: ("line_seg", 4), 2: ("circle", 3), 3: ("ellipse", 4), 5: ("plane", 9), 6: ("circle_arc", 6),
                 7: ("ellipse_arc", 8), 8: ("quad_bezier", 8), 9: ("cubic_bezier", 10), 15: ("line_rail", 4),
                 16: ("line_rail3", 6), 4: ("sphere", 10), 12: ("cylinder", 10), 13: ("line3", 8),
-                10: ("bspline", 6), 11: ("composite", 2)}
+                10: ("bspline", 6), 11: ("composite", 2), 14: ("bsplinesurf", 9)}
 
 
 def flat_wire(

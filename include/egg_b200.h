@@ -64,6 +64,11 @@ extern "C" {
 #define EGG_B200_TAG_CYLINDER 12 /* 3D record (o(3), ax(3), ay(3), r): untrimmed cylinder about ax x ay */
 #define EGG_B200_TAG_LINE3 13    /* 3D record (p0(3), p1(3), t0, t1): line trimmed to [t0, t1] */
 #define EGG_B200_TAG_LINERAIL3 16 /* 3D record (s(3), e(3)): open-ended segment, released beyond its ends */
+#define EGG_B200_TAG_BSPLINESURF 14 /* 3D record (pu, pv, nu, nv, ku_at, kv_at, ctrl_at, w_at, has_w, trim_at):
+                                     * B-spline / NURBS surface, degrees <= 7, the *_at fields offsets into
+                                     * entity_arena (knots nu+pu+1 and nv+pv+1, ctrl 3 nu nv u-major, weights
+                                     * nu nv); trim_at < 0 untrimmed, else the offset of (n_loop_entries,
+                                     * loops_at, verts_at) describing the UV trim polygon */
 #define EGG_B200_ENTITY_FIELDS 10 /* reals per entity record in entity_params */
 
 typedef struct egg_b200_session egg_b200_session;

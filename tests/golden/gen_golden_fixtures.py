@@ -799,6 +799,84 @@ def gen_reference_free() -> None:
     print(f"ref_free.npz: {len(out)} arrays")
 
 
+# B-spline / NURBS surfaces (entity tag 14), reference fp64 core: sweeps,
+# two run calls (the seeds persist, each call's first sweep projects from
+# them in world space), FAS, and the reference's batched projection onto a
+# polynomial, a rational and a UV-trimmed surface -> ref_bsurf.npz.
+BSURF_CASE = ("cube_bsurf", dict(n=9, seed=15))
+BSURF_RUNS = [("barrier", 0.0, 1.0, 20), ("barrier", 0.0, 0.8, 20), ("shape_size", 0.0, 1.0, 10)]
+# a trim polygon in the top surface's (u, v): an outer loop and a hole
+BSURF_TRIM = [np.array([[0.05, 0.05], [0.95, 0.08], [0.9, 0.95], [0.1, 0.9]]),
+              np.array([[0.4, 0.4], [0.6, 0.4], [0.55, 0.6]])]
+
+
+def bsurf_entities():
+    """(name, tag, record, seg) of the three projection surfaces."""
+    from egg_b200 import configs
+
+    top, side, w = configs.bsurf_nets()
+    out = []
+    for name, kw, net, wt, trim in (("poly", configs.BSURF_TOP, top, None, None),
+                                    ("nurbs", configs.BSURF_SIDE, side, w, None),
+                                    ("trimmed", configs.BSURF_TOP, top, None, BSURF_TRIM)):
+        tag, rec, seg = configs._bsurf_entity(kw["pu"], kw["pv"], kw["ku"], kw["kv"], net, wt, trim)
+        out.append((name, tag, np.asarray(rec), [{"data": np.asarray(a, dtype=np.float64),
+                                                   "off": np.array([0, np.asarray(a).size], dtype=np.int32)}
+                                                  for a in seg]))
+    return out
+
+
+def _bsurf_runs() -> dict:
+    from egg_b200 import configs
+    from oracle import oracle
+
+    ref = oracle.load_ref("fp64")
+    if ref is None:
+        raise SystemExit("oracle/_ref/fp64 missing: run oracle/build_ref.sh first")
+    out = {}
+    g = getattr(configs, BSURF_CASE[0])(**BSURF_CASE[1])
+    ctx, st = g.wire(), g.structured()
+    for phase, delta, omega, n in BSURF_RUNS:
+        X1, _e1, _m1 = ref.cpp_structured_sweep(ctx, st, g.X_flat(), 1, device="cpu", phase=phase, delta=delta,
+                                                omega=omega, report_every=1, dim=3)
+        Xn, en, mn = ref.cpp_structured_sweep(ctx, st, g.X_flat(), n, device="cpu", phase=phase, delta=delta,
+                                              omega=omega, report_every=1, dim=3)
+        key = f"{phase}/{omega}"
+        out[key + "/X1"] = X1
+        out[key + "/Xn"] = Xn
+        out[key + "/E"] = en
+        out[key + "/M"] = mn
+    sess = ref.CppStructuredSweepSession(ctx, st, g.X_flat(), device="cpu", dim=3)
+    e_a, _ = sess.run(5, report_every=1)
+    e_b, _ = sess.run(10, report_every=1)
+    out["twocalls/E"] = np.concatenate([e_a, e_b])
+    out["twocalls/X"] = sess.get_X()
+    sess = ref.CppStructuredSweepSession(ctx, st, g.X_flat(), device="cpu", dim=3)
+    E, M = sess.run_fas(3, nu_pre=2, nu_post=2, nu_coarse=16, omega=1.0, max_levels=32, phase="barrier")
+    out["fas/E"] = E
+    out["fas/M"] = M
+    out["fas/X"] = sess.get_X()
+    rng = np.random.default_rng(41)
+    for name, tag, rec, seg in bsurf_entities():
+        Q = rng.uniform(-0.2, 1.2, size=(48, 3))
+        Q[:, 2 if name != "nurbs" else 0] = 1.0 + rng.uniform(-0.3, 0.3, 48)
+        feet, basis = ref.geometry_project_batch(Q, tag, rec, seg)
+        out[f"project/{name}/q"] = Q
+        out[f"project/{name}/foot"] = np.asarray(feet)
+        out[f"project/{name}/basis"] = np.asarray(basis)
+    return out
+
+
+def gen_reference_bsurf() -> None:
+    out = _bsurf_runs()
+    np.savez_compressed(HERE / "ref_bsurf.npz", **out)
+    print(f"ref_bsurf.npz: {len(out)} arrays")
+
+
+if __name__ == "__main__" and len(sys.argv) == 2 and sys.argv[1] == "--bsurf":
+    gen_reference_bsurf()
+    raise SystemExit(0)
+
 if __name__ == "__main__" and len(sys.argv) == 2 and sys.argv[1] == "--free":
     gen_reference_free()
     raise SystemExit(0)
@@ -830,3 +908,4 @@ if __name__ == "__main__":
     gen_reference_soft(ref_root)
     gen_reference_configs()
     gen_reference_free()
+    gen_reference_bsurf()
