@@ -348,10 +348,13 @@ __device__ void frame_entity(int tag, const double* rec, const double* arena, co
         t[0][0] = tx;
         t[0][1] = ty;
     } else if (tag == EGG_B200_TAG_BSPLINESURF) {
-        const BSplineSurf bs = bsurf_view(rec, arena);
-        double B[2][3], g2[3];
-        bsurf_project_frame(bs, p, foot, B);
-        bsurf_project_frame(bs, foot, g2, t);
+        double io[3] = {p[0], p[1], p[2]}, B[6];
+        bsurf_dof(kBsurfFrame, rec, arena, nullptr, nullptr, nullptr, 0.0, 0.0, nullptr, nullptr, nullptr, io, B);
+        for (int k = 0; k < 3; ++k) { foot[k] = io[k]; }
+        bsurf_dof(kBsurfFrame, rec, arena, nullptr, nullptr, nullptr, 0.0, 0.0, nullptr, nullptr, nullptr, io, B);
+        for (int a = 0; a < 2; ++a) {
+            for (int k = 0; k < 3; ++k) { t[a][k] = B[a * 3 + k]; }
+        }
     } else {
         entity3_project(tag, rec, p, foot);
         if (is_surf3(tag)) {

@@ -316,7 +316,11 @@ EGG_HD void param3_warm_step(int tag, const double* e, const double h[6], const 
 // quotient rule); the foot by Newton on ((S - p) . S_u, (S - p) . S_v) = 0:
 // Gauss-Newton from a seed (the DOF's last foot), else from the 4 best of a
 // 9 x 9 parameter grid polished by damped Newton (Levenberg-Marquardt with
-// residual backtracking), the nearest foot winning.
+// residual backtracking), the nearest foot winning.  These functions are
+// inlined into one out-of-line entry, bsurf_dof: out-of-line device copies
+// of them calling one another returned wrong partials on sm_100a, and
+// inlining them into every stored-patch kernel instantiation costs more
+// compile time than the entry's call does at run time.
 constexpr double kSurfTiny = 1e-30;    // det / denominator floor
 constexpr double kSurfNewton = 1e-9;   // |dq| break of the foot iterations
 
@@ -374,6 +378,9 @@ EGG_HD BSplineSurf bsurf_view(const double* e, const double* arena)
     s.v.knots = arena + int64_t(e[5]);
     s.u.ctrl = s.v.ctrl = nullptr;
     s.u.w = s.v.w = nullptr;
+    s.u.t0 = s.v.t0 = 0.0;
+    s.u.t1 = s.v.t1 = 1.0;
+    s.u.closed = s.v.closed = false;
     s.ctrl = arena + int64_t(e[6]);
     s.w = e[8] != 0.0 ? arena + int64_t(e[7]) : nullptr;
     s.loops = s.verts = nullptr;
@@ -388,7 +395,7 @@ EGG_HD BSplineSurf bsurf_view(const double* e, const double* arena)
 }
 
 // Surface partials S00, S10, S01, S20, S02, S11 (rows 0..5) up to order nd.
-EGG_OUTLINE void bsurf_ders(const BSplineSurf& s, const double q[2], int nd, double S[6][3])
+EGG_HD void bsurf_ders(const BSplineSurf& s, const double q[2], int nd, double S[6][3])
 {
     const int su = bspline_span(s.u, q[0]), sv = bspline_span(s.v, q[1]);
     double du[3][kBSplineCap], dv[3][kBSplineCap];
@@ -505,10 +512,11 @@ EGG_HD void bsurf_trim_clamp(const BSplineSurf& s, double q[2])
 // stopping when the clamped iterate moves less than kSurfNewton or the
 // Jacobian is singular.  EXACT adds the curvature terms (d . S_uv...).  J
 // receives the raw frame (S_u, S_v) of the last iterate evaluated.
-EGG_OUTLINE void bsurf_newton(const BSplineSurf& s, const double* p, double q[2], bool exact, double J[2][3])
+EGG_HD void bsurf_newton(const BSplineSurf& s, const double* p, double q[2], bool exact, double J[2][3])
 {
     double u0, u1, v0, v1;
     bsurf_domain(s, u0, u1, v0, v1);
+    #pragma unroll 1
     for (int it = 0; it < 12; ++it) {
         double S[6][3];
         bsurf_ders(s, q, exact ? 2 : 1, S);
@@ -538,7 +546,7 @@ EGG_OUTLINE void bsurf_newton(const BSplineSurf& s, const double* p, double q[2]
 // Damped Newton from one seed (cold multi-start only): the damping bridges
 // Gauss-Newton and gradient descent, and a step is kept only if it lowers
 // |S - p|^2 (up to 6 damping increases per iteration).
-EGG_OUTLINE void bsurf_newton_lm(const BSplineSurf& s, const double* p, double q[2], double J[2][3])
+EGG_HD void bsurf_newton_lm(const BSplineSurf& s, const double* p, double q[2], double J[2][3])
 {
     double u0, u1, v0, v1;
     bsurf_domain(s, u0, u1, v0, v1);
@@ -549,6 +557,7 @@ EGG_OUTLINE void bsurf_newton_lm(const BSplineSurf& s, const double* p, double q
     double d[3] = {S[0][0] - p[0], S[0][1] - p[1], S[0][2] - p[2]};
     double r = dot3v(d, d);
     double lambda = 1e-3 * (dot3v(S[1], S[1]) + dot3v(S[2], S[2]) + kSurfTiny);
+    #pragma unroll 1
     for (int it = 0; it < 16; ++it) {
         const double f1 = dot3v(d, S[1]), f2 = dot3v(d, S[2]);
         const double j11 = dot3v(S[1], S[1]) + dot3v(d, S[3]);
@@ -556,6 +565,7 @@ EGG_OUTLINE void bsurf_newton_lm(const BSplineSurf& s, const double* p, double q
         const double j22 = dot3v(S[2], S[2]) + dot3v(d, S[4]);
         double du = 0.0, dv = 0.0;
         bool accepted = false;
+        #pragma unroll 1
         for (int bt = 0; bt < 6; ++bt) {
             const double a11 = j11 + lambda, a22 = j22 + lambda;
             const double det = a11 * a22 - j12 * j12;
@@ -593,7 +603,7 @@ EGG_OUTLINE void bsurf_newton_lm(const BSplineSurf& s, const double* p, double q
 // Foot parameter of p (src/geometry.hpp:1342-1420 invert_seeded): from the
 // seed when there is one (Gauss-Newton), else the multi-start search; J is
 // the raw frame the chosen iteration saw last.
-EGG_OUTLINE void bsurf_invert(const BSplineSurf& s, const double* p, const double seed[2], bool has_seed, double q[2],
+EGG_HD void bsurf_invert(const BSplineSurf& s, const double* p, const double seed[2], bool has_seed, double q[2],
                               double J[2][3])
 {
     double u0, u1, v0, v1;
@@ -611,7 +621,9 @@ EGG_OUTLINE void bsurf_invert(const BSplineSurf& s, const double* p, const doubl
         bestq[k][0] = u0;
         bestq[k][1] = v0;
     }
+    #pragma unroll 1
     for (int i = 0; i <= kGrid; ++i) {
+        #pragma unroll 1
         for (int j = 0; j <= kGrid; ++j) {
             const double t[2] = {u0 + ((u1 - u0) * i) / kGrid, v0 + ((v1 - v0) * j) / kGrid};
             double e[3];
@@ -634,6 +646,7 @@ EGG_OUTLINE void bsurf_invert(const BSplineSurf& s, const double* p, const doubl
     q[0] = u0;
     q[1] = v0;
     double best = INFINITY;
+    #pragma unroll 1
     for (int k = 0; k < kStarts; ++k) {
         if (bestd[k] == INFINITY) { continue; }
         double f[2] = {bestq[k][0], bestq[k][1]}, Jk[2][3];
@@ -657,7 +670,7 @@ EGG_OUTLINE void bsurf_invert(const BSplineSurf& s, const double* p, const doubl
 // the unclamped foot; a foot outside the trim is clamped onto it): the
 // world-space path of the first sweep of a run call and of cold trials
 // (src/geometry.hpp:230-260).
-EGG_OUTLINE void bsurf_foot_seeded(const BSplineSurf& s, const double* p, double seed[2], double q[2])
+EGG_HD void bsurf_foot_seeded(const BSplineSurf& s, const double* p, double seed[2], double q[2])
 {
     const bool has = isfinite(seed[0]);
     double J[2][3];
@@ -732,6 +745,40 @@ EGG_HD void bsurf_project_frame(const BSplineSurf& s, const double* p, double fo
     bsurf_foot_seeded(s, p, seed, q);
     bsurf_eval(s, q, foot);
     bsurf_basis_at(s, q, B);
+}
+
+// The one out-of-line entry into the B-spline-surface code for the kernels
+// (record er, arena): kBsurfCold -- the cold step d on the seeded foot's
+// frame (io = d); kBsurfWarm -- the warm parametric step (qs, dq), seed :=
+// q*; kBsurfColdTrial -- io (a raw trial) projected from the seed, which it
+// advances; kBsurfWarmTrial -- io = eval(trim clamp(qs + alpha dq));
+// kBsurfFrame -- io (a point) replaced by its cold foot, B the basis there.
+enum BsurfOp : int { kBsurfCold = 0, kBsurfWarm, kBsurfColdTrial, kBsurfWarmTrial, kBsurfFrame };
+
+EGG_OUTLINE void bsurf_dof(int op, const double* er, const double* arena, const double* h, const double* g,
+                           const double* pos, double omega, double alpha, double* seed, double* qs, double* dq,
+                           double* io, double* B)
+{
+    const BSplineSurf s = bsurf_view(er, arena);
+    if (op == kBsurfCold) {
+        bsurf_cold_step(s, h, g, pos, seed, io);
+    } else if (op == kBsurfWarm) {
+        bsurf_warm_step(s, h, g, pos, omega, seed, qs, dq);
+    } else if (op == kBsurfColdTrial) {
+        const double raw[3] = {io[0], io[1], io[2]};
+        bsurf_project_seeded(s, raw, seed, io);
+    } else if (op == kBsurfWarmTrial) {
+        double qt[2] = {qs[0] + alpha * dq[0], qs[1] + alpha * dq[1]};
+        bsurf_trim_clamp(s, qt);
+        bsurf_eval(s, qt, io);
+    } else {
+        const double p[3] = {io[0], io[1], io[2]};
+        double Bl[2][3];
+        bsurf_project_frame(s, p, io, Bl);
+        for (int a = 0; a < 2; ++a) {
+            for (int k = 0; k < 3; ++k) { B[a * 3 + k] = Bl[a][k]; }
+        }
+    }
 }
 
 }  // namespace egg_b200

@@ -563,10 +563,8 @@ __global__ void stored3_kernel(StoredPatch3 sp, const double* __restrict__ Xin, 
         // parameters, every trial clamped onto the trim polygon
         // (src/sweep.hpp:1820-1832: the clamp applies inside the trim too).
         const bool bsurf = etag == EGG_B200_TAG_BSPLINESURF;
-        BSplineSurf bs {};
         double seed[2] = {NAN, NAN};
         if (bsurf) {
-            bs = bsurf_view(er, sp.arena);
             seed[0] = sp.seeds[2 * d];
             seed[1] = sp.seeds[2 * d + 1];
         }
@@ -576,9 +574,9 @@ __global__ void stored3_kernel(StoredPatch3 sp, const double* __restrict__ Xin, 
         if (etag == 0) {
             solve3<double>(h, g, dl);
         } else if (bsurf && warm_param) {
-            bsurf_warm_step(bs, h, g, pos, omega, seed, qs, dq);
+            bsurf_dof(kBsurfWarm, er, sp.arena, h, g, pos, omega, 0.0, seed, qs, dq, nullptr, nullptr);
         } else if (bsurf) {
-            bsurf_cold_step(bs, h, g, pos, seed, dl);
+            bsurf_dof(kBsurfCold, er, sp.arena, h, g, pos, omega, 0.0, seed, qs, dq, dl, nullptr);
             for (int q = 0; q < 3; ++q) { dl[q] *= omega; }
         } else if (warm_param) {
             param3_warm_step(etag, er, h, g, pos, omega, qs, dq);
@@ -590,13 +588,9 @@ __global__ void stored3_kernel(StoredPatch3 sp, const double* __restrict__ Xin, 
         double cur[3] = {pos[0], pos[1], pos[2]};
         for (int it = 0; it < 10; ++it) {
             double tr[3] = {pos[0] + alpha * dl[0], pos[1] + alpha * dl[1], pos[2] + alpha * dl[2]};
-            if (bsurf && warm_param) {
-                double qt[2] = {qs[0] + alpha * dq[0], qs[1] + alpha * dq[1]};
-                bsurf_trim_clamp(bs, qt);
-                bsurf_eval(bs, qt, tr);
-            } else if (bsurf) {
-                const double raw[3] = {tr[0], tr[1], tr[2]};
-                bsurf_project_seeded(bs, raw, seed, tr);
+            if (bsurf) {
+                bsurf_dof(warm_param ? kBsurfWarmTrial : kBsurfColdTrial, er, sp.arena, h, g, pos, omega, alpha,
+                          seed, qs, dq, tr, nullptr);
             } else if (warm_param) {
                 double qt[2] = {qs[0] + alpha * dq[0], qs[1] + alpha * dq[1]};
                 p3_clamp(etag, er, qt);

@@ -1992,11 +1992,12 @@ __global__ void entity_frame_kernel(int dim, int tag, const double* __restrict__
     }
     const double* p = q + 3 * i;
     if (tag == EGG_B200_TAG_BSPLINESURF) {
-        double B[2][3];
-        bsurf_project_frame(bsurf_view(e, arena), p, foot + 3 * i, B);
+        double io[3] = {p[0], p[1], p[2]}, B[6];
+        bsurf_dof(kBsurfFrame, e, arena, nullptr, nullptr, nullptr, 0.0, 0.0, nullptr, nullptr, nullptr, io, B);
         for (int k = 0; k < 3; ++k) {
-            basis[(3 * i + k) * 2] = B[0][k];
-            basis[(3 * i + k) * 2 + 1] = B[1][k];
+            foot[3 * i + k] = io[k];
+            basis[(3 * i + k) * 2] = B[k];
+            basis[(3 * i + k) * 2 + 1] = B[3 + k];
         }
         return;
     }
