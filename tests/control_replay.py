@@ -8,8 +8,9 @@ are compared field by field: energies, min dets, step lengths, iteration
 count and convergence at the trajectory tolerances of the other fp64 control
 tests.  A PCG solve that stops at rtol may take a few iterations more or
 fewer when its dot products round differently, so its iteration count is
-compared to within two or 5%, whichever is larger, and its final relative
-residual to within one decade.
+compared to within two or 5%, whichever is larger (four or 25% for the
+inexact solves of a forcing run), and its final relative residual to within
+one decade.
 """
 
 from __future__ import annotations
@@ -29,7 +30,7 @@ def load(name: str) -> list[dict]:
         return pickle.load(f)["events"]
 
 
-def check_report(got, want, what, rtol=RTOL, atol=ATOL):
+def check_report(got, want, what, rtol=RTOL, atol=ATOL, forcing=False):
     for k in ("energies", "mindets", "alphas"):
         g, w = np.asarray(got[k]), np.asarray(want[k])
         assert g.shape == w.shape, (what, k, g, w)
@@ -42,7 +43,11 @@ def check_report(got, want, what, rtol=RTOL, atol=ATOL):
     np.testing.assert_allclose(fg, fw, rtol=0, atol=rtol * scale + atol, err_msg=f"{what}.frame_jumps")
     gi, wi = np.asarray(got["pcg_iters"]), np.asarray(want["pcg_iters"])
     assert gi.shape == wi.shape, (what, gi, wi)
-    assert np.all(np.abs(gi - wi) <= np.maximum(2, 0.05 * wi)), (what, gi, wi)
+    # an inexact solve (forcing: stop at a relative residual up to 0.5) stops
+    # wherever its residual first crosses a loose bound, so its count moves
+    # further with the same rounding
+    slack = np.maximum(4, 0.25 * wi) if forcing else np.maximum(2, 0.05 * wi)
+    assert np.all(np.abs(gi - wi) <= slack), (what, gi, wi)
     gr, wr = np.asarray(got["pcg_relres"]), np.asarray(want["pcg_relres"])
     assert gr.shape == wr.shape
     pos = wr > 0
@@ -79,7 +84,7 @@ def replay(core, events, scenario, rtol=RTOL, atol=ATOL, x_atol=1e-10):
         got = getattr(sessions[ev["sid"]], ev["name"])(*ev["args"], **ev["kwargs"])
         what = f"{scenario}:{ev['name']}#{n}"
         if ev["name"] == "run_control":
-            check_report(got, ev["result"], what, rtol, atol)
+            check_report(got, ev["result"], what, rtol, atol, forcing=ev["kwargs"].get("pcg_forcing", True))
         elif ev["name"] in ("get_C", "get_X"):
             np.testing.assert_allclose(got, ev["result"], rtol=rtol, atol=x_atol, err_msg=what)
         else:

@@ -77,8 +77,10 @@ def test_bsurf_projection_matches_reference(gpu, name):
     ent = {n: (t, r, s) for n, t, r, s in bsurf_entities()}[name]
     tag, rec, seg = ent
     feet, basis = gpu.geometry_project_batch(_FX[f"project/{name}/q"], tag, rec, seg)
-    np.testing.assert_allclose(feet, _FX[f"project/{name}/foot"], rtol=0, atol=1e-10)
-    np.testing.assert_allclose(basis, _FX[f"project/{name}/basis"], rtol=0, atol=1e-8)
+    # the foot iterations stop once the parameter moves less than 1e-9, so a
+    # foot is fixed to about that much of |S_u|, |S_v| (~1)
+    np.testing.assert_allclose(feet, _FX[f"project/{name}/foot"], rtol=0, atol=1e-8)
+    np.testing.assert_allclose(basis, _FX[f"project/{name}/basis"], rtol=0, atol=1e-7)
 
 
 def test_bsurf_nodes_stay_on_their_surfaces(gpu):
