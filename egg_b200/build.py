@@ -25,8 +25,17 @@ LIB = PKG / "libegg_b200.so"
 EXT = sysconfig.get_config_var("EXT_SUFFIX")
 CORE = PKG / f"cpp_core{EXT}"
 
-CU_SOURCES = [CSRC / "session.cu"]
-CU_DEPS = sorted(CSRC.glob("*.cuh")) + sorted(CSRC.glob("*.inc")) + [INCLUDE / "egg_b200.h"]
+OBJ_DIR = ROOT / "_build"
+# Translation units of libegg_b200.so: the sweep core (session.cu with every
+# kernel header) and the device-side wire builder (wire.cu, standalone).  Each
+# compiles to its own object, in parallel, and only when its inputs changed.
+CU_UNITS = {
+    "session": (CSRC / "session.cu",
+                sorted(CSRC.glob("*.cuh")) + sorted(CSRC.glob("*.inc")) + [INCLUDE / "egg_b200.h"]),
+    "wire": (CSRC / "wire.cu", [INCLUDE / "egg_b200.h"]),
+}
+NVCC_FLAGS = [*ARCH, "-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", "-Xptxas", "-warn-spills",
+              f"-I{INCLUDE}", f"-I{CSRC}"]
 
 
 def _stale(target: Path, deps) -> bool:
@@ -41,14 +50,25 @@ def _run(cmd, **kw):
     subprocess.run([str(c) for c in cmd], check=True, **kw)
 
 
+def _compile(name: str, force: bool) -> Path:
+    src, deps = CU_UNITS[name]
+    obj = OBJ_DIR / f"{name}.o"
+    if force or _stale(obj, [src, *deps, Path(__file__)]):
+        OBJ_DIR.mkdir(exist_ok=True)
+        tmp = obj.with_suffix(".o.tmp")
+        _run([NVCC, *NVCC_FLAGS, "-c", src, "-o", tmp])
+        os.replace(tmp, obj)
+    return obj
+
+
 def build_lib(force: bool = False) -> Path:
-    if force or _stale(LIB, CU_SOURCES + CU_DEPS + [Path(__file__)]):
+    from concurrent.futures import ThreadPoolExecutor
+
+    with ThreadPoolExecutor(len(CU_UNITS)) as ex:
+        objs = list(ex.map(lambda n: _compile(n, force), CU_UNITS))
+    if force or _stale(LIB, objs):
         tmp = LIB.with_suffix(".so.tmp")
-        _run(
-            [NVCC, *ARCH, "-O3", "-lineinfo", "-std=c++17", "-shared", "-Xcompiler", "-fPIC",
-             "-Xptxas", "-warn-spills", f"-I{INCLUDE}", f"-I{CSRC}", *CU_SOURCES, "-o", tmp,
-             "-lcudart"]
-        )
+        _run([NVCC, *ARCH, "-shared", *objs, "-o", tmp, "-lcudart"])
         os.replace(tmp, LIB)
     return LIB
 

@@ -56,10 +56,10 @@ class Grid:
     def num_free(self) -> int:
         return int(self.free.sum())
 
-    def wire(self, *, w_inv=None, compact: bool = False) -> dict:
+    def wire(self, *, w_inv=None, compact: bool = False, device: str | None = None) -> dict:
         return _wire.flat_wire(self.blocks, self.free, self.d, w_inv=w_inv, compact=compact,
                                constraints=self.constraints, directional=self.soft.get("directional"),
-                               curvature=self.soft.get("curvature"))
+                               curvature=self.soft.get("curvature"), device=device)
 
     def structured(self) -> dict:
         return _wire.structured_tables(self.blocks)

@@ -1481,4 +1481,103 @@ PYBIND11_MODULE(cpp_core, m)
       },
       py::arg("X"), py::arg("nodes"), py::arg("kind"), py::arg("ref"), py::arg("weight"), py::arg("eps") = 1e-12,
       "Directional soft-energy total and gradient over a sample table, on the GPU. Returns (energy, grad (n_nodes, d)).");
+    m.def(
+      "wire_build",
+      [](int dim, const IArr& shapes, const py::array_t<int64_t, py::array::c_style | py::array::forcecast>& ids,
+         const py::array_t<uint8_t, py::array::c_style | py::array::forcecast>& moving, const py::object& stored,
+         bool synth_interior, bool energy_arrays, const std::string& device) {
+          if (dim != 2 && dim != 3) { throw py::value_error("wire_build: dim must be 2 or 3"); }
+          if (shapes.size() % dim != 0) { throw py::value_error("wire_build: shapes length must be a multiple of dim"); }
+          py::array_t<uint8_t, py::array::c_style | py::array::forcecast> st;
+          if (!stored.is_none()) {
+              st = py::array_t<uint8_t, py::array::c_style | py::array::forcecast>::ensure(stored);
+              if (!st || st.size() != moving.size()) {
+                  throw py::value_error("wire_build: stored must be a mask of num_nodes entries");
+              }
+          }
+          egg_b200_wire_desc d {};
+          d.dim = dim;
+          d.num_blocks = int32_t(shapes.size() / dim);
+          d.shapes = shapes.data();
+          d.block_ids = ids.data();
+          d.num_nodes = int64_t(moving.size());
+          d.moving = moving.data();
+          d.stored = stored.is_none() ? nullptr : st.data();
+          d.synth_interior = synth_interior ? 1 : 0;
+          d.energy_arrays = energy_arrays ? 1 : 0;
+          d.device = device_of(device);
+          int64_t total = 1;
+          int64_t want = 0;
+          for (int b = 0; b < d.num_blocks; ++b) {
+              total = 1;
+              for (int k = 0; k < dim; ++k) { total *= shapes.data()[b * dim + k]; }
+              want += total;
+          }
+          if (int64_t(ids.size()) != want) { throw py::value_error("wire_build: block_ids length != sum of prod(shape)"); }
+          egg_b200_wire* w = nullptr;
+          int rc = EGG_B200_OK;
+          {
+              py::gil_scoped_release nogil;
+              rc = egg_b200_wire_build(&d, &w);
+          }
+          check(rc);
+          std::unique_ptr<egg_b200_wire, int (*)(egg_b200_wire*)> guard(w, egg_b200_wire_destroy);
+          int64_t sz[3] = {0, 0, 0};
+          check(egg_b200_wire_sizes(w, sz));
+          const py::ssize_t nd = sz[0], nr = sz[1], ns = sz[2];
+          py::dict out;
+          egg_b200_wire_out o {};
+          auto iarr = [&](const char* key, py::ssize_t n) {
+              py::array_t<int32_t> a(n);
+              out[key] = a;
+              return a.mutable_data();
+          };
+          auto darr = [&](const char* key, py::ssize_t n) {
+              py::array_t<double> a(n);
+              out[key] = a;
+              return a.mutable_data();
+          };
+          o.dof_idx = iarr("dof_idx", nd);
+          o.P_of = iarr("P_of", nd);
+          o.interior_block = iarr("interior_block", nd);
+          {
+              py::array_t<int32_t> a({nd, py::ssize_t(dim)});
+              out["interior_logical"] = a;
+              o.interior_logical = a.mutable_data();
+          }
+          o.role = iarr("role", nr);
+          {
+              py::array_t<int64_t> a(nr);
+              out["sid"] = a;
+              o.sid = a.mutable_data();
+          }
+          o.gc = iarr("gc", nr);
+          const char* gnk[3] = {"gn0", "gn1", "gn2"};
+          const char* sk[3] = {"s0", "s1", "s2"};
+          const char* es_gnk[3] = {"es_gn0", "es_gn1", "es_gn2"};
+          const char* es_sk[3] = {"es_s0", "es_s1", "es_s2"};
+          for (int k = 0; k < dim; ++k) {
+              o.gn[k] = iarr(gnk[k], nr);
+              o.s[k] = darr(sk[k], nr);
+          }
+          if (energy_arrays) {
+              o.es_gc = iarr("es_gc", ns);
+              for (int k = 0; k < dim; ++k) {
+                  o.es_gn[k] = iarr(es_gnk[k], ns);
+                  o.es_s[k] = darr(es_sk[k], ns);
+              }
+          }
+          out["num_samples"] = ns;
+          {
+              py::gil_scoped_release nogil;
+              rc = egg_b200_wire_download(w, &o);
+          }
+          check(rc);
+          return out;
+      },
+      py::arg("dim"), py::arg("shapes"), py::arg("block_ids"), py::arg("moving"), py::arg("stored") = py::none(),
+      py::arg("synth_interior") = true, py::arg("energy_arrays") = true, py::arg("device") = "auto",
+      "Device-side build of the sweep-context wire's index arrays (the array work of build_flat_context): "
+      "returns a dict of the group's dof_idx, P_of, interior_block, interior_logical, role, sid, gc, gn*, s* and, "
+      "with energy_arrays, the energy stencil's es_gc, es_gn*, es_s*, plus num_samples.");
 }

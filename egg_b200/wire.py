@@ -129,6 +129,7 @@ def flat_wire(
     constraints: dict | None = None,
     directional: dict | None = None,
     curvature: dict | None = None,
+    device: str | None = None,
 ) -> dict:
     """The ``{"groups", "energy_stencil"}`` wire for Free DOFs and, optionally,
     constrained boundary DOFs.
@@ -147,6 +148,10 @@ def flat_wire(
     ``directional`` (``nodes`` (n, 4) -1 padded, ``kind``, ``ref`` (n, d),
     ``axis`` (n, d), ``weight``, ``eps``) and ``curvature`` (``nodes`` (W, 4),
     ``weight``) add the soft-term tables (``soft_tables``).
+    ``device`` (``"auto"``, ``"gpu"`` or ``"cuda:N"``) builds the index arrays
+    -- interior classification, the stored DOFs' membership rows sorted by
+    node, ``P_of`` and the energy stencil -- with the core's kernels
+    (``cpp_core.wire_build``); the result is identical to the host build's.
     """
     constraints = constraints or {}
     con_ids = np.array(sorted(constraints), dtype=np.int64)
@@ -165,77 +170,42 @@ def flat_wire(
         np.allclose(w0, w0[0, 0] * np.eye(d)) and (uniform_w or np.allclose(w_inv, w0))
     )
 
-    # Interior-eligible nodes: strictly inside one block on every axis.
-    node_block = np.full(N, -1, dtype=np.int32)
-    node_logical = np.zeros((N, d), dtype=np.int32)
-    if synth_interior:
-        for bi, ids in enumerate(blocks):
-            sh = ids.shape
-            if any(s < 3 for s in sh):
-                continue
-            inner = ids[tuple(slice(1, s - 1) for s in sh)].reshape(-1)
-            grids = np.meshgrid(*[np.arange(1, s - 1, dtype=np.int32) for s in sh], indexing="ij")
-            node_block[inner] = bi
-            node_logical[inner] = np.stack([g.reshape(-1) for g in grids], axis=1)
-    node_block[con_ids] = -1  # constrained nodes always take a stored patch
-    node_interior = node_block >= 0
     moving = np.asarray(free_mask, dtype=bool).copy()
     moving[con_ids] = True
+    stored = None
+    if con_ids.size:
+        stored = np.zeros(N, dtype=bool)
+        stored[con_ids] = True
+    if device is None:
+        arr = _host_arrays(blocks, moving, stored, d, synth_interior, not compact)
+    else:
+        arr = _device_arrays(blocks, moving, stored, d, synth_interior, not compact, device)
+    ns = int(arr["num_samples"])
 
-    C = cell_corner_ids(blocks, d)
-    ncell = C.shape[0]
-    ns = ncell * nc
-    bits = axis_bits(d)
-    bidx = np.arange(nc)
-    sgn = np.where((bidx[:, None] & bits[None, :]) == 0, 1.0, -1.0)
-    role = role_table(d)
-
-    # Membership only for stored-patch DOFs (moving, not interior-eligible):
-    # restrict to cells that touch such a node, so large grids with few stored
-    # DOFs never materialise the full node x sample table.
-    stored_node = moving & ~node_interior
-    touch = stored_node[C]  # (ncell, nc)
-    cells = np.flatnonzero(touch.any(axis=1))
-    Ct = C[cells]  # (m, nc)
-    # Rows (cell, a, b) restricted to stored nodes at corner a.
-    m_node = np.repeat(Ct[:, :, None], nc, axis=2).reshape(-1)
-    m_sid = (nc * cells[:, None, None] + bidx[None, None, :]).repeat(nc, axis=1).reshape(-1)
-    m_role = np.tile(role.reshape(-1), cells.shape[0])
-    keep = stored_node[m_node]
-    m_node, m_sid, m_role = m_node[keep], m_sid[keep], m_role[keep]
-    perm = np.argsort(m_node, kind="stable")
-    m_node, m_sid, m_role = m_node[perm], m_sid[perm], m_role[perm]
-
-    def fields(sid: np.ndarray, *, uniform_out: bool) -> dict:
-        cell = sid // nc
-        b = sid % nc
-        out = {"gc": C[cell, b].astype(np.int32)}
+    def fields(pre: str, sid, rows: int, *, uniform_out: bool) -> dict:
+        out = {"gc": arr[pre + "gc"]}
         for k in range(d):
-            out[f"gn{k}"] = C[cell, b ^ bits[k]].astype(np.int32)
-            out[f"s{k}"] = sgn[b, k].astype(np.float64)
+            out[f"gn{k}"] = arr[f"{pre}gn{k}"]
+            out[f"s{k}"] = arr[f"{pre}s{k}"]
         if uniform_w and uniform_out:
             W = w_inv.reshape(1, dd)
         elif uniform_w:
-            W = np.broadcast_to(w_inv, (sid.shape[0], d, d)).reshape(-1, dd)
+            W = np.broadcast_to(w_inv, (rows, d, d)).reshape(-1, dd)
         else:
             W = w_inv[sid].reshape(-1, dd)
         out["W_inv"] = np.ascontiguousarray(W, dtype=np.float64)
         return out
 
     groups = []
-    dofs = np.flatnonzero(moving)
+    dofs = arr["dof_idx"]
     if dofs.size:
-        P_of = np.zeros(dofs.size, dtype=np.int32)
-        if m_node.size:
-            uniq, cnt = np.unique(m_node, return_counts=True)
-            P_of[np.searchsorted(dofs, uniq)] = cnt
         g = {
             "D": int(dofs.size),
-            "role": m_role.astype(np.int32),
-            "dof_idx": dofs.astype(np.int32),
-            "P_of": P_of,
-            "interior_block": np.ascontiguousarray(node_block[dofs]),
-            "interior_logical": np.ascontiguousarray(node_logical[dofs]),
+            "role": arr["role"],
+            "dof_idx": dofs,
+            "P_of": arr["P_of"],
+            "interior_block": arr["interior_block"],
+            "interior_logical": arr["interior_logical"],
             "entities": {
                 "free": {
                     "tag": 0,
@@ -260,7 +230,7 @@ def flat_wire(
                     seg.append({"data": np.concatenate(parts) if parts else np.zeros(0), "off": off})
                 g["entities"][name]["seg"] = seg
 
-        g.update(fields(m_sid, uniform_out=True))
+        g.update(fields("", arr["sid"], int(arr["role"].size), uniform_out=True))
         g.update(soft_tables(moving, d, directional=directional, curvature=curvature))
         groups.append(g)
 
@@ -269,8 +239,8 @@ def flat_wire(
             raise ValueError("compact wire requires a uniform target")
         es = {"num_samples": int(ns), "structured": 1, "W_inv": w_inv.reshape(1, dd).copy()}
     else:
-        es = {"num_samples": int(ns)}
-        es.update(fields(np.arange(ns, dtype=np.int64), uniform_out=True))
+        es = {"num_samples": ns}
+        es.update(fields("es_", np.arange(ns, dtype=np.int64), ns, uniform_out=True))
     if directional is not None and len(directional["kind"]):
         es.update({
             "dir_num": int(len(directional["kind"])),
@@ -282,6 +252,93 @@ def flat_wire(
             "dir_weight": np.ascontiguousarray(np.asarray(directional["weight"], dtype=np.float64)),
         })
     return {"groups": groups, "energy_stencil": es}
+
+
+def _host_arrays(blocks, moving, stored, d: int, synth_interior: bool, energy_arrays: bool) -> dict:
+    """Index arrays of the wire, vectorised numpy (the layout of
+    ``egg/smoothing/flat_context.py:211-272``): interior-eligible nodes name
+    (block, logical); the membership rows (cell, a, b) of moving, non-interior
+    nodes, stably sorted by node; the energy stencil in sample order."""
+    N = moving.shape[0]
+    nc = 1 << d
+    node_block = np.full(N, -1, dtype=np.int32)
+    node_logical = np.zeros((N, d), dtype=np.int32)
+    if synth_interior:
+        for bi, ids in enumerate(blocks):
+            sh = ids.shape
+            if any(s < 3 for s in sh):
+                continue
+            inner = ids[tuple(slice(1, s - 1) for s in sh)].reshape(-1)
+            grids = np.meshgrid(*[np.arange(1, s - 1, dtype=np.int32) for s in sh], indexing="ij")
+            node_block[inner] = bi
+            node_logical[inner] = np.stack([g.reshape(-1) for g in grids], axis=1)
+    if stored is not None:
+        node_block[stored] = -1  # constrained nodes always take a stored patch
+    node_interior = node_block >= 0
+
+    C = cell_corner_ids(blocks, d)
+    ns = C.shape[0] * nc
+    bits = axis_bits(d)
+    bidx = np.arange(nc)
+    sgn = np.where((bidx[:, None] & bits[None, :]) == 0, 1.0, -1.0)
+    role = role_table(d)
+
+    # Membership only for stored-patch DOFs (moving, not interior-eligible):
+    # restrict to cells that touch such a node, so large grids with few stored
+    # DOFs never materialise the full node x sample table.
+    stored_node = moving & ~node_interior
+    touch = stored_node[C]  # (ncell, nc)
+    cells = np.flatnonzero(touch.any(axis=1))
+    Ct = C[cells]  # (m, nc)
+    # Rows (cell, a, b) restricted to stored nodes at corner a.
+    m_node = np.repeat(Ct[:, :, None], nc, axis=2).reshape(-1)
+    m_sid = (nc * cells[:, None, None] + bidx[None, None, :]).repeat(nc, axis=1).reshape(-1)
+    m_role = np.tile(role.reshape(-1), cells.shape[0])
+    keep = stored_node[m_node]
+    m_node, m_sid, m_role = m_node[keep], m_sid[keep], m_role[keep]
+    perm = np.argsort(m_node, kind="stable")
+    m_node, m_sid, m_role = m_node[perm], m_sid[perm], m_role[perm]
+
+    dofs = np.flatnonzero(moving)
+    P_of = np.zeros(dofs.size, dtype=np.int32)
+    if m_node.size:
+        uniq, cnt = np.unique(m_node, return_counts=True)
+        P_of[np.searchsorted(dofs, uniq)] = cnt
+    out = {
+        "num_samples": ns,
+        "dof_idx": dofs.astype(np.int32),
+        "P_of": P_of,
+        "interior_block": np.ascontiguousarray(node_block[dofs]),
+        "interior_logical": np.ascontiguousarray(node_logical[dofs]),
+        "role": m_role.astype(np.int32),
+        "sid": m_sid,
+    }
+
+    def rows(pre: str, sid: np.ndarray) -> None:
+        cell = sid // nc
+        b = sid % nc
+        out[pre + "gc"] = C[cell, b].astype(np.int32)
+        for k in range(d):
+            out[f"{pre}gn{k}"] = C[cell, b ^ bits[k]].astype(np.int32)
+            out[f"{pre}s{k}"] = sgn[b, k].astype(np.float64)
+
+    rows("", m_sid)
+    if energy_arrays:
+        rows("es_", np.arange(ns, dtype=np.int64))
+    return out
+
+
+def _device_arrays(blocks, moving, stored, d: int, synth_interior: bool, energy_arrays: bool, device: str) -> dict:
+    """The same index arrays built on the GPU (``cpp_core.wire_build``)."""
+    from . import load_core
+
+    core = load_core()
+    shapes = np.array([b.shape for b in blocks], dtype=np.int32).reshape(-1)
+    ids = (np.concatenate([np.asarray(b, dtype=np.int64).reshape(-1) for b in blocks])
+           if blocks else np.zeros(0, dtype=np.int64))
+    return core.wire_build(d, shapes, ids, moving.view(np.uint8),
+                           None if stored is None else stored.view(np.uint8),
+                           synth_interior=synth_interior, energy_arrays=energy_arrays, device=device)
 
 
 DIR_ARITY = {0: 2, 1: 3, 2: 2}  # parallel, line, stem; other kinds are reserved (arity 0)

@@ -608,6 +608,56 @@ int egg_b200_directional_eval(int32_t dim, const double* X, int64_t n_nodes, int
                               const int32_t* kind, const double* ref, const double* weight, double eps,
                               double* energy, double* grad);
 
+/* Device-side wire build: the bulk index arrays of the sweep-context wire,
+ * computed by kernels from the blocks' global node ids.  Replaces the array
+ * work of egg/smoothing/flat_context.py:136-346 (build_flat_context, with
+ * its cell_stencil at :40-121); the per-entity partitions, soft-term tables
+ * and W_inv rows stay with the host caller.  Outputs equal the reference
+ * builder's bit for bit:
+ *   group: dof_idx, P_of, interior_block, interior_logical [n_dofs*dim],
+ *          role, gc, gn0..gn{dim-1} (int32) and s0..s{dim-1} (float64) [n_rows];
+ *   energy stencil (energy_arrays != 0): gc, gn*, s* [n_samples].
+ * moving[n] = 1 marks a moving DOF (Free or constrained); stored[n] = 1
+ * (optional) forces a stored patch (constrained DOFs; their interior_logical
+ * is still filled, interior_block is -1).  synth_interior = 1 when the target
+ * is a uniform multiple of the identity: interior-eligible DOFs then carry no
+ * rows.  Node ids must lie in [0, num_nodes) (EGG_B200_EINVAL otherwise) and
+ * fit int32 (EGG_B200_ENOTSUP).  device < 0 uses the current device.
+ * build keeps the arrays on the device; sizes gives {n_dofs, n_rows,
+ * n_samples}; download copies every non-NULL output (host memory sized from
+ * sizes); destroy frees them. */
+typedef struct egg_b200_wire egg_b200_wire;
+typedef struct egg_b200_wire_desc {
+    int32_t dim;
+    int32_t num_blocks;
+    const int32_t* shapes;    /* [num_blocks * dim] nodes per axis */
+    const int64_t* block_ids; /* global ids of every block's nodes, C order, blocks back to back */
+    int64_t num_nodes;
+    const uint8_t* moving;    /* [num_nodes] */
+    const uint8_t* stored;    /* [num_nodes] or NULL */
+    int32_t synth_interior;
+    int32_t energy_arrays;
+    int32_t device;
+} egg_b200_wire_desc;
+typedef struct egg_b200_wire_out {
+    int32_t* dof_idx;
+    int32_t* P_of;
+    int32_t* interior_block;
+    int32_t* interior_logical;
+    int32_t* role;
+    int64_t* sid;             /* [n_rows] sample id of each row (2^dim * cell + corner) */
+    int32_t* gc;
+    int32_t* gn[3];
+    double* s[3];
+    int32_t* es_gc;
+    int32_t* es_gn[3];
+    double* es_s[3];
+} egg_b200_wire_out;
+int egg_b200_wire_build(const egg_b200_wire_desc* desc, egg_b200_wire** out);
+int egg_b200_wire_sizes(egg_b200_wire* w, int64_t* sizes);
+int egg_b200_wire_download(egg_b200_wire* w, const egg_b200_wire_out* out);
+int egg_b200_wire_destroy(egg_b200_wire* w);
+
 #ifdef __cplusplus
 }
 #endif
