@@ -404,6 +404,37 @@ def run_workload(args):
     return 0
 
 
+def side_configs(args, local):
+    """The other benchmark configurations (bench_workloads.py: the 5-block
+    disk, the 1025^2 untangle, the 7-block sphere FAS, the 256-mesh batch),
+    each on a short sample -- at most 2 timed steps after 1 warm-up, bounded
+    reference-core samples -- so the default run reports every configuration.
+    A failing configuration reports its error instead of a value."""
+    import types
+
+    import torch
+
+    import bench_workloads
+    from egg_b200 import cpp_core
+
+    sub = types.SimpleNamespace(steps=max(1, min(args.steps, 2)), warmup=1, no_cpu_baseline=args.no_cpu_baseline,
+                                cpu_target_s=3.0)
+    out = {}
+    for name, fn in bench_workloads.WORKLOADS.items():
+        t0 = time.perf_counter()
+        try:
+            with ClockSampler(local) as clk:
+                line = fn(torch, cpp_core, sub, local)
+            line["clocks"] = clk.summary()
+            line["steps"], line["warmup"] = sub.steps, sub.warmup
+        except Exception as exc:  # reported in the line, the headline stands
+            line = {"workload": name, "error": f"{type(exc).__name__}: {exc}"}
+        line["wall_s"] = time.perf_counter() - t0
+        out[name] = line
+        torch.cuda.empty_cache()
+    return out
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -417,6 +448,8 @@ def main():
     ap.add_argument("--n", type=int, default=N_SIDE, help="grid side (profiling runs)")
     ap.add_argument("--variant", type=int, default=None,
                     help="pin the interior-kernel variant instead of autotuning (profiling runs)")
+    ap.add_argument("--no-configs", action="store_true",
+                    help="skip the other configurations' short samples in the default line")
     ap.add_argument("--workload", default="square4097",
                     help="square4097 (default), disk_oh65, untangle1025, sphere129_fas, batch256")
     args = ap.parse_args()
@@ -576,6 +609,8 @@ def main():
     }
     if not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline()
+    if ws == 1 and not args.no_configs and args.only is None and args.n == N_SIDE:
+        line["configs"] = side_configs(args, local)
     print(json.dumps(line))
     if dist is not None:
         dist.destroy_process_group()

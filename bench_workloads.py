@@ -61,6 +61,12 @@ def _cpu(kind, sample, value):
     return {"value": value, "unit": UNIT, "cores": os.cpu_count(), "kind": kind, "sample": sample}
 
 
+def _cpu_target(args, default: float) -> float:
+    """Seconds of reference-core work per CPU baseline (shorter when the
+    workload runs as a side configuration of the default bench)."""
+    return float(getattr(args, "cpu_target_s", None) or default)
+
+
 def _omp():
     os.environ.setdefault("OMP_NUM_THREADS", str(os.cpu_count()))
 
@@ -70,7 +76,8 @@ def disk_oh65(torch, cpp_core, args, local):
     from oracle import oracle
 
     g = configs.disk_oh(65, frac=0.25, seed=0)
-    s = cpp_core.CppStructuredSweepSession(g.wire(compact=True), g.structured(), g.X_flat(), precision="fp64")
+    s = cpp_core.CppStructuredSweepSession(g.wire(compact=True, device=f"cuda:{local}"), g.structured(), g.X_flat(),
+                                           precision="fp64")
     s.autotune("barrier", 3)
     s.checkpoint()
     F = g.num_free
@@ -107,7 +114,7 @@ def disk_oh65(torch, cpp_core, args, local):
         r.run(1)
         t0 = time.perf_counter()
         reps = 0
-        while time.perf_counter() - t0 < 5.0:
+        while time.perf_counter() - t0 < _cpu_target(args, 5.0):
             r.run(40, report_every=20)
             reps += 1
         dt_r = time.perf_counter() - t0
@@ -172,7 +179,7 @@ def untangle1025(torch, cpp_core, args, local):
         _omp()
         v, n, dt = _ref_rate(lambda: ref.CppStructuredSweepSession(g.wire(), g.structured(), g.X_flat(),
                                                                    device="cpu"),
-                             5, F, phase="untangle", delta=1e-4, omega=0.5)
+                             5, F, target_s=_cpu_target(args, 10.0), phase="untangle", delta=1e-4, omega=0.5)
         line["cpu_baseline"] = _cpu("reference", f"untangle sweeps on the full grid, {n} sweeps in {dt:.1f} s", v)
     return line
 
@@ -183,8 +190,8 @@ def sphere129_fas(torch, cpp_core, args, local):
 
     n = int(os.environ.get("EGG_B200_SPHERE_N", "129"))
     g = configs.sphere_in_cube(n, frac=0.2, seed=0)
-    s = cpp_core.CppStructuredSweepSession(g.wire(compact=True), g.structured(), g.X_flat(), dim=3,
-                                           precision="mixed")
+    s = cpp_core.CppStructuredSweepSession(g.wire(compact=True, device=f"cuda:{local}"), g.structured(), g.X_flat(),
+                                           dim=3, precision="mixed")
     E0, M0 = s.energy()
     # the +-0.2h noise inverts a few thousand samples at the skewed shell
     # corners: untangle first (delta continuation), as the pipeline does
@@ -229,7 +236,8 @@ def sphere129_fas(torch, cpp_core, args, local):
         _omp()
         gs = configs.sphere_in_cube(33, frac=0.2, seed=0)
         v, nn, dt_r = _ref_rate(lambda: ref.CppStructuredSweepSession(gs.wire(), gs.structured(), gs.X_flat(),
-                                                                      device="cpu", dim=3), 2, gs.num_free)
+                                                                      device="cpu", dim=3), 2, gs.num_free,
+                              target_s=_cpu_target(args, 10.0))
         line["cpu_baseline"] = _cpu("reference", f"Jacobi sweeps on the 7 x 33^3 sphere-in-cube, {nn} sweeps in "
                                                  f"{dt_r:.1f} s", v)
     return line
@@ -279,13 +287,13 @@ def batch256(torch, cpp_core, args, local):
     ref = oracle.load_ref("fp64")
     if ref is not None and not args.no_cpu_baseline:
         _omp()
-        sample = ms[:16]
+        sample = ms[:16] if _cpu_target(args, 10.0) >= 10.0 else ms[:4]
         t0 = time.perf_counter()
         for g in sample:
             r = ref.CppStructuredSweepSession(g.wire(), g.structured(), g.X_flat(), device="cpu")
             r.run(20, report_every=20)
         dt_r = time.perf_counter() - t0
-        line["cpu_baseline"] = _cpu("reference", f"the first 16 meshes, one session and 20 sweeps each, "
+        line["cpu_baseline"] = _cpu("reference", f"the first {len(sample)} meshes, one session and 20 sweeps each, "
                                                  f"{dt_r:.1f} s (session build included)",
                                     sum(g.num_free for g in sample) * 20 / dt_r)
     return line
