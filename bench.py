@@ -539,9 +539,14 @@ def main():
     value = ws * F * sweeps * args.steps / mixed["dt"]
     v64 = ws * F * sweeps * args.steps / results["fp64"]["dt"]
 
-    # e2e through the public API with host buffers (mixed precision).
+    # e2e through the public API with host buffers (mixed precision).  The
+    # step's input sits in page-locked host memory -- a get_X result, which
+    # the core hands out from its pinned pool -- so set_X and get_X are one
+    # DMA each.
     s = mixed["session"]
-    Xh = np.ascontiguousarray(X0)
+    s.set_X(np.ascontiguousarray(X0))
+    Xh = s.get_X()
+    assert np.array_equal(Xh, X0)
     s.set_X(Xh)
     s.run(sweeps)
     warm = [s.get_X(), s.get_X()]  # warm-up: the loop below holds one result while fetching the next

@@ -213,7 +213,6 @@ void fill_desc(Desc& D, const py::dict& ctx, const py::dict& st, const DArr& X, 
         D.tags.assign(size_t(d.ndof), -1);
         bool constrained = false;
         if (g.contains("entities")) {
-            D.eparams.assign(size_t(d.ndof) * EGG_B200_ENTITY_FIELDS, 0.0);
             for (auto item : g["entities"].cast<py::dict>()) {
                 py::dict ed = item.second.cast<py::dict>();
                 if (!ed.contains("tag")) {
@@ -250,6 +249,9 @@ void fill_desc(Desc& D, const py::dict& ctx, const py::dict& st, const DArr& X, 
                         seg_off.push_back(off);
                     }
                 }
+                // records of constrained DOFs only: a wire of Free DOFs (every
+                // structured interior) allocates none
+                if (tag != 0 && D.eparams.empty()) { D.eparams.assign(size_t(d.ndof) * EGG_B200_ENTITY_FIELDS, 0.0); }
                 if (tag == EGG_B200_TAG_BSPLINE && seg_off.size() < 2) {
                     throw py::value_error("validate_context: a B-spline partition needs its knots and ctrl seg fields");
                 }

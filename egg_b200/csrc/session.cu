@@ -72,17 +72,26 @@ template <class T> struct DevBuf {
         if (count) { EGG_CK(cudaMalloc(reinterpret_cast<void**>(&p), count * sizeof(T))); }
         n = count;
     }
+    // A cudaMemcpy from pageable memory may return before its DMA lands, and
+    // the sessions' streams do not wait for the legacy stream: the copy is
+    // complete when upload() returns, so kernels on any stream see it.
     void upload(const std::vector<T>& h)
     {
         alloc(h.size());
-        if (n) { EGG_CK(cudaMemcpy(p, h.data(), n * sizeof(T), cudaMemcpyHostToDevice)); }
+        copy_in(h);
     }
     // upload() that keeps an allocation of the same size; only for buffers
     // that no queued work still reads (the caller has synchronised).
     void put(const std::vector<T>& h)
     {
         if (h.size() != n) { alloc(h.size()); }
-        if (n) { EGG_CK(cudaMemcpy(p, h.data(), n * sizeof(T), cudaMemcpyHostToDevice)); }
+        copy_in(h);
+    }
+    void copy_in(const std::vector<T>& h)
+    {
+        if (!n) { return; }
+        EGG_CK(cudaMemcpy(p, h.data(), n * sizeof(T), cudaMemcpyHostToDevice));
+        EGG_CK(cudaStreamSynchronize(cudaStreamLegacy));
     }
 };
 
@@ -346,6 +355,74 @@ struct Session : LevelData {
 
     double* X(int i) { return Xbuf[i].p; }
 };
+
+// ---------------------------------------------------------------------------
+// X in global node order <-> the packed store
+// ---------------------------------------------------------------------------
+// store slot i <- X[slot_gid[i]]: every copy of a node takes its value.
+template <int D>
+__global__ void gather_global_kernel(const double* __restrict__ Xg, const int32_t* __restrict__ slot_gid, int64_t n,
+                                     double* __restrict__ store)
+{
+    for (int64_t i = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; i < n; i += int64_t(gridDim.x) * blockDim.x) {
+        const int64_t g = slot_gid[i];
+        if constexpr (D == 2) {
+            reinterpret_cast<double2*>(store)[i] = reinterpret_cast<const double2*>(Xg)[g];
+        } else {
+#pragma unroll
+            for (int k = 0; k < D; ++k) { store[i * D + k] = Xg[g * D + k]; }
+        }
+    }
+}
+
+// X[g] <- store[g2s[g]] (the owner slot) for every node in a block; nodes in
+// no block are left for the host to fill.
+template <int D>
+__global__ void scatter_global_kernel(const double* __restrict__ store, const int32_t* __restrict__ g2s, int64_t M,
+                                      double* __restrict__ Xg)
+{
+    for (int64_t g = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; g < M; g += int64_t(gridDim.x) * blockDim.x) {
+        const int64_t s = g2s[g];
+        if (s < 0) { continue; }
+        if constexpr (D == 2) {
+            reinterpret_cast<double2*>(Xg)[g] = reinterpret_cast<const double2*>(store)[s];
+        } else {
+#pragma unroll
+            for (int k = 0; k < D; ++k) { Xg[g * D + k] = store[s * D + k]; }
+        }
+    }
+}
+
+// Grid of the remap kernels: one thread per item up to 8 CTAs per SM.
+static int remap_grid(int64_t n) { return int(std::max<int64_t>(1, std::min<int64_t>((n + 255) / 256, 148 * 8))); }
+
+// Host copy threads for a transfer of `bytes`: one per 4 MiB slice, at most
+// the hardware threads and kMaxCopyThreads.
+static int copy_threads(size_t bytes)
+{
+    const size_t hw = std::max(1u, std::thread::hardware_concurrency());
+    const size_t by_size = bytes >> 22;
+    return int(std::max<size_t>(1, std::min({hw, size_t(kMaxCopyThreads), by_size})));
+}
+
+// Runs body(t) for t in [0, T): slice 0 on the calling thread, the others on
+// new threads (inline when a thread cannot be started).  body must not throw.
+template <class F> static void run_slices(int T, F&& body)
+{
+    std::vector<std::thread> th;
+    th.reserve(size_t(std::max(T - 1, 0)));
+    int started = 1;
+    try {
+        for (; started < T; ++started) { th.emplace_back(body, started); }
+    } catch (...) {
+    }
+    for (int t = started; t < T; ++t) { body(t); }
+    body(0);
+    for (auto& x : th) { x.join(); }
+}
+
+// Slice t of T over n doubles.
+static inline size_t slice_begin(size_t n, int t, int T) { return n * size_t(t) / size_t(T); }
 
 // ---------------------------------------------------------------------------
 // Session construction
@@ -1013,32 +1090,50 @@ static Session* create_session(const egg_b200_session_desc& d)
             require_ptr(d.es_gn[k], ns, "energy_stencil gn");
             require_ptr(d.es_s[k], ns, "energy_stencil s");
         }
-        for (int64_t i = 0; i < ns; ++i) {
-            auto chk = [&](int32_t v) {
-                if (v < 0 || v >= M) {
-                    invalid("validate_context: energy_stencil index " + std::to_string(v) + " out of range [0, " +
-                            std::to_string(M) + ")");
+        // Index checks and the canonical-form test run on host threads over
+        // slices of the samples (cells); a failure reports the first bad
+        // sample in sample order, as a serial scan would.
+        const int T = copy_threads(size_t(ns) * 64);
+        std::vector<int64_t> bad_at(T, -1);
+        std::vector<int32_t> bad_val(T, 0);
+        run_slices(T, [&](int t) {
+            const int64_t i0 = int64_t(slice_begin(size_t(ns), t, T)), i1 = int64_t(slice_begin(size_t(ns), t + 1, T));
+            for (int64_t i = i0; i < i1; ++i) {
+                for (int k = -1; k < D; ++k) {
+                    const int32_t v = k < 0 ? d.es_gc[i] : d.es_gn[k][i];
+                    if (v < 0 || v >= M || S->g2s[v] < 0) {
+                        bad_at[t] = i;
+                        bad_val[t] = v;
+                        return;
+                    }
                 }
-                if (S->g2s[v] < 0) {
-                    invalid("structured: an energy-stencil index references a global node absent from every "
-                            "block's interior map");
-                }
-            };
-            chk(d.es_gc[i]);
-            for (int k = 0; k < D; ++k) { chk(d.es_gn[k][i]); }
+            }
+        });
+        for (int t = 0; t < T; ++t) {
+            if (bad_at[t] < 0) { continue; }
+            const int32_t v = bad_val[t];
+            if (v < 0 || v >= M) {
+                invalid("validate_context: energy_stencil index " + std::to_string(v) + " out of range [0, " +
+                        std::to_string(M) + ")");
+            }
+            invalid("structured: an energy-stencil index references a global node absent from every "
+                    "block's interior map");
         }
         // Canonical cell stencil of the blocks?  Sample 2^D * cell + b:
         // corner at cell base + bits(b) (axis 0 most significant), axis-k
         // neighbour at corner ^ bit_k, sign -1 where bit k of b is set.
         if (ns == ncell * nc) {
-            structured = true;
-            for (int b = 0; b < nb && structured; ++b) {
-                const BlockInfo& bi = S->blocks_h[b];
-                const int64_t c0 = std::max(0, bi.n[0] - 1), c1 = std::max(0, bi.n[1] - 1);
-                const int64_t c2 = D == 3 ? std::max(0, bi.n[2] - 1) : 1;
-                const int64_t cells = c0 * c1 * c2;
-                for (int64_t lc = 0; lc < cells && structured; ++lc) {
-                    const int64_t i = lc / (c1 * c2), j = (lc / c2) % c1, k = lc % c2;
+            std::vector<uint8_t> ok(T, 1);
+            run_slices(T, [&](int t) {
+                const int64_t c0 = int64_t(slice_begin(size_t(ncell), t, T));
+                const int64_t c1 = int64_t(slice_begin(size_t(ncell), t + 1, T));
+                int b = 0;
+                for (int64_t cell = c0; cell < c1; ++cell) {
+                    while (cell >= cell_off[b + 1]) { ++b; }
+                    const BlockInfo& bi = S->blocks_h[b];
+                    const int64_t c1b = std::max(0, bi.n[1] - 1), c2b = D == 3 ? std::max(0, bi.n[2] - 1) : 1;
+                    const int64_t lc = cell - cell_off[b];
+                    const int64_t i = lc / (c1b * c2b), j = (lc / c2b) % c1b, k = lc % c2b;
                     int32_t cg[8];
                     for (int a = 0; a < nc; ++a) {
                         int64_t u, v, w;
@@ -1053,19 +1148,23 @@ static Session* create_session(const egg_b200_session_desc& d)
                         }
                         cg[a] = S->slot_gid[bi.off + (u * bi.n[1] + v) * bi.n[2] + w];
                     }
-                    const int64_t cell = cell_off[b] + lc;
-                    for (int bb = 0; bb < nc && structured; ++bb) {
+                    for (int bb = 0; bb < nc; ++bb) {
                         const int64_t sid = cell * nc + bb;
-                        if (d.es_gc[sid] != cg[bb]) { structured = false; }
-                        for (int ax = 0; ax < D && structured; ++ax) {
+                        if (d.es_gc[sid] != cg[bb]) {
+                            ok[t] = 0;
+                            return;
+                        }
+                        for (int ax = 0; ax < D; ++ax) {
                             const int bit = 1 << (D - 1 - ax);
                             if (d.es_gn[ax][sid] != cg[bb ^ bit] || d.es_s[ax][sid] != ((bb & bit) ? -1.0 : 1.0)) {
-                                structured = false;
+                                ok[t] = 0;
+                                return;
                             }
                         }
                     }
                 }
-            }
+            });
+            structured = std::all_of(ok.begin(), ok.end(), [](uint8_t x) { return x != 0; });
         }
     }
     S->es_struct = structured;
@@ -1098,21 +1197,25 @@ static Session* create_session(const egg_b200_session_desc& d)
         es_b1.resize(ns);
         es_s0h.resize(ns);
         es_s1h.resize(ns);
-        for (int64_t i = 0; i < ns; ++i) {
-            es_a[i] = S->g2s[d.es_gc[i]];
-            es_b0[i] = S->g2s[d.es_gn[0][i]];
-            es_b1[i] = S->g2s[d.es_gn[1][i]];
-            es_s0h[i] = d.es_s[0][i] < 0 ? -1 : 1;
-            es_s1h[i] = d.es_s[1][i] < 0 ? -1 : 1;
-        }
         if (D == 3) {
             es_b2.resize(ns);
             es_s2h.resize(ns);
-            for (int64_t i = 0; i < ns; ++i) {
-                es_b2[i] = S->g2s[d.es_gn[2][i]];
-                es_s2h[i] = d.es_s[2][i] < 0 ? -1 : 1;
-            }
         }
+        const int T = copy_threads(size_t(ns) * 64);
+        run_slices(T, [&](int t) {
+            const int64_t i0 = int64_t(slice_begin(size_t(ns), t, T)), i1 = int64_t(slice_begin(size_t(ns), t + 1, T));
+            for (int64_t i = i0; i < i1; ++i) {
+                es_a[i] = S->g2s[d.es_gc[i]];
+                es_b0[i] = S->g2s[d.es_gn[0][i]];
+                es_b1[i] = S->g2s[d.es_gn[1][i]];
+                es_s0h[i] = d.es_s[0][i] < 0 ? -1 : 1;
+                es_s1h[i] = d.es_s[1][i] < 0 ? -1 : 1;
+                if (D == 3) {
+                    es_b2[i] = S->g2s[d.es_gn[2][i]];
+                    es_s2h[i] = d.es_s[2][i] < 0 ? -1 : 1;
+                }
+            }
+        });
     }
 
     S->active_h = std::move(active);
@@ -1214,12 +1317,37 @@ static Session* create_session(const egg_b200_session_desc& d)
     }
     S->sh_src.upload(sh_src);
     S->sh_dst.upload(sh_dst);
-    std::vector<double> Xs(off * D);
-    for (int64_t i = 0; i < off; ++i) {
-        for (int k = 0; k < D; ++k) { Xs[i * D + k] = d.X[int64_t(S->slot_gid[i]) * D + k]; }
+    // The packed store is filled on the device: X goes up in global node
+    // order and every slot gathers its node, the X remap of the reference's
+    // apply_structured_remap (src/bindings.cpp:757-1101) as one kernel.  The
+    // global-order buffer and the slot and owner tables stay for later
+    // transfers.
+    // (The copies go on the session stream, which orders them before the
+    // gather; a pageable cudaMemcpy may return before its DMA lands.)
+    S->slot_gid_d.alloc(S->slot_gid.size());
+    if (off) {
+        EGG_CK(cudaMemcpyAsync(S->slot_gid_d.p, S->slot_gid.data(), size_t(off) * sizeof(int32_t),
+                               cudaMemcpyHostToDevice, S->stream));
     }
-    S->Xbuf[0].upload(Xs);
-    S->Xbuf[1].alloc(Xs.size());
+    S->g2s_d.alloc(S->g2s.size());
+    if (M) {
+        EGG_CK(cudaMemcpyAsync(S->g2s_d.p, S->g2s.data(), size_t(M) * sizeof(int32_t), cudaMemcpyHostToDevice,
+                               S->stream));
+    }
+    S->Xg.alloc(size_t(M) * D);
+    if (M) {
+        EGG_CK(cudaMemcpyAsync(S->Xg.p, d.X, size_t(M) * D * sizeof(double), cudaMemcpyHostToDevice, S->stream));
+    }
+    S->Xbuf[0].alloc(size_t(off) * D);
+    S->Xbuf[1].alloc(size_t(off) * D);
+    if (off) {
+        if (D == 2) {
+            gather_global_kernel<2><<<remap_grid(off), 256, 0, S->stream>>>(S->Xg.p, S->slot_gid_d.p, off, S->Xbuf[0].p);
+        } else {
+            gather_global_kernel<3><<<remap_grid(off), 256, 0, S->stream>>>(S->Xg.p, S->slot_gid_d.p, off, S->Xbuf[0].p);
+        }
+        EGG_CK(cudaGetLastError());
+    }
     S->cur = 0;
     S->red_grid = 148 * 4;
     S->part.alloc(3 * size_t(S->red_grid));
@@ -2083,70 +2211,6 @@ struct egg_b200_session {
     Session* impl;
 };
 
-// ---------------------------------------------------------------------------
-// X in global node order <-> the packed store
-// ---------------------------------------------------------------------------
-// store slot i <- X[slot_gid[i]]: every copy of a node takes its value.
-template <int D>
-__global__ void gather_global_kernel(const double* __restrict__ Xg, const int32_t* __restrict__ slot_gid, int64_t n,
-                                     double* __restrict__ store)
-{
-    for (int64_t i = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; i < n; i += int64_t(gridDim.x) * blockDim.x) {
-        const int64_t g = slot_gid[i];
-        if constexpr (D == 2) {
-            reinterpret_cast<double2*>(store)[i] = reinterpret_cast<const double2*>(Xg)[g];
-        } else {
-#pragma unroll
-            for (int k = 0; k < D; ++k) { store[i * D + k] = Xg[g * D + k]; }
-        }
-    }
-}
-
-// X[g] <- store[g2s[g]] (the owner slot) for every node in a block; nodes in
-// no block are left for the host to fill.
-template <int D>
-__global__ void scatter_global_kernel(const double* __restrict__ store, const int32_t* __restrict__ g2s, int64_t M,
-                                      double* __restrict__ Xg)
-{
-    for (int64_t g = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; g < M; g += int64_t(gridDim.x) * blockDim.x) {
-        const int64_t s = g2s[g];
-        if (s < 0) { continue; }
-        if constexpr (D == 2) {
-            reinterpret_cast<double2*>(Xg)[g] = reinterpret_cast<const double2*>(store)[s];
-        } else {
-#pragma unroll
-            for (int k = 0; k < D; ++k) { Xg[g * D + k] = store[s * D + k]; }
-        }
-    }
-}
-
-// Host copy threads for a transfer of `bytes`: one per 4 MiB slice, at most
-// the hardware threads and kMaxCopyThreads.
-static int copy_threads(size_t bytes)
-{
-    const size_t hw = std::max(1u, std::thread::hardware_concurrency());
-    const size_t by_size = bytes >> 22;
-    return int(std::max<size_t>(1, std::min({hw, size_t(kMaxCopyThreads), by_size})));
-}
-
-// Runs body(t) for t in [0, T): slice 0 on the calling thread, the others on
-// new threads (inline when a thread cannot be started).  body must not throw.
-template <class F> static void run_slices(int T, F&& body)
-{
-    std::vector<std::thread> th;
-    th.reserve(size_t(std::max(T - 1, 0)));
-    int started = 1;
-    try {
-        for (; started < T; ++started) { th.emplace_back(body, started); }
-    } catch (...) {
-    }
-    for (int t = started; t < T; ++t) { body(t); }
-    body(0);
-    for (auto& x : th) { x.join(); }
-}
-
-// Slice t of T over n doubles.
-static inline size_t slice_begin(size_t n, int t, int T) { return n * size_t(t) / size_t(T); }
 
 static void ensure_xfer(Session& S)
 {
@@ -2169,7 +2233,6 @@ static void reset_seeds(Session& S)
     if (S.n_bspline) { EGG_CK(cudaMemsetAsync(S.seeds.p, 0xFF, S.seeds.n * sizeof(double), S.stream)); }
 }
 
-static int remap_grid(int64_t n) { return int(std::max<int64_t>(1, std::min<int64_t>((n + 255) / 256, 148 * 8))); }
 
 extern "C" {
 
@@ -2651,20 +2714,29 @@ int egg_b200_session_set_X(egg_b200_session* s, const double* X, int64_t len)
         EGG_CK(cudaSetDevice(S.device));
         ensure_xfer(S);
         const size_t n = size_t(len);
-        // Host thread t stages slice t in pinned memory and queues its H2D, so
-        // the DMA of early slices overlaps the staging of later ones.
-        const int T = copy_threads(n * sizeof(double));
+        // Page-locked input: one DMA straight from it.  Otherwise host thread
+        // t stages slice t in pinned memory and queues its H2D, so the DMA of
+        // early slices overlaps the staging of later ones.
+        cudaPointerAttributes attr {};
+        const bool pinned = cudaPointerGetAttributes(&attr, X) == cudaSuccess && attr.type == cudaMemoryTypeHost;
+        cudaGetLastError();
+        if (pinned && n) {
+            EGG_CK(cudaMemcpyAsync(S.Xg.p, X, n * sizeof(double), cudaMemcpyHostToDevice, S.stream));
+        }
+        const int T = pinned ? 0 : copy_threads(n * sizeof(double));
         cudaError_t err[kMaxCopyThreads] = {};
-        run_slices(T, [&](int t) {
-            const size_t a = slice_begin(n, t, T), b = slice_begin(n, t + 1, T);
-            if (b == a) { return; }
-            std::memcpy(S.pin + a, X + a, (b - a) * sizeof(double));
-            err[t] = cudaSetDevice(S.device);
-            if (err[t] == cudaSuccess) {
-                err[t] = cudaMemcpyAsync(S.Xg.p + a, S.pin + a, (b - a) * sizeof(double), cudaMemcpyHostToDevice,
-                                         S.stream);
-            }
-        });
+        if (T > 0) {
+            run_slices(T, [&](int t) {
+                const size_t a = slice_begin(n, t, T), b = slice_begin(n, t + 1, T);
+                if (b == a) { return; }
+                std::memcpy(S.pin + a, X + a, (b - a) * sizeof(double));
+                err[t] = cudaSetDevice(S.device);
+                if (err[t] == cudaSuccess) {
+                    err[t] = cudaMemcpyAsync(S.Xg.p + a, S.pin + a, (b - a) * sizeof(double), cudaMemcpyHostToDevice,
+                                             S.stream);
+                }
+            });
+        }
         for (int t = 0; t < T; ++t) { EGG_CK(err[t]); }
         if (S.nstore) {
             if (D == 2) {

@@ -128,3 +128,20 @@ def test_constrained_dofs_are_rejected(core):
                     "records": np.zeros(4 * grp["D"])}}
     with pytest.raises((NotImplementedError, RuntimeError)):
         core.CppStructuredSweepSession({**ctx, "groups": [{**grp, "entities": ent}]}, st, X)
+
+
+def test_energy_stencil_checks_on_many_threads_report_the_first_bad_sample(core):
+    """The reference-form stencil is validated on host threads over sample
+    slices (257^2: 262,144 samples, several slices); a bad index in a late
+    slice is still found, and with two bad samples the earlier one is
+    reported, as a serial scan would (src/bindings.cpp:98-252 messages)."""
+    g = configs.unit_square(257, frac=0.2, seed=0)
+    ctx, st, X = g.wire(), g.structured(), g.X_flat()
+    es = ctx["energy_stencil"]
+    ns = es["num_samples"]
+    gn1 = es["gn1"].copy()
+    gn1[ns - 3] = g.num_nodes + 5
+    _expect_value_error(core, {**ctx, "energy_stencil": {**es, "gn1": gn1}}, st, X, f"index {g.num_nodes + 5} out")
+    gc = es["gc"].copy()
+    gc[ns // 3] = -7
+    _expect_value_error(core, {**ctx, "energy_stencil": {**es, "gn1": gn1, "gc": gc}}, st, X, "index -7 out")

@@ -353,3 +353,22 @@ def test_get_x_results_are_independent_pooled_arrays(gpu):
     assert not np.array_equal(c, b_copy)
     s.set_X(c)
     np.testing.assert_array_equal(s.get_X(), c)
+
+
+def test_set_X_from_page_locked_and_pageable_buffers(gpu):
+    """set_X takes one DMA from a page-locked array (a get_X result comes from
+    the core's pinned pool) and threaded staging from pageable memory; both
+    land the same positions, and a later sweep starts from them."""
+    g = configs.disk_oh(17, frac=0.25, seed=2)
+    s = gpu.CppStructuredSweepSession(g.wire(), g.structured(), g.X_flat(), device="cuda:0")
+    s.run(3)
+    Xp = s.get_X()
+    Xq = np.array(Xp, copy=True)
+    t = gpu.CppStructuredSweepSession(g.wire(), g.structured(), g.X_flat(), device="cuda:0")
+    t.set_X(Xp)
+    np.testing.assert_array_equal(t.get_X(), Xq)
+    Ea, _ = t.run(2, report_every=1)
+    t.set_X(Xq)
+    np.testing.assert_array_equal(t.get_X(), Xq)
+    Eb, _ = t.run(2, report_every=1)
+    np.testing.assert_array_equal(Ea, Eb)

@@ -112,3 +112,28 @@ def test_device_wire_edge_cases(gpu):
     with pytest.raises(ValueError, match="block_ids length"):
         core.wire_build(2, np.array([3, 4], dtype=np.int32), np.arange(11, dtype=np.int64),
                         np.zeros(12, dtype=np.uint8))
+
+
+@pytest.mark.parametrize("make", [lambda: configs.unit_square(513, frac=0.3, seed=1),
+                                  lambda: configs.disk_oh(65, frac=0.25, seed=0)], ids=["square513", "disk_oh65"])
+def test_reference_form_wire_sessions(gpu, make):
+    """A reference-form wire (per-sample energy-stencil arrays, checked and
+    remapped on host threads) gives the compact wire's sweeps bit for bit;
+    with its samples permuted (no longer the canonical stencil) it takes
+    the stored-stencil reduction, whose energies agree to rounding."""
+    g = make()
+    full, comp = g.wire(device="cuda:0"), g.wire(compact=True, device="cuda:0")
+    es = full["energy_stencil"]
+    perm = np.random.default_rng(0).permutation(es["num_samples"])
+    shuffled = {**full, "energy_stencil": {**es, **{k: es[k][perm] for k in es
+                                                   if k[:2] in ("gc", "gn", "s0", "s1")}}}
+    out = []
+    for ctx in (comp, full, shuffled):
+        s = gpu.CppStructuredSweepSession(ctx, g.structured(), g.X_flat(), device="cuda:0")
+        E, M = s.run(3, report_every=1)
+        out.append((s.get_X(), E, M, s.info()))
+    for a, b in zip(out[0][:3], out[1][:3]):
+        np.testing.assert_array_equal(a, b)
+    np.testing.assert_array_equal(out[0][0], out[2][0])
+    np.testing.assert_allclose(out[2][1], out[0][1], rtol=1e-12)
+    np.testing.assert_array_equal(out[2][2], out[0][2])
