@@ -147,6 +147,9 @@ struct LevelData {
     // the coarsest FAS level of a mixed-precision session sweeps its
     // interior with the fp64 kernels (tiles of the first fp64 variant)
     bool fp64_tiles = false;
+    // interior-kernel variant of a coarse FAS level, tuned on the level's
+    // own data (-1: the session's variant)
+    int variant = -1;
     int64_t n_stored = 0;
     DevBuf<int32_t> st_slot, st_gc, st_gn0, st_gn1, st_gn2, st_role;
     DevBuf<int64_t> st_off;
@@ -214,6 +217,7 @@ struct Session : LevelData {
 
     int variant = 0;
     bool tuned = false;
+    bool pinned_variant = false;  // set_variant: every level sweeps with S.variant
     double variant_ms[kNumVariants] = {};
     // energy stencil
     bool es_struct = false;
@@ -1417,11 +1421,12 @@ static void launch_interior(Session& S, LevelData& L, const double* xin, double*
         }
         return;
     }
+    const int var = L.variant >= 0 ? L.variant : S.variant;
 #define EGG_V3(T, C, i) \
     launch_tile3<T[i].ci, T[i].cj, T[i].ck, T[i].minb, KIND, C>(S, L, xin, xout, tau, delta, omega, gout)
     if (S.dim == 3) {
         if (S.prec == EGG_B200_PREC_FP64) {
-            switch (S.variant) {
+            switch (var) {
             case 0: EGG_V3(kVar3_64, double, 0); break;
             case 1: EGG_V3(kVar3_64, double, 1); break;
             case 2: EGG_V3(kVar3_64, double, 2); break;
@@ -1429,7 +1434,7 @@ static void launch_interior(Session& S, LevelData& L, const double* xin, double*
             default: EGG_V3(kVar3_64, double, 4); break;
             }
         } else {
-            switch (S.variant) {
+            switch (var) {
             case 0: EGG_V3(kVar3_32, float, 0); break;
             case 1: EGG_V3(kVar3_32, float, 1); break;
             case 2: EGG_V3(kVar3_32, float, 2); break;
@@ -1441,7 +1446,7 @@ static void launch_interior(Session& S, LevelData& L, const double* xin, double*
     }
 #undef EGG_V3
     if (S.prec == EGG_B200_PREC_FP64) {
-        switch (S.variant) {
+        switch (var) {
         case 0: launch_tile<kVar64[0].ci, kVar64[0].cj, kVar64[0].minb, KIND, double, kVar64[0].fd>(S, L, xin, xout, tau, delta, omega, gout); break;
         case 1: launch_tile<kVar64[1].ci, kVar64[1].cj, kVar64[1].minb, KIND, double, kVar64[1].fd>(S, L, xin, xout, tau, delta, omega, gout); break;
         case 2: launch_tile<kVar64[2].ci, kVar64[2].cj, kVar64[2].minb, KIND, double, kVar64[2].fd>(S, L, xin, xout, tau, delta, omega, gout); break;
@@ -1449,7 +1454,7 @@ static void launch_interior(Session& S, LevelData& L, const double* xin, double*
         default: launch_tile<kVar64[4].ci, kVar64[4].cj, kVar64[4].minb, KIND, double, kVar64[4].fd>(S, L, xin, xout, tau, delta, omega, gout); break;
         }
     } else {
-        switch (S.variant) {
+        switch (var) {
         case 0: launch_tile<kVar32[0].ci, kVar32[0].cj, kVar32[0].minb, KIND, float, kVar32[0].fd>(S, L, xin, xout, tau, delta, omega, gout); break;
         case 1: launch_tile<kVar32[1].ci, kVar32[1].cj, kVar32[1].minb, KIND, float, kVar32[1].fd>(S, L, xin, xout, tau, delta, omega, gout); break;
         case 2: launch_tile<kVar32[2].ci, kVar32[2].cj, kVar32[2].minb, KIND, float, kVar32[2].fd>(S, L, xin, xout, tau, delta, omega, gout); break;
@@ -2843,6 +2848,8 @@ int egg_b200_session_set_variant(egg_b200_session* s, int32_t variant)
         S.variant = variant;
         set_tiles(S, S, variant_shape(S, variant));
         S.tuned = true;
+        S.pinned_variant = true;
+        for (auto& L : S.levels) { L->variant = -1; }
     });
 }
 

@@ -123,3 +123,29 @@ def test_fas_agrees_with_jacobi_minimiser(gpu):
     Ej, _ = _session(gpu, g).run(600, omega=0.8)
     assert Ef[-1] <= Ej[-1] + 1e-8 * max(1.0, abs(Ej[-1])), (Ef[-1], Ej[-1])
 
+
+
+@pytest.mark.parametrize("make,prec", [(lambda: configs.unit_square(257, frac=0.3, seed=2), "mixed"),
+                                       (lambda: configs.sphere_in_cube(17, frac=0.15, seed=1), "fp64")],
+                         ids=["square257-mixed", "sphere17-fp64"])
+def test_fas_coarse_levels_tuned_per_level(gpu, make, prec):
+    """Coarse levels pick their own tile variant on their first smoothing;
+    the V-cycles then match a session whose variant is pinned on every level
+    up to the rounding of the kernel variants, and pinned sessions repeat
+    bit for bit."""
+    g = make()
+    a = _session(gpu, g, prec)
+    Ea, Ma = a.run_fas(3, nu_pre=2, nu_post=2, max_levels=4)
+    v = a.variants()["variant"]
+    runs = []
+    for _ in range(2):
+        b = _session(gpu, g, prec)
+        b.set_variant(v)
+        runs.append(b.run_fas(3, nu_pre=2, nu_post=2, max_levels=4))
+    np.testing.assert_array_equal(runs[0][0], runs[1][0])
+    np.testing.assert_array_equal(runs[0][1], runs[1][1])
+    tol = 1e-9 if prec == "fp64" else 1e-6  # fp32 coarse tiles round differently per variant
+    np.testing.assert_allclose(Ea, runs[0][0], rtol=tol)
+    np.testing.assert_allclose(Ma, runs[0][1], rtol=1e3 * tol)
+    Ea2, _ = a.run_fas(1, nu_pre=2, nu_post=2, max_levels=4)  # tuned levels are kept across calls
+    assert np.isfinite(Ea2).all() and Ea2[0] <= Ea[-1] + 1e-9 * abs(Ea[-1])
