@@ -9,10 +9,12 @@
 #include <pybind11/pybind11.h>
 #include <pybind11/stl.h>
 
+#include <algorithm>
 #include <cstdlib>
 #include <memory>
 #include <stdexcept>
 #include <string>
+#include <thread>
 #include <vector>
 
 namespace py = pybind11;
@@ -115,6 +117,31 @@ int64_t checked_num_nodes(const DArr& X, int d)
                               " coordinates per node); got " + std::to_string(buf.shape[0]) + ".");
     }
     return int64_t(buf.shape[0]) / d;
+}
+
+// Write one byte per page of every span, on up to 16 threads (spans of
+// 64 MiB or more are split), so later writes into them do not fault.
+void prefault(const std::vector<std::pair<char*, size_t>>& spans)
+{
+    constexpr size_t kChunk = size_t(64) << 20, kPage = 4096;
+    std::vector<std::pair<char*, size_t>> work;
+    size_t total = 0;
+    for (const auto& sp : spans) {
+        for (size_t a = 0; a < sp.second; a += kChunk) { work.emplace_back(sp.first + a, std::min(kChunk, sp.second - a)); }
+        total += sp.second;
+    }
+    const size_t hw = std::max(1u, std::thread::hardware_concurrency());
+    const size_t T = std::min({hw, size_t(16), std::max<size_t>(1, total >> 26)});
+    auto body = [&](size_t t) {
+        for (size_t i = t; i < work.size(); i += T) {
+            volatile char* p = work[i].first;
+            for (size_t o = 0; o < work[i].second; o += kPage) { p[o] = 0; }
+        }
+    };
+    std::vector<std::thread> th;
+    for (size_t t = 1; t < T; ++t) { th.emplace_back(body, t); }
+    body(0);
+    for (auto& x : th) { x.join(); }
 }
 
 struct PinnedBuf {
@@ -1529,14 +1556,17 @@ PYBIND11_MODULE(cpp_core, m)
           const py::ssize_t nd = sz[0], nr = sz[1], ns = sz[2];
           py::dict out;
           egg_b200_wire_out o {};
+          std::vector<std::pair<char*, size_t>> out_spans;
           auto iarr = [&](const char* key, py::ssize_t n) {
               py::array_t<int32_t> a(n);
               out[key] = a;
+              out_spans.emplace_back(reinterpret_cast<char*>(a.mutable_data()), size_t(n) * sizeof(int32_t));
               return a.mutable_data();
           };
           auto darr = [&](const char* key, py::ssize_t n) {
               py::array_t<double> a(n);
               out[key] = a;
+              out_spans.emplace_back(reinterpret_cast<char*>(a.mutable_data()), size_t(n) * sizeof(double));
               return a.mutable_data();
           };
           o.dof_idx = iarr("dof_idx", nd);
@@ -1572,6 +1602,9 @@ PYBIND11_MODULE(cpp_core, m)
           out["num_samples"] = ns;
           {
               py::gil_scoped_release nogil;
+              // Fresh arrays fault in their pages on first touch; touch them
+              // on several threads first, so the copies land in resident pages.
+              prefault(out_spans);
               rc = egg_b200_wire_download(w, &o);
           }
           check(rc);

@@ -42,6 +42,7 @@ from __future__ import annotations
 import numpy as np
 
 __all__ = [
+    "build_flat_context",
     "axis_bits",
     "role_table",
     "cell_corner_ids",
@@ -339,6 +340,91 @@ def _device_arrays(blocks, moving, stored, d: int, synth_interior: bool, energy_
     return core.wire_build(d, shapes, ids, moving.view(np.uint8),
                            None if stored is None else stored.view(np.uint8),
                            synth_interior=synth_interior, energy_arrays=energy_arrays, device=device)
+
+
+def build_flat_context(blocks, free_mask, dof_entities, d: int, *, w_inv, interface=None, curvature=None,
+                       directional=None, device: str = "auto") -> dict:
+    """Drop-in for the reference's ``egg.smoothing.flat_context.build_flat_context``
+    (``flat_context.py:136-346``; same arguments and result) whose index
+    arrays -- interior classification, the moving DOFs' membership rows
+    sorted by node, ``P_of`` and the energy stencil -- are built on the GPU
+    (``cpp_core.wire_build``).  The entity partitions and the soft-term
+    tables come from the reference's own packers
+    (``egg.geometry.entity_soa.group_entities_by_type``,
+    ``egg.smoothing.interface_c2.curvature_dof_table``,
+    ``egg.smoothing.directional.directional_dof_table`` /
+    ``directional_energy_table``), so the reference's ``egg`` package must
+    be importable.  ``free_mask`` marks every moving DOF, ``dof_entities``
+    maps constrained ones to their entity, as in the reference.  Interface
+    samples (the composed orthogonality term) are not built here and raise
+    ``NotImplementedError``; pass them to the reference builder."""
+    if interface is not None and len(interface) > 0:
+        raise NotImplementedError("build_flat_context (device): interface samples are not supported")
+    from egg.geometry.entity_soa import group_entities_by_type
+
+    blocks = [np.asarray(b) for b in blocks]
+    moving = np.asarray(free_mask, dtype=bool)
+    dd = d * d
+    w_inv = np.asarray(w_inv, dtype=np.float64)
+    uniform_w = w_inv.shape == (d, d)
+    w0 = w_inv if uniform_w else (w_inv[0] if len(w_inv) else np.eye(d))
+    synth_interior = bool(np.allclose(w0, w0[0, 0] * np.eye(d)) and (uniform_w or np.allclose(w_inv, w0)))
+    arr = _device_arrays(blocks, moving, None, d, synth_interior, True, device)
+    ns = int(arr["num_samples"])
+
+    def fields(pre: str, sid) -> dict:
+        out = {"gc": arr[pre + "gc"]}
+        for k in range(d):
+            out[f"gn{k}"] = arr[f"{pre}gn{k}"]
+            out[f"s{k}"] = arr[f"{pre}s{k}"]
+        out["W_inv"] = np.ascontiguousarray(w_inv.reshape(1, dd) if uniform_w else w_inv[sid].reshape(-1, dd))
+        return out
+
+    groups = []
+    dofs = arr["dof_idx"]
+    if dofs.size:
+        g = {
+            "D": int(dofs.size),
+            "role": arr["role"],
+            "dof_idx": dofs,
+            "P_of": arr["P_of"],
+            "interior_block": arr["interior_block"],
+            "interior_logical": arr["interior_logical"],
+            "entities": group_entities_by_type(dofs.astype(np.int64).tolist(), dof_entities, d=d),
+        }
+        g.update(fields("", arr["sid"]))
+        if curvature is not None and len(curvature) > 0:
+            from egg.smoothing.interface_c2 import curvature_dof_table
+
+            tab = curvature_dof_table(moving, curvature)
+            if tab:
+                g["curv_k"] = tab["curv_k"]
+                for key in ("curv_nodes", "curv_slot", "curv_weight"):
+                    g[key] = np.ascontiguousarray(tab[key].reshape(-1))
+        if directional is not None and directional.n > 0:
+            from egg.smoothing.directional import directional_dof_table
+
+            tab = directional_dof_table(moving, directional)
+            if tab:
+                g["dir_k"] = tab["dir_k"]
+                g["dir_eps"] = tab["dir_eps"]
+                for key in ("dir_nodes", "dir_slot", "dir_kind", "dir_ref", "dir_axis", "dir_weight"):
+                    g[key] = np.ascontiguousarray(tab[key].reshape(-1))
+        groups.append(g)
+    es = {"num_samples": ns}
+    es.update(fields("es_", np.arange(ns, dtype=np.int64)))
+    if directional is not None and directional.n > 0:
+        from egg.smoothing.directional import directional_energy_table
+
+        tab = directional_energy_table(directional)
+        if tab:
+            es["dir_num"] = tab["dir_num"]
+            es["dir_eps"] = tab["dir_eps"]
+            for key in ("dir_nodes", "dir_axis", "dir_ref"):
+                es[key] = np.ascontiguousarray(tab[key].reshape(-1))
+            es["dir_kind"] = tab["dir_kind"]
+            es["dir_weight"] = tab["dir_weight"]
+    return {"groups": groups, "energy_stencil": es}
 
 
 DIR_ARITY = {0: 2, 1: 3, 2: 2}  # parallel, line, stem; other kinds are reserved (arity 0)
