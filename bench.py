@@ -621,7 +621,7 @@ def main():
         "time_to_energy_tol": tte,
         "setup": setup,
     }
-    if not args.no_cpu_baseline:
+    if ws == 1 and not args.no_cpu_baseline:  # a reported baseline at N = 1 only
         line["cpu_baseline"] = cpu_baseline()
     if ws == 1 and not args.no_configs and args.only is None and args.n == N_SIDE:
         line["configs"] = side_configs(args, local)
