@@ -31,7 +31,9 @@ __host__ __device__ constexpr int bit3(int k) { return 4 >> k; }
 template <int TI, int TJ, int TK> struct Win3 {
     static constexpr int WI = TI + 2, WJ = TJ + 2, WK = TK + 2;
     static constexpr int N = WI * WJ * WK;
+    static constexpr int NC = (WI - 1) * (WJ - 1) * (WK - 1);  // cells of the window
     __device__ static int idx(int u, int v, int w) { return (u * WJ + v) * WK + w; }
+    __device__ static int cidx(int u, int v, int w) { return (u * (WJ - 1) + v) * (WK - 1) + w; }
 };
 
 template <int TI, int TJ, int TK> struct Tile3Shared {
@@ -96,6 +98,26 @@ template <class R> __device__ __forceinline__ bool below3(const R t[9], R det, R
     return !(det > R(0)) || det * det < thr * thr * n[0] * n[1] * n[2];
 }
 
+// Bit b set: sample b of the cell with base (bu, bv, bw) is inverted or
+// badly shaped (below3 at kBadCell), from the fp32 edge cache; the det is
+// formed as shared3 forms it (first cofactor row).
+template <int TI, int TJ, int TK>
+__device__ __forceinline__ unsigned cell_bad3(const float* __restrict__ fe, int bu, int bv, int bw)
+{
+    unsigned mask = 0u;
+#pragma unroll
+    for (int b = 0; b < 8; ++b) {
+        float t[9];
+        edges3f<TI, TJ, TK>(fe, bu, bv, bw, b, t);
+        const float c0 = t[4] * t[8] - t[5] * t[7];
+        const float c1 = t[5] * t[6] - t[3] * t[8];
+        const float c2 = t[3] * t[7] - t[4] * t[6];
+        const float D = t[0] * c0 + t[1] * c1 + t[2] * c2;
+        if (below3<float>(t, D, float(kBadCell))) { mask |= 1u << b; }
+    }
+    return mask;
+}
+
 template <int KIND, class R>
 __device__ __forceinline__ void sample3_shared(const double t64[9], double delta, Shared3<R>& S)
 {
@@ -129,8 +151,8 @@ __device__ __noinline__ float dmu3_guard64(const Tile3Shared<TI, TJ, TK>& sm, in
 }
 
 template <int TI, int TJ, int TK, int KIND, class R>
-__device__ bool dof3_update(const Tile3Shared<TI, TJ, TK>& sm, const float* __restrict__ fe, int ti, int tj, int tk,
-                            const double tau[3],
+__device__ bool dof3_update(const Tile3Shared<TI, TJ, TK>& sm, const float* __restrict__ fe,
+                            const uint8_t* __restrict__ cbad, int ti, int tj, int tk, const double tau[3],
                             double delta, double omega, double out[3], bool grad_only = false)
 {
     using W = Win3<TI, TJ, TK>;
@@ -141,6 +163,19 @@ __device__ bool dof3_update(const Tile3Shared<TI, TJ, TK>& sm, const float* __re
     R e0 = R(0), econst = R(0);
     R mdconst = R(INFINITY);
     const double none[3] = {0.0, 0.0, 0.0};
+    if constexpr (std::is_same_v<R, float>) {
+        // Every sample of the DOF's 8 cells is in its patch (4 move it, 4 do
+        // not).  If any is inverted or badly shaped the DOF relaxes in fp64;
+        // otherwise the samples that do not move it have positive dets and
+        // the fp32 accept test needs nothing else from them (it sums metric
+        // changes, and their min det cannot decide the sign of the trial min).
+        unsigned bad = 0u;
+#pragma unroll
+        for (int cell = 0; cell < 8; ++cell) {
+            bad |= cbad[W::cidx(ti + (cell >> 2), tj + ((cell >> 1) & 1), tk + (cell & 1))];
+        }
+        if (bad) { return false; }
+    } else {
     // Samples that do not move the DOF: constant energy and det.
 #pragma unroll 1
     for (int cell = 0; cell < 8; ++cell) {
@@ -159,12 +194,10 @@ __device__ bool dof3_update(const Tile3Shared<TI, TJ, TK>& sm, const float* __re
                 edges3<TI, TJ, TK>(sm, ti + ci, tj + cj, tk + ck, b, -1, none, t);
                 sample3_shared<KIND, R>(t, delta, S);
             }
-            if constexpr (std::is_same_v<R, float>) {
-                if (below3<float>(S.t, S.D, float(kBadCell))) { return false; }
-            }
             econst += mu3_from<R>(KIND, S);
             mdconst = fmin(mdconst, S.D);
         }
+    }
     }
     // Samples that move it: role r (0 corner, 1+k axis-k neighbour).
 #pragma unroll
@@ -183,9 +216,6 @@ __device__ bool dof3_update(const Tile3Shared<TI, TJ, TK>& sm, const float* __re
                 double t[9];
                 edges3<TI, TJ, TK>(sm, ti + ci, tj + cj, tk + ck, b, -1, none, t);
                 sample3_shared<KIND, R>(t, delta, S);
-            }
-            if constexpr (std::is_same_v<R, float>) {
-                if (below3<float>(S.t, S.D, float(kBadCell))) { return false; }
             }
             e0 += mu3_from<R>(KIND, S);
             R v[3];
@@ -361,6 +391,7 @@ __global__ void __launch_bounds__(TI* TJ* TK, MINB)
     using W = Win3<TI, TJ, TK>;
     __shared__ Tile3Shared<TI, TJ, TK> sm;
     __shared__ float fe[std::is_same_v<C, float> ? 9 * W::N : 1];  // fp32 forward edges (mixed)
+    __shared__ uint8_t cbad[std::is_same_v<C, float> ? W::NC : 1];  // per window cell: bad-sample bits (mixed)
     const Tile3 tile = tiles[blockIdx.x];
     const BlockInfo bi = blocks[tile.block];
     const int n0 = bi.n[0], n1 = bi.n[1], n2 = bi.n[2];
@@ -396,6 +427,14 @@ __global__ void __launch_bounds__(TI* TJ* TK, MINB)
             }
         }
         __syncthreads();
+        // each window cell's 8 samples checked once for the whole tile (a
+        // DOF's patch covers all 8 samples of its 8 cells); cells reaching
+        // past the block hold zero positions and are read by no DOF
+        for (int c = threadIdx.x; c < W::NC; c += NT) {
+            const int cu = c / ((W::WJ - 1) * (W::WK - 1)), cv = (c / (W::WK - 1)) % (W::WJ - 1), cw = c % (W::WK - 1);
+            cbad[c] = uint8_t(cell_bad3<TI, TJ, TK>(fe, cu, cv, cw));
+        }
+        __syncthreads();
     }
     const int ti = threadIdx.x / (TJ * TK), tj = (threadIdx.x / TK) % TJ, tk = threadIdx.x % TK;
     const int gi = tile.i0 + ti, gj = tile.j0 + tj, gk = tile.k0 + tk;
@@ -410,8 +449,8 @@ __global__ void __launch_bounds__(TI* TJ* TK, MINB)
     }
     double out[3];
     const bool go = grad_out != nullptr;
-    if (!dof3_update<TI, TJ, TK, KIND, C>(sm, fe, ti, tj, tk, tv, delta, omega, out, go)) {
-        dof3_update<TI, TJ, TK, KIND, double>(sm, nullptr, ti, tj, tk, tv, delta, omega, out, go);
+    if (!dof3_update<TI, TJ, TK, KIND, C>(sm, fe, cbad, ti, tj, tk, tv, delta, omega, out, go)) {
+        dof3_update<TI, TJ, TK, KIND, double>(sm, nullptr, nullptr, ti, tj, tk, tv, delta, omega, out, go);
     }
     double* dst = go ? grad_out : Xout;
     dst[3 * slot] = out[0];

@@ -105,3 +105,64 @@ def test_compact_wire_3d_matches_full(gpu):
     ea, _ = a.run(4, report_every=1)
     eb, _ = b.run(4, report_every=1)
     np.testing.assert_allclose(ea, eb, rtol=1e-13)
+
+
+def _sample_quality3(ids, X):
+    """Per cell and corner sample: det of its edge matrix and det^2 over the
+    product of its column norms squared (the kernels' shape test)."""
+    n0, n1, n2 = ids.shape
+    D = np.zeros((n0 - 1, n1 - 1, n2 - 1, 8))
+    Q = np.zeros_like(D)
+    for b in range(8):
+        o = ((b >> 2) & 1, (b >> 1) & 1, b & 1)
+        pc = X[ids[o[0]:o[0] + n0 - 1, o[1]:o[1] + n1 - 1, o[2]:o[2] + n2 - 1]]
+        cols = []
+        for ax in range(3):
+            nb = b ^ (4 >> ax)
+            q = ((nb >> 2) & 1, (nb >> 1) & 1, nb & 1)
+            s = -1.0 if b & (4 >> ax) else 1.0
+            cols.append(s * (X[ids[q[0]:q[0] + n0 - 1, q[1]:q[1] + n1 - 1, q[2]:q[2] + n2 - 1]] - pc))
+        T = np.stack(cols, axis=-1)
+        D[..., b] = np.linalg.det(T)
+        Q[..., b] = D[..., b] ** 2 / np.prod((T * T).sum(axis=-2), axis=-1)
+    return D, Q
+
+
+@pytest.mark.parametrize("phase,delta", [("barrier", 0.0), ("untangle", 1e-4)])
+def test_mixed_3d_bad_cell_dofs_relax_in_fp64(gpu, phase, delta):
+    """A 17^3 cube with +-0.3h noise holds 86 inverted or badly shaped
+    samples.  A DOF whose 8 cells hold one relaxes in fp64 (the tile's
+    per-cell masks send it there), so in every mixed kernel variant the DOFs
+    next to a clearly bad sample land exactly where the fp64 session puts
+    them; the variants agree with one another to rounding (the per-DOF code
+    is shared, only the tiling differs); and the whole first sweep stays
+    within 5e-5 h of fp64 on this tangled grid (the clean grids hold 1e-5 h)."""
+    g = configs.unit_cube(17, frac=0.3, seed=3)
+    ids = np.asarray(g.blocks[0])
+    D, Q = _sample_quality3(ids, g.X)
+    thr2 = 0.1 ** 2
+    clearly_bad = ((D <= 0.0) | (Q < 0.5 * thr2)).any(axis=-1)  # per cell
+    cb = np.zeros(ids.shape, dtype=bool)  # DOFs (interior nodes) touching such a cell
+    for o in np.ndindex(2, 2, 2):
+        cb[o[0]:o[0] + 16, o[1]:o[1] + 16, o[2]:o[2] + 16] |= clearly_bad
+    cb[0, :, :] = cb[-1, :, :] = cb[:, 0, :] = cb[:, -1, :] = cb[:, :, 0] = cb[:, :, -1] = False
+    nodes = ids[cb]
+    assert nodes.size > 20
+    h = _hmin(g)
+    first = None
+    for variant in range(5):
+        f = _session(gpu, g)
+        f.set_variant(variant)
+        f.run(1, phase=phase, delta=delta, omega=0.8)
+        Xf = f.get_X().reshape(-1, 3)
+        m = _session(gpu, g, precision="mixed")
+        m.set_variant(variant)
+        m.run(1, phase=phase, delta=delta, omega=0.8)
+        Xm = m.get_X().reshape(-1, 3)
+        # fp64 on both sides (the fp32 path would differ by ~1e-7 h or more)
+        np.testing.assert_allclose(Xm[nodes], Xf[nodes], rtol=0, atol=1e-10 * h)
+        assert np.abs(Xm - Xf).max() <= 5e-5 * h
+        if first is None:
+            first = Xm
+        else:  # same per-DOF code; instances may contract FMAs differently
+            np.testing.assert_allclose(Xm, first, rtol=0, atol=1e-12 * h)
